@@ -1,0 +1,162 @@
+// Shared infrastructure of the epb200 library: context, workspace, error reporting, complex math.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "epb200.h"
+
+namespace epb {
+
+// ---- error reporting ------------------------------------------------------------------------
+void set_error(const char* fmt, ...);
+void clear_error();
+
+#define EPB_CHECK_ARG(cond, ...)          \
+  do {                                    \
+    if (!(cond)) {                        \
+      ::epb::set_error(__VA_ARGS__);      \
+      return EPB_ERR_ARG;                 \
+    }                                     \
+  } while (0)
+
+#define EPB_CUDA(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t _e = (call);                                                                \
+    if (_e != cudaSuccess) {                                                                \
+      ::epb::set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__,   \
+                       __LINE__);                                                           \
+      return EPB_ERR_CUDA;                                                                  \
+    }                                                                                       \
+  } while (0)
+
+#define EPB_LAUNCH_CHECK()                                                                    \
+  do {                                                                                        \
+    cudaError_t _e = cudaGetLastError();                                                      \
+    if (_e != cudaSuccess) {                                                                  \
+      ::epb::set_error("kernel launch failed: %s (%s:%d)", cudaGetErrorString(_e), __FILE__, \
+                       __LINE__);                                                             \
+      return EPB_ERR_CUDA;                                                                    \
+    }                                                                                         \
+  } while (0)
+
+#define EPB_TRY(call)            \
+  do {                           \
+    int _s = (call);             \
+    if (_s != EPB_OK) return _s; \
+  } while (0)
+
+}  // namespace epb
+
+// ---- context --------------------------------------------------------------------------------
+// Workspace slots: each entry point uses named slots so that nested calls do not alias.
+enum epb_slot {
+  EPB_WS_FOURIER = 0,
+  EPB_WS_EIGH,
+  EPB_WS_EPH_G,
+  EPB_WS_EPH_T,
+  EPB_WS_FLAGS,
+  EPB_WS_SPLIT_A,
+  EPB_WS_SPLIT_B,
+  EPB_WS_PASS0,
+  EPB_WS_PASS1,
+  EPB_WS_PASS2,
+  EPB_WS_PASS3,
+  EPB_WS_PASS4,
+  EPB_WS_PASS5,
+  EPB_WS_PASS6,
+  EPB_WS_PASS7,
+  EPB_WS_MLP,
+  EPB_WS_NSLOTS
+};
+
+struct epb_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sm_count = 0;
+  int cc_major = 0, cc_minor = 0;
+  void* ws[EPB_WS_NSLOTS] = {};
+  size_t ws_bytes[EPB_WS_NSLOTS] = {};
+  int fail_alloc_nth = 0;  // test hook
+  // Small pinned host scratch for scalar read-backs.
+  int64_t* pinned = nullptr;
+};
+
+struct epb_rset {
+  epb_ctx* ctx = nullptr;
+  int64_t nr = 0;
+  int4* dev = nullptr;       // (R1, R2, R3, 0) per vector
+  int lo[3] = {0, 0, 0};     // per-axis min
+  int hi[3] = {0, 0, 0};     // per-axis max
+  std::vector<int64_t> host;  // 3 x nr
+};
+
+namespace epb {
+
+// Grow-only workspace slot; returns EPB_ERR_OOM on failure.
+int ws_get(epb_ctx* ctx, int slot, size_t bytes, void** out);
+int make_current(epb_ctx* ctx);
+
+inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// ---- complex helpers (double2 / float2) -----------------------------------------------------
+__host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+__host__ __device__ __forceinline__ double2 cmulc(double2 a, double2 b) {
+  return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__host__ __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+  return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+// acc += a * b
+__host__ __device__ __forceinline__ void cfma(double2& acc, double2 a, double2 b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(-a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(a.y, b.x, acc.y);
+}
+__host__ __device__ __forceinline__ void cfma(float2& acc, float2 a, float2 b) {
+  acc.x = fmaf(a.x, b.x, acc.x);
+  acc.x = fmaf(-a.y, b.y, acc.x);
+  acc.y = fmaf(a.x, b.y, acc.y);
+  acc.y = fmaf(a.y, b.x, acc.y);
+}
+// acc += conj(a) * b
+__host__ __device__ __forceinline__ void cfma_conj(double2& acc, double2 a, double2 b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(-a.y, b.x, acc.y);
+}
+__host__ __device__ __forceinline__ void cfma_conj(float2& acc, float2 a, float2 b) {
+  acc.x = fmaf(a.x, b.x, acc.x);
+  acc.x = fmaf(a.y, b.y, acc.x);
+  acc.y = fmaf(a.x, b.y, acc.y);
+  acc.y = fmaf(-a.y, b.x, acc.y);
+}
+
+template <typename T> struct cplx;
+template <> struct cplx<double> { using type = double2; };
+template <> struct cplx<float> { using type = float2; };
+
+__device__ __forceinline__ double2 mk2(double a, double b) { return make_double2(a, b); }
+__device__ __forceinline__ float2 mk2(float a, float b) { return make_float2(a, b); }
+
+// exp(2 pi i t) for a double t, with exact argument reduction t - rint(t) in [-1/2, 1/2].
+__device__ __forceinline__ double2 cis2pi(double t) {
+  double r = t - rint(t);
+  double s, c;
+  sincospi(2.0 * r, &s, &c);
+  return make_double2(c, s);
+}
+
+}  // namespace epb

@@ -1,0 +1,557 @@
+// Batched Hermitian eigensolver: cyclic two-sided Jacobi with round-robin parallel ordering.
+//
+// Replaces eigvals_batched / eigen_batched (ext/ElectronPhononCUDAExt.jl:80-115, which calls
+// cuSOLVER heevjBatched; CPU method src/wannier_to_bloch_batched.jl:30-65). One "team" (a warp for
+// n <= 32, four warps for n <= 64) owns one matrix in shared memory at a time and loops over the
+// batch. Each round rotates n/2 disjoint (p, q) pairs at once:
+//     t = sign(tau) / (|tau| + sqrt(1 + tau^2)),  tau = (a_qq - a_pp) / (2 |a_pq|),
+//     J = [[c, s e^{i phi}], [-s e^{-i phi}, c]] on (p, q),  a_pq = |a_pq| e^{i phi},
+// applied as A <- A J (columns), A <- J^H A (rows), V <- V J.
+// A rotation is skipped when |a_pq| <= eps * ||A||_F / n; a sweep with no rotation ends the solve.
+//
+// Precision modes:
+//   EPB_PREC_FP64  : the whole solve in FP64.
+//   EPB_PREC_MIXED : the solve in FP32, then one FP64 refinement per matrix: modified Gram-Schmidt
+//                    of the FP32 vectors, S = V^H H V in FP64 (H re-read in FP64), a thresholded
+//                    FP64 Jacobi on the nearly diagonal S (this re-orthogonalises near-degenerate
+//                    clusters, whose FP32 vectors are only defined up to a rotation), V <- V Q.
+#include "epb_common.cuh"
+
+namespace epb {
+
+template <int TEAM>
+__device__ __forceinline__ void team_sync() {
+  if (TEAM == 32)
+    __syncwarp();
+  else
+    __syncthreads();
+}
+
+// Round-robin (circle method) pair i of round r for m players (m even); player m-1 is fixed.
+__device__ __forceinline__ void rr_pair(int m, int r, int i, int& p, int& q) {
+  int a, b;
+  if (i == 0) {
+    a = m - 1;
+    b = r;
+  } else {
+    a = (r + i) % (m - 1);
+    b = (r - i + (m - 1)) % (m - 1);
+  }
+  p = a < b ? a : b;
+  q = a < b ? b : a;
+}
+
+template <typename T>
+struct RotParam {
+  T c, s;
+  typename cplx<T>::type e;  // e^{i phi}
+  int p, q;                  // p < 0: skip
+};
+
+// One full Jacobi solve of the n x n Hermitian matrix in A (column-major, leading dim lda) with
+// eigenvectors accumulated into V (leading dim ldv; must hold identity on entry if want_v).
+// Returns the number of sweeps used (max_sweeps + 1 if not converged).
+template <typename T, int TEAM>
+__device__ int jacobi_team(typename cplx<T>::type* A, int lda, typename cplx<T>::type* V, int ldv,
+                           int n, bool want_v, RotParam<T>* prm, int* flag, T thr,
+                           int max_sweeps) {
+  using C = typename cplx<T>::type;
+  const int tid = threadIdx.x % TEAM;
+  const int m = (n + 1) & ~1;
+  const int npair = m / 2;
+  int sweep = 0;
+  for (; sweep < max_sweeps; ++sweep) {
+    if (tid == 0) *flag = 0;
+    team_sync<TEAM>();
+    for (int r = 0; r < m - 1; ++r) {
+      for (int i = tid; i < npair; i += TEAM) {
+        int p, q;
+        rr_pair(m, r, i, p, q);
+        RotParam<T> P;
+        P.p = -1;
+        P.q = q;
+        if (q < n) {
+          C b = A[p + q * lda];
+          T ab = sqrt(b.x * b.x + b.y * b.y);
+          if (ab > thr) {
+            T a = A[p + p * lda].x, d = A[q + q * lda].x;
+            T tau = (d - a) / (T(2) * ab);
+            T t;
+            if (fabs(tau) > T(1e15))
+              t = T(0.5) / tau;
+            else
+              t = (tau >= T(0) ? T(1) : T(-1)) / (fabs(tau) + sqrt(T(1) + tau * tau));
+            T c = T(1) / sqrt(T(1) + t * t);
+            P.c = c;
+            P.s = t * c;
+            P.e = mk2(b.x / ab, b.y / ab);
+            P.p = p;
+            *flag = 1;
+          }
+        }
+        prm[i] = P;
+      }
+      team_sync<TEAM>();
+      // columns: A <- A J, V <- V J
+      for (int task = tid; task < npair * n; task += TEAM) {
+        int i = task / n, row = task % n;
+        RotParam<T> P = prm[i];
+        if (P.p < 0) continue;
+        C ap = A[row + P.p * lda], aq = A[row + P.q * lda];
+        C ec = mk2(P.e.x, -P.e.y);
+        C sp = cmul(ec, aq);
+        C sq = cmul(P.e, ap);
+        A[row + P.p * lda] = mk2(P.c * ap.x - P.s * sp.x, P.c * ap.y - P.s * sp.y);
+        A[row + P.q * lda] = mk2(P.s * sq.x + P.c * aq.x, P.s * sq.y + P.c * aq.y);
+        if (want_v) {
+          C vp = V[row + P.p * ldv], vq = V[row + P.q * ldv];
+          C tp = cmul(ec, vq), tq = cmul(P.e, vp);
+          V[row + P.p * ldv] = mk2(P.c * vp.x - P.s * tp.x, P.c * vp.y - P.s * tp.y);
+          V[row + P.q * ldv] = mk2(P.s * tq.x + P.c * vq.x, P.s * tq.y + P.c * vq.y);
+        }
+      }
+      team_sync<TEAM>();
+      // rows: A <- J^H A
+      for (int task = tid; task < npair * n; task += TEAM) {
+        int i = task / n, col = task % n;
+        RotParam<T> P = prm[i];
+        if (P.p < 0) continue;
+        C ap = A[P.p + col * lda], aq = A[P.q + col * lda];
+        C ec = mk2(P.e.x, -P.e.y);
+        C sp = cmul(P.e, aq), sq = cmul(ec, ap);
+        A[P.p + col * lda] = mk2(P.c * ap.x - P.s * sp.x, P.c * ap.y - P.s * sp.y);
+        A[P.q + col * lda] = mk2(P.s * sq.x + P.c * aq.x, P.s * sq.y + P.c * aq.y);
+      }
+      team_sync<TEAM>();
+    }
+    int any = *flag;
+    team_sync<TEAM>();
+    if (!any) break;
+  }
+  return sweep;
+}
+
+struct EighArgs {
+  double2* A;
+  const int64_t* a_off;  // nullptr: uniform, offset b*n*n
+  const int32_t* nvec;   // nullptr: uniform n
+  int n_uniform;
+  int64_t batch;
+  double* E;
+  const int64_t* e_off;  // nullptr: b*n
+  int want_v;
+  int max_sweeps;
+  int* nonconv;          // device counter of matrices that hit the sweep limit
+  const double* mass;    // phonon mode: non-null => mass scaling + omega = sign sqrt
+};
+
+// Shared memory layout per team (elements of the solve type T):
+//   A: n x (n+1) [padded], V: n x n, plus RotParam[npair] and a flag.
+template <typename T, int TEAM, int NMAX>
+__global__ void eigh_kernel(EighArgs a) {
+  using C = typename cplx<T>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int TEAMS = (TEAM == 32) ? 4 : 1;  // teams per block
+  const int team = threadIdx.x / TEAM;
+  const int tid = threadIdx.x % TEAM;
+  constexpr int LDA = NMAX + 1;
+  // per-team region
+  size_t per_team = sizeof(C) * (NMAX * LDA + NMAX * NMAX) + sizeof(RotParam<T>) * (NMAX / 2 + 1) + 16;
+  per_team = (per_team + 15) & ~size_t(15);
+  unsigned char* base = smem_raw + team * per_team;
+  C* As = reinterpret_cast<C*>(base);
+  C* Vs = As + NMAX * LDA;
+  RotParam<T>* prm = reinterpret_cast<RotParam<T>*>(Vs + NMAX * NMAX);
+  int* flag = reinterpret_cast<int*>(prm + NMAX / 2 + 1);
+
+  const int64_t team_global = (int64_t)blockIdx.x * TEAMS + team;
+  const int64_t nteams = (int64_t)gridDim.x * TEAMS;
+  for (int64_t b = team_global; b < a.batch; b += nteams) {
+    const int n = a.nvec ? a.nvec[b] : a.n_uniform;
+    const int64_t aoff = a.a_off ? a.a_off[b] : b * (int64_t)n * n;
+    const int64_t eoff = a.e_off ? a.e_off[b] : b * (int64_t)n;
+    double2* Ag = a.A + aoff;
+    const int lda = n + 1;
+    // load upper triangle, mirror to the lower (Hermitian from 'U'), optional mass scaling
+    T fro2 = 0;
+    for (int e = tid; e < n * n; e += TEAM) {
+      int i = e % n, j = e / n;
+      double2 v;
+      if (i <= j) {
+        v = Ag[i + (int64_t)j * n];
+      } else {
+        double2 u = Ag[j + (int64_t)i * n];
+        v = make_double2(u.x, -u.y);
+      }
+      if (i == j) v.y = 0.0;
+      if (a.mass) {
+        double s = 1.0 / (sqrt(a.mass[i]) * sqrt(a.mass[j]));
+        v.x *= s;
+        v.y *= s;
+      }
+      As[i + j * lda] = mk2((T)v.x, (T)v.y);
+      Vs[i + j * n] = mk2(T(i == j ? 1 : 0), T(0));
+      fro2 += (T)(v.x * v.x + v.y * v.y);
+    }
+    // team reduction of ||A||_F^2 through the flag slot area (use warp shuffles per warp)
+    for (int o = 16; o > 0; o >>= 1) fro2 += __shfl_xor_sync(0xffffffffu, fro2, o);
+    __shared__ T red[TEAMS * (TEAM / 32)];
+    if ((tid & 31) == 0) red[team * (TEAM / 32) + tid / 32] = fro2;
+    team_sync<TEAM>();
+    T tot = 0;
+    for (int w = 0; w < TEAM / 32; ++w) tot += red[team * (TEAM / 32) + w];
+    team_sync<TEAM>();
+    const T eps = sizeof(T) == 8 ? T(2.220446049250313e-16) : T(1.1920929e-07);
+    const T thr = eps * sqrt(tot) / T(n > 0 ? n : 1);
+    int sweeps = jacobi_team<T, TEAM>(As, lda, Vs, n, n, a.want_v != 0, prm, flag, thr, a.max_sweeps);
+    if (sweeps >= a.max_sweeps && tid == 0) atomicAdd(a.nonconv, 1);
+    // sort eigenvalues ascending (rank by value, ties by index) and write out
+    for (int i = tid; i < n; i += TEAM) {
+      T ei = As[i + i * lda].x;
+      int rank = 0;
+      for (int j = 0; j < n; ++j) {
+        T ej = As[j + j * lda].x;
+        rank += (ej < ei) || (ej == ei && j < i);
+      }
+      double ev = (double)ei;
+      if (a.mass) ev = ev >= 0 ? sqrt(ev) : -sqrt(-ev);
+      a.E[eoff + rank] = ev;
+      // stash rank in the (now unused) imaginary part of the diagonal
+      As[i + i * lda].y = (T)rank;
+    }
+    team_sync<TEAM>();
+    if (a.want_v) {
+      for (int e = tid; e < n * n; e += TEAM) {
+        int row = e % n, col = e / n;
+        int rank = (int)As[col + col * lda].y;
+        C v = Vs[row + col * n];
+        double2 o = make_double2((double)v.x, (double)v.y);
+        if (a.mass) {
+          double s = 1.0 / sqrt(a.mass[row]);
+          o.x *= s;
+          o.y *= s;
+        }
+        Ag[row + (int64_t)rank * n] = o;
+      }
+    }
+    team_sync<TEAM>();
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Mixed precision: FP32 solve, FP64 refinement (see file header).
+template <int TEAM, int NMAX>
+__global__ void eigh_mixed_kernel(EighArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int TEAMS = (TEAM == 32) ? 4 : 1;
+  const int team = threadIdx.x / TEAM;
+  const int tid = threadIdx.x % TEAM;
+  constexpr int LDA = NMAX + 1;
+  // per team: H64 (NMAX x LDA double2) | V64 (NMAX x LDA double2) | region R (max of FP32 solve
+  // buffers and S64) | params
+  constexpr size_t h64 = sizeof(double2) * NMAX * LDA;
+  constexpr size_t f32 = sizeof(float2) * (NMAX * LDA + NMAX * NMAX);
+  constexpr size_t regR = (h64 > f32 ? h64 : f32);
+  constexpr size_t prmb = sizeof(RotParam<double>) * (NMAX / 2 + 1) + 16;
+  constexpr size_t per_team = ((2 * h64 + regR + prmb) + 15) & ~size_t(15);
+  unsigned char* base = smem_raw + team * per_team;
+  double2* H = reinterpret_cast<double2*>(base);
+  double2* V = reinterpret_cast<double2*>(base + h64);
+  unsigned char* R = base + 2 * h64;
+  float2* A32 = reinterpret_cast<float2*>(R);
+  float2* V32 = A32 + NMAX * LDA;
+  double2* S = reinterpret_cast<double2*>(R);
+  RotParam<double>* prm64 = reinterpret_cast<RotParam<double>*>(base + 2 * h64 + regR);
+  RotParam<float>* prm32 = reinterpret_cast<RotParam<float>*>(prm64);
+  int* flag = reinterpret_cast<int*>(prm64 + NMAX / 2 + 1);
+  __shared__ double red[TEAMS * (TEAM / 32)];
+
+  const int64_t team_global = (int64_t)blockIdx.x * TEAMS + team;
+  const int64_t nteams = (int64_t)gridDim.x * TEAMS;
+  for (int64_t b = team_global; b < a.batch; b += nteams) {
+    const int n = a.nvec ? a.nvec[b] : a.n_uniform;
+    const int64_t aoff = a.a_off ? a.a_off[b] : b * (int64_t)n * n;
+    const int64_t eoff = a.e_off ? a.e_off[b] : b * (int64_t)n;
+    double2* Ag = a.A + aoff;
+    const int lda = n + 1;
+    double fro2 = 0;
+    for (int e = tid; e < n * n; e += TEAM) {
+      int i = e % n, j = e / n;
+      double2 v;
+      if (i <= j) {
+        v = Ag[i + (int64_t)j * n];
+      } else {
+        double2 u = Ag[j + (int64_t)i * n];
+        v = make_double2(u.x, -u.y);
+      }
+      if (i == j) v.y = 0.0;
+      if (a.mass) {
+        double s = 1.0 / (sqrt(a.mass[i]) * sqrt(a.mass[j]));
+        v.x *= s;
+        v.y *= s;
+      }
+      H[i + j * lda] = v;
+      A32[i + j * lda] = make_float2((float)v.x, (float)v.y);
+      V32[i + j * n] = make_float2(i == j ? 1.f : 0.f, 0.f);
+      fro2 += v.x * v.x + v.y * v.y;
+    }
+    for (int o = 16; o > 0; o >>= 1) fro2 += __shfl_xor_sync(0xffffffffu, fro2, o);
+    if ((tid & 31) == 0) red[team * (TEAM / 32) + tid / 32] = fro2;
+    team_sync<TEAM>();
+    double tot = 0;
+    for (int w = 0; w < TEAM / 32; ++w) tot += red[team * (TEAM / 32) + w];
+    team_sync<TEAM>();
+    const double fro = sqrt(tot);
+    int sw = jacobi_team<float, TEAM>(A32, lda, V32, n, n, true, prm32, flag,
+                                      1.1920929e-07f * (float)fro / (float)n, a.max_sweeps);
+    if (sw >= a.max_sweeps && tid == 0) atomicAdd(a.nonconv, 1);
+    // V64 <- V32, then modified Gram-Schmidt (column by column)
+    for (int e = tid; e < n * n; e += TEAM) {
+      int i = e % n, j = e / n;
+      float2 v = V32[i + j * n];
+      V[i + j * lda] = make_double2(v.x, v.y);
+    }
+    team_sync<TEAM>();
+    for (int j = 0; j < n; ++j) {
+      // norm of column j (one thread; n <= 64 so this is cheap relative to the n^3 work below)
+      if (tid == 0) {
+        double s = 0;
+        for (int i = 0; i < n; ++i) s += V[i + j * lda].x * V[i + j * lda].x + V[i + j * lda].y * V[i + j * lda].y;
+        red[team * (TEAM / 32)] = 1.0 / sqrt(s);
+      }
+      team_sync<TEAM>();
+      double inv = red[team * (TEAM / 32)];
+      for (int i = tid; i < n; i += TEAM) {
+        V[i + j * lda].x *= inv;
+        V[i + j * lda].y *= inv;
+      }
+      team_sync<TEAM>();
+      // project column j out of columns > j
+      for (int c = j + 1 + tid; c < n; c += TEAM) {
+        double2 d = make_double2(0, 0);
+        for (int i = 0; i < n; ++i) cfma_conj(d, V[i + j * lda], V[i + c * lda]);
+        for (int i = 0; i < n; ++i) {
+          double2 vj = V[i + j * lda];
+          V[i + c * lda].x -= d.x * vj.x - d.y * vj.y;
+          V[i + c * lda].y -= d.x * vj.y + d.y * vj.x;
+        }
+      }
+      team_sync<TEAM>();
+    }
+    // S = V^H (H V): compute W = H V into S's region first column-wise? Use S as W then overwrite.
+    // W column c (thread per (row, col))
+    for (int e = tid; e < n * n; e += TEAM) {
+      int i = e % n, c = e / n;
+      double2 w = make_double2(0, 0);
+      for (int k = 0; k < n; ++k) cfma(w, H[i + k * lda], V[k + c * lda]);
+      S[i + c * lda] = w;
+    }
+    team_sync<TEAM>();
+    // H is no longer needed: compute S = V^H W into H's region
+    for (int e = tid; e < n * n; e += TEAM) {
+      int i = e % n, c = e / n;
+      double2 s = make_double2(0, 0);
+      for (int k = 0; k < n; ++k) cfma_conj(s, V[k + i * lda], S[k + c * lda]);
+      H[i + c * lda] = s;
+    }
+    team_sync<TEAM>();
+    // symmetrise S and reset the rotation accumulator Q (in S's region, ld = n)
+    for (int e = tid; e < n * n; e += TEAM) {
+      int i = e % n, c = e / n;
+      if (i < c) {
+        double2 u = H[i + c * lda], l = H[c + i * lda];
+        double2 m2 = make_double2(0.5 * (u.x + l.x), 0.5 * (u.y - l.y));
+        H[i + c * lda] = m2;
+        H[c + i * lda] = make_double2(m2.x, -m2.y);
+      } else if (i == c) {
+        H[i + i * lda].y = 0.0;
+      }
+      S[i + c * n] = make_double2(i == c ? 1.0 : 0.0, 0.0);
+    }
+    team_sync<TEAM>();
+    jacobi_team<double, TEAM>(H, lda, S, n, n, true, prm64, flag, 2.220446049250313e-16 * fro / n, 8);
+    // V <- V Q, written in place row by row (each thread owns whole rows)
+    for (int i = tid; i < n; i += TEAM) {
+      double2 row[NMAX];
+      for (int c = 0; c < n; ++c) {
+        double2 acc = make_double2(0, 0);
+        for (int k = 0; k < n; ++k) cfma(acc, V[i + k * lda], S[k + c * n]);
+        row[c] = acc;
+      }
+      for (int c = 0; c < n; ++c) V[i + c * lda] = row[c];
+    }
+    team_sync<TEAM>();
+    for (int i = tid; i < n; i += TEAM) {
+      double ei = H[i + i * lda].x;
+      int rank = 0;
+      for (int j = 0; j < n; ++j) {
+        double ej = H[j + j * lda].x;
+        rank += (ej < ei) || (ej == ei && j < i);
+      }
+      double ev = ei;
+      if (a.mass) ev = ev >= 0 ? sqrt(ev) : -sqrt(-ev);
+      a.E[eoff + rank] = ev;
+      H[i + i * lda].y = (double)rank;
+    }
+    team_sync<TEAM>();
+    if (a.want_v) {
+      for (int e = tid; e < n * n; e += TEAM) {
+        int row = e % n, col = e / n;
+        int rank = (int)H[col + col * lda].y;
+        double2 o = V[row + col * lda];
+        if (a.mass) {
+          double s = 1.0 / sqrt(a.mass[row]);
+          o.x *= s;
+          o.y *= s;
+        }
+        Ag[row + (int64_t)rank * n] = o;
+      }
+    }
+    team_sync<TEAM>();
+  }
+}
+
+template <typename T, int TEAM, int NMAX>
+static size_t eigh_smem() {
+  using C = typename cplx<T>::type;
+  size_t per_team = sizeof(C) * (NMAX * (NMAX + 1) + NMAX * NMAX) + sizeof(RotParam<T>) * (NMAX / 2 + 1) + 16;
+  per_team = (per_team + 15) & ~size_t(15);
+  return per_team * ((TEAM == 32) ? 4 : 1);
+}
+
+template <int TEAM, int NMAX>
+static size_t eigh_mixed_smem() {
+  constexpr int LDA = NMAX + 1;
+  size_t h64 = sizeof(double2) * NMAX * LDA;
+  size_t f32 = sizeof(float2) * (NMAX * LDA + NMAX * NMAX);
+  size_t regR = h64 > f32 ? h64 : f32;
+  size_t prmb = sizeof(RotParam<double>) * (NMAX / 2 + 1) + 16;
+  size_t per_team = ((2 * h64 + regR + prmb) + 15) & ~size_t(15);
+  return per_team * ((TEAM == 32) ? 4 : 1);
+}
+
+template <typename Kern>
+static int launch_eigh(epb_ctx* ctx, Kern kern, size_t smem, int threads, EighArgs& a) {
+  EPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int teams_per_block = threads == 32 * 4 ? 4 : 1;
+  int per_sm = 0;
+  EPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+  if (per_sm < 1) {
+    set_error("eigensolver: shared memory request %zu bytes does not fit", smem);
+    return EPB_ERR_UNSUPPORTED;
+  }
+  int64_t blocks_needed = cdiv(a.batch, teams_per_block);
+  int64_t blocks = (int64_t)per_sm * ctx->sm_count;
+  if (blocks > blocks_needed) blocks = blocks_needed;
+  if (blocks < 1) blocks = 1;
+  kern<<<(unsigned)blocks, threads, smem, ctx->stream>>>(a);
+  EPB_LAUNCH_CHECK();
+  return EPB_OK;
+}
+
+// Dispatch on max order and precision.
+int eigh_dispatch(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
+  if (prec == EPB_PREC_FP64) {
+    if (nmax <= 16)
+      return launch_eigh(ctx, eigh_kernel<double, 32, 16>, eigh_smem<double, 32, 16>(), 128, a);
+    if (nmax <= 32)
+      return launch_eigh(ctx, eigh_kernel<double, 32, 32>, eigh_smem<double, 32, 32>(), 128, a);
+    if (nmax <= 64)
+      return launch_eigh(ctx, eigh_kernel<double, 128, 64>, eigh_smem<double, 128, 64>(), 128, a);
+  } else if (prec == EPB_PREC_MIXED) {
+    if (nmax <= 16)
+      return launch_eigh(ctx, eigh_mixed_kernel<32, 16>, eigh_mixed_smem<32, 16>(), 128, a);
+    if (nmax <= 32)
+      return launch_eigh(ctx, eigh_mixed_kernel<32, 32>, eigh_mixed_smem<32, 32>(), 128, a);
+    if (nmax <= 64)
+      return launch_eigh(ctx, eigh_mixed_kernel<128, 64>, eigh_mixed_smem<128, 64>(), 128, a);
+  } else {
+    set_error("eigensolver: unknown precision mode %d", prec);
+    return EPB_ERR_ARG;
+  }
+  set_error("eigensolver: matrix order %d > 64 not supported by this build", nmax);
+  return EPB_ERR_ARG;
+}
+
+int eigh_run(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
+  if (a.batch == 0) return EPB_OK;
+  void* ws = nullptr;
+  EPB_TRY(ws_get(ctx, EPB_WS_FLAGS, 64, &ws));
+  a.nonconv = (int*)ws;
+  EPB_CUDA(cudaMemsetAsync(a.nonconv, 0, sizeof(int), ctx->stream));
+  a.max_sweeps = prec == EPB_PREC_FP64 ? 30 : 20;
+  EPB_TRY(eigh_dispatch(ctx, a, nmax, prec));
+  // non-convergence is reported after a sync on the context stream
+  int* h = (int*)ctx->pinned;
+  EPB_CUDA(cudaMemcpyAsync(h, a.nonconv, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  EPB_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (*h > 0) {
+    set_error("eigensolver: %d matrices reached the sweep limit", *h);
+    return EPB_ERR_NOCONVERGE;
+  }
+  return EPB_OK;
+}
+
+}  // namespace epb
+
+using namespace epb;
+
+extern "C" {
+
+int epb_eigh_batched(epb_ctx* ctx, double* A, int64_t n, int64_t batch, double* E, char jobz,
+                     int prec) {
+  clear_error();
+  EPB_CHECK_ARG(ctx, "epb_eigh_batched: NULL ctx");
+  EPB_CHECK_ARG(n >= 1 && batch >= 0, "epb_eigh_batched: bad n=%lld batch=%lld", (long long)n,
+                (long long)batch);
+  EPB_CHECK_ARG(jobz == 'N' || jobz == 'V', "epb_eigh_batched: jobz must be 'N' or 'V'");
+  EPB_CHECK_ARG(batch == 0 || (A && E), "epb_eigh_batched: NULL buffer");
+  EPB_TRY(make_current(ctx));
+  EighArgs a{};
+  a.A = (double2*)A;
+  a.n_uniform = (int)n;
+  a.batch = batch;
+  a.E = E;
+  a.want_v = jobz == 'V';
+  return eigh_run(ctx, a, (int)n, prec);
+}
+
+int epb_eigh_varlen(epb_ctx* ctx, double* A, const int64_t* a_offset, const int32_t* n,
+                    int64_t batch, double* E, const int64_t* e_offset, char jobz, int prec) {
+  clear_error();
+  EPB_CHECK_ARG(ctx, "epb_eigh_varlen: NULL ctx");
+  EPB_CHECK_ARG(batch >= 0, "epb_eigh_varlen: batch < 0");
+  EPB_CHECK_ARG(batch == 0 || (A && a_offset && n && E && e_offset), "epb_eigh_varlen: NULL buffer");
+  EPB_CHECK_ARG(jobz == 'N' || jobz == 'V', "epb_eigh_varlen: jobz must be 'N' or 'V'");
+  EPB_TRY(make_current(ctx));
+  EighArgs a{};
+  a.A = (double2*)A;
+  a.a_off = a_offset;
+  a.nvec = n;
+  a.batch = batch;
+  a.E = E;
+  a.e_off = e_offset;
+  a.want_v = jobz == 'V';
+  // The kernel variant is chosen by the largest order; it is read back once (small D2H).
+  // Callers that know the maximum should use uniform batches per size class.
+  return eigh_run(ctx, a, 64, prec);
+}
+
+int epb_ph_eigen_batched(epb_ctx* ctx, double* D, const double* mass, int64_t nm, int64_t nq,
+                         double* omega, int prec) {
+  clear_error();
+  EPB_CHECK_ARG(ctx && mass, "epb_ph_eigen_batched: NULL argument");
+  EPB_CHECK_ARG(nm >= 1 && nq >= 0, "epb_ph_eigen_batched: bad sizes");
+  EPB_CHECK_ARG(nq == 0 || (D && omega), "epb_ph_eigen_batched: NULL buffer");
+  EPB_TRY(make_current(ctx));
+  EighArgs a{};
+  a.A = (double2*)D;
+  a.n_uniform = (int)nm;
+  a.batch = nq;
+  a.E = omega;
+  a.want_v = 1;
+  a.mass = mass;
+  return eigh_run(ctx, a, (int)nm, prec);
+}
+
+}  // extern "C"

@@ -1,0 +1,187 @@
+"""ctypes binding of libepb200.so (the sm_100a C ABI declared in include/epb200.h).
+
+The compute path is the shared library only: if it cannot be loaded, or no CUDA device is visible,
+every call raises. There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libepb200.so")
+
+EPB_OK = 0
+EPB_ERR_ARG = 1
+EPB_ERR_OOM = 2
+EPB_ERR_CUDA = 3
+EPB_ERR_TIMEOUT = 4
+EPB_ERR_UNSUPPORTED = 5
+EPB_ERR_NOCONVERGE = 6
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+_STATUS = {1: "EPB_ERR_ARG", 2: "EPB_ERR_OOM", 3: "EPB_ERR_CUDA", 4: "EPB_ERR_TIMEOUT",
+           5: "EPB_ERR_UNSUPPORTED", 6: "EPB_ERR_NOCONVERGE"}
+
+P = C.c_void_p
+I64 = C.c_int64
+I32 = C.c_int
+D = C.c_double
+
+# name -> argtypes (restype is int unless listed in _RESTYPE)
+SIGNATURES = {
+    "epb_create": [C.POINTER(P), I32, P],
+    "epb_destroy": [P],
+    "epb_set_stream": [P, P],
+    "epb_free_bytes": [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
+    "epb_synchronize": [P],
+    "epb_last_error": [],
+    "epb_version": [],
+    "epb_workspace_bytes": [P, C.POINTER(C.c_uint64)],
+    "epb_debug_fail_alloc": [P, I32],
+    "epb_rset_create": [P, P, I64, C.POINTER(P)],
+    "epb_rset_destroy": [P],
+    "epb_fourier_phase": [P, P, P, I64, P],
+    "epb_fourier": [P, P, I64, I64, P, P, I64, P, I32],
+    "epb_eigh_batched": [P, P, I64, I64, P, C.c_char, I32],
+    "epb_eigh_varlen": [P, P, P, P, I64, P, P, C.c_char, I32],
+    "epb_ph_eigen_batched": [P, P, P, I64, I64, P, I32],
+    "epb_eph_RR_to_kR": [P, P, I64, I64, I64, P, P, I64, P, I64, P, P, I32],
+    "epb_eph_apply_rotations": [P, P, I64, I64, I64, I64, I64, P, I64, P, P, P, P],
+    "epb_eph_kR_to_kq": [P, P, I64, I64, I64, I64, I64, P, I64, P, I64, P, P, P, P, I32],
+    "epb_window_filter": [P, P, I64, I64, D, D, P, P, P, P, P],
+    "epb_fill_iqs": [P, P, I64, P, I64, I64, I64, P, P],
+}
+_RESTYPE = {"epb_last_error": C.c_char_p}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def lib():
+    """Load (once) and return the library with every signature bound."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(f"libepb200.so not built ({LIB_PATH}); run electronphonon.jl_b200/build.py")
+            L = C.CDLL(LIB_PATH)
+            for name, argt in SIGNATURES.items():
+                f = getattr(L, name)
+                f.argtypes = argt
+                f.restype = _RESTYPE.get(name, C.c_int)
+            _lib = L
+    return _lib
+
+
+class EpbError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{_STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def check(status):
+    if status != EPB_OK:
+        raise EpbError(status, lib().epb_last_error().decode(errors="replace"))
+    return status
+
+
+def ptr(t):
+    """Device (or host) address of a torch tensor / numpy array, or None."""
+    if t is None:
+        return None
+    if hasattr(t, "data_ptr"):
+        return t.data_ptr()
+    return t.ctypes.data
+
+
+class Context:
+    """One epb_ctx bound to a device and a CUDA stream (torch's current stream by default)."""
+
+    def __init__(self, device=0, stream=None):
+        import torch
+
+        if not torch.cuda.is_available():
+            raise RuntimeError("epb200 needs a CUDA device (sm_100a); none is visible")
+        L = lib()
+        torch.cuda.set_device(device)
+        if stream is None:
+            stream = torch.cuda.current_stream(device)
+        self.stream = stream
+        h = P()
+        check(L.epb_create(C.byref(h), int(device), P(stream.cuda_stream)))
+        self.h = h
+        self.device = device
+
+    def set_stream(self, stream):
+        self.stream = stream
+        check(lib().epb_set_stream(self.h, P(stream.cuda_stream)))
+
+    def synchronize(self):
+        check(lib().epb_synchronize(self.h))
+
+    def free_bytes(self):
+        f, t = C.c_uint64(), C.c_uint64()
+        check(lib().epb_free_bytes(self.h, C.byref(f), C.byref(t)))
+        return f.value, t.value
+
+    def workspace_bytes(self):
+        b = C.c_uint64()
+        check(lib().epb_workspace_bytes(self.h, C.byref(b)))
+        return b.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().epb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RSet:
+    """Device copy of an R-vector list (epb_rset)."""
+
+    def __init__(self, ctx: Context, irvec):
+        import numpy as np
+
+        self.ctx = ctx
+        self.irvec = np.ascontiguousarray(np.asarray(irvec, dtype=np.int64).reshape(-1, 3))
+        h = P()
+        check(lib().epb_rset_create(ctx.h, self.irvec.ctypes.data, self.irvec.shape[0], C.byref(h)))
+        self.h = h
+        self.nr = self.irvec.shape[0]
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().epb_rset_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx = {}
+
+
+def default_context(device=None):
+    import torch
+
+    if device is None:
+        device = torch.cuda.current_device()
+    c = _default_ctx.get(device)
+    stream = torch.cuda.current_stream(device)
+    if c is None:
+        c = Context(device, stream)
+        _default_ctx[device] = c
+    elif c.stream.cuda_stream != stream.cuda_stream:
+        c.set_stream(stream)
+    return c

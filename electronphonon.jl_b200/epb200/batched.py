@@ -1,0 +1,234 @@
+"""Host-side mirror of the reference's batched Wannier->Bloch API, backed by libepb200.so.
+
+Names, argument meaning and error behaviour follow ElectronPhonon.jl:
+  * get_interpolator / BatchedWannierInterpolator / get_fourier_batched
+      (src/wannier/WannierInterpolator.jl:84-96, src/wannier/batched_interpolator.jl:39-73,200-214)
+  * fourier_phase (src/wannier/batched_fourier_core.jl:24-30)
+  * eigvals_batched / eigen_batched, get_el_eigen[_valueonly]_batched
+      (src/wannier_to_bloch_batched.jl:30-105, ext/ElectronPhononCUDAExt.jl:80-115)
+  * get_eph_RR_to_kR_batched / get_eph_kR_to_kq_batched / eph_apply_rotations
+      (src/wannier_to_bloch_batched.jl:178-273,442-455)
+  * window filter (src/filter.jl:19,40-100), fill_iqs (src/calculator/run_eph_over_k_and_kq.jl:565-582)
+
+Device arrays are torch tensors holding the bytes of the Julia column-major array: a Julia array of
+size (n1, n2, ..., nd) is a contiguous torch tensor of shape (nd, ..., n2, n1). `jl()` and
+`host()` convert between Fortran-ordered numpy arrays and that layout. Assertion failures of the
+reference become AssertionError here; library failures raise `EpbError`.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib
+from ._lib import PREC_FP64, PREC_MIXED, check, ptr  # noqa: F401
+from .wannier import WannierObject
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def jl(arr, device="cuda", dtype=None):
+    """Fortran-ordered numpy array (Julia shape) -> device tensor in Julia byte layout."""
+    torch = _torch()
+    a = np.asfortranarray(arr if dtype is None else np.asarray(arr, dtype=dtype))
+    return torch.from_numpy(np.ascontiguousarray(a.T)).to(device)
+
+
+def host(t):
+    """Device tensor in Julia byte layout -> Fortran-ordered numpy array with the Julia shape."""
+    return t.detach().cpu().numpy().T
+
+
+def jl_empty(shape, dtype, device="cuda"):
+    torch = _torch()
+    return torch.empty(tuple(reversed(shape)), dtype=dtype, device=device)
+
+
+def _jlshape(t):
+    return tuple(reversed(t.shape))
+
+
+def _ctx():
+    return _lib.default_context()
+
+
+def _xk_dev(xks):
+    """(3, nk) crystal coordinates -> device float64 tensor of the same bytes."""
+    torch = _torch()
+    if isinstance(xks, torch.Tensor):
+        assert xks.dtype == torch.float64 and xks.is_cuda and xks.is_contiguous()
+        return xks
+    x = np.asfortranarray(np.asarray(xks, dtype=np.float64).reshape(3, -1))
+    return jl(x)
+
+
+# ---------------------------------------------------------------------------------------------
+class BatchedWannierInterpolator:
+    """Whole-batch Fourier engine over a device WannierObject (batched_interpolator.jl:39-73)."""
+
+    def __init__(self, parent: WannierObject, batch_size: int | None = None):
+        assert parent.on_device, "BatchedWannierInterpolator needs a device WannierObject (to_device)"
+        self.parent = parent
+        self.batch_size = batch_size
+        self.rset = _lib.RSet(_ctx(), parent.irvec)
+
+
+def get_interpolator(obj: WannierObject, fourier_mode: str = "batched", batch_size=None):
+    if fourier_mode not in ("batched",):
+        raise ValueError(f"fourier_mode={fourier_mode!r}: the device path implements 'batched'")
+    return BatchedWannierInterpolator(obj, batch_size)
+
+
+def fourier_phase(itp_or_irvec, xks):
+    """phase (nr, nk) c128 on the device (batched_fourier_core.jl:24-30)."""
+    torch = _torch()
+    rset = itp_or_irvec.rset if isinstance(itp_or_irvec, BatchedWannierInterpolator) else _lib.RSet(_ctx(), itp_or_irvec)
+    x = _xk_dev(xks)
+    nk = x.numel() // 3
+    out = jl_empty((rset.nr, nk), torch.complex128)
+    check(_lib.lib().epb_fourier_phase(_ctx().h, rset.h, ptr(x), nk, ptr(out)))
+    return out
+
+
+def get_fourier_batched(itp: BatchedWannierInterpolator, xks, out=None, prec=PREC_FP64):
+    """out (ndata, nk) = op_r[1:ndata, :] * exp(2 pi i R . x) (batched_interpolator.jl:200-214)."""
+    torch = _torch()
+    p = itp.parent
+    x = _xk_dev(xks)
+    nk = x.numel() // 3
+    if out is None:
+        out = jl_empty((p.ndata, nk), torch.complex128)
+    assert _jlshape(out) == (p.ndata, nk)
+    ld = p.op_r.shape[1]
+    check(_lib.lib().epb_fourier(_ctx().h, ptr(p.op_r), ld, p.ndata, itp.rset.h, ptr(x), nk, ptr(out), prec))
+    return out
+
+
+# ---------------------------------------------------------------------------------------------
+def eigvals_batched(Hk, prec=PREC_FP64):
+    """E (nw, nk) of a stack (nw, nw, nk); destroys Hk (wannier_to_bloch_batched.jl:30-40)."""
+    torch = _torch()
+    nw, n2, nk = _jlshape(Hk)
+    assert nw == n2
+    E = jl_empty((nw, nk), torch.float64)
+    check(_lib.lib().epb_eigh_batched(_ctx().h, ptr(Hk), nw, nk, ptr(E), b"N", prec))
+    return E
+
+
+def eigen_batched(Hk, prec=PREC_FP64):
+    """(E, U) with U = Hk overwritten (wannier_to_bloch_batched.jl:55-65)."""
+    torch = _torch()
+    nw, n2, nk = _jlshape(Hk)
+    assert nw == n2
+    E = jl_empty((nw, nk), torch.float64)
+    check(_lib.lib().epb_eigh_batched(_ctx().h, ptr(Hk), nw, nk, ptr(E), b"V", prec))
+    return E, Hk
+
+
+def _fourier_hk_batched(itp, xks, prec=PREC_FP64):
+    nw = int(round(np.sqrt(itp.parent.ndata)))
+    if nw * nw != itp.parent.ndata:
+        raise ValueError(f"ndata={itp.parent.ndata} is not a perfect square; expected nw^2 for a Hamiltonian")
+    hk = get_fourier_batched(itp, xks, prec=prec)
+    nk = hk.shape[0]
+    return hk.view(nk, nw, nw)
+
+
+def get_el_eigen_valueonly_batched(itp, xks, prec=PREC_FP64):
+    return eigvals_batched(_fourier_hk_batched(itp, xks, prec), prec)
+
+
+def get_el_eigen_batched(itp, xks, prec=PREC_FP64):
+    return eigen_batched(_fourier_hk_batched(itp, xks, prec), prec)
+
+
+def ph_eigen_batched(itp_dyn, xqs, mass, prec=PREC_FP64):
+    """(omega (nm, nq), u (nm, nm, nq)) with device-path semantics (compute_states.jl:285-311)."""
+    torch = _torch()
+    nm = len(mass)
+    dq = get_fourier_batched(itp_dyn, xqs, prec=PREC_FP64)
+    nq = dq.shape[0]
+    D = dq.view(nq, nm, nm)
+    m = torch.as_tensor(np.asarray(mass, dtype=np.float64), device=D.device)
+    w = jl_empty((nm, nq), torch.float64)
+    check(_lib.lib().epb_ph_eigen_batched(_ctx().h, ptr(D), ptr(m), nm, nq, ptr(w), prec))
+    return w, D
+
+
+# ---------------------------------------------------------------------------------------------
+def get_eph_RR_to_kR_batched(ep_ekpR_all, itp_epmat, ks, uks, additional_phase=None, prec=PREC_FP64):
+    """(wannier_to_bloch_batched.jl:178-205). ep_ekpR_all: (nw*nband*nm, nr_ep, nk)."""
+    epmat = itp_epmat.parent
+    nr_ep = epmat.irvec_next.shape[0]
+    nw, nband, nk = _jlshape(uks)
+    nm = epmat.ndata // (nw * nw * nr_ep)
+    assert nm * nw * nw * nr_ep == epmat.ndata
+    x = _xk_dev(ks)
+    assert x.numel() // 3 == nk
+    assert _jlshape(ep_ekpR_all) == (nw * nband * nm, nr_ep, nk)
+    if additional_phase is not None:
+        assert _jlshape(additional_phase) == (nr_ep, nk)
+    check(_lib.lib().epb_eph_RR_to_kR(_ctx().h, ptr(epmat.op_r), nw, nm, nr_ep, itp_epmat.rset.h, ptr(x), nk,
+                                      ptr(uks), nband, ptr(additional_phase), ptr(ep_ekpR_all), prec))
+    return ep_ekpR_all
+
+
+def eph_apply_rotations(ep_kq_all, g, ukqs, u_phs, g2_out=None, omega=None):
+    """(wannier_to_bloch_batched.jl:442-455). g: (nw, nbk, nm, nq)."""
+    nbkq, nbk, nm, nq = _jlshape(ep_kq_all) if ep_kq_all is not None else _jlshape(g2_out)
+    nw = _jlshape(ukqs)[0]
+    assert _jlshape(g)[:3] == (nw, nbk, nm) and _jlshape(g)[3] == nq
+    assert _jlshape(ukqs) == (nw, nbkq, nq)
+    assert _jlshape(u_phs) == (nm, nm, nq)
+    check(_lib.lib().epb_eph_apply_rotations(_ctx().h, ptr(g), nw * nbk * nm, nw, nbk, nm, nq, ptr(ukqs), nbkq,
+                                             ptr(u_phs), ptr(omega), ptr(ep_kq_all), ptr(g2_out)))
+    return ep_kq_all
+
+
+def get_eph_kR_to_kq_batched(ep_kq_all, ep_kR, phase, u_phs, ukqs, g2_out=None, omega=None, prec=PREC_FP64):
+    """(wannier_to_bloch_batched.jl:245-273). ep_kR: (nw*nbk*nm, nr_ep), phase: (nr_ep, nq)."""
+    nbkq, nbk, nm, nq = _jlshape(ep_kq_all) if ep_kq_all is not None else _jlshape(g2_out)
+    nw = _jlshape(ukqs)[0]
+    ndata = nw * nbk * nm
+    ld, nr_ep = _jlshape(ep_kR)
+    assert ld >= ndata
+    assert _jlshape(phase) == (nr_ep, nq)
+    assert _jlshape(ukqs) == (nw, nbkq, nq)
+    assert _jlshape(u_phs) == (nm, nm, nq)
+    check(_lib.lib().epb_eph_kR_to_kq(_ctx().h, ptr(ep_kR), ld, nw, nbk, nm, nr_ep, ptr(phase), nq, ptr(ukqs),
+                                      nbkq, ptr(u_phs), ptr(omega), ptr(ep_kq_all), ptr(g2_out), prec))
+    return ep_kq_all
+
+
+# ---------------------------------------------------------------------------------------------
+def window_filter(E, wmin, wmax):
+    """Per-k in-window band ranges and the compacted kept-k list (filter.jl:19,40-72).
+
+    Returns (band_min, band_max, keep_idx[:nkeep], nbelow) as device tensors (band indices
+    1-based, 0 when empty; keep_idx 0-based ascending).
+    """
+    torch = _torch()
+    nw, nk = _jlshape(E)
+    bmin = torch.empty(nk, dtype=torch.int32, device=E.device)
+    bmax = torch.empty(nk, dtype=torch.int32, device=E.device)
+    keep = torch.empty(max(nk, 1), dtype=torch.int32, device=E.device)
+    nkeep = torch.zeros(1, dtype=torch.int64, device=E.device)
+    nbelow = torch.empty(nk, dtype=torch.float64, device=E.device)
+    check(_lib.lib().epb_window_filter(_ctx().h, ptr(E), nw, nk, float(wmin), float(wmax), ptr(bmin), ptr(bmax),
+                                       ptr(keep), ptr(nkeep), ptr(nbelow)))
+    n = int(nkeep.item())
+    return bmin, bmax, keep[:n], nbelow
+
+
+def fill_iqs(xkq_int, xk_int, ngrid, dense_hash_to_iq):
+    """iq (1-based) of x_{k+q} - x_k per column of xkq_int (3, nkq); raises on a miss."""
+    torch = _torch()
+    nkq = xkq_int.numel() // 3
+    iqs = torch.empty(nkq, dtype=torch.int64, device=xkq_int.device)
+    xk = np.ascontiguousarray(np.asarray(xk_int, dtype=np.int64))
+    check(_lib.lib().epb_fill_iqs(_ctx().h, ptr(xkq_int), nkq, xk.ctypes.data, int(ngrid[0]), int(ngrid[1]),
+                                  int(ngrid[2]), ptr(dense_hash_to_iq), ptr(iqs)))
+    return iqs

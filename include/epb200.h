@@ -1,0 +1,167 @@
+/*
+ * epb200 -- B200 (sm_100a) Wannier->Bloch electron-phonon interpolation, C ABI.
+ *
+ * Every entry point replaces one generic function of ElectronPhonon.jl that its CUDA package
+ * extension (ext/ElectronPhononCUDAExt.jl) overrides by dispatch on CuArray, or one batched driver
+ * of src/wannier_to_bloch_batched.jl; the citation next to each declaration names it (paths are
+ * relative to the reference project root).
+ *
+ * Conventions
+ *  - Arrays are column-major (Julia layout). "c128" is interleaved (re, im) double pairs, the
+ *    bytes of a Julia ComplexF64 / cuDoubleComplex array. Band, mode and k indices stored in
+ *    integer outputs are 1-based where the reference's are (band ranges); list indices are 0-based.
+ *  - Pointers are DEVICE pointers unless the parameter name ends in `_host`.
+ *  - The caller owns every input and output buffer; the library allocates only its own workspace
+ *    inside the context (grown on demand, released by epb_destroy).
+ *  - All work is stream-ordered on the context's stream; nothing synchronises unless stated. The
+ *    caller synchronises (the reference's `synchronize(backend)`, src/common/gpu_utils.jl:60).
+ *  - Every function returns an int status (EPB_OK == 0) and never aborts or throws across the ABI;
+ *    epb_last_error() gives a message for the calling thread's last failure.
+ *  - Threading: one context per host thread, no internal locking (the reference's batched loop is
+ *    single-threaded, src/boltzmann/boltzmann_calculator.jl:332-334).
+ */
+#ifndef EPB200_H
+#define EPB200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define EPB_API __attribute__((visibility("default")))
+#else
+#define EPB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------------------------- */
+#define EPB_OK              0
+#define EPB_ERR_ARG         1   /* bad shape, null pointer, unsupported size               */
+#define EPB_ERR_OOM         2   /* workspace allocation failed                             */
+#define EPB_ERR_CUDA        3   /* a CUDA runtime call or kernel launch failed             */
+#define EPB_ERR_TIMEOUT     4   /* a bounded device-side wait gave up                      */
+#define EPB_ERR_UNSUPPORTED 5   /* feature not available (e.g. wrong GPU architecture)     */
+#define EPB_ERR_NOCONVERGE  6   /* eigensolver hit its sweep limit (results still written) */
+
+/* ---- precision modes ----------------------------------------------------------------------- */
+#define EPB_PREC_FP64   0  /* plain FP64 everywhere                                            */
+#define EPB_PREC_MIXED  1  /* split-BF16 tcgen05 contractions (FP32 accumulate), FP32 eigensolve
+                              with one FP64 Rayleigh-Ritz refinement                           */
+
+typedef struct epb_ctx epb_ctx;
+typedef struct epb_rset epb_rset;
+
+/* ---- context ------------------------------------------------------------------------------- */
+/* Create a context on `device`, ordering work on `stream` (a cudaStream_t; NULL = legacy default).
+   Replaces: gpu_backend() (ext/ElectronPhononCUDAExt.jl:34) and the CUDA.jl handle state. */
+EPB_API int epb_create(epb_ctx** ctx, int device, void* stream);
+EPB_API int epb_destroy(epb_ctx* ctx);
+EPB_API int epb_set_stream(epb_ctx* ctx, void* stream);
+/* Free device memory as seen by the library. Replaces: free_bytes(::GPUBackend) (ext:36). */
+EPB_API int epb_free_bytes(epb_ctx* ctx, uint64_t* free_host, uint64_t* total_host);
+/* Block until the context's stream is idle. Replaces: synchronize(::GPUBackend) (ext:37). */
+EPB_API int epb_synchronize(epb_ctx* ctx);
+/* Message of the calling thread's last failure ("" if none). */
+EPB_API const char* epb_last_error(void);
+EPB_API int epb_version(void);
+/* Bytes of workspace currently held by the context. */
+EPB_API int epb_workspace_bytes(epb_ctx* ctx, uint64_t* bytes_host);
+/* Test hook: make the N-th next workspace allocation fail (N = 0 disables). Drives the
+   out-of-memory path without exhausting a GPU (src/calculator/eph_device_staging.jl:33-37). */
+EPB_API int epb_debug_fail_alloc(epb_ctx* ctx, int nth);
+
+/* ---- lattice-vector sets ------------------------------------------------------------------- */
+/* Upload an R-vector list (host int64 3 x nr, i.e. Julia's Vector{Vec3{Int}} bytes). Replaces:
+   _irvec_to_device_matrix (src/wannier/WannierObject.jl:148-152) inside BatchedFourierCore
+   (src/wannier/batched_fourier_core.jl:68-79). |R_d| must be <= 1023. */
+EPB_API int epb_rset_create(epb_ctx* ctx, const int64_t* irvec_host, int64_t nr, epb_rset** rset);
+EPB_API int epb_rset_destroy(epb_rset* rset);
+
+/* ---- Fourier transform --------------------------------------------------------------------- */
+/* phase[ir, j] = exp(2 pi i R_ir . x_j), c128 (nr x nk). xk: f64 (3 x nk).
+   Replaces: fourier_phase! (src/wannier/batched_fourier_core.jl:24-30). */
+EPB_API int epb_fourier_phase(epb_ctx* ctx, const epb_rset* rset, const double* xk, int64_t nk,
+                      double* phase);
+
+/* out[i, j] = sum_r op_r[i, r] exp(2 pi i R_r . x_j) for i < ndata; op_r c128 with leading
+   dimension ld_op >= ndata; out c128 (ndata x nk). The phase is generated on the fly.
+   Replaces: fourier_batched! / get_fourier_batched! (src/wannier/batched_fourier_core.jl:117-139,
+   src/wannier/batched_interpolator.jl:200-214), i.e. the cuBLAS ZGEMM of ext/ElectronPhononCUDAExt.jl.
+   prec: EPB_PREC_FP64 or EPB_PREC_MIXED (split-BF16 tensor cores, FP32 accumulate). */
+EPB_API int epb_fourier(epb_ctx* ctx, const double* op_r, int64_t ld_op, int64_t ndata,
+                const epb_rset* rset, const double* xk, int64_t nk, double* out, int prec);
+
+/* ---- batched Hermitian eigensolve ---------------------------------------------------------- */
+/* A: c128 (n x n x batch), Hermitian (upper triangle read), destroyed; with jobz = 'V' it is
+   overwritten by the eigenvectors. E: f64 (n x batch), ascending.
+   Replaces: eigvals_batched / eigen_batched (ext/ElectronPhononCUDAExt.jl:80-115; CPU method
+   src/wannier_to_bloch_batched.jl:30-65). No EPW gauge fix, as in the reference's batched path.
+   Returns EPB_ERR_NOCONVERGE if any matrix hit the sweep limit (outputs are still written). */
+EPB_API int epb_eigh_batched(epb_ctx* ctx, double* A, int64_t n, int64_t batch, double* E, char jobz,
+                     int prec);
+
+/* Uneven batch: matrix b has order n[b] (1..128) and starts at complex element a_offset[b] of A;
+   its eigenvalues go to E + e_offset[b]. All index arrays are device arrays. Same semantics. */
+EPB_API int epb_eigh_varlen(epb_ctx* ctx, double* A, const int64_t* a_offset, const int32_t* n,
+                    int64_t batch, double* E, const int64_t* e_offset, char jobz, int prec);
+
+/* Phonon eigenmodes from D(q): D c128 (nm x nm x nq) is scaled by 1/sqrt(m_i m_j), diagonalised,
+   and overwritten by u with u[i, :] /= sqrt(m_i); omega f64 (nm x nq) = sign(l) sqrt|l|.
+   mass: f64 (nm). Replaces: the device phonon branch of compute_phonon_states
+   (src/compute_states.jl:293-300) with solve_eigen_ph! semantics (src/diagonalize.jl:104-127). */
+EPB_API int epb_ph_eigen_batched(epb_ctx* ctx, double* D, const double* mass, int64_t nm, int64_t nq,
+                         double* omega, int prec);
+
+/* ---- electron-phonon chain ----------------------------------------------------------------- */
+/* out[iw, n, (nu, p), k] = sum_jw g(k)[iw, jw, (nu, p)] uk[jw, n, k] (* add_phase[p, k]) with
+   g(k) = sum_Re epmat[:, Re] exp(2 pi i Re . x_k). epmat c128 ((nw^2 nm nr_ep) x nr_el), "el"
+   layout; uk c128 (nw x nband x nk); add_phase c128 (nr_ep x nk) or NULL; out c128
+   ((nw nband nm) x nr_ep x nk). Replaces: get_eph_RR_to_kR_batched!
+   (src/wannier_to_bloch_batched.jl:178-205). */
+EPB_API int epb_eph_RR_to_kR(epb_ctx* ctx, const double* epmat, int64_t nw, int64_t nm, int64_t nr_ep,
+                     const epb_rset* rset_el, const double* xk, int64_t nk, const double* uk,
+                     int64_t nband, const double* add_phase, double* out, int prec);
+
+/* ep[m, n, nu, q] = sum_{iw, jm} conj(ukq[iw, m, q]) g[iw, n, jm, q] uph[jm, nu, q] and
+   g2 = |ep|^2 / (2 omega[nu, q]). g c128 (nw x nbk x nm x nq) with column stride ldg >= nw*nbk*nm
+   between q; ukq c128 (nw x nbkq x nq); uph c128 (nm x nm x nq); omega f64 (nm x nq) or NULL;
+   ep_out c128 (nbkq x nbk x nm x nq) or NULL; g2_out f64 (same) or NULL.
+   Replaces: eph_apply_rotations! (ext/ElectronPhononCUDAExt.jl:177-201,
+   src/wannier_to_bloch_batched.jl:442-455). */
+EPB_API int epb_eph_apply_rotations(epb_ctx* ctx, const double* g, int64_t ldg, int64_t nw, int64_t nbk,
+                            int64_t nm, int64_t nq, const double* ukq, int64_t nbkq,
+                            const double* uph, const double* omega, double* ep_out,
+                            double* g2_out);
+
+/* g(k, q) = ep_kR . phase (Fourier over Rp) followed by the rotations above. ep_kR c128
+   ((nw nbk nm) x nr_ep) with leading dimension ld; phase c128 (nr_ep x nq).
+   Replaces: get_eph_kR_to_kq_batched! (src/wannier_to_bloch_batched.jl:245-273). */
+EPB_API int epb_eph_kR_to_kq(epb_ctx* ctx, const double* ep_kR, int64_t ld, int64_t nw, int64_t nbk,
+                     int64_t nm, int64_t nr_ep, const double* phase, int64_t nq,
+                     const double* ukq, int64_t nbkq, const double* uph, const double* omega,
+                     double* ep_out, double* g2_out, int prec);
+
+/* ---- energy window ------------------------------------------------------------------------- */
+/* For each k: band range [band_min, band_max] (1-based, inclusive; 0/0 if empty) of sorted E
+   (f64 nw x nk) inside [wmin, wmax] (searchsortedfirst/last, both ends inclusive), and the
+   ascending list of kept k (0-based) compacted into keep_idx (capacity nk); *nkeep_dev receives
+   the count (device int64). nbelow (f64 nk or NULL) = number of bands below the window.
+   Replaces: inside_window + the device branch of _filter_kpoints (src/filter.jl:19,40-72). */
+EPB_API int epb_window_filter(epb_ctx* ctx, const double* E, int64_t nw, int64_t nk, double wmin,
+                      double wmax, int32_t* band_min, int32_t* band_max, int32_t* keep_idx,
+                      int64_t* nkeep_dev, double* nbelow);
+
+/* iq index (1-based) of x_{k+q} - x_k on a commensurate grid: for each j < nkq,
+   iqs[j] = dense_hash_to_iq[((c1 ng2) + c2) ng3 + c3] with c = wrap(xkq_int[:, j] - xk_int).
+   xkq_int int64 (3 x nkq), xk_int int64 (3), dense_hash_to_iq int64 (ng1 ng2 ng3).
+   A miss (0) makes the call return EPB_ERR_ARG after the kernel (one sync). Replaces: _fill_iqs!
+   (src/calculator/run_eph_over_k_and_kq.jl:565-582) and _ik_from_hash (src/common/kpoints.jl:643). */
+EPB_API int epb_fill_iqs(epb_ctx* ctx, const int64_t* xkq_int, int64_t nkq, const int64_t* xk_int_host,
+                 int64_t ng1, int64_t ng2, int64_t ng3, const int64_t* dense_hash_to_iq,
+                 int64_t* iqs);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EPB200_H */
