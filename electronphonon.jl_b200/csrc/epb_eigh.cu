@@ -142,6 +142,7 @@ struct EighArgs {
   int want_v;
   int max_sweeps;
   int* nonconv;          // device counter of matrices that hit the sweep limit
+  int* badsize;          // device counter of matrices whose order exceeds the kernel's maximum
   const double* mass;    // phonon mode: non-null => mass scaling + omega = sign sqrt
 };
 
@@ -168,6 +169,10 @@ __global__ void eigh_kernel(EighArgs a) {
   const int64_t nteams = (int64_t)gridDim.x * TEAMS;
   for (int64_t b = team_global; b < a.batch; b += nteams) {
     const int n = a.nvec ? a.nvec[b] : a.n_uniform;
+    if (n < 1 || n > NMAX) {  // order outside this kernel's shared-memory plan: skip, report
+      if (tid == 0) atomicAdd(a.badsize, 1);
+      continue;
+    }
     const int64_t aoff = a.a_off ? a.a_off[b] : b * (int64_t)n * n;
     const int64_t eoff = a.e_off ? a.e_off[b] : b * (int64_t)n;
     double2* Ag = a.A + aoff;
@@ -270,6 +275,10 @@ __global__ void eigh_mixed_kernel(EighArgs a) {
   const int64_t nteams = (int64_t)gridDim.x * TEAMS;
   for (int64_t b = team_global; b < a.batch; b += nteams) {
     const int n = a.nvec ? a.nvec[b] : a.n_uniform;
+    if (n < 1 || n > NMAX) {  // order outside this kernel's shared-memory plan: skip, report
+      if (tid == 0) atomicAdd(a.badsize, 1);
+      continue;
+    }
     const int64_t aoff = a.a_off ? a.a_off[b] : b * (int64_t)n * n;
     const int64_t eoff = a.e_off ? a.e_off[b] : b * (int64_t)n;
     double2* Ag = a.A + aoff;
@@ -478,13 +487,18 @@ int eigh_run(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
   void* ws = nullptr;
   EPB_TRY(ws_get(ctx, EPB_WS_FLAGS, 64, &ws));
   a.nonconv = (int*)ws;
-  EPB_CUDA(cudaMemsetAsync(a.nonconv, 0, sizeof(int), ctx->stream));
+  a.badsize = a.nonconv + 1;
+  EPB_CUDA(cudaMemsetAsync(a.nonconv, 0, 2 * sizeof(int), ctx->stream));
   a.max_sweeps = prec == EPB_PREC_FP64 ? 30 : 20;
   EPB_TRY(eigh_dispatch(ctx, a, nmax, prec));
   // non-convergence is reported after a sync on the context stream
   int* h = (int*)ctx->pinned;
-  EPB_CUDA(cudaMemcpyAsync(h, a.nonconv, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  EPB_CUDA(cudaMemcpyAsync(h, a.nonconv, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   EPB_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (h[1] > 0) {
+    set_error("eigensolver: %d matrices have an order outside 1..%d (skipped)", h[1], nmax);
+    return EPB_ERR_ARG;
+  }
   if (*h > 0) {
     set_error("eigensolver: %d matrices reached the sweep limit", *h);
     return EPB_ERR_NOCONVERGE;
