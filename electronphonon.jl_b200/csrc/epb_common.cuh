@@ -151,6 +151,13 @@ template <> struct cplx<float> { using type = float2; };
 __device__ __forceinline__ double2 mk2(double a, double b) { return make_double2(a, b); }
 __device__ __forceinline__ float2 mk2(float a, float b) { return make_float2(a, b); }
 
+// R . x evaluated as (R1 x1 + R2 x2) + R3 x3 with every product and sum rounded separately (no FMA
+// contraction), i.e. the same rounding as the reference's broadcast in fourier_phase!
+// (src/wannier/batched_fourier_core.jl:26-28).
+__device__ __forceinline__ double rdotx(int r1, int r2, int r3, double x1, double x2, double x3) {
+  return __dadd_rn(__dadd_rn(__dmul_rn((double)r1, x1), __dmul_rn((double)r2, x2)), __dmul_rn((double)r3, x3));
+}
+
 // exp(2 pi i t) for a double t, with exact argument reduction t - rint(t) in [-1/2, 1/2].
 __device__ __forceinline__ double2 cis2pi(double t) {
   double r = t - rint(t);

@@ -20,8 +20,7 @@ __global__ void phase_kernel(const int4* __restrict__ rv, int64_t nr, const doub
   if (idx >= total) return;
   int64_t ir = idx % nr, j = idx / nr;
   int4 r = rv[ir];
-  double t = ((double)r.x * xk[3 * j] + (double)r.y * xk[3 * j + 1]) + (double)r.z * xk[3 * j + 2];
-  phase[idx] = cis2pi(t);
+  phase[idx] = cis2pi(rdotx(r.x, r.y, r.z, xk[3 * j], xk[3 * j + 1], xk[3 * j + 2]));
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -101,8 +100,7 @@ __global__ void __launch_bounds__(F_THREADS, 2) fourier_f64_kernel(FourierArgs a
           v = cmul(cmul(p0, p1), p2);
         } else {
           const double* x = a.xk + 3 * col;
-          double t3 = ((double)r.x * x[0] + (double)r.y * x[1]) + (double)r.z * x[2];
-          v = cis2pi(t3);
+          v = cis2pi(rdotx(r.x, r.y, r.z, x[0], x[1], x[2]));
         }
       }
       Bs[(buf * F_BK + kk) * F_BN + jj] = v;
@@ -172,15 +170,15 @@ int fourier_f64(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, const ep
   dim3 grid((unsigned)cdiv(N, F_BN), (unsigned)cdiv(M, F_BM));
   EPB_CHECK_ARG(grid.y <= 65535, "fourier: ndata=%lld too large for one launch", (long long)M);
   size_t smem = fourier_smem_bytes();
+  static bool attr = false;
+  if (!attr) {
+    EPB_CUDA(cudaFuncSetAttribute(fourier_f64_kernel<true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    EPB_CUDA(cudaFuncSetAttribute(fourier_f64_kernel<false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = true;
+  }
   if (table) {
-    static bool attr = false;
-    if (!attr) {
-      EPB_CUDA(cudaFuncSetAttribute(fourier_f64_kernel<true>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      EPB_CUDA(cudaFuncSetAttribute(fourier_f64_kernel<false>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      attr = true;
-    }
     fourier_f64_kernel<true><<<grid, F_THREADS, smem, ctx->stream>>>(a);
   } else {
     fourier_f64_kernel<false><<<grid, F_THREADS, smem, ctx->stream>>>(a);

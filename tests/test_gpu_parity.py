@@ -175,7 +175,7 @@ def test_kq_convention_identity_gpu(B):
     B.get_eph_RR_to_kR_batched(kR, itp, xk, B.jl(f["uks"][:, :, :1]))
     ref = B.jl_empty((nwe, nwe, nm, nq), torch.complex128)
     B.get_eph_kR_to_kq_batched(ref, kR[0], B.fourier_phase(f["irvec_ep"], qs), B.jl(f["uphs"]), B.jl(f["ukqs"]))
-    pmk = torch.conj(B.fourier_phase(f["irvec_ep"], xk)).contiguous()
+    pmk = torch.conj_physical(B.fourier_phase(f["irvec_ep"], xk))
     kR2 = B.jl_empty((ndata, nr_ep, 1), torch.complex128)
     B.get_eph_RR_to_kR_batched(kR2, itp, xk, B.jl(f["uks"][:, :, :1]), additional_phase=pmk)
     out = B.jl_empty((nwe, nwe, nm, nq), torch.complex128)
@@ -189,6 +189,7 @@ def test_window_filter_exact(B):
     E = np.sort(rng.standard_normal((nw, nk)) * 3, axis=0)
     E[:, 7] = 0.25  # degenerate values at the window edge
     E[3, 11] = 0.25
+    E = np.sort(E, axis=0)  # the contract is sorted energies per k
     wmin, wmax = -0.1, 0.25
     bmin, bmax, keep, nbelow = B.window_filter(B.jl(np.asfortranarray(E)), wmin, wmax)
     ref = O.filter_kpoints(E, np.ones(nk), wmin, wmax)
