@@ -1,0 +1,371 @@
+"""Benchmark: g(k,q,nu) elements/s of the full-band e-ph pass on the config-2 workload.
+
+Workload (synthetic, seeded): nw = 16 electrons on a 9^3 Re grid (729), natom = 4 (12 modes) on a
+5^3 Rp grid (125), g(Re,Rp) ~ CN(0,1) exp(-|Re|/2 - |Rp|/1.5), H(R) ~ CN(0,1) exp(-|R|/1.5),
+spring-model force constants; 2048 random k x 8192 random q; all bands (no energy window), i.e.
+2048 * 8192 * 16 * 16 * 12 = 5.15e10 g elements per pass. One step = one whole pass (both
+electron eigensolves, phonons, both Fourier stages, rotations, g2 and its in-place reduction).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--prec mixed|fp64] [--impl epb|reference]
+
+Multi-GPU: one process per GPU (torchrun); every rank runs its own full pass on its own k set
+(weak scaling, no data-path collective); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "electronphonon.jl_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "g(k,q,ν) elems/s, nw=16: mixed-prec+filter vs FP64 plain, |g|² rel err≤1e-5"
+UNIT = "elements/s"
+NW, NATOM, N_EL, N_PH = 16, 4, 4, 2
+NK, NQ = 2048, 8192
+SEED = 2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="epb", choices=["epb", "reference"])
+    ap.add_argument("--prec", default="auto", choices=["auto", "mixed", "fp64"])
+    ap.add_argument("--nk", type=int, default=NK)
+    ap.add_argument("--nq", type=int, default=NQ)
+    ap.add_argument("--k-batch", type=int, default=16)
+    ap.add_argument("--sample-stride", type=int, default=4096)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-nk", type=int, default=16)
+    ap.add_argument("--cpu-nq", type=int, default=1024)
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def build_model_host_small():
+    """Host model without epmat (H and D only); the 4.5 GB epmat is generated on the device."""
+    from epb200 import synth
+
+    return synth.config2_model(seed=SEED, with_epmat=False)
+
+
+def config_dict(args, prec_name):
+    return {"workload": f"config2 full-band e-ph pass: nw={NW}, natom={NATOM} (nm={3 * NATOM}), "
+                        f"Re {2 * N_EL + 1}^3, Rp {2 * N_PH + 1}^3, {args.nk} random k x {args.nq} random q",
+            "nk": args.nk, "nq": args.nq, "nw": NW, "nmodes": 3 * NATOM, "nr_el": (2 * N_EL + 1) ** 3,
+            "nr_ep": (2 * N_PH + 1) ** 3, "window": "all bands", "precision": prec_name,
+            "k_batch": args.k_batch,
+            "l2": "inputs larger than L2 (g(Re,Rp) is 4.48 GB and is re-read every pass)",
+            "parallelism": f"dp{args.gpus} (k sharded per rank, weak)"}
+
+
+# ---------------------------------------------------------------------------------------------
+def clocks_start():
+    try:
+        f = open(os.path.join(ROOT, "gpurun_out", "bench_clocks.csv") if os.path.isdir(os.path.join(ROOT, "gpurun_out"))
+                 else os.devnull, "w")
+        p = subprocess.Popen(["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+                              "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                              "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        return (p, f)
+    except Exception:
+        return None
+
+
+def clocks_stop(h, device_index):
+    if h is None:
+        return None
+    p, f = h
+    p.terminate()
+    try:
+        out, _ = p.communicate(timeout=5)
+    except Exception:
+        p.kill()
+        out = ""
+    f.write(out)
+    f.close()
+    sm, mx, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in out.strip().splitlines():
+        parts = [x.strip() for x in line.split(",")]
+        if len(parts) < 9 or parts[0] != str(device_index):
+            continue
+        try:
+            sm.append(float(parts[1]))
+            mx = float(parts[2])
+        except ValueError:
+            continue
+        for n, v in zip(names, parts[5:9]):
+            if v.lower() == "active":
+                reasons.add(n)
+    if not sm:
+        return None
+    return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return d, "measured (MEASURED_PEAKS.json)"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def measure_fp64_peak(torch):
+    """cuBLAS DGEMM 8192^3 throughput (TFLOP/s), the FP64 denominator (no FP64 figure is provided)."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 1e9
+    for _ in range(3):
+        e0.record()
+        a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
+# Algorithmic flops per launch of each kernel family (8 real flops per complex MAC).
+def family_flops(name, args, nkb):
+    nw2, nm, nr_el, nr_ep = NW * NW, 3 * NATOM, (2 * N_EL + 1) ** 3, (2 * N_PH + 1) ** 3
+    if name == "zgemm":      # kR->kq for one k: (nw^2 nm) x nr_ep x nq
+        return 8.0 * nw2 * nm * nr_ep * args.nq
+    if name == "umma_kq":    # kR->kq for a k batch
+        return 8.0 * nw2 * nm * nr_ep * args.nq * nkb
+    if name in ("fourier_f64", "umma_h"):  # dominated by H(k+q): nw^2 x nr_el per k+q point
+        return 8.0 * nw2 * nr_el * args.nq * nkb
+    return None
+
+
+def run_epb(args):
+    import torch
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    from epb200 import pipeline, synth
+    from epb200 import _lib
+
+    prec = {"auto": None, "mixed": pipeline.PREC_MIXED, "fp64": pipeline.PREC_FP64}[args.prec]
+    m = build_model_host_small()
+    ep_dev = synth.epmat_el_device(SEED, NW, 3 * NATOM, m.el_ham.irvec, synth.irvec_box(N_PH))
+    m.epmat = synth.device_epmat_object(ep_dev, m.el_ham.irvec, synth.irvec_box(N_PH))
+    want_mixed = prec in (None, pipeline.PREC_MIXED)
+    try:
+        dm = pipeline.DeviceModel(m, mixed=want_mixed)
+    except _lib.EpbError:
+        if prec == pipeline.PREC_MIXED:
+            raise
+        dm = pipeline.DeviceModel(m, mixed=False)
+        want_mixed = False
+    if prec is None:
+        prec = pipeline.PREC_MIXED if want_mixed else pipeline.PREC_FP64
+    prec_name = "mixed (split-BF16 tcgen05 + FP32/FP64 eigensolve)" if prec == pipeline.PREC_MIXED else "fp64"
+    xks = synth.random_kpoints(args.nk, 1000 + rank)
+    xqs = synth.random_kpoints(args.nq, 2000)
+    from epb200.batched import jl
+
+    xk_d, xq_d = jl(xks), jl(xqs)
+    ctx = dm.ctx
+    run = lambda: pipeline.run_eph_over_k_and_q(dm, xk_d, xq_d, prec=prec, k_batch=args.k_batch,
+                                                sample_stride=args.sample_stride, out=out_holder[0])
+    out_holder = [None]
+    out_holder[0] = run()
+    for _ in range(max(args.warmup - 1, 0)):
+        run()
+    torch.cuda.synchronize()
+    # ---- device-timed region ----
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clk = clocks_start()
+    launches0 = ctx.launch_count()
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(args.steps):
+        run()
+    e1.record(s)
+    torch.cuda.synchronize()
+    launches = ctx.launch_count() - launches0
+    clocks = clocks_stop(clk, local)
+    ms = e0.elapsed_time(e1) / args.steps
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    n_el = out_holder[0].n_elements
+    value = ws * n_el / (ms * 1e-3)
+
+    # ---- per-kernel profile of one extra pass (not part of the timed region) ----
+    ctx.profile(True)
+    run()
+    torch.cuda.synchronize()
+    prof = ctx.profile_read(reset=True)
+    ctx.profile(False)
+    peaks, peak_src = measured_peaks()
+    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    dom_name, (dom_ms, dom_cnt) = dom
+    flops = family_flops(dom_name, args, args.k_batch)
+    roof = None
+    if flops is not None and dom_cnt > 0:
+        avg_s = dom_ms / dom_cnt * 1e-3
+        if dom_name.startswith("umma"):
+            nprod = 6
+            peak = peaks["bf16_tflops_sustained"] / nprod
+            psrc = f"{peak_src} bf16 sustained / {nprod} split products"
+        else:
+            peak = measure_fp64_peak(torch)
+            psrc = "measured live: cuBLAS DGEMM 8192^3 (no FP64 figure in MEASURED_PEAKS.json)"
+        ach = flops / avg_s / 1e12
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tp):
+            with open(tp) as fh:
+                traffic = json.load(fh).get(dom_name)
+        roof = {"bound": "tensor", "kernel": dom_name, "achieved": round(ach, 3), "peak": round(peak, 2),
+                "unit": "TFLOP/s", "frac": round(ach / peak, 4), "traffic": traffic, "peak_source": psrc,
+                "launch_ms": round(dom_ms / dom_cnt, 4), "launches_per_pass": dom_cnt,
+                "algorithmic_flops_per_launch": flops,
+                "share_of_pass": {k: round(v[0] / sum(x[0] for x in prof.values()), 4) for k, v in prof.items() if v[1]}}
+
+    # ---- end to end through the public API with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        xk_h = torch.from_numpy(np.ascontiguousarray(xks.T)).pin_memory()
+        xq_h = torch.from_numpy(np.ascontiguousarray(xqs.T)).pin_memory()
+        r0 = out_holder[0]
+        outs = [r0.ek, r0.omega, r0.g2sum] + ([r0.g2_sample] if r0.g2_sample is not None else [])
+        host_outs = [torch.empty(o.shape, dtype=o.dtype).pin_memory() for o in outs]
+        bi = xk_h.numel() * 8 + xq_h.numel() * 8
+        bo = sum(o.numel() * o.element_size() for o in outs)
+        torch.cuda.synchronize()
+        e0.record(s)
+        for _ in range(args.steps):
+            xk_dd = xk_h.to("cuda", non_blocking=True)
+            xq_dd = xq_h.to("cuda", non_blocking=True)
+            r = pipeline.run_eph_over_k_and_q(dm, xk_dd, xq_dd, prec=prec, k_batch=args.k_batch,
+                                              sample_stride=args.sample_stride, out=r0)
+            for ho, o in zip(host_outs, outs):
+                ho.copy_(o, non_blocking=True)
+        e1.record(s)
+        torch.cuda.synchronize()
+        ms_e2e = e0.elapsed_time(e1) / args.steps
+        if ws > 1:
+            t = torch.tensor([ms_e2e], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms_e2e = float(t.item())
+        e2e = {"value": ws * n_el / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": bi,
+               "d2h_bytes_per_step": bo, "ms_per_step": round(ms_e2e, 3)}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args, m_host_for_cpu(m, ep_dev), xks, xqs)
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16x3/f32/f64" if prec == pipeline.PREC_MIXED else "f64",
+            "data": "synthetic (seeded generator; random-init Wannier model of the config-2 shape)",
+            "config": config_dict(args, prec_name), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clocks, "impl": "epb"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def m_host_for_cpu(m, ep_dev):
+    """Host copy of the model (the device-generated epmat copied back) for the CPU port."""
+    from epb200 import synth
+    from epb200.wannier import WannierObject
+
+    op = ep_dev.cpu().numpy().T  # Fortran-ordered (ndata, nr_el)
+    mm = synth.SynthModel(m.nw, m.nmodes, m.mass, m.el_ham, m.ph_dyn,
+                          WannierObject(m.el_ham.irvec, op, irvec_next=synth.irvec_box(N_PH)), m.seed)
+    return mm
+
+
+def cpu_baseline(args, model, xks, xqs):
+    """CPU port of the reference's batched path (oracle/cpu_pass.py) on a bounded sample."""
+    from oracle import cpu_pass
+
+    nk, nq = min(args.cpu_nk, xks.shape[1]), min(args.cpu_nq, xqs.shape[1])
+    xk, xq = np.asfortranarray(xks[:, :nk]), np.asfortranarray(xqs[:, :nq])
+    t0 = time.perf_counter()
+    r = cpu_pass.eph_pass_cpu(model, xk, xq)
+    dt = time.perf_counter() - t0
+    cores = int(os.environ.get("OPENBLAS_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": r["n_elements"] / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{nk} k x {nq} q of the same model (all bands), {dt:.1f} s; numpy/scipy OpenBLAS "
+                      f"ZGEMM + LAPACK ZHEEV per matrix"}
+
+
+def run_reference(args):
+    """Reference arm: the reference's CPU batched path restated (the Julia reference cannot run here)."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from epb200 import synth
+    from oracle import cpu_pass
+
+    m = synth.config2_model(seed=SEED)
+    xks = synth.random_kpoints(args.nk, 1000)
+    xqs = synth.random_kpoints(args.nq, 2000)
+    nk, nq = min(args.cpu_nk, args.nk), min(args.cpu_nq, args.nq)
+    xk, xq = np.asfortranarray(xks[:, :nk]), np.asfortranarray(xqs[:, :nq])
+    for _ in range(args.warmup):
+        cpu_pass.eph_pass_cpu(m, xk[:, :1], xq[:, :64])
+    t0 = time.perf_counter()
+    n = 0
+    for _ in range(args.steps):
+        r = cpu_pass.eph_pass_cpu(m, xk, xq)
+        n += r["n_elements"]
+    dt = time.perf_counter() - t0
+    v = n / dt
+    cores = int(os.environ.get("OPENBLAS_NUM_THREADS", os.cpu_count() or 1))
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+            "config": config_dict(args, "fp64 (CPU)"),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{nk} k x {nq} q per step of the config-2 model, all bands"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_epb(a)

@@ -36,6 +36,7 @@ void clear_error();
 
 #define EPB_LAUNCH_CHECK()                                                                    \
   do {                                                                                        \
+    ++ctx->launches;                                                                          \
     cudaError_t _e = cudaGetLastError();                                                      \
     if (_e != cudaSuccess) {                                                                  \
       ::epb::set_error("kernel launch failed: %s (%s:%d)", cudaGetErrorString(_e), __FILE__, \
@@ -74,6 +75,26 @@ enum epb_slot {
   EPB_WS_NSLOTS
 };
 
+// Kernel families timed by the optional profiler (epb_profile_*).
+enum epb_prof_id {
+  EPB_PROF_FOURIER_F64 = 0,
+  EPB_PROF_ZGEMM,
+  EPB_PROF_EIGH,
+  EPB_PROF_ROT,
+  EPB_PROF_RR_ROT,
+  EPB_PROF_UMMA_H,
+  EPB_PROF_UMMA_KQ,
+  EPB_PROF_UMMA_RR,
+  EPB_PROF_SPLIT,
+  EPB_PROF_OTHER,
+  EPB_PROF_N
+};
+
+struct epb_prof_rec {
+  cudaEvent_t a, b;
+  int id;
+};
+
 struct epb_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -84,6 +105,13 @@ struct epb_ctx {
   int fail_alloc_nth = 0;  // test hook
   // Small pinned host scratch for scalar read-backs.
   int64_t* pinned = nullptr;
+  // instrumentation
+  int64_t launches = 0;          // kernels launched by the library on this context
+  bool prof_on = false;
+  std::vector<epb_prof_rec> prof;  // event pairs recorded while profiling
+  size_t prof_used = 0;
+  double prof_ms[EPB_PROF_N] = {};
+  int64_t prof_cnt[EPB_PROF_N] = {};
 };
 
 struct epb_rset {
@@ -96,6 +124,10 @@ struct epb_rset {
 };
 
 namespace epb {
+
+// Profiler brackets around a launch (no-ops unless epb_profile_enable was called).
+void prof_begin(epb_ctx* ctx, int id);
+void prof_end(epb_ctx* ctx);
 
 // Grow-only workspace slot; returns EPB_ERR_OOM on failure.
 int ws_get(epb_ctx* ctx, int slot, size_t bytes, void** out);

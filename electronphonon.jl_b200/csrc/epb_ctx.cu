@@ -58,6 +58,41 @@ int ws_get(epb_ctx* ctx, int slot, size_t bytes, void** out) {
   return EPB_OK;
 }
 
+void prof_begin(epb_ctx* ctx, int id) {
+  if (!ctx->prof_on) return;
+  if (ctx->prof_used == ctx->prof.size()) {
+    epb_prof_rec r;
+    if (cudaEventCreate(&r.a) != cudaSuccess || cudaEventCreate(&r.b) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    ctx->prof.push_back(r);
+  }
+  epb_prof_rec& r = ctx->prof[ctx->prof_used];
+  r.id = id;
+  cudaEventRecord(r.a, ctx->stream);
+}
+
+void prof_end(epb_ctx* ctx) {
+  if (!ctx->prof_on || ctx->prof_used == ctx->prof.size()) return;
+  cudaEventRecord(ctx->prof[ctx->prof_used].b, ctx->stream);
+  ++ctx->prof_used;
+}
+
+// Fold recorded event pairs into the per-id totals (synchronises on the events).
+static int prof_flush(epb_ctx* ctx) {
+  for (size_t i = 0; i < ctx->prof_used; ++i) {
+    epb_prof_rec& r = ctx->prof[i];
+    EPB_CUDA(cudaEventSynchronize(r.b));
+    float ms = 0.f;
+    EPB_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+    ctx->prof_ms[r.id] += ms;
+    ctx->prof_cnt[r.id] += 1;
+  }
+  ctx->prof_used = 0;
+  return EPB_OK;
+}
+
 }  // namespace epb
 
 using namespace epb;
@@ -103,6 +138,10 @@ int epb_destroy(epb_ctx* ctx) {
   if (!ctx) return EPB_OK;
   make_current(ctx);
   cudaStreamSynchronize(ctx->stream);
+  for (auto& r : ctx->prof) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
   for (int i = 0; i < EPB_WS_NSLOTS; ++i)
     if (ctx->ws[i]) cudaFree(ctx->ws[i]);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
@@ -138,6 +177,35 @@ int epb_workspace_bytes(epb_ctx* ctx, uint64_t* bytes_host) {
   uint64_t s = 0;
   for (int i = 0; i < EPB_WS_NSLOTS; ++i) s += ctx->ws_bytes[i];
   *bytes_host = s;
+  return EPB_OK;
+}
+
+int epb_launch_count(epb_ctx* ctx, int64_t* count_host) {
+  EPB_CHECK_ARG(ctx && count_host, "epb_launch_count: NULL argument");
+  *count_host = ctx->launches;
+  return EPB_OK;
+}
+
+int epb_profile_enable(epb_ctx* ctx, int on) {
+  EPB_CHECK_ARG(ctx, "epb_profile_enable: NULL ctx");
+  EPB_TRY(make_current(ctx));
+  if (ctx->prof_on && !on) EPB_TRY(prof_flush(ctx));
+  ctx->prof_on = on != 0;
+  return EPB_OK;
+}
+
+int epb_profile_read(epb_ctx* ctx, double* ms_host, int64_t* count_host, int n, int reset) {
+  EPB_CHECK_ARG(ctx && ms_host && count_host && n >= 1, "epb_profile_read: bad argument");
+  EPB_TRY(make_current(ctx));
+  EPB_TRY(prof_flush(ctx));
+  for (int i = 0; i < n && i < EPB_PROF_N; ++i) {
+    ms_host[i] = ctx->prof_ms[i];
+    count_host[i] = ctx->prof_cnt[i];
+    if (reset) {
+      ctx->prof_ms[i] = 0;
+      ctx->prof_cnt[i] = 0;
+    }
+  }
   return EPB_OK;
 }
 

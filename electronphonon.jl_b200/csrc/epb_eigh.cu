@@ -220,7 +220,7 @@ __global__ void eigh_kernel(EighArgs a) {
       }
       double ev = (double)ei;
       if (a.mass) ev = ev >= 0 ? sqrt(ev) : -sqrt(-ev);
-      a.E[eoff + rank] = ev;
+      if (a.E) a.E[eoff + rank] = ev;
       // stash rank in the (now unused) imaginary part of the diagonal
       As[i + i * lda].y = (T)rank;
     }
@@ -399,7 +399,7 @@ __global__ void eigh_mixed_kernel(EighArgs a) {
       }
       double ev = ei;
       if (a.mass) ev = ev >= 0 ? sqrt(ev) : -sqrt(-ev);
-      a.E[eoff + rank] = ev;
+      if (a.E) a.E[eoff + rank] = ev;
       H[i + i * lda].y = (double)rank;
     }
     team_sync<TEAM>();
@@ -453,7 +453,9 @@ static int launch_eigh(epb_ctx* ctx, Kern kern, size_t smem, int threads, EighAr
   int64_t blocks = (int64_t)per_sm * ctx->sm_count;
   if (blocks > blocks_needed) blocks = blocks_needed;
   if (blocks < 1) blocks = 1;
+  prof_begin(ctx, EPB_PROF_EIGH);
   kern<<<(unsigned)blocks, threads, smem, ctx->stream>>>(a);
+  prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
 }
@@ -501,6 +503,45 @@ int eigh_run(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
   }
   if (*h > 0) {
     set_error("eigensolver: %d matrices reached the sweep limit", *h);
+    return EPB_ERR_NOCONVERGE;
+  }
+  return EPB_OK;
+}
+
+// Stream-ordered variant for the pass pipeline: counters accumulate in a context slot until
+// eigh_check() reads them back (one sync per pass instead of one per call).
+int eigh_async(epb_ctx* ctx, double2* A, int64_t n, int64_t batch, double* E, bool want_v,
+               const double* mass, int prec) {
+  if (batch == 0) return EPB_OK;
+  void* ws = nullptr;
+  bool fresh = ctx->ws[EPB_WS_EIGH] == nullptr;
+  EPB_TRY(ws_get(ctx, EPB_WS_EIGH, 64, &ws));
+  if (fresh) EPB_CUDA(cudaMemsetAsync(ws, 0, 64, ctx->stream));
+  EighArgs a{};
+  a.A = A;
+  a.n_uniform = (int)n;
+  a.batch = batch;
+  a.E = E;
+  a.want_v = want_v;
+  a.mass = mass;
+  a.nonconv = (int*)ws;
+  a.badsize = a.nonconv + 1;
+  a.max_sweeps = prec == EPB_PREC_FP64 ? 30 : 20;
+  return eigh_dispatch(ctx, a, (int)n, prec);
+}
+
+int eigh_check(epb_ctx* ctx) {
+  if (!ctx->ws[EPB_WS_EIGH]) return EPB_OK;
+  int* h = (int*)ctx->pinned;
+  EPB_CUDA(cudaMemcpyAsync(h, ctx->ws[EPB_WS_EIGH], 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  EPB_CUDA(cudaMemsetAsync(ctx->ws[EPB_WS_EIGH], 0, 64, ctx->stream));
+  EPB_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (h[1] > 0) {
+    set_error("eigensolver: %d matrices have an unsupported order (skipped)", h[1]);
+    return EPB_ERR_ARG;
+  }
+  if (h[0] > 0) {
+    set_error("eigensolver: %d matrices reached the sweep limit", h[0]);
     return EPB_ERR_NOCONVERGE;
   }
   return EPB_OK;

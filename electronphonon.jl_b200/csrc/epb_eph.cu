@@ -83,7 +83,9 @@ int zgemm_nn(epb_ctx* ctx, const double2* A, int64_t lda, const double2* B, int6
   if (M == 0 || N == 0) return EPB_OK;
   dim3 grid((unsigned)cdiv(N, G_BN), (unsigned)cdiv(M, G_BM));
   EPB_CHECK_ARG(grid.y <= 65535, "zgemm: M=%lld too large for one launch", (long long)M);
+  prof_begin(ctx, EPB_PROF_ZGEMM);
   zgemm_nn_kernel<<<grid, G_THREADS, 0, ctx->stream>>>(A, lda, B, ldb, C, ldc, M, N, K);
+  prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
 }
@@ -172,8 +174,10 @@ int eph_rotations_f64(epb_ctx* ctx, const double2* g, int64_t ldg, int nw, int n
     attr = true;
   }
   int64_t blocks = nq < (int64_t)ctx->sm_count * 8 ? nq : (int64_t)ctx->sm_count * 8;
+  prof_begin(ctx, EPB_PROF_ROT);
   eph_rot_kernel<<<(unsigned)blocks, 256, smem, ctx->stream>>>(g, ldg, ukq, uph, omega, ep, g2, nw,
                                                                 nbk, nm, nbkq, nq);
+  prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
 }
@@ -210,9 +214,11 @@ int epb_eph_RR_to_kR(epb_ctx* ctx, const double* epmat, int64_t nw, int64_t nm, 
     int64_t total = outk * kn;
     int64_t blocks = cdiv(total, 256);
     if (blocks > (int64_t)ctx->sm_count * 32) blocks = (int64_t)ctx->sm_count * 32;
+    prof_begin(ctx, EPB_PROF_RR_ROT);
     rr_rotate_kernel<<<(unsigned)blocks, 256, 0, ctx->stream>>>(
         g, (const double2*)uk + k0 * nw * nband, add_phase ? (const double2*)add_phase + k0 * nr_ep : nullptr,
         (double2*)out + k0 * outk, (int)nw, (int)nband, (int)nm, (int)nr_ep, kn);
+    prof_end(ctx);
     EPB_LAUNCH_CHECK();
   }
   return EPB_OK;

@@ -142,6 +142,14 @@ __global__ void __launch_bounds__(F_THREADS, 2) fourier_f64_kernel(FourierArgs a
   }
 }
 
+int launch_phase(epb_ctx* ctx, const epb_rset* rs, const double* xk, int64_t nk, double2* phase) {
+  int64_t total = rs->nr * nk;
+  if (total == 0) return EPB_OK;
+  phase_kernel<<<(unsigned)cdiv(total, 256), 256, 0, ctx->stream>>>(rs->dev, rs->nr, xk, nk, phase);
+  EPB_LAUNCH_CHECK();
+  return EPB_OK;
+}
+
 static size_t fourier_smem_bytes() {
   return sizeof(double2) * (2 * F_BK * F_BM + 2 * F_BK * F_BN + 3 * F_TAB * F_BN);
 }
@@ -178,11 +186,13 @@ int fourier_f64(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, const ep
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr = true;
   }
+  prof_begin(ctx, EPB_PROF_FOURIER_F64);
   if (table) {
     fourier_f64_kernel<true><<<grid, F_THREADS, smem, ctx->stream>>>(a);
   } else {
     fourier_f64_kernel<false><<<grid, F_THREADS, smem, ctx->stream>>>(a);
   }
+  prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
 }

@@ -1,0 +1,252 @@
+// Whole e-ph pass over random k x random q (the arbitrary-q semantics of run_eph_over_k_and_q,
+// src/calculator/run_eph_over_k_and_q.jl:251-330, batched the way the GPU outer-k loop batches,
+// src/calculator/run_eph_over_k_and_kq.jl:792-892):
+//
+//   q side (once):  D(q) -> omega, u_ph;  P[p, q] = exp(2 pi i Rp . q)     (q convention)
+//   per k batch:    H(k) -> e_k, u_k;  g(k, Rp) = RR->kR rotated by u_k
+//                   H(k+q) -> e_kq, u_kq for every (k, q) pair of the batch
+//                   g(k, q) = sum_p g(k, Rp) P[p, q];  ep = u_kq^dagger g u_ph;  g2 = |ep|^2 / (2 omega)
+//
+// The 5e10 g2 values of a full pass are never materialised: the rotation kernel consumes each
+// (k, q) block in place, accumulating g2sum[nu, k] = sum_{m, n, q} g2 and writing the full block
+// only for the sampled q (q % sample_stride == 0), which is what the parity checks read.
+#include <vector>
+
+#include "epb_common.cuh"
+
+struct epb_model {
+  epb_ctx* ctx = nullptr;
+  int64_t nw = 0, nm = 0, nr_el = 0, nr_ph = 0, nr_ep = 0;
+  const double2* ham = nullptr;   // (nw^2, nr_el)
+  const double2* dyn = nullptr;   // (nm^2, nr_ph)
+  const double* mass = nullptr;   // (nm)
+  const double2* epmat = nullptr; // (nw^2 nm nr_ep, nr_el)
+  epb_rset* rs_el = nullptr;
+  epb_rset* rs_ph = nullptr;
+  epb_rset* rs_ep = nullptr;
+  // mixed-precision operand planes (owned), see epb_umma.cu
+  void* mixed = nullptr;
+};
+
+namespace epb {
+
+int fourier_f64(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, const epb_rset* rs,
+                const double* xk, int64_t N, double2* out, int64_t ldo);
+int zgemm_nn(epb_ctx* ctx, const double2* A, int64_t lda, const double2* B, int64_t ldb, double2* C,
+             int64_t ldc, int64_t M, int64_t N, int64_t K);
+int eigh_async(epb_ctx* ctx, double2* A, int64_t n, int64_t batch, double* E, bool want_v,
+               const double* mass, int prec);
+int eigh_check(epb_ctx* ctx);
+int mixed_pass_batch(epb_ctx* ctx, epb_model* m, const double* xk_b, int64_t nkb, const double* xq,
+                     int64_t nq, const double2* uk_b, const double2* uph, const double* omega,
+                     const double2* phase, double* g2sum_b, double* g2_sample_b, int64_t sample_stride,
+                     int64_t* stats);
+int mixed_model_prepare(epb_ctx* ctx, epb_model* m);
+void mixed_model_free(epb_model* m);
+
+// x_{k+q} for every (k_local, q) pair, q fastest: xkq[:, kl * nq + q] = xk[:, kl] + xq[:, q]
+__global__ void xkq_kernel(const double* __restrict__ xk, int64_t nkb, const double* __restrict__ xq,
+                           int64_t nq, double* __restrict__ xkq) {
+  int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nkb * nq) return;
+  int64_t kl = idx / nq, q = idx % nq;
+  xkq[3 * idx + 0] = xk[3 * kl + 0] + xq[3 * q + 0];
+  xkq[3 * idx + 1] = xk[3 * kl + 1] + xq[3 * q + 1];
+  xkq[3 * idx + 2] = xk[3 * kl + 2] + xq[3 * q + 2];
+}
+
+int launch_phase(epb_ctx* ctx, const epb_rset* rs, const double* xk, int64_t nk, double2* phase);
+
+// Rotation + |g|^2 fold + in-place reduction for one k over all q (FP64).
+// g: (nw, nw, nm, nq) for this k (ld = nw*nw*nm per q); ukq: (nw, nw, nq) for this k.
+__global__ void eph_rot_reduce_kernel(const double2* __restrict__ g, const double2* __restrict__ ukq,
+                                      const double2* __restrict__ uph, const double* __restrict__ omega,
+                                      int nw, int nm, int64_t nq, double* __restrict__ g2sum,
+                                      double* __restrict__ sample, int64_t stride) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nb = nw;  // full band window
+  const int ng = nw * nb * nm, nt = nb * nb * nm;
+  double2* gs = reinterpret_cast<double2*>(smem_raw);
+  double2* ts = gs + ng;
+  double2* us = ts + nt;
+  double2* ps = us + nw * nb;
+  double* red = reinterpret_cast<double*>(ps + nm * nm);  // [nm]
+  for (int e = threadIdx.x; e < nm; e += blockDim.x) red[e] = 0.0;
+  for (int64_t q = blockIdx.x; q < nq; q += gridDim.x) {
+    __syncthreads();
+    const double2* gq = g + q * (int64_t)ng;
+    for (int e = threadIdx.x; e < ng; e += blockDim.x) gs[e] = gq[e];
+    for (int e = threadIdx.x; e < nw * nb; e += blockDim.x) us[e] = ukq[q * nw * nb + e];
+    for (int e = threadIdx.x; e < nm * nm; e += blockDim.x) ps[e] = uph[q * nm * nm + e];
+    __syncthreads();
+    for (int e = threadIdx.x; e < nt; e += blockDim.x) {
+      int m = e % nb, r = e / nb;
+      double2 acc = make_double2(0, 0);
+      const double2* gc = gs + r * nw;
+      const double2* uc = us + m * nw;
+      for (int iw = 0; iw < nw; ++iw) cfma_conj(acc, uc[iw], gc[iw]);
+      ts[e] = acc;
+    }
+    __syncthreads();
+    const int mn = nb * nb;
+    const bool samp = sample && (q % stride == 0);
+    double* sq = samp ? sample + (q / stride) * (int64_t)nt : nullptr;
+    for (int e = threadIdx.x; e < nt; e += blockDim.x) {
+      int mnidx = e % mn, nu = e / mn;
+      double2 acc = make_double2(0, 0);
+      for (int jm = 0; jm < nm; ++jm) cfma(acc, ts[mnidx + jm * mn], ps[jm + nu * nm]);
+      double v = (acc.x * acc.x + acc.y * acc.y) / (2.0 * omega[nu + q * nm]);
+      if (samp) sq[e] = v;
+      atomicAdd(&red[nu], v);
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nm; e += blockDim.x) atomicAdd(&g2sum[e], red[e]);
+}
+
+}  // namespace epb
+
+using namespace epb;
+
+extern "C" {
+
+int epb_model_create(epb_ctx* ctx, const double* ham_op, int64_t nw, const int64_t* irvec_el_host,
+                     int64_t nr_el, const double* dyn_op, const double* mass, int64_t nm,
+                     const int64_t* irvec_ph_host, int64_t nr_ph, const double* epmat_op,
+                     const int64_t* irvec_ep_host, int64_t nr_ep, int flags, epb_model** out) {
+  clear_error();
+  EPB_CHECK_ARG(ctx && out && ham_op && irvec_el_host && dyn_op && mass && irvec_ph_host && epmat_op &&
+                    irvec_ep_host,
+                "epb_model_create: NULL argument");
+  EPB_CHECK_ARG(nw >= 1 && nw <= 32 && nm >= 1 && nm <= 32 && nr_el >= 1 && nr_ph >= 1 && nr_ep >= 1,
+                "epb_model_create: unsupported sizes (nw=%lld nm=%lld)", (long long)nw, (long long)nm);
+  EPB_TRY(make_current(ctx));
+  epb_model* m = new epb_model();
+  m->ctx = ctx;
+  m->nw = nw;
+  m->nm = nm;
+  m->nr_el = nr_el;
+  m->nr_ph = nr_ph;
+  m->nr_ep = nr_ep;
+  m->ham = (const double2*)ham_op;
+  m->dyn = (const double2*)dyn_op;
+  m->mass = mass;
+  m->epmat = (const double2*)epmat_op;
+  int st = epb_rset_create(ctx, irvec_el_host, nr_el, &m->rs_el);
+  if (st == EPB_OK) st = epb_rset_create(ctx, irvec_ph_host, nr_ph, &m->rs_ph);
+  if (st == EPB_OK) st = epb_rset_create(ctx, irvec_ep_host, nr_ep, &m->rs_ep);
+  if (st == EPB_OK && (flags & 1)) st = mixed_model_prepare(ctx, m);
+  if (st != EPB_OK) {
+    epb_model_destroy(m);
+    return st;
+  }
+  *out = m;
+  return EPB_OK;
+}
+
+int epb_model_destroy(epb_model* m) {
+  if (!m) return EPB_OK;
+  if (m->ctx) make_current(m->ctx);
+  mixed_model_free(m);
+  epb_rset_destroy(m->rs_el);
+  epb_rset_destroy(m->rs_ph);
+  epb_rset_destroy(m->rs_ep);
+  delete m;
+  return EPB_OK;
+}
+
+int epb_eph_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double* xq, int64_t nq,
+                 int prec, int64_t k_batch, int64_t sample_stride, double* ek_out, double* omega_out,
+                 double* g2sum_out, double* g2_sample, int64_t* stats_host) {
+  clear_error();
+  EPB_CHECK_ARG(ctx && m && xk && xq && ek_out && omega_out && g2sum_out, "epb_eph_pass: NULL argument");
+  EPB_CHECK_ARG(nk >= 1 && nq >= 1 && k_batch >= 1, "epb_eph_pass: bad sizes");
+  EPB_CHECK_ARG(prec == EPB_PREC_FP64 || prec == EPB_PREC_MIXED, "epb_eph_pass: bad prec");
+  EPB_CHECK_ARG(!g2_sample || sample_stride >= 1, "epb_eph_pass: sample_stride must be >= 1");
+  EPB_CHECK_ARG(prec != EPB_PREC_MIXED || m->mixed, "epb_eph_pass: model was created without mixed planes");
+  EPB_TRY(make_current(ctx));
+  const int64_t nw = m->nw, nm = m->nm, nr_ep = m->nr_ep;
+  const int64_t nw2 = nw * nw;
+  if (k_batch > nk) k_batch = nk;
+  // ---- workspace layout ----------------------------------------------------------------------
+  size_t off = 0;
+  auto carve = [&](size_t bytes) {
+    size_t o = off;
+    off += (bytes + 255) & ~size_t(255);
+    return o;
+  };
+  const size_t o_dq = carve(16ull * nm * nm * nq);
+  const size_t o_ph = carve(16ull * nr_ep * nq);
+  const size_t o_hk = carve(16ull * nw2 * k_batch);
+  const size_t o_G = carve(16ull * nw2 * nm * nr_ep * k_batch);
+  const size_t o_xkq = carve(24ull * k_batch * nq);
+  const size_t o_hkq = carve(16ull * nw2 * k_batch * nq);
+  const size_t o_g = prec == EPB_PREC_FP64 ? carve(16ull * nw2 * nm * nq) : carve(0);
+  void* base = nullptr;
+  EPB_TRY(ws_get(ctx, EPB_WS_PASS0, off, &base));
+  char* b = (char*)base;
+  double2* Dq = (double2*)(b + o_dq);
+  double2* P = (double2*)(b + o_ph);
+  double2* Hk = (double2*)(b + o_hk);
+  double2* G = (double2*)(b + o_G);
+  double* Xkq = (double*)(b + o_xkq);
+  double2* Hkq = (double2*)(b + o_hkq);
+  double2* gb = (double2*)(b + o_g);
+  EPB_CUDA(cudaMemsetAsync(g2sum_out, 0, sizeof(double) * nm * nk, ctx->stream));
+  const int64_t nsamp = g2_sample ? (nq + sample_stride - 1) / sample_stride : 0;
+  int64_t stats[4] = {0, 0, 0, 0};
+
+  // ---- q side --------------------------------------------------------------------------------
+  EPB_TRY(fourier_f64(ctx, m->dyn, nm * nm, nm * nm, m->rs_ph, xq, nq, Dq, nm * nm));
+  EPB_TRY(eigh_async(ctx, Dq, nm, nq, omega_out, true, m->mass, EPB_PREC_FP64));
+  EPB_TRY(launch_phase(ctx, m->rs_ep, xq, nq, P));
+
+  // ---- k batches -----------------------------------------------------------------------------
+  static bool attr = false;
+  size_t rsmem = sizeof(double2) * (nw2 * nm * 2 + nw2 + nm * nm) + sizeof(double) * nm;
+  EPB_CHECK_ARG(rsmem <= 200 * 1024, "epb_eph_pass: rotation block too large");
+  if (!attr) {
+    EPB_CUDA(cudaFuncSetAttribute(eph_rot_reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr = true;
+  }
+  for (int64_t k0 = 0; k0 < nk; k0 += k_batch) {
+    const int64_t nkb = nk - k0 < k_batch ? nk - k0 : k_batch;
+    const double* xkb = xk + 3 * k0;
+    // electrons at k: FP64 in both modes (2048 points; the k side is not the bulk of the work)
+    EPB_TRY(fourier_f64(ctx, m->ham, nw2, nw2, m->rs_el, xkb, nkb, Hk, nw2));
+    EPB_TRY(eigh_async(ctx, Hk, nw, nkb, ek_out + nw * k0, true, nullptr, EPB_PREC_FP64));
+    // x_{k+q}
+    xkq_kernel<<<(unsigned)cdiv(nkb * nq, 256), 256, 0, ctx->stream>>>(xkb, nkb, xq, nq, Xkq);
+    EPB_LAUNCH_CHECK();
+    if (prec == EPB_PREC_FP64) {
+      EPB_TRY(epb_eph_RR_to_kR(ctx, (const double*)m->epmat, nw, nm, nr_ep, m->rs_el, xkb, nkb,
+                               (const double*)Hk, nw, nullptr, (double*)G, EPB_PREC_FP64));
+      EPB_TRY(fourier_f64(ctx, m->ham, nw2, nw2, m->rs_el, Xkq, nkb * nq, Hkq, nw2));
+      EPB_TRY(eigh_async(ctx, Hkq, nw, nkb * nq, nullptr, true, nullptr, EPB_PREC_FP64));
+      const int64_t ndata = nw2 * nm;
+      for (int64_t kl = 0; kl < nkb; ++kl) {
+        EPB_TRY(zgemm_nn(ctx, G + kl * ndata * nr_ep, ndata, P, nr_ep, gb, ndata, ndata, nq, nr_ep));
+        int64_t blocks = nq < (int64_t)ctx->sm_count * 8 ? nq : (int64_t)ctx->sm_count * 8;
+        prof_begin(ctx, EPB_PROF_ROT);
+        eph_rot_reduce_kernel<<<(unsigned)blocks, 256, rsmem, ctx->stream>>>(
+            gb, Hkq + kl * nq * nw2, Dq, omega_out, (int)nw, (int)nm, nq, g2sum_out + nm * (k0 + kl),
+            g2_sample ? g2_sample + (k0 + kl) * nsamp * nw2 * nm : nullptr, sample_stride);
+        prof_end(ctx);
+        EPB_LAUNCH_CHECK();
+      }
+    } else {
+      EPB_TRY(mixed_pass_batch(ctx, m, xkb, nkb, xq, nq, Hk, Dq, omega_out, P, g2sum_out + nm * k0,
+                               g2_sample ? g2_sample + k0 * nsamp * nw2 * nm : nullptr, sample_stride, stats));
+    }
+  }
+  EPB_TRY(eigh_check(ctx));
+  if (stats_host) {
+    stats_host[0] = nk * nq * nw2 * nm;  // g elements produced (all bands)
+    stats_host[1] = stats[1];
+    stats_host[2] = stats[2];
+    stats_host[3] = stats[3];
+  }
+  return EPB_OK;
+}
+
+}  // extern "C"

@@ -41,6 +41,9 @@ SIGNATURES = {
     "epb_version": [],
     "epb_workspace_bytes": [P, C.POINTER(C.c_uint64)],
     "epb_debug_fail_alloc": [P, I32],
+    "epb_launch_count": [P, C.POINTER(I64)],
+    "epb_profile_enable": [P, I32],
+    "epb_profile_read": [P, P, P, I32, I32],
     "epb_rset_create": [P, P, I64, C.POINTER(P)],
     "epb_rset_destroy": [P],
     "epb_fourier_phase": [P, P, P, I64, P],
@@ -53,6 +56,9 @@ SIGNATURES = {
     "epb_eph_kR_to_kq": [P, P, I64, I64, I64, I64, I64, P, I64, P, I64, P, P, P, P, I32],
     "epb_window_filter": [P, P, I64, I64, D, D, P, P, P, P, P],
     "epb_fill_iqs": [P, P, I64, P, I64, I64, I64, P, P],
+    "epb_model_create": [P, P, I64, P, I64, P, P, I64, P, I64, P, P, I64, I32, C.POINTER(P)],
+    "epb_model_destroy": [P],
+    "epb_eph_pass": [P, P, P, I64, P, I64, I32, I64, I64, P, P, P, P, P],
 }
 _RESTYPE = {"epb_last_error": C.c_char_p}
 
@@ -131,6 +137,26 @@ class Context:
         b = C.c_uint64()
         check(lib().epb_workspace_bytes(self.h, C.byref(b)))
         return b.value
+
+    def launch_count(self):
+        c = I64()
+        check(lib().epb_launch_count(self.h, C.byref(c)))
+        return c.value
+
+    PROF_NAMES = ["fourier_f64", "zgemm", "eigh", "rotation", "rr_rotation", "umma_h", "umma_kq", "umma_rr",
+                  "split", "other"]
+
+    def profile(self, on=True):
+        check(lib().epb_profile_enable(self.h, 1 if on else 0))
+
+    def profile_read(self, reset=True):
+        import numpy as np
+
+        n = len(self.PROF_NAMES)
+        ms = np.zeros(n)
+        cnt = np.zeros(n, dtype=np.int64)
+        check(lib().epb_profile_read(self.h, ms.ctypes.data, cnt.ctypes.data, n, 1 if reset else 0))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.PROF_NAMES)}
 
     def close(self):
         if getattr(self, "h", None):

@@ -184,3 +184,37 @@ def config3_matrices(count, seed=3, sizes=None, degenerate_frac=0.05, spacing=1e
             a = (a + a.conj().T) / 2
         mats.append(np.asfortranarray(a))
     return ns.astype(np.int64), mats
+
+
+def epmat_el_device(seed, nw, nm, irvec_el, irvec_ep, decay_e=2.0, decay_p=1.5, device="cuda"):
+    """g(Re,Rp) of the "el" layout generated on the GPU with torch's seeded Philox generator
+    (same distribution as `epmat_el_op_r`; used for the 4.5 GB full-size workload, where host
+    generation would dominate start-up). Returns a complex128 tensor of shape (nr_el, ndata), i.e.
+    the column-major (ndata, nr_el) operator."""
+    import torch
+
+    nr_el, nr_ep = irvec_el.shape[0], irvec_ep.shape[0]
+    ndata = nw * nw * nm * nr_ep
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    out = torch.randn((nr_el, ndata), dtype=torch.complex128, device=device, generator=g)  # CN(0,1)
+    fe = torch.as_tensor(np.exp(-np.linalg.norm(irvec_el, axis=1) / decay_e), device=device)
+    fp = torch.as_tensor(np.repeat(np.exp(-np.linalg.norm(irvec_ep, axis=1) / decay_p), nw * nw * nm), device=device)
+    out *= fe[:, None]
+    out *= fp[None, :]
+    return out
+
+
+class DeviceOnlyWannierObject:
+    """A two-stage operator whose op_r exists only on the device (full-size generated workloads)."""
+
+    def __init__(self, op_dev, irvec, irvec_next):
+        self.op_r = op_dev
+        self.irvec = np.ascontiguousarray(irvec, dtype=np.int64)
+        self.irvec_next = np.ascontiguousarray(irvec_next, dtype=np.int64)
+        self.nr = self.irvec.shape[0]
+        self.ndata = op_dev.shape[1]
+
+
+def device_epmat_object(op_dev, irvec_el, irvec_ep):
+    return DeviceOnlyWannierObject(op_dev, irvec_el, irvec_ep)

@@ -67,6 +67,14 @@ EPB_API const char* epb_last_error(void);
 EPB_API int epb_version(void);
 /* Bytes of workspace currently held by the context. */
 EPB_API int epb_workspace_bytes(epb_ctx* ctx, uint64_t* bytes_host);
+/* Number of kernels this context has launched so far (instrumentation). */
+EPB_API int epb_launch_count(epb_ctx* ctx, int64_t* count_host);
+/* Per-kernel-family CUDA-event timing on the context stream (the reference's @timing /
+   TimerOutputs instrumentation, src/common/timer.jl:5-24). Families, in order: fourier_f64, zgemm,
+   eigh, rotation, rr_rotation, umma_h, umma_kq, umma_rr, split, other. epb_profile_read
+   synchronises, returns total ms and launch counts for the first n families, optionally resets. */
+EPB_API int epb_profile_enable(epb_ctx* ctx, int on);
+EPB_API int epb_profile_read(epb_ctx* ctx, double* ms_host, int64_t* count_host, int n, int reset);
 /* Test hook: make the N-th next workspace allocation fail (N = 0 disables). Drives the
    out-of-memory path without exhausting a GPU (src/calculator/eph_device_staging.jl:33-37). */
 EPB_API int epb_debug_fail_alloc(epb_ctx* ctx, int nth);
@@ -160,6 +168,32 @@ EPB_API int epb_window_filter(epb_ctx* ctx, const double* E, int64_t nw, int64_t
 EPB_API int epb_fill_iqs(epb_ctx* ctx, const int64_t* xkq_int, int64_t nkq, const int64_t* xk_int_host,
                  int64_t ng1, int64_t ng2, int64_t ng3, const int64_t* dense_hash_to_iq,
                  int64_t* iqs);
+
+/* ---- whole e-ph pass ---------------------------------------------------------------------- */
+typedef struct epb_model epb_model;
+
+/* Bind a model's device operators (the reference's Model fields el_ham, ph_dyn, mass, epmat in the
+   "el" layout; src/model.jl:24-85, src/model_new.jl:551-565) and upload the three R-vector sets.
+   The operators stay caller-owned and must outlive the model. flags bit 0: also build the
+   split-BF16 operand planes used by EPB_PREC_MIXED (one-time cost, like to_device,
+   ext/ElectronPhononCUDAExt.jl:51-53). */
+EPB_API int epb_model_create(epb_ctx* ctx, const double* ham_op, int64_t nw, const int64_t* irvec_el_host,
+                             int64_t nr_el, const double* dyn_op, const double* mass, int64_t nm,
+                             const int64_t* irvec_ph_host, int64_t nr_ph, const double* epmat_op,
+                             const int64_t* irvec_ep_host, int64_t nr_ep, int flags, epb_model** out);
+EPB_API int epb_model_destroy(epb_model* model);
+
+/* Full-band e-ph pass over random k x random q in the q convention: electrons at k and k+q,
+   phonons at q, g(k,q) = ukq^dagger g u_ph, g2 = |g|^2/(2 omega). Outputs: ek (nw x nk),
+   omega (nm x nq), g2sum (nm x nk) = sum over bands and q of g2, and, if g2_sample != NULL, the full
+   g2 block (nw x nw x nm) of every q with q % sample_stride == 0, laid out
+   (nw, nw, nm, nsamp, nk) with nsamp = ceil(nq / sample_stride). stats_host (4 int64, may be NULL):
+   [0] = g elements produced. Replaces: the per-(k, q) loop of run_eph_over_k_and_q
+   (src/calculator/run_eph_over_k_and_q.jl:251-330) run the batched way of
+   _loop_eph_over_k_and_kq_batched (src/calculator/run_eph_over_k_and_kq.jl:792-892). */
+EPB_API int epb_eph_pass(epb_ctx* ctx, epb_model* model, const double* xk, int64_t nk, const double* xq,
+                         int64_t nq, int prec, int64_t k_batch, int64_t sample_stride, double* ek_out,
+                         double* omega_out, double* g2sum_out, double* g2_sample, int64_t* stats_host);
 
 #ifdef __cplusplus
 }
