@@ -236,6 +236,9 @@ def run_epb(args):
     dom = max(prof.items(), key=lambda kv: kv[1][0])
     dom_name, (dom_ms, dom_cnt) = dom
     flops = family_flops(dom_name, args, args.k_batch)
+    tot_ms = sum(v[0] for v in prof.values())
+    profile = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / tot_ms, 4)}
+               for k, v in prof.items() if v[1]}
     roof = None
     if flops is not None and dom_cnt > 0:
         avg_s = dom_ms / dom_cnt * 1e-3
@@ -296,7 +299,7 @@ def run_epb(args):
             "vs_baseline": None, "dtype": "bf16x3/f32/f64" if prec == pipeline.PREC_MIXED else "f64",
             "data": "synthetic (seeded generator; random-init Wannier model of the config-2 shape)",
             "config": config_dict(args, prec_name), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": launches, "clocks": clocks, "impl": "epb"}
+            "gpu_launches": launches, "clocks": clocks, "impl": "epb", "profile_one_pass": profile}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:

@@ -105,6 +105,9 @@ struct epb_ctx {
   int fail_alloc_nth = 0;  // test hook
   // Small pinned host scratch for scalar read-backs.
   int64_t* pinned = nullptr;
+  // Device status words: [0] eigensolver non-convergence count, [1] eigensolver bad order count,
+  // [2] tensor-core GEMM timeout flag, [3] iq-hash miss count.
+  int* dstat = nullptr;
   // instrumentation
   int64_t launches = 0;          // kernels launched by the library on this context
   bool prof_on = false;

@@ -124,10 +124,14 @@ int epb_create(epb_ctx** out, int device, void* stream) {
   c->sm_count = prop.multiProcessorCount;
   c->cc_major = prop.major;
   c->cc_minor = prop.minor;
-  if (cudaMallocHost(&c->pinned, 64 * sizeof(int64_t)) != cudaSuccess) {
+  if (cudaMallocHost(&c->pinned, 64 * sizeof(int64_t)) != cudaSuccess ||
+      cudaMalloc(&c->dstat, 64 * sizeof(int)) != cudaSuccess ||
+      cudaMemset(c->dstat, 0, 64 * sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
+    if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->dstat) cudaFree(c->dstat);
     delete c;
-    set_error("epb_create: pinned host scratch allocation failed");
+    set_error("epb_create: status/scratch allocation failed");
     return EPB_ERR_OOM;
   }
   *out = c;
@@ -145,6 +149,7 @@ int epb_destroy(epb_ctx* ctx) {
   for (int i = 0; i < EPB_WS_NSLOTS; ++i)
     if (ctx->ws[i]) cudaFree(ctx->ws[i]);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  if (ctx->dstat) cudaFree(ctx->dstat);
   delete ctx;
   return EPB_OK;
 }

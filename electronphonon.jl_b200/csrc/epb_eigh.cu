@@ -484,28 +484,16 @@ int eigh_dispatch(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
   return EPB_ERR_ARG;
 }
 
+int eigh_check(epb_ctx* ctx);
+
 int eigh_run(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
   if (a.batch == 0) return EPB_OK;
-  void* ws = nullptr;
-  EPB_TRY(ws_get(ctx, EPB_WS_FLAGS, 64, &ws));
-  a.nonconv = (int*)ws;
-  a.badsize = a.nonconv + 1;
-  EPB_CUDA(cudaMemsetAsync(a.nonconv, 0, 2 * sizeof(int), ctx->stream));
+  a.nonconv = ctx->dstat + 0;
+  a.badsize = ctx->dstat + 1;
+  EPB_CUDA(cudaMemsetAsync(ctx->dstat, 0, 2 * sizeof(int), ctx->stream));
   a.max_sweeps = prec == EPB_PREC_FP64 ? 30 : 20;
   EPB_TRY(eigh_dispatch(ctx, a, nmax, prec));
-  // non-convergence is reported after a sync on the context stream
-  int* h = (int*)ctx->pinned;
-  EPB_CUDA(cudaMemcpyAsync(h, a.nonconv, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  EPB_CUDA(cudaStreamSynchronize(ctx->stream));
-  if (h[1] > 0) {
-    set_error("eigensolver: %d matrices have an order outside 1..%d (skipped)", h[1], nmax);
-    return EPB_ERR_ARG;
-  }
-  if (*h > 0) {
-    set_error("eigensolver: %d matrices reached the sweep limit", *h);
-    return EPB_ERR_NOCONVERGE;
-  }
-  return EPB_OK;
+  return eigh_check(ctx);
 }
 
 // Stream-ordered variant for the pass pipeline: counters accumulate in a context slot until
@@ -513,10 +501,6 @@ int eigh_run(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
 int eigh_async(epb_ctx* ctx, double2* A, int64_t n, int64_t batch, double* E, bool want_v,
                const double* mass, int prec) {
   if (batch == 0) return EPB_OK;
-  void* ws = nullptr;
-  bool fresh = ctx->ws[EPB_WS_EIGH] == nullptr;
-  EPB_TRY(ws_get(ctx, EPB_WS_EIGH, 64, &ws));
-  if (fresh) EPB_CUDA(cudaMemsetAsync(ws, 0, 64, ctx->stream));
   EighArgs a{};
   a.A = A;
   a.n_uniform = (int)n;
@@ -524,20 +508,20 @@ int eigh_async(epb_ctx* ctx, double2* A, int64_t n, int64_t batch, double* E, bo
   a.E = E;
   a.want_v = want_v;
   a.mass = mass;
-  a.nonconv = (int*)ws;
-  a.badsize = a.nonconv + 1;
+  a.nonconv = ctx->dstat + 0;
+  a.badsize = ctx->dstat + 1;
   a.max_sweeps = prec == EPB_PREC_FP64 ? 30 : 20;
   return eigh_dispatch(ctx, a, (int)n, prec);
 }
 
+// Read back (one sync) and clear the eigensolver status words accumulated since the last check.
 int eigh_check(epb_ctx* ctx) {
-  if (!ctx->ws[EPB_WS_EIGH]) return EPB_OK;
   int* h = (int*)ctx->pinned;
-  EPB_CUDA(cudaMemcpyAsync(h, ctx->ws[EPB_WS_EIGH], 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  EPB_CUDA(cudaMemsetAsync(ctx->ws[EPB_WS_EIGH], 0, 64, ctx->stream));
+  EPB_CUDA(cudaMemcpyAsync(h, ctx->dstat, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  EPB_CUDA(cudaMemsetAsync(ctx->dstat, 0, 2 * sizeof(int), ctx->stream));
   EPB_CUDA(cudaStreamSynchronize(ctx->stream));
   if (h[1] > 0) {
-    set_error("eigensolver: %d matrices have an unsupported order (skipped)", h[1]);
+    set_error("eigensolver: %d matrices have an order outside the supported range (skipped)", h[1]);
     return EPB_ERR_ARG;
   }
   if (h[0] > 0) {

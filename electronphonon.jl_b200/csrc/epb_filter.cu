@@ -165,9 +165,7 @@ int epb_fill_iqs(epb_ctx* ctx, const int64_t* xkq_int, int64_t nkq, const int64_
   EPB_CHECK_ARG(nkq == 0 || (xkq_int && dense_hash_to_iq && iqs), "epb_fill_iqs: NULL buffer");
   EPB_TRY(make_current(ctx));
   if (nkq == 0) return EPB_OK;
-  void* ws = nullptr;
-  EPB_TRY(ws_get(ctx, EPB_WS_FLAGS, 64, &ws));
-  int* miss = (int*)ws;
+  int* miss = ctx->dstat + 3;
   EPB_CUDA(cudaMemsetAsync(miss, 0, sizeof(int), ctx->stream));
   fill_iqs_kernel<<<(unsigned)cdiv(nkq, 256), 256, 0, ctx->stream>>>(
       xkq_int, nkq, xk_int_host[0], xk_int_host[1], xk_int_host[2], ng1, ng2, ng3, dense_hash_to_iq, iqs, miss);
