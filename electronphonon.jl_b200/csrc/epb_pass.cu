@@ -72,6 +72,11 @@ __global__ void eph_rot_reduce_kernel(const double2* __restrict__ g, const doubl
   double2* ps = us + nw * nb;
   double* red = reinterpret_cast<double*>(ps + nm * nm);  // [nm]
   for (int e = threadIdx.x; e < nm; e += blockDim.x) red[e] = 0.0;
+  // Per-thread partial sums: element e belongs to mode e / (nb*nb); with blockDim a multiple of
+  // nb*nb each thread always sees the same modes, so 32 register accumulators cover nm <= 32.
+  double part[32];
+#pragma unroll
+  for (int i = 0; i < 32; ++i) part[i] = 0.0;
   for (int64_t q = blockIdx.x; q < nq; q += gridDim.x) {
     __syncthreads();
     const double2* gq = g + q * (int64_t)ng;
@@ -97,7 +102,18 @@ __global__ void eph_rot_reduce_kernel(const double2* __restrict__ g, const doubl
       for (int jm = 0; jm < nm; ++jm) cfma(acc, ts[mnidx + jm * mn], ps[jm + nu * nm]);
       double v = (acc.x * acc.x + acc.y * acc.y) / (2.0 * omega[nu + q * nm]);
       if (samp) sq[e] = v;
-      atomicAdd(&red[nu], v);
+#pragma unroll
+      for (int i = 0; i < 32; ++i)
+        if (i == nu) part[i] += v;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    if (i < nm) {
+      double v = part[i];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&red[i], v);
     }
   }
   __syncthreads();

@@ -246,7 +246,8 @@ struct GemmCfg {
   static constexpr int STAGE = NPL * TILE_BYTES + NPL * B_SUB * B_TILE;
   static constexpr int STAGES = (200 * 1024) / STAGE > 4 ? 4 : (200 * 1024) / STAGE;
   static constexpr int SMEM = STAGES * STAGE + 1024 /*align*/ + 256 /*barriers*/;
-  static constexpr int TMEM_COLS = 2 * NT < 32 ? 32 : 2 * NT;
+  // two accumulators (leading h*h term, correction terms) x two alternating buffers
+  static constexpr int TMEM_COLS = 4 * NT < 32 ? 32 : 4 * NT;
 };
 
 template <bool BF16, int NPL, int NT>
@@ -343,7 +344,10 @@ __global__ void __launch_bounds__(192, 1) split_gemm_kernel(SplitGemmArgs a) {
       const uint32_t use = (uint32_t)(u >> 1) & 1u;
       if (!mbar_wait(&tempty[b], use ^ 1u, err, a.timeout)) break;
       tc_fence_after();
-      const uint32_t dcol = tmem + b * NT;
+      // accumulator 0 (columns [0, NT)) takes the leading h*h product, accumulator 1 (columns
+      // [NT, 2NT)) all correction products: the tensor core aligns addends to the accumulator, so
+      // O(2^-16) corrections added onto the O(1) sum would lose their low bits.
+      const uint32_t dcol = tmem + b * 2 * NT;
       for (int kc = 0; kc < a.KC; ++kc) {
         if (!mbar_wait(&full[s], ph, err, a.timeout)) {
           ok = false;
@@ -355,9 +359,12 @@ __global__ void __launch_bounds__(192, 1) split_gemm_kernel(SplitGemmArgs a) {
         for (int sub = 0; sub < 4; ++sub) {
 #pragma unroll
           for (int pr = 0; pr < Pr::N; ++pr) {
+            const bool lead = Pr::a(pr) == 0 && Pr::b(pr) == 0;
             uint64_t ad = smem_desc_sw128(st + Pr::a(pr) * TILE_BYTES + sub * 32);
             uint64_t bd = smem_desc_sw128(st + NPL * TILE_BYTES + Pr::b(pr) * Cfg::B_SUB * Cfg::B_TILE + sub * 32);
-            mma_f16(dcol, ad, bd, IDESC, (kc | sub | pr) != 0 ? 1u : 0u);
+            // first MMA into each accumulator of the tile overwrites it
+            const bool first = kc == 0 && sub == 0 && (lead || pr == 0);
+            mma_f16(dcol + (lead ? 0u : (uint32_t)NT), ad, bd, IDESC, first ? 0u : 1u);
           }
         }
         mma_commit(&empty[s]);
@@ -392,13 +399,15 @@ __global__ void __launch_bounds__(192, 1) split_gemm_kernel(SplitGemmArgs a) {
       const bool row_ok = row < a.m_valid;
 #pragma unroll 1
       for (int c0 = 0; c0 < NT; c0 += 16) {
-        float v[16];
-        tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + b * NT + c0, v);
+        float v[16], w[16];
+        const uint32_t ta = tmem + ((uint32_t)(quarter * 32) << 16) + b * 2 * NT + c0;
+        tmem_ld16(ta, v);
+        tmem_ld16(ta + NT, w);
         if (row_ok) {
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
             int64_t col = nt * NT + c0 + j;
-            if (col < a.n_valid) cb[col * a.ldc_n] = v[j];
+            if (col < a.n_valid) cb[col * a.ldc_n] = (float)((double)v[j] + (double)w[j]);
           }
         }
       }
