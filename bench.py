@@ -158,6 +158,8 @@ def family_flops(name, args, nkb):
         return 8.0 * nw2 * nm * nr_ep * args.nq
     if name == "umma_kq":    # kR->kq for a k batch
         return 8.0 * nw2 * nm * nr_ep * args.nq * nkb
+    if name == "umma_rr":    # RR->kR for 256 k: (nw^2 nm nr_ep) x nr_el x 256
+        return 8.0 * nw2 * nm * nr_ep * nr_el * min(256, args.nk)
     if name in ("fourier_f64", "umma_h"):  # dominated by H(k+q): nw^2 x nr_el per k+q point
         return 8.0 * nw2 * nr_el * args.nq * nkb
     return None
@@ -243,7 +245,7 @@ def run_epb(args):
     if flops is not None and dom_cnt > 0:
         avg_s = dom_ms / dom_cnt * 1e-3
         if dom_name.startswith("umma"):
-            nprod = 6
+            nprod = 6  # split BF16x3: six bf16 products per real MAC
             peak = peaks["bf16_tflops_sustained"] / nprod
             psrc = f"{peak_src} bf16 sustained / {nprod} split products"
         else:

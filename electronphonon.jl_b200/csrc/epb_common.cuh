@@ -126,6 +126,21 @@ struct epb_rset {
   std::vector<int64_t> host;  // 3 x nr
 };
 
+// A model's hot-path operators (caller-owned device memory) plus the library's derived data.
+struct epb_model {
+  epb_ctx* ctx = nullptr;
+  int64_t nw = 0, nm = 0, nr_el = 0, nr_ph = 0, nr_ep = 0;
+  const double2* ham = nullptr;   // (nw^2, nr_el)
+  const double2* dyn = nullptr;   // (nm^2, nr_ph)
+  const double* mass = nullptr;   // (nm)
+  const double2* epmat = nullptr; // (nw^2 nm nr_ep, nr_el)
+  epb_rset* rs_el = nullptr;
+  epb_rset* rs_ph = nullptr;
+  epb_rset* rs_ep = nullptr;
+  // mixed-precision operand planes (owned), see epb_umma.cu
+  void* mixed = nullptr;
+};
+
 namespace epb {
 
 // Profiler brackets around a launch (no-ops unless epb_profile_enable was called).

@@ -144,6 +144,9 @@ struct EighArgs {
   int* nonconv;          // device counter of matrices that hit the sweep limit
   int* badsize;          // device counter of matrices whose order exceeds the kernel's maximum
   const double* mass;    // phonon mode: non-null => mass scaling + omega = sign sqrt
+  const float* Hp;       // mixed kernel only: packed FP32 Hermitian input (n*n floats per matrix:
+                         // Re H_ij for i <= j then Im H_ij for i < j, both column by column)
+  float2* U32;           // mixed kernel only: eigenvectors as complex64 (n x n per matrix)
 };
 
 // Shared memory layout per team (elements of the solve type T):
@@ -281,13 +284,20 @@ __global__ void eigh_mixed_kernel(EighArgs a) {
     }
     const int64_t aoff = a.a_off ? a.a_off[b] : b * (int64_t)n * n;
     const int64_t eoff = a.e_off ? a.e_off[b] : b * (int64_t)n;
-    double2* Ag = a.A + aoff;
+    double2* Ag = a.A ? a.A + aoff : nullptr;
+    const float* Hp = a.Hp ? a.Hp + b * (int64_t)n * n : nullptr;
     const int lda = n + 1;
+    const int nre = n * (n + 1) / 2;
     double fro2 = 0;
     for (int e = tid; e < n * n; e += TEAM) {
       int i = e % n, j = e / n;
       double2 v;
-      if (i <= j) {
+      if (Hp) {
+        int ii = i <= j ? i : j, jj = i <= j ? j : i;
+        double re = Hp[jj * (jj + 1) / 2 + ii];
+        double im = ii < jj ? Hp[nre + jj * (jj - 1) / 2 + ii] : 0.0;
+        v = make_double2(re, i <= j ? im : -im);
+      } else if (i <= j) {
         v = Ag[i + (int64_t)j * n];
       } else {
         double2 u = Ag[j + (int64_t)i * n];
@@ -413,7 +423,10 @@ __global__ void eigh_mixed_kernel(EighArgs a) {
           o.x *= s;
           o.y *= s;
         }
-        Ag[row + (int64_t)rank * n] = o;
+        if (a.U32)
+          a.U32[b * (int64_t)n * n + row + (int64_t)rank * n] = make_float2((float)o.x, (float)o.y);
+        else
+          Ag[row + (int64_t)rank * n] = o;
       }
     }
     team_sync<TEAM>();
@@ -512,6 +525,23 @@ int eigh_async(epb_ctx* ctx, double2* A, int64_t n, int64_t batch, double* E, bo
   a.badsize = ctx->dstat + 1;
   a.max_sweeps = prec == EPB_PREC_FP64 ? 30 : 20;
   return eigh_dispatch(ctx, a, (int)n, prec);
+}
+
+// Mixed-precision eigensolve of packed FP32 Hermitian matrices (the tensor-core H(k+q) output),
+// eigenvectors written as complex64, eigenvalues (optional) as FP64. Stream-ordered.
+int eigh_mixed_packed(epb_ctx* ctx, const float* Hp, int64_t n, int64_t batch, float2* U, double* E) {
+  if (batch == 0) return EPB_OK;
+  EighArgs a{};
+  a.Hp = Hp;
+  a.U32 = U;
+  a.n_uniform = (int)n;
+  a.batch = batch;
+  a.E = E;
+  a.want_v = 1;
+  a.nonconv = ctx->dstat + 0;
+  a.badsize = ctx->dstat + 1;
+  a.max_sweeps = 20;
+  return eigh_dispatch(ctx, a, (int)n, EPB_PREC_MIXED);
 }
 
 // Read back (one sync) and clear the eigensolver status words accumulated since the last check.

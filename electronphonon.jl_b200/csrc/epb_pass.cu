@@ -14,19 +14,7 @@
 
 #include "epb_common.cuh"
 
-struct epb_model {
-  epb_ctx* ctx = nullptr;
-  int64_t nw = 0, nm = 0, nr_el = 0, nr_ph = 0, nr_ep = 0;
-  const double2* ham = nullptr;   // (nw^2, nr_el)
-  const double2* dyn = nullptr;   // (nm^2, nr_ph)
-  const double* mass = nullptr;   // (nm)
-  const double2* epmat = nullptr; // (nw^2 nm nr_ep, nr_el)
-  epb_rset* rs_el = nullptr;
-  epb_rset* rs_ph = nullptr;
-  epb_rset* rs_ep = nullptr;
-  // mixed-precision operand planes (owned), see epb_umma.cu
-  void* mixed = nullptr;
-};
+
 
 namespace epb {
 
@@ -37,10 +25,9 @@ int zgemm_nn(epb_ctx* ctx, const double2* A, int64_t lda, const double2* B, int6
 int eigh_async(epb_ctx* ctx, double2* A, int64_t n, int64_t batch, double* E, bool want_v,
                const double* mass, int prec);
 int eigh_check(epb_ctx* ctx);
-int mixed_pass_batch(epb_ctx* ctx, epb_model* m, const double* xk_b, int64_t nkb, const double* xq,
-                     int64_t nq, const double2* uk_b, const double2* uph, const double* omega,
-                     const double2* phase, double* g2sum_b, double* g2_sample_b, int64_t sample_stride,
-                     int64_t* stats);
+int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double* xq, int64_t nq,
+               const double2* uph, const double* omega, double* ek_out, double* g2sum, double* g2_sample,
+               int64_t sample_stride, int64_t kbi_max);
 int mixed_model_prepare(epb_ctx* ctx, epb_model* m);
 void mixed_model_free(epb_model* m);
 
@@ -193,11 +180,12 @@ int epb_eph_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const
   };
   const size_t o_dq = carve(16ull * nm * nm * nq);
   const size_t o_ph = carve(16ull * nr_ep * nq);
+  const bool f64 = prec == EPB_PREC_FP64;
   const size_t o_hk = carve(16ull * nw2 * k_batch);
-  const size_t o_G = carve(16ull * nw2 * nm * nr_ep * k_batch);
-  const size_t o_xkq = carve(24ull * k_batch * nq);
-  const size_t o_hkq = carve(16ull * nw2 * k_batch * nq);
-  const size_t o_g = prec == EPB_PREC_FP64 ? carve(16ull * nw2 * nm * nq) : carve(0);
+  const size_t o_G = carve(f64 ? 16ull * nw2 * nm * nr_ep * k_batch : 0);
+  const size_t o_xkq = carve(f64 ? 24ull * k_batch * nq : 0);
+  const size_t o_hkq = carve(f64 ? 16ull * nw2 * k_batch * nq : 0);
+  const size_t o_g = carve(f64 ? 16ull * nw2 * nm * nq : 0);
   void* base = nullptr;
   EPB_TRY(ws_get(ctx, EPB_WS_PASS0, off, &base));
   char* b = (char*)base;
@@ -225,7 +213,10 @@ int epb_eph_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const
     EPB_CUDA(cudaFuncSetAttribute(eph_rot_reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     attr = true;
   }
-  for (int64_t k0 = 0; k0 < nk; k0 += k_batch) {
+  if (prec == EPB_PREC_MIXED) {
+    EPB_TRY(mixed_pass(ctx, m, xk, nk, xq, nq, Dq, omega_out, ek_out, g2sum_out, g2_sample, sample_stride, k_batch));
+  }
+  for (int64_t k0 = 0; prec == EPB_PREC_FP64 && k0 < nk; k0 += k_batch) {
     const int64_t nkb = nk - k0 < k_batch ? nk - k0 : k_batch;
     const double* xkb = xk + 3 * k0;
     // electrons at k: FP64 in both modes (2048 points; the k side is not the bulk of the work)
@@ -234,25 +225,20 @@ int epb_eph_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const
     // x_{k+q}
     xkq_kernel<<<(unsigned)cdiv(nkb * nq, 256), 256, 0, ctx->stream>>>(xkb, nkb, xq, nq, Xkq);
     EPB_LAUNCH_CHECK();
-    if (prec == EPB_PREC_FP64) {
-      EPB_TRY(epb_eph_RR_to_kR(ctx, (const double*)m->epmat, nw, nm, nr_ep, m->rs_el, xkb, nkb,
-                               (const double*)Hk, nw, nullptr, (double*)G, EPB_PREC_FP64));
-      EPB_TRY(fourier_f64(ctx, m->ham, nw2, nw2, m->rs_el, Xkq, nkb * nq, Hkq, nw2));
-      EPB_TRY(eigh_async(ctx, Hkq, nw, nkb * nq, nullptr, true, nullptr, EPB_PREC_FP64));
-      const int64_t ndata = nw2 * nm;
-      for (int64_t kl = 0; kl < nkb; ++kl) {
-        EPB_TRY(zgemm_nn(ctx, G + kl * ndata * nr_ep, ndata, P, nr_ep, gb, ndata, ndata, nq, nr_ep));
-        int64_t blocks = nq < (int64_t)ctx->sm_count * 8 ? nq : (int64_t)ctx->sm_count * 8;
-        prof_begin(ctx, EPB_PROF_ROT);
-        eph_rot_reduce_kernel<<<(unsigned)blocks, 256, rsmem, ctx->stream>>>(
-            gb, Hkq + kl * nq * nw2, Dq, omega_out, (int)nw, (int)nm, nq, g2sum_out + nm * (k0 + kl),
-            g2_sample ? g2_sample + (k0 + kl) * nsamp * nw2 * nm : nullptr, sample_stride);
-        prof_end(ctx);
-        EPB_LAUNCH_CHECK();
-      }
-    } else {
-      EPB_TRY(mixed_pass_batch(ctx, m, xkb, nkb, xq, nq, Hk, Dq, omega_out, P, g2sum_out + nm * k0,
-                               g2_sample ? g2_sample + k0 * nsamp * nw2 * nm : nullptr, sample_stride, stats));
+    EPB_TRY(epb_eph_RR_to_kR(ctx, (const double*)m->epmat, nw, nm, nr_ep, m->rs_el, xkb, nkb,
+                             (const double*)Hk, nw, nullptr, (double*)G, EPB_PREC_FP64));
+    EPB_TRY(fourier_f64(ctx, m->ham, nw2, nw2, m->rs_el, Xkq, nkb * nq, Hkq, nw2));
+    EPB_TRY(eigh_async(ctx, Hkq, nw, nkb * nq, nullptr, true, nullptr, EPB_PREC_FP64));
+    const int64_t ndata = nw2 * nm;
+    for (int64_t kl = 0; kl < nkb; ++kl) {
+      EPB_TRY(zgemm_nn(ctx, G + kl * ndata * nr_ep, ndata, P, nr_ep, gb, ndata, ndata, nq, nr_ep));
+      int64_t blocks = nq < (int64_t)ctx->sm_count * 8 ? nq : (int64_t)ctx->sm_count * 8;
+      prof_begin(ctx, EPB_PROF_ROT);
+      eph_rot_reduce_kernel<<<(unsigned)blocks, 256, rsmem, ctx->stream>>>(
+          gb, Hkq + kl * nq * nw2, Dq, omega_out, (int)nw, (int)nm, nq, g2sum_out + nm * (k0 + kl),
+          g2_sample ? g2_sample + (k0 + kl) * nsamp * nw2 * nm : nullptr, sample_stride);
+      prof_end(ctx);
+      EPB_LAUNCH_CHECK();
     }
   }
   EPB_TRY(eigh_check(ctx));

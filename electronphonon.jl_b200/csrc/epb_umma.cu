@@ -26,8 +26,6 @@
 #include "epb_common.cuh"
 #include "epb_umma.cuh"
 
-struct epb_model;
-
 namespace epb {
 
 using namespace umma;
@@ -76,36 +74,69 @@ __device__ __forceinline__ int64_t tiled_offset(int64_t row, int64_t k, int64_t 
 }
 
 // ---------------------------------------------------------------------------------------------
-// Packers. All write every element of the padded planes (zeros in the padding).
+// Packers. Each thread produces 8 consecutive K' values of one row, i.e. one 16-byte chunk of the
+// swizzled tile per plane. The K' axis holds the cos coefficients at [0, K) and the sin
+// coefficients at [koff, koff + K) with koff = round_up(K, 8); everything else is zero.
 
-// Generic complex operand A (M x K complex, column-major, leading dim ld) -> A2 (2M_pad x K2_pad).
+template <bool BF16, int NPL>
+__device__ __forceinline__ void store_split8(uint8_t* base, int64_t plane_bytes, int64_t off, const double* v) {
+  double r[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) r[e] = v[e];
+#pragma unroll
+  for (int p = 0; p < NPL; ++p) {
+    uint16_t b[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      b[e] = to_half_bits<BF16>(r[e]);
+      r[e] -= from_half_bits<BF16>(b[e]);
+    }
+    uint4 w;
+    w.x = (uint32_t)b[0] | ((uint32_t)b[1] << 16);
+    w.y = (uint32_t)b[2] | ((uint32_t)b[3] << 16);
+    w.z = (uint32_t)b[4] | ((uint32_t)b[5] << 16);
+    w.w = (uint32_t)b[6] | ((uint32_t)b[7] << 16);
+    *reinterpret_cast<uint4*>(base + p * plane_bytes + off) = w;
+  }
+}
+
+__host__ __device__ __forceinline__ int64_t sin_offset(int64_t K) { return (K + 7) / 8 * 8; }
+__host__ __device__ __forceinline__ int64_t kchunks(int64_t K) { return (sin_offset(K) + K + 63) / 64; }
+
+// Generic complex operand A (M x K complex, column-major, leading dim ld) -> A2 rows 2i / 2i+1.
 template <bool BF16, int NPL>
 __global__ void pack_a_complex_kernel(const double2* __restrict__ a, int64_t ld, int64_t M, int64_t K,
                                       int64_t rows_pad, int64_t KC, uint8_t* __restrict__ planes,
                                       int64_t plane_bytes) {
-  const int64_t Kp = KC * 64;
-  const int64_t total = rows_pad * Kp;
+  const int64_t nch = KC * 8, koff = sin_offset(K);
+  const int64_t total = rows_pad * nch;
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
-    int64_t k = idx % Kp, row = idx / Kp;
-    double v = 0.0;
+    int64_t ch = idx % nch, row = idx / nch;
     int64_t i = row >> 1;
     int part = (int)(row & 1);
-    if (i < M) {
-      if (k < K) {
-        double2 x = a[i + k * ld];
-        v = part == 0 ? x.x : x.y;
-      } else if (k < 2 * K) {
-        double2 x = a[i + (k - K) * ld];
-        v = part == 0 ? -x.y : x.x;
+    double v[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      int64_t k = ch * 8 + e;
+      double x = 0.0;
+      if (i < M) {
+        if (k < K) {
+          double2 z = a[i + k * ld];
+          x = part == 0 ? z.x : z.y;
+        } else if (k >= koff && k < koff + K) {
+          double2 z = a[i + (k - koff) * ld];
+          x = part == 0 ? -z.y : z.x;
+        }
       }
+      v[e] = x;
     }
-    store_split<BF16, NPL>(planes, plane_bytes, tiled_offset(row, k, KC), v);
+    store_split8<BF16, NPL>(planes, plane_bytes, tiled_offset(row, ch * 8, KC), v);
   }
 }
 
 // Hermitian operand (nw x nw per R, column-major op_r (nw^2 x K)) -> packed real rows:
-// rows [0, nw(nw+1)/2): Re H_ij (i <= j, ordered j-major), rows after: Im H_ij (i < j).
+// rows [0, nw(nw+1)/2): Re H_ij (i <= j, column by column), then Im H_ij (i < j).
 __device__ __forceinline__ void herm_row_to_ij(int row, int nw, int& i, int& j, int& part) {
   const int nre = nw * (nw + 1) / 2;
   int r = row;
@@ -113,7 +144,6 @@ __device__ __forceinline__ void herm_row_to_ij(int row, int nw, int& i, int& j, 
   if (r >= nre) {
     part = 1;
     r -= nre;
-    // strictly upper: column j has j entries (i < j)
     int jj = 1;
     while (r >= jj) {
       r -= jj;
@@ -135,40 +165,50 @@ __device__ __forceinline__ void herm_row_to_ij(int row, int nw, int& i, int& j, 
 template <bool BF16, int NPL>
 __global__ void pack_a_herm_kernel(const double2* __restrict__ op, int nw, int64_t K, int64_t rows_pad,
                                    int64_t KC, uint8_t* __restrict__ planes, int64_t plane_bytes) {
-  const int64_t Kp = KC * 64;
-  const int64_t total = rows_pad * Kp;
+  const int64_t nch = KC * 8, koff = sin_offset(K);
+  const int64_t total = rows_pad * nch;
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
-    int64_t k = idx % Kp, row = idx / Kp;
-    double v = 0.0;
-    if (row < (int64_t)nw * nw && k < 2 * K) {
-      int i, j, part;
-      herm_row_to_ij((int)row, nw, i, j, part);
-      int64_t kk = k < K ? k : k - K;
-      double2 x = op[(i + (int64_t)j * nw) + kk * (int64_t)nw * nw];
-      if (part == 0)
-        v = k < K ? x.x : -x.y;   // Re H = Re h cos - Im h sin
-      else
-        v = k < K ? x.y : x.x;    // Im H = Im h cos + Re h sin
+    int64_t ch = idx % nch, row = idx / nch;
+    double v[8];
+    int i = 0, j = 0, part = 0;
+    const bool live = row < (int64_t)nw * nw;
+    if (live) herm_row_to_ij((int)row, nw, i, j, part);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      int64_t k = ch * 8 + e;
+      double x = 0.0;
+      if (live) {
+        if (k < K) {
+          double2 z = op[(i + (int64_t)j * nw) + k * (int64_t)nw * nw];
+          x = part == 0 ? z.x : z.y;        // cos coefficient: Re h (real row) / Im h (imag row)
+        } else if (k >= koff && k < koff + K) {
+          double2 z = op[(i + (int64_t)j * nw) + (k - koff) * (int64_t)nw * nw];
+          x = part == 0 ? -z.y : z.x;       // sin coefficient: -Im h (real row) / Re h (imag row)
+        }
+      }
+      v[e] = x;
     }
-    store_split<BF16, NPL>(planes, plane_bytes, tiled_offset(row, k, KC), v);
+    store_split8<BF16, NPL>(planes, plane_bytes, tiled_offset(row, ch * 8, KC), v);
   }
 }
 
-// Phase operand: column j of B2 = [cos 2 pi R.x_j (K) ; sin 2 pi R.x_j (K) ; 0], stored as the
-// K-major row j. x_j = xa[:, ja] + xb[:, jb] with (ja, jb) = (j / nb, j % nb) when xb != null
-// (x_{k+q} for every pair of a k batch), else x_j = xa[:, j].
+// Phase operand: row j of B2 = [cos 2 pi R.x_j | sin 2 pi R.x_j] (K-major), x_j = xa[:, j / nb] +
+// xb[:, j % nb] when xb != null (x_{k+q} for every pair of a k batch), else x_j = xa[:, j].
 template <bool BF16, int NPL>
 __global__ void pack_b_phase_kernel(const int4* __restrict__ rv, int64_t K, const double* __restrict__ xa,
                                     const double* __restrict__ xb, int64_t nb, int64_t N, int64_t rows_pad,
                                     int64_t KC, uint8_t* __restrict__ planes, int64_t plane_bytes) {
-  const int64_t total = rows_pad * K;  // one thread per (point, R): writes both cos and sin
+  const int64_t koff = sin_offset(K);
+  const int64_t ncos = koff / 8;           // chunks covering [0, koff)
+  const int64_t nch = KC * 8;
+  const int64_t total = rows_pad * ncos;    // one thread per (point, 8 R vectors): cos and sin chunks
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
-    int64_t p = idx % K, j = idx / K;
-    double c = 0.0, s = 0.0;
+    int64_t ch = idx % ncos, j = idx / ncos;
+    double c[8], sn[8];
+    double x0 = 0, x1 = 0, x2 = 0;
     if (j < N) {
-      double x0, x1, x2;
       if (xb) {
         int64_t ja = j / nb, jb = j % nb;
         x0 = xa[3 * ja] + xb[3 * jb];
@@ -179,24 +219,25 @@ __global__ void pack_b_phase_kernel(const int4* __restrict__ rv, int64_t K, cons
         x1 = xa[3 * j + 1];
         x2 = xa[3 * j + 2];
       }
-      int4 r = rv[p];
-      double t = rdotx(r.x, r.y, r.z, x0, x1, x2);
-      double2 e = cis2pi(t);
-      c = e.x;
-      s = e.y;
     }
-    store_split<BF16, NPL>(planes, plane_bytes, tiled_offset(j, p, KC), c);
-    store_split<BF16, NPL>(planes, plane_bytes, tiled_offset(j, K + p, KC), s);
-  }
-  // zero the K padding columns [2K, Kp)
-  const int64_t Kp = KC * 64;
-  const int64_t npad = Kp - 2 * K;
-  if (npad > 0) {
-    const int64_t tp = rows_pad * npad;
-    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < tp;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-      int64_t k = 2 * K + idx % npad, j = idx / npad;
-      store_split<BF16, NPL>(planes, plane_bytes, tiled_offset(j, k, KC), 0.0);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      int64_t p = ch * 8 + e;
+      c[e] = 0.0;
+      sn[e] = 0.0;
+      if (j < N && p < K) {
+        int4 r = rv[p];
+        double2 z = cis2pi(rdotx(r.x, r.y, r.z, x0, x1, x2));
+        c[e] = z.x;
+        sn[e] = z.y;
+      }
+    }
+    store_split8<BF16, NPL>(planes, plane_bytes, tiled_offset(j, ch * 8, KC), c);
+    store_split8<BF16, NPL>(planes, plane_bytes, tiled_offset(j, koff + ch * 8, KC), sn);
+    // trailing zero chunks beyond koff + koff (when KC*64 > 2*koff)
+    for (int64_t z = 2 * ncos + ch; z < nch; z += ncos) {
+      double zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      store_split8<BF16, NPL>(planes, plane_bytes, tiled_offset(j, z * 8, KC), zero);
     }
   }
 }
@@ -506,11 +547,11 @@ int split_gemm_check(epb_ctx* ctx) {
 
 int pack_a_complex(epb_ctx* ctx, const double2* a, int64_t ld, int64_t M, int64_t K, Planes& out, uint8_t* mem) {
   out.rows_pad = round_up(2 * M, 128);
-  out.KC = cdiv(2 * K, 64);
+  out.KC = kchunks(K);
   out.plane_bytes = plane_bytes_for(out.rows_pad, out.KC);
   out.npl = MX_NPL;
   out.p = mem;
-  int64_t total = out.rows_pad * out.KC * 64;
+  int64_t total = out.rows_pad * out.KC * 8;
   prof_begin(ctx, EPB_PROF_SPLIT);
   pack_a_complex_kernel<MX_BF16, MX_NPL><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
       a, ld, M, K, out.rows_pad, out.KC, out.p, out.plane_bytes);
@@ -521,11 +562,11 @@ int pack_a_complex(epb_ctx* ctx, const double2* a, int64_t ld, int64_t M, int64_
 
 int pack_a_herm(epb_ctx* ctx, const double2* op, int nw, int64_t K, Planes& out, uint8_t* mem) {
   out.rows_pad = round_up((int64_t)nw * nw, 128);
-  out.KC = cdiv(2 * K, 64);
+  out.KC = kchunks(K);
   out.plane_bytes = plane_bytes_for(out.rows_pad, out.KC);
   out.npl = MX_NPL;
   out.p = mem;
-  int64_t total = out.rows_pad * out.KC * 64;
+  int64_t total = out.rows_pad * out.KC * 8;
   prof_begin(ctx, EPB_PROF_SPLIT);
   pack_a_herm_kernel<MX_BF16, MX_NPL><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(op, nw, K, out.rows_pad, out.KC,
                                                                                     out.p, out.plane_bytes);
@@ -537,11 +578,11 @@ int pack_a_herm(epb_ctx* ctx, const double2* op, int nw, int64_t K, Planes& out,
 int pack_b_phase(epb_ctx* ctx, const epb_rset* rs, const double* xa, const double* xb, int64_t nb, int64_t N,
                  Planes& out, uint8_t* mem) {
   out.rows_pad = round_up(N, MX_NT);
-  out.KC = cdiv(2 * rs->nr, 64);
+  out.KC = kchunks(rs->nr);
   out.plane_bytes = plane_bytes_for(out.rows_pad, out.KC);
   out.npl = MX_NPL;
   out.p = mem;
-  int64_t total = out.rows_pad * rs->nr;
+  int64_t total = out.rows_pad * (sin_offset(rs->nr) / 8);
   prof_begin(ctx, EPB_PROF_SPLIT);
   pack_b_phase_kernel<MX_BF16, MX_NPL><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
       rs->dev, rs->nr, xa, xb, nb, N, out.rows_pad, out.KC, out.p, out.plane_bytes);
@@ -551,7 +592,7 @@ int pack_b_phase(epb_ctx* ctx, const epb_rset* rs, const double* xa, const doubl
 }
 
 int64_t planes_bytes(int64_t rows, int64_t K) {
-  return MX_NPL * plane_bytes_for(round_up(rows, 128), cdiv(2 * K, 64));
+  return MX_NPL * plane_bytes_for(round_up(rows, 128), kchunks(K));
 }
 
 __global__ void c64_to_c128_kernel(const float2* __restrict__ in, double2* __restrict__ out, int64_t M,
@@ -571,7 +612,7 @@ int fourier_mixed(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, const 
   if (M == 0 || N == 0) return EPB_OK;
   const int64_t K = rs->nr;
   const int64_t a_bytes = planes_bytes(2 * M, K);
-  const int64_t b_bytes = MX_NPL * plane_bytes_for(round_up(N, MX_NT), cdiv(2 * K, 64));
+  const int64_t b_bytes = MX_NPL * plane_bytes_for(round_up(N, MX_NT), kchunks(K));
   const int64_t c_bytes = 8 * M * N;
   void* ws = nullptr;
   EPB_TRY(ws_get(ctx, EPB_WS_SPLIT_A, a_bytes + b_bytes + c_bytes + 1024, &ws));
@@ -587,22 +628,291 @@ int fourier_mixed(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, const 
   return split_gemm_check(ctx);
 }
 
+// =============================================================================================
+// Mixed-precision e-ph pass.
+
+struct MixedModel {
+  uint8_t* mem = nullptr;
+  Planes H;   // H(R), Hermitian-packed rows (nw^2), K = nr_el
+  Planes EP;  // g(Re, Rp), complex rows (2 * nw^2 nm nr_ep), K = nr_el
+};
+
 int mixed_model_prepare(epb_ctx* ctx, epb_model* m) {
-  (void)ctx;
-  (void)m;
-  set_error("mixed-precision model planes are not available in this build");
-  return EPB_ERR_UNSUPPORTED;
+  const int64_t nw = m->nw, nd_ep = m->nw * m->nw * m->nm * m->nr_ep;
+  const int64_t hb = MX_NPL * plane_bytes_for(round_up(nw * nw, 128), kchunks(m->nr_el));
+  const int64_t eb = MX_NPL * plane_bytes_for(round_up(2 * nd_ep, 128), kchunks(m->nr_el));
+  MixedModel* mm = new MixedModel();
+  cudaError_t e = cudaMalloc(&mm->mem, hb + eb + 1024);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    delete mm;
+    set_error("mixed model planes: allocation of %lld bytes failed", (long long)(hb + eb));
+    return EPB_ERR_OOM;
+  }
+  uint8_t* base = (uint8_t*)(((uintptr_t)mm->mem + 1023) & ~uintptr_t(1023));
+  int st = pack_a_herm(ctx, m->ham, (int)nw, m->nr_el, mm->H, base);
+  if (st == EPB_OK) st = pack_a_complex(ctx, m->epmat, nd_ep, nd_ep, m->nr_el, mm->EP, base + hb);
+  if (st != EPB_OK) {
+    cudaFree(mm->mem);
+    delete mm;
+    return st;
+  }
+  m->mixed = mm;
+  return EPB_OK;
 }
 
-void mixed_model_free(epb_model* m) { (void)m; }
+void mixed_model_free(epb_model* m) {
+  if (!m || !m->mixed) return;
+  MixedModel* mm = (MixedModel*)m->mixed;
+  if (mm->mem) cudaFree(mm->mem);
+  delete mm;
+  m->mixed = nullptr;
+}
 
-int mixed_pass_batch(epb_ctx* ctx, epb_model* m, const double* xk_b, int64_t nkb, const double* xq, int64_t nq,
-                     const double2* uk_b, const double2* uph, const double* omega, const double2* phase,
-                     double* g2sum_b, double* g2_sample_b, int64_t sample_stride, int64_t* stats) {
-  (void)ctx; (void)m; (void)xk_b; (void)nkb; (void)xq; (void)nq; (void)uk_b; (void)uph; (void)omega;
-  (void)phase; (void)g2sum_b; (void)g2_sample_b; (void)sample_stride; (void)stats;
-  set_error("mixed-precision pass is not available in this build");
-  return EPB_ERR_UNSUPPORTED;
+// RR->kR rotation on the k leg fused with the packing of the kR->kq operand:
+//   G_k[iw, n, nu, p] = sum_jw g_k[iw, jw, nu, p] uk[jw, n]      (src/wannier_to_bloch_batched.jl:190-203)
+// written straight into the split planes of A2 for the batched kR->kq GEMM: batch k, rows
+// 2r / 2r+1 (r = iw + nw (n + nw nu)), K' = [cos p | sin p] with koff = round_up(nr_ep, 8).
+template <bool BF16, int NPL>
+__global__ void rr_rotate_pack_kernel(const float2* __restrict__ gk, const double2* __restrict__ uk, int nw,
+                                      int nm, int nr_ep, int64_t nk, int64_t rows_pad_k, int64_t KC,
+                                      uint8_t* __restrict__ planes, int64_t plane_bytes) {
+  const int64_t nd = (int64_t)nw * nw * nm;  // complex rows r per k
+  const int64_t koff = sin_offset(nr_ep);
+  const int64_t npc = koff / 8;               // 8-wide p chunks
+  const int64_t total = nk * nd * npc;
+  const int64_t ndata = nd * nr_ep;           // complex length of g_k
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = idx % nd;
+    int64_t rest = idx / nd;
+    int64_t pc = rest % npc, k = rest / npc;
+    int iw = (int)(r % nw);
+    int n = (int)((r / nw) % nw);
+    int nu = (int)(r / ((int64_t)nw * nw));
+    const float2* g = gk + k * ndata;
+    const double2* u = uk + (k * nw + n) * nw;
+    double re[8], im[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      int p = (int)(pc * 8 + e);
+      double2 acc = make_double2(0.0, 0.0);
+      if (p < nr_ep) {
+        const float2* gp = g + iw + (int64_t)nw * nw * (nu + (int64_t)nm * p);
+        for (int jw = 0; jw < nw; ++jw) {
+          float2 x = gp[(int64_t)jw * nw];
+          cfma(acc, make_double2(x.x, x.y), u[jw]);
+        }
+      }
+      re[e] = acc.x;
+      im[e] = acc.y;
+    }
+    const int64_t row0 = k * rows_pad_k + 2 * r;
+    double t[8];
+    // real row: [Re G | -Im G];  imaginary row: [Im G | Re G]
+    store_split8<BF16, NPL>(planes, plane_bytes, tiled_offset(row0, pc * 8, KC), re);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) t[e] = -im[e];
+    store_split8<BF16, NPL>(planes, plane_bytes, tiled_offset(row0, koff + pc * 8, KC), t);
+    store_split8<BF16, NPL>(planes, plane_bytes, tiled_offset(row0 + 1, pc * 8, KC), im);
+    store_split8<BF16, NPL>(planes, plane_bytes, tiled_offset(row0 + 1, koff + pc * 8, KC), re);
+  }
+}
+
+__global__ void c128_to_c64_kernel(const double2* __restrict__ in, float2* __restrict__ out, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = make_float2((float)in[i].x, (float)in[i].y);
+}
+
+// Rotation + |g|^2 fold + in-place reduction, FP32, one CTA per (k, q) block:
+//   T[m, n, jm] = sum_iw conj(ukq[iw, m]) g[iw, n, jm]  (thread per column (n, jm), g column in registers)
+//   ep[m, n, nu] = sum_jm T[m, n, jm] uph[jm, nu]        (thread per (m, n), all nu in registers)
+// g2 = |ep|^2 / (2 omega) accumulated in FP64 per thread, reduced per CTA into g2sum[nu, k].
+template <int NW, int NM>
+__global__ void __launch_bounds__(256) eph_rot_reduce_f32_kernel(
+    const float* __restrict__ g, int64_t g_stride, const float2* __restrict__ ukq, const float2* __restrict__ uph,
+    const double* __restrict__ omega, int64_t nkb, int64_t nq, double* __restrict__ g2sum,
+    double* __restrict__ sample, int64_t stride, int64_t nsamp) {
+  constexpr int NB = NW;
+  constexpr int NT = NB * NB * NM;
+  __shared__ float2 us[NW * NB];
+  __shared__ float2 ps[NM * NM];
+  __shared__ float2 ts[NT];
+  __shared__ float om[NM];
+  __shared__ double red[NM];
+  for (int e = threadIdx.x; e < NM; e += blockDim.x) red[e] = 0.0;
+  double part[NM];
+#pragma unroll
+  for (int i = 0; i < NM; ++i) part[i] = 0.0;
+  const int64_t nblk = nkb * nq;
+  int64_t kcur = -1;
+  for (int64_t blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+    const int64_t kl = blk / nq, q = blk % nq;
+    if (kl != kcur) {  // flush partial sums when the block moves to another k
+      if (kcur >= 0) {
+#pragma unroll
+        for (int i = 0; i < NM; ++i) {
+          double v = part[i];
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&g2sum[i + NM * kcur], v);
+          part[i] = 0.0;
+        }
+      }
+      kcur = kl;
+    }
+    __syncthreads();
+    const float2* uq = ukq + blk * NW * NB;
+    for (int e = threadIdx.x; e < NW * NB; e += blockDim.x) us[e] = uq[e];
+    for (int e = threadIdx.x; e < NM * NM; e += blockDim.x) ps[e] = uph[q * NM * NM + e];
+    for (int e = threadIdx.x; e < NM; e += blockDim.x) om[e] = (float)(1.0 / (2.0 * omega[e + q * NM]));
+    __syncthreads();
+    const float2* gb = reinterpret_cast<const float2*>(g + blk * g_stride);
+    for (int c = threadIdx.x; c < NB * NM; c += blockDim.x) {  // column c = n + NB * jm
+      float2 gc[NW];
+#pragma unroll
+      for (int iw = 0; iw < NW; ++iw) gc[iw] = gb[iw + NW * c];
+#pragma unroll 4
+      for (int m = 0; m < NB; ++m) {
+        float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int iw = 0; iw < NW; ++iw) cfma_conj(acc, us[iw + NW * m], gc[iw]);
+        ts[m + NB * c] = acc;
+      }
+    }
+    __syncthreads();
+    const bool samp = sample && (q % stride == 0);
+    double* sq = samp ? sample + ((kl * nsamp) + q / stride) * (int64_t)NT : nullptr;
+    for (int mn = threadIdx.x; mn < NB * NB; mn += blockDim.x) {
+      float2 t[NM];
+#pragma unroll
+      for (int jm = 0; jm < NM; ++jm) t[jm] = ts[mn + NB * NB * jm];
+#pragma unroll
+      for (int nu = 0; nu < NM; ++nu) {
+        float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int jm = 0; jm < NM; ++jm) cfma(acc, t[jm], ps[jm + NM * nu]);
+        float v = (acc.x * acc.x + acc.y * acc.y) * om[nu];
+        part[nu] += (double)v;
+        if (samp) sq[mn + NB * NB * nu] = (double)v;
+      }
+    }
+  }
+  if (kcur >= 0) {
+#pragma unroll
+    for (int i = 0; i < NM; ++i) {
+      double v = part[i];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&g2sum[i + NM * kcur], v);
+    }
+  }
+}
+
+int fourier_f64(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, const epb_rset* rs, const double* xk,
+                int64_t N, double2* out, int64_t ldo);
+int eigh_async(epb_ctx* ctx, double2* A, int64_t n, int64_t batch, double* E, bool want_v, const double* mass,
+               int prec);
+int eigh_mixed_packed(epb_ctx* ctx, const float* Hp, int64_t n, int64_t batch, float2* U, double* E);
+
+// The whole mixed pass after the q side (omega, u_ph in FP64) has been computed.
+int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double* xq, int64_t nq,
+               const double2* uph, const double* omega, double* ek_out, double* g2sum, double* g2_sample,
+               int64_t sample_stride, int64_t kbi_max) {
+  MixedModel* mm = (MixedModel*)m->mixed;
+  const int64_t nw = m->nw, nm = m->nm, nw2 = nw * nw;
+  const int64_t nd = nw2 * nm, nd_ep = nd * m->nr_ep;
+  EPB_CHECK_ARG(nw == 16 && nm == 12, "mixed pass: this build instantiates the rotation for nw=16, nm=12");
+  const int64_t KO = 256;                               // RR->kR batch (one read of the g(Re,Rp) planes)
+  const int64_t kbi = kbi_max < KO ? kbi_max : KO;      // H(k+q) / kR->kq batch
+  const int64_t KC_ep = kchunks(m->nr_ep), KC_el = kchunks(m->nr_el);
+  const int64_t rows_pad_k = round_up(2 * nd, 128);
+  // ---- workspace ----
+  size_t off = 0;
+  auto carve = [&](int64_t bytes) {
+    size_t o = off;
+    off += ((size_t)bytes + 1023) & ~size_t(1023);
+    return o;
+  };
+  const size_t o_bp = carve(MX_NPL * plane_bytes_for(round_up(nq, MX_NT), KC_ep));
+  const size_t o_uph = carve(8 * nm * nm * nq);
+  const size_t o_hk = carve(16 * nw2 * KO);
+  const size_t o_bk = carve(MX_NPL * plane_bytes_for(round_up(KO, MX_NT), KC_el));
+  const size_t o_c0 = carve(4 * 2 * nd_ep * KO);
+  const size_t o_a2 = carve(MX_NPL * plane_bytes_for(rows_pad_k * KO, KC_ep));
+  const size_t o_bkq = carve(MX_NPL * plane_bytes_for(round_up(kbi * nq, MX_NT), KC_el));
+  const size_t o_c1 = carve(4 * nw2 * kbi * nq);
+  const size_t o_u32 = carve(8 * nw2 * kbi * nq);
+  const size_t o_c2 = carve(4 * 2 * nd * kbi * nq);
+  void* ws = nullptr;
+  EPB_TRY(ws_get(ctx, EPB_WS_PASS1, off + 1024, &ws));
+  uint8_t* base = (uint8_t*)(((uintptr_t)ws + 1023) & ~uintptr_t(1023));
+  float2* uph32 = (float2*)(base + o_uph);
+  double2* Hk = (double2*)(base + o_hk);
+  float* C0 = (float*)(base + o_c0);
+  float* C1 = (float*)(base + o_c1);
+  float2* U32 = (float2*)(base + o_u32);
+  float* C2 = (float*)(base + o_c2);
+  const int64_t nsamp = g2_sample ? (nq + sample_stride - 1) / sample_stride : 0;
+
+  // ---- q side: phase planes of the q list, u_ph in complex64 ----
+  Planes Bp;
+  EPB_TRY(pack_b_phase(ctx, m->rs_ep, xq, nullptr, 1, nq, Bp, base + o_bp));
+  c128_to_c64_kernel<<<grid_for(ctx, nm * nm * nq), 256, 0, ctx->stream>>>(uph, uph32, nm * nm * nq);
+  EPB_LAUNCH_CHECK();
+  Planes A2;
+  A2.rows_pad = rows_pad_k * KO;
+  A2.KC = KC_ep;
+  A2.plane_bytes = plane_bytes_for(A2.rows_pad, KC_ep);
+  A2.npl = MX_NPL;
+  A2.p = base + o_a2;
+  if (rows_pad_k != 2 * nd) EPB_CUDA(cudaMemsetAsync(A2.p, 0, MX_NPL * A2.plane_bytes, ctx->stream));
+
+  for (int64_t ko = 0; ko < nk; ko += KO) {
+    const int64_t nko = nk - ko < KO ? nk - ko : KO;
+    const double* xko = xk + 3 * ko;
+    // electrons at k (FP64: the k side is 0.01% of the pass and fixes the k-leg gauge)
+    EPB_TRY(fourier_f64(ctx, m->ham, nw2, nw2, m->rs_el, xko, nko, Hk, nw2));
+    EPB_TRY(eigh_async(ctx, Hk, nw, nko, ek_out + nw * ko, true, nullptr, EPB_PREC_FP64));
+    // RR->kR on the tensor cores: C0[:, k] = g(k) (complex64, "el" row order)
+    Planes Bk;
+    EPB_TRY(pack_b_phase(ctx, m->rs_el, xko, nullptr, 1, nko, Bk, base + o_bk));
+    EPB_TRY(split_gemm(ctx, EPB_PROF_UMMA_RR, mm->EP, Bk, mm->EP.rows_pad / 128, 1, 2 * nd_ep, nko, false, C0, 0,
+                       2 * nd_ep));
+    // k-leg rotation by u_k fused into the A2 packing of the kR->kq GEMM
+    {
+      const int64_t total = nko * nd * (sin_offset(m->nr_ep) / 8);
+      prof_begin(ctx, EPB_PROF_RR_ROT);
+      rr_rotate_pack_kernel<MX_BF16, MX_NPL><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
+          (const float2*)C0, Hk, (int)nw, (int)nm, (int)m->nr_ep, nko, rows_pad_k, KC_ep, A2.p, A2.plane_bytes);
+      prof_end(ctx);
+      EPB_LAUNCH_CHECK();
+    }
+    for (int64_t ki = 0; ki < nko; ki += kbi) {
+      const int64_t nki = nko - ki < kbi ? nko - ki : kbi;
+      const int64_t np = nki * nq;
+      // H(k+q) on the tensor cores (Hermitian-packed rows), then FP32 solve + FP64 refinement
+      Planes Bkq;
+      EPB_TRY(pack_b_phase(ctx, m->rs_el, xko + 3 * ki, xq, nq, np, Bkq, base + o_bkq));
+      EPB_TRY(split_gemm(ctx, EPB_PROF_UMMA_H, mm->H, Bkq, mm->H.rows_pad / 128, 1, nw2, np, true, C1, 0, nw2));
+      EPB_TRY(eigh_mixed_packed(ctx, C1, nw, np, U32, nullptr));
+      // kR->kq on the tensor cores, batched over the k of this inner batch
+      Planes A2i = A2;
+      A2i.p = A2.p + ki * rows_pad_k / 128 * KC_ep * TILE_BYTES;
+      EPB_TRY(split_gemm(ctx, EPB_PROF_UMMA_KQ, A2i, Bp, rows_pad_k / 128, nki, 2 * nd, nq, false, C2,
+                         2 * nd * nq, 2 * nd));
+      // rotations, g2, in-place reduction
+      {
+        int64_t nblk = np;
+        unsigned grid = (unsigned)(nblk < (int64_t)ctx->sm_count * 8 ? nblk : (int64_t)ctx->sm_count * 8);
+        prof_begin(ctx, EPB_PROF_ROT);
+        eph_rot_reduce_f32_kernel<16, 12><<<grid, 256, 0, ctx->stream>>>(
+            C2, 2 * nd, U32, uph32, omega, nki, nq, g2sum + nm * (ko + ki),
+            g2_sample ? g2_sample + (ko + ki) * nsamp * nd : nullptr, sample_stride, nsamp);
+        prof_end(ctx);
+        EPB_LAUNCH_CHECK();
+      }
+    }
+  }
+  return split_gemm_check(ctx);
 }
 
 }  // namespace epb

@@ -46,3 +46,33 @@ def test_gpu_pass_fp64(gpu_lib, nw, natom, nk, nq, kb):
     s, sr = host(r.g2_sample), ref["g2_sample"]
     np.testing.assert_allclose(s, sr, rtol=1e-7, atol=1e-10 * sr.max())
     assert r.n_elements == nk * nq * nw * nw * 3 * natom
+
+
+def _block_rel_err(s, sr):
+    """Per sampled (k, q) block: ||g2 - g2_ref||_F / ||g2_ref||_F (max over blocks)."""
+    d = s - sr
+    num = np.sqrt((np.abs(d) ** 2).sum(axis=(0, 1, 2)))
+    den = np.sqrt((np.abs(sr) ** 2).sum(axis=(0, 1, 2)))
+    return (num / den).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nk,nq,kb", [(5, 64, 2), (3, 200, 3)])
+def test_gpu_pass_mixed(gpu_lib, nk, nq, kb):
+    """Mixed-precision pass vs the FP64 CPU port: |g|^2 normwise error per (k, q) block <= 1e-5,
+    band/q sums <= 1e-6, electron energies (FP64 k side) and phonons at the FP64 level."""
+    from epb200 import pipeline
+    from epb200.batched import host
+
+    m = synth.config2_model(seed=41, n_el=2, n_ph=1, nw=16, natom=4)
+    xks = synth.random_kpoints(nk, 5)
+    xqs = synth.random_kpoints(nq, 6)
+    dm = pipeline.DeviceModel(m, mixed=True)
+    r = pipeline.run_eph_over_k_and_q(dm, xks, xqs, prec=pipeline.PREC_MIXED, k_batch=kb, sample_stride=5)
+    ref = cpu_pass.eph_pass_cpu(m, xks, xqs, sample_stride=5)
+    np.testing.assert_allclose(host(r.ek), ref["ek"], atol=1e-11 * np.abs(ref["ek"]).max())
+    np.testing.assert_allclose(host(r.omega), ref["omega"], rtol=1e-10)
+    np.testing.assert_allclose(host(r.g2sum), ref["g2sum"], rtol=1e-6)
+    err = _block_rel_err(host(r.g2_sample), ref["g2_sample"])
+    print("max per-block |g|^2 normwise rel err", err)
+    assert err <= 1e-5
