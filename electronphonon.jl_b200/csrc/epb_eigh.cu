@@ -173,7 +173,7 @@ __global__ void eigh_kernel(EighArgs a) {
   for (int64_t b = team_global; b < a.batch; b += nteams) {
     const int n = a.nvec ? a.nvec[b] : a.n_uniform;
     if (n < 1 || n > NMAX) {  // order outside this kernel's shared-memory plan: skip, report
-      if (tid == 0) atomicAdd(a.badsize, 1);
+      if (n != 0 && tid == 0) atomicAdd(a.badsize, 1);
       continue;
     }
     const int64_t aoff = a.a_off ? a.a_off[b] : b * (int64_t)n * n;
@@ -279,7 +279,7 @@ __global__ void eigh_mixed_kernel(EighArgs a) {
   for (int64_t b = team_global; b < a.batch; b += nteams) {
     const int n = a.nvec ? a.nvec[b] : a.n_uniform;
     if (n < 1 || n > NMAX) {  // order outside this kernel's shared-memory plan: skip, report
-      if (tid == 0) atomicAdd(a.badsize, 1);
+      if (n != 0 && tid == 0) atomicAdd(a.badsize, 1);
       continue;
     }
     const int64_t aoff = a.a_off ? a.a_off[b] : b * (int64_t)n * n;
@@ -499,13 +499,104 @@ int eigh_dispatch(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
 
 int eigh_check(epb_ctx* ctx);
 
+struct Eigh16Args {
+  const double2* A;
+  const float* Hp;
+  double2* U64;
+  float2* U32;
+  double* E;
+  const double* mass;
+  int n;
+  int64_t batch;
+  int max_sweeps;
+  int* nonconv;
+  int refine;
+  int64_t* flag_list;
+  int* flag_count;
+};
+int eigh16_launch(epb_ctx* ctx, Eigh16Args& a, bool mixed);
+
+// Offsets of the listed matrices for the FP64 slow path.
+__global__ void flag_offsets_kernel(const int64_t* __restrict__ list, const int* __restrict__ count, int64_t n,
+                                    int64_t* __restrict__ a_off, int64_t* __restrict__ e_off, int32_t* __restrict__ nvec,
+                                    int64_t cap) {
+  int64_t c = *count;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += (int64_t)gridDim.x * blockDim.x) {
+    if (i < c) {
+      a_off[i] = list[i] * n * n;
+      e_off[i] = list[i] * n;
+      nvec[i] = (int32_t)n;
+    } else {
+      nvec[i] = 0;  // unused slots: order 0 is skipped by the kernel without being reported
+    }
+  }
+}
+
+// Uniform batches of order <= 16 go to the register-resident one-sided Jacobi (epb_eigh16.cu).
+// With c128 in/out (the public API) the FP64 refinement runs twice, and matrices with a
+// near-degenerate pair outside first-order validity (planted clusters) are re-solved by the FP64
+// two-sided Jacobi, which reads the untouched input.
+static int eigh_small(epb_ctx* ctx, const EighArgs& a, int prec) {
+  Eigh16Args b{};
+  b.A = a.A;
+  b.Hp = a.Hp;
+  b.U64 = a.want_v && !a.U32 ? a.A : nullptr;
+  b.U32 = a.U32;
+  b.E = a.E;
+  b.mass = a.mass;
+  b.n = a.n_uniform;
+  b.batch = a.batch;
+  b.max_sweeps = prec == EPB_PREC_FP64 ? 30 : 20;
+  b.nonconv = ctx->dstat + 0;
+  b.refine = a.U32 ? 1 : 2;
+  const bool slow_path = prec == EPB_PREC_MIXED && !a.Hp && a.A;
+  int64_t* list = nullptr;
+  if (slow_path) {
+    void* ws = nullptr;
+    EPB_TRY(ws_get(ctx, EPB_WS_EIGH, (size_t)a.batch * 32 + 64, &ws));
+    list = (int64_t*)((char*)ws + 64);
+    b.flag_list = list;
+    b.flag_count = ctx->dstat + 4;
+    EPB_CUDA(cudaMemsetAsync(b.flag_count, 0, sizeof(int), ctx->stream));
+  }
+  EPB_TRY(eigh16_launch(ctx, b, prec == EPB_PREC_MIXED));
+  if (!slow_path) return EPB_OK;
+  // slow path on the (rare) flagged matrices: capacity = batch, count read on the device
+  int64_t* a_off = list + a.batch;
+  int64_t* e_off = a_off + a.batch;
+  int32_t* nvec = (int32_t*)(e_off + a.batch);
+  flag_offsets_kernel<<<(unsigned)cdiv(a.batch, 256), 256, 0, ctx->stream>>>(list, b.flag_count, a.n_uniform,
+                                                                            a_off, e_off, nvec, a.batch);
+  EPB_LAUNCH_CHECK();
+  int* h = (int*)ctx->pinned;
+  EPB_CUDA(cudaMemcpyAsync(h, b.flag_count, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  EPB_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (*h == 0) return EPB_OK;
+  EighArgs s{};
+  s.A = a.A;
+  s.a_off = a_off;
+  s.nvec = nvec;
+  s.batch = *h;
+  s.E = a.E;
+  s.e_off = e_off;
+  s.want_v = a.want_v;
+  s.mass = a.mass;
+  s.nonconv = ctx->dstat + 0;
+  s.badsize = ctx->dstat + 1;
+  s.max_sweeps = 30;
+  return eigh_dispatch(ctx, s, 16, EPB_PREC_FP64);
+}
+
 int eigh_run(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
   if (a.batch == 0) return EPB_OK;
   a.nonconv = ctx->dstat + 0;
   a.badsize = ctx->dstat + 1;
   EPB_CUDA(cudaMemsetAsync(ctx->dstat, 0, 2 * sizeof(int), ctx->stream));
   a.max_sweeps = prec == EPB_PREC_FP64 ? 30 : 20;
-  EPB_TRY(eigh_dispatch(ctx, a, nmax, prec));
+  if (!a.nvec && a.n_uniform <= 16 && (prec == EPB_PREC_FP64 || prec == EPB_PREC_MIXED))
+    EPB_TRY(eigh_small(ctx, a, prec));
+  else
+    EPB_TRY(eigh_dispatch(ctx, a, nmax, prec));
   return eigh_check(ctx);
 }
 
@@ -524,6 +615,7 @@ int eigh_async(epb_ctx* ctx, double2* A, int64_t n, int64_t batch, double* E, bo
   a.nonconv = ctx->dstat + 0;
   a.badsize = ctx->dstat + 1;
   a.max_sweeps = prec == EPB_PREC_FP64 ? 30 : 20;
+  if (n <= 16) return eigh_small(ctx, a, prec);
   return eigh_dispatch(ctx, a, (int)n, prec);
 }
 
@@ -541,6 +633,7 @@ int eigh_mixed_packed(epb_ctx* ctx, const float* Hp, int64_t n, int64_t batch, f
   a.nonconv = ctx->dstat + 0;
   a.badsize = ctx->dstat + 1;
   a.max_sweeps = 20;
+  if (n <= 16) return eigh_small(ctx, a, EPB_PREC_MIXED);
   return eigh_dispatch(ctx, a, (int)n, EPB_PREC_MIXED);
 }
 
