@@ -50,7 +50,14 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-nk", type=int, default=16)
     ap.add_argument("--cpu-nq", type=int, default=1024)
-    return ap.parse_args()
+    ap.add_argument("--small", action="store_true",
+                    help="profiling case: Re grid 5^3, 32 k x 2048 q (a few GB on the device)")
+    a = ap.parse_args()
+    if a.small:
+        global N_EL
+        N_EL = 2
+        a.nk, a.nq = 32, 2048
+    return a
 
 
 def dist_env():
@@ -64,7 +71,7 @@ def build_model_host_small():
     """Host model without epmat (H and D only); the 4.5 GB epmat is generated on the device."""
     from epb200 import synth
 
-    return synth.config2_model(seed=SEED, with_epmat=False)
+    return synth.config2_model(seed=SEED, with_epmat=False, n_el=N_EL)
 
 
 def config_dict(args, prec_name):
