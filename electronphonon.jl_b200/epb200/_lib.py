@@ -55,6 +55,7 @@ SIGNATURES = {
     "epb_eph_apply_rotations": [P, P, I64, I64, I64, I64, I64, P, I64, P, P, P, P],
     "epb_eph_kR_to_kq": [P, P, I64, I64, I64, I64, I64, P, I64, P, I64, P, P, P, P, I32],
     "epb_window_filter": [P, P, I64, I64, D, D, P, P, P, P, P],
+    "epb_window_filter_noalloc": [P, P, I64, I64, D, D, P, P, P, P, P],
     "epb_fill_iqs": [P, P, I64, P, I64, I64, I64, P, P],
     "epb_model_create": [P, P, I64, P, I64, P, P, I64, P, I64, P, P, I64, I32, C.POINTER(P)],
     "epb_model_destroy": [P],

@@ -160,6 +160,18 @@ EPB_API int epb_window_filter(epb_ctx* ctx, const double* E, int64_t nw, int64_t
                       double wmax, int32_t* band_min, int32_t* band_max, int32_t* keep_idx,
                       int64_t* nkeep_dev, double* nbelow);
 
+/* The same window filter, allocating nothing: no counterpart in the reference. For callers that
+   cannot let a library allocate device memory (their memory is owned by a caching allocator such as
+   a Julia CUDA.jl or PyTorch pool, or a hot loop must not pay an allocation's latency or risk its
+   failure). Takes a plain cudaStream_t instead of an epb_ctx. Its only scratch is a fixed 64 KB
+   device array held by every GPU that loads the library until exit: nk <= 16,777,216, larger nk
+   returns EPB_ERR_ARG. Calls share that array, so calls that overlap on the GPU race; calls on one
+   stream are safe. The first call on a device resolves the array's address with that device
+   current and should come before any stream capture. Results equal epb_window_filter's. */
+EPB_API int epb_window_filter_noalloc(void* stream, const double* E, int64_t nw, int64_t nk, double wmin,
+                                      double wmax, int32_t* band_min, int32_t* band_max, int32_t* keep_idx,
+                                      int64_t* nkeep_dev, double* nbelow);
+
 /* iq index (1-based) of x_{k+q} - x_k on a commensurate grid: for each j < nkq,
    iqs[j] = dense_hash_to_iq[((c1 ng2) + c2) ng3 + c3] with c = wrap(xkq_int[:, j] - xk_int).
    xkq_int int64 (3 x nkq), xk_int int64 (3), dense_hash_to_iq int64 (ng1 ng2 ng3).
