@@ -87,6 +87,7 @@ enum epb_prof_id {
   EPB_PROF_UMMA_RR,
   EPB_PROF_SPLIT,
   EPB_PROF_OTHER,
+  EPB_PROF_REFINE,
   EPB_PROF_N
 };
 

@@ -513,6 +513,7 @@ struct Eigh16Args {
   int refine;
   int64_t* flag_list;
   int* flag_count;
+  float2* V32;
 };
 int eigh16_launch(epb_ctx* ctx, Eigh16Args& a, bool mixed);
 
@@ -551,13 +552,18 @@ static int eigh_small(epb_ctx* ctx, const EighArgs& a, int prec) {
   b.refine = a.U32 ? 1 : 2;
   const bool slow_path = prec == EPB_PREC_MIXED && !a.Hp && a.A;
   int64_t* list = nullptr;
-  if (slow_path) {
+  if (prec == EPB_PREC_MIXED) {
+    // workspace: FP32 eigenvectors (16 x 16 per matrix), then the slow-path list and offsets
+    const size_t v32 = (size_t)a.batch * 16 * 16 * sizeof(float2);
     void* ws = nullptr;
-    EPB_TRY(ws_get(ctx, EPB_WS_EIGH, (size_t)a.batch * 32 + 64, &ws));
-    list = (int64_t*)((char*)ws + 64);
-    b.flag_list = list;
-    b.flag_count = ctx->dstat + 4;
-    EPB_CUDA(cudaMemsetAsync(b.flag_count, 0, sizeof(int), ctx->stream));
+    EPB_TRY(ws_get(ctx, EPB_WS_EIGH, v32 + (slow_path ? (size_t)a.batch * 32 : 0) + 256, &ws));
+    b.V32 = (float2*)ws;
+    if (slow_path) {
+      list = (int64_t*)((char*)ws + ((v32 + 255) & ~size_t(255)));
+      b.flag_list = list;
+      b.flag_count = ctx->dstat + 4;
+      EPB_CUDA(cudaMemsetAsync(b.flag_count, 0, sizeof(int), ctx->stream));
+    }
   }
   EPB_TRY(eigh16_launch(ctx, b, prec == EPB_PREC_MIXED));
   if (!slow_path) return EPB_OK;

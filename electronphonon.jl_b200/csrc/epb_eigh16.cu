@@ -72,14 +72,18 @@ __device__ int onesided_sweeps(typename cplx<T>::type (&a)[E16], T tol, int max_
       for (int i = 0; i < E16; ++i) b[i] = shfl2(a[i], src);
       const T nb = shfl(nrm, src);
       const bool isP = l < pl;
-      C g = mk2(T(0), T(0));
+      C g0 = mk2(T(0), T(0)), g1 = mk2(T(0), T(0));  // two chains: shorter dependency
 #pragma unroll
-      for (int i = 0; i < E16; ++i) {
-        if (isP)
-          cfma_conj(g, a[i], b[i]);
-        else
-          cfma_conj(g, b[i], a[i]);
+      for (int i = 0; i < E16; i += 2) {
+        if (isP) {
+          cfma_conj(g0, a[i], b[i]);
+          cfma_conj(g1, a[i + 1], b[i + 1]);
+        } else {
+          cfma_conj(g0, b[i], a[i]);
+          cfma_conj(g1, b[i + 1], a[i + 1]);
+        }
       }
+      const C g = mk2(g0.x + g1.x, g0.y + g1.y);
       const T ap = isP ? nrm : nb, aq = isP ? nb : nrm;
       const T ag = sqrt(g.x * g.x + g.y * g.y);
       if (ag > tol * sqrt(ap * aq) && ag > T(0)) {
@@ -125,209 +129,260 @@ struct Eigh16Args {
   int refine;         // FP64 refinement iterations (mixed only)
   int64_t* flag_list; // if non-null: matrices with a near-degenerate pair are listed, not written
   int* flag_count;
+  float2* V32;        // FP32 eigenvector workspace between the Jacobi and refinement kernels
 };
 
-template <bool MIXED>
-__global__ void __launch_bounds__(128) eigh16_kernel(Eigh16Args a) {
-  using T = typename std::conditional<MIXED, float, double>::type;
+// Load column l of matrix b (FP64), optionally mass-scaled; zero outside the live n x n block.
+__device__ __forceinline__ double2 load_h(const Eigh16Args& a, int64_t b, int i, int l, int n) {
+  double2 v = make_double2(0.0, 0.0);
+  if (l < n && i < n) {
+    if (a.Hp) {
+      const float* hp = a.Hp + b * (int64_t)n * n;
+      const int nre = n * (n + 1) / 2;
+      int ii = i <= l ? i : l, jj = i <= l ? l : i;
+      double re = hp[jj * (jj + 1) / 2 + ii];
+      double im = ii < jj ? hp[nre + jj * (jj - 1) / 2 + ii] : 0.0;
+      v = make_double2(re, i <= l ? im : -im);
+    } else {
+      const double2* ab = a.A + b * (int64_t)n * n;
+      if (i <= l) {
+        v = ab[i + (int64_t)l * n];
+      } else {
+        double2 u = ab[l + (int64_t)i * n];
+        v = make_double2(u.x, -u.y);
+      }
+    }
+    if (i == l) v.y = 0.0;
+    if (a.mass) {
+      double s = 1.0 / (sqrt(a.mass[i]) * sqrt(a.mass[l]));
+      v.x *= s;
+      v.y *= s;
+    }
+  }
+  return v;
+}
+
+// Rank of this lane's eigenvalue among the live lanes of its half-warp, then the outputs.
+__device__ __forceinline__ void write_sorted(const Eigh16Args& a, int64_t b, bool live, int lane, int l, int n,
+                                             double lam, const double2 (&v)[E16]) {
+  int rank = 0;
+#pragma unroll
+  for (int k = 0; k < E16; ++k) {
+    double lk = __shfl_sync(0xffffffffu, lam, (lane & 16) + k);
+    rank += (k < n) && (lk < lam || (lk == lam && k < l));
+  }
+  if (live && l < n) {
+    double ev = lam;
+    if (a.mass) ev = ev >= 0 ? sqrt(ev) : -sqrt(-ev);
+    if (a.E) a.E[b * n + rank] = ev;
+#pragma unroll
+    for (int i = 0; i < E16; ++i) {
+      if (i < n) {
+        double2 o = v[i];
+        if (a.mass) {
+          double s = 1.0 / sqrt(a.mass[i]);
+          o.x *= s;
+          o.y *= s;
+        }
+        if (a.U32) a.U32[b * (int64_t)n * n + i + (int64_t)rank * n] = make_float2((float)o.x, (float)o.y);
+        if (a.U64) a.U64[b * (int64_t)n * n + i + (int64_t)rank * n] = o;
+      }
+    }
+  }
+}
+
+// MODE 0: whole solve in FP64 (sorted output).  MODE 1: FP32 sweeps only; writes the normalised,
+// unsorted FP32 columns to a.V32 (16 x 16 per matrix) for MODE 2.
+template <int MODE>
+__global__ void __launch_bounds__(128) eigh16_jacobi_kernel(Eigh16Args a) {
+  using T = typename std::conditional<MODE == 0, double, float>::type;
   using C = typename cplx<T>::type;
-  // per matrix: H (FP64, 16 x 16) and V (FP64, 16 x 16) for the refinement; 8 matrices per block
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  auto Hs = reinterpret_cast<double2(*)[E16 * E16]>(smem_raw);
-  auto Vs = reinterpret_cast<double2(*)[E16 * E16]>(smem_raw + 8 * E16 * E16 * sizeof(double2));
   const int lane = threadIdx.x & 31;
   const int l = lane & 15;
-  const int slot = (threadIdx.x >> 4);  // matrix slot within the block (0..7)
+  const int slot = threadIdx.x >> 4;
   const int n = a.n;
   const int64_t per_block = blockDim.x / 16;
   for (int64_t b0 = (int64_t)blockIdx.x * per_block; b0 < a.batch; b0 += (int64_t)gridDim.x * per_block) {
     const int64_t b = b0 + slot;
     const bool live = b < a.batch;
-    // ---- load column l of H (FP64), Frobenius norm ----
-    double2 h[E16];
-#pragma unroll
-    for (int i = 0; i < E16; ++i) {
-      double2 v = make_double2(0.0, 0.0);
-      if (live && l < n && i < n) {
-        if (a.Hp) {
-          const float* hp = a.Hp + b * (int64_t)n * n;
-          const int nre = n * (n + 1) / 2;
-          int ii = i <= l ? i : l, jj = i <= l ? l : i;
-          double re = hp[jj * (jj + 1) / 2 + ii];
-          double im = ii < jj ? hp[nre + jj * (jj - 1) / 2 + ii] : 0.0;
-          v = make_double2(re, i <= l ? im : -im);
-        } else {
-          const double2* ab = a.A + b * (int64_t)n * n;
-          if (i <= l) {
-            v = ab[i + (int64_t)l * n];
-          } else {
-            double2 u = ab[l + (int64_t)i * n];
-            v = make_double2(u.x, -u.y);
-          }
-        }
-        if (i == l) v.y = 0.0;
-        if (a.mass) {
-          double s = 1.0 / (sqrt(a.mass[i]) * sqrt(a.mass[l]));
-          v.x *= s;
-          v.y *= s;
-        }
-      }
-      h[i] = v;
-    }
+    C col[E16];
     double f2 = 0.0;
 #pragma unroll
-    for (int i = 0; i < E16; ++i) f2 += h[i].x * h[i].x + h[i].y * h[i].y;
-    for (int o = 8; o > 0; o >>= 1) f2 += __shfl_xor_sync(0xffffffffu, f2, o);  // within the half-warp
-    const double sigma = f2 > 0.0 ? 1.1 * sqrt(f2) : 1.0;  // zero (or padding) matrices: shift 1
-    // ---- one-sided Jacobi on A = H + sigma I ----
-    C col[E16];
-#pragma unroll
     for (int i = 0; i < E16; ++i) {
-      double2 v = h[i];
-      if (i == l) v.x += sigma;  // lanes >= n: sigma e_l
+      double2 v = live ? load_h(a, b, i, l, n) : make_double2(0.0, 0.0);
+      f2 += v.x * v.x + v.y * v.y;
       col[i] = mk2((T)v.x, (T)v.y);
     }
-    if (MIXED) {
+    for (int o = 8; o > 0; o >>= 1) f2 += __shfl_xor_sync(0xffffffffu, f2, o);  // within the half-warp
+    const double sigma = f2 > 0.0 ? 1.1 * sqrt(f2) : 1.0;  // zero (or padding) matrices: shift 1
 #pragma unroll
-      for (int i = 0; i < E16; ++i) Hs[slot][i + E16 * l] = h[i];
-    }
-    const T tol = MIXED ? T(1e-6) : T(1e-15);
+    for (int i = 0; i < E16; ++i)
+      if (i == l) col[i].x += (T)sigma;  // lanes >= n: sigma e_l
+    const T tol = MODE == 0 ? T(1e-15) : T(1e-6);
     int sw = onesided_sweeps<T>(col, tol, a.max_sweeps);
     if (sw >= a.max_sweeps && lane == 0) atomicAdd(a.nonconv, 1);
-    // eigenvector = normalised column, eigenvalue = |column| - sigma
     double nr2 = 0.0;
 #pragma unroll
     for (int i = 0; i < E16; ++i) nr2 += (double)col[i].x * col[i].x + (double)col[i].y * col[i].y;
     const double inv = 1.0 / sqrt(nr2);
+    if (MODE == 1) {
+      if (live) {
+        float2* vo = a.V32 + b * (int64_t)E16 * E16 + (int64_t)E16 * l;
+#pragma unroll
+        for (int i = 0; i < E16; ++i) vo[i] = make_float2((float)(col[i].x * inv), (float)(col[i].y * inv));
+      }
+    } else {
+      double2 v[E16];
+#pragma unroll
+      for (int i = 0; i < E16; ++i) v[i] = make_double2(col[i].x * inv, col[i].y * inv);
+      write_sorted(a, b, live, lane, l, n, sqrt(nr2) - sigma, v);
+    }
+  }
+}
+
+// MODE 2: FP64 refinement of FP32 eigenvectors (see the file header), sorted output.
+__global__ void __launch_bounds__(128) eigh16_refine_kernel(Eigh16Args a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto Hs = reinterpret_cast<double2(*)[E16 * E16]>(smem_raw);
+  auto Vs = reinterpret_cast<double2(*)[E16 * E16]>(smem_raw + 8 * E16 * E16 * sizeof(double2));
+  const int lane = threadIdx.x & 31;
+  const int l = lane & 15;
+  const int slot = threadIdx.x >> 4;
+  const int n = a.n;
+  const int64_t per_block = blockDim.x / 16;
+  for (int64_t b0 = (int64_t)blockIdx.x * per_block; b0 < a.batch; b0 += (int64_t)gridDim.x * per_block) {
+    const int64_t b = b0 + slot;
+    const bool live = b < a.batch;
+    double f2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < E16; ++i) {
+      double2 hv = live ? load_h(a, b, i, l, n) : make_double2(0.0, 0.0);
+      f2 += hv.x * hv.x + hv.y * hv.y;
+      Hs[slot][i + E16 * l] = hv;
+    }
+    for (int o = 8; o > 0; o >>= 1) f2 += __shfl_xor_sync(0xffffffffu, f2, o);
+    const double sigma = f2 > 0.0 ? 1.1 * sqrt(f2) : 1.0;
     double2 v[E16];
+    {
+      const float2* vi = a.V32 + (live ? b : 0) * (int64_t)E16 * E16 + (int64_t)E16 * l;
 #pragma unroll
-    for (int i = 0; i < E16; ++i) v[i] = make_double2(col[i].x * inv, col[i].y * inv);
-    double lam = sqrt(nr2) - sigma;
-    bool cluster = false;  // some pair stayed outside first-order validity (near-degenerate)
-    if (MIXED) {
-      // ---- FP64 refinement (a.refine iterations) ----
-      for (int it = 0; it < a.refine; ++it) {
-#pragma unroll
-        for (int i = 0; i < E16; ++i) Vs[slot][i + E16 * l] = v[i];
-        __syncwarp();
-        double2 w[E16];  // w = H v
-#pragma unroll
-        for (int i = 0; i < E16; ++i) w[i] = make_double2(0.0, 0.0);
-#pragma unroll
-        for (int k = 0; k < E16; ++k) {
-          double2 vk = v[k];
-#pragma unroll
-          for (int i = 0; i < E16; ++i) cfma(w[i], Hs[slot][i + E16 * k], vk);
-        }
-        double d = 0.0, fll = 0.0;
-#pragma unroll
-        for (int i = 0; i < E16; ++i) {
-          d += v[i].x * w[i].x + v[i].y * w[i].y;   // Re v^H H v
-          fll += v[i].x * v[i].x + v[i].y * v[i].y;
-        }
-        fll -= 1.0;
-        const double dp = d * (1.0 - fll);          // S'_ll
-        double2 tcol[E16];                          // column l of (E - F/2)
-        double lam_corr = 0.0;
-        cluster = false;
-#pragma unroll
-        for (int k = 0; k < E16; ++k) {
-          const double dk = __shfl_sync(0xffffffffu, d, (lane & 16) + k);
-          const double dpk = __shfl_sync(0xffffffffu, dp, (lane & 16) + k);
-          double2 s = make_double2(0.0, 0.0), g = make_double2(0.0, 0.0);
-#pragma unroll
-          for (int i = 0; i < E16; ++i) {
-            double2 vik = Vs[slot][i + E16 * k];
-            cfma_conj(s, vik, w[i]);
-            cfma_conj(g, vik, v[i]);
-          }
-          double2 t;
-          if (k == l) {
-            t = make_double2(-0.5 * fll, 0.0);
-          } else {
-            double2 sp = make_double2(s.x - 0.5 * g.x * (dk + d), s.y - 0.5 * g.y * (dk + d));
-            double gap = dp - dpk;
-            double asp = sqrt(sp.x * sp.x + sp.y * sp.y);
-            t = make_double2(-0.5 * g.x, -0.5 * g.y);
-            if (k < n && l < n) {
-              if (asp < 0.1 * fabs(gap)) {
-                t.x += sp.x / gap;
-                t.y += sp.y / gap;
-                lam_corr += asp * asp / gap;
-              } else if (asp > 1e-13 * sigma) {
-                cluster = true;
-              }
-            }
-          }
-          tcol[k] = t;
-        }
-        double2 vn[E16];
-#pragma unroll
-        for (int i = 0; i < E16; ++i) vn[i] = v[i];
-#pragma unroll
-        for (int k = 0; k < E16; ++k) {
-          double2 t = tcol[k];
-#pragma unroll
-          for (int i = 0; i < E16; ++i) cfma(vn[i], Vs[slot][i + E16 * k], t);
-        }
-#pragma unroll
-        for (int i = 0; i < E16; ++i) v[i] = vn[i];
-        lam = dp + lam_corr;
-        __syncwarp();
+      for (int i = 0; i < E16; ++i) {
+        float2 x = live ? vi[i] : make_float2(i == l ? 1.f : 0.f, 0.f);
+        v[i] = make_double2(x.x, x.y);
       }
     }
-    // a matrix with a near-degenerate pair is re-solved by the FP64 slow path when requested
-    const bool flagged = __any_sync(0xffffffffu, cluster && live) &&
-                         (__ballot_sync(0xffffffffu, cluster && live) & (0xFFFFu << (lane & 16)));
+    double lam = 0.0;
+    bool cluster = false;
+    for (int it = 0; it < a.refine; ++it) {
+#pragma unroll
+      for (int i = 0; i < E16; ++i) Vs[slot][i + E16 * l] = v[i];
+      __syncwarp();
+      double2 w[E16];  // w = H v
+#pragma unroll
+      for (int i = 0; i < E16; ++i) w[i] = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < E16; ++k) {
+        double2 vk = v[k];
+#pragma unroll
+        for (int i = 0; i < E16; ++i) cfma(w[i], Hs[slot][i + E16 * k], vk);
+      }
+      double d = 0.0, fll = 0.0;
+#pragma unroll
+      for (int i = 0; i < E16; ++i) {
+        d += v[i].x * w[i].x + v[i].y * w[i].y;
+        fll += v[i].x * v[i].x + v[i].y * v[i].y;
+      }
+      fll -= 1.0;
+      const double dp = d * (1.0 - fll);
+      double2 tcol[E16];
+      double lam_corr = 0.0;
+      cluster = false;
+#pragma unroll
+      for (int k = 0; k < E16; ++k) {
+        const double dk = __shfl_sync(0xffffffffu, d, (lane & 16) + k);
+        const double dpk = __shfl_sync(0xffffffffu, dp, (lane & 16) + k);
+        double2 s0 = make_double2(0.0, 0.0), s1 = s0, g0 = s0, g1 = s0;
+#pragma unroll
+        for (int i = 0; i < E16; i += 2) {
+          double2 v0 = Vs[slot][i + E16 * k], v1 = Vs[slot][i + 1 + E16 * k];
+          cfma_conj(s0, v0, w[i]);
+          cfma_conj(s1, v1, w[i + 1]);
+          cfma_conj(g0, v0, v[i]);
+          cfma_conj(g1, v1, v[i + 1]);
+        }
+        const double2 s = make_double2(s0.x + s1.x, s0.y + s1.y), g = make_double2(g0.x + g1.x, g0.y + g1.y);
+        double2 t;
+        if (k == l) {
+          t = make_double2(-0.5 * fll, 0.0);
+        } else {
+          double2 sp = make_double2(s.x - 0.5 * g.x * (dk + d), s.y - 0.5 * g.y * (dk + d));
+          double gap = dp - dpk;
+          double asp = sqrt(sp.x * sp.x + sp.y * sp.y);
+          t = make_double2(-0.5 * g.x, -0.5 * g.y);
+          if (k < n && l < n) {
+            if (asp < 0.1 * fabs(gap)) {
+              t.x += sp.x / gap;
+              t.y += sp.y / gap;
+              lam_corr += asp * asp / gap;
+            } else if (asp > 1e-13 * sigma) {
+              cluster = true;
+            }
+          }
+        }
+        tcol[k] = t;
+      }
+      // v <- v + V t  (w is dead after the S / G sums: reuse it for V t)
+#pragma unroll
+      for (int i = 0; i < E16; ++i) w[i] = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < E16; ++k) {
+        double2 t = tcol[k];
+#pragma unroll
+        for (int i = 0; i < E16; ++i) cfma(w[i], Vs[slot][i + E16 * k], t);
+      }
+#pragma unroll
+      for (int i = 0; i < E16; ++i) v[i] = make_double2(v[i].x + w[i].x, v[i].y + w[i].y);
+      lam = dp + lam_corr;
+      __syncwarp();
+    }
+    const bool flagged = (__ballot_sync(0xffffffffu, cluster && live) & (0xFFFFu << (lane & 16))) != 0;
     if (a.flag_list && flagged && l == 0) {
       int pos = atomicAdd(a.flag_count, 1);
       a.flag_list[pos] = b;
     }
-    // ---- sort (rank among live lanes) and write ----
-    int rank = 0;
-#pragma unroll
-    for (int k = 0; k < E16; ++k) {
-      double lk = __shfl_sync(0xffffffffu, lam, (lane & 16) + k);
-      rank += (k < n) && (lk < lam || (lk == lam && k < l));
-    }
-    if (live && l < n && !(a.flag_list && flagged)) {
-      double ev = lam;
-      if (a.mass) ev = ev >= 0 ? sqrt(ev) : -sqrt(-ev);
-      if (a.E) a.E[b * n + rank] = ev;
-#pragma unroll
-      for (int i = 0; i < E16; ++i) {
-        if (i < n) {
-          double2 o = v[i];
-          if (a.mass) {
-            double s = 1.0 / sqrt(a.mass[i]);
-            o.x *= s;
-            o.y *= s;
-          }
-          if (a.U32) a.U32[b * (int64_t)n * n + i + (int64_t)rank * n] = make_float2((float)o.x, (float)o.y);
-          if (a.U64) a.U64[b * (int64_t)n * n + i + (int64_t)rank * n] = o;
-        }
-      }
-    }
+    if (!(a.flag_list && flagged)) write_sorted(a, b, live, lane, l, n, lam, v);
+    __syncwarp();
   }
 }
 
 int eigh16_launch(epb_ctx* ctx, Eigh16Args& a, bool mixed) {
   if (a.batch == 0) return EPB_OK;
   const int threads = 128;  // 8 matrices per block
-  int64_t blocks_needed = cdiv(a.batch, threads / 16);
-  int64_t cap = (int64_t)ctx->sm_count * (mixed ? 8 : 8);
-  unsigned grid = (unsigned)(blocks_needed < cap ? blocks_needed : cap);
-  const size_t smem = mixed ? 2 * 8 * E16 * E16 * sizeof(double2) : 0;
+  const int64_t blocks_needed = cdiv(a.batch, threads / 16);
+  auto grid_cap = [&](int per_sm) {
+    int64_t cap = (int64_t)ctx->sm_count * per_sm;
+    return (unsigned)(blocks_needed < cap ? blocks_needed : cap);
+  };
+  if (!mixed) {
+    prof_begin(ctx, EPB_PROF_EIGH);
+    eigh16_jacobi_kernel<0><<<grid_cap(8), threads, 0, ctx->stream>>>(a);
+    prof_end(ctx);
+    EPB_LAUNCH_CHECK();
+    return EPB_OK;
+  }
+  EPB_CHECK_ARG(a.V32 != nullptr, "eigh16: mixed mode needs a V32 workspace");
+  const size_t smem = 2 * 8 * E16 * E16 * sizeof(double2);
   static bool attr = false;
   if (!attr) {
-    EPB_CUDA(cudaFuncSetAttribute(eigh16_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * 8 * E16 * E16 * sizeof(double2))));
+    EPB_CUDA(cudaFuncSetAttribute(eigh16_refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr = true;
   }
   prof_begin(ctx, EPB_PROF_EIGH);
-  if (mixed)
-    eigh16_kernel<true><<<grid, threads, smem, ctx->stream>>>(a);
-  else
-    eigh16_kernel<false><<<grid, threads, 0, ctx->stream>>>(a);
+  eigh16_jacobi_kernel<1><<<grid_cap(16), threads, 0, ctx->stream>>>(a);
+  prof_end(ctx);
+  EPB_LAUNCH_CHECK();
+  prof_begin(ctx, EPB_PROF_REFINE);
+  eigh16_refine_kernel<<<grid_cap(8), threads, smem, ctx->stream>>>(a);
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;

@@ -724,85 +724,124 @@ __global__ void c128_to_c64_kernel(const double2* __restrict__ in, float2* __res
     out[i] = make_float2((float)in[i].x, (float)in[i].y);
 }
 
-// Rotation + |g|^2 fold + in-place reduction, FP32, one CTA per (k, q) block:
+// Rotation + |g|^2 fold + in-place reduction, FP32, one (k, q) block at a time per CTA:
 //   T[m, n, jm] = sum_iw conj(ukq[iw, m]) g[iw, n, jm]  (thread per column (n, jm), g column in registers)
 //   ep[m, n, nu] = sum_jm T[m, n, jm] uph[jm, nu]        (thread per (m, n), all nu in registers)
 // g2 = |ep|^2 / (2 omega) accumulated in FP64 per thread, reduced per CTA into g2sum[nu, k].
+// The next block's operands (g 24 KB, ukq 2 KB, uph 1.1 KB) are fetched with cp.async into the
+// other half of a double buffer while the current block computes; two CTAs fit on an SM.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
 template <int NW, int NM>
-__global__ void __launch_bounds__(256) eph_rot_reduce_f32_kernel(
+struct RotSmem {
+  static constexpr int NB = NW, NT = NW * NW * NM;
+  static constexpr int G = NT * 8, U = NW * NB * 8, PH = NM * NM * 8;
+  static constexpr int BUF = G + U + PH;            // bytes of one operand buffer
+  static constexpr int TOTAL = 2 * BUF + NT * 8;    // two buffers + T
+};
+
+template <int NW, int NM>
+__global__ void __launch_bounds__(256, 2) eph_rot_reduce_f32_kernel(
     const float* __restrict__ g, int64_t g_stride, const float2* __restrict__ ukq, const float2* __restrict__ uph,
     const double* __restrict__ omega, int64_t nkb, int64_t nq, double* __restrict__ g2sum,
     double* __restrict__ sample, int64_t stride, int64_t nsamp) {
+  using L = RotSmem<NW, NM>;
   constexpr int NB = NW;
-  constexpr int NT = NB * NB * NM;
-  __shared__ float2 us[NW * NB];
-  __shared__ float2 ps[NM * NM];
-  __shared__ float2 ts[NT];
-  __shared__ float om[NM];
-  __shared__ double red[NM];
-  for (int e = threadIdx.x; e < NM; e += blockDim.x) red[e] = 0.0;
-  double part[NM];
-#pragma unroll
-  for (int i = 0; i < NM; ++i) part[i] = 0.0;
+  constexpr int NT = L::NT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* ts = reinterpret_cast<float2*>(smem_raw + 2 * L::BUF);
+  __shared__ double wred[8 * NM];  // per-warp partial sums of g2 per mode (blockDim = 256)
+  for (int e = threadIdx.x; e < 8 * NM; e += blockDim.x) wred[e] = 0.0;
   const int64_t nblk = nkb * nq;
+  auto prefetch = [&](int64_t blk, int buf) {
+    if (blk < nblk) {
+      const int64_t q = blk % nq;
+      unsigned char* dst = smem_raw + buf * L::BUF;
+      const char* gs = reinterpret_cast<const char*>(g + blk * g_stride);
+      const char* us = reinterpret_cast<const char*>(ukq + blk * NW * NB);
+      const char* ps = reinterpret_cast<const char*>(uph + q * NM * NM);
+      for (int c = threadIdx.x; c < L::G / 16; c += blockDim.x) cp_async16(dst + 16 * c, gs + 16 * c);
+      for (int c = threadIdx.x; c < L::U / 16; c += blockDim.x) cp_async16(dst + L::G + 16 * c, us + 16 * c);
+      for (int c = threadIdx.x; c < L::PH / 16; c += blockDim.x) cp_async16(dst + L::G + L::U + 16 * c, ps + 16 * c);
+    }
+    cp_async_commit();
+  };
   int64_t kcur = -1;
-  for (int64_t blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+  int buf = 0;
+  prefetch(blockIdx.x, 0);
+  for (int64_t blk = blockIdx.x; blk < nblk; blk += gridDim.x, buf ^= 1) {
+    prefetch(blk + gridDim.x, buf ^ 1);
     const int64_t kl = blk / nq, q = blk % nq;
-    if (kl != kcur) {  // flush partial sums when the block moves to another k
+    if (kl != kcur) {  // flush partial sums when the block moves to another k (uniform across the CTA)
       if (kcur >= 0) {
-#pragma unroll
-        for (int i = 0; i < NM; ++i) {
-          double v = part[i];
-          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-          if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&g2sum[i + NM * kcur], v);
-          part[i] = 0.0;
+        __syncthreads();
+        if (threadIdx.x < NM) {
+          double v = 0.0;
+          for (int w = 0; w < 8; ++w) {
+            v += wred[w * NM + threadIdx.x];
+            wred[w * NM + threadIdx.x] = 0.0;
+          }
+          atomicAdd(&g2sum[threadIdx.x + NM * kcur], v);
         }
       }
       kcur = kl;
     }
+    cp_async_wait1();
     __syncthreads();
-    const float2* uq = ukq + blk * NW * NB;
-    for (int e = threadIdx.x; e < NW * NB; e += blockDim.x) us[e] = uq[e];
-    for (int e = threadIdx.x; e < NM * NM; e += blockDim.x) ps[e] = uph[q * NM * NM + e];
-    for (int e = threadIdx.x; e < NM; e += blockDim.x) om[e] = (float)(1.0 / (2.0 * omega[e + q * NM]));
-    __syncthreads();
-    const float2* gb = reinterpret_cast<const float2*>(g + blk * g_stride);
+    const unsigned char* cb = smem_raw + buf * L::BUF;
+    const float2* gb = reinterpret_cast<const float2*>(cb);
+    const float2* us = reinterpret_cast<const float2*>(cb + L::G);
+    const float2* ps = reinterpret_cast<const float2*>(cb + L::G + L::U);
     for (int c = threadIdx.x; c < NB * NM; c += blockDim.x) {  // column c = n + NB * jm
       float2 gc[NW];
 #pragma unroll
       for (int iw = 0; iw < NW; ++iw) gc[iw] = gb[iw + NW * c];
-#pragma unroll 4
+#pragma unroll 2
       for (int m = 0; m < NB; ++m) {
-        float2 acc = make_float2(0.f, 0.f);
+        float2 a0 = make_float2(0.f, 0.f), a1 = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int iw = 0; iw < NW; ++iw) cfma_conj(acc, us[iw + NW * m], gc[iw]);
-        ts[m + NB * c] = acc;
+        for (int iw = 0; iw < NW; iw += 2) {
+          cfma_conj(a0, us[iw + NW * m], gc[iw]);
+          cfma_conj(a1, us[iw + 1 + NW * m], gc[iw + 1]);
+        }
+        ts[m + NB * c] = make_float2(a0.x + a1.x, a0.y + a1.y);
       }
     }
     __syncthreads();
     const bool samp = sample && (q % stride == 0);
     double* sq = samp ? sample + ((kl * nsamp) + q / stride) * (int64_t)NT : nullptr;
+    const double* om = omega + q * NM;
     for (int mn = threadIdx.x; mn < NB * NB; mn += blockDim.x) {
       float2 t[NM];
 #pragma unroll
       for (int jm = 0; jm < NM; ++jm) t[jm] = ts[mn + NB * NB * jm];
-#pragma unroll
+#pragma unroll 1
       for (int nu = 0; nu < NM; ++nu) {
         float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
         for (int jm = 0; jm < NM; ++jm) cfma(acc, t[jm], ps[jm + NM * nu]);
-        float v = (acc.x * acc.x + acc.y * acc.y) * om[nu];
-        part[nu] += (double)v;
+        const float v = (acc.x * acc.x + acc.y * acc.y) * (float)(0.5 / om[nu]);
         if (samp) sq[mn + NB * NB * nu] = (double)v;
+        // warp sum of this mode's contributions, kept per warp in shared memory
+        float w = v;
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        if ((threadIdx.x & 31) == 0) wred[(threadIdx.x >> 5) * NM + nu] += (double)w;
       }
     }
+    __syncthreads();  // the next iteration's prefetch overwrites this buffer
   }
   if (kcur >= 0) {
-#pragma unroll
-    for (int i = 0; i < NM; ++i) {
-      double v = part[i];
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&g2sum[i + NM * kcur], v);
+    __syncthreads();
+    if (threadIdx.x < NM) {
+      double v = 0.0;
+      for (int w = 0; w < 8; ++w) v += wred[w * NM + threadIdx.x];
+      atomicAdd(&g2sum[threadIdx.x + NM * kcur], v);
     }
   }
 }
@@ -902,9 +941,15 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
       // rotations, g2, in-place reduction
       {
         int64_t nblk = np;
-        unsigned grid = (unsigned)(nblk < (int64_t)ctx->sm_count * 8 ? nblk : (int64_t)ctx->sm_count * 8);
+        constexpr int RS = RotSmem<16, 12>::TOTAL;
+        static bool rattr = false;
+        if (!rattr) {
+          EPB_CUDA(cudaFuncSetAttribute(eph_rot_reduce_f32_kernel<16, 12>, cudaFuncAttributeMaxDynamicSharedMemorySize, RS));
+          rattr = true;
+        }
+        unsigned grid = (unsigned)(nblk < (int64_t)ctx->sm_count * 2 ? nblk : (int64_t)ctx->sm_count * 2);
         prof_begin(ctx, EPB_PROF_ROT);
-        eph_rot_reduce_f32_kernel<16, 12><<<grid, 256, 0, ctx->stream>>>(
+        eph_rot_reduce_f32_kernel<16, 12><<<grid, 256, RS, ctx->stream>>>(
             C2, 2 * nd, U32, uph32, omega, nki, nq, g2sum + nm * (ko + ki),
             g2_sample ? g2_sample + (ko + ki) * nsamp * nd : nullptr, sample_stride, nsamp);
         prof_end(ctx);

@@ -145,7 +145,7 @@ class Context:
         return c.value
 
     PROF_NAMES = ["fourier_f64", "zgemm", "eigh", "rotation", "rr_rotation", "umma_h", "umma_kq", "umma_rr",
-                  "split", "other"]
+                  "split", "other", "eigh_refine"]
 
     def profile(self, on=True):
         check(lib().epb_profile_enable(self.h, 1 if on else 0))

@@ -71,8 +71,9 @@ EPB_API int epb_workspace_bytes(epb_ctx* ctx, uint64_t* bytes_host);
 EPB_API int epb_launch_count(epb_ctx* ctx, int64_t* count_host);
 /* Per-kernel-family CUDA-event timing on the context stream (the reference's @timing /
    TimerOutputs instrumentation, src/common/timer.jl:5-24). Families, in order: fourier_f64, zgemm,
-   eigh, rotation, rr_rotation, umma_h, umma_kq, umma_rr, split, other. epb_profile_read
-   synchronises, returns total ms and launch counts for the first n families, optionally resets. */
+   eigh, rotation, rr_rotation, umma_h, umma_kq, umma_rr, split, other, eigh_refine. epb_profile_read
+   synchronises, returns total ms and launch counts for the first n families, optionally resets.
+   An eleventh family, eigh_refine, is the FP64 refinement stage of the mixed eigensolver. */
 EPB_API int epb_profile_enable(epb_ctx* ctx, int on);
 EPB_API int epb_profile_read(epb_ctx* ctx, double* ms_host, int64_t* count_host, int n, int reset);
 /* Test hook: make the N-th next workspace allocation fail (N = 0 disables). Drives the
