@@ -740,24 +740,34 @@ __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_g
 
 template <int NW, int NM>
 struct RotSmem {
-  static constexpr int NB = NW, NT = NW * NW * NM;
-  static constexpr int G = NT * 8, U = NW * NB * 8, PH = NM * NM * 8;
+  static constexpr int NB = NW, NT = NW * NW * NM, NC = NB * NM;  // NC columns (n, jm) of g
+  static constexpr int GLD = NW + 2;                // padded column stride (complex): conflict-free float4 reads
+  static constexpr int G = NC * GLD * 8, U = NW * NB * 8, PH = NM * NM * 8;
   static constexpr int BUF = G + U + PH;            // bytes of one operand buffer
-  static constexpr int TOTAL = 2 * BUF + NT * 8;    // two buffers + T
+  static constexpr int TLD = NB + 1;                // padded stride of T: conflict-free stores
+  static constexpr int TOTAL = 2 * BUF + TLD * NC * 8;  // two buffers + T
 };
 
+// Thread tiles (256 threads, nw = 16, nm = 12):
+//   stage 1: thread (mg, cg): m = 4 mg .. 4 mg + 3 (mg uniform per warp pair, so u reads broadcast),
+//            c = cg + 64 j, j = 0..2; two iw per 16-byte load.
+//   stage 2: thread (mng, ng): mn = mng + 64 i, i = 0..3, nu = 3 ng .. 3 ng + 2 (ng uniform per warp).
 template <int NW, int NM>
 __global__ void __launch_bounds__(256, 2) eph_rot_reduce_f32_kernel(
     const float* __restrict__ g, int64_t g_stride, const float2* __restrict__ ukq, const float2* __restrict__ uph,
     const double* __restrict__ omega, int64_t nkb, int64_t nq, double* __restrict__ g2sum,
     double* __restrict__ sample, int64_t stride, int64_t nsamp) {
+  static_assert(NW == 16 && NM == 12, "thread tiling written for nw = 16, nm = 12");
   using L = RotSmem<NW, NM>;
-  constexpr int NB = NW;
-  constexpr int NT = L::NT;
+  constexpr int NB = NW, NT = L::NT, NC = L::NC, GLD = L::GLD, TLD = L::TLD;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* ts = reinterpret_cast<float2*>(smem_raw + 2 * L::BUF);
-  __shared__ double wred[8 * NM];  // per-warp partial sums of g2 per mode (blockDim = 256)
-  for (int e = threadIdx.x; e < 8 * NM; e += blockDim.x) wred[e] = 0.0;
+  __shared__ double red[NM];
+  for (int e = threadIdx.x; e < NM; e += blockDim.x) red[e] = 0.0;
+  double part[3] = {0.0, 0.0, 0.0};
+  const int tid = threadIdx.x;
+  const int mg = tid >> 6, cg = tid & 63;          // stage 1
+  const int mng = tid & 63, ng = tid >> 6;         // stage 2
   const int64_t nblk = nkb * nq;
   auto prefetch = [&](int64_t blk, int buf) {
     if (blk < nblk) {
@@ -766,11 +776,28 @@ __global__ void __launch_bounds__(256, 2) eph_rot_reduce_f32_kernel(
       const char* gs = reinterpret_cast<const char*>(g + blk * g_stride);
       const char* us = reinterpret_cast<const char*>(ukq + blk * NW * NB);
       const char* ps = reinterpret_cast<const char*>(uph + q * NM * NM);
-      for (int c = threadIdx.x; c < L::G / 16; c += blockDim.x) cp_async16(dst + 16 * c, gs + 16 * c);
-      for (int c = threadIdx.x; c < L::U / 16; c += blockDim.x) cp_async16(dst + L::G + 16 * c, us + 16 * c);
-      for (int c = threadIdx.x; c < L::PH / 16; c += blockDim.x) cp_async16(dst + L::G + L::U + 16 * c, ps + 16 * c);
+      // g: column c (NW complex = 128 B = 8 chunks) goes to the padded slot c * GLD
+      for (int ch = tid; ch < NC * 8; ch += blockDim.x) {
+        const int c = ch >> 3, w = ch & 7;
+        cp_async16(dst + (c * GLD) * 8 + 16 * w, gs + 128 * c + 16 * w);
+      }
+      for (int ch = tid; ch < L::U / 16; ch += blockDim.x) cp_async16(dst + L::G + 16 * ch, us + 16 * ch);
+      for (int ch = tid; ch < L::PH / 16; ch += blockDim.x) cp_async16(dst + L::G + L::U + 16 * ch, ps + 16 * ch);
     }
     cp_async_commit();
+  };
+  auto flush = [&](int64_t k) {
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      atomicAdd(&red[3 * ng + j], part[j]);
+      part[j] = 0.0;
+    }
+    __syncthreads();
+    if (tid < NM) {
+      atomicAdd(&g2sum[tid + NM * k], red[tid]);
+      red[tid] = 0.0;
+    }
   };
   int64_t kcur = -1;
   int buf = 0;
@@ -778,72 +805,87 @@ __global__ void __launch_bounds__(256, 2) eph_rot_reduce_f32_kernel(
   for (int64_t blk = blockIdx.x; blk < nblk; blk += gridDim.x, buf ^= 1) {
     prefetch(blk + gridDim.x, buf ^ 1);
     const int64_t kl = blk / nq, q = blk % nq;
-    if (kl != kcur) {  // flush partial sums when the block moves to another k (uniform across the CTA)
-      if (kcur >= 0) {
-        __syncthreads();
-        if (threadIdx.x < NM) {
-          double v = 0.0;
-          for (int w = 0; w < 8; ++w) {
-            v += wred[w * NM + threadIdx.x];
-            wred[w * NM + threadIdx.x] = 0.0;
-          }
-          atomicAdd(&g2sum[threadIdx.x + NM * kcur], v);
-        }
-      }
+    if (kl != kcur) {  // uniform across the CTA
+      if (kcur >= 0) flush(kcur);
       kcur = kl;
     }
     cp_async_wait1();
     __syncthreads();
     const unsigned char* cb = smem_raw + buf * L::BUF;
-    const float2* gb = reinterpret_cast<const float2*>(cb);
-    const float2* us = reinterpret_cast<const float2*>(cb + L::G);
+    const float4* g4 = reinterpret_cast<const float4*>(cb);              // (iw, iw+1) pairs, column stride GLD/2
+    const float4* u4 = reinterpret_cast<const float4*>(cb + L::G);       // column m: 8 float4
     const float2* ps = reinterpret_cast<const float2*>(cb + L::G + L::U);
-    for (int c = threadIdx.x; c < NB * NM; c += blockDim.x) {  // column c = n + NB * jm
-      float2 gc[NW];
+    // ---- stage 1: T[m, c] = sum_iw conj(u[iw, m]) g[iw, c] ----
+    {
+      float2 acc[4][3];
 #pragma unroll
-      for (int iw = 0; iw < NW; ++iw) gc[iw] = gb[iw + NW * c];
-#pragma unroll 2
-      for (int m = 0; m < NB; ++m) {
-        float2 a0 = make_float2(0.f, 0.f), a1 = make_float2(0.f, 0.f);
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int iw = 0; iw < NW; iw += 2) {
-          cfma_conj(a0, us[iw + NW * m], gc[iw]);
-          cfma_conj(a1, us[iw + 1 + NW * m], gc[iw + 1]);
-        }
-        ts[m + NB * c] = make_float2(a0.x + a1.x, a0.y + a1.y);
+        for (int j = 0; j < 3; ++j) acc[i][j] = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int ip = 0; ip < NW / 2; ++ip) {
+        float4 uu[4], gg[3];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) uu[i] = u4[(4 * mg + i) * (NW / 2) + ip];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) gg[j] = g4[(cg + 64 * j) * (GLD / 2) + ip];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            cfma_conj(acc[i][j], make_float2(uu[i].x, uu[i].y), make_float2(gg[j].x, gg[j].y));
+            cfma_conj(acc[i][j], make_float2(uu[i].z, uu[i].w), make_float2(gg[j].z, gg[j].w));
+          }
       }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) ts[(4 * mg + i) + TLD * (cg + 64 * j)] = acc[i][j];
     }
     __syncthreads();
-    const bool samp = sample && (q % stride == 0);
-    double* sq = samp ? sample + ((kl * nsamp) + q / stride) * (int64_t)NT : nullptr;
-    const double* om = omega + q * NM;
-    for (int mn = threadIdx.x; mn < NB * NB; mn += blockDim.x) {
-      float2 t[NM];
+    // ---- stage 2: ep[mn, nu] = sum_jm T[mn, jm] uph[jm, nu], g2, partial sums ----
+    {
+      float2 acc[4][3];
 #pragma unroll
-      for (int jm = 0; jm < NM; ++jm) t[jm] = ts[mn + NB * NB * jm];
-#pragma unroll 1
-      for (int nu = 0; nu < NM; ++nu) {
-        float2 acc = make_float2(0.f, 0.f);
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int jm = 0; jm < NM; ++jm) cfma(acc, t[jm], ps[jm + NM * nu]);
-        const float v = (acc.x * acc.x + acc.y * acc.y) * (float)(0.5 / om[nu]);
-        if (samp) sq[mn + NB * NB * nu] = (double)v;
-        // warp sum of this mode's contributions, kept per warp in shared memory
-        float w = v;
-        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
-        if ((threadIdx.x & 31) == 0) wred[(threadIdx.x >> 5) * NM + nu] += (double)w;
+        for (int j = 0; j < 3; ++j) acc[i][j] = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int jm = 0; jm < NM; ++jm) {
+        float2 tt[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int mn = mng + 64 * i, m = mn & (NB - 1), n = mn / NB;
+          tt[i] = ts[m + TLD * (n + NB * jm)];
+        }
+        float2 pp[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) pp[j] = ps[jm + NM * (3 * ng + j)];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) cfma(acc[i][j], tt[i], pp[j]);
+      }
+      const bool samp = sample && (q % stride == 0);
+      double* sq = samp ? sample + ((kl * nsamp) + q / stride) * (int64_t)NT : nullptr;
+      const double* om = omega + q * NM;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const int nu = 3 * ng + j;
+        const float inv2w = (float)(0.5 / om[nu]);
+        float s = 0.f;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const float v = (acc[i][j].x * acc[i][j].x + acc[i][j].y * acc[i][j].y) * inv2w;
+          s += v;
+          if (samp) sq[mng + 64 * i + NB * NB * nu] = (double)v;
+        }
+        part[j] += (double)s;
       }
     }
     __syncthreads();  // the next iteration's prefetch overwrites this buffer
   }
-  if (kcur >= 0) {
-    __syncthreads();
-    if (threadIdx.x < NM) {
-      double v = 0.0;
-      for (int w = 0; w < 8; ++w) v += wred[w * NM + threadIdx.x];
-      atomicAdd(&g2sum[threadIdx.x + NM * kcur], v);
-    }
-  }
+  if (kcur >= 0) flush(kcur);
 }
 
 int fourier_f64(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, const epb_rset* rs, const double* xk,
