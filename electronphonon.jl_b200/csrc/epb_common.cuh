@@ -72,6 +72,12 @@ enum epb_slot {
   EPB_WS_PASS6,
   EPB_WS_PASS7,
   EPB_WS_MLP,
+  EPB_WS_MLP_OUT,
+  EPB_WS_MLP_CAL,
+  EPB_WS_PAIR0,
+  EPB_WS_PAIR1,
+  EPB_WS_PAIR2,
+  EPB_WS_PAIR3,
   EPB_WS_NSLOTS
 };
 
@@ -88,6 +94,10 @@ enum epb_prof_id {
   EPB_PROF_SPLIT,
   EPB_PROF_OTHER,
   EPB_PROF_REFINE,
+  EPB_PROF_TRIDIAG,
+  EPB_PROF_MLP_TRAIN,
+  EPB_PROF_MLP_INFER,
+  EPB_PROF_PAIRS,
   EPB_PROF_N
 };
 

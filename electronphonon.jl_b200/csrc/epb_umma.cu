@@ -193,12 +193,14 @@ __global__ void pack_a_herm_kernel(const double2* __restrict__ op, int nw, int64
   }
 }
 
-// Phase operand: row j of B2 = [cos 2 pi R.x_j | sin 2 pi R.x_j] (K-major), x_j = xa[:, j / nb] +
-// xb[:, j % nb] when xb != null (x_{k+q} for every pair of a k batch), else x_j = xa[:, j].
+// Phase operand: row j of B2 = [cos 2 pi R.x_j | sin 2 pi R.x_j] (K-major), x_j = xa[:, p / nb] +
+// xb[:, p % nb] with p = pidx[j] (pidx != null) or pair0 + j when xb != null (x_{k+q} for pairs of
+// a k list and a q list), else x_j = xa[:, j].
 template <bool BF16, int NPL>
 __global__ void pack_b_phase_kernel(const int4* __restrict__ rv, int64_t K, const double* __restrict__ xa,
-                                    const double* __restrict__ xb, int64_t nb, int64_t N, int64_t rows_pad,
-                                    int64_t KC, uint8_t* __restrict__ planes, int64_t plane_bytes) {
+                                    const double* __restrict__ xb, int64_t nb, const int64_t* __restrict__ pidx,
+                                    int64_t pair0, int64_t N, int64_t rows_pad, int64_t KC,
+                                    uint8_t* __restrict__ planes, int64_t plane_bytes) {
   const int64_t koff = sin_offset(K);
   const int64_t ncos = koff / 8;           // chunks covering [0, koff)
   const int64_t nch = KC * 8;
@@ -210,7 +212,8 @@ __global__ void pack_b_phase_kernel(const int4* __restrict__ rv, int64_t K, cons
     double x0 = 0, x1 = 0, x2 = 0;
     if (j < N) {
       if (xb) {
-        int64_t ja = j / nb, jb = j % nb;
+        const int64_t pj = pidx ? pidx[j] : pair0 + j;
+        int64_t ja = pj / nb, jb = pj % nb;
         x0 = xa[3 * ja] + xb[3 * jb];
         x1 = xa[3 * ja + 1] + xb[3 * jb + 1];
         x2 = xa[3 * ja + 2] + xb[3 * jb + 2];
@@ -576,7 +579,7 @@ int pack_a_herm(epb_ctx* ctx, const double2* op, int nw, int64_t K, Planes& out,
 }
 
 int pack_b_phase(epb_ctx* ctx, const epb_rset* rs, const double* xa, const double* xb, int64_t nb, int64_t N,
-                 Planes& out, uint8_t* mem) {
+                 Planes& out, uint8_t* mem, const int64_t* pidx = nullptr, int64_t pair0 = 0) {
   out.rows_pad = round_up(N, MX_NT);
   out.KC = kchunks(rs->nr);
   out.plane_bytes = plane_bytes_for(out.rows_pad, out.KC);
@@ -585,7 +588,7 @@ int pack_b_phase(epb_ctx* ctx, const epb_rset* rs, const double* xa, const doubl
   int64_t total = out.rows_pad * (sin_offset(rs->nr) / 8);
   prof_begin(ctx, EPB_PROF_SPLIT);
   pack_b_phase_kernel<MX_BF16, MX_NPL><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
-      rs->dev, rs->nr, xa, xb, nb, N, out.rows_pad, out.KC, out.p, out.plane_bytes);
+      rs->dev, rs->nr, xa, xb, nb, pidx, pair0, N, out.rows_pad, out.KC, out.p, out.plane_bytes);
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
@@ -626,6 +629,65 @@ int fourier_mixed(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, const 
   c64_to_c128_kernel<<<grid_for(ctx, M * N), 256, 0, ctx->stream>>>((const float2*)C, out, M, N, M, ldo);
   EPB_LAUNCH_CHECK();
   return split_gemm_check(ctx);
+}
+
+// =============================================================================================
+// Band energies on the tensor cores: the Hermitian-packed H(R) planes of a model, and H(x) for a
+// list of points as packed FP32 matrices (n^2 floats per point: Re of i <= j, then Im of i < j).
+
+struct BandPlanes {
+  uint8_t* mem = nullptr;
+  Planes H;
+};
+
+int band_planes_prepare(epb_ctx* ctx, const double2* ham, int nw, const epb_rset* rs, void** out) {
+  const int64_t hb = MX_NPL * plane_bytes_for(round_up((int64_t)nw * nw, 128), kchunks(rs->nr));
+  BandPlanes* bp = new BandPlanes();
+  if (cudaMalloc(&bp->mem, hb + 1024) != cudaSuccess) {
+    cudaGetLastError();
+    delete bp;
+    set_error("band planes: allocation of %lld bytes failed", (long long)hb);
+    return EPB_ERR_OOM;
+  }
+  uint8_t* base = (uint8_t*)(((uintptr_t)bp->mem + 1023) & ~uintptr_t(1023));
+  int st = pack_a_herm(ctx, ham, nw, rs->nr, bp->H, base);
+  if (st != EPB_OK) {
+    cudaFree(bp->mem);
+    delete bp;
+    return st;
+  }
+  *out = bp;
+  return EPB_OK;
+}
+
+void band_planes_free(void* p) {
+  BandPlanes* bp = (BandPlanes*)p;
+  if (!bp) return;
+  cudaFree(bp->mem);
+  delete bp;
+}
+
+// Largest point count per call of band_hk_packed (bounds its phase-plane workspace).
+int64_t band_hk_chunk(const epb_rset* rs) {
+  const int64_t per = MX_NPL * kchunks(rs->nr) * TILE_BYTES / 128;  // plane bytes per point
+  int64_t c = ((int64_t)768 << 20) / per;
+  c = c / MX_NT * MX_NT;
+  return c < MX_NT ? MX_NT : c;
+}
+
+// Hp[:, j] = packed H(x_j), points as in pack_b_phase_kernel; N <= band_hk_chunk(rs).
+int band_hk_packed(epb_ctx* ctx, const void* planes, const epb_rset* rs, int nw, const double* xa, const double* xb,
+                   int64_t nb, const int64_t* pidx, int64_t pair0, int64_t N, float* Hp) {
+  if (N == 0) return EPB_OK;
+  const BandPlanes* bp = (const BandPlanes*)planes;
+  const int64_t bbytes = MX_NPL * plane_bytes_for(round_up(N, MX_NT), kchunks(rs->nr));
+  void* ws = nullptr;
+  EPB_TRY(ws_get(ctx, EPB_WS_PAIR3, bbytes + 1024, &ws));
+  uint8_t* base = (uint8_t*)(((uintptr_t)ws + 1023) & ~uintptr_t(1023));
+  Planes B;
+  EPB_TRY(pack_b_phase(ctx, rs, xa, xb, nb, N, B, base, pidx, pair0));
+  const int64_t n2 = (int64_t)nw * nw;
+  return split_gemm(ctx, EPB_PROF_UMMA_H, bp->H, B, bp->H.rows_pad / 128, 1, n2, N, true, Hp, 0, n2);
 }
 
 // =============================================================================================

@@ -60,7 +60,38 @@ SIGNATURES = {
     "epb_model_create": [P, P, I64, P, I64, P, P, I64, P, I64, P, P, I64, I32, C.POINTER(P)],
     "epb_model_destroy": [P],
     "epb_eph_pass": [P, P, P, I64, P, I64, I32, I64, I64, P, P, P, P, P],
+    "epb_bands_create": [P, P, I64, P, I64, C.POINTER(P)],
+    "epb_bands_destroy": [P],
+    "epb_bands_eigvals": [P, P, P, I64, P, I32],
+    "epb_bands_window": [P, P, P, I64, D, D, I32, D, P, P, P, C.POINTER(I64), P],
+    "epb_pair_window": [P, P, P, I64, P, I64, D, D, P, I32, D, P, P, P, I64, C.POINTER(I64), P],
+    "epb_mlp_create": [P, P, I64, I64, I64, I64, C.c_uint64, C.POINTER(P)],
+    "epb_mlp_destroy": [P],
+    "epb_mlp_info": [P, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)],
+    "epb_mlp_get_params": [P, P, P],
+    "epb_mlp_set_params": [P, P, P],
+    "epb_mlp_set_scaling": [P, P, P, P],
+    "epb_mlp_get_scaling": [P, P, P, P],
+    "epb_mlp_features": [P, P, P, I64, P],
+    "epb_mlp_loss_grad": [P, P, P, P, I64, P, P],
+    "epb_mlp_train": [P, P, P, P, I64, P, P],
+    "epb_mlp_predict": [P, P, P, I64, P],
+    "epb_mlp_calibrate": [P, P, P, P, I64, D, P],
 }
+
+
+class WindowStats(C.Structure):
+    """epb_window_stats."""
+    _fields_ = [("tested", I64), ("culled", I64), ("evaluated", I64), ("rechecked", I64), ("kept", I64)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
+class MlpTrainOpts(C.Structure):
+    """epb_mlp_train_opts."""
+    _fields_ = [("epochs", I64), ("batch", I64), ("lr", D), ("lr_final", D), ("seed", C.c_uint64),
+                ("use_graph", C.c_int32), ("reserved", C.c_int32)]
 _RESTYPE = {"epb_last_error": C.c_char_p}
 
 _lock = threading.Lock()
@@ -145,7 +176,7 @@ class Context:
         return c.value
 
     PROF_NAMES = ["fourier_f64", "zgemm", "eigh", "rotation", "rr_rotation", "umma_h", "umma_kq", "umma_rr",
-                  "split", "other", "eigh_refine"]
+                  "split", "other", "eigh_refine", "tridiag", "mlp_train", "mlp_infer", "pairs"]
 
     def profile(self, on=True):
         check(lib().epb_profile_enable(self.h, 1 if on else 0))

@@ -71,9 +71,11 @@ EPB_API int epb_workspace_bytes(epb_ctx* ctx, uint64_t* bytes_host);
 EPB_API int epb_launch_count(epb_ctx* ctx, int64_t* count_host);
 /* Per-kernel-family CUDA-event timing on the context stream (the reference's @timing /
    TimerOutputs instrumentation, src/common/timer.jl:5-24). Families, in order: fourier_f64, zgemm,
-   eigh, rotation, rr_rotation, umma_h, umma_kq, umma_rr, split, other, eigh_refine. epb_profile_read
-   synchronises, returns total ms and launch counts for the first n families, optionally resets.
-   An eleventh family, eigh_refine, is the FP64 refinement stage of the mixed eigensolver. */
+   eigh, rotation, rr_rotation, umma_h, umma_kq, umma_rr, split, other, eigh_refine, tridiag,
+   mlp_train, mlp_infer, pairs. epb_profile_read synchronises, returns total ms and launch counts for
+   the first n families, optionally resets. eigh_refine is the FP64 refinement stage of the mixed
+   eigensolver; tridiag the Householder/Sturm eigenvalue path; mlp_* the surrogate's kernels; pairs
+   the (k, q) pair filter's compaction kernels. */
 EPB_API int epb_profile_enable(epb_ctx* ctx, int on);
 EPB_API int epb_profile_read(epb_ctx* ctx, double* ms_host, int64_t* count_host, int n, int reset);
 /* Test hook: make the N-th next workspace allocation fail (N = 0 disables). Drives the
@@ -181,6 +183,100 @@ EPB_API int epb_window_filter_noalloc(void* stream, const double* E, int64_t nw,
 EPB_API int epb_fill_iqs(epb_ctx* ctx, const int64_t* xkq_int, int64_t nkq, const int64_t* xk_int_host,
                  int64_t ng1, int64_t ng2, int64_t ng3, const int64_t* dense_hash_to_iq,
                  int64_t* iqs);
+
+/* ---- band energies, energy windows and the learned pre-filter ------------------------------ */
+typedef struct epb_bands epb_bands;
+typedef struct epb_mlp epb_mlp;
+
+/* Counters of one window call (host struct). tested: points (k) or pairs (k, q) considered;
+   culled: pairs removed by the surrogate; evaluated: points given the plain evaluation; rechecked:
+   points re-evaluated in FP64 by the mixed path's guard; kept: points / pairs with a non-empty
+   window. */
+typedef struct {
+  int64_t tested, culled, evaluated, rechecked, kept;
+} epb_window_stats;
+
+/* Bind an electron Hamiltonian H(R) (c128, (nw^2, nr), caller-owned; irvec int64 3 x nr, host)
+   for band-energy and window queries; builds its tensor-core operand planes once.
+   Replaces: the el_ham interpolator of compute_electron_states (src/electron_state.jl:118-150). */
+EPB_API int epb_bands_create(epb_ctx* ctx, const double* ham_op, int64_t nw, const int64_t* irvec_host,
+                             int64_t nr, epb_bands** out);
+EPB_API int epb_bands_destroy(epb_bands* bands);
+
+/* Ascending band energies E (nw x nk) at the points xk (3 x nk): H(x) by the Fourier sum (FP64, or
+   split-BF16 tensor cores for EPB_PREC_MIXED), Householder tridiagonalisation and bisection in
+   FP64 (order <= 32). Replaces: get_el_eigen_valueonly_batched
+   (src/wannier_to_bloch_batched.jl:75-88) for eigenvalue-only callers. */
+EPB_API int epb_bands_eigvals(epb_ctx* ctx, const epb_bands* bands, const double* xk, int64_t nk, double* E,
+                              int prec);
+
+/* Energy window of every point of xk (3 x nk): band_min / band_max (int32, 1-based, 0 / 0 when
+   empty) = searchsortedfirst(e, wmin) / searchsortedlast(e, wmax) from Sturm counts on the
+   tridiagonal, and the ascending 0-based list of kept points keep_idx (capacity nk) with its count
+   in *nkeep_host (synchronises). prec FP64: exact FP64 evaluation; MIXED: tensor-core H, FP32
+   counts at wmin -/+ guard and wmax -/+ guard, FP64 re-evaluation of points whose counts differ
+   across a guard interval (guard in Ry, > 0). Replaces: _filter_kpoints (src/filter.jl:40-72)
+   without the eigenvalue download. */
+EPB_API int epb_bands_window(epb_ctx* ctx, const epb_bands* bands, const double* xk, int64_t nk, double wmin,
+                             double wmax, int prec, double guard, int32_t* band_min, int32_t* band_max,
+                             int32_t* keep_idx, int64_t* nkeep_host, epb_window_stats* stats_host);
+
+/* (k, q) pair window: for every pair of the k list xk (3 x nk, normally the kept k) and the q list
+   xq (3 x nq), the band range at x_k + x_q; kept pairs (non-empty range) are written in ascending
+   pair order as pair index p = ik * nq + iq (int64) with band_min / band_max, up to `capacity`;
+   *npairs_host = the number of kept pairs (EPB_ERR_ARG, with the count, if it exceeds capacity).
+   mlp (may be NULL): a calibrated surrogate; pairs whose predicted bands all lie outside
+   [wmin - margin_n, wmax + margin_n] are culled before the plain evaluation. The kept set is the
+   same with and without the surrogate whenever its margins hold. Synchronises.
+   Replaces: the window skip of the pair loop (src/calculator/run_eph_over_k_and_q.jl:303-307) and
+   filter_qpoints (src/filter.jl:109-133). */
+EPB_API int epb_pair_window(epb_ctx* ctx, const epb_bands* bands, const double* xk, int64_t nk, const double* xq,
+                            int64_t nq, double wmin, double wmax, const epb_mlp* mlp, int prec, double guard,
+                            int64_t* pairs, int32_t* band_min, int32_t* band_max, int64_t capacity,
+                            int64_t* npairs_host, epb_window_stats* stats_host);
+
+/* Learned band-energy surrogate (no counterpart in the reference): an MLP on Fourier features
+   [cos 2 pi f.k, sin 2 pi f.k] of nf integer vectors f (int32 3 x nf, host), nhidden SiLU layers of
+   width `hidden`, nout linear outputs (normalised band energies). Parameters FP32, flat layout: per
+   layer W (in x out, row-major) then b (out), each block padded to a multiple of 4 floats.
+   Initialised from `seed` (uniform Glorot). */
+EPB_API int epb_mlp_create(epb_ctx* ctx, const int32_t* fvec_host, int64_t nf, int64_t hidden, int64_t nhidden,
+                           int64_t nout, uint64_t seed, epb_mlp** out);
+EPB_API int epb_mlp_destroy(epb_mlp* mlp);
+EPB_API int epb_mlp_info(const epb_mlp* mlp, int64_t* nparam_host, int64_t* nin_host, int64_t* nout_host);
+EPB_API int epb_mlp_get_params(epb_ctx* ctx, const epb_mlp* mlp, float* params);
+EPB_API int epb_mlp_set_params(epb_ctx* ctx, epb_mlp* mlp, const float* params);
+/* Target normalisation: output b predicts (E_b - mu_b) / sc_b (host arrays of nout). */
+EPB_API int epb_mlp_set_scaling(epb_ctx* ctx, epb_mlp* mlp, const double* mu_host, const double* sc_host);
+EPB_API int epb_mlp_get_scaling(epb_ctx* ctx, const epb_mlp* mlp, double* mu_host, double* sc_host);
+/* Feature rows (n x 2 nf, FP32) of the points x (3 x n). */
+EPB_API int epb_mlp_features(epb_ctx* ctx, const epb_mlp* mlp, const double* x, int64_t n, float* feat);
+/* Gradient of L = sum (y_pred - (E - mu) / sc)^2 / (n nout) over the n points x (3 x n) with band
+   energies E (nout x n), with respect to every parameter (FP32, nparam), and L itself (host, may be
+   NULL). n a multiple of 4, at most 65536. */
+EPB_API int epb_mlp_loss_grad(epb_ctx* ctx, epb_mlp* mlp, const double* x, const double* E, int64_t n, float* grad,
+                              double* loss_host);
+typedef struct {
+  int64_t epochs;     /* passes over the training set                                        */
+  int64_t batch;      /* rows per step, multiple of 16                                        */
+  double lr;          /* Adam learning rate at step 0 (cosine decay to lr_final)              */
+  double lr_final;
+  uint64_t seed;      /* shuffle seed                                                        */
+  int32_t use_graph;  /* 1: capture one epoch as a CUDA graph and replay it                  */
+  int32_t reserved;
+} epb_mlp_train_opts;
+/* Train on n points x (3 x n) with band energies E (nout x n): per-band normalisation from E, then
+   epochs x floor(n / batch) Adam steps. loss_host (epochs entries, may be NULL): mean batch loss of
+   each epoch. Synchronises. */
+EPB_API int epb_mlp_train(epb_ctx* ctx, epb_mlp* mlp, const double* x, const double* E, int64_t n,
+                          const epb_mlp_train_opts* opts, double* loss_host);
+/* Predicted band energies E (nout x n, FP64) at the points x (3 x n). */
+EPB_API int epb_mlp_predict(epb_ctx* ctx, const epb_mlp* mlp, const double* x, int64_t n, double* E);
+/* Culling margins: margin_b = safety * max over the held-out points x (3 x n) of
+   |predicted - E| for band b (E nout x n); stored in the model and returned in margin_host (nout,
+   may be NULL). safety >= 1. Synchronises. */
+EPB_API int epb_mlp_calibrate(epb_ctx* ctx, epb_mlp* mlp, const double* x, const double* E, int64_t n, double safety,
+                              double* margin_host);
 
 /* ---- whole e-ph pass ---------------------------------------------------------------------- */
 typedef struct epb_model epb_model;
