@@ -8,6 +8,11 @@ electron eigensolves, phonons, both Fourier stages, rotations, g2 and its in-pla
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--prec mixed|fp64] [--impl epb|reference]
 
+`--workload filter` measures the learned energy-window filter instead (config 4: nw = 32, R grid
+11^3, 96^3 k grid, 8192 random q, window E_F -/+ 0.3 eV with E_F the median of band 16): (k, k+q)
+pair tests per second over the kept k, with the surrogate pre-filter and without it (the plain
+window), whose kept sets must be identical.
+
 Multi-GPU: one process per GPU (torchrun); every rank runs its own full pass on its own k set
 (weak scaling, no data-path collective); the step time is the max over ranks.
 """
@@ -50,6 +55,10 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-nk", type=int, default=16)
     ap.add_argument("--cpu-nq", type=int, default=1024)
+    ap.add_argument("--workload", default="pass", choices=["pass", "filter"])
+    ap.add_argument("--grid", type=int, default=96, help="filter workload: k grid per axis")
+    ap.add_argument("--decay", type=float, default=1.5, help="filter workload: H(R) decay length")
+    ap.add_argument("--epochs", type=int, default=200, help="filter workload: surrogate training epochs")
     ap.add_argument("--small", action="store_true",
                     help="profiling case: Re grid 5^3, 32 k x 2048 q (a few GB on the device)")
     a = ap.parse_args()
@@ -375,9 +384,162 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------------------------
+FILTER_METRIC = "(k, k+q) pair window tests/s, nw=32 learned filter (kept set identical to the plain filter)"
+FILTER_UNIT = "pairs/s"
+
+
+def filter_setup(args, torch):
+    """Config-4 model, E_F, kept k, trained + calibrated surrogate (untimed setup)."""
+    from epb200 import learned, synth
+    from epb200.wannier import WannierObject
+
+    rng = np.random.default_rng(4)
+    irvec = synth.irvec_box(5)
+    ham = WannierObject(irvec, synth.hermitian_op_r(rng, 32, irvec, args.decay))
+    bm = learned.BandModel(ham)
+    xk_grid = synth.grid_kpoints((args.grid,) * 3)
+    xqs = synth.random_kpoints(args.nq, 4000)
+    t0 = time.perf_counter()
+    ef = float(torch.median(bm.band_energy(xk_grid, 16)).item())
+    half = 0.3 * synth.UNIT_EV
+    wmin, wmax = ef - half, ef + half
+    _, _, kkeep, kst = bm.window(xk_grid, wmin, wmax, prec=learned.PREC_MIXED)
+    from epb200.batched import jl
+
+    xk_kept = jl(xk_grid).index_select(0, kkeep.long()).contiguous()
+    t_grid = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    r2 = np.random.default_rng(44)
+    xt, xh = r2.random((3, 1 << 15)), r2.random((3, 1 << 14))
+    Et, Eh = bm.eigvals(xt), bm.eigvals(xh)
+    mlp = learned.Surrogate(nf=128, hidden=256, nhidden=3, nout=32, seed=45)
+    loss = mlp.train(xt, Et, epochs=args.epochs, batch=2048, lr=2e-3, lr_final=2e-5)
+    margin = mlp.calibrate(xh, Eh)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    info = {"e_fermi_ry": ef, "window_ry": [wmin, wmax], "k_grid": args.grid ** 3, "k_kept": int(kkeep.numel()),
+            "k_window_stats": kst, "train_points": 1 << 15, "train_energies": 32 << 15, "holdout_points": 1 << 14,
+            "train_loss_first_last": [float(loss[0]), float(loss[-1])], "margin_ry_max": float(margin.max()),
+            "margin_ry_mean": float(margin.mean()), "setup_s": {"grid": round(t_grid, 2), "surrogate": round(t_train, 2)}}
+    return bm, mlp, xk_kept, xqs, wmin, wmax, info
+
+
+def run_filter(args):
+    import torch
+
+    from epb200 import learned
+    from epb200.batched import jl
+
+    torch.cuda.set_device(0)
+    bm, mlp, xk_kept, xqs, wmin, wmax, info = filter_setup(args, torch)
+    xq_d = jl(xqs)
+    ctx = bm.ctx
+    nk = xk_kept.shape[0]
+    npairs = nk * args.nq
+    cap = max(npairs // 4, 1 << 20)
+
+    def step(use_mlp):
+        return learned.pair_window(bm, xk_kept, xq_d, wmin, wmax, mlp=mlp if use_mlp else None,
+                                   prec=learned.PREC_MIXED, capacity=cap)
+
+    res = {}
+    for use_mlp in (True, False):
+        for _ in range(args.warmup):
+            out = step(use_mlp)
+        torch.cuda.synchronize()
+        clk = clocks_start() if use_mlp else None
+        l0 = ctx.launch_count()
+        s = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(args.steps):
+            out = step(use_mlp)
+        e1.record(s)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        res[use_mlp] = {"ms": ms, "out": out, "launches": ctx.launch_count() - l0,
+                        "clocks": clocks_stop(clk, 0) if use_mlp else None}
+    a, b = res[True]["out"], res[False]["out"]
+    identical = bool(torch.equal(a[0], b[0]) and torch.equal(a[1], b[1]) and torch.equal(a[2], b[2]))
+    # per-family profile of one learned step
+    ctx.profile(True)
+    step(True)
+    torch.cuda.synchronize()
+    prof = ctx.profile_read(reset=True)
+    ctx.profile(False)
+    tot = sum(v[0] for v in prof.values())
+    profile = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / tot, 4)} for k, v in prof.items() if v[1]}
+    st = a[3]
+    peaks, psrc = measured_peaks()
+    roof = None
+    dom_name, (dom_ms, dom_cnt) = max(prof.items(), key=lambda kv: kv[1][0])
+    if dom_name == "umma_h" and dom_cnt:
+        # H(x) of every plainly evaluated point: 1024 x 1331 complex MACs, 8 flops each
+        flops = 8.0 * 1024 * 1331 * st["evaluated"]
+        ach = flops / (dom_ms * 1e-3) / 1e12
+        peak = peaks["bf16_tflops_sustained"] / 6
+        roof = {"bound": "tensor", "kernel": dom_name, "achieved": round(ach, 3), "peak": round(peak, 2),
+                "unit": "TFLOP/s", "frac": round(ach / peak, 4), "traffic": None,
+                "peak_source": f"{psrc} bf16 sustained / 6 split products"}
+    # end to end: host k / q lists in, kept pairs out
+    xk_h = xk_kept.cpu().pin_memory()
+    xq_h = xq_d.cpu().pin_memory()
+    kept = a[0].numel()
+    ho = [torch.empty(kept, dtype=torch.int64).pin_memory(), torch.empty(kept, dtype=torch.int32).pin_memory(),
+          torch.empty(kept, dtype=torch.int32).pin_memory()]
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(args.steps):
+        xk_dd = xk_h.to("cuda", non_blocking=True)
+        xq_dd = xq_h.to("cuda", non_blocking=True)
+        o = learned.pair_window(bm, xk_dd, xq_dd, wmin, wmax, mlp=mlp, prec=learned.PREC_MIXED, capacity=cap)
+        for h, d in zip(ho, o[:3]):
+            h.copy_(d, non_blocking=True)
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1) / args.steps
+    cpu = None
+    if not args.no_cpu:
+        from oracle import mlp_oracle as M
+
+        xk_s = xk_kept[:2].cpu().numpy().T.copy(order="F")
+        xq_s = xqs[:, :256]
+        t0 = time.perf_counter()
+        M.pair_window(bm.ham_host_op, 32, bm.ham.irvec, xk_s, xq_s, wmin, wmax)
+        dt = time.perf_counter() - t0
+        cores = int(os.environ.get("OPENBLAS_NUM_THREADS", os.cpu_count() or 1))
+        cpu = {"value": 2 * 256 / dt, "unit": FILTER_UNIT, "cores": cores, "kind": "port",
+               "sample": f"2 kept k x 256 q: FP64 Fourier (GEMM) + LAPACK ZHEEV + searchsorted, {dt:.1f} s"}
+    ms = res[True]["ms"]
+    line = {"metric": FILTER_METRIC, "value": npairs / (ms * 1e-3), "unit": FILTER_UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3/f32/f64 (window), f32 (surrogate)",
+            "data": f"synthetic (seeded; H(R) ~ CN(0,1) exp(-|R|/{args.decay}))",
+            "config": {"workload": f"config4 learned window filter: nw=32, R 11^3, {args.grid}^3 k grid, {args.nq} random q, "
+                                   "window E_F -/+ 0.3 eV, E_F = median of band 16",
+                       "pairs_per_step": npairs, "l2": "inputs larger than L2 (phase planes and H planes per chunk)",
+                       **info},
+            "plain_ms_per_step": round(res[False]["ms"], 3), "plain_value": npairs / (res[False]["ms"] * 1e-3),
+            "learned_speedup_vs_plain": round(res[False]["ms"] / ms, 3), "kept_sets_identical": identical,
+            "window_stats": st, "roofline": roof, "cpu_baseline": cpu,
+            "e2e": {"value": npairs / (ms_e2e * 1e-3), "unit": FILTER_UNIT,
+                    "h2d_bytes_per_step": xk_h.numel() * 8 + xq_h.numel() * 8,
+                    "d2h_bytes_per_step": kept * 16, "ms_per_step": round(ms_e2e, 3)},
+            "gpu_launches": res[True]["launches"] // args.steps * args.steps, "clocks": res[True]["clocks"],
+            "impl": "epb", "profile_one_step": profile}
+    print(json.dumps(line), flush=True)
+
+
 if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.workload == "filter":
+        if a.nq == NQ:
+            a.nq = 8192
+        run_filter(a)
     else:
         run_epb(a)

@@ -44,6 +44,8 @@ int fourier_f64(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, const ep
 int tridiag_window(epb_ctx* ctx, const float* Hp, const double2* A, int n, int64_t batch, double wmin, double wmax,
                    double delta, int32_t* bmin, int32_t* bmax, int32_t* flag);
 int tridiag_eigvals(epb_ctx* ctx, const float* Hp, const double2* A, int n, int64_t batch, double* E);
+int tridiag_band(epb_ctx* ctx, const float* Hp, const double2* A, int n, int64_t batch, int band, double* Dt,
+                 double* E2t, double* out);
 int mlp_predict_norm(epb_ctx* ctx, const epb_mlp* m, const double* xa, const double* xb, int64_t nb,
                      const int64_t* pidx, int64_t pair0, int64_t n, float* out_all);
 int split_gemm_check(epb_ctx* ctx);
@@ -366,6 +368,37 @@ int epb_bands_eigvals(epb_ctx* ctx, const epb_bands* bd, const double* xk, int64
     } else {
       EPB_TRY(band_hk_packed(ctx, bd->planes, bd->rs, (int)bd->nw, xk + 3 * k0, nullptr, 1, nullptr, 0, n, w.Hp));
       EPB_TRY(tridiag_eigvals(ctx, w.Hp, nullptr, (int)bd->nw, n, E + k0 * bd->nw));
+    }
+  }
+  return prec == EPB_PREC_MIXED ? split_gemm_check(ctx) : EPB_OK;
+}
+
+int epb_bands_band_energy(epb_ctx* ctx, const epb_bands* bd, const double* xk, int64_t nk, int64_t band,
+                          double* E, int prec) {
+  clear_error();
+  EPB_CHECK_ARG(ctx && bd, "epb_bands_band_energy: NULL argument");
+  EPB_CHECK_ARG(nk >= 0 && (nk == 0 || (xk && E)), "epb_bands_band_energy: bad arguments");
+  EPB_CHECK_ARG(band >= 1 && band <= bd->nw, "epb_bands_band_energy: band %lld outside 1..%lld", (long long)band,
+                (long long)bd->nw);
+  EPB_CHECK_ARG(prec == EPB_PREC_FP64 || prec == EPB_PREC_MIXED, "epb_bands_band_energy: unknown precision %d", prec);
+  if (nk == 0) return EPB_OK;
+  EPB_TRY(make_current(ctx));
+  const int64_t ch = eval_chunk(bd);
+  EvalWs w;
+  EPB_TRY(eval_ws(ctx, bd, std::min(ch, nk), w));
+  void* ws = nullptr;
+  EPB_TRY(ws_get(ctx, EPB_WS_PAIR2, (size_t)std::min(ch, nk) * 64 * sizeof(double) + 256, &ws));
+  double* Dt = (double*)ws;
+  double* E2t = Dt + std::min(ch, nk) * 32;
+  const int64_t n2 = bd->nw * bd->nw;
+  for (int64_t k0 = 0; k0 < nk; k0 += ch) {
+    const int64_t n = std::min(ch, nk - k0);
+    if (prec == EPB_PREC_FP64) {
+      EPB_TRY(fourier_f64(ctx, bd->ham, n2, n2, bd->rs, xk + 3 * k0, n, w.Hc, n2));
+      EPB_TRY(tridiag_band(ctx, nullptr, w.Hc, (int)bd->nw, n, (int)band - 1, Dt, E2t, E + k0));
+    } else {
+      EPB_TRY(band_hk_packed(ctx, bd->planes, bd->rs, (int)bd->nw, xk + 3 * k0, nullptr, 1, nullptr, 0, n, w.Hp));
+      EPB_TRY(tridiag_band(ctx, w.Hp, nullptr, (int)bd->nw, n, (int)band - 1, Dt, E2t, E + k0));
     }
   }
   return prec == EPB_PREC_MIXED ? split_gemm_check(ctx) : EPB_OK;

@@ -19,6 +19,8 @@
 // Sturm count (number of eigenvalues below sigma): q_0 = d_0 - sigma,
 // q_i = d_i - sigma - e_{i-1}^2 / q_{i-1}, count the negative q_i; |q| < pivmin is replaced by
 // -pivmin (the LAPACK dstebz convention).
+#include <algorithm>
+
 #include "epb_common.cuh"
 
 namespace epb {
@@ -38,6 +40,9 @@ struct TriArgs {
   int32_t* flag;       // guarded mode: 1 if an eigenvalue may lie within delta of a window edge
   // eigenvalue mode
   double* E;           // (n, batch) ascending
+  // tridiagonal mode: d and e^2 per matrix (32 doubles each)
+  double* Dt;
+  double* E2t;
 };
 
 template <typename T>
@@ -188,7 +193,8 @@ __device__ __forceinline__ void load_rows(const TriArgs& a, int64_t b, int lane,
   }
 }
 
-// MODE 0: window band ranges from Sturm counts at the shifts; MODE 1: all eigenvalues.
+// MODE 0: window band ranges from Sturm counts at the shifts; MODE 1: all eigenvalues; MODE 2: the
+// tridiagonal itself (d, e^2) for a later per-band bisection.
 template <typename T, int N, int MODE>
 __global__ void __launch_bounds__(32 * TRI_WARPS) tridiag_kernel(TriArgs a) {
   __shared__ TriSmem<T> smem[TRI_WARPS];
@@ -200,6 +206,12 @@ __global__ void __launch_bounds__(32 * TRI_WARPS) tridiag_kernel(TriArgs a) {
     T ar[N], ai[N];
     load_rows<T, N>(a, b, lane, ar, ai, s);
     householder_tridiag<T, N>(ar, ai, s, lane);
+    if (MODE == 2) {
+      a.Dt[b * 32 + lane] = (double)s.d[lane];
+      a.E2t[b * 32 + lane] = (double)s.e2[lane];
+      __syncwarp();
+      continue;
+    }
     // pivmin: smallest safe pivot scaled by the largest off-diagonal (dstebz)
     T emax = 0;
     for (int i = 0; i < n; ++i) emax = fmax(emax, s.e2[i]);
@@ -220,7 +232,7 @@ __global__ void __launch_bounds__(32 * TRI_WARPS) tridiag_kernel(TriArgs a) {
         a.bmax[b] = keep ? last : 0;
         if (a.flag) a.flag[b] = a.nsh == 4 && ((c0 != c1) || (c2 != c3));
       }
-    } else {
+    } else if (MODE == 1) {
       // Gershgorin interval of T, then bisection for eigenvalue `lane` (the (lane+1)-th smallest)
       T lo = 0, hi = 0;
       for (int i = 0; i < n; ++i) {
@@ -246,6 +258,39 @@ __global__ void __launch_bounds__(32 * TRI_WARPS) tridiag_kernel(TriArgs a) {
       }
     }
     __syncwarp();
+  }
+}
+
+// One eigenvalue (0-based index `band`) per stored tridiagonal, one thread per matrix: bisection
+// on the Gershgorin interval with Sturm counts, as in MODE 1.
+__global__ void tridiag_band_kernel(const double* __restrict__ Dt, const double* __restrict__ E2t, int n, int64_t batch,
+                                    int band, double* __restrict__ out) {
+  for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < batch; b += (int64_t)gridDim.x * blockDim.x) {
+    double d[32], e2[32];
+    double emax = 0, lo = 0, hi = 0;
+    for (int i = 0; i < n; ++i) {
+      d[i] = Dt[b * 32 + i];
+      e2[i] = E2t[b * 32 + i];
+    }
+    for (int i = 0; i < n; ++i) {
+      emax = fmax(emax, e2[i]);
+      const double r = (i > 0 ? sqrt(e2[i - 1]) : 0.0) + (i < n - 1 ? sqrt(e2[i]) : 0.0);
+      lo = i == 0 ? d[i] - r : fmin(lo, d[i] - r);
+      hi = i == 0 ? d[i] + r : fmax(hi, d[i] + r);
+    }
+    const double pivmin = 2.2250738585072014e-308 * fmax(1.0, emax), eps = 2.220446049250313e-16;
+    const double span = fmax(fabs(lo), fabs(hi));
+    lo -= 2 * eps * span + 2 * pivmin;
+    hi += 2 * eps * span + 2 * pivmin;
+    for (int it = 0; it < 200; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      if (!(hi - lo > 2 * eps * fmax(fabs(lo), fabs(hi)) + pivmin) || mid <= lo || mid >= hi) break;
+      if (sturm_count<double>(d, e2, n, mid, pivmin) > band)
+        hi = mid;
+      else
+        lo = mid;
+    }
+    out[b] = 0.5 * (lo + hi);
   }
 }
 
@@ -293,6 +338,28 @@ int tridiag_window(epb_ctx* ctx, const float* Hp, const double2* A, int n, int64
   a.sh[0] = wmin;
   a.sh[1] = nextafter(wmax, INFINITY);
   return launch_tridiag<double, 0>(ctx, a);
+}
+
+// Energy of band `band` (0-based) of each matrix: FP64 reduction stored to Dt/E2t (batch x 32
+// doubles each, caller workspace), then one bisection per matrix.
+int tridiag_band(epb_ctx* ctx, const float* Hp, const double2* A, int n, int64_t batch, int band, double* Dt,
+                 double* E2t, double* out) {
+  if (batch == 0) return EPB_OK;
+  EPB_CHECK_ARG(n >= 1 && n <= 32 && band >= 0 && band < n, "band energy: order %d / band %d", n, band);
+  TriArgs a{};
+  a.Hp = Hp;
+  a.A = A;
+  a.n = n;
+  a.batch = batch;
+  a.Dt = Dt;
+  a.E2t = E2t;
+  EPB_TRY((launch_tridiag<double, 2>(ctx, a)));
+  const int64_t blocks = std::min<int64_t>(cdiv(batch, 128), (int64_t)ctx->sm_count * 16);
+  prof_begin(ctx, EPB_PROF_TRIDIAG);
+  tridiag_band_kernel<<<(unsigned)std::max<int64_t>(blocks, 1), 128, 0, ctx->stream>>>(Dt, E2t, n, batch, band, out);
+  prof_end(ctx);
+  EPB_LAUNCH_CHECK();
+  return EPB_OK;
 }
 
 // Ascending eigenvalues (FP64 reduction and bisection) of a batch of order-n Hermitian matrices.

@@ -63,6 +63,7 @@ SIGNATURES = {
     "epb_bands_create": [P, P, I64, P, I64, C.POINTER(P)],
     "epb_bands_destroy": [P],
     "epb_bands_eigvals": [P, P, P, I64, P, I32],
+    "epb_bands_band_energy": [P, P, P, I64, I64, P, I32],
     "epb_bands_window": [P, P, P, I64, D, D, I32, D, P, P, P, C.POINTER(I64), P],
     "epb_pair_window": [P, P, P, I64, P, I64, D, D, P, I32, D, P, P, P, I64, C.POINTER(I64), P],
     "epb_mlp_create": [P, P, I64, I64, I64, I64, C.c_uint64, C.POINTER(P)],

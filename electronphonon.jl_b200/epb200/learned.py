@@ -54,6 +54,7 @@ class BandModel:
     """epb_bands: H(R) on the device plus its tensor-core operand planes."""
 
     def __init__(self, ham: WannierObject):
+        self.ham_host_op = None if ham.on_device else ham.op_r
         if not ham.on_device:
             ham = to_device(ham)
         self.ham = ham
@@ -83,6 +84,15 @@ class BandModel:
         nk = x.numel() // 3
         E = jl_empty((self.nw, nk), torch.float64)
         check(_lib.lib().epb_bands_eigvals(self.ctx.h, self.h, ptr(x), nk, ptr(E), prec))
+        return E
+
+    def band_energy(self, xks, band, prec=PREC_FP64):
+        """Energy of band `band` (1-based) at every point, device (nk,)."""
+        torch = _torch()
+        x = _xk_dev(xks)
+        nk = x.numel() // 3
+        E = torch.empty(nk, dtype=torch.float64, device=x.device)
+        check(_lib.lib().epb_bands_band_energy(self.ctx.h, self.h, ptr(x), nk, int(band), ptr(E), prec))
         return E
 
     def window(self, xks, wmin, wmax, prec=PREC_FP64, guard=DEFAULT_GUARD):
@@ -256,8 +266,8 @@ def learned_pair_filter(bands: BandModel, xk_grid, xqs, half_window, fermi_band,
     torch = _torch()
     t = {}
     t0 = time.perf_counter()
-    E_grid = bands.eigvals(xk_grid, prec=PREC_FP64)  # torch (nk, nw)
-    ef = float(torch.median(E_grid[:, fermi_band - 1]).item())
+    e_band = bands.band_energy(xk_grid, fermi_band, prec=PREC_FP64)
+    ef = float(torch.median(e_band).item())
     wmin, wmax = ef - half_window, ef + half_window
     _, _, k_keep, _ = bands.window(xk_grid, wmin, wmax, prec=prec, guard=guard)
     xk_all = _xk_dev(xk_grid)

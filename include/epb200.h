@@ -210,6 +210,11 @@ EPB_API int epb_bands_destroy(epb_bands* bands);
 EPB_API int epb_bands_eigvals(epb_ctx* ctx, const epb_bands* bands, const double* xk, int64_t nk, double* E,
                               int prec);
 
+/* Energy of one band (1-based `band`) at every point of xk (3 x nk): FP64 tridiagonalisation, then
+   one bisection per point. E has nk entries. */
+EPB_API int epb_bands_band_energy(epb_ctx* ctx, const epb_bands* bands, const double* xk, int64_t nk, int64_t band,
+                                  double* E, int prec);
+
 /* Energy window of every point of xk (3 x nk): band_min / band_max (int32, 1-based, 0 / 0 when
    empty) = searchsortedfirst(e, wmin) / searchsortedlast(e, wmax) from Sturm counts on the
    tridiagonal, and the ascending 0-based list of kept points keep_idx (capacity nk) with its count

@@ -197,6 +197,17 @@ def test_bands_eigvals_vs_lapack(L, nw, n_el):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("nw,band", [(8, 1), (13, 7), (32, 16), (32, 32)])
+def test_bands_band_energy(L, nw, band):
+    ham = _ham(nw, 2, 90 + nw)
+    bm = L.BandModel(ham)
+    x = np.random.default_rng(band).random((3, 131))
+    e = bm.band_energy(x, band).cpu().numpy()
+    ref = M.band_energies(ham.op_r, nw, ham.irvec, x)[band - 1]
+    assert np.max(np.abs(e - ref)) <= 1e-9
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("nw,n_el", [(8, 2), (13, 2), (32, 3)])
 def test_bands_window_vs_oracle(L, nw, n_el):
     ham = _ham(nw, n_el, 30 + nw)
