@@ -267,38 +267,50 @@ static int eval_ws(epb_ctx* ctx, const epb_bands* bd, int64_t cap, EvalWs& w) {
   return EPB_OK;
 }
 
-// Band ranges of N <= w.cap points (as in gather_points_kernel) into bmin/bmax; counts the FP64
-// re-evaluations into *rechecked.
-static int eval_points(epb_ctx* ctx, const epb_bands* bd, EvalWs& w, const double* xa, const double* xb, int64_t nb,
-                       const int64_t* pidx, int64_t pair0, int64_t N, double wmin, double wmax, int prec, double guard,
-                       int32_t* bmin, int32_t* bmax, int64_t* rechecked) {
-  if (N == 0) return EPB_OK;
+// Band ranges of ncand points (position c: pair pidx[c], or pair0 + c; see gather_points_kernel)
+// into cmin / cmax [0, ncand), in sub-chunks of at most w.cap points. In the mixed mode the flagged
+// positions of every sub-chunk are appended to rc_list (capacity ncand) and re-evaluated in FP64
+// together at the end (one count read-back per call).
+static int eval_candidates(epb_ctx* ctx, const epb_bands* bd, EvalWs& w, const double* xa, const double* xb,
+                           int64_t nb, const int64_t* pidx, int64_t pair0, int64_t ncand, double wmin, double wmax,
+                           int prec, double guard, int32_t* cmin, int32_t* cmax, int64_t* rc_list,
+                           int64_t* rechecked) {
+  if (ncand == 0) return EPB_OK;
   const int nw = (int)bd->nw;
   const int64_t n2 = bd->nw * bd->nw;
   if (prec == EPB_PREC_FP64) {
-    gather_points_kernel<<<grid_pts(ctx, N), 256, 0, ctx->stream>>>(xa, xb, nb, pidx, pair0, nullptr, N, w.x);
-    EPB_LAUNCH_CHECK();
-    EPB_TRY(fourier_f64(ctx, bd->ham, n2, n2, bd->rs, w.x, N, w.Hc, n2));
-    return tridiag_window(ctx, nullptr, w.Hc, nw, N, wmin, wmax, 0.0, bmin, bmax, nullptr);
+    for (int64_t c0 = 0; c0 < ncand; c0 += w.cap) {
+      const int64_t n = std::min(w.cap, ncand - c0);
+      gather_points_kernel<<<grid_pts(ctx, n), 256, 0, ctx->stream>>>(xa, xb, nb, pidx ? pidx + c0 : nullptr,
+                                                                      pair0 + c0, nullptr, n, w.x);
+      EPB_LAUNCH_CHECK();
+      EPB_TRY(fourier_f64(ctx, bd->ham, n2, n2, bd->rs, w.x, n, w.Hc, n2));
+      EPB_TRY(tridiag_window(ctx, nullptr, w.Hc, nw, n, wmin, wmax, 0.0, cmin + c0, cmax + c0, nullptr));
+    }
+    return EPB_OK;
   }
-  EPB_TRY(band_hk_packed(ctx, bd->planes, bd->rs, nw, xa, xb, nb, pidx, pair0, N, w.Hp));
-  EPB_TRY(tridiag_window(ctx, w.Hp, nullptr, nw, N, wmin, wmax, guard, bmin, bmax, w.flag));
-  // flagged points (positions in this call): FP64 re-evaluation
   EPB_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(int64_t), ctx->stream));
-  EPB_TRY(compact(ctx, w.cmp, w.flag, N, nullptr, 0, w.cnt, w.list, nullptr, nullptr, nullptr, nullptr, N));
+  for (int64_t c0 = 0; c0 < ncand; c0 += w.cap) {
+    const int64_t n = std::min(w.cap, ncand - c0);
+    EPB_TRY(band_hk_packed(ctx, bd->planes, bd->rs, nw, xa, xb, nb, pidx ? pidx + c0 : nullptr, pair0 + c0, n, w.Hp));
+    EPB_TRY(tridiag_window(ctx, w.Hp, nullptr, nw, n, wmin, wmax, guard, cmin + c0, cmax + c0, w.flag));
+    EPB_TRY(compact(ctx, w.cmp, w.flag, n, nullptr, c0, w.cnt, rc_list, nullptr, nullptr, nullptr, nullptr, ncand));
+  }
   const int64_t nf = read_i64(ctx, w.cnt);
   if (nf < 0) {
     set_error("window evaluation: reading the re-evaluation count failed");
     return EPB_ERR_CUDA;
   }
   *rechecked += nf;
-  if (nf == 0) return EPB_OK;
-  gather_points_kernel<<<grid_pts(ctx, nf), 256, 0, ctx->stream>>>(xa, xb, nb, pidx, pair0, w.list, nf, w.x);
-  EPB_LAUNCH_CHECK();
-  EPB_TRY(fourier_f64(ctx, bd->ham, n2, n2, bd->rs, w.x, nf, w.Hc, n2));
-  EPB_TRY(tridiag_window(ctx, nullptr, w.Hc, nw, nf, wmin, wmax, 0.0, w.rmin, w.rmax, nullptr));
-  recheck_merge_kernel<<<grid_pts(ctx, nf), 256, 0, ctx->stream>>>(w.list, nf, w.rmin, w.rmax, bmin, bmax);
-  EPB_LAUNCH_CHECK();
+  for (int64_t r0 = 0; r0 < nf; r0 += w.cap) {
+    const int64_t n = std::min(w.cap, nf - r0);
+    gather_points_kernel<<<grid_pts(ctx, n), 256, 0, ctx->stream>>>(xa, xb, nb, pidx, pair0, rc_list + r0, n, w.x);
+    EPB_LAUNCH_CHECK();
+    EPB_TRY(fourier_f64(ctx, bd->ham, n2, n2, bd->rs, w.x, n, w.Hc, n2));
+    EPB_TRY(tridiag_window(ctx, nullptr, w.Hc, nw, n, wmin, wmax, 0.0, w.rmin, w.rmax, nullptr));
+    recheck_merge_kernel<<<grid_pts(ctx, n), 256, 0, ctx->stream>>>(rc_list + r0, n, w.rmin, w.rmax, cmin, cmax);
+    EPB_LAUNCH_CHECK();
+  }
   return EPB_OK;
 }
 
@@ -423,27 +435,38 @@ int epb_bands_window(epb_ctx* ctx, const epb_bands* bd, const double* xk, int64_
   const int64_t ch = eval_chunk(bd);
   EvalWs w;
   EPB_TRY(eval_ws(ctx, bd, std::min(ch, nk), w));
-  void* ws = nullptr;
-  EPB_TRY(ws_get(ctx, EPB_WS_PAIR0, (size_t)std::min(ch, nk) * sizeof(int32_t) + 1024, &ws));
-  int32_t* kflag = (int32_t*)ws;
-  int64_t* running = (int64_t*)((uint8_t*)ws + ((size_t)std::min(ch, nk) * sizeof(int32_t) + 255) / 256 * 256);
-  EPB_CUDA(cudaMemsetAsync(running, 0, sizeof(int64_t), ctx->stream));
-  // keep indices are int32 (k lists of the reference are Int ranges over one grid)
   EPB_CHECK_ARG(nk <= INT32_MAX, "epb_bands_window: nk too large for int32 indices");
-  int64_t* kidx = nullptr;
-  void* ws2 = nullptr;
-  EPB_TRY(ws_get(ctx, EPB_WS_PAIR2, (size_t)nk * sizeof(int64_t) + 256, &ws2));
-  kidx = (int64_t*)ws2;
-  for (int64_t k0 = 0; k0 < nk; k0 += ch) {
-    const int64_t n = std::min(ch, nk - k0);
-    prof_begin(ctx, EPB_PROF_PAIRS);
-    EPB_TRY(eval_points(ctx, bd, w, xk + 3 * k0, nullptr, 1, nullptr, 0, n, wmin, wmax, prec, guard, bmin + k0,
-                        bmax + k0, &st.rechecked));
-    range_nonempty_kernel<<<grid_pts(ctx, n), 256, 0, ctx->stream>>>(bmin + k0, n, kflag);
-    EPB_LAUNCH_CHECK();
-    EPB_TRY(compact(ctx, w.cmp, kflag, n, nullptr, k0, running, kidx, nullptr, nullptr, nullptr, nullptr, nk));
-    prof_end(ctx);
-  }
+  // nk flags | running count | kept list (int64) | re-evaluation list | compaction scratch
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off += (bytes + 255) & ~size_t(255);
+    return o;
+  };
+  const size_t o_f = take((size_t)nk * sizeof(int32_t));
+  const size_t o_r = take(64);
+  const size_t o_k = take((size_t)nk * sizeof(int64_t));
+  const size_t o_l = take((size_t)nk * sizeof(int64_t));
+  const size_t o_bc = take((size_t)(cdiv(nk, CMP_THREADS) + 1) * sizeof(int32_t));
+  const size_t o_bo = take((size_t)(cdiv(nk, CMP_THREADS) + 1) * sizeof(int64_t));
+  void* ws = nullptr;
+  EPB_TRY(ws_get(ctx, EPB_WS_PAIR0, off + 256, &ws));
+  uint8_t* base = (uint8_t*)ws;
+  int32_t* kflag = (int32_t*)(base + o_f);
+  int64_t* running = (int64_t*)(base + o_r);
+  int64_t* kidx = (int64_t*)(base + o_k);
+  int64_t* rc_list = (int64_t*)(base + o_l);
+  Compactor kc;
+  kc.bcount = (int32_t*)(base + o_bc);
+  kc.boff = (int64_t*)(base + o_bo);
+  EPB_CUDA(cudaMemsetAsync(running, 0, sizeof(int64_t), ctx->stream));
+  prof_begin(ctx, EPB_PROF_PAIRS);
+  EPB_TRY(eval_candidates(ctx, bd, w, xk, nullptr, 1, nullptr, 0, nk, wmin, wmax, prec, guard, bmin, bmax, rc_list,
+                          &st.rechecked));
+  range_nonempty_kernel<<<grid_pts(ctx, nk), 256, 0, ctx->stream>>>(bmin, nk, kflag);
+  EPB_LAUNCH_CHECK();
+  EPB_TRY(compact(ctx, kc, kflag, nk, nullptr, 0, running, kidx, nullptr, nullptr, nullptr, nullptr, nk));
+  prof_end(ctx);
   const int64_t nkeep = read_i64(ctx, running);
   if (nkeep < 0) {
     set_error("epb_bands_window: reading the kept count failed");
@@ -508,6 +531,7 @@ int epb_pair_window(epb_ctx* ctx, const epb_bands* bd, const double* xk, int64_t
   const size_t o_b1 = take((size_t)pch * sizeof(int32_t));
   const size_t o_f = take((size_t)pch * sizeof(int32_t));
   const size_t o_o = take(mlp ? (size_t)pch * nout * sizeof(float) : 0);
+  const size_t o_rc = take((size_t)pch * sizeof(int64_t));
   const size_t o_r = take(64);
   const size_t o_bc = take((size_t)(cdiv(pch, CMP_THREADS) + 1) * sizeof(int32_t));
   const size_t o_bo = take((size_t)(cdiv(pch, CMP_THREADS) + 1) * sizeof(int64_t));
@@ -521,6 +545,7 @@ int epb_pair_window(epb_ctx* ctx, const epb_bands* bd, const double* xk, int64_t
   float* pred = (float*)(base + o_o);
   int64_t* running = (int64_t*)(base + o_r);
   int64_t* ccount = running + 1;
+  int64_t* rc_list = (int64_t*)(base + o_rc);
   Compactor cc;
   cc.bcount = (int32_t*)(base + o_bc);
   cc.boff = (int64_t*)(base + o_bo);
@@ -550,11 +575,8 @@ int epb_pair_window(epb_ctx* ctx, const epb_bands* bd, const double* xk, int64_t
       st.culled += np - ncand;
     }
     st.evaluated += ncand;
-    for (int64_t c0 = 0; c0 < ncand; c0 += ech) {
-      const int64_t n = std::min(ech, ncand - c0);
-      EPB_TRY(eval_points(ctx, bd, w, xk, xq, nq, cl ? cl + c0 : nullptr, pair0 + c0, n, wmin, wmax, prec, guard,
-                          cmin + c0, cmax + c0, &st.rechecked));
-    }
+    EPB_TRY(eval_candidates(ctx, bd, w, xk, xq, nq, cl, pair0, ncand, wmin, wmax, prec, guard, cmin, cmax, rc_list,
+                            &st.rechecked));
     prof_begin(ctx, EPB_PROF_PAIRS);
     range_nonempty_kernel<<<grid_pts(ctx, ncand), 256, 0, ctx->stream>>>(cmin, ncand, flag);
     EPB_LAUNCH_CHECK();

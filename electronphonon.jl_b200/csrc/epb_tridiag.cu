@@ -47,8 +47,8 @@ struct TriArgs {
 
 template <typename T>
 struct TriSmem {
-  T u[2][32];   // reflector u (re, im)
-  T w[2][32];   // w (re, im)
+  typename cplx<T>::type u[32];  // reflector u
+  typename cplx<T>::type w[32];  // w = p - K u
   T d[32];      // tridiagonal
   T e2[32];
   float stage[32 * 32];  // packed FP32 input staging
@@ -65,6 +65,10 @@ __device__ __forceinline__ float warp_sum(float v) {
   return v;
 }
 
+__device__ __forceinline__ double sturm_div(double a, double b) { return a / b; }
+// FP32 counts are only used with guard intervals far wider than the 2-ulp fast division error.
+__device__ __forceinline__ float sturm_div(float a, float b) { return __fdividef(a, b); }
+
 template <typename T>
 __device__ __forceinline__ int sturm_count(const T* d, const T* e2, int n, T sigma, T pivmin) {
   int c = 0;
@@ -72,7 +76,7 @@ __device__ __forceinline__ int sturm_count(const T* d, const T* e2, int n, T sig
   if (fabs(q) < pivmin) q = -pivmin;
   c += q < T(0);
   for (int i = 1; i < n; ++i) {
-    q = (d[i] - sigma) - e2[i - 1] / q;
+    q = (d[i] - sigma) - sturm_div(e2[i - 1], q);
     if (fabs(q) < pivmin) q = -pivmin;
     c += q < T(0);
   }
@@ -105,19 +109,26 @@ __device__ __forceinline__ void householder_tridiag(T (&ar)[N], T (&ai)[N], TriS
       ur = a1 > T(0) ? x1r * f : xn;
       ui = a1 > T(0) ? x1i * f : T(0);
     }
-    s.u[0][lane] = ur;
-    s.u[1][lane] = ui;
+    s.u[lane] = mk2(ur, ui);
     __syncwarp();
-    // p_i = beta sum_{j>k} A[i][j] u_j
-    T pr = 0, pi = 0;
+    // p_i = beta sum_{j>k} A[i][j] u_j (two interleaved partial sums for instruction-level parallelism)
+    T pr0 = 0, pi0 = 0, pr1 = 0, pi1 = 0;
 #pragma unroll
     for (int j = k + 1; j < N; ++j) {
-      const T vr = s.u[0][j], vi = s.u[1][j];
-      pr += ar[j] * vr - ai[j] * vi;
-      pi += ar[j] * vi + ai[j] * vr;
+      const auto v = s.u[j];
+      if ((j & 1) == 0) {
+        pr0 = fma(ar[j], v.x, pr0);
+        pr0 = fma(-ai[j], v.y, pr0);
+        pi0 = fma(ar[j], v.y, pi0);
+        pi0 = fma(ai[j], v.x, pi0);
+      } else {
+        pr1 = fma(ar[j], v.x, pr1);
+        pr1 = fma(-ai[j], v.y, pr1);
+        pi1 = fma(ar[j], v.y, pi1);
+        pi1 = fma(ai[j], v.x, pi1);
+      }
     }
-    pr *= beta;
-    pi *= beta;
+    T pr = (pr0 + pr1) * beta, pi = (pi0 + pi1) * beta;
     if (lane <= k) {
       pr = T(0);
       pi = T(0);
@@ -125,13 +136,13 @@ __device__ __forceinline__ void householder_tridiag(T (&ar)[N], T (&ai)[N], TriS
     // K = (beta / 2) Re(u^H p)
     const T kk = T(0.5) * beta * warp_sum(ur * pr + ui * pi);
     const T wr = pr - kk * ur, wi = pi - kk * ui;
-    s.w[0][lane] = wr;
-    s.w[1][lane] = wi;
+    s.w[lane] = mk2(wr, wi);
     __syncwarp();
     if (lane > k) {
 #pragma unroll
       for (int j = k + 1; j < N; ++j) {
-        const T ujr = s.u[0][j], uji = s.u[1][j], wjr = s.w[0][j], wji = s.w[1][j];
+        const auto uj = s.u[j], wj = s.w[j];
+        const T ujr = uj.x, uji = uj.y, wjr = wj.x, wji = wj.y;
         // A[i][j] -= u_i conj(w_j) + w_i conj(u_j)
         ar[j] -= (ur * wjr + ui * wji) + (wr * ujr + wi * uji);
         ai[j] -= (ui * wjr - ur * wji) + (wi * ujr - wr * uji);
@@ -219,7 +230,8 @@ __global__ void __launch_bounds__(32 * TRI_WARPS) tridiag_kernel(TriArgs a) {
     const T pivmin = tiny * fmax(T(1), emax);
     if (MODE == 0) {
       int c = 0;
-      if (lane < a.nsh) c = sturm_count<T>(s.d, s.e2, n, (T)a.sh[lane], pivmin);
+      const double shv = lane == 0 ? a.sh[0] : lane == 1 ? a.sh[1] : lane == 2 ? a.sh[2] : a.sh[3];
+      if (lane < a.nsh) c = sturm_count<T>(s.d, s.e2, n, (T)shv, pivmin);
       const int c0 = __shfl_sync(0xffffffffu, c, 0), c1 = __shfl_sync(0xffffffffu, c, 1);
       const int c2 = __shfl_sync(0xffffffffu, c, 2), c3 = __shfl_sync(0xffffffffu, c, 3);
       if (lane == 0) {

@@ -24,6 +24,7 @@
 // Every wait is bounded (clock64 budget); on timeout the kernel raises an error flag, drains its
 // own copies and MMAs, frees TMEM and returns (EPB_ERR_TIMEOUT on the host).
 #include "epb_common.cuh"
+
 #include "epb_umma.cuh"
 
 namespace epb {
