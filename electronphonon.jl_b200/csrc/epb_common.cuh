@@ -72,6 +72,7 @@ enum epb_slot {
   EPB_WS_PASS6,
   EPB_WS_PASS7,
   EPB_WS_MLP,
+  EPB_WS_EIGH_BIG,
   EPB_WS_MLP_OUT,
   EPB_WS_MLP_CAL,
   EPB_WS_PAIR0,

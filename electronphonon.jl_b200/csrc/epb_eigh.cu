@@ -15,121 +15,12 @@
 //                    of the FP32 vectors, S = V^H H V in FP64 (H re-read in FP64), a thresholded
 //                    FP64 Jacobi on the nearly diagonal S (this re-orthogonalises near-degenerate
 //                    clusters, whose FP32 vectors are only defined up to a rotation), V <- V Q.
-#include "epb_common.cuh"
+#include <algorithm>
+#include <cstring>
+
+#include "epb_jacobi.cuh"
 
 namespace epb {
-
-template <int TEAM>
-__device__ __forceinline__ void team_sync() {
-  if (TEAM == 32)
-    __syncwarp();
-  else
-    __syncthreads();
-}
-
-// Round-robin (circle method) pair i of round r for m players (m even); player m-1 is fixed.
-__device__ __forceinline__ void rr_pair(int m, int r, int i, int& p, int& q) {
-  int a, b;
-  if (i == 0) {
-    a = m - 1;
-    b = r;
-  } else {
-    a = (r + i) % (m - 1);
-    b = (r - i + (m - 1)) % (m - 1);
-  }
-  p = a < b ? a : b;
-  q = a < b ? b : a;
-}
-
-template <typename T>
-struct RotParam {
-  T c, s;
-  typename cplx<T>::type e;  // e^{i phi}
-  int p, q;                  // p < 0: skip
-};
-
-// One full Jacobi solve of the n x n Hermitian matrix in A (column-major, leading dim lda) with
-// eigenvectors accumulated into V (leading dim ldv; must hold identity on entry if want_v).
-// Returns the number of sweeps used (max_sweeps + 1 if not converged).
-template <typename T, int TEAM>
-__device__ int jacobi_team(typename cplx<T>::type* A, int lda, typename cplx<T>::type* V, int ldv,
-                           int n, bool want_v, RotParam<T>* prm, int* flag, T thr,
-                           int max_sweeps) {
-  using C = typename cplx<T>::type;
-  const int tid = threadIdx.x % TEAM;
-  const int m = (n + 1) & ~1;
-  const int npair = m / 2;
-  int sweep = 0;
-  for (; sweep < max_sweeps; ++sweep) {
-    if (tid == 0) *flag = 0;
-    team_sync<TEAM>();
-    for (int r = 0; r < m - 1; ++r) {
-      for (int i = tid; i < npair; i += TEAM) {
-        int p, q;
-        rr_pair(m, r, i, p, q);
-        RotParam<T> P;
-        P.p = -1;
-        P.q = q;
-        if (q < n) {
-          C b = A[p + q * lda];
-          T ab = sqrt(b.x * b.x + b.y * b.y);
-          if (ab > thr) {
-            T a = A[p + p * lda].x, d = A[q + q * lda].x;
-            T tau = (d - a) / (T(2) * ab);
-            T t;
-            if (fabs(tau) > T(1e15))
-              t = T(0.5) / tau;
-            else
-              t = (tau >= T(0) ? T(1) : T(-1)) / (fabs(tau) + sqrt(T(1) + tau * tau));
-            T c = T(1) / sqrt(T(1) + t * t);
-            P.c = c;
-            P.s = t * c;
-            P.e = mk2(b.x / ab, b.y / ab);
-            P.p = p;
-            *flag = 1;
-          }
-        }
-        prm[i] = P;
-      }
-      team_sync<TEAM>();
-      // columns: A <- A J, V <- V J
-      for (int task = tid; task < npair * n; task += TEAM) {
-        int i = task / n, row = task % n;
-        RotParam<T> P = prm[i];
-        if (P.p < 0) continue;
-        C ap = A[row + P.p * lda], aq = A[row + P.q * lda];
-        C ec = mk2(P.e.x, -P.e.y);
-        C sp = cmul(ec, aq);
-        C sq = cmul(P.e, ap);
-        A[row + P.p * lda] = mk2(P.c * ap.x - P.s * sp.x, P.c * ap.y - P.s * sp.y);
-        A[row + P.q * lda] = mk2(P.s * sq.x + P.c * aq.x, P.s * sq.y + P.c * aq.y);
-        if (want_v) {
-          C vp = V[row + P.p * ldv], vq = V[row + P.q * ldv];
-          C tp = cmul(ec, vq), tq = cmul(P.e, vp);
-          V[row + P.p * ldv] = mk2(P.c * vp.x - P.s * tp.x, P.c * vp.y - P.s * tp.y);
-          V[row + P.q * ldv] = mk2(P.s * tq.x + P.c * vq.x, P.s * tq.y + P.c * vq.y);
-        }
-      }
-      team_sync<TEAM>();
-      // rows: A <- J^H A
-      for (int task = tid; task < npair * n; task += TEAM) {
-        int i = task / n, col = task % n;
-        RotParam<T> P = prm[i];
-        if (P.p < 0) continue;
-        C ap = A[P.p + col * lda], aq = A[P.q + col * lda];
-        C ec = mk2(P.e.x, -P.e.y);
-        C sp = cmul(P.e, aq), sq = cmul(ec, ap);
-        A[P.p + col * lda] = mk2(P.c * ap.x - P.s * sp.x, P.c * ap.y - P.s * sp.y);
-        A[P.q + col * lda] = mk2(P.s * sq.x + P.c * aq.x, P.s * sq.y + P.c * aq.y);
-      }
-      team_sync<TEAM>();
-    }
-    int any = *flag;
-    team_sync<TEAM>();
-    if (!any) break;
-  }
-  return sweep;
-}
 
 struct EighArgs {
   double2* A;
@@ -147,7 +38,17 @@ struct EighArgs {
   const float* Hp;       // mixed kernel only: packed FP32 Hermitian input (n*n floats per matrix:
                          // Re H_ij for i <= j then Im H_ij for i < j, both column by column)
   float2* U32;           // mixed kernel only: eigenvectors as complex64 (n x n per matrix)
+  int n_lo;              // varlen size classes: orders <= n_lo belong to other kernels (skipped silently);
+  int skip_hi;           // nonzero: orders above NMAX are skipped silently too (the caller counts bad orders)
 };
+
+// Matrix order outside this kernel's class: skip; count only orders that no kernel handles.
+__device__ __forceinline__ bool eigh_skip(const EighArgs& a, int n, int nmax, int tid) {
+  if (n >= 1 && n <= nmax && n > a.n_lo) return false;
+  const bool bad = a.skip_hi == 0 && (n < 0 || n > nmax);
+  if (bad && tid == 0) atomicAdd(a.badsize, 1);
+  return true;
+}
 
 // Shared memory layout per team (elements of the solve type T):
 //   A: n x (n+1) [padded], V: n x n, plus RotParam[npair] and a flag.
@@ -172,10 +73,7 @@ __global__ void eigh_kernel(EighArgs a) {
   const int64_t nteams = (int64_t)gridDim.x * TEAMS;
   for (int64_t b = team_global; b < a.batch; b += nteams) {
     const int n = a.nvec ? a.nvec[b] : a.n_uniform;
-    if (n < 1 || n > NMAX) {  // order outside this kernel's shared-memory plan: skip, report
-      if (n != 0 && tid == 0) atomicAdd(a.badsize, 1);
-      continue;
-    }
+    if (eigh_skip(a, n, NMAX, tid)) continue;
     const int64_t aoff = a.a_off ? a.a_off[b] : b * (int64_t)n * n;
     const int64_t eoff = a.e_off ? a.e_off[b] : b * (int64_t)n;
     double2* Ag = a.A + aoff;
@@ -278,10 +176,7 @@ __global__ void eigh_mixed_kernel(EighArgs a) {
   const int64_t nteams = (int64_t)gridDim.x * TEAMS;
   for (int64_t b = team_global; b < a.batch; b += nteams) {
     const int n = a.nvec ? a.nvec[b] : a.n_uniform;
-    if (n < 1 || n > NMAX) {  // order outside this kernel's shared-memory plan: skip, report
-      if (n != 0 && tid == 0) atomicAdd(a.badsize, 1);
-      continue;
-    }
+    if (eigh_skip(a, n, NMAX, tid)) continue;
     const int64_t aoff = a.a_off ? a.a_off[b] : b * (int64_t)n * n;
     const int64_t eoff = a.e_off ? a.e_off[b] : b * (int64_t)n;
     double2* Ag = a.A ? a.A + aoff : nullptr;
@@ -321,8 +216,10 @@ __global__ void eigh_mixed_kernel(EighArgs a) {
     for (int w = 0; w < TEAM / 32; ++w) tot += red[team * (TEAM / 32) + w];
     team_sync<TEAM>();
     const double fro = sqrt(tot);
+    // FP32 stop at 8 eps32 x the RMS eigenvalue (rounding of degenerate pairs stays below it); the FP64
+    // stage below supplies the accuracy
     int sw = jacobi_team<float, TEAM>(A32, lda, V32, n, n, true, prm32, flag,
-                                      1.1920929e-07f * (float)fro / (float)n, a.max_sweeps);
+                                      8.f * 1.1920929e-07f * (float)(fro / sqrt((double)n)), a.max_sweeps);
     if (sw >= a.max_sweeps && tid == 0) atomicAdd(a.nonconv, 1);
     // V64 <- V32, then modified Gram-Schmidt (column by column)
     for (int e = tid; e < n * n; e += TEAM) {
@@ -593,17 +490,81 @@ static int eigh_small(epb_ctx* ctx, const EighArgs& a, int prec) {
   return eigh_dispatch(ctx, s, 16, EPB_PREC_FP64);
 }
 
+int eigh_big_launch(epb_ctx* ctx, double2* A, const int64_t* a_off, const int32_t* nvec, int n_uniform, int64_t batch,
+                    double* E, const int64_t* e_off, bool want_v, int n_lo, int prec, int* nonconv, int* badsize);
+
+// Orders per size class of a varlen batch: [0] 1..16, [1] 17..32, [2] 33..64, [3] 65..96, [4] outside
+// 0..96 (unsupported; order 0 is an empty matrix).
+__global__ void eigh_class_count_kernel(const int32_t* __restrict__ nvec, int64_t batch, int* __restrict__ cnt) {
+  int c[5] = {0, 0, 0, 0, 0};
+  for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < batch; b += (int64_t)gridDim.x * blockDim.x) {
+    const int n = nvec[b];
+    c[0] += n >= 1 && n <= 16;
+    c[1] += n > 16 && n <= 32;
+    c[2] += n > 32 && n <= 64;
+    c[3] += n > 64 && n <= 96;
+    c[4] += n < 0 || n > 96;
+  }
+  for (int i = 0; i < 5; ++i) {
+    int v = c[i];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(cnt + i, v);
+  }
+}
+
 int eigh_run(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
   if (a.batch == 0) return EPB_OK;
+  EPB_CHECK_ARG(prec == EPB_PREC_FP64 || prec == EPB_PREC_MIXED, "eigensolver: unknown precision mode %d", prec);
   a.nonconv = ctx->dstat + 0;
   a.badsize = ctx->dstat + 1;
   EPB_CUDA(cudaMemsetAsync(ctx->dstat, 0, 2 * sizeof(int), ctx->stream));
   a.max_sweeps = prec == EPB_PREC_FP64 ? 30 : 20;
-  if (!a.nvec && a.n_uniform <= 16 && (prec == EPB_PREC_FP64 || prec == EPB_PREC_MIXED))
-    EPB_TRY(eigh_small(ctx, a, prec));
-  else
-    EPB_TRY(eigh_dispatch(ctx, a, nmax, prec));
-  return eigh_check(ctx);
+  if (!a.nvec) {
+    const int n = a.n_uniform;
+    if (n <= 16)
+      EPB_TRY(eigh_small(ctx, a, prec));
+    else if (n <= 64)
+      EPB_TRY(eigh_dispatch(ctx, a, n, prec));
+    else if (n <= 96) {
+      EPB_CHECK_ARG(!a.mass, "eigensolver: phonon (mass-scaled) batches are limited to order 64");
+      EPB_TRY(eigh_big_launch(ctx, a.A, nullptr, nullptr, n, a.batch, a.E, nullptr, a.want_v != 0, 0, prec, a.nonconv,
+                              a.badsize));
+    } else {
+      set_error("eigensolver: matrix order %d > 96 not supported by this build", n);
+      return EPB_ERR_ARG;
+    }
+    return eigh_check(ctx);
+  }
+  // varlen: one kernel per size class present in the batch (one small read-back of the class counts)
+  (void)nmax;
+  int* cnt = ctx->dstat + 8;
+  EPB_CUDA(cudaMemsetAsync(cnt, 0, 5 * sizeof(int), ctx->stream));
+  eigh_class_count_kernel<<<(unsigned)std::min<int64_t>(cdiv(a.batch, 256), (int64_t)ctx->sm_count * 8), 256, 0,
+                            ctx->stream>>>(a.nvec, a.batch, cnt);
+  EPB_LAUNCH_CHECK();
+  int hc[5];
+  EPB_CUDA(cudaMemcpyAsync(ctx->pinned, cnt, 5 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  EPB_CUDA(cudaStreamSynchronize(ctx->stream));
+  memcpy(hc, ctx->pinned, sizeof(hc));
+  const int lo[3] = {0, 16, 32}, hi[3] = {16, 32, 64};
+  for (int c = 0; c < 3; ++c) {
+    if (hc[c] == 0) continue;
+    EighArgs s = a;
+    s.n_lo = lo[c];
+    s.skip_hi = 1;
+    EPB_TRY(eigh_dispatch(ctx, s, hi[c], prec));
+  }
+  if (hc[3] > 0) {
+    EPB_CHECK_ARG(!a.mass, "eigensolver: phonon (mass-scaled) batches are limited to order 64");
+    EPB_TRY(eigh_big_launch(ctx, a.A, a.a_off, a.nvec, 0, a.batch, a.E, a.e_off, a.want_v != 0, 64, prec, a.nonconv,
+                            a.badsize));
+  }
+  EPB_TRY(eigh_check(ctx));
+  if (hc[4] > 0) {
+    set_error("eigensolver: %d matrices have an order outside 0..96 (skipped)", hc[4]);
+    return EPB_ERR_ARG;
+  }
+  return EPB_OK;
 }
 
 // Stream-ordered variant for the pass pipeline: counters accumulate in a context slot until

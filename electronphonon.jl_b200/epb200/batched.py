@@ -128,6 +128,47 @@ def eigen_batched(Hk, prec=PREC_FP64):
     return E, Hk
 
 
+class VarlenBatch:
+    """Matrices of uneven order packed back to back (each column-major), as epb_eigh_varlen reads them."""
+
+    def __init__(self, mats, device="cuda"):
+        torch = _torch()
+        ns = np.array([m.shape[0] for m in mats], dtype=np.int64)
+        a_off = np.zeros(len(mats), dtype=np.int64)
+        e_off = np.zeros(len(mats), dtype=np.int64)
+        if len(mats):
+            a_off[1:] = np.cumsum(ns * ns)[:-1]
+            e_off[1:] = np.cumsum(ns)[:-1]
+        flat = np.concatenate([np.asfortranarray(m, dtype=np.complex128).reshape(-1, order="F") for m in mats]) \
+            if len(mats) else np.zeros(1, np.complex128)
+        self.ns, self.a_off_h, self.e_off_h = ns, a_off, e_off
+        self.A = torch.from_numpy(flat).to(device)
+        self.n = torch.from_numpy(ns.astype(np.int32)).to(device)
+        self.a_off = torch.from_numpy(a_off).to(device)
+        self.e_off = torch.from_numpy(e_off).to(device)
+        self.E = torch.empty(max(int(ns.sum()), 1), dtype=torch.float64, device=device)
+
+    def unpack(self):
+        """(list of eigenvalue vectors, list of eigenvector matrices) on the host."""
+        A = self.A.cpu().numpy()
+        E = self.E.cpu().numpy()
+        es, us = [], []
+        for n, ao, eo in zip(self.ns, self.a_off_h, self.e_off_h):
+            es.append(E[eo:eo + n].copy())
+            us.append(A[ao:ao + n * n].reshape(n, n, order="F").copy())
+        return es, us
+
+
+def eigen_varlen(mats, prec=PREC_FP64, jobz="V"):
+    """Batched eigensolve of matrices of uneven order (upper triangle read, eigenvectors in place);
+    returns (eigenvalues, eigenvectors) lists. Replaces eigen_batched over ragged inputs
+    (`ext/ElectronPhononCUDAExt.jl:80-115`)."""
+    vb = VarlenBatch(mats)
+    check(_lib.lib().epb_eigh_varlen(_ctx().h, ptr(vb.A), ptr(vb.a_off), ptr(vb.n), len(mats), ptr(vb.E),
+                                     ptr(vb.e_off), jobz.encode(), prec))
+    return vb.unpack()
+
+
 def _fourier_hk_batched(itp, xks, prec=PREC_FP64):
     nw = int(round(np.sqrt(itp.parent.ndata)))
     if nw * nw != itp.parent.ndata:
