@@ -23,28 +23,7 @@
 #include <cmath>
 #include <vector>
 
-#include "epb_common.cuh"
-
-struct epb_mlp {
-  epb_ctx* ctx = nullptr;
-  int nf = 0, nin = 0, hidden = 0, nhidden = 0, nout = 0;
-  int64_t nparam = 0;
-  std::vector<int64_t> w_off, b_off;  // per linear layer
-  std::vector<int> fan_in, fan_out;
-  int4* fvec = nullptr;     // feature vectors (device)
-  float* params = nullptr;  // [nparam]
-  float* adam_m = nullptr;
-  float* adam_v = nullptr;
-  float* y_mu = nullptr;    // [nout]
-  float* y_sc = nullptr;    // [nout]
-  double* margin = nullptr;  // [nout] calibrated culling margin (Ry)
-  std::vector<double> margin_host;
-  bool scaled = false;
-  bool calibrated = false;
-  int64_t* step = nullptr;  // device step counter (Adam t)
-  double* loss_acc = nullptr;  // device per-epoch loss sums (grown on demand)
-  int64_t loss_cap = 0;
-};
+#include "epb_mlp.cuh"
 
 namespace epb {
 
@@ -632,6 +611,7 @@ int epb_mlp_create(epb_ctx* ctx, const int32_t* fvec_host, int64_t nf, int64_t h
     EPB_LAUNCH_CHECK();
   }
   m->margin_host.assign(nout, 0.0);
+  m->tc_dirty = true;
   EPB_CUDA(cudaStreamSynchronize(ctx->stream));
   *out = m;
   return EPB_OK;
@@ -643,6 +623,7 @@ int epb_mlp_destroy(epb_mlp* m) {
   cudaFree(m->params);
   cudaFree(m->step);
   cudaFree(m->loss_acc);
+  cudaFree(m->tc_image);
   delete m;
   return EPB_OK;
 }
@@ -670,6 +651,7 @@ int epb_mlp_set_params(epb_ctx* ctx, epb_mlp* m, const float* src) {
   EPB_TRY(make_current(ctx));
   EPB_CUDA(cudaMemcpyAsync(m->params, src, m->nparam * sizeof(float), cudaMemcpyDeviceToDevice, ctx->stream));
   m->calibrated = false;
+  m->tc_dirty = true;
   return EPB_OK;
 }
 
@@ -801,6 +783,7 @@ int epb_mlp_train(epb_ctx* ctx, epb_mlp* m, const double* x, const double* E, in
   EPB_CUDA(cudaMemsetAsync(m->adam_m, 0, 2 * m->nparam * sizeof(float), ctx->stream));
   m->scaled = true;
   m->calibrated = false;
+  m->tc_dirty = true;
 
   TrainShape ts{};
   ts.n = n;
@@ -897,9 +880,17 @@ namespace epb {
 
 // Normalised predictions of the n points given as coordinates (xb == null) or as pairs xa + xb
 // (pair indices pidx, or pair0 + j): out (n x nout, FP32) in a caller buffer. Chunked internally.
+bool mlp_tc_eligible(const epb_mlp* m);
+int mlp_predict_tc(epb_ctx* ctx, const epb_mlp* m, const double* xa, const double* xb, int64_t nb, const int64_t* pidx,
+                   int64_t pair0, int64_t n, float* out);
+int mlp_tc_check(epb_ctx* ctx);
+
+// The inference path of the model (tensor cores when eligible and selected, else the FP32 kernels);
+// calibration and screening both go through here, so the margins match the path that screens.
 int mlp_predict_norm(epb_ctx* ctx, const epb_mlp* m, const double* xa, const double* xb, int64_t nb,
                      const int64_t* pidx, int64_t pair0, int64_t n, float* out_all) {
   if (n == 0) return EPB_OK;
+  if (mlp_tc_eligible(m)) return mlp_predict_tc(ctx, m, xa, xb, nb, pidx, pair0, n, out_all);
   const int64_t CH = 32768;
   void* ws = nullptr;
   const int64_t rows = std::min<int64_t>(cdiv(n, 4) * 4, CH);
@@ -952,6 +943,21 @@ int epb_mlp_predict(epb_ctx* ctx, const epb_mlp* m, const double* x, int64_t n, 
   mlp_denorm_kernel<<<grid1d(ctx, n * m->nout), 256, 0, ctx->stream>>>(out, m->nout, n, m->y_mu, m->y_sc, E);
   EPB_LAUNCH_CHECK();
   prof_end(ctx);
+  return mlp_tc_eligible(m) ? mlp_tc_check(ctx) : EPB_OK;
+}
+
+int epb_mlp_set_inference(epb_mlp* m, int mode) {
+  clear_error();
+  EPB_CHECK_ARG(m && (mode == 0 || mode == 1), "epb_mlp_set_inference: mode must be 0 (FP32) or 1 (BF16 tensor cores)");
+  if (m->infer_mode != mode) m->calibrated = false;  // margins belong to the path that was calibrated
+  m->infer_mode = mode;
+  return EPB_OK;
+}
+
+int epb_mlp_inference_path(const epb_mlp* m, int* path_host) {
+  clear_error();
+  EPB_CHECK_ARG(m && path_host, "epb_mlp_inference_path: NULL argument");
+  *path_host = mlp_tc_eligible(m) ? 1 : 0;
   return EPB_OK;
 }
 

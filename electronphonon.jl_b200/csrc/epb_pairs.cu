@@ -49,6 +49,7 @@ int tridiag_band(epb_ctx* ctx, const float* Hp, const double2* A, int n, int64_t
 int mlp_predict_norm(epb_ctx* ctx, const epb_mlp* m, const double* xa, const double* xb, int64_t nb,
                      const int64_t* pidx, int64_t pair0, int64_t n, float* out_all);
 int split_gemm_check(epb_ctx* ctx);
+int mlp_tc_check(epb_ctx* ctx);
 int mlp_screen_params(const epb_mlp* m, const float** mu, const float** sc, const double** margin, int* nout,
                       bool* calibrated);
 
@@ -584,6 +585,7 @@ int epb_pair_window(epb_ctx* ctx, const epb_bands* bd, const double* xk, int64_t
     prof_end(ctx);
   }
   if (prec == EPB_PREC_MIXED) EPB_TRY(split_gemm_check(ctx));
+  if (mlp) EPB_TRY(mlp_tc_check(ctx));
   const int64_t nk_out = read_i64(ctx, running);
   if (nk_out < 0) {
     set_error("epb_pair_window: reading the kept count failed");

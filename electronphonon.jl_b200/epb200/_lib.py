@@ -78,6 +78,8 @@ SIGNATURES = {
     "epb_mlp_train": [P, P, P, P, I64, P, P],
     "epb_mlp_predict": [P, P, P, I64, P],
     "epb_mlp_calibrate": [P, P, P, P, I64, D, P],
+    "epb_mlp_set_inference": [P, I32],
+    "epb_mlp_inference_path": [P, C.POINTER(I32)],
 }
 
 

@@ -197,6 +197,16 @@ class Surrogate:
         self.history = loss
         return loss
 
+    def set_inference(self, mode):
+        """1: BF16 tensor cores (default), 0: FP32 kernels. Clears the calibration."""
+        check(_lib.lib().epb_mlp_set_inference(self.h, int(mode)))
+        self.margin = None
+
+    def inference_path(self):
+        v = C.c_int()
+        check(_lib.lib().epb_mlp_inference_path(self.h, C.byref(v)))
+        return v.value
+
     def predict(self, xks):
         torch = _torch()
         x = _xk_dev(xks)

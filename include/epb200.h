@@ -275,6 +275,11 @@ typedef struct {
    each epoch. Synchronises. */
 EPB_API int epb_mlp_train(epb_ctx* ctx, epb_mlp* mlp, const double* x, const double* E, int64_t n,
                           const epb_mlp_train_opts* opts, double* loss_host);
+/* Inference path: 1 (default) = BF16 tensor cores (tcgen05; layer widths multiples of 64 up to 256,
+   nout a multiple of 16 up to 256, nf a multiple of 4), 0 = the FP32 kernels used in training.
+   Changing it clears the calibration. epb_mlp_inference_path reports the path in use (1 or 0). */
+EPB_API int epb_mlp_set_inference(epb_mlp* mlp, int mode);
+EPB_API int epb_mlp_inference_path(const epb_mlp* mlp, int* path_host);
 /* Predicted band energies E (nout x n, FP64) at the points x (3 x n). */
 EPB_API int epb_mlp_predict(epb_ctx* ctx, const epb_mlp* mlp, const double* x, int64_t n, double* E);
 /* Culling margins: margin_b = safety * max over the held-out points x (3 x n) of

@@ -109,6 +109,24 @@ def adam_step(p, m, v, g, t, lr, b1=0.9, b2=0.999, eps=1e-8):
     return p - lr * mh / (np.sqrt(vh) + eps), m, v
 
 
+def bf16_round(x):
+    """Round to the nearest BF16 value (ties to even), returned as float64."""
+    u = np.ascontiguousarray(np.asarray(x, dtype=np.float32)).view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    return u.view(np.float32).astype(np.float64)
+
+
+def forward_bf16(params, shapes, X):
+    """Normalised outputs of the tensor-core inference: BF16 inputs, weights and hidden activations,
+    wide accumulation, FP32 bias and activation."""
+    Ws, bs = unpack(params, shapes)
+    h = bf16_round(X)
+    for l, (W, b) in enumerate(zip(Ws, bs)):
+        z = h @ bf16_round(W) + b
+        h = bf16_round(z * _sig(z)) if l < len(Ws) - 1 else z
+    return h
+
+
 def predict(params, shapes, fvec, x, mu, sc):
     """Denormalised band energies (nout, n) at the points x (3, n)."""
     out, _ = forward(params, shapes, features(fvec, x))

@@ -106,6 +106,7 @@ def test_mlp_features(L):
 @pytest.mark.gpu
 def test_mlp_forward_matches_oracle(L):
     s = L.Surrogate(nf=64, hidden=64, nhidden=3, nout=16, seed=5)
+    s.set_inference(0)  # the FP32 kernels of training
     shapes, nparam = M.layer_shapes(s.nin, 64, 3, 16)
     assert nparam == s.nparam
     rng = np.random.default_rng(4)
@@ -119,6 +120,31 @@ def test_mlp_forward_matches_oracle(L):
     out, _ = M.forward(p.astype(np.float64), shapes, F)
     ref = (out * sc.astype(np.float32).astype(np.float64)[None, :] + mu.astype(np.float32)[None, :]).T
     assert np.max(np.abs(E - ref)) <= 2e-5 * max(1.0, np.max(np.abs(ref)))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nf,hidden,nhidden,nout", [(64, 64, 3, 16), (128, 256, 3, 32), (32, 128, 2, 48)])
+def test_mlp_tensor_core_inference(L, nf, hidden, nhidden, nout):
+    """tcgen05 BF16 inference vs a BF16-rounding emulation of the same network (FP64 accumulation)."""
+    s = L.Surrogate(nf=nf, hidden=hidden, nhidden=nhidden, nout=nout, seed=21)
+    assert s.inference_path() == 1
+    shapes, nparam = M.layer_shapes(s.nin, hidden, nhidden, nout)
+    rng = np.random.default_rng(22)
+    p = _rand_params(shapes, nparam, rng).astype(np.float32)
+    s.set_params(p)
+    s.set_scaling(np.zeros(nout), np.ones(nout))
+    x = rng.random((3, 1000)) * 2 - 0.5  # 8 tiles, the last one ragged
+    E = s.predict(x).cpu().numpy()  # torch shape (n, nout) = Julia (nout, n)
+    F = s.features(x).cpu().numpy().astype(np.float64)
+    ref = M.forward_bf16(p.astype(np.float64), shapes, F)
+    err = np.abs(E - ref)
+    scale = np.abs(ref).max()
+    assert np.linalg.norm(E - ref) <= 2e-3 * np.linalg.norm(ref), np.linalg.norm(E - ref) / np.linalg.norm(ref)
+    assert err.max() <= 2e-2 * scale, err.max() / scale
+    # and it is close to the FP32 path (BF16 rounding only)
+    s.set_inference(0)
+    E32 = s.predict(x).cpu().numpy()
+    assert np.linalg.norm(E - E32) <= 5e-2 * np.linalg.norm(E32)
 
 
 @pytest.mark.gpu
