@@ -416,7 +416,7 @@ def filter_setup(args, torch):
     t_grid = time.perf_counter() - t0
     t0 = time.perf_counter()
     r2 = np.random.default_rng(44)
-    xt, xh = r2.random((3, 1 << 15)), r2.random((3, 1 << 14))
+    xt, xh = r2.random((3, 1 << 15)), r2.random((3, 1 << 16))
     Et, Eh = bm.eigvals(xt), bm.eigvals(xh)
     mlp = learned.Surrogate(nf=128, hidden=256, nhidden=3, nout=32, seed=45)
     loss = mlp.train(xt, Et, epochs=args.epochs, batch=2048, lr=2e-3, lr_final=2e-5)
@@ -424,7 +424,8 @@ def filter_setup(args, torch):
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
     info = {"e_fermi_ry": ef, "window_ry": [wmin, wmax], "k_grid": args.grid ** 3, "k_kept": int(kkeep.numel()),
-            "k_window_stats": kst, "train_points": 1 << 15, "train_energies": 32 << 15, "holdout_points": 1 << 14,
+            "k_window_stats": kst, "train_points": 1 << 15, "train_energies": 32 << 15, "holdout_points": 1 << 16,
+            "margin_safety": 1.5,
             "train_loss_first_last": [float(loss[0]), float(loss[-1])], "margin_ry_max": float(margin.max()),
             "margin_ry_mean": float(margin.mean()), "setup_s": {"grid": round(t_grid, 2), "surrogate": round(t_train, 2)}}
     return bm, mlp, xk_kept, xqs, wmin, wmax, info

@@ -54,6 +54,7 @@ int mlp_screen_params(const epb_mlp* m, const float** mu, const float** sc, cons
                       bool* calibrated);
 
 constexpr int CMP_THREADS = 1024;
+constexpr int64_t EPB_AUDIT_STRIDE = 64;  // one culled pair in 64 is re-evaluated by the plain path
 
 static unsigned grid_pts(epb_ctx* ctx, int64_t total) {
   int64_t b = cdiv(total, 256);
@@ -174,6 +175,26 @@ __global__ void recheck_merge_kernel(const int64_t* __restrict__ list, int64_t n
 __global__ void i64_to_i32_kernel(const int64_t* __restrict__ a, int64_t n, int32_t* __restrict__ b) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     b[i] = (int32_t)a[i];
+}
+
+// Audit sample: every `stride`-th pair of the chunk that the surrogate culled.
+__global__ void audit_mark_kernel(const int32_t* __restrict__ flag, int64_t n, int64_t stride,
+                                  int32_t* __restrict__ aflag) {
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x)
+    aflag[j] = flag[j] == 0 && j % stride == 0;
+}
+
+__global__ void count_nonempty_kernel(const int32_t* __restrict__ bmin, int64_t n, int64_t* __restrict__ count) {
+  int c = 0;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x)
+    c += bmin[j] > 0;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd((unsigned long long*)count, (unsigned long long)c);
+}
+
+__global__ void fill_one_kernel(int32_t* __restrict__ flag, int64_t n) {
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x)
+    flag[j] = 1;
 }
 
 // Surrogate screen: flag[j] = 1 unless every predicted band lies outside [wmin - m_b, wmax + m_b].
@@ -533,6 +554,7 @@ int epb_pair_window(epb_ctx* ctx, const epb_bands* bd, const double* xk, int64_t
   const size_t o_f = take((size_t)pch * sizeof(int32_t));
   const size_t o_o = take(mlp ? (size_t)pch * nout * sizeof(float) : 0);
   const size_t o_rc = take((size_t)pch * sizeof(int64_t));
+  const size_t o_af = take(mlp ? (size_t)pch * sizeof(int32_t) : 0);
   const size_t o_r = take(64);
   const size_t o_bc = take((size_t)(cdiv(pch, CMP_THREADS) + 1) * sizeof(int32_t));
   const size_t o_bo = take((size_t)(cdiv(pch, CMP_THREADS) + 1) * sizeof(int64_t));
@@ -547,6 +569,8 @@ int epb_pair_window(epb_ctx* ctx, const epb_bands* bd, const double* xk, int64_t
   int64_t* running = (int64_t*)(base + o_r);
   int64_t* ccount = running + 1;
   int64_t* rc_list = (int64_t*)(base + o_rc);
+  int32_t* aflag = (int32_t*)(base + o_af);
+  int64_t* vcount = running + 2;
   Compactor cc;
   cc.bcount = (int32_t*)(base + o_bc);
   cc.boff = (int64_t*)(base + o_bo);
@@ -563,6 +587,36 @@ int epb_pair_window(epb_ctx* ctx, const epb_bands* bd, const double* xk, int64_t
       mlp_screen_kernel<<<grid_pts(ctx, np), 256, 0, ctx->stream>>>(pred, nout, np, mu, sc, margin, wmin, wmax, flag);
       prof_end(ctx);
       EPB_LAUNCH_CHECK();
+      // the plain path judges the surrogate: evaluate an evenly spaced sample of the culled pairs; a
+      // culled pair with a non-empty window sends the whole chunk to the plain evaluation
+      audit_mark_kernel<<<grid_pts(ctx, np), 256, 0, ctx->stream>>>(flag, np, EPB_AUDIT_STRIDE, aflag);
+      EPB_LAUNCH_CHECK();
+      EPB_CUDA(cudaMemsetAsync(ccount, 0, 2 * sizeof(int64_t), ctx->stream));  // ccount, vcount
+      EPB_TRY(compact(ctx, cc, aflag, np, nullptr, pair0, ccount, cand, nullptr, nullptr, nullptr, nullptr, np));
+      const int64_t na = read_i64(ctx, ccount);
+      if (na < 0) {
+        set_error("epb_pair_window: reading the audit count failed");
+        return EPB_ERR_CUDA;
+      }
+      int64_t viol = 0;
+      if (na > 0) {
+        EPB_TRY(eval_candidates(ctx, bd, w, xk, xq, nq, cand, 0, na, wmin, wmax, prec, guard, cmin, cmax, rc_list,
+                                &st.rechecked));
+        count_nonempty_kernel<<<grid_pts(ctx, na), 256, 0, ctx->stream>>>(cmin, na, vcount);
+        EPB_LAUNCH_CHECK();
+        viol = read_i64(ctx, vcount);
+        if (viol < 0) {
+          set_error("epb_pair_window: reading the audit result failed");
+          return EPB_ERR_CUDA;
+        }
+      }
+      st.audited += na;
+      st.violations += viol;
+      if (viol > 0) {
+        ++st.fallback_chunks;
+        fill_one_kernel<<<grid_pts(ctx, np), 256, 0, ctx->stream>>>(flag, np);
+        EPB_LAUNCH_CHECK();
+      }
       EPB_CUDA(cudaMemsetAsync(ccount, 0, sizeof(int64_t), ctx->stream));
       prof_begin(ctx, EPB_PROF_PAIRS);
       EPB_TRY(compact(ctx, cc, flag, np, nullptr, pair0, ccount, cand, nullptr, nullptr, nullptr, nullptr, np));

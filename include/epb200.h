@@ -191,9 +191,11 @@ typedef struct epb_mlp epb_mlp;
 /* Counters of one window call (host struct). tested: points (k) or pairs (k, q) considered;
    culled: pairs removed by the surrogate; evaluated: points given the plain evaluation; rechecked:
    points re-evaluated in FP64 by the mixed path's guard; kept: points / pairs with a non-empty
-   window. */
+   window; audited: culled pairs re-evaluated by the plain path as a check of the surrogate (one in
+   64 per chunk); violations: audited pairs whose window was not empty; fallback_chunks: chunks
+   that, after a violation, were evaluated entirely by the plain path. */
 typedef struct {
-  int64_t tested, culled, evaluated, rechecked, kept;
+  int64_t tested, culled, evaluated, rechecked, kept, audited, violations, fallback_chunks;
 } epb_window_stats;
 
 /* Bind an electron Hamiltonian H(R) (c128, (nw^2, nr), caller-owned; irvec int64 3 x nr, host)
