@@ -83,18 +83,27 @@ __device__ __forceinline__ int sturm_count(const T* d, const T* e2, int n, T sig
   return c;
 }
 
-// Reduce the matrix held row-wise in (ar, ai) to tridiagonal form; writes d, e2 to shared memory.
-template <typename T, int N>
-__device__ __forceinline__ void householder_tridiag(T (&ar)[N], T (&ai)[N], TriSmem<T>& s, int lane) {
-  T dk = 0, ek2 = 0;
+// Steps k = J0 .. min(J0 + 8, N - 1) - 1 of the reduction (see the file header). The step loop is not
+// unrolled (a fully unrolled 31-step reduction overflows the instruction cache); the inner loops run
+// over the compile-time range j = J0 .. N - 1 with the columns j <= k masked, and column k is picked
+// from registers by an 8-way select.
+template <typename T, int N, int J0>
+__device__ __forceinline__ void householder_phase(T (&ar)[N], T (&ai)[N], TriSmem<T>& s, int lane, T& dk, T& ek2) {
+  constexpr int KEND = (J0 + 8 < N - 1) ? J0 + 8 : N - 1;
+#pragma unroll 1
+  for (int k = J0; k < KEND; ++k) {
+    // column k below the diagonal: x_i = A[i][k], i > k (row `lane`, column k)
+    T xr = 0, xi = 0;
 #pragma unroll
-  for (int k = 0; k < N - 1; ++k) {
-    if (lane == k) dk = ar[k];
-    // column k below the diagonal: x_i = A[i][k], i > k
-    const T xr = ar[k], xi = ai[k];
+    for (int j = J0; j < J0 + 8 && j < N; ++j)
+      if (j == k) {
+        xr = ar[j];
+        xi = ai[j];
+      }
+    if (lane == k) dk = xr;
     const T xn2 = warp_sum(lane > k ? xr * xr + xi * xi : T(0));
     if (lane == k) ek2 = xn2;
-    if (k == N - 2) break;  // last off-diagonal: no reflection left to apply
+    if (k == N - 2) break;      // last off-diagonal: no reflection left to apply
     if (xn2 == T(0)) continue;  // warp-uniform: column already reduced
     const T x1r = __shfl_sync(0xffffffffu, xr, k + 1), x1i = __shfl_sync(0xffffffffu, xi, k + 1);
     const T xn = sqrt(xn2), a1 = sqrt(x1r * x1r + x1i * x1i);
@@ -109,12 +118,12 @@ __device__ __forceinline__ void householder_tridiag(T (&ar)[N], T (&ai)[N], TriS
       ur = a1 > T(0) ? x1r * f : xn;
       ui = a1 > T(0) ? x1i * f : T(0);
     }
-    s.u[lane] = mk2(ur, ui);
+    s.u[lane] = mk2(ur, ui);  // zero for lanes <= k
     __syncwarp();
-    // p_i = beta sum_{j>k} A[i][j] u_j (two interleaved partial sums for instruction-level parallelism)
+    // p_i = beta sum_{j>k} A[i][j] u_j (u_j = 0 for j <= k; two partial sums for ILP)
     T pr0 = 0, pi0 = 0, pr1 = 0, pi1 = 0;
 #pragma unroll
-    for (int j = k + 1; j < N; ++j) {
+    for (int j = J0 + 1; j < N; ++j) {
       const auto v = s.u[j];
       if ((j & 1) == 0) {
         pr0 = fma(ar[j], v.x, pr0);
@@ -140,16 +149,28 @@ __device__ __forceinline__ void householder_tridiag(T (&ar)[N], T (&ai)[N], TriS
     __syncwarp();
     if (lane > k) {
 #pragma unroll
-      for (int j = k + 1; j < N; ++j) {
-        const auto uj = s.u[j], wj = s.w[j];
-        const T ujr = uj.x, uji = uj.y, wjr = wj.x, wji = wj.y;
-        // A[i][j] -= u_i conj(w_j) + w_i conj(u_j)
-        ar[j] -= (ur * wjr + ui * wji) + (wr * ujr + wi * uji);
-        ai[j] -= (ui * wjr - ur * wji) + (wi * ujr - wr * uji);
+      for (int j = J0 + 1; j < N; ++j) {
+        if (j > k) {
+          const auto uj = s.u[j], wj = s.w[j];
+          // A[i][j] -= u_i conj(w_j) + w_i conj(u_j)
+          ar[j] -= (ur * wj.x + ui * wj.y) + (wr * uj.x + wi * uj.y);
+          ai[j] -= (ui * wj.x - ur * wj.y) + (wi * uj.x - wr * uj.y);
+        }
       }
     }
     __syncwarp();
   }
+}
+
+// Reduce the matrix held row-wise in (ar, ai) to tridiagonal form; writes d, e2 to shared memory.
+template <typename T, int N>
+__device__ __forceinline__ void householder_tridiag(T (&ar)[N], T (&ai)[N], TriSmem<T>& s, int lane) {
+  static_assert(N == 32, "the reduction is laid out in four phases of eight steps");
+  T dk = 0, ek2 = 0;
+  householder_phase<T, N, 0>(ar, ai, s, lane, dk, ek2);
+  householder_phase<T, N, 8>(ar, ai, s, lane, dk, ek2);
+  householder_phase<T, N, 16>(ar, ai, s, lane, dk, ek2);
+  householder_phase<T, N, 24>(ar, ai, s, lane, dk, ek2);
   if (lane == N - 1) dk = ar[N - 1];
   s.d[lane] = dk;
   s.e2[lane] = ek2;
