@@ -79,6 +79,7 @@ SIGNATURES = {
     "epb_mlp_predict": [P, P, P, I64, P],
     "epb_mlp_calibrate": [P, P, P, P, I64, D, P],
     "epb_mlp_set_inference": [P, I32],
+    "epb_bte_serta": [P, P, P, P, P, I64, P],
     "epb_mlp_inference_path": [P, C.POINTER(I32)],
 }
 
@@ -90,6 +91,13 @@ class WindowStats(C.Structure):
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
+class BteParams(C.Structure):
+    """epb_bte_params."""
+    _fields_ = [("ngrid", I64), ("wmin", D), ("wmax", D), ("mu", D), ("temperature", D), ("smearing", D),
+                ("omega_cutoff", D), ("spin_degeneracy", D), ("volume", D), ("lattice", D * 9), ("method", C.c_int32),
+                ("prec", C.c_int32), ("k_batch", I64)]
 
 
 class MlpTrainOpts(C.Structure):

@@ -316,6 +316,35 @@ EPB_API int epb_eph_pass(epb_ctx* ctx, epb_model* model, const double* xk, int64
                          int64_t nq, int prec, int64_t k_batch, int64_t sample_stride, double* ek_out,
                          double* omega_out, double* g2sum_out, double* g2_sample, int64_t* stats_host);
 
+/* ---- SERTA Boltzmann consumer -------------------------------------------------------------- */
+typedef struct {
+  int64_t ngrid;            /* k = q grid ngrid^3 (commensurate), k fastest (kpoints.jl:135-153)   */
+  double wmin, wmax;        /* energy window (Ry) of the initial and final electron states         */
+  double mu, temperature;   /* chemical potential, temperature (Ry)                                */
+  double smearing;          /* Gaussian width (Ry)                                                */
+  double omega_cutoff;      /* phonon modes below it are skipped (Ry; constants.jl:5)               */
+  double spin_degeneracy;
+  double volume;            /* unit-cell volume                                                  */
+  double lattice[9];        /* column-major, column d = lattice vector a_d (Cartesian)            */
+  int32_t method;           /* occupation method 1..6 (bte_scattering_core.jl:9-84)               */
+  int32_t prec;             /* EPB_PREC_FP64                                                     */
+  int64_t k_batch;          /* kept k per batch (<= 256)                                         */
+} epb_bte_params;
+
+/* SERTA conductivity over commensurate k = q grids: electron states, windows and phonons on the grid,
+   band velocities (Hellmann-Feynman with dH/dk from the Fourier sum), |g|^2 of every in-window
+   (n at k, m at k+q, nu) triple in the q convention, out-scattering rates S_out[n, k] from the
+   occupation increments with Gaussian smearing and weight 1/N per final state, and
+   sigma_ab = (spin / V) sum_{k, n in window} (1/N) (-f'(e - mu) / S_out) v_a v_b (host, 9 values,
+   column-major). inv_tau (device, capacity inv_tau_cap, may be NULL with capacity 0): S_out of the
+   window states, kept k ascending then band ascending. stats_host (4 int64, may be NULL): kept k,
+   window states, (k, q) pairs with a non-empty k+q window, widest window. Synchronises.
+   Replaces: the batched k / k+q loop with the Boltzmann calculator
+   (src/calculator/run_eph_over_k_and_kq.jl:792-892, src/boltzmann/boltzmann_calculator.jl:336-362)
+   and the SERTA conductivity of solve_electron_bte (src/boltzmann/electron_lbte.jl:43-49,153-185). */
+EPB_API int epb_bte_serta(epb_ctx* ctx, epb_model* model, const epb_bte_params* params, double* sigma_host,
+                          double* inv_tau, int64_t inv_tau_cap, int64_t* stats_host);
+
 #ifdef __cplusplus
 }
 #endif
