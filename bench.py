@@ -16,6 +16,10 @@ window), whose kept sets must be identical.
 `--workload bands` measures config 1 (nw = 8, R grid 7^3, 4096 random k): H(k) by the Fourier sum and
 all eigenvalues + eigenvectors, FP64 and mixed (eigenvalue deviation of the mixed path reported).
 
+`--workload bte` measures the SERTA consumer (config 5: the config-2 model on 64^3 k = q grids,
+window E_F -/+ 0.3 eV around the median of band 8, T = 300 K, Gaussian 10 meV, method 5):
+in-window (k, k+q) pairs per second and the conductivity tensor.
+
 `--workload eigh` measures the uneven batched eigensolve (config 3: 1,000,000 Hermitian matrices,
 n uniform in {4, 8, ..., 96}, 5 % with planted 2-4-fold clusters spaced 1e-10, eigenvalues and
 eigenvectors, FP32 solve + FP64 refinement): matrices per second.
@@ -62,7 +66,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-nk", type=int, default=16)
     ap.add_argument("--cpu-nq", type=int, default=1024)
-    ap.add_argument("--workload", default="pass", choices=["pass", "filter", "eigh", "bands"])
+    ap.add_argument("--workload", default="pass", choices=["pass", "filter", "eigh", "bands", "bte"])
     ap.add_argument("--count", type=int, default=1_000_000, help="eigh workload: matrices per batch")
     ap.add_argument("--grid", type=int, default=96, help="filter workload: k grid per axis")
     ap.add_argument("--decay", type=float, default=1.5, help="filter workload: H(R) decay length")
@@ -543,6 +547,71 @@ def run_filter(args):
 
 
 # ---------------------------------------------------------------------------------------------
+BTE_METRIC = "SERTA in-window (k, k+q) pairs/s, config-2 model on 64^3 k = q grids (sigma vs FP64)"
+
+
+def run_bte(args):
+    import torch
+
+    from epb200 import bte, pipeline, synth
+    from oracle import bte_oracle as BO
+    from oracle import epb_oracle as O
+
+    torch.cuda.set_device(0)
+    ng = args.grid if args.grid != 96 else 64
+    m = build_model_host_small()
+    ep_dev = synth.epmat_el_device(SEED, NW, 3 * NATOM, m.el_ham.irvec, synth.irvec_box(N_PH))
+    m.epmat = synth.device_epmat_object(ep_dev, m.el_ham.irvec, synth.irvec_box(N_PH))
+    dm = pipeline.DeviceModel(m, mixed=True)
+    # E_F = median of band 8 over the grid (host, from the grid energies of a coarse sample of the grid)
+    xs, _ = BO.grid_points(16)
+    hk = O.fourier_batched(m.el_ham.op_r, NW * NW, m.el_ham.irvec, xs)
+    Es = O.eigvals_batched(np.asfortranarray(hk.reshape(NW, NW, -1, order="F")))
+    ef = float(np.median(Es[NW // 2 - 1]))
+    half = 0.3 * synth.UNIT_EV
+    T, eta = 300 * O.UNIT_K, 0.01 * synth.UNIT_EV
+    kw = dict(method=5, k_batch=32, prec=pipeline.PREC_MIXED if args.prec != "fp64" else pipeline.PREC_FP64)
+    for _ in range(args.warmup):
+        sig, st, _ = bte.serta(dm, ng, ef - half, ef + half, ef, T, eta, **kw)
+    torch.cuda.synchronize()
+    clk = clocks_start()
+    l0 = dm.ctx.launch_count()
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(args.steps):
+        sig, st, _ = bte.serta(dm, ng, ef - half, ef + half, ef, T, eta, **kw)
+    e1.record(s)
+    torch.cuda.synchronize()
+    clocks = clocks_stop(clk, 0)
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = dm.ctx.launch_count() - l0
+    dm.ctx.profile(True)
+    bte.serta(dm, ng, ef - half, ef + half, ef, T, eta, **kw)
+    torch.cuda.synchronize()
+    prof = dm.ctx.profile_read(reset=True)
+    dm.ctx.profile(False)
+    profile = {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in prof.items() if v[1]}
+    # the FP64 plain path on the same inputs: time and conductivity for the comparison
+    kw64 = dict(kw, prec=pipeline.PREC_FP64)
+    e0.record(s)
+    sig64, st64, _ = bte.serta(dm, ng, ef - half, ef + half, ef, T, eta, **kw64)
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms64 = e0.elapsed_time(e1)
+    rel = float(np.max(np.abs(sig - sig64)) / np.abs(sig64).max())
+    line = {"metric": BTE_METRIC, "value": st["pairs"] / (ms * 1e-3), "unit": "pairs/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3/f64" if kw["prec"] == 1 else "f64",
+            "data": "synthetic (seeded config-2 model; g(Re,Rp) generated on the device)",
+            "config": {"workload": f"config5 SERTA: nw=16, nm=12, Re 9^3, Rp 5^3, {ng}^3 k = q grids, window E_F -/+ 0.3 eV, "
+                                   "T = 300 K, Gaussian 10 meV, method 5", "e_fermi_ry": ef, **st},
+            "sigma": sig.tolist(), "sigma_fp64": sig64.tolist(), "sigma_max_rel_dev_vs_fp64": rel,
+            "fp64_ms_per_step": round(ms64, 3), "speedup_vs_fp64": round(ms64 / ms, 3), "roofline": None, "cpu_baseline": None, "gpu_launches": launches,
+            "clocks": clocks, "impl": "epb", "profile_one_step": profile}
+    print(json.dumps(line), flush=True)
+
+
 BANDS_METRIC = "k-points/s: H(k) Fourier + eigenvalues and eigenvectors, nw=8 tight-binding (config 1)"
 
 
@@ -759,6 +828,8 @@ if __name__ == "__main__":
         run_eigh(a)
     elif a.workload == "bands":
         run_bands(a)
+    elif a.workload == "bte":
+        run_bte(a)
     elif a.workload == "filter":
         if a.nq == NQ:
             a.nq = 8192

@@ -13,7 +13,8 @@
 //  2. phonons on the same grid (D(q) Fourier sum, mass-scaled eigensolve);
 //  3. band velocities of the kept states: dH/dk_a = sum_R i R_cart,a H(R) e^{2 pi i x.R} (three
 //     Fourier sums), v_n = Re u_n^H dH_a u_n;
-//  4. per batch of kept k: g(k, Rp) for a fixed band slice of width W containing the window
+//  4. per batch of kept k: g(k, Rp) (FP64 Fourier sum, or the split-BF16 tensor-core GEMM in the mixed
+//     mode, the largest contraction of the consumer) for a fixed band slice of width W containing the window
 //     (offset o_k = min(band_min - 1, nw - W)); the pairs (k, q) whose k+q window is non-empty
 //     (grid-hash flags + compaction, one count read-back per batch); per k: q phases, g(k,q) =
 //     g(k,Rp) P (ZGEMM), rotations by u_{k+q} (its band slice) and u_ph with |g|^2 / (2 omega), and
@@ -38,6 +39,9 @@ int zgemm_nn(epb_ctx* ctx, const double2* A, int64_t lda, const double2* B, int6
              int64_t M, int64_t N, int64_t K);
 int eph_rotations_f64(epb_ctx* ctx, const double2* g, int64_t ldg, int nw, int nbk, int nm, int64_t nq,
                       const double2* ukq, int nbkq, const double2* uph, const double* omega, double2* ep, double* g2);
+int mixed_rr_to_kR(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double2* uk, int nband,
+                   double2* out);
+int split_gemm_check(epb_ctx* ctx);
 
 static unsigned gsz(epb_ctx* ctx, int64_t total) {
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(total, 256), (int64_t)ctx->sm_count * 16));
@@ -370,7 +374,10 @@ int epb_bte_serta(epb_ctx* ctx, epb_model* m, const epb_bte_params* prm, double*
   EPB_CHECK_ARG(ng >= 1 && ng <= 128, "epb_bte_serta: ngrid %lld outside 1..128", (long long)ng);
   EPB_CHECK_ARG(prm->temperature > 0 && prm->smearing > 0 && prm->volume > 0, "epb_bte_serta: bad physical parameters");
   EPB_CHECK_ARG(prm->method >= 1 && prm->method <= 6, "epb_bte_serta: method %d outside 1..6", prm->method);
-  EPB_CHECK_ARG(prm->prec == EPB_PREC_FP64, "epb_bte_serta: only EPB_PREC_FP64 is implemented");
+  EPB_CHECK_ARG(prm->prec == EPB_PREC_FP64 || prm->prec == EPB_PREC_MIXED, "epb_bte_serta: unknown precision %d",
+                prm->prec);
+  EPB_CHECK_ARG(prm->prec == EPB_PREC_FP64 || m->mixed,
+                "epb_bte_serta: EPB_PREC_MIXED needs a model created with the mixed operand planes");
   EPB_CHECK_ARG(inv_tau_cap == 0 || inv_tau, "epb_bte_serta: NULL inv_tau with a capacity");
   EPB_TRY(make_current(ctx));
   const int nw = (int)m->nw, nm = (int)m->nm;
@@ -513,8 +520,11 @@ int epb_bte_serta(epb_ctx* ctx, epb_model* m, const epb_bte_params* prm, double*
       EPB_LAUNCH_CHECK();
       bte_gather_uk_kernel<<<gsz(ctx, nkb * nw * W), 256, 0, ctx->stream>>>(U, keep, b0, nkb, bmin, nw, W, ukb);
       EPB_LAUNCH_CHECK();
-      EPB_TRY(epb_eph_RR_to_kR(ctx, (const double*)m->epmat, nw, nm, nr_ep, m->rs_el, xkb, nkb, (const double*)ukb, W,
-                               nullptr, (double*)kR, EPB_PREC_FP64));
+      if (prm->prec == EPB_PREC_MIXED)
+        EPB_TRY(mixed_rr_to_kR(ctx, m, xkb, nkb, ukb, W, kR));
+      else
+        EPB_TRY(epb_eph_RR_to_kR(ctx, (const double*)m->epmat, nw, nm, nr_ep, m->rs_el, xkb, nkb, (const double*)ukb, W,
+                                 nullptr, (double*)kR, EPB_PREC_FP64));
       // pairs (kk, q) with a non-empty window at k+q, ascending
       const int64_t nf = nkb * N, nb = cdiv(nf, 1024);
       bte_pair_flags_kernel<<<gsz(ctx, nf), 256, 0, ctx->stream>>>(keep, b0, nkb, ng, bmin, pflag);
@@ -563,6 +573,7 @@ int epb_bte_serta(epb_ctx* ctx, epb_model* m, const epb_bte_params* prm, double*
       EPB_LAUNCH_CHECK();
     }
   }
+  if (prm->prec == EPB_PREC_MIXED) EPB_TRY(split_gemm_check(ctx));
   double sh[9];
   EPB_CUDA(cudaMemcpyAsync(sh, sig_d, 9 * 8, cudaMemcpyDeviceToHost, ctx->stream));
   EPB_CUDA(cudaStreamSynchronize(ctx->stream));

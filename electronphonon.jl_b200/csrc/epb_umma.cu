@@ -23,6 +23,8 @@
 //   warps 2-5   epilogue: tcgen05.ld of the accumulator, FP32 stores to C
 // Every wait is bounded (clock64 budget); on timeout the kernel raises an error flag, drains its
 // own copies and MMAs, frees TMEM and returns (EPB_ERR_TIMEOUT on the host).
+#include <algorithm>
+
 #include "epb_common.cuh"
 
 #include "epb_umma.cuh"
@@ -730,6 +732,67 @@ void mixed_model_free(epb_model* m) {
   if (mm->mem) cudaFree(mm->mem);
   delete mm;
   m->mixed = nullptr;
+}
+
+// g(k, Rp) rotated on the k leg from the tensor-core Fourier output (complex64, "el" row order, one
+// column of nd = nw^2 nm nr_ep per k): out[iw, n, mp, k] = sum_jw g[iw, jw, mp, k] uk[jw, n, k], FP64.
+__global__ void rr_rotate_c64_kernel(const float2* __restrict__ g, const double2* __restrict__ uk,
+                                     double2* __restrict__ out, int nw, int nband, int nm, int nr_ep, int64_t kc) {
+  const int64_t M = (int64_t)nm * nr_ep;
+  const int64_t total = (int64_t)nw * nband * M * kc;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (int64_t)gridDim.x * blockDim.x) {
+    const int iw = (int)(idx % nw);
+    int64_t r = idx / nw;
+    const int n = (int)(r % nband);
+    r /= nband;
+    const int64_t mp = r % M, k = r / M;
+    const float2* gb = g + ((k * M + mp) * nw) * nw;
+    const double2* ub = uk + (k * nband + n) * nw;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int jw = 0; jw < nw; ++jw) {
+      const float2 v = gb[iw + jw * nw];
+      cfma(acc, make_double2(v.x, v.y), ub[jw]);
+    }
+    out[idx] = acc;
+  }
+}
+
+// get_eph_RR_to_kR on the tensor cores: g(k, Rp) = sum_Re e^{2 pi i k.Re} g(Re, Rp) as a split-BF16x3 GEMM
+// against the model's operand planes (epb_model_create with the mixed flag), then the k-leg rotation
+// by uk (nw x nband x nk, FP64) into out (nw nband nm nr_ep x nk, c128). Stream-ordered; the GEMM's
+// timeout flag is left for the caller's split_gemm_check.
+int mixed_rr_to_kR(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double2* uk, int nband,
+                   double2* out) {
+  MixedModel* mm = (MixedModel*)m->mixed;
+  EPB_CHECK_ARG(mm, "mixed RR->kR: the model was created without the mixed operand planes");
+  if (nk == 0) return EPB_OK;
+  const int64_t nw = m->nw, nm = m->nm, nd_ep = nw * nw * nm * m->nr_ep;
+  const int64_t KC_el = kchunks(m->nr_el);
+  int64_t kc = ((int64_t)768 << 20) / (8 * nd_ep);
+  kc = std::max<int64_t>(1, std::min<int64_t>(kc, 256));
+  kc = std::min(kc, nk);
+  const int64_t bbytes = MX_NPL * plane_bytes_for(round_up(kc, MX_NT), KC_el);
+  const int64_t cbytes = 8 * nd_ep * kc;
+  void* ws = nullptr;
+  EPB_TRY(ws_get(ctx, EPB_WS_PASS4, bbytes + cbytes + 2048, &ws));
+  uint8_t* base = (uint8_t*)(((uintptr_t)ws + 1023) & ~uintptr_t(1023));
+  float* C0 = (float*)(base + ((bbytes + 1023) & ~int64_t(1023)));
+  const int64_t outk = nw * nband * nm * m->nr_ep;
+  for (int64_t k0 = 0; k0 < nk; k0 += kc) {
+    const int64_t kn = std::min(kc, nk - k0);
+    Planes Bk;
+    EPB_TRY(pack_b_phase(ctx, m->rs_el, xk + 3 * k0, nullptr, 1, kn, Bk, base));
+    EPB_TRY(split_gemm(ctx, EPB_PROF_UMMA_RR, mm->EP, Bk, mm->EP.rows_pad / 128, 1, 2 * nd_ep, kn, false, C0, 0,
+                       2 * nd_ep));
+    const int64_t total = nw * nband * nm * m->nr_ep * kn;
+    prof_begin(ctx, EPB_PROF_RR_ROT);
+    rr_rotate_c64_kernel<<<grid_for(ctx, total), 256, 0, ctx->stream>>>((const float2*)C0, uk + k0 * nw * nband,
+                                                                        out + k0 * outk, (int)nw, nband, (int)nm,
+                                                                        (int)m->nr_ep, kn);
+    prof_end(ctx);
+    EPB_LAUNCH_CHECK();
+  }
+  return EPB_OK;
 }
 
 // RR->kR rotation on the k leg fused with the packing of the kR->kq operand:

@@ -327,7 +327,8 @@ typedef struct {
   double volume;            /* unit-cell volume                                                  */
   double lattice[9];        /* column-major, column d = lattice vector a_d (Cartesian)            */
   int32_t method;           /* occupation method 1..6 (bte_scattering_core.jl:9-84)               */
-  int32_t prec;             /* EPB_PREC_FP64                                                     */
+  int32_t prec;             /* EPB_PREC_FP64, or EPB_PREC_MIXED: g(k, Rp) on the tensor cores (model
+                               created with the mixed flag), everything else FP64                  */
   int64_t k_batch;          /* kept k per batch (<= 256)                                         */
 } epb_bte_params;
 

@@ -42,3 +42,23 @@ def test_gpu_serta_vs_oracle(gpu_lib, nw, natom, ng, method):
     assert st["states"] == len(itau_ref)
     np.testing.assert_allclose(itau, itau_ref, rtol=1e-9, atol=1e-12 * np.abs(itau_ref).max())
     np.testing.assert_allclose(sig, ref, rtol=1e-9, atol=1e-9 * np.abs(ref).max())
+
+
+@pytest.mark.gpu
+def test_gpu_serta_mixed_vs_fp64(gpu_lib):
+    """Mixed mode (g(k, Rp) on the tensor cores): conductivity within 1e-4 of the FP64 path, the
+    tolerance the north star states for sigma."""
+    from epb200 import bte, pipeline
+
+    m = synth.make_model(8, 2, 2, 1, seed=61)
+    x, _ = BO.grid_points(5)
+    E = O.eigvals_batched(np.asfortranarray(
+        O.fourier_batched(m.el_ham.op_r, 64, m.el_ham.irvec, x).reshape(8, 8, -1, order="F")))
+    ef = float(np.median(E[4]))
+    dm = pipeline.DeviceModel(m, mixed=True)
+    args = (dm, 5, ef - 0.8, ef + 0.8, ef, 0.08, 0.06)
+    s64, st64, it64 = bte.serta(*args, prec=bte.PREC_FP64, want_inv_tau=True)
+    smx, stmx, itmx = bte.serta(*args, prec=1, want_inv_tau=True)
+    assert st64 == stmx
+    assert np.max(np.abs(smx - s64)) <= 1e-4 * np.abs(s64).max()
+    np.testing.assert_allclose(itmx, it64, rtol=1e-4, atol=1e-6 * np.abs(it64).max())
