@@ -179,6 +179,48 @@ def measure_fp64_peak(torch):
     return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
 
 
+def measure_fp32_simt_peak(torch):
+    """FP32 CUDA-core throughput (TFLOP/s): cuBLAS SGEMM 8192^3 with TF32 disabled (FFMA path)."""
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        a = torch.randn(8192, 8192, dtype=torch.float32, device="cuda")
+        b = torch.randn(8192, 8192, dtype=torch.float32, device="cuda")
+        for _ in range(2):
+            a @ b
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        best = 1e9
+        for _ in range(3):
+            e0.record()
+            a @ b
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        del a, b
+        return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+
+
+# Algorithmic HBM bytes and FP32 flops per launch of the CUDA-core families of the mixed pass (one
+# launch covers one inner batch of nkb k x nq q, i.e. nkb * nq matrices / pairs):
+#   eigh (FP32 Jacobi): packed FP32 H (nw^2 floats) in, FP32 eigenvectors (nw^2 complex64) out;
+#       ~40 n^3 FP32 flops per sweep-equivalent x 6 sweeps;
+#   eigh_refine: H (nw^2 floats) + FP32 vectors in, FP32 vectors out; FP64 work;
+#   rotation: g(k,q) block (2 nw^2 nm floats) + U (nw^2 complex64) in; 8 (nw^3 nm + nw^2 nm^2) flops.
+def family_bytes_flops(name, args, nkb):
+    nw2, nm = NW * NW, 3 * NATOM
+    units = nkb * args.nq
+    if name == "eigh":
+        return units * (4 * nw2 + 8 * nw2), units * 6 * 40.0 * NW ** 3
+    if name == "eigh_refine":
+        return units * (4 * nw2 + 8 * nw2 + 8 * nw2), None
+    if name == "rotation":
+        return units * (8 * nw2 * nm + 8 * nw2), units * 8.0 * (NW ** 3 * nm + nw2 * nm * nm)
+    return None, None
+
+
 # Algorithmic flops per launch of each kernel family (8 real flops per complex MAC).
 def family_flops(name, args, nkb):
     nw2, nm, nr_el, nr_ep = NW * NW, 3 * NATOM, (2 * N_EL + 1) ** 3, (2 * N_PH + 1) ** 3
@@ -270,6 +312,32 @@ def run_epb(args):
     profile = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / tot_ms, 4)}
                for k, v in prof.items() if v[1]}
     roof = None
+    roof_compute = None
+    if flops is None and dom_cnt > 0:
+        # a CUDA-core family dominates: HBM roofline from its algorithmic bytes (the schema's bounds are
+        # HBM or tensor), plus its FP32 compute roofline against a live FFMA (SGEMM) measurement
+        nbytes, nflops = family_bytes_flops(dom_name, args, args.k_batch)
+        if nbytes is not None:
+            avg_s = dom_ms / dom_cnt * 1e-3
+            ach = nbytes / avg_s / 1e9
+            traffic = None
+            tp = os.path.join(ROOT, "profiles", "traffic.json")
+            if os.path.exists(tp):
+                with open(tp) as fh:
+                    traffic = json.load(fh).get(dom_name)
+            roof = {"bound": "hbm", "kernel": dom_name, "achieved": round(ach, 2), "peak": peaks["hbm_gbs"],
+                    "unit": "GB/s", "frac": round(ach / peaks["hbm_gbs"], 5), "traffic": traffic,
+                    "peak_source": f"{peak_src} hbm copy", "launch_ms": round(dom_ms / dom_cnt, 4),
+                    "launches_per_pass": dom_cnt, "algorithmic_bytes_per_launch": nbytes,
+                    "note": "the family is FP32 CUDA-core compute bound; see roofline_compute",
+                    "share_of_pass": {k: round(v[0] / tot_ms, 4) for k, v in prof.items() if v[1]}}
+            if nflops is not None:
+                p32 = measure_fp32_simt_peak(torch)
+                a32 = nflops / avg_s / 1e12
+                roof_compute = {"bound": "fp32 cuda cores", "kernel": dom_name, "achieved": round(a32, 2),
+                                "peak": round(p32, 2), "unit": "TFLOP/s", "frac": round(a32 / p32, 4),
+                                "peak_source": "measured live: cuBLAS SGEMM 8192^3, TF32 off",
+                                "algorithmic_flops_per_launch": nflops}
     if flops is not None and dom_cnt > 0:
         avg_s = dom_ms / dom_cnt * 1e-3
         if dom_name.startswith("umma"):
@@ -328,7 +396,8 @@ def run_epb(args):
             "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16x3/f32/f64" if prec == pipeline.PREC_MIXED else "f64",
             "data": "synthetic (seeded generator; random-init Wannier model of the config-2 shape)",
-            "config": config_dict(args, prec_name), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "config": config_dict(args, prec_name), "roofline": roof, "roofline_compute": roof_compute,
+            "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": clocks, "impl": "epb", "profile_one_pass": profile}
     if rank == 0:
         print(json.dumps(line), flush=True)
