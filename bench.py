@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--prec", default="auto", choices=["auto", "mixed", "fp64"])
     ap.add_argument("--nk", type=int, default=NK)
     ap.add_argument("--nq", type=int, default=NQ)
-    ap.add_argument("--k-batch", type=int, default=16)
+    ap.add_argument("--k-batch", type=int, default=0, help="inner k batch of the pass; 0 = autotuned")
     ap.add_argument("--sample-stride", type=int, default=4096)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -100,7 +100,7 @@ def config_dict(args, prec_name):
                         f"Re {2 * N_EL + 1}^3, Rp {2 * N_PH + 1}^3, {args.nk} random k x {args.nq} random q",
             "nk": args.nk, "nq": args.nq, "nw": NW, "nmodes": 3 * NATOM, "nr_el": (2 * N_EL + 1) ** 3,
             "nr_ep": (2 * N_PH + 1) ** 3, "window": "all bands", "precision": prec_name,
-            "k_batch": args.k_batch,
+            "k_batch": args.k_batch if args.k_batch > 0 else "autotuned",
             "l2": "inputs larger than L2 (g(Re,Rp) is 4.48 GB and is re-read every pass)",
             "parallelism": f"dp{args.gpus} (k sharded per rank, weak)"}
 
@@ -307,7 +307,8 @@ def run_epb(args):
     peaks, peak_src = measured_peaks()
     dom = max(prof.items(), key=lambda kv: kv[1][0])
     dom_name, (dom_ms, dom_cnt) = dom
-    flops = family_flops(dom_name, args, args.k_batch)
+    kb_used = out_holder[0].k_batch or args.k_batch
+    flops = family_flops(dom_name, args, kb_used)
     tot_ms = sum(v[0] for v in prof.values())
     profile = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / tot_ms, 4)}
                for k, v in prof.items() if v[1]}
@@ -316,7 +317,7 @@ def run_epb(args):
     if flops is None and dom_cnt > 0:
         # a CUDA-core family dominates: HBM roofline from its algorithmic bytes (the schema's bounds are
         # HBM or tensor), plus its FP32 compute roofline against a live FFMA (SGEMM) measurement
-        nbytes, nflops = family_bytes_flops(dom_name, args, args.k_batch)
+        nbytes, nflops = family_bytes_flops(dom_name, args, kb_used)
         if nbytes is not None:
             avg_s = dom_ms / dom_cnt * 1e-3
             ach = nbytes / avg_s / 1e9
@@ -396,7 +397,8 @@ def run_epb(args):
             "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16x3/f32/f64" if prec == pipeline.PREC_MIXED else "f64",
             "data": "synthetic (seeded generator; random-init Wannier model of the config-2 shape)",
-            "config": config_dict(args, prec_name), "roofline": roof, "roofline_compute": roof_compute,
+            "config": dict(config_dict(args, prec_name), k_batch_used=kb_used), "roofline": roof,
+            "roofline_compute": roof_compute,
             "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": clocks, "impl": "epb", "profile_one_pass": profile}
     if rank == 0:

@@ -126,6 +126,8 @@ struct epb_ctx {
   std::vector<epb_prof_rec> prof;  // event pairs recorded while profiling
   size_t prof_used = 0;
   double prof_ms[EPB_PROF_N] = {};
+  // autotuner results: shape key -> chosen parameter (epb_eph_pass inner k batch)
+  std::vector<std::pair<std::string, int64_t>> tuned;
   int64_t prof_cnt[EPB_PROF_N] = {};
 };
 

@@ -10,6 +10,7 @@
 // The 5e10 g2 values of a full pass are never materialised: the rotation kernel consumes each
 // (k, q) block in place, accumulating g2sum[nu, k] = sum_{m, n, q} g2 and writing the full block
 // only for the sampled q (q % sample_stride == 0), which is what the parity checks read.
+#include <algorithm>
 #include <vector>
 
 #include "epb_common.cuh"
@@ -158,12 +159,82 @@ int epb_model_destroy(epb_model* m) {
   return EPB_OK;
 }
 
+static int eph_pass_run(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double* xq, int64_t nq,
+                        int prec, int64_t k_batch, int64_t sample_stride, double* ek_out, double* omega_out,
+                        double* g2sum_out, double* g2_sample, int64_t* stats_host);
+
+// Autotuner of the pass's inner k batch (the k+q eigensolve / kR->kq / rotation batch): times each
+// candidate on the first min(nk, 64) k against the caller's q list (CUDA events on the context stream,
+// one untimed run first), keeps the fastest per (nw, nm, nq, prec) in the context. The trial passes
+// write the caller's outputs for those k, which the real pass then rewrites.
+static int tune_k_batch(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double* xq, int64_t nq, int prec,
+                        double* ek_out, double* omega_out, double* g2sum_out, int64_t* chosen) {
+  char key[128];
+  snprintf(key, sizeof(key), "pass_kb/%lld/%lld/%lld/%d", (long long)m->nw, (long long)m->nm, (long long)nq, prec);
+  for (auto& kv : ctx->tuned)
+    if (kv.first == key) {
+      *chosen = kv.second;
+      return EPB_OK;
+    }
+  const int64_t ns = std::min<int64_t>(nk, 64);
+  const int64_t cands[4] = {4, 8, 16, 32};
+  cudaEvent_t e0, e1;
+  EPB_CUDA(cudaEventCreate(&e0));
+  EPB_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int64_t pick = 16;
+  for (int64_t c : cands) {
+    if (c > ns && c != cands[0]) continue;
+    int st = eph_pass_run(ctx, m, xk, ns, xq, nq, prec, c, 1, ek_out, omega_out, g2sum_out, nullptr, nullptr);
+    if (st == EPB_OK) {
+      cudaEventRecord(e0, ctx->stream);
+      st = eph_pass_run(ctx, m, xk, ns, xq, nq, prec, c, 1, ek_out, omega_out, g2sum_out, nullptr, nullptr);
+      cudaEventRecord(e1, ctx->stream);
+    }
+    if (st == EPB_ERR_OOM) {  // a larger batch does not fit: the smaller ones stand
+      clear_error();
+      break;
+    }
+    if (st != EPB_OK) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return st;
+    }
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) {
+      best = ms;
+      pick = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ctx->tuned.emplace_back(key, pick);
+  *chosen = pick;
+  return EPB_OK;
+}
+
 int epb_eph_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double* xq, int64_t nq,
                  int prec, int64_t k_batch, int64_t sample_stride, double* ek_out, double* omega_out,
                  double* g2sum_out, double* g2_sample, int64_t* stats_host) {
   clear_error();
   EPB_CHECK_ARG(ctx && m && xk && xq && ek_out && omega_out && g2sum_out, "epb_eph_pass: NULL argument");
-  EPB_CHECK_ARG(nk >= 1 && nq >= 1 && k_batch >= 1, "epb_eph_pass: bad sizes");
+  EPB_CHECK_ARG(nk >= 1 && nq >= 1, "epb_eph_pass: bad sizes");
+  EPB_CHECK_ARG(prec == EPB_PREC_FP64 || prec == EPB_PREC_MIXED, "epb_eph_pass: bad prec");
+  EPB_CHECK_ARG(prec != EPB_PREC_MIXED || m->mixed, "epb_eph_pass: model was created without mixed planes");
+  EPB_TRY(make_current(ctx));
+  if (k_batch <= 0) EPB_TRY(tune_k_batch(ctx, m, xk, nk, xq, nq, prec, ek_out, omega_out, g2sum_out, &k_batch));
+  int st = eph_pass_run(ctx, m, xk, nk, xq, nq, prec, k_batch, sample_stride, ek_out, omega_out, g2sum_out, g2_sample,
+                        stats_host);
+  if (st == EPB_OK && stats_host) stats_host[1] = k_batch;
+  return st;
+}
+
+static int eph_pass_run(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double* xq, int64_t nq,
+                        int prec, int64_t k_batch, int64_t sample_stride, double* ek_out, double* omega_out,
+                        double* g2sum_out, double* g2_sample, int64_t* stats_host) {
+  EPB_CHECK_ARG(k_batch >= 1, "epb_eph_pass: bad k batch");
   EPB_CHECK_ARG(prec == EPB_PREC_FP64 || prec == EPB_PREC_MIXED, "epb_eph_pass: bad prec");
   EPB_CHECK_ARG(!g2_sample || sample_stride >= 1, "epb_eph_pass: sample_stride must be >= 1");
   EPB_CHECK_ARG(prec != EPB_PREC_MIXED || m->mixed, "epb_eph_pass: model was created without mixed planes");

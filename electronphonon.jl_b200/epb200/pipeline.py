@@ -26,6 +26,7 @@ class PassResult:
     g2_sample: object  # (nw, nw, nm, nsamp, nk) or None
     n_elements: int
     sample_stride: int
+    k_batch: int = 0  # inner k batch the library used (autotuned when not given)
 
 
 class DeviceModel:
@@ -73,7 +74,8 @@ class DeviceModel:
 def run_eph_over_k_and_q(dm: DeviceModel, xks, xqs, *, prec=PREC_FP64, k_batch=16, sample_stride=None,
                          out=None):
     """Full-band pass over the k list `xks` (3, nk) and the q list `xqs` (3, nq) (device float64 tensors
-    in Julia layout, or numpy arrays). Returns a PassResult with device tensors."""
+    in Julia layout, or numpy arrays). Returns a PassResult with device tensors. k_batch <= 0 (or None)
+    lets the library's autotuner choose the inner k batch (`PassResult.k_batch` reports it)."""
     import torch
 
     xk = xks if isinstance(xks, torch.Tensor) else jl(np.asfortranarray(xks, dtype=np.float64))
@@ -88,8 +90,9 @@ def run_eph_over_k_and_q(dm: DeviceModel, xks, xqs, *, prec=PREC_FP64, k_batch=1
             g2_sample=None if sample_stride is None else jl_empty((nw, nw, nm, nsamp, nk), torch.float64),
             n_elements=0, sample_stride=sample_stride or 0)
     stats = np.zeros(4, dtype=np.int64)
-    check(_lib.lib().epb_eph_pass(dm.ctx.h, dm.h, ptr(xk), nk, ptr(xq), nq, int(prec), int(k_batch),
+    check(_lib.lib().epb_eph_pass(dm.ctx.h, dm.h, ptr(xk), nk, ptr(xq), nq, int(prec), int(k_batch or 0),
                                   int(sample_stride or 1), ptr(out.ek), ptr(out.omega), ptr(out.g2sum),
                                   ptr(out.g2_sample), stats.ctypes.data))
     out.n_elements = int(stats[0])
+    out.k_batch = int(stats[1])
     return out

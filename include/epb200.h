@@ -308,8 +308,10 @@ EPB_API int epb_model_destroy(epb_model* model);
    phonons at q, g(k,q) = ukq^dagger g u_ph, g2 = |g|^2/(2 omega). Outputs: ek (nw x nk),
    omega (nm x nq), g2sum (nm x nk) = sum over bands and q of g2, and, if g2_sample != NULL, the full
    g2 block (nw x nw x nm) of every q with q % sample_stride == 0, laid out
-   (nw, nw, nm, nsamp, nk) with nsamp = ceil(nq / sample_stride). stats_host (4 int64, may be NULL):
-   [0] = g elements produced. Replaces: the per-(k, q) loop of run_eph_over_k_and_q
+   (nw, nw, nm, nsamp, nk) with nsamp = ceil(nq / sample_stride). k_batch: k per inner batch, or
+   <= 0 to let the autotuner pick it (candidates 4, 8, 16, 32 timed on the first 64 k with this q list,
+   cached in the context per (nw, nm, nq, prec)). stats_host (4 int64, may be NULL): [0] = g elements
+   produced, [1] = k batch used. Replaces: the per-(k, q) loop of run_eph_over_k_and_q
    (src/calculator/run_eph_over_k_and_q.jl:251-330) run the batched way of
    _loop_eph_over_k_and_kq_batched (src/calculator/run_eph_over_k_and_kq.jl:792-892). */
 EPB_API int epb_eph_pass(epb_ctx* ctx, epb_model* model, const double* xk, int64_t nk, const double* xq,

@@ -76,3 +76,21 @@ def test_gpu_pass_mixed(gpu_lib, nk, nq, kb):
     err = _block_rel_err(host(r.g2_sample), ref["g2_sample"])
     print("max per-block |g|^2 normwise rel err", err)
     assert err <= 1e-5
+
+
+@pytest.mark.gpu
+def test_gpu_pass_autotuned_k_batch(gpu_lib):
+    """k_batch <= 0: the library times the candidates, keeps one, and the pass equals an explicit run."""
+    from epb200 import pipeline
+    from epb200.batched import host
+
+    m = synth.config2_model(seed=43, n_el=2, n_ph=1, nw=16, natom=4)
+    xks = synth.random_kpoints(40, 7)
+    xqs = synth.random_kpoints(96, 8)
+    dm = pipeline.DeviceModel(m, mixed=True)
+    r = pipeline.run_eph_over_k_and_q(dm, xks, xqs, prec=pipeline.PREC_MIXED, k_batch=0)
+    assert r.k_batch in (4, 8, 16, 32)
+    r2 = pipeline.run_eph_over_k_and_q(dm, xks, xqs, prec=pipeline.PREC_MIXED, k_batch=0)
+    assert r2.k_batch == r.k_batch  # cached in the context
+    r3 = pipeline.run_eph_over_k_and_q(dm, xks, xqs, prec=pipeline.PREC_MIXED, k_batch=r.k_batch)
+    np.testing.assert_array_equal(host(r.g2sum), host(r3.g2sum))
