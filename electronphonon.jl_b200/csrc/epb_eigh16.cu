@@ -23,6 +23,7 @@
 // Pairs whose first-order coupling is not small (|S'_kl| > 0.1 |S'_ll - S'_kk|) are left to the
 // orthonormalisation (their vectors are accurate as a subspace, which is what gauge-invariant
 // quantities use). EPB_PREC_FP64 runs the sweeps in FP64 to tol = 1e-15 and skips the refinement.
+#include <algorithm>
 #include <type_traits>
 
 #include "epb_common.cuh"
@@ -355,6 +356,149 @@ __global__ void __launch_bounds__(128) eigh16_refine_kernel(Eigh16Args a) {
   }
 }
 
+// MODE 2, two lanes per column: the same refinement as eigh16_refine_kernel, one matrix per warp;
+// lane (l, h) holds rows 8h .. 8h + 7 of column l, partial column sums are combined with one shuffle
+// across the halves. Half the per-lane state of the one-lane-per-column form (fits in ~128
+// registers, twice the resident warps) and half the unrolled code.
+constexpr int RLD = E16 + 1;  // padded leading dimension of the shared H and V tiles
+
+__global__ void __launch_bounds__(128, 3) eigh16_refine2_kernel(Eigh16Args a) {
+  __shared__ double2 Hs[4][E16 * RLD];  // H[i][k] at i * RLD + k
+  __shared__ double2 Vs[4][E16 * RLD];  // V[i][k] at i * RLD + k
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int l = lane & 15, h = lane >> 4, r0 = 8 * h;
+  const int n = a.n;
+  double2* H = Hs[warp];
+  double2* V = Vs[warp];
+  for (int64_t b = (int64_t)blockIdx.x * 4 + warp; b - warp < a.batch; b += (int64_t)gridDim.x * 4) {
+    const bool live = b < a.batch;
+    double f2 = 0.0;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const double2 hv = live ? load_h(a, b, r0 + r, l, n) : make_double2(0.0, 0.0);
+      f2 += hv.x * hv.x + hv.y * hv.y;
+      H[(r0 + r) * RLD + l] = hv;
+    }
+    for (int o = 16; o > 0; o >>= 1) f2 += __shfl_xor_sync(0xffffffffu, f2, o);
+    const double sigma = f2 > 0.0 ? 1.1 * sqrt(f2) : 1.0;
+    double2 v[8];
+    {
+      const float2* vi = a.V32 + (live ? b : 0) * (int64_t)E16 * E16 + (int64_t)E16 * l + r0;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const float2 x = live ? vi[r] : make_float2(r0 + r == l ? 1.f : 0.f, 0.f);
+        v[r] = make_double2(x.x, x.y);
+      }
+    }
+    double lam = 0.0;
+    bool cluster = false;
+    for (int it = 0; it < a.refine; ++it) {
+#pragma unroll
+      for (int r = 0; r < 8; ++r) V[(r0 + r) * RLD + l] = v[r];
+      __syncwarp();
+      // w = H v on this lane's rows; d = Re v^H w, fll = |v|^2 - 1 (whole column)
+      double2 w[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) w[r] = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < E16; ++k) {
+        const double2 vk = V[k * RLD + l];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) cfma(w[r], H[(r0 + r) * RLD + k], vk);
+      }
+      double d = 0.0, fll = 0.0;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        d += v[r].x * w[r].x + v[r].y * w[r].y;
+        fll += v[r].x * v[r].x + v[r].y * v[r].y;
+      }
+      d += __shfl_xor_sync(0xffffffffu, d, 16);
+      fll += __shfl_xor_sync(0xffffffffu, fll, 16);
+      fll -= 1.0;
+      const double dp = d * (1.0 - fll);
+      double lam_corr = 0.0;
+      cluster = false;
+      double2 u[8];  // V t accumulated over k
+#pragma unroll
+      for (int r = 0; r < 8; ++r) u[r] = make_double2(0.0, 0.0);
+#pragma unroll 4
+      for (int k = 0; k < E16; ++k) {
+        const double dk = __shfl_sync(0xffffffffu, d, k);
+        const double dpk = __shfl_sync(0xffffffffu, dp, k);
+        double2 s = make_double2(0.0, 0.0), g = s;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const double2 vik = V[(r0 + r) * RLD + k];
+          cfma_conj(s, vik, w[r]);
+          cfma_conj(g, vik, v[r]);
+        }
+        s.x += __shfl_xor_sync(0xffffffffu, s.x, 16);
+        s.y += __shfl_xor_sync(0xffffffffu, s.y, 16);
+        g.x += __shfl_xor_sync(0xffffffffu, g.x, 16);
+        g.y += __shfl_xor_sync(0xffffffffu, g.y, 16);
+        double2 t;
+        if (k == l) {
+          t = make_double2(-0.5 * fll, 0.0);
+        } else {
+          const double2 sp = make_double2(s.x - 0.5 * g.x * (dk + d), s.y - 0.5 * g.y * (dk + d));
+          const double gap = dp - dpk;
+          const double asp = sqrt(sp.x * sp.x + sp.y * sp.y);
+          t = make_double2(-0.5 * g.x, -0.5 * g.y);
+          if (k < n && l < n) {
+            if (asp < 0.1 * fabs(gap)) {
+              t.x += sp.x / gap;
+              t.y += sp.y / gap;
+              lam_corr += asp * asp / gap;
+            } else if (asp > 1e-13 * sigma) {
+              cluster = true;
+            }
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < 8; ++r) cfma(u[r], V[(r0 + r) * RLD + k], t);
+      }
+#pragma unroll
+      for (int r = 0; r < 8; ++r) v[r] = make_double2(v[r].x + u[r].x, v[r].y + u[r].y);
+      lam = dp + lam_corr;
+      __syncwarp();
+    }
+    // both halves agree on lam and on the flag (each half saw the whole column sums)
+    const bool flagged = __ballot_sync(0xffffffffu, cluster && live) != 0;
+    if (a.flag_list && flagged && lane == 0) {
+      const int pos = atomicAdd(a.flag_count, 1);
+      a.flag_list[pos] = b;
+    }
+    if (!(a.flag_list && flagged)) {
+      int rank = 0;
+#pragma unroll
+      for (int k = 0; k < E16; ++k) {
+        const double lk = __shfl_sync(0xffffffffu, lam, k);
+        rank += (k < n) && (lk < lam || (lk == lam && k < l));
+      }
+      if (live && l < n) {
+        double ev = lam;
+        if (a.mass) ev = ev >= 0 ? sqrt(ev) : -sqrt(-ev);
+        if (a.E && h == 0) a.E[b * n + rank] = ev;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          const int i = r0 + r;
+          if (i < n) {
+            double2 o = v[r];
+            if (a.mass) {
+              const double sc = 1.0 / sqrt(a.mass[i]);
+              o.x *= sc;
+              o.y *= sc;
+            }
+            if (a.U32) a.U32[b * (int64_t)n * n + i + (int64_t)rank * n] = make_float2((float)o.x, (float)o.y);
+            if (a.U64) a.U64[b * (int64_t)n * n + i + (int64_t)rank * n] = o;
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
 int eigh16_launch(epb_ctx* ctx, Eigh16Args& a, bool mixed) {
   if (a.batch == 0) return EPB_OK;
   const int threads = 128;  // 8 matrices per block
@@ -382,7 +526,10 @@ int eigh16_launch(epb_ctx* ctx, Eigh16Args& a, bool mixed) {
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   prof_begin(ctx, EPB_PROF_REFINE);
-  eigh16_refine_kernel<<<grid_cap(8), threads, smem, ctx->stream>>>(a);
+  {
+    const int64_t blocks = std::min<int64_t>(cdiv(a.batch, 4), (int64_t)ctx->sm_count * 8);
+    eigh16_refine2_kernel<<<(unsigned)blocks, 128, 0, ctx->stream>>>(a);
+  }
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
