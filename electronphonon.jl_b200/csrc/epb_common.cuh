@@ -126,6 +126,7 @@ struct epb_ctx {
   std::vector<epb_prof_rec> prof;  // event pairs recorded while profiling
   size_t prof_used = 0;
   double prof_ms[EPB_PROF_N] = {};
+  bool graph_mode = false;  // epb_eph_pass: capture and replay as a CUDA graph (epb_set_graph_mode)
   // autotuner results: shape key -> chosen parameter (epb_eph_pass inner k batch)
   std::vector<std::pair<std::string, int64_t>> tuned;
   int64_t prof_cnt[EPB_PROF_N] = {};
@@ -141,6 +142,27 @@ struct epb_rset {
 };
 
 // A model's hot-path operators (caller-owned device memory) plus the library's derived data.
+// Arguments a captured pass was recorded with (a replay is valid only for the same buffers and sizes).
+struct PassKey {
+  const void* xk = nullptr;
+  int64_t nk = 0;
+  const void* xq = nullptr;
+  int64_t nq = 0;
+  int prec = -1;
+  int64_t k_batch = 0, stride = 0;
+  const void *ek = nullptr, *om = nullptr, *g2 = nullptr, *samp = nullptr;
+  bool operator==(const PassKey& o) const {
+    return xk == o.xk && nk == o.nk && xq == o.xq && nq == o.nq && prec == o.prec && k_batch == o.k_batch &&
+           stride == o.stride && ek == o.ek && om == o.om && g2 == o.g2 && samp == o.samp;
+  }
+};
+struct PassGraph {
+  PassKey key;
+  bool warm = false;                 // one eager run with `key` has sized the workspaces
+  cudaGraphExec_t exec = nullptr;    // the captured pass for `key`
+  int64_t launches = 0;              // kernels in the graph
+};
+
 struct epb_model {
   epb_ctx* ctx = nullptr;
   int64_t nw = 0, nm = 0, nr_el = 0, nr_ph = 0, nr_ep = 0;
@@ -153,6 +175,7 @@ struct epb_model {
   epb_rset* rs_ep = nullptr;
   // mixed-precision operand planes (owned), see epb_umma.cu
   void* mixed = nullptr;
+  PassGraph graph;  // graph mode of epb_eph_pass
 };
 
 namespace epb {

@@ -28,7 +28,8 @@ int eigh_async(epb_ctx* ctx, double2* A, int64_t n, int64_t batch, double* E, bo
 int eigh_check(epb_ctx* ctx);
 int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double* xq, int64_t nq,
                const double2* uph, const double* omega, double* ek_out, double* g2sum, double* g2_sample,
-               int64_t sample_stride, int64_t kbi_max);
+               int64_t sample_stride, int64_t kbi_max, bool defer_checks);
+int split_gemm_check(epb_ctx* ctx);
 int mixed_model_prepare(epb_ctx* ctx, epb_model* m);
 void mixed_model_free(epb_model* m);
 
@@ -155,13 +156,14 @@ int epb_model_destroy(epb_model* m) {
   epb_rset_destroy(m->rs_el);
   epb_rset_destroy(m->rs_ph);
   epb_rset_destroy(m->rs_ep);
+  if (m->graph.exec) cudaGraphExecDestroy(m->graph.exec);
   delete m;
   return EPB_OK;
 }
 
 static int eph_pass_run(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double* xq, int64_t nq,
                         int prec, int64_t k_batch, int64_t sample_stride, double* ek_out, double* omega_out,
-                        double* g2sum_out, double* g2_sample, int64_t* stats_host);
+                        double* g2sum_out, double* g2_sample, int64_t* stats_host, bool defer_checks = false);
 
 // Autotuner of the pass's inner k batch (the k+q eigensolve / kR->kq / rotation batch): times each
 // candidate on the first min(nk, 64) k against the caller's q list (CUDA events on the context stream,
@@ -225,15 +227,70 @@ int epb_eph_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const
   EPB_CHECK_ARG(prec != EPB_PREC_MIXED || m->mixed, "epb_eph_pass: model was created without mixed planes");
   EPB_TRY(make_current(ctx));
   if (k_batch <= 0) EPB_TRY(tune_k_batch(ctx, m, xk, nk, xq, nq, prec, ek_out, omega_out, g2sum_out, &k_batch));
-  int st = eph_pass_run(ctx, m, xk, nk, xq, nq, prec, k_batch, sample_stride, ek_out, omega_out, g2sum_out, g2_sample,
-                        stats_host);
-  if (st == EPB_OK && stats_host) stats_host[1] = k_batch;
-  return st;
+  const bool capturable = ctx->graph_mode && !ctx->prof_on && ctx->stream != nullptr && ctx->stream != cudaStreamLegacy;
+  if (!capturable) {
+    int st = eph_pass_run(ctx, m, xk, nk, xq, nq, prec, k_batch, sample_stride, ek_out, omega_out, g2sum_out, g2_sample,
+                          stats_host);
+    if (st == EPB_OK && stats_host) stats_host[1] = k_batch;
+    return st;
+  }
+  // Graph mode: the first call with these arguments runs eagerly (sizing every workspace), the
+  // second captures the pass (status checks left out of the graph), later ones replay it.
+  PassGraph& pg = m->graph;
+  const PassKey key{xk, nk, xq, nq, prec, k_batch, sample_stride, ek_out, omega_out, g2sum_out, g2_sample};
+  if (pg.exec && pg.key == key) {
+    EPB_CUDA(cudaGraphLaunch(pg.exec, ctx->stream));
+    ctx->launches += pg.launches;
+  } else if (pg.warm && pg.key == key) {
+    if (pg.exec) {
+      cudaGraphExecDestroy(pg.exec);
+      pg.exec = nullptr;
+    }
+    cudaGraph_t graph = nullptr;
+    const int64_t l0 = ctx->launches;
+    EPB_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int st = eph_pass_run(ctx, m, xk, nk, xq, nq, prec, k_batch, sample_stride, ek_out, omega_out, g2sum_out, g2_sample,
+                          nullptr, true);
+    cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+    pg.launches = ctx->launches - l0;
+    ctx->launches = l0;
+    if (st != EPB_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+    }
+    EPB_CUDA(ce);
+    ce = cudaGraphInstantiate(&pg.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    EPB_CUDA(ce);
+    EPB_CUDA(cudaGraphLaunch(pg.exec, ctx->stream));
+    ctx->launches += pg.launches;
+  } else {
+    int st = eph_pass_run(ctx, m, xk, nk, xq, nq, prec, k_batch, sample_stride, ek_out, omega_out, g2sum_out, g2_sample,
+                          nullptr);
+    if (st != EPB_OK) return st;
+    pg.key = key;
+    pg.warm = true;
+  }
+  EPB_TRY(eigh_check(ctx));
+  if (prec == EPB_PREC_MIXED) EPB_TRY(split_gemm_check(ctx));
+  if (stats_host) {
+    stats_host[0] = nk * nq * m->nw * m->nw * m->nm;
+    stats_host[1] = k_batch;
+    stats_host[2] = stats_host[3] = 0;
+  }
+  return EPB_OK;
+}
+
+int epb_set_graph_mode(epb_ctx* ctx, int on) {
+  clear_error();
+  EPB_CHECK_ARG(ctx, "epb_set_graph_mode: NULL ctx");
+  ctx->graph_mode = on != 0;
+  return EPB_OK;
 }
 
 static int eph_pass_run(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double* xq, int64_t nq,
                         int prec, int64_t k_batch, int64_t sample_stride, double* ek_out, double* omega_out,
-                        double* g2sum_out, double* g2_sample, int64_t* stats_host) {
+                        double* g2sum_out, double* g2_sample, int64_t* stats_host, bool defer_checks) {
   EPB_CHECK_ARG(k_batch >= 1, "epb_eph_pass: bad k batch");
   EPB_CHECK_ARG(prec == EPB_PREC_FP64 || prec == EPB_PREC_MIXED, "epb_eph_pass: bad prec");
   EPB_CHECK_ARG(!g2_sample || sample_stride >= 1, "epb_eph_pass: sample_stride must be >= 1");
@@ -285,7 +342,8 @@ static int eph_pass_run(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk
     attr = true;
   }
   if (prec == EPB_PREC_MIXED) {
-    EPB_TRY(mixed_pass(ctx, m, xk, nk, xq, nq, Dq, omega_out, ek_out, g2sum_out, g2_sample, sample_stride, k_batch));
+    EPB_TRY(mixed_pass(ctx, m, xk, nk, xq, nq, Dq, omega_out, ek_out, g2sum_out, g2_sample, sample_stride, k_batch,
+                       defer_checks));
   }
   for (int64_t k0 = 0; prec == EPB_PREC_FP64 && k0 < nk; k0 += k_batch) {
     const int64_t nkb = nk - k0 < k_batch ? nk - k0 : k_batch;
@@ -312,7 +370,7 @@ static int eph_pass_run(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk
       EPB_LAUNCH_CHECK();
     }
   }
-  EPB_TRY(eigh_check(ctx));
+  if (!defer_checks) EPB_TRY(eigh_check(ctx));
   if (stats_host) {
     stats_host[0] = nk * nq * nw2 * nm;  // g elements produced (all bands)
     stats_host[1] = stats[1];

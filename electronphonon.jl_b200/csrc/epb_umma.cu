@@ -1023,7 +1023,7 @@ int eigh_mixed_packed(epb_ctx* ctx, const float* Hp, int64_t n, int64_t batch, f
 // The whole mixed pass after the q side (omega, u_ph in FP64) has been computed.
 int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double* xq, int64_t nq,
                const double2* uph, const double* omega, double* ek_out, double* g2sum, double* g2_sample,
-               int64_t sample_stride, int64_t kbi_max) {
+               int64_t sample_stride, int64_t kbi_max, bool defer_checks) {
   MixedModel* mm = (MixedModel*)m->mixed;
   const int64_t nw = m->nw, nm = m->nm, nw2 = nw * nw;
   const int64_t nd = nw2 * nm, nd_ep = nd * m->nr_ep;
@@ -1125,7 +1125,7 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
       }
     }
   }
-  return split_gemm_check(ctx);
+  return defer_checks ? EPB_OK : split_gemm_check(ctx);
 }
 
 }  // namespace epb

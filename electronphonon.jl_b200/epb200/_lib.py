@@ -80,6 +80,7 @@ SIGNATURES = {
     "epb_mlp_calibrate": [P, P, P, P, I64, D, P],
     "epb_mlp_set_inference": [P, I32],
     "epb_bte_serta": [P, P, P, P, P, I64, P],
+    "epb_set_graph_mode": [P, I32],
     "epb_mlp_inference_path": [P, C.POINTER(I32)],
 }
 
@@ -171,6 +172,10 @@ class Context:
 
     def synchronize(self):
         check(lib().epb_synchronize(self.h))
+
+    def set_graph_mode(self, on=True):
+        """Capture epb_eph_pass as a CUDA graph and replay it for repeated calls on the same buffers."""
+        check(lib().epb_set_graph_mode(self.h, 1 if on else 0))
 
     def free_bytes(self):
         f, t = C.c_uint64(), C.c_uint64()

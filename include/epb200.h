@@ -314,6 +314,11 @@ EPB_API int epb_model_destroy(epb_model* model);
    produced, [1] = k batch used. Replaces: the per-(k, q) loop of run_eph_over_k_and_q
    (src/calculator/run_eph_over_k_and_q.jl:251-330) run the batched way of
    _loop_eph_over_k_and_kq_batched (src/calculator/run_eph_over_k_and_kq.jl:792-892). */
+/* Graph mode (off by default): epb_eph_pass runs the first call with a given argument set eagerly,
+   captures the second as a CUDA graph and replays it on later calls with the same buffers and sizes
+   (the production loop refills the same device buffers). Ignored on the legacy default stream and
+   while profiling. */
+EPB_API int epb_set_graph_mode(epb_ctx* ctx, int on);
 EPB_API int epb_eph_pass(epb_ctx* ctx, epb_model* model, const double* xk, int64_t nk, const double* xq,
                          int64_t nq, int prec, int64_t k_batch, int64_t sample_stride, double* ek_out,
                          double* omega_out, double* g2sum_out, double* g2_sample, int64_t* stats_host);
