@@ -273,3 +273,28 @@ def fill_iqs(xkq_int, xk_int, ngrid, dense_hash_to_iq):
     check(_lib.lib().epb_fill_iqs(_ctx().h, ptr(xkq_int), nkq, xk.ctypes.data, int(ngrid[0]), int(ngrid[1]),
                                   int(ngrid[2]), ptr(dense_hash_to_iq), ptr(iqs)))
     return iqs
+
+
+# ---------------------------------------------------------------------------------------------
+def eph_window_scatter(g2_out, omega_out, g2vals, imap_i_col, imap_f, ikqs, omega, ni_stride, i0):
+    """eph_window_scatter! (src/calculator/calculator_utils.jl:36-50): device arrays in Julia layout,
+    index maps int64 1-based (0 = out of window)."""
+    nbkq, nbk, nm, nqb = _jlshape(g2vals)
+    ld_f = _jlshape(imap_f)[0]
+    check(_lib.lib().epb_eph_window_scatter(_ctx().h, ptr(g2_out), ptr(omega_out), ptr(g2vals), ptr(imap_i_col),
+                                            ptr(imap_f), ld_f, ptr(ikqs), ptr(omega), nbkq, nbk, nm, nqb,
+                                            int(ni_stride), int(i0)))
+
+
+def bte_window_accumulate(sout, sin, g2vals, omega, imap_i_at_k, imap_f, ikqs, e_i, e_f, wf, mus, ts, etas, method,
+                          omega_cutoff, i0):
+    """bte_window_accumulate! (src/boltzmann/boltzmann_calculator.jl:336-362). sout (n_i, nT),
+    sin (ni_tile, n_f, nT) or None, Julia layout device arrays."""
+    nbkq, nbk, nm, nqb = _jlshape(g2vals)
+    n_i, nT = _jlshape(sout)
+    ni_tile, n_f = (_jlshape(sin)[:2] if sin is not None else (0, 0))
+    ld_f = _jlshape(imap_f)[0]
+    check(_lib.lib().epb_bte_window_accumulate(_ctx().h, ptr(sout), n_i, ptr(sin), ni_tile, n_f, ptr(g2vals), ptr(omega),
+                                               ptr(imap_i_at_k), ptr(imap_f), ld_f, ptr(ikqs), ptr(e_i), ptr(e_f),
+                                               ptr(wf), ptr(mus), ptr(ts), ptr(etas), nT, int(method),
+                                               float(omega_cutoff), nbkq, nbk, nm, nqb, int(i0)))

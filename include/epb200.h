@@ -323,6 +323,32 @@ EPB_API int epb_eph_pass(epb_ctx* ctx, epb_model* model, const double* xk, int64
                          int64_t nq, int prec, int64_t k_batch, int64_t sample_stride, double* ek_out,
                          double* omega_out, double* g2sum_out, double* g2_sample, int64_t* stats_host);
 
+/* ---- calculator hooks of the batched loop -------------------------------------------------- */
+/* Window scatter of one batch into a device-resident calculator buffer: for every (m, n, nu, j) of
+   g2vals (nbandkq, nbandk, nm, nq_batch), i = imap_i_col[n], f = imap_f[m, ikqs[j]] (Int64, 1-based,
+   0 = out of window; imap_f column-major with leading dimension ld_imap_f); when both are > 0,
+   g2_out / omega_out at the 1-based slot nu + nm (i - i0 - 1) + nm ni_stride (f - 1) receive
+   g2vals[m, n, nu, j] / omega[nu, j]. Slots are unique across a run (no atomics).
+   Replaces: eph_window_scatter! (src/calculator/calculator_utils.jl:36-50, ext:280-313). */
+EPB_API int epb_eph_window_scatter(epb_ctx* ctx, double* g2_out, double* omega_out, const double* g2vals,
+                                   const int64_t* imap_i_col, const int64_t* imap_f, int64_t ld_imap_f,
+                                   const int64_t* ikqs, const double* omega, int64_t nbandkq, int64_t nbandk,
+                                   int64_t nm, int64_t nq_batch, int64_t ni_stride, int64_t i0);
+/* Boltzmann accumulation of one batch: for every (m, n, j) with i = imap_i_at_k[n] > 0 and
+   f = imap_f[m, ikqs[j]] > 0, and every temperature iT, the increments of
+   bte_scattering_increments(method, e_i[i], e_f[f], omega[nu, j], g2vals[m, n, nu, j], wf[f],
+   mus[iT], ts[iT], etas[iT]) summed over modes with omega >= omega_cutoff:
+   sout[i, iT] += s_out (sout (n_i, nT)); sin[i - i0, f, iT] = s_in (sin (ni_tile, n_f, nT), may be
+   NULL). Replaces: bte_window_accumulate! (src/boltzmann/boltzmann_calculator.jl:336-362,
+   ext:323-372). */
+EPB_API int epb_bte_window_accumulate(epb_ctx* ctx, double* sout, int64_t n_i, double* sin, int64_t ni_tile,
+                                      int64_t n_f, const double* g2vals, const double* omega,
+                                      const int64_t* imap_i_at_k, const int64_t* imap_f, int64_t ld_imap_f,
+                                      const int64_t* ikqs, const double* e_i, const double* e_f, const double* wf,
+                                      const double* mus, const double* ts, const double* etas, int64_t nT,
+                                      int method, double omega_cutoff, int64_t nbandkq, int64_t nbandk,
+                                      int64_t nmodes, int64_t nq_batch, int64_t i0);
+
 /* ---- SERTA Boltzmann consumer -------------------------------------------------------------- */
 typedef struct {
   int64_t ngrid;            /* k = q grid ngrid^3 (commensurate), k fastest (kpoints.jl:135-153)   */

@@ -426,3 +426,48 @@ def eph_pairs(model, xks, xqs, pairs, window=(-np.inf, np.inf), gauge_fix=False)
             entry["g2"] = epstate_set_g2(e, w)
         res.append(entry)
     return res
+
+
+# --------------------------------------------------------------------------------------------
+# Calculator hooks of the batched loop
+
+def eph_window_scatter(g2_out, om_out, g2vals, imap_i_col, imap_f, ikqs, om, ni_stride, i0):
+    """`src/calculator/calculator_utils.jl:36-50` on flat 0-based numpy outputs (1-based maps)."""
+    nbkq, nbk, nm, nqb = g2vals.shape
+    for j in range(nqb):
+        for nu in range(nm):
+            for n in range(nbk):
+                for m in range(nbkq):
+                    i = imap_i_col[n]
+                    f = imap_f[m, ikqs[j] - 1]
+                    if i > 0 and f > 0:
+                        lin = nu + nm * (i - i0 - 1) + nm * ni_stride * (f - 1)
+                        g2_out[lin] = g2vals[m, n, nu, j]
+                        om_out[lin] = om[nu, j]
+
+
+def bte_window_accumulate(sout, sin, g2vals, om, imap_i_at_k, imap_f, ikqs, e_i, e_f, wf, mus, ts, etas, method,
+                          omega_cutoff, i0):
+    """`src/boltzmann/boltzmann_calculator.jl:336-362` (1-based maps, 0-based numpy arrays)."""
+    nbkq, nbk, nm, nqb = g2vals.shape
+    for j in range(nqb):
+        for n in range(nbk):
+            for m in range(nbkq):
+                i = imap_i_at_k[n]
+                if i <= 0:
+                    continue
+                f = imap_f[m, ikqs[j] - 1]
+                if f <= 0:
+                    continue
+                for iT in range(len(mus)):
+                    so = si = 0.0
+                    for nu in range(nm):
+                        if om[nu, j] < omega_cutoff:
+                            continue
+                        a, b = bte_scattering_increments(method, e_i[i - 1], e_f[f - 1], om[nu, j], g2vals[m, n, nu, j],
+                                                         wf[f - 1], mus[iT], ts[iT], etas[iT])
+                        so += a
+                        si += b
+                    sout[i - 1, iT] += so
+                    if sin is not None:
+                        sin[i - i0 - 1, f - 1, iT] = si
