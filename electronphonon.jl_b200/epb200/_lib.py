@@ -81,6 +81,9 @@ SIGNATURES = {
     "epb_mlp_set_inference": [P, I32],
     "epb_bte_serta": [P, P, P, P, P, I64, P],
     "epb_set_graph_mode": [P, I32],
+    "epb_epmat_el_to_ph": [P, P, I64, I64, I64, I64, P],
+    "epb_eph_RR_to_Rq": [P, P, I64, I64, I64, P, P, I64, P, P, I32],
+    "epb_eph_Rq_to_kq": [P, P, I64, I64, P, P, I64, P, I64, P, I64, P, P, P, I32],
     "epb_eph_window_scatter": [P, P, P, P, P, P, I64, P, P, I64, I64, I64, I64, I64, I64],
     "epb_bte_window_accumulate": [P, P, I64, P, I64, I64, P, P, P, P, I64, P, P, P, P, P, P, P, I64, I32, D, I64, I64,
                                   I64, I64, I64],

@@ -8,6 +8,8 @@ Names, argument meaning and error behaviour follow ElectronPhonon.jl:
       (src/wannier_to_bloch_batched.jl:30-105, ext/ElectronPhononCUDAExt.jl:80-115)
   * get_eph_RR_to_kR_batched / get_eph_kR_to_kq_batched / eph_apply_rotations
       (src/wannier_to_bloch_batched.jl:178-273,442-455)
+  * epmat_el_to_ph / get_eph_RR_to_Rq_batched / get_eph_Rq_to_kq_batched, the outer-q loop
+      (src/model_new.jl:551-565, src/wannier_to_bloch.jl:277-300, src/wannier_to_bloch_batched.jl:317-377)
   * window filter (src/filter.jl:19,40-100), fill_iqs (src/calculator/run_eph_over_k_and_kq.jl:565-582)
 
 Device arrays are torch tensors holding the bytes of the Julia column-major array: a Julia array of
@@ -241,6 +243,64 @@ def get_eph_kR_to_kq_batched(ep_kq_all, ep_kR, phase, u_phs, ukqs, g2_out=None, 
     assert _jlshape(u_phs) == (nm, nm, nq)
     check(_lib.lib().epb_eph_kR_to_kq(_ctx().h, ptr(ep_kR), ld, nw, nbk, nm, nr_ep, ptr(phase), nq, ptr(ukqs),
                                       nbkq, ptr(u_phs), ptr(omega), ptr(ep_kq_all), ptr(g2_out), prec))
+    return ep_kq_all
+
+
+# ---------------------------------------------------------------------------------------------
+# Outer-q loop (the "ph" epmat layout)
+def epmat_el_to_ph(epmat_el: WannierObject, nw, nm):
+    """The "el"-layout e-ph matrix (rows (i, j, nu, Rp), columns Re) as a "ph"-layout WannierObject
+    (rows (i, j, nu, Re), columns Rp, irvec = R_ph, irvec_next = R_el) (src/model_new.jl:551-565)."""
+    torch = _torch()
+    nr_el = epmat_el.irvec.shape[0]
+    nr_ep = epmat_el.irvec_next.shape[0]
+    assert epmat_el.ndata == nw * nw * nm * nr_ep
+    out = jl_empty((nw * nw * nm * nr_el, nr_ep), torch.complex128, device=epmat_el.op_r.device)
+    check(_lib.lib().epb_epmat_el_to_ph(_ctx().h, ptr(epmat_el.op_r), nw, nm, nr_el, nr_ep, ptr(out)))
+    obj = WannierObject.__new__(WannierObject)
+    obj.irvec, obj.nr, obj.op_r = epmat_el.irvec_next, nr_ep, out
+    obj.ndata, obj.irvec_next, obj._id = nw * nw * nm * nr_el, epmat_el.irvec, 0
+    obj._irvec_dev = torch.from_numpy(np.ascontiguousarray(obj.irvec)).to(out.device)
+    return obj
+
+
+def get_eph_RR_to_Rq_batched(ep_Rq_all, itp_epmat_ph, xqs, u_phs, prec=PREC_FP64):
+    """g(Re, q) in the phonon eigenmode basis for every q of xqs (src/wannier_to_bloch.jl:277-300, a
+    list of q at once). itp_epmat_ph: interpolator over the "ph"-layout epmat (its irvec = R_ph);
+    u_phs (nm, nm, nq); ep_Rq_all (nw^2 nm, nr_el, nq), rows (i, j, nu). Pass the identity for u_phs to
+    keep the Cartesian basis."""
+    epmat = itp_epmat_ph.parent
+    nr_el = epmat.irvec_next.shape[0]
+    nm, _, nq = _jlshape(u_phs)
+    nb = epmat.ndata // (nm * nr_el)
+    nw = int(round(np.sqrt(nb)))
+    assert nw * nw * nm * nr_el == epmat.ndata
+    assert _jlshape(u_phs) == (nm, nm, nq)
+    assert _jlshape(ep_Rq_all) == (nw * nw * nm, nr_el, nq)
+    x = _xk_dev(xqs)
+    assert x.numel() // 3 == nq
+    check(_lib.lib().epb_eph_RR_to_Rq(_ctx().h, ptr(epmat.op_r), nw, nm, nr_el, itp_epmat_ph.rset.h, ptr(x), nq,
+                                      ptr(u_phs), ptr(ep_Rq_all), prec))
+    return ep_Rq_all
+
+
+def get_eph_Rq_to_kq_batched(ep_kq_all, ep_Rq, rset_el, ks, uks, ukqs, g2_out=None, omega=None, prec=PREC_FP64):
+    """ep[m, n, nu, k] = sum conj(ukqs[iw, m, k]) g(k, q)[iw, jw, nu] uks[jw, n, k] for one q
+    (src/wannier_to_bloch_batched.jl:317-377). ep_Rq: (nw^2 nm, nr_el), one q of
+    get_eph_RR_to_Rq_batched; rset_el: R_el as an `_lib.RSet` or an (nr_el, 3) array; optional
+    g2_out = |ep|^2 / (2 omega_nu) with omega (nm,)."""
+    nbkq, nbk, nm, nk = _jlshape(ep_kq_all) if ep_kq_all is not None else _jlshape(g2_out)
+    nw = _jlshape(uks)[0]
+    assert _jlshape(uks) == (nw, nbk, nk)
+    assert _jlshape(ukqs) == (nw, nbkq, nk)
+    rs = rset_el if isinstance(rset_el, _lib.RSet) else _lib.RSet(_ctx(), rset_el)
+    assert _jlshape(ep_Rq)[:2] == (nw * nw * nm, rs.nr)
+    if g2_out is not None:
+        assert omega is not None and omega.numel() >= nm
+    x = _xk_dev(ks)
+    assert x.numel() // 3 == nk
+    check(_lib.lib().epb_eph_Rq_to_kq(_ctx().h, ptr(ep_Rq), nw, nm, rs.h, ptr(x), nk, ptr(uks), nbk, ptr(ukqs),
+                                      nbkq, ptr(omega), ptr(ep_kq_all), ptr(g2_out), prec))
     return ep_kq_all
 
 

@@ -323,6 +323,26 @@ EPB_API int epb_eph_pass(epb_ctx* ctx, epb_model* model, const double* xk, int64
                          int64_t nq, int prec, int64_t k_batch, int64_t sample_stride, double* ek_out,
                          double* omega_out, double* g2sum_out, double* g2_sample, int64_t* stats_host);
 
+/* ---- outer-q loop ----------------------------------------------------------------------------- */
+/* "el" layout (nw^2 nm nr_ep rows (i, j, nu, Rp), nr_el columns Re) -> "ph" layout (nw^2 nm nr_el rows
+   (i, j, nu, Re), nr_ep columns Rp), c128: permutedims [1,2,3,5,4] of src/model.jl:80-81,293-296. */
+EPB_API int epb_epmat_el_to_ph(epb_ctx* ctx, const double* epmat_el, int64_t nw, int64_t nm, int64_t nr_el,
+                               int64_t nr_ep, double* epmat_ph);
+/* g(Re, q) for each q of xq (3 x nq): the Fourier sum over Rp of the "ph"-layout epmat_ph, then the mode
+   rotation by uph (nm x nm x nq); out (nw^2 nm x nr_el x nq), rows (i, j, nu). Replaces:
+   get_eph_RR_to_Rq! (src/wannier_to_bloch.jl:277-300) for a list of q. */
+EPB_API int epb_eph_RR_to_Rq(epb_ctx* ctx, const double* epmat_ph, int64_t nw, int64_t nm, int64_t nr_el,
+                             const epb_rset* rset_ph, const double* xq, int64_t nq, const double* uph, double* out,
+                             int prec);
+/* For one q: g(k, q) = sum_Re e^{2 pi i k.Re} g(Re, q) at each k of xk (3 x nk) (g_Rq from
+   epb_eph_RR_to_Rq, rset_el its Re set), then ep[m, n, nu, k] = sum conj(ukq[iw, m, k]) g[iw, jw, nu, k]
+   uk[jw, n, k] (uks (nw, nbk, nk), ukqs (nw, nbkq, nk)); outputs ep (nbkq, nbk, nm, nk) and/or
+   g2 = |ep|^2 / (2 omega_nu) (omega: nm values of this q). Replaces: get_eph_Rq_to_kq_batched! +
+   eph_apply_rotations_rqkq! (src/wannier_to_bloch_batched.jl:317-377, ext:206-258). */
+EPB_API int epb_eph_Rq_to_kq(epb_ctx* ctx, const double* g_Rq, int64_t nw, int64_t nm, const epb_rset* rset_el,
+                             const double* xk, int64_t nk, const double* uks, int64_t nbk, const double* ukqs,
+                             int64_t nbkq, const double* omega, double* ep_out, double* g2_out, int prec);
+
 /* ---- calculator hooks of the batched loop -------------------------------------------------- */
 /* Window scatter of one batch into a device-resident calculator buffer: for every (m, n, nu, j) of
    g2vals (nbandkq, nbandk, nm, nq_batch), i = imap_i_col[n], f = imap_f[m, ikqs[j]] (Int64, 1-based,

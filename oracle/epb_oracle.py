@@ -225,6 +225,32 @@ def get_eph_kR_to_kq(ep_kR, irvec_ep, xq1, u_ph, ukq, nbk):
     return (ab1 @ u_ph).reshape(ukq.shape[1], nbk, nm, order="F")
 
 
+def epmat_el_to_ph(op_r_el, nw, nmodes, nr_el, nr_ep):
+    """(i, j, nu, Rp, Re) -> (i, j, nu, Re, Rp), the two layouts of `src/model_new.jl:551-565`
+    (permutedims [1,2,3,5,4], `src/model.jl:80-81,293-296`)."""
+    a = np.asarray(op_r_el).reshape(nw * nw * nmodes, nr_ep, nr_el, order="F")
+    return np.asfortranarray(a.transpose(0, 2, 1).reshape(nw * nw * nmodes * nr_el, nr_ep, order="F"))
+
+
+def get_eph_RR_to_Rq(op_r_ph, irvec_ep, nw, nmodes, nr_el, xq1, u_ph):
+    """g(Re, q) rotated into the phonon eigenmode basis, one Re at a time
+    (`src/wannier_to_bloch.jl:277-300`). Returns (nw*nw*nmodes, nr_el), rows (i, j, nu)."""
+    g = get_fourier(op_r_ph, op_r_ph.shape[0], irvec_ep, xq1).reshape(nw * nw, nmodes, nr_el, order="F")
+    out = np.empty_like(g)
+    for ir in range(nr_el):
+        out[:, :, ir] = g[:, :, ir] @ u_ph
+    return out.reshape(nw * nw * nmodes, nr_el, order="F")
+
+
+def get_eph_Rq_to_kq_batched(g_Rq, irvec_el, xks, uks, ukqs, nmodes):
+    """ep[m, n, nu, k] = sum_{iw, jw} conj(ukqs[iw, m, k]) g(k, q)[iw, jw, nu] uks[jw, n, k]
+    (`src/wannier_to_bloch_batched.jl:317-377`; the per-k form `src/wannier_to_bloch.jl:326-350`)."""
+    nw = uks.shape[0]
+    nk = xks.shape[1]
+    g = fourier_batched(g_Rq, g_Rq.shape[0], irvec_el, xks).reshape(nw, nw, nmodes, nk, order="F")
+    return np.asfortranarray(np.einsum("imk,ijak,jnk->mnak", ukqs.conj(), g, uks))
+
+
 def epstate_set_g2(ep, omega):
     """g2[:,:,nu] = |ep|^2 / (2 omega_nu), no frequency floor; `src/EPState.jl:73-81`."""
     return np.abs(ep) ** 2 * (1.0 / (2.0 * np.asarray(omega)))[None, None, :]
