@@ -79,6 +79,9 @@ enum epb_slot {
   EPB_WS_PAIR1,
   EPB_WS_PAIR2,
   EPB_WS_PAIR3,
+  EPB_WS_OQ0,  // outer-q loop: k and q states (whole run)
+  EPB_WS_OQ1,  // outer-q loop: g(Re, q) of a q chunk
+  EPB_WS_OQ2,  // outer-q loop: per k batch
   EPB_WS_NSLOTS
 };
 
@@ -176,6 +179,7 @@ struct epb_model {
   // mixed-precision operand planes (owned), see epb_umma.cu
   void* mixed = nullptr;
   PassGraph graph;  // graph mode of epb_eph_pass
+  double2* epmat_ph = nullptr;  // owned "ph"-layout copy of epmat (outer-q loop), made on first use
 };
 
 namespace epb {

@@ -13,6 +13,22 @@ namespace epb {
 
 int fourier_f64(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, const epb_rset* rs, const double* xk,
                 int64_t N, double2* out, int64_t ldo);
+int fourier_mixed(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, const epb_rset* rs, const double* xk,
+                  int64_t N, double2* out, int64_t ldo);
+int eigh_async(epb_ctx* ctx, double2* A, int64_t n, int64_t batch, double* E, bool want_v, const double* mass,
+               int prec);
+int eigh_check(epb_ctx* ctx);
+int window_filter(epb_ctx* ctx, const double* E, int64_t nw, int64_t nk, double wmin, double wmax, int32_t* bmin,
+                  int32_t* bmax, int32_t* keep_idx, int64_t* nkeep, double* nbelow);
+
+// FP64 Fourier sum over row blocks of at most 2^20 rows (one launch's grid limit is far above that).
+static int fourier_rows(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, const epb_rset* rs, const double* x,
+                        int64_t N, double2* out, int64_t ldo) {
+  const int64_t RB = (int64_t)1 << 20;
+  for (int64_t r0 = 0; r0 < M; r0 += RB)
+    EPB_TRY(fourier_f64(ctx, op + r0, ld, std::min(RB, M - r0), rs, x, N, out + r0, ldo));
+  return EPB_OK;
+}
 
 static unsigned grid_oq(epb_ctx* ctx, int64_t n) {
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, 256), (int64_t)ctx->sm_count * 32));
@@ -71,6 +87,154 @@ __global__ void epmat_el_to_ph_kernel(const double2* __restrict__ in, int64_t nb
   }
 }
 
+
+// ---- outer-q driver kernels -------------------------------------------------------------------
+// Kept k (keep list from the window filter): positions, weights, energies, and eigenvectors with the
+// columns outside the k window [bmin, bmax] (1-based) set to zero.
+__global__ void oq_gather_k_kernel(const int32_t* __restrict__ keep, const int64_t* __restrict__ nkeep_d,
+                                   const double* __restrict__ xk, const double* __restrict__ wtk,
+                                   const double* __restrict__ E, const double2* __restrict__ U,
+                                   const int32_t* __restrict__ bmin, const int32_t* __restrict__ bmax, int nw,
+                                   double* __restrict__ xo, double* __restrict__ wo, double* __restrict__ Eo,
+                                   double2* __restrict__ Uo) {
+  const int64_t nkeep = *nkeep_d;
+  const int64_t nw2 = (int64_t)nw * nw;
+  const int64_t total = nkeep * nw2;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = e / nw2, r = e % nw2;
+    const int64_t k = keep[j];
+    const int col = (int)(r / nw) + 1;
+    Uo[e] = (col >= bmin[k] && col <= bmax[k]) ? U[k * nw2 + r] : make_double2(0.0, 0.0);
+    if (r < nw) Eo[j * nw + r] = E[k * nw + r];
+    if (r < 3) xo[3 * j + r] = xk[3 * k + r];
+    if (r == 0) wo[j] = wtk ? wtk[k] : 1.0;
+  }
+}
+
+__global__ void oq_shift_kernel(const double* __restrict__ xk, int64_t nk, const double* __restrict__ xq,
+                                double* __restrict__ xkq) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < 3 * nk; e += (int64_t)gridDim.x * blockDim.x)
+    xkq[e] = xk[e] + xq[e % 3];
+}
+
+// Zero the eigenvector columns m whose energy lies outside [wmin, wmax] (the k+q window mask of
+// src/calculator/run_eph_over_q_and_k.jl:577-580).
+__global__ void oq_mask_kernel(double2* __restrict__ U, const double* __restrict__ E, int nw, int64_t nk, double wmin,
+                               double wmax) {
+  const int64_t nw2 = (int64_t)nw * nw;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nk * nw2; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = e / nw2;
+    const int m = (int)((e % nw2) / nw);
+    const double v = E[k * nw + m];
+    if (!(v >= wmin && v <= wmax)) U[e] = make_double2(0.0, 0.0);
+  }
+}
+
+__global__ void oq_identity_kernel(double2* __restrict__ u, int nm, int64_t nq) {
+  const int64_t nm2 = (int64_t)nm * nm;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nq * nm2; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = e % nm2;
+    u[e] = make_double2((r % nm) == (r / nm) ? 1.0 : 0.0, 0.0);
+  }
+}
+
+// One block per k: ep[m, n, nu] = sum_{iw, jw} conj(ukq[iw, m]) g[iw, jw, nu] uk[jw, n] through shared
+// memory (T[m, jw] = sum_iw conj(ukq[iw, m]) g[iw, jw, nu], then T uk), and part[k] = wtk[k] sum |ep|^2.
+// Shared memory: four nw x (nw + 1) complex tiles (conj(ukq)^T, uk, g_nu, T).
+constexpr int OQ_ROT_THREADS = 256;
+template <bool STORE>
+__global__ void __launch_bounds__(OQ_ROT_THREADS) oq_rot_kernel(const double2* __restrict__ g, const double2* __restrict__ uk,
+                                                              const double2* __restrict__ ukq, const double* __restrict__ wtk,
+                                                              int nw, int nm, int64_t nk, double2* __restrict__ ep,
+                                                              double* __restrict__ part) {
+  extern __shared__ double2 oq_sm[];
+  const int L = nw + 1, nw2 = nw * nw;
+  double2* sq = oq_sm;         // sq[m * L + iw] = conj(ukq[iw, m])
+  double2* sk = sq + nw * L;   // sk[n * L + jw] = uk[jw, n]
+  double2* sg = sk + nw * L;   // sg[jw * L + iw] = g[iw, jw, nu]
+  double2* st = sg + nw * L;   // st[jw * L + m] = T[m, jw]
+  __shared__ double red[OQ_ROT_THREADS / 32];
+  for (int64_t k = blockIdx.x; k < nk; k += gridDim.x) {
+    __syncthreads();
+    const double2* uq = ukq + k * nw2;
+    const double2* ukk = uk + k * nw2;
+    for (int e = threadIdx.x; e < nw2; e += blockDim.x) {
+      const int i = e % nw, c = e / nw;
+      const double2 a = uq[e];
+      sq[c * L + i] = make_double2(a.x, -a.y);
+      sk[c * L + i] = ukk[e];
+    }
+    double acc2 = 0.0;
+    for (int nu = 0; nu < nm; ++nu) {
+      const double2* gk = g + (k * nm + nu) * nw2;
+      for (int e = threadIdx.x; e < nw2; e += blockDim.x) sg[(e / nw) * L + (e % nw)] = gk[e];
+      __syncthreads();
+      for (int e = threadIdx.x; e < nw2; e += blockDim.x) {
+        const int m = e % nw, jw = e / nw;
+        const double2* a = sq + m * L;
+        const double2* b = sg + jw * L;
+        double2 t = make_double2(0.0, 0.0);
+        for (int iw = 0; iw < nw; ++iw) cfma(t, a[iw], b[iw]);
+        st[jw * L + m] = t;
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < nw2; e += blockDim.x) {
+        const int m = e % nw, n = e / nw;
+        const double2* b = sk + n * L;
+        double2 v = make_double2(0.0, 0.0);
+        for (int jw = 0; jw < nw; ++jw) cfma(v, st[jw * L + m], b[jw]);
+        if (STORE) ep[(k * nm + nu) * nw2 + e] = v;
+        acc2 += v.x * v.x + v.y * v.y;
+      }
+      __syncthreads();
+    }
+    if (part) {
+      for (int o = 16; o > 0; o >>= 1) acc2 += __shfl_xor_sync(0xffffffffu, acc2, o);
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc2;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+        part[k] = wtk[k] * s;
+      }
+    }
+  }
+}
+
+// A[iq] += sum_k part[k], one block, fixed order (deterministic).
+__global__ void oq_record_kernel(const double* __restrict__ part, int64_t nk, double* __restrict__ A) {
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int64_t k = threadIdx.x; k < nk; k += blockDim.x) s += part[k];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *A += red[0];
+}
+
+static size_t oq_rot_smem(int nw) { return (size_t)4 * nw * (nw + 1) * sizeof(double2); }
+
+static int oq_rotate(epb_ctx* ctx, const double2* g, const double2* uk, const double2* ukq, const double* wtk, int nw,
+                     int nm, int64_t nk, double2* ep, double* part) {
+  const size_t sm = oq_rot_smem(nw);
+  if (sm > 48 * 1024) {
+    EPB_CUDA(cudaFuncSetAttribute(oq_rot_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    EPB_CUDA(cudaFuncSetAttribute(oq_rot_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  }
+  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nk, (int64_t)ctx->sm_count * 8));
+  prof_begin(ctx, EPB_PROF_ROT);
+  if (ep)
+    oq_rot_kernel<true><<<grid, OQ_ROT_THREADS, sm, ctx->stream>>>(g, uk, ukq, wtk, nw, nm, nk, ep, part);
+  else
+    oq_rot_kernel<false><<<grid, OQ_ROT_THREADS, sm, ctx->stream>>>(g, uk, ukq, wtk, nw, nm, nk, ep, part);
+  prof_end(ctx);
+  EPB_LAUNCH_CHECK();
+  return EPB_OK;
+}
+
 }  // namespace epb
 
 using namespace epb;
@@ -108,7 +272,7 @@ int epb_eph_RR_to_Rq(epb_ctx* ctx, const double* epmat_ph, int64_t nw, int64_t n
   double2* g = (double2*)ws;
   for (int64_t q0 = 0; q0 < nq; q0 += qc) {
     const int64_t qn = std::min(qc, nq - q0);
-    EPB_TRY(fourier_f64(ctx, (const double2*)epmat_ph, ndata, ndata, rset_ph, xq + 3 * q0, qn, g, ndata));
+    EPB_TRY(fourier_rows(ctx, (const double2*)epmat_ph, ndata, ndata, rset_ph, xq + 3 * q0, qn, g, ndata));
     prof_begin(ctx, EPB_PROF_RR_ROT);
     rq_mode_rotate_kernel<<<grid_oq(ctx, ndata * qn), 256, 0, ctx->stream>>>(
         g, (const double2*)uph + q0 * nm * nm, nb, nm, nr_el, qn, (double2*)out + q0 * ndata);
@@ -137,7 +301,10 @@ int epb_eph_Rq_to_kq(epb_ctx* ctx, const double* g_Rq, int64_t nw, int64_t nm, c
   double2* g = (double2*)ws;
   for (int64_t k0 = 0; k0 < nk; k0 += kc) {
     const int64_t kn = std::min(kc, nk - k0);
-    EPB_TRY(fourier_f64(ctx, (const double2*)g_Rq, ndata, ndata, rset_el, xk + 3 * k0, kn, g, ndata));
+    if (prec == EPB_PREC_MIXED)
+      EPB_TRY(fourier_mixed(ctx, (const double2*)g_Rq, ndata, ndata, rset_el, xk + 3 * k0, kn, g, ndata));
+    else
+      EPB_TRY(fourier_f64(ctx, (const double2*)g_Rq, ndata, ndata, rset_el, xk + 3 * k0, kn, g, ndata));
     const int64_t o = nbkq * nbk * nm * k0;
     prof_begin(ctx, EPB_PROF_ROT);
     rqkq_rot_kernel<<<grid_oq(ctx, nbkq * nbk * kn), 256, 0, ctx->stream>>>(
@@ -146,6 +313,222 @@ int epb_eph_Rq_to_kq(epb_ctx* ctx, const double* g_Rq, int64_t nw, int64_t nm, c
     prof_end(ctx);
     EPB_LAUNCH_CHECK();
   }
+  return EPB_OK;
+}
+
+
+int epb_eph_outer_q(epb_ctx* ctx, epb_model* m, const double* xk_host, const double* wtk_host, int64_t nk,
+                    const double* xq_host, int64_t nq, const epb_outer_q_params* prm, const epb_outer_q_calc* calcs,
+                    int ncalc, double* A_host, int64_t* stats_host) {
+  clear_error();
+  EPB_CHECK_ARG(ctx && m && prm, "epb_eph_outer_q: NULL ctx, model or params");
+  EPB_CHECK_ARG(nk >= 0 && nq >= 0 && ncalc >= 0, "epb_eph_outer_q: bad sizes");
+  EPB_CHECK_ARG((nk == 0 || xk_host) && (nq == 0 || xq_host) && (ncalc == 0 || calcs),
+                "epb_eph_outer_q: NULL buffer");
+  EPB_CHECK_ARG(prm->prec == EPB_PREC_FP64 || prm->prec == EPB_PREC_MIXED, "epb_eph_outer_q: bad prec");
+  EPB_CHECK_ARG(prm->phonon_basis == 0 || prm->phonon_basis == 1, "epb_eph_outer_q: phonon_basis must be 0 or 1");
+  for (int c = 0; c < ncalc; ++c)
+    EPB_CHECK_ARG(calcs[c].run_batch, "epb_eph_outer_q: calculator %d has no run_batch", c);
+  EPB_TRY(make_current(ctx));
+  const int nw = (int)m->nw, nm = (int)m->nm;
+  const int64_t nw2 = (int64_t)nw * nw, nd = nw2 * nm, nr_el = m->nr_el;
+  const int prec = prm->prec;
+  if (stats_host)
+    for (int i = 0; i < 4; ++i) stats_host[i] = 0;
+  if (A_host)
+    for (int64_t i = 0; i < nq; ++i) A_host[i] = 0.0;
+  if (nq == 0) return EPB_OK;
+
+  // "ph"-layout epmat, made once per model
+  if (!m->epmat_ph) {
+    EPB_CUDA(cudaMalloc(&m->epmat_ph, (size_t)16 * nd * m->nr_ep * nr_el));
+    epmat_el_to_ph_kernel<<<grid_oq(ctx, nd * nr_el * m->nr_ep), 256, 0, ctx->stream>>>(m->epmat, nd, nr_el, m->nr_ep,
+                                                                                      m->epmat_ph);
+    EPB_LAUNCH_CHECK();
+  }
+
+  // ---- k and q states (whole run) ----
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off += (bytes + 255) & ~size_t(255);
+    return o;
+  };
+  const int64_t nk1 = std::max<int64_t>(nk, 1);
+  const size_t o_xk = take(24 * nk1), o_wk = take(8 * nk1), o_U = take(16 * nw2 * nk1), o_E = take(8 * nw * nk1),
+               o_bmin = take(4 * nk1), o_bmax = take(4 * nk1), o_keep = take(4 * nk1), o_nkeep = take(64),
+               o_xkk = take(24 * nk1), o_wkk = take(8 * nk1), o_Uk = take(16 * nw2 * nk1), o_Ek = take(8 * nw * nk1),
+               o_xq = take(24 * nq), o_uph = take(16 * (int64_t)nm * nm * nq), o_om = take(8 * (int64_t)nm * nq),
+               o_A = take(8 * nq);
+  void* ws0 = nullptr;
+  EPB_TRY(ws_get(ctx, EPB_WS_OQ0, off + 256, &ws0));
+  uint8_t* b0 = (uint8_t*)ws0;
+  double* xk_d = (double*)(b0 + o_xk);
+  double* wk_d = (double*)(b0 + o_wk);
+  double2* U_all = (double2*)(b0 + o_U);
+  double* E_all = (double*)(b0 + o_E);
+  int32_t* bmin = (int32_t*)(b0 + o_bmin);
+  int32_t* bmax = (int32_t*)(b0 + o_bmax);
+  int32_t* keep = (int32_t*)(b0 + o_keep);
+  int64_t* nkeep_d = (int64_t*)(b0 + o_nkeep);
+  double* xkk = (double*)(b0 + o_xkk);
+  double* wkk = (double*)(b0 + o_wkk);
+  double2* Uk = (double2*)(b0 + o_Uk);
+  double* Ek = (double*)(b0 + o_Ek);
+  double* xq_d = (double*)(b0 + o_xq);
+  double2* uph = (double2*)(b0 + o_uph);
+  double* om = (double*)(b0 + o_om);
+  double* A_d = (double*)(b0 + o_A);
+
+  if (nk > 0) {
+    EPB_CUDA(cudaMemcpyAsync(xk_d, xk_host, 24 * nk, cudaMemcpyHostToDevice, ctx->stream));
+    if (wtk_host) EPB_CUDA(cudaMemcpyAsync(wk_d, wtk_host, 8 * nk, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  EPB_CUDA(cudaMemcpyAsync(xq_d, xq_host, 24 * nq, cudaMemcpyHostToDevice, ctx->stream));
+  EPB_CUDA(cudaMemsetAsync(A_d, 0, 8 * nq, ctx->stream));
+  const int64_t HC = 65536;
+  for (int64_t k0 = 0; k0 < nk; k0 += HC) {
+    const int64_t kn = std::min(HC, nk - k0);
+    EPB_TRY(fourier_f64(ctx, m->ham, nw2, nw2, m->rs_el, xk_d + 3 * k0, kn, U_all + k0 * nw2, nw2));
+    EPB_TRY(eigh_async(ctx, U_all + k0 * nw2, nw, kn, E_all + k0 * nw, true, nullptr, prec));
+  }
+  EPB_TRY(window_filter(ctx, E_all, nw, nk, prm->wmin_k, prm->wmax_k, bmin, bmax, keep, nkeep_d, nullptr));
+  if (nk > 0) {
+    oq_gather_k_kernel<<<grid_oq(ctx, nk * nw2), 256, 0, ctx->stream>>>(keep, nkeep_d, xk_d, wtk_host ? wk_d : nullptr,
+                                                                        E_all, U_all, bmin, bmax, nw, xkk, wkk, Ek, Uk);
+    EPB_LAUNCH_CHECK();
+  }
+  const int64_t nmm = (int64_t)nm * nm;
+  for (int64_t q0 = 0; q0 < nq; q0 += HC) {
+    const int64_t qn = std::min(HC, nq - q0);
+    EPB_TRY(fourier_f64(ctx, m->dyn, nmm, nmm, m->rs_ph, xq_d + 3 * q0, qn, uph + q0 * nmm, nmm));
+    EPB_TRY(eigh_async(ctx, uph + q0 * nmm, nm, qn, om + q0 * nm, true, m->mass, EPB_PREC_FP64));
+  }
+  if (prm->phonon_basis == 1) {
+    oq_identity_kernel<<<grid_oq(ctx, nq * nmm), 256, 0, ctx->stream>>>(uph, nm, nq);
+    EPB_LAUNCH_CHECK();
+  }
+  EPB_TRY(eigh_check(ctx));
+  int64_t nkeep = 0;
+  {
+    int64_t* h = (int64_t*)ctx->pinned;
+    EPB_CUDA(cudaMemcpyAsync(h, nkeep_d, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    EPB_CUDA(cudaStreamSynchronize(ctx->stream));
+    nkeep = h[0];
+  }
+
+  // ---- batch sizes ----
+  const int64_t KB = std::max<int64_t>(1, std::min<int64_t>(nkeep, prm->k_batch > 0 ? prm->k_batch : 4096));
+  const int64_t per_q = 16 * nd * nr_el;
+  const int64_t QC = std::max<int64_t>(
+      1, std::min<int64_t>(nq, prm->q_chunk > 0 ? prm->q_chunk : std::max<int64_t>(1, ((int64_t)1 << 30) / per_q)));
+  if (stats_host) {
+    stats_host[0] = nkeep;
+    stats_host[1] = KB;
+    stats_host[2] = QC;
+  }
+  void* ws1 = nullptr;
+  EPB_TRY(ws_get(ctx, EPB_WS_OQ1, (size_t)per_q * QC * (prm->phonon_basis == 0 ? 2 : 1) + 256, &ws1));
+  double2* Gq = (double2*)ws1;                                       // Fourier over Rp, (nd nr_el, QC)
+  double2* Grq = prm->phonon_basis == 0 ? Gq + nd * nr_el * QC : Gq;  // after the mode rotation
+  size_t off2 = 0;
+  auto take2 = [&](size_t bytes) {
+    size_t o = off2;
+    off2 += (bytes + 255) & ~size_t(255);
+    return o;
+  };
+  const size_t o_xkq = take2(24 * KB), o_H = take2(16 * nw2 * KB), o_Ekq = take2(8 * nw * KB),
+               o_g = take2(16 * nd * KB), o_ep = take2(ncalc > 0 ? 16 * nd * KB : 0), o_part = take2(8 * KB);
+  void* ws2 = nullptr;
+  EPB_TRY(ws_get(ctx, EPB_WS_OQ2, off2 + 256, &ws2));
+  uint8_t* b2 = (uint8_t*)ws2;
+  double* xkq = (double*)(b2 + o_xkq);
+  double2* Hkq = (double2*)(b2 + o_H);
+  double* Ekq = (double*)(b2 + o_Ekq);
+  double2* gk = (double2*)(b2 + o_g);
+  double2* ep = ncalc > 0 ? (double2*)(b2 + o_ep) : nullptr;
+  double* part = (double*)(b2 + o_part);
+
+  int64_t nbatches = 0;
+  for (int64_t q0 = 0; q0 < nq; q0 += QC) {
+    const int64_t qn = std::min(QC, nq - q0);
+    // g(Re, q) = sum_Rp e^{2 pi i q.Rp} g(Re, Rp) for the chunk, then the mode rotation
+    EPB_TRY(fourier_rows(ctx, m->epmat_ph, nd * nr_el, nd * nr_el, m->rs_ep, xq_d + 3 * q0, qn, Gq, nd * nr_el));
+    if (prm->phonon_basis == 0) {
+      prof_begin(ctx, EPB_PROF_RR_ROT);
+      rq_mode_rotate_kernel<<<grid_oq(ctx, nd * nr_el * qn), 256, 0, ctx->stream>>>(Gq, uph + q0 * nmm, nw2, nm, nr_el,
+                                                                                  qn, Grq);
+      prof_end(ctx);
+      EPB_LAUNCH_CHECK();
+    }
+    for (int64_t iq = q0; iq < q0 + qn; ++iq) {
+      for (int c = 0; c < ncalc; ++c)
+        if (calcs[c].begin_q) {
+          const int st = calcs[c].begin_q(calcs[c].user, iq, (void*)ctx->stream);
+          if (st != 0) {
+            set_error("epb_eph_outer_q: calculator %d begin_q returned %d at iq=%lld", c, st, (long long)iq);
+            return EPB_ERR_ARG;
+          }
+        }
+      const double2* gRq = Grq + (iq - q0) * nd * nr_el;
+      for (int64_t k0 = 0; k0 < nkeep; k0 += KB) {
+        const int64_t kn = std::min(KB, nkeep - k0);
+        oq_shift_kernel<<<grid_oq(ctx, 3 * kn), 256, 0, ctx->stream>>>(xkk + 3 * k0, kn, xq_d + 3 * iq, xkq);
+        EPB_LAUNCH_CHECK();
+        EPB_TRY(fourier_f64(ctx, m->ham, nw2, nw2, m->rs_el, xkq, kn, Hkq, nw2));
+        EPB_TRY(eigh_async(ctx, Hkq, nw, kn, Ekq, true, nullptr, prec));
+        oq_mask_kernel<<<grid_oq(ctx, kn * nw2), 256, 0, ctx->stream>>>(Hkq, Ekq, nw, kn, prm->wmin_kq, prm->wmax_kq);
+        EPB_LAUNCH_CHECK();
+        if (prec == EPB_PREC_MIXED)
+          EPB_TRY(fourier_mixed(ctx, gRq, nd, nd, m->rs_el, xkk + 3 * k0, kn, gk, nd));
+        else
+          EPB_TRY(fourier_f64(ctx, gRq, nd, nd, m->rs_el, xkk + 3 * k0, kn, gk, nd));
+        EPB_TRY(oq_rotate(ctx, gk, Uk + k0 * nw2, Hkq, wkk + k0, nw, nm, kn, ep, part));
+        oq_record_kernel<<<1, 256, 0, ctx->stream>>>(part, kn, A_d + iq);
+        EPB_LAUNCH_CHECK();
+        ++nbatches;
+        if (ncalc > 0) {
+          epb_kbatch_payload p;
+          p.iq = iq;
+          p.k0 = k0;
+          p.nk = kn;
+          p.nw = nw;
+          p.nm = nm;
+          p.eps = (const double*)ep;
+          p.ek = Ek + k0 * nw;
+          p.ekq = Ekq;
+          p.uk = (const double*)(Uk + k0 * nw2);
+          p.ukq = (const double*)Hkq;
+          p.wtk = wkk + k0;
+          p.xk = xkk + 3 * k0;
+          p.ik = keep + k0;
+          p.omega = om + iq * nm;
+          p.stream = (void*)ctx->stream;
+          for (int c = 0; c < ncalc; ++c) {
+            const int st = calcs[c].run_batch(calcs[c].user, &p);
+            if (st != 0) {
+              set_error("epb_eph_outer_q: calculator %d run_batch returned %d at iq=%lld", c, st, (long long)iq);
+              return EPB_ERR_ARG;
+            }
+          }
+        }
+      }
+      EPB_TRY(eigh_check(ctx));
+      for (int c = 0; c < ncalc; ++c)
+        if (calcs[c].end_q) {
+          const int st = calcs[c].end_q(calcs[c].user, iq, (void*)ctx->stream);
+          if (st != 0) {
+            set_error("epb_eph_outer_q: calculator %d end_q returned %d at iq=%lld", c, st, (long long)iq);
+            return EPB_ERR_ARG;
+          }
+        }
+    }
+  }
+  if (stats_host) stats_host[3] = nbatches;
+  if (A_host) {
+    EPB_CUDA(cudaMemcpyAsync(A_host, A_d, 8 * nq, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  EPB_CUDA(cudaStreamSynchronize(ctx->stream));
   return EPB_OK;
 }
 

@@ -157,6 +157,7 @@ int epb_model_destroy(epb_model* m) {
   epb_rset_destroy(m->rs_ph);
   epb_rset_destroy(m->rs_ep);
   if (m->graph.exec) cudaGraphExecDestroy(m->graph.exec);
+  if (m->epmat_ph) cudaFree(m->epmat_ph);
   delete m;
   return EPB_OK;
 }

@@ -84,6 +84,7 @@ SIGNATURES = {
     "epb_epmat_el_to_ph": [P, P, I64, I64, I64, I64, P],
     "epb_eph_RR_to_Rq": [P, P, I64, I64, I64, P, P, I64, P, P, I32],
     "epb_eph_Rq_to_kq": [P, P, I64, I64, P, P, I64, P, I64, P, I64, P, P, P, I32],
+    "epb_eph_outer_q": [P, P, P, P, I64, P, I64, P, P, I32, P, P],
     "epb_eph_window_scatter": [P, P, P, P, P, P, I64, P, P, I64, I64, I64, I64, I64, I64],
     "epb_bte_window_accumulate": [P, P, I64, P, I64, I64, P, P, P, P, I64, P, P, P, P, P, P, P, I64, I32, D, I64, I64,
                                   I64, I64, I64],
@@ -105,6 +106,28 @@ class BteParams(C.Structure):
     _fields_ = [("ngrid", I64), ("wmin", D), ("wmax", D), ("mu", D), ("temperature", D), ("smearing", D),
                 ("omega_cutoff", D), ("spin_degeneracy", D), ("volume", D), ("lattice", D * 9), ("method", C.c_int32),
                 ("prec", C.c_int32), ("k_batch", I64)]
+
+
+class OuterQParams(C.Structure):
+    """epb_outer_q_params."""
+    _fields_ = [("wmin_k", D), ("wmax_k", D), ("wmin_kq", D), ("wmax_kq", D), ("k_batch", I64), ("q_chunk", I64),
+                ("prec", C.c_int32), ("phonon_basis", C.c_int32)]
+
+
+class KBatchPayload(C.Structure):
+    """epb_kbatch_payload (device pointers)."""
+    _fields_ = [("iq", I64), ("k0", I64), ("nk", I64), ("nw", I64), ("nm", I64), ("eps", P), ("ek", P), ("ekq", P),
+                ("uk", P), ("ukq", P), ("wtk", P), ("xk", P), ("ik", P), ("omega", P), ("stream", P)]
+
+
+BEGIN_Q_FN = C.CFUNCTYPE(C.c_int, P, I64, P)
+RUN_BATCH_FN = C.CFUNCTYPE(C.c_int, P, C.POINTER(KBatchPayload))
+END_Q_FN = C.CFUNCTYPE(C.c_int, P, I64, P)
+
+
+class OuterQCalc(C.Structure):
+    """epb_outer_q_calc."""
+    _fields_ = [("begin_q", BEGIN_Q_FN), ("run_batch", RUN_BATCH_FN), ("end_q", END_Q_FN), ("user", P)]
 
 
 class MlpTrainOpts(C.Structure):

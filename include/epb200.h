@@ -343,6 +343,54 @@ EPB_API int epb_eph_Rq_to_kq(epb_ctx* ctx, const double* g_Rq, int64_t nw, int64
                              const double* xk, int64_t nk, const double* uks, int64_t nbk, const double* ukqs,
                              int64_t nbkq, const double* omega, double* ep_out, double* g2_out, int prec);
 
+/* Outer-q batched loop (src/calculator/run_eph_over_q_and_k.jl:428-613): for each q, g(Re, q) from the
+   "ph"-layout epmat (made once per model from the "el" layout) and the phonon eigenmodes at q; then per
+   batch of kept k (k with a non-empty window_k range; eigenvectors zero outside it): H(k+q), its eigen,
+   eigenvector columns outside window_kq set to zero, ep = ukq^H g(k, q) uk, and the calculators'
+   run_batch with the EPDataKBatched payload (src/EPData.jl:76-114). A_out[iq] (optional, host) receives
+   the gauge-invariant record sum_k wtk sum_{m, n, nu} |ep|^2. */
+typedef struct epb_outer_q_params {
+  double wmin_k, wmax_k;    /* k window (window_k) */
+  double wmin_kq, wmax_kq;  /* k+q window (window_kq) */
+  int64_t k_batch;          /* kept k per batch; <= 0: min(nk kept, 4096) (nk_batch_max) */
+  int64_t q_chunk;          /* q per RR->Rq launch; <= 0: as many as fit 1 GiB of g(Re, q) */
+  int prec;                 /* EPB_PREC_FP64, or EPB_PREC_MIXED (FP32 + FP64-refined eigensolves, split-BF16
+                               Fourier over Re) */
+  int phonon_basis;         /* 0 eigenmode, 1 Cartesian (u_ph = identity) (eph_phonon_basis) */
+} epb_outer_q_params;
+
+/* EPDataKBatched (src/EPData.jl:76-114) plus the batch position; device pointers valid until run_batch
+   returns; work that reads them must be ordered on `stream` (the context's). */
+typedef struct epb_kbatch_payload {
+  int64_t iq, k0, nk;  /* q index, first kept-k index of the batch, batch width */
+  int64_t nw, nm;
+  const double* eps;   /* (nw, nw, nm, nk) c128, out-of-window bands zero */
+  const double* ek;    /* (nw, nk) */
+  const double* ekq;   /* (nw, nk) */
+  const double* uk;    /* (nw, nw, nk) c128, zero outside the k window */
+  const double* ukq;   /* (nw, nw, nk) c128, zero outside the k+q window */
+  const double* wtk;   /* (nk) */
+  const double* xk;    /* (3, nk) */
+  const int32_t* ik;   /* (nk) index of each k in the caller's k list */
+  const double* omega; /* (nm) phonon frequencies at q */
+  void* stream;        /* cudaStream_t */
+} epb_kbatch_payload;
+
+/* One calculator: calculator_begin!/end!(OuterIteration) and run_calculator!(::EPDataKBatched)
+   (src/calculator/AbstractCalculator.jl). A non-zero return aborts the loop with EPB_ERR_ARG. */
+typedef struct epb_outer_q_calc {
+  int (*begin_q)(void* user, int64_t iq, void* stream);
+  int (*run_batch)(void* user, const epb_kbatch_payload* p);
+  int (*end_q)(void* user, int64_t iq, void* stream);
+  void* user;
+} epb_outer_q_calc;
+
+/* xk_host (3 x nk), wtk_host (nk, NULL: 1), xq_host (3 x nq) on the host; stats_host (4): kept k, k batch,
+   q chunk, batches. */
+EPB_API int epb_eph_outer_q(epb_ctx* ctx, epb_model* model, const double* xk_host, const double* wtk_host, int64_t nk,
+                            const double* xq_host, int64_t nq, const epb_outer_q_params* params,
+                            const epb_outer_q_calc* calcs, int ncalc, double* A_out, int64_t* stats_host);
+
 /* ---- calculator hooks of the batched loop -------------------------------------------------- */
 /* Window scatter of one batch into a device-resident calculator buffer: for every (m, n, nu, j) of
    g2vals (nbandkq, nbandk, nm, nq_batch), i = imap_i_col[n], f = imap_f[m, ikqs[j]] (Int64, 1-based,

@@ -251,6 +251,46 @@ def get_eph_Rq_to_kq_batched(g_Rq, irvec_el, xks, uks, ukqs, nmodes):
     return np.asfortranarray(np.einsum("imk,ijak,jnk->mnak", ukqs.conj(), g, uks))
 
 
+def outer_q_record(model, xks, xqs, wtk=None, window_k=(-np.inf, np.inf), window_kq=(-np.inf, np.inf),
+                   phonon_basis="eigenmode"):
+    """A[iq] = sum_k wtk[k] sum_{m in window_kq(k+q), n in window_k(k), nu} |ep[m, n, nu]|^2 through the
+    per-point outer-q chain (`src/wannier_to_bloch.jl:277-350`); k with an empty window_k range are
+    dropped (`src/filter.jl:40-72`). The record calculator of test/test_gpu.jl:589-654."""
+    nw, nm = model.nw, model.nmodes
+    ham, ep = model.el_ham, model.epmat
+    nr_el, nr_ep = ep.irvec.shape[0], ep.irvec_next.shape[0]
+    op_ph = epmat_el_to_ph(ep.op_r, nw, nm, nr_el, nr_ep)
+    xks = np.asarray(xks, dtype=np.float64).reshape(3, -1)
+    xqs = np.asarray(xqs, dtype=np.float64).reshape(3, -1)
+    nk, nq = xks.shape[1], xqs.shape[1]
+    w = np.ones(nk) if wtk is None else np.asarray(wtk, dtype=np.float64)
+    hk = fourier_batched(ham.op_r, ham.ndata, ham.irvec, xks).reshape(nw, nw, nk, order="F")
+    Ek, Uk = eigen_batched(hk)
+    A = np.zeros(nq)
+    for iq in range(nq):
+        xq = xqs[:, iq]
+        if phonon_basis == "eigenmode":
+            _, u = ph_eigen_batched(xq.reshape(3, 1), model.ph_dyn.op_r, model.ph_dyn.irvec, model.mass)
+            uph = u[:, :, 0]
+        else:
+            uph = np.eye(nm, dtype=np.complex128)
+        gRq = get_eph_RR_to_Rq(op_ph, ep.irvec_next, nw, nm, nr_el, xq, uph)
+        xkq = xks + xq[:, None]
+        hkq = fourier_batched(ham.op_r, ham.ndata, ham.irvec, xkq).reshape(nw, nw, nk, order="F")
+        Ekq, Ukq = eigen_batched(hkq)
+        for k in range(nk):
+            s, t = inside_window(Ek[:, k], *window_k)
+            if t < s:
+                continue
+            s2, t2 = inside_window(Ekq[:, k], *window_kq)
+            if t2 < s2:
+                continue
+            e = get_eph_Rq_to_kq_batched(gRq, ep.irvec, xks[:, k:k + 1], Uk[:, s - 1:t, k:k + 1],
+                                         Ukq[:, s2 - 1:t2, k:k + 1], nm)
+            A[iq] += w[k] * float(np.sum(np.abs(e) ** 2))
+    return A
+
+
 def epstate_set_g2(ep, omega):
     """g2[:,:,nu] = |ep|^2 / (2 omega_nu), no frequency floor; `src/EPState.jl:73-81`."""
     return np.abs(ep) ** 2 * (1.0 / (2.0 * np.asarray(omega)))[None, None, :]

@@ -180,3 +180,173 @@ def test_outerq_edge_cases(B):
         _lib.check(_lib.lib().epb_eph_Rq_to_kq(_lib.default_context().h, _lib.ptr(g), nw, nm,
                                                _lib.RSet(_lib.default_context(), irvec_el).h, _lib.ptr(out), 1,
                                                _lib.ptr(out), nw, _lib.ptr(out), nw, 0, 0, _lib.ptr(out), 0))
+
+
+# ---- the batched outer-q loop (run_eph_over_q_and_k) ---------------------------------------------
+def _outer_k_record(m, xk, xq, window_k, window_kq):
+    """The same gauge-invariant record through the outer-k chain (RR->kR, kR->kq)."""
+    nw, nm = m.nw, m.nmodes
+    ham = m.el_ham
+    A = np.zeros(xq.shape[1])
+    for iq in range(xq.shape[1]):
+        x2 = np.concatenate([xk, xk + xq[:, iq:iq + 1]], 1)
+        hk = O.fourier_batched(ham.op_r, ham.ndata, ham.irvec, x2).reshape(nw, nw, -1, order="F")
+        E, U = O.eigen_batched(hk)
+        _, uph = O.ph_eigen_batched(xq[:, iq:iq + 1], m.ph_dyn.op_r, m.ph_dyn.irvec, m.mass)
+        nk = xk.shape[1]
+        for k in range(nk):
+            s, t = O.inside_window(E[:, k], *window_k)
+            s2, t2 = O.inside_window(E[:, nk + k], *window_kq)
+            if t < s or t2 < s2:
+                continue
+            e = _outer_k(m, xk[:, k], xq[:, iq], U[:, s - 1:t, k], U[:, s2 - 1:t2, nk + k], uph[:, :, 0])
+            A[iq] += np.sum(np.abs(e) ** 2)
+    return A
+
+
+def test_oracle_outer_q_record_matches_outer_k():
+    m = _model(seed=41, nw=8)
+    xk = synth.random_kpoints(12, 1)
+    xq = synth.random_kpoints(3, 2)
+    win_k, win_kq = (-5.0, 3.0), (-8.0, 6.0)
+    A = O.outer_q_record(m, xk, xq, window_k=win_k, window_kq=win_kq)
+    B = _outer_k_record(m, xk, xq, win_k, win_kq)
+    assert np.all(A > 0)
+    np.testing.assert_allclose(A, B, rtol=1e-11)
+
+
+@pytest.fixture(scope="module")
+def P(gpu_lib):
+    from epb200 import outer_q, pipeline
+
+    return outer_q, pipeline
+
+
+class _Record:
+    """The record calculator of test/test_gpu.jl:589-654 on the payload: per q, sum wtk |ep|^2."""
+
+    def __init__(self, nq):
+        import torch
+
+        self.A = np.zeros(nq)
+        self.acc = None
+        self.begins = self.ends = 0
+        self.widths = []
+        self.torch = torch
+
+    def begin_q(self, iq):
+        self.begins += 1
+        self.acc = self.torch.zeros((), dtype=self.torch.float64, device="cuda")
+
+    def run_batch(self, p):
+        self.widths.append(p.nk)
+        self.acc += (p.eps.abs() ** 2 * p.wtk.view(-1, 1, 1, 1)).sum()
+
+    def end_q(self, iq):
+        self.ends += 1
+        self.A[iq] = float(self.acc)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("basis", ["eigenmode", "cartesian"])
+def test_outer_q_loop_fp64(P, basis):
+    """Record A[iq] vs the oracle's per-point outer-q chain (rtol 1e-10; the reference's CPU-vs-GPU bar is
+    1e-8, test/test_gpu.jl:673), with windows on both sides and weights."""
+    outer_q, pipeline = P
+    m = _model(seed=41, nw=8)
+    xk = synth.random_kpoints(37, 1)
+    xq = synth.random_kpoints(4, 2)
+    wtk = np.random.default_rng(0).random(37)
+    win_k, win_kq = (0.0, 1.5), (-8.0, 6.0)
+    dm = pipeline.DeviceModel(m)
+    A, st = outer_q.run_eph_over_q_and_k(dm, xk, xq, wtk=wtk, window_k=win_k, window_kq=win_kq,
+                                         eph_phonon_basis=basis)
+    ref = O.outer_q_record(m, xk, xq, wtk=wtk, window_k=win_k, window_kq=win_kq, phonon_basis=basis)
+    assert 0 < st["kept_k"] < 37
+    np.testing.assert_allclose(A, ref, rtol=1e-10)
+
+
+@pytest.mark.gpu
+def test_outer_q_loop_partial_batches_and_payload(P):
+    """A partial final k batch (nk_batch_max below nk, test/test_gpu.jl:707-715) and a q chunk of 2 give
+    the same record; the Python record calculator over the payload agrees; payload invariants hold."""
+    import torch
+
+    outer_q, pipeline = P
+    m = _model(seed=43, nw=8)
+    nk, nq = 29, 5
+    xk = synth.random_kpoints(nk, 3)
+    xq = synth.random_kpoints(nq, 4)
+    win_k, win_kq = (0.0, 1.5), (-7.0, 5.0)
+    dm = pipeline.DeviceModel(m)
+    A0, st0 = outer_q.run_eph_over_q_and_k(dm, xk, xq, window_k=win_k, window_kq=win_kq)
+    rec = _Record(nq)
+    seen = {}
+
+    class Check:
+        def run_batch(self, p):
+            assert p.eps.shape == (p.nk, m.nmodes, m.nw, m.nw)
+            ik = p.ik.cpu().numpy()
+            assert np.all((ik >= 0) & (ik < nk))
+            np.testing.assert_allclose(p.xks.cpu().numpy().T, xk[:, ik], atol=0)
+            ekq, ukq = p.ekq.cpu().numpy().T, p.ukq.cpu().numpy().T  # (nw, nk), (nw, nw, nk)
+            out = (ekq < win_kq[0]) | (ekq > win_kq[1])
+            for j in range(p.nk):
+                assert np.all(ukq[:, out[:, j], j] == 0)
+            seen.setdefault(p.iq, 0)
+            seen[p.iq] += p.nk
+
+    A1, st1 = outer_q.run_eph_over_q_and_k(dm, xk, xq, window_k=win_k, window_kq=win_kq, calculators=[rec, Check()],
+                                           nk_batch_max=10, q_chunk=2)
+    torch.cuda.synchronize()
+    assert st1["k_batch"] == 10 and st1["q_chunk"] == 2
+    assert rec.begins == nq and rec.ends == nq
+    assert all(v == st1["kept_k"] for v in seen.values()) and len(seen) == nq
+    assert st1["kept_k"] == 13 and sorted(set(rec.widths)) == [3, 10]
+    np.testing.assert_allclose(A1, A0, rtol=1e-12)
+    np.testing.assert_allclose(rec.A, A0, rtol=1e-12)
+    ref = O.outer_q_record(m, xk, xq, window_k=win_k, window_kq=win_kq)
+    np.testing.assert_allclose(A0, ref, rtol=1e-10)
+
+
+@pytest.mark.gpu
+def test_outer_q_loop_mixed(P):
+    """Mixed precision (FP32 + FP64-refined eigensolves, split-BF16 Fourier over Re): record within 1e-5
+    relative of FP64 (the |g|^2 bar of the mixed path)."""
+    from epb200._lib import PREC_MIXED
+
+    outer_q, pipeline = P
+    m = synth.config2_model(seed=44, n_el=2, n_ph=1, nw=16, natom=4)
+    xk = synth.random_kpoints(300, 5)
+    xq = synth.random_kpoints(3, 6)
+    dm = pipeline.DeviceModel(m)
+    A64, _ = outer_q.run_eph_over_q_and_k(dm, xk, xq, window_k=(-5.0, 5.0), window_kq=(-8.0, 8.0))
+    A32, _ = outer_q.run_eph_over_q_and_k(dm, xk, xq, window_k=(-5.0, 5.0), window_kq=(-8.0, 8.0), prec=PREC_MIXED)
+    assert np.max(np.abs(A32 - A64) / np.abs(A64)) <= 1e-5
+
+
+@pytest.mark.gpu
+def test_outer_q_loop_errors(P):
+    """A calculator that raises aborts the loop with its exception; the context stays usable; an empty
+    k window or an empty k list gives zeros; a calculator without run_batch is rejected up front."""
+    outer_q, pipeline = P
+    m = _model(seed=45, nw=4)
+    xk = synth.random_kpoints(8, 7)
+    xq = synth.random_kpoints(2, 8)
+    dm = pipeline.DeviceModel(m)
+
+    class Boom:
+        def run_batch(self, p):
+            raise RuntimeError("calculator failure")
+
+    with pytest.raises(RuntimeError, match="calculator failure"):
+        outer_q.run_eph_over_q_and_k(dm, xk, xq, calculators=[Boom()])
+    with pytest.raises(TypeError):
+        outer_q.run_eph_over_q_and_k(dm, xk, xq, calculators=[object()])
+    A, st = outer_q.run_eph_over_q_and_k(dm, xk, xq, window_k=(100.0, 200.0))
+    assert st["kept_k"] == 0 and np.all(A == 0)
+    A, st = outer_q.run_eph_over_q_and_k(dm, np.zeros((3, 0)), xq)
+    assert np.all(A == 0)
+    A, st = outer_q.run_eph_over_q_and_k(dm, xk, xq)
+    ref = O.outer_q_record(m, xk, xq)
+    np.testing.assert_allclose(A, ref, rtol=1e-10)
