@@ -20,6 +20,10 @@ all eigenvalues + eigenvectors, FP64 and mixed (eigenvalue deviation of the mixe
 window E_F -/+ 0.3 eV around the median of band 8, T = 300 K, Gaussian 10 meV, method 5):
 in-window (k, k+q) pairs per second and the conductivity tensor.
 
+`--workload outerq` measures the batched outer-q loop (run_eph_over_q_and_k) on the config-2 model:
+8192 random k x 64 random q, all bands, eigenmode basis, the per-q gauge-invariant record as the only
+consumer: g(k,q,nu) elements per second (nk nq nw^2 nm per step), mixed and FP64.
+
 `--workload eigh` measures the uneven batched eigensolve (config 3: 1,000,000 Hermitian matrices,
 n uniform in {4, 8, ..., 96}, 5 % with planted 2-4-fold clusters spaced 1e-10, eigenvalues and
 eigenvectors, FP32 solve + FP64 refinement): matrices per second.
@@ -66,7 +70,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-nk", type=int, default=16)
     ap.add_argument("--cpu-nq", type=int, default=1024)
-    ap.add_argument("--workload", default="pass", choices=["pass", "filter", "eigh", "bands", "bte"])
+    ap.add_argument("--workload", default="pass", choices=["pass", "filter", "eigh", "bands", "bte", "outerq"])
     ap.add_argument("--count", type=int, default=1_000_000, help="eigh workload: matrices per batch")
     ap.add_argument("--grid", type=int, default=96, help="filter workload: k grid per axis")
     ap.add_argument("--decay", type=float, default=1.5, help="filter workload: H(R) decay length")
@@ -673,6 +677,41 @@ def run_bte(args):
     torch.cuda.synchronize()
     ms64 = e0.elapsed_time(e1)
     rel = float(np.max(np.abs(sig - sig64)) / np.abs(sig64).max())
+    # roofline of the dominant family (total algorithmic flops of one step / its total device time)
+    peaks, peak_src = measured_peaks()
+    tot = sum(v[0] for v in prof.values())
+    for k in profile:
+        profile[k]["share"] = round(profile[k]["ms"] / tot, 4)
+    dom_name, (dom_ms, dom_cnt) = max(prof.items(), key=lambda kv: kv[1][0])
+    nm, nr_el, nr_ep = 3 * NATOM, (2 * N_EL + 1) ** 3, (2 * N_PH + 1) ** 3
+    W = max(int(st["width"]), 1)
+    roof = None
+    if dom_name == "zgemm":   # kR->kq per kept k: (nw W nm) x nr_ep x pairs of that k, FP64
+        flops = 8.0 * NW * W * nm * nr_ep * st["pairs"]
+        peak, psrc = measure_fp64_peak(torch), "measured live: cuBLAS DGEMM 8192^3"
+    elif dom_name == "umma_rr":  # RR->kR over Re for the kept k, split BF16x3
+        flops = 8.0 * NW * W * nm * nr_ep * nr_el * st["kept_k"]
+        peak, psrc = peaks["bf16_tflops_sustained"] / 6, f"{peak_src} bf16 sustained / 6 split products"
+    else:
+        flops = None
+    if flops is not None and dom_cnt:
+        ach = flops / (dom_ms * 1e-3) / 1e12
+        roof = {"bound": "tensor", "kernel": dom_name, "achieved": round(ach, 3), "peak": round(peak, 2),
+                "unit": "TFLOP/s", "frac": round(ach / peak, 4), "traffic": None, "peak_source": psrc,
+                "launch_ms": round(dom_ms / dom_cnt, 4), "launches_per_step": dom_cnt,
+                "algorithmic_flops_per_step": flops}
+    cpu = None
+    if not args.no_cpu:
+        mh = m_host_for_cpu(m, ep_dev)
+        cng = 16
+        t0 = time.perf_counter()
+        _, _, info = BO.serta(mh, cng, ef - half, ef + half, ef, T, eta, method=5)
+        dt = time.perf_counter() - t0
+        cores = int(os.environ.get("OPENBLAS_NUM_THREADS", os.cpu_count() or 1))
+        cpu = {"value": info["npairs"] / dt, "unit": "pairs/s", "cores": cores, "kind": "port",
+               "sample": f"the same model and window on a {cng}^3 k = q grid ({len(info['kept'])} kept k, "
+                         f"{info['npairs']} pairs), {dt:.1f} s; numpy/scipy per-pair chain"}
+        del mh
     line = {"metric": BTE_METRIC, "value": st["pairs"] / (ms * 1e-3), "unit": "pairs/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3/f64" if kw["prec"] == 1 else "f64",
@@ -680,8 +719,142 @@ def run_bte(args):
             "config": {"workload": f"config5 SERTA: nw=16, nm=12, Re 9^3, Rp 5^3, {ng}^3 k = q grids, window E_F -/+ 0.3 eV, "
                                    "T = 300 K, Gaussian 10 meV, method 5", "e_fermi_ry": ef, **st},
             "sigma": sig.tolist(), "sigma_fp64": sig64.tolist(), "sigma_max_rel_dev_vs_fp64": rel,
-            "fp64_ms_per_step": round(ms64, 3), "speedup_vs_fp64": round(ms64 / ms, 3), "roofline": None, "cpu_baseline": None, "gpu_launches": launches,
+            "fp64_ms_per_step": round(ms64, 3), "speedup_vs_fp64": round(ms64 / ms, 3), "roofline": roof, "cpu_baseline": cpu,
+            "e2e": {"value": st["pairs"] / (ms * 1e-3), "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 72,
+                    "note": "the public call takes the grid size and returns sigma (9 doubles) to the host"},
+            "gpu_launches": launches,
             "clocks": clocks, "impl": "epb", "profile_one_step": profile}
+    print(json.dumps(line), flush=True)
+
+
+OUTERQ_METRIC = "g(k,q,ν) elems/s of the batched outer-q loop, nw=16 config-2 model, all bands"
+
+
+def outerq_family_work(name, nk, nq, kb, nd, nr_el, nr_ep):
+    """Algorithmic (flops, bytes) of one outer-q step for a profiler family (8 real flops per complex MAC).
+
+    umma_kq / umma_h / umma_rr (mixed): g(k, q) over Re (nd x nr_el x nk per q), H(k+q) (nw^2 x nr_el x nk
+    per q), RR->Rq (nd nr_el x nr_ep x nq); fourier_f64 (FP64 mode): H(k+q) + RR->Rq + the k / q states;
+    rotation: g(k, q) block (16 nd bytes) + two nw^2 eigenvector blocks in, 16 nw^3 nm flops per k and q."""
+    nw2 = NW * NW
+    nm = 3 * NATOM
+    if name == "umma_kq":   # g(k, q) of the mixed mode
+        return 8.0 * nd * nr_el * nk * nq, None
+    if name == "umma_h":    # H(k+q) of the mixed mode
+        return 8.0 * nw2 * nr_el * nk * nq, None
+    if name == "umma_rr":   # RR->Rq of the mixed mode
+        return 8.0 * nd * nr_el * nr_ep * nq, None
+    if name == "fourier_f64":
+        return 8.0 * (nw2 * nr_el * nk * nq + nd * nr_el * nr_ep * nq + nw2 * nr_el * nk), None
+    if name == "rotation":
+        return 16.0 * NW ** 3 * nm * nk * nq, (16.0 * nd + 32.0 * nw2) * nk * nq
+    return None, None
+
+
+def run_outerq(args):
+    import torch
+
+    from epb200 import outer_q, pipeline, synth
+    from oracle import epb_oracle as O
+
+    torch.cuda.set_device(0)
+    nk = args.nk if args.nk != NK else 8192
+    nq = args.nq if args.nq != NQ else 64
+    m = build_model_host_small()
+    ep_dev = synth.epmat_el_device(SEED, NW, 3 * NATOM, m.el_ham.irvec, synth.irvec_box(N_PH))
+    m.epmat = synth.device_epmat_object(ep_dev, m.el_ham.irvec, synth.irvec_box(N_PH))
+    dm = pipeline.DeviceModel(m)
+    xks = synth.random_kpoints(nk, 3000)
+    xqs = synth.random_kpoints(nq, 4000)
+    nm, nr_el, nr_ep = 3 * NATOM, (2 * N_EL + 1) ** 3, (2 * N_PH + 1) ** 3
+    nd = NW * NW * nm
+    n_el = nk * nq * NW * NW * nm
+    prec = pipeline.PREC_FP64 if args.prec == "fp64" else pipeline.PREC_MIXED
+    kw = dict(prec=prec, nk_batch_max=args.k_batch if args.k_batch > 0 else 0)
+
+    def step(p=prec):
+        return outer_q.run_eph_over_q_and_k(dm, xks, xqs, **dict(kw, prec=p))
+
+    for _ in range(args.warmup):
+        A, st = step()
+    torch.cuda.synchronize()
+    clk = clocks_start()
+    l0 = dm.ctx.launch_count()
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(args.steps):
+        A, st = step()
+    e1.record(s)
+    torch.cuda.synchronize()
+    clocks = clocks_stop(clk, 0)
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = dm.ctx.launch_count() - l0
+    dm.ctx.profile(True)
+    step()
+    torch.cuda.synchronize()
+    prof = dm.ctx.profile_read(reset=True)
+    dm.ctx.profile(False)
+    tot = sum(v[0] for v in prof.values())
+    profile = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / tot, 4)} for k, v in prof.items() if v[1]}
+    # FP64 on the same inputs: time and the record deviation of the mixed path
+    e0.record(s)
+    A64, _ = step(pipeline.PREC_FP64)
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms64 = e0.elapsed_time(e1)
+    rel = float(np.max(np.abs(A - A64) / np.abs(A64)))
+
+    peaks, peak_src = measured_peaks()
+    dom_name, (dom_ms, dom_cnt) = max(prof.items(), key=lambda kv: kv[1][0])
+    flops, nbytes = outerq_family_work(dom_name, nk, nq, st["k_batch"], nd, nr_el, nr_ep)
+    roof = None
+    if flops is not None and dom_cnt:
+        t = dom_ms * 1e-3
+        if dom_name.startswith("umma"):
+            peak, psrc, bound = peaks["bf16_tflops_sustained"] / 6, f"{peak_src} bf16 sustained / 6 split products", "tensor"
+        elif dom_name == "rotation":
+            peak, psrc, bound = None, None, "hbm"
+        else:
+            peak, psrc, bound = measure_fp64_peak(torch), "measured live: cuBLAS DGEMM 8192^3", "tensor"
+        if bound == "hbm":
+            ach = nbytes / t / 1e9
+            roof = {"bound": "hbm", "kernel": dom_name, "achieved": round(ach, 2), "peak": peaks["hbm_gbs"],
+                    "unit": "GB/s", "frac": round(ach / peaks["hbm_gbs"], 5), "traffic": None,
+                    "peak_source": f"{peak_src} hbm copy"}
+        else:
+            ach = flops / t / 1e12
+            roof = {"bound": bound, "kernel": dom_name, "achieved": round(ach, 3), "peak": round(peak, 2),
+                    "unit": "TFLOP/s", "frac": round(ach / peak, 4), "traffic": None, "peak_source": psrc}
+        roof.update({"launch_ms": round(dom_ms / dom_cnt, 4), "launches_per_step": dom_cnt,
+                     "algorithmic_work_per_step": flops if bound != "hbm" else nbytes})
+
+    cpu = None
+    if not args.no_cpu:
+        # the oracle's per-point outer-q chain on a bounded sample of the same workload
+        mh = m_host_for_cpu(m, ep_dev)
+        cnk, cnq = min(256, nk), 2
+        t0 = time.perf_counter()
+        Ac = O.outer_q_record(mh, xks[:, :cnk], xqs[:, :cnq])
+        dt = time.perf_counter() - t0
+        cores = int(os.environ.get("OPENBLAS_NUM_THREADS", os.cpu_count() or 1))
+        cpu = {"value": cnk * cnq * NW * NW * nm / dt, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{cnk} k x {cnq} q of the same model (all bands), {dt:.1f} s; numpy/scipy per-point "
+                         "outer-q chain (RR->Rq per q, Rq->kq per k, ZHEEV)"}
+        del mh
+    line = {"metric": OUTERQ_METRIC, "value": n_el / (ms * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16x3/f32/f64" if prec == pipeline.PREC_MIXED else "f64",
+            "data": "synthetic (seeded config-2 model; g(Re,Rp) generated on the device)",
+            "config": {"workload": f"outer-q loop: nw=16, nm=12, Re 9^3, Rp 5^3, {nk} random k x {nq} random q, "
+                                   "all bands, eigenmode basis, record consumer", **st,
+                       "l2": "inputs larger than L2 (g(Re,Rp) 4.48 GB re-read per q chunk)"},
+            "record_max_rel_dev_vs_fp64": rel, "fp64_ms_per_step": round(ms64, 3),
+            "speedup_vs_fp64": round(ms64 / ms, 3), "roofline": roof, "cpu_baseline": cpu,
+            "e2e": {"value": n_el / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 24 * (nk + nq),
+                    "d2h_bytes_per_step": 8 * nq, "note": "the public call takes host k / q lists and returns "
+                                                          "the host record; the timed step is that call"},
+            "gpu_launches": launches, "clocks": clocks, "impl": "epb", "profile_one_step": profile}
     print(json.dumps(line), flush=True)
 
 
@@ -903,6 +1076,8 @@ if __name__ == "__main__":
         run_bands(a)
     elif a.workload == "bte":
         run_bte(a)
+    elif a.workload == "outerq":
+        run_outerq(a)
     elif a.workload == "filter":
         if a.nq == NQ:
             a.nq = 8192

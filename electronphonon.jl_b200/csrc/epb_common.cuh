@@ -180,6 +180,7 @@ struct epb_model {
   void* mixed = nullptr;
   PassGraph graph;  // graph mode of epb_eph_pass
   double2* epmat_ph = nullptr;  // owned "ph"-layout copy of epmat (outer-q loop), made on first use
+  uint8_t* epmat_ph_planes = nullptr;  // owned split-BF16 planes of epmat_ph (mixed outer-q loop)
 };
 
 namespace epb {

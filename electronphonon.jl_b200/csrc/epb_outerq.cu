@@ -6,6 +6,7 @@
 // plus the conversion of the e-ph matrix from the "el" layout (rows (i, j, nu, Rp), columns Re) to
 // the "ph" layout (rows (i, j, nu, Re), columns Rp) (src/model.jl:80-81,293-296, src/model_new.jl:551-565).
 #include <algorithm>
+#include <type_traits>
 
 #include "epb_common.cuh"
 
@@ -18,6 +19,13 @@ int fourier_mixed(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, const 
 int eigh_async(epb_ctx* ctx, double2* A, int64_t n, int64_t batch, double* E, bool want_v, const double* mass,
                int prec);
 int eigh_check(epb_ctx* ctx);
+int split_gemm_check(epb_ctx* ctx);
+int64_t oq_a_bytes(int64_t M, int64_t K);
+int64_t oq_b_bytes(int64_t N, int64_t K);
+int oq_pack_a(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, int64_t K, uint8_t* mem);
+int oq_pack_b(epb_ctx* ctx, const epb_rset* rs, const double* x, int64_t N, uint8_t* mem);
+int oq_gemm(epb_ctx* ctx, int prof_id, const uint8_t* a_mem, int64_t M, int64_t K, const uint8_t* b_mem, int64_t N,
+            int64_t n0, int64_t nn, float2* C, int64_t ldc);
 int window_filter(epb_ctx* ctx, const double* E, int64_t nw, int64_t nk, double wmin, double wmax, int32_t* bmin,
                   int32_t* bmax, int32_t* keep_idx, int64_t* nkeep, double* nbelow);
 
@@ -36,16 +44,20 @@ static unsigned grid_oq(epb_ctx* ctx, int64_t n) {
 
 // out[b, ir, q] (b = (i, j) pair, ir = Re) with the mode index rotated:
 // out[(ij, nu), ir, q] = sum_mu g[(ij, mu), ir, q] uph[mu, nu, q].
-__global__ void rq_mode_rotate_kernel(const double2* __restrict__ g, const double2* __restrict__ uph, int64_t nb,
+__device__ __forceinline__ double2 as_c128(double2 v) { return v; }
+__device__ __forceinline__ double2 as_c128(float2 v) { return make_double2(v.x, v.y); }
+
+template <typename G>
+__global__ void rq_mode_rotate_kernel(const G* __restrict__ g, const double2* __restrict__ uph, int64_t nb,
                                       int64_t nm, int64_t nr, int64_t nq, double2* __restrict__ out) {
   const int64_t total = nb * nm * nr * nq;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
     const int64_t b = e % nb, nu = (e / nb) % nm, rq = e / (nb * nm);  // rq = ir + nr q
     const int64_t q = rq / nr;
-    const double2* gp = g + rq * nb * nm + b;
+    const G* gp = g + rq * nb * nm + b;
     const double2* up = uph + q * nm * nm + nu * nm;
     double2 acc = make_double2(0.0, 0.0);
-    for (int64_t mu = 0; mu < nm; ++mu) cfma(acc, gp[mu * nb], up[mu]);
+    for (int64_t mu = 0; mu < nm; ++mu) cfma(acc, as_c128(gp[mu * nb]), up[mu]);
     out[e] = acc;
   }
 }
@@ -130,6 +142,11 @@ __global__ void oq_mask_kernel(double2* __restrict__ U, const double* __restrict
   }
 }
 
+__global__ void oq_widen_kernel(const float2* __restrict__ in, int64_t n, double2* __restrict__ out) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+    out[e] = make_double2(in[e].x, in[e].y);
+}
+
 __global__ void oq_identity_kernel(double2* __restrict__ u, int nm, int64_t nq) {
   const int64_t nm2 = (int64_t)nm * nm;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nq * nm2; e += (int64_t)gridDim.x * blockDim.x) {
@@ -201,6 +218,90 @@ __global__ void __launch_bounds__(OQ_ROT_THREADS) oq_rot_kernel(const double2* _
   }
 }
 
+// nw <= 16: the whole g(k) block (nm x nw columns of nw, padded to nw + 1) is staged once; thread (m, jw)
+// forms T[m, jw, nu] = sum_iw conj(ukq[iw, m]) g[iw, jw, nu] for OQ_NC modes at a time in registers and,
+// after a barrier, writes T over the g columns it came from (only threads of the same column read them);
+// then thread (m, n) forms ep[m, n, nu] = sum_jw T[m, jw, nu] uk[jw, n] for every nu. One global read of
+// g(k), no per-mode round trips. Same outputs as oq_rot_kernel.
+constexpr int OQ_NC = 4;
+template <typename C> __device__ __forceinline__ C to_c(double2 v);
+template <> __device__ __forceinline__ double2 to_c<double2>(double2 v) { return v; }
+template <> __device__ __forceinline__ float2 to_c<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
+template <typename C> __device__ __forceinline__ C to_c(float2 v);
+template <> __device__ __forceinline__ double2 to_c<double2>(float2 v) { return make_double2(v.x, v.y); }
+template <> __device__ __forceinline__ float2 to_c<float2>(float2 v) { return v; }
+
+// C = double2: FP64 throughout; C = float2: FP32 arithmetic (the mixed mode, whose g(k, q) is FP32-level).
+template <bool STORE, typename G, typename C>
+__global__ void __launch_bounds__(OQ_ROT_THREADS, sizeof(C) == 8 ? 4 : 2) oq_rot_block_kernel(
+    const G* __restrict__ g, const double2* __restrict__ uk, const double2* __restrict__ ukq,
+    const double* __restrict__ wtk, int nw, int nm, int64_t nk, double2* __restrict__ ep, double* __restrict__ part) {
+  extern __shared__ __align__(16) unsigned char oq_smb[];
+  C* oq_sm = reinterpret_cast<C*>(oq_smb);
+  const int L = nw + 1, nw2 = nw * nw, ncol = nm * nw;
+  C* sq = oq_sm;        // sq[m * L + iw] = conj(ukq[iw, m])
+  C* sk = sq + nw * L;  // sk[n * L + jw] = uk[jw, n]
+  C* sg = sk + nw * L;  // sg[(nu * nw + jw) * L + iw] = g[iw, jw, nu], later T[iw := m]
+  __shared__ double red[OQ_ROT_THREADS / 32];
+  const int t = threadIdx.x;
+  const int m = t % nw, c = t / nw;  // (m, jw) in the T stage, (m, n) in the ep stage
+  const bool act = t < nw2;
+  for (int64_t k = blockIdx.x; k < nk; k += gridDim.x) {
+    const double2* uq = ukq + k * nw2;
+    const double2* ukk = uk + k * nw2;
+    const G* gk = g + k * (int64_t)nw2 * nm;
+    for (int e = t; e < nw2; e += blockDim.x) {
+      const int i = e % nw, j = e / nw;
+      const double2 a = uq[e];
+      sq[j * L + i] = to_c<C>(make_double2(a.x, -a.y));
+      sk[j * L + i] = to_c<C>(ukk[e]);
+    }
+    for (int e = t; e < ncol * nw; e += blockDim.x) sg[(e / nw) * L + (e % nw)] = to_c<C>(gk[e]);
+    __syncthreads();
+    for (int nu0 = 0; nu0 < nm; nu0 += OQ_NC) {
+      C tv[OQ_NC];
+#pragma unroll
+      for (int r = 0; r < OQ_NC; ++r) tv[r] = to_c<C>(make_double2(0.0, 0.0));
+      if (act) {
+        const C* a = sq + m * L;
+        for (int iw = 0; iw < nw; ++iw) {
+          const C av = a[iw];
+#pragma unroll
+          for (int r = 0; r < OQ_NC; ++r)
+            if (nu0 + r < nm) cfma(tv[r], av, sg[((nu0 + r) * nw + c) * L + iw]);
+        }
+      }
+      __syncthreads();
+      if (act) {
+#pragma unroll
+        for (int r = 0; r < OQ_NC; ++r)
+          if (nu0 + r < nm) sg[((nu0 + r) * nw + c) * L + m] = tv[r];
+      }
+    }
+    __syncthreads();
+    double acc2 = 0.0;
+    if (act) {
+      const C* b = sk + c * L;
+      for (int nu = 0; nu < nm; ++nu) {
+        const C* tc = sg + (nu * nw) * L + m;
+        C v = to_c<C>(make_double2(0.0, 0.0));
+        for (int jw = 0; jw < nw; ++jw) cfma(v, tc[jw * L], b[jw]);
+        const double vx = v.x, vy = v.y;
+        if (STORE) ep[(k * nm + nu) * nw2 + t] = make_double2(vx, vy);
+        acc2 += vx * vx + vy * vy;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) acc2 += __shfl_xor_sync(0xffffffffu, acc2, o);
+    if ((t & 31) == 0) red[t >> 5] = acc2;
+    __syncthreads();
+    if (t == 0) {
+      double s = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+      part[k] = wtk[k] * s;
+    }
+  }
+}
+
 // A[iq] += sum_k part[k], one block, fixed order (deterministic).
 __global__ void oq_record_kernel(const double* __restrict__ part, int64_t nk, double* __restrict__ A) {
   __shared__ double red[256];
@@ -217,8 +318,32 @@ __global__ void oq_record_kernel(const double* __restrict__ part, int64_t nk, do
 
 static size_t oq_rot_smem(int nw) { return (size_t)4 * nw * (nw + 1) * sizeof(double2); }
 
-static int oq_rotate(epb_ctx* ctx, const double2* g, const double2* uk, const double2* ukq, const double* wtk, int nw,
+// G = float2 (mixed mode): FP32 arithmetic; G = double2: FP64.
+template <typename G>
+static int oq_rotate(epb_ctx* ctx, const G* g, const double2* uk, const double2* ukq, const double* wtk, int nw,
                      int nm, int64_t nk, double2* ep, double* part) {
+  if (nw <= 16) {
+    using C = G;
+    const size_t smb = (size_t)(2 + nm) * nw * (nw + 1) * sizeof(C);
+    if (smb > 48 * 1024) {
+      EPB_CUDA(cudaFuncSetAttribute(oq_rot_block_kernel<true, G, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb));
+      EPB_CUDA(cudaFuncSetAttribute(oq_rot_block_kernel<false, G, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb));
+    }
+    const int per_sm = sizeof(C) == 8 ? 4 : 2;
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nk, (int64_t)ctx->sm_count * per_sm));
+    prof_begin(ctx, EPB_PROF_ROT);
+    if (ep)
+      oq_rot_block_kernel<true, G, C><<<grid, OQ_ROT_THREADS, smb, ctx->stream>>>(g, uk, ukq, wtk, nw, nm, nk, ep, part);
+    else
+      oq_rot_block_kernel<false, G, C><<<grid, OQ_ROT_THREADS, smb, ctx->stream>>>(g, uk, ukq, wtk, nw, nm, nk, ep, part);
+    prof_end(ctx);
+    EPB_LAUNCH_CHECK();
+    return EPB_OK;
+  }
+  if constexpr (!std::is_same<G, double2>::value) {
+    set_error("oq_rotate: complex64 g needs nw <= 16");
+    return EPB_ERR_ARG;
+  } else {
   const size_t sm = oq_rot_smem(nw);
   if (sm > 48 * 1024) {
     EPB_CUDA(cudaFuncSetAttribute(oq_rot_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -233,6 +358,7 @@ static int oq_rotate(epb_ctx* ctx, const double2* g, const double2* uk, const do
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
+  }
 }
 
 }  // namespace epb
@@ -274,7 +400,7 @@ int epb_eph_RR_to_Rq(epb_ctx* ctx, const double* epmat_ph, int64_t nw, int64_t n
     const int64_t qn = std::min(qc, nq - q0);
     EPB_TRY(fourier_rows(ctx, (const double2*)epmat_ph, ndata, ndata, rset_ph, xq + 3 * q0, qn, g, ndata));
     prof_begin(ctx, EPB_PROF_RR_ROT);
-    rq_mode_rotate_kernel<<<grid_oq(ctx, ndata * qn), 256, 0, ctx->stream>>>(
+    rq_mode_rotate_kernel<double2><<<grid_oq(ctx, ndata * qn), 256, 0, ctx->stream>>>(
         g, (const double2*)uph + q0 * nm * nm, nb, nm, nr_el, qn, (double2*)out + q0 * ndata);
     prof_end(ctx);
     EPB_LAUNCH_CHECK();
@@ -421,45 +547,94 @@ int epb_eph_outer_q(epb_ctx* ctx, epb_model* m, const double* xk_host, const dou
   const int64_t KB = std::max<int64_t>(1, std::min<int64_t>(nkeep, prm->k_batch > 0 ? prm->k_batch : 4096));
   const int64_t per_q = 16 * nd * nr_el;
   const int64_t QC = std::max<int64_t>(
-      1, std::min<int64_t>(nq, prm->q_chunk > 0 ? prm->q_chunk : std::max<int64_t>(1, ((int64_t)1 << 30) / per_q)));
+      1, std::min<int64_t>(nq, prm->q_chunk > 0 ? prm->q_chunk : std::max<int64_t>(1, ((int64_t)1 << 31) / per_q)));
   if (stats_host) {
     stats_host[0] = nkeep;
-    stats_host[1] = KB;
+    stats_host[1] = (prec == EPB_PREC_MIXED && nkeep > KB) ? (KB + 127) / 128 * 128 : KB;
     stats_host[2] = QC;
   }
+  const bool mixed = prec == EPB_PREC_MIXED;
+  // per-run / per-q buffers: g(Re, q) of a chunk (and its mode rotation); in the mixed mode the packed
+  // split-BF16 operands that live across batches: H(R) (per run), the phases of every kept k (per run),
+  // g(Re, q) of the current q
+  size_t off1 = 0;
+  auto take1 = [&](size_t bytes) {
+    size_t o = off1;
+    off1 += (bytes + 1023) & ~size_t(1023);
+    return o;
+  };
+  const size_t o_Gq = take1((size_t)per_q * QC),
+               o_Grq = (prm->phonon_basis == 0 || mixed) ? take1((size_t)per_q * QC) : o_Gq,
+               o_ah = mixed ? take1(oq_a_bytes(nw2, nr_el)) : 0,
+               o_bk = mixed && nkeep > 0 ? take1(oq_b_bytes(nkeep, nr_el)) : 0,
+               o_ag = mixed ? take1(oq_a_bytes(nd, nr_el)) : 0, o_bq = mixed ? take1(oq_b_bytes(QC, m->nr_ep)) : 0;
   void* ws1 = nullptr;
-  EPB_TRY(ws_get(ctx, EPB_WS_OQ1, (size_t)per_q * QC * (prm->phonon_basis == 0 ? 2 : 1) + 256, &ws1));
-  double2* Gq = (double2*)ws1;                                       // Fourier over Rp, (nd nr_el, QC)
-  double2* Grq = prm->phonon_basis == 0 ? Gq + nd * nr_el * QC : Gq;  // after the mode rotation
+  EPB_TRY(ws_get(ctx, EPB_WS_OQ1, off1 + 1024, &ws1));
+  uint8_t* b1 = (uint8_t*)(((uintptr_t)ws1 + 1023) & ~uintptr_t(1023));
+  double2* Gq = (double2*)(b1 + o_Gq);    // Fourier over Rp, (nd nr_el, QC)
+  double2* Grq = (double2*)(b1 + o_Grq);  // after the mode rotation
+  uint8_t* a_h = b1 + o_ah;
+  uint8_t* b_k = b1 + o_bk;
+  uint8_t* a_g = b1 + o_ag;
+  uint8_t* b_q = b1 + o_bq;
+  if (mixed && !m->epmat_ph_planes) {  // split-BF16 planes of the "ph"-layout epmat, once per model
+    EPB_CUDA(cudaMalloc(&m->epmat_ph_planes, (size_t)oq_a_bytes(nd * nr_el, m->nr_ep)));
+    EPB_TRY(oq_pack_a(ctx, m->epmat_ph, nd * nr_el, nd * nr_el, m->nr_ep, m->epmat_ph_planes));
+  }
+  // per-batch buffers; the mixed mode keeps a multiple of 128 k per batch (packed phase tiles)
+  const int64_t KBm = (mixed && nkeep > KB) ? (KB + 127) / 128 * 128 : KB;
   size_t off2 = 0;
   auto take2 = [&](size_t bytes) {
     size_t o = off2;
-    off2 += (bytes + 255) & ~size_t(255);
+    off2 += (bytes + 1023) & ~size_t(1023);
     return o;
   };
-  const size_t o_xkq = take2(24 * KB), o_H = take2(16 * nw2 * KB), o_Ekq = take2(8 * nw * KB),
-               o_g = take2(16 * nd * KB), o_ep = take2(ncalc > 0 ? 16 * nd * KB : 0), o_part = take2(8 * KB);
+  const size_t o_xkq = take2(24 * KBm), o_H = take2(16 * nw2 * KBm), o_Ekq = take2(8 * nw * KBm),
+               o_g = take2((mixed ? 8 : 16) * nd * KBm), o_ep = take2(ncalc > 0 ? 16 * nd * KBm : 0),
+               o_part = take2(8 * KBm), o_bh = mixed ? take2(oq_b_bytes(KBm, nr_el)) : 0,
+               o_ch = mixed ? take2(8 * nw2 * KBm) : 0, o_gw = mixed && nw > 16 ? take2(16 * nd * KBm) : 0;
   void* ws2 = nullptr;
-  EPB_TRY(ws_get(ctx, EPB_WS_OQ2, off2 + 256, &ws2));
-  uint8_t* b2 = (uint8_t*)ws2;
+  EPB_TRY(ws_get(ctx, EPB_WS_OQ2, off2 + 1024, &ws2));
+  uint8_t* b2 = (uint8_t*)(((uintptr_t)ws2 + 1023) & ~uintptr_t(1023));
   double* xkq = (double*)(b2 + o_xkq);
   double2* Hkq = (double2*)(b2 + o_H);
   double* Ekq = (double*)(b2 + o_Ekq);
   double2* gk = (double2*)(b2 + o_g);
+  float2* gk32 = (float2*)(b2 + o_g);
   double2* ep = ncalc > 0 ? (double2*)(b2 + o_ep) : nullptr;
   double* part = (double*)(b2 + o_part);
+  uint8_t* b_h = b2 + o_bh;
+  float2* ch = (float2*)(b2 + o_ch);
+  if (mixed) {
+    EPB_TRY(oq_pack_a(ctx, m->ham, nw2, nw2, nr_el, a_h));
+    if (nkeep > 0) EPB_TRY(oq_pack_b(ctx, m->rs_el, xkk, nkeep, b_k));
+  }
 
   int64_t nbatches = 0;
   for (int64_t q0 = 0; q0 < nq; q0 += QC) {
     const int64_t qn = std::min(QC, nq - q0);
     // g(Re, q) = sum_Rp e^{2 pi i q.Rp} g(Re, Rp) for the chunk, then the mode rotation
-    EPB_TRY(fourier_rows(ctx, m->epmat_ph, nd * nr_el, nd * nr_el, m->rs_ep, xq_d + 3 * q0, qn, Gq, nd * nr_el));
-    if (prm->phonon_basis == 0) {
+    if (mixed) {  // split-BF16 tensor cores: complex64 g(Re, q), widened by the mode rotation (or a copy)
+      float2* G32 = (float2*)Gq;
+      EPB_TRY(oq_pack_b(ctx, m->rs_ep, xq_d + 3 * q0, qn, b_q));
+      EPB_TRY(oq_gemm(ctx, EPB_PROF_UMMA_RR, m->epmat_ph_planes, nd * nr_el, m->nr_ep, b_q, qn, 0, qn, G32, nd * nr_el));
       prof_begin(ctx, EPB_PROF_RR_ROT);
-      rq_mode_rotate_kernel<<<grid_oq(ctx, nd * nr_el * qn), 256, 0, ctx->stream>>>(Gq, uph + q0 * nmm, nw2, nm, nr_el,
-                                                                                  qn, Grq);
+      if (prm->phonon_basis == 0)
+        rq_mode_rotate_kernel<float2><<<grid_oq(ctx, nd * nr_el * qn), 256, 0, ctx->stream>>>(
+            G32, uph + q0 * nmm, nw2, nm, nr_el, qn, Grq);
+      else
+        oq_widen_kernel<<<grid_oq(ctx, nd * nr_el * qn), 256, 0, ctx->stream>>>(G32, nd * nr_el * qn, Grq);
       prof_end(ctx);
       EPB_LAUNCH_CHECK();
+    } else {
+      EPB_TRY(fourier_rows(ctx, m->epmat_ph, nd * nr_el, nd * nr_el, m->rs_ep, xq_d + 3 * q0, qn, Gq, nd * nr_el));
+      if (prm->phonon_basis == 0) {
+        prof_begin(ctx, EPB_PROF_RR_ROT);
+        rq_mode_rotate_kernel<double2><<<grid_oq(ctx, nd * nr_el * qn), 256, 0, ctx->stream>>>(
+            Gq, uph + q0 * nmm, nw2, nm, nr_el, qn, Grq);
+        prof_end(ctx);
+        EPB_LAUNCH_CHECK();
+      }
     }
     for (int64_t iq = q0; iq < q0 + qn; ++iq) {
       for (int c = 0; c < ncalc; ++c)
@@ -471,19 +646,38 @@ int epb_eph_outer_q(epb_ctx* ctx, epb_model* m, const double* xk_host, const dou
           }
         }
       const double2* gRq = Grq + (iq - q0) * nd * nr_el;
-      for (int64_t k0 = 0; k0 < nkeep; k0 += KB) {
-        const int64_t kn = std::min(KB, nkeep - k0);
+      if (mixed && nkeep > 0) EPB_TRY(oq_pack_a(ctx, gRq, nd, nd, nr_el, a_g));
+      for (int64_t k0 = 0; k0 < nkeep; k0 += KBm) {
+        const int64_t kn = std::min(KBm, nkeep - k0);
         oq_shift_kernel<<<grid_oq(ctx, 3 * kn), 256, 0, ctx->stream>>>(xkk + 3 * k0, kn, xq_d + 3 * iq, xkq);
         EPB_LAUNCH_CHECK();
-        EPB_TRY(fourier_f64(ctx, m->ham, nw2, nw2, m->rs_el, xkq, kn, Hkq, nw2));
+        // H(k+q): split-BF16 tensor cores in the mixed mode (FP32-level H, as in the mixed outer-k pass)
+        if (mixed) {
+          EPB_TRY(oq_pack_b(ctx, m->rs_el, xkq, kn, b_h));
+          EPB_TRY(oq_gemm(ctx, EPB_PROF_UMMA_H, a_h, nw2, nr_el, b_h, kn, 0, kn, ch, nw2));
+          oq_widen_kernel<<<grid_oq(ctx, nw2 * kn), 256, 0, ctx->stream>>>(ch, nw2 * kn, Hkq);
+          EPB_LAUNCH_CHECK();
+        } else {
+          EPB_TRY(fourier_f64(ctx, m->ham, nw2, nw2, m->rs_el, xkq, kn, Hkq, nw2));
+        }
         EPB_TRY(eigh_async(ctx, Hkq, nw, kn, Ekq, true, nullptr, prec));
         oq_mask_kernel<<<grid_oq(ctx, kn * nw2), 256, 0, ctx->stream>>>(Hkq, Ekq, nw, kn, prm->wmin_kq, prm->wmax_kq);
         EPB_LAUNCH_CHECK();
-        if (prec == EPB_PREC_MIXED)
-          EPB_TRY(fourier_mixed(ctx, gRq, nd, nd, m->rs_el, xkk + 3 * k0, kn, gk, nd));
-        else
+        if (mixed) {
+          // g(k, q) stays complex64 (the split GEMM's output precision) and is widened in the rotation
+          EPB_TRY(oq_gemm(ctx, EPB_PROF_UMMA_KQ, a_g, nd, nr_el, b_k, nkeep, k0, kn, gk32, nd));
+          if (nw <= 16) {
+            EPB_TRY(oq_rotate(ctx, (const float2*)gk32, Uk + k0 * nw2, Hkq, wkk + k0, nw, nm, kn, ep, part));
+          } else {  // nw > 16: widen to complex128 for the per-mode kernel
+            double2* gw = (double2*)(b2 + o_gw);
+            oq_widen_kernel<<<grid_oq(ctx, nd * kn), 256, 0, ctx->stream>>>(gk32, nd * kn, gw);
+            EPB_LAUNCH_CHECK();
+            EPB_TRY(oq_rotate(ctx, (const double2*)gw, Uk + k0 * nw2, Hkq, wkk + k0, nw, nm, kn, ep, part));
+          }
+        } else {
           EPB_TRY(fourier_f64(ctx, gRq, nd, nd, m->rs_el, xkk + 3 * k0, kn, gk, nd));
-        EPB_TRY(oq_rotate(ctx, gk, Uk + k0 * nw2, Hkq, wkk + k0, nw, nm, kn, ep, part));
+          EPB_TRY(oq_rotate(ctx, (const double2*)gk, Uk + k0 * nw2, Hkq, wkk + k0, nw, nm, kn, ep, part));
+        }
         oq_record_kernel<<<1, 256, 0, ctx->stream>>>(part, kn, A_d + iq);
         EPB_LAUNCH_CHECK();
         ++nbatches;
@@ -514,6 +708,7 @@ int epb_eph_outer_q(epb_ctx* ctx, epb_model* m, const double* xk_host, const dou
         }
       }
       EPB_TRY(eigh_check(ctx));
+      if (mixed) EPB_TRY(split_gemm_check(ctx));
       for (int c = 0; c < ncalc; ++c)
         if (calcs[c].end_q) {
           const int st = calcs[c].end_q(calcs[c].user, iq, (void*)ctx->stream);

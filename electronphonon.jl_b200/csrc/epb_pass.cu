@@ -158,6 +158,7 @@ int epb_model_destroy(epb_model* m) {
   epb_rset_destroy(m->rs_ep);
   if (m->graph.exec) cudaGraphExecDestroy(m->graph.exec);
   if (m->epmat_ph) cudaFree(m->epmat_ph);
+  if (m->epmat_ph_planes) cudaFree(m->epmat_ph_planes);
   delete m;
   return EPB_OK;
 }

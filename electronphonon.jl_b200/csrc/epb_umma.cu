@@ -612,6 +612,38 @@ __global__ void c64_to_c128_kernel(const float2* __restrict__ in, double2* __res
   }
 }
 
+// ---- packed operands that live across calls (outer-q loop) ----------------------------------
+int64_t oq_a_bytes(int64_t M, int64_t K) { return planes_bytes(2 * M, K); }
+int64_t oq_b_bytes(int64_t N, int64_t K) { return MX_NPL * plane_bytes_for(round_up(N, MX_NT), kchunks(K)); }
+int oq_pack_a(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, int64_t K, uint8_t* mem) {
+  Planes A;
+  return pack_a_complex(ctx, op, ld, M, K, A, mem);
+}
+int oq_pack_b(epb_ctx* ctx, const epb_rset* rs, const double* x, int64_t N, uint8_t* mem) {
+  Planes B;
+  return pack_b_phase(ctx, rs, x, nullptr, 1, N, B, mem);
+}
+// C (complex64 columns of M, column stride ldc complex) = A (op packed by oq_pack_a, M x K) times the phase
+// columns [n0, n0 + nn) of the N points packed by oq_pack_b; n0 a multiple of 128. No host sync: a bounded
+// wait that timed out is reported by the next split_gemm_check.
+int oq_gemm(epb_ctx* ctx, int prof_id, const uint8_t* a_mem, int64_t M, int64_t K, const uint8_t* b_mem, int64_t N,
+            int64_t n0, int64_t nn, float2* C, int64_t ldc) {
+  EPB_CHECK_ARG(n0 % MX_NT == 0 && n0 + nn <= N, "oq_gemm: bad column range");
+  Planes A, B;
+  A.rows_pad = round_up(2 * M, 128);
+  A.KC = kchunks(K);
+  A.plane_bytes = plane_bytes_for(A.rows_pad, A.KC);
+  A.npl = MX_NPL;
+  A.p = const_cast<uint8_t*>(a_mem);
+  B.rows_pad = round_up(N, MX_NT);
+  B.KC = A.KC;
+  B.plane_bytes = plane_bytes_for(B.rows_pad, B.KC);
+  B.npl = MX_NPL;
+  B.p = const_cast<uint8_t*>(b_mem) + (n0 / 128) * B.KC * (int64_t)TILE_BYTES;
+  B.rows_pad -= n0;
+  return split_gemm(ctx, prof_id, A, B, A.rows_pad / 128, 1, 2 * M, nn, true, (float*)C, 0, 2 * ldc);
+}
+
 // epb_fourier(..., EPB_PREC_MIXED): pack op_r and the phases, split GEMM, widen to c128.
 int fourier_mixed(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, const epb_rset* rs,
                   const double* xk, int64_t N, double2* out, int64_t ldo) {

@@ -63,6 +63,7 @@ def serta(model, ng, wmin, wmax, mu, temp, eta, method=5, omega_cutoff=O.OMEGA_A
     kept = [k for k in range(N) if win[k][1] >= win[k][0]]
     V = velocities(ham.op_r, nw, ham.irvec, lattice, x[:, kept], U[:, :, kept]) if kept else None
     sout = {}
+    npairs = 0
     for kk, k in enumerate(kept):
         s, t = win[k]
         kR = O.get_eph_RR_to_kR(ep.op_r, ep.irvec, nr_ep, nw, nm, x[:, k], U[:, s - 1:t, k])
@@ -71,6 +72,7 @@ def serta(model, ng, wmin, wmax, mu, temp, eta, method=5, omega_cutoff=O.OMEGA_A
             s2, t2 = win[ikq]
             if t2 < s2:
                 continue
+            npairs += 1
             e = O.get_eph_kR_to_kq(kR, ep.irvec_next, x[:, iq], u_ph[:, :, iq], U[:, s2 - 1:t2, ikq], t - s + 1)
             g2 = O.epstate_set_g2(e, w_ph[:, iq])  # (nbkq, nbk, nm)
             for n in range(t - s + 1):
@@ -95,4 +97,4 @@ def serta(model, ng, wmin, wmax, mu, temp, eta, method=5, omega_cutoff=O.OMEGA_A
             df = -O._occ_fd_deriv(E[n, k] - mu, temp) / it
             vv = V[:, n, kk]
             sigma += (1.0 / N) * df * np.outer(vv, vv)
-    return sigma * spin / volume, np.array(inv_tau), dict(kept=kept, E=E, win=win)
+    return sigma * spin / volume, np.array(inv_tau), dict(kept=kept, E=E, win=win, npairs=npairs)

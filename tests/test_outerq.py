@@ -248,12 +248,13 @@ class _Record:
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("basis", ["eigenmode", "cartesian"])
-def test_outer_q_loop_fp64(P, basis):
+@pytest.mark.parametrize("basis,nw", [("eigenmode", 8), ("cartesian", 8), ("eigenmode", 20)])
+def test_outer_q_loop_fp64(P, basis, nw):
     """Record A[iq] vs the oracle's per-point outer-q chain (rtol 1e-10; the reference's CPU-vs-GPU bar is
-    1e-8, test/test_gpu.jl:673), with windows on both sides and weights."""
+    1e-8, test/test_gpu.jl:673), with windows on both sides and weights. nw = 20 takes the per-mode
+    rotation kernel (the staged one covers nw <= 16)."""
     outer_q, pipeline = P
-    m = _model(seed=41, nw=8)
+    m = _model(seed=41, nw=nw)
     xk = synth.random_kpoints(37, 1)
     xq = synth.random_kpoints(4, 2)
     wtk = np.random.default_rng(0).random(37)
@@ -262,7 +263,7 @@ def test_outer_q_loop_fp64(P, basis):
     A, st = outer_q.run_eph_over_q_and_k(dm, xk, xq, wtk=wtk, window_k=win_k, window_kq=win_kq,
                                          eph_phonon_basis=basis)
     ref = O.outer_q_record(m, xk, xq, wtk=wtk, window_k=win_k, window_kq=win_kq, phonon_basis=basis)
-    assert 0 < st["kept_k"] < 37
+    assert 0 < st["kept_k"] <= 37
     np.testing.assert_allclose(A, ref, rtol=1e-10)
 
 
@@ -310,18 +311,23 @@ def test_outer_q_loop_partial_batches_and_payload(P):
 
 
 @pytest.mark.gpu
-def test_outer_q_loop_mixed(P):
-    """Mixed precision (FP32 + FP64-refined eigensolves, split-BF16 Fourier over Re): record within 1e-5
-    relative of FP64 (the |g|^2 bar of the mixed path)."""
+@pytest.mark.parametrize("nw,nk,kb", [(16, 300, 0), (16, 700, 200), (20, 130, 0)])
+def test_outer_q_loop_mixed(P, nw, nk, kb):
+    """Mixed precision (split-BF16 H(k+q) and g(k, q), FP32 + FP64-refined eigensolves): record within 1e-5
+    relative of FP64 (the |g|^2 bar of the mixed path); several k batches (rounded to 256 here) and the
+    nw > 16 rotation included."""
     from epb200._lib import PREC_MIXED
 
     outer_q, pipeline = P
-    m = synth.config2_model(seed=44, n_el=2, n_ph=1, nw=16, natom=4)
-    xk = synth.random_kpoints(300, 5)
+    m = synth.config2_model(seed=44, n_el=2, n_ph=1, nw=nw, natom=4)
+    xk = synth.random_kpoints(nk, 5)
     xq = synth.random_kpoints(3, 6)
     dm = pipeline.DeviceModel(m)
     A64, _ = outer_q.run_eph_over_q_and_k(dm, xk, xq, window_k=(-5.0, 5.0), window_kq=(-8.0, 8.0))
-    A32, _ = outer_q.run_eph_over_q_and_k(dm, xk, xq, window_k=(-5.0, 5.0), window_kq=(-8.0, 8.0), prec=PREC_MIXED)
+    A32, st = outer_q.run_eph_over_q_and_k(dm, xk, xq, window_k=(-5.0, 5.0), window_kq=(-8.0, 8.0), prec=PREC_MIXED,
+                                           nk_batch_max=kb)
+    if kb:
+        assert st["k_batch"] == 256 and st["batches"] == 3 * -(-st["kept_k"] // 256)
     assert np.max(np.abs(A32 - A64) / np.abs(A64)) <= 1e-5
 
 
