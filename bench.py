@@ -760,6 +760,8 @@ def run_outerq(args):
     torch.cuda.set_device(0)
     nk = args.nk if args.nk != NK else 8192
     nq = args.nq if args.nq != NQ else 64
+    if args.small:  # profiling case: Re 5^3, 4096 k x 8 q (a few GB on the device)
+        nk, nq = 4096, 8
     m = build_model_host_small()
     ep_dev = synth.epmat_el_device(SEED, NW, 3 * NATOM, m.el_ham.irvec, synth.irvec_box(N_PH))
     m.epmat = synth.device_epmat_object(ep_dev, m.el_ham.irvec, synth.irvec_box(N_PH))
@@ -846,7 +848,7 @@ def run_outerq(args):
             "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16x3/f32/f64" if prec == pipeline.PREC_MIXED else "f64",
             "data": "synthetic (seeded config-2 model; g(Re,Rp) generated on the device)",
-            "config": {"workload": f"outer-q loop: nw=16, nm=12, Re 9^3, Rp 5^3, {nk} random k x {nq} random q, "
+            "config": {"workload": f"outer-q loop: nw=16, nm=12, Re {2 * N_EL + 1}^3, Rp 5^3, {nk} random k x {nq} random q, "
                                    "all bands, eigenmode basis, record consumer", **st,
                        "l2": "inputs larger than L2 (g(Re,Rp) 4.48 GB re-read per q chunk)"},
             "record_max_rel_dev_vs_fp64": rel, "fp64_ms_per_step": round(ms64, 3),
