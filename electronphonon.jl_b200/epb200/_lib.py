@@ -85,6 +85,16 @@ SIGNATURES = {
     "epb_eph_RR_to_Rq": [P, P, I64, I64, I64, P, P, I64, P, P, I32],
     "epb_eph_Rq_to_kq": [P, P, I64, I64, P, P, I64, P, I64, P, I64, P, P, P, I32],
     "epb_eph_outer_q": [P, P, P, P, I64, P, I64, P, P, I32, P, P],
+    "epb_ind_range_for_k_range": [P, I64, I64, I64, I64, P, P],
+    "epb_tiled_plan": [P, I64, I64, I64, P],
+    "epb_residency_use_block": [P, I64, D, P],
+    "epb_tiled_create": [P, P, I32, I32, I32, I64, I32, D, P, I64, I64, I64, P],
+    "epb_tiled_begin": [P, P, I64, I64],
+    "epb_tiled_get_info": [P, P],
+    "epb_tiled_device_array": [P, I32, P],
+    "epb_tiled_download": [P, P, I32, P],
+    "epb_tiled_free": [P],
+    "epb_tiled_destroy": [P],
     "epb_eph_window_scatter": [P, P, P, P, P, P, I64, P, P, I64, I64, I64, I64, I64, I64],
     "epb_bte_window_accumulate": [P, P, I64, P, I64, I64, P, P, P, P, I64, P, P, P, P, P, P, P, I64, I32, D, I64, I64,
                                   I64, I64, I64],
@@ -106,6 +116,12 @@ class BteParams(C.Structure):
     _fields_ = [("ngrid", I64), ("wmin", D), ("wmax", D), ("mu", D), ("temperature", D), ("smearing", D),
                 ("omega_cutoff", D), ("spin_degeneracy", D), ("volume", D), ("lattice", D * 9), ("method", C.c_int32),
                 ("prec", C.c_int32), ("k_batch", I64)]
+
+
+class TiledInfo(C.Structure):
+    """epb_tiled_info."""
+    _fields_ = [("allocated", C.c_int32), ("block", C.c_int32), ("ni_cap", I64), ("tile_offset", I64),
+                ("tile_length", I64), ("tile_stride", I64)]
 
 
 class OuterQParams(C.Structure):

@@ -21,7 +21,7 @@ import numpy as np
 from . import _lib
 from ._lib import PREC_FP64, check
 
-_DT = {"c128": ("<c16", 16), "f64": ("<f8", 8), "i32": ("<i4", 4)}
+_DT = {"c128": ("<c16", 16), "f64": ("<f8", 8), "f32": ("<f4", 4), "i32": ("<i4", 4)}
 
 
 class _DevView:
@@ -41,7 +41,7 @@ def _view(ptr, shape, kind, stream):
     import torch
 
     if any(n == 0 for n in shape):
-        dt = {"c128": torch.complex128, "f64": torch.float64, "i32": torch.int32}[kind]
+        dt = {"c128": torch.complex128, "f64": torch.float64, "f32": torch.float32, "i32": torch.int32}[kind]
         return torch.empty(tuple(reversed(shape)), dtype=dt, device="cuda")
     return torch.as_tensor(_DevView(ptr, shape, kind, stream), device="cuda")
 

@@ -417,6 +417,43 @@ EPB_API int epb_bte_window_accumulate(epb_ctx* ctx, double* sout, int64_t n_i, d
                                       int method, double omega_cutoff, int64_t nbandkq, int64_t nbandk,
                                       int64_t nmodes, int64_t nq_batch, int64_t i0);
 
+/* ---- tiled device output of the batched calculators ---------------------------------------- */
+/* TiledDeviceOutput (src/calculator/tiled_device_output.jl): narr arrays (elements of elem_bytes = 4, 8 or
+   16) of the column-major shape dims, axis i_axis (0-based) running over the outer states; iks (n_states,
+   host) the 1-based k index of each state, nk k points, batches of at most n_batch_max k. force_block: -1
+   decide from free device memory (block when headroom x the full bytes exceed it), 0 whole output resident,
+   1 one outer-k tile at a time. The scatter into epb_tiled_device_array uses tile_offset / tile_stride. */
+typedef struct epb_tiled epb_tiled;
+typedef struct epb_tiled_info {
+  int allocated, block;
+  int64_t ni_cap;       /* tile capacity along the tiled axis (block mode) */
+  int64_t tile_offset;  /* global state offset of the current tile (0 in full mode) (tile_offset) */
+  int64_t tile_length;  /* states in the current tile (tile_length) */
+  int64_t tile_stride;  /* the buffers' extent along the tiled axis (tile_stride) */
+} epb_tiled_info;
+/* (first, last) 1-based states of the k range kstart:kend, (1, 0) when empty; EPB_ERR_ARG when they are not
+   contiguous. Replaces: ind_range_for_k_range (src/band_states.jl:416-428). Host only. */
+EPB_API int epb_ind_range_for_k_range(const int64_t* iks, int64_t n, int64_t nk, int64_t kstart, int64_t kend,
+                                      int64_t* first, int64_t* last);
+/* The block-mode tile capacity: the largest state count of the k batches 1:n_batch_max, ... Host only. */
+EPB_API int epb_tiled_plan(const int64_t* iks, int64_t n, int64_t nk, int64_t n_batch_max, int64_t* ni_cap);
+/* residency_use_block (tiled_device_output.jl:59-60). */
+EPB_API int epb_residency_use_block(epb_ctx* ctx, int64_t full_bytes, double headroom, int* use_block);
+EPB_API int epb_tiled_create(epb_ctx* ctx, const int64_t* dims, int ndims, int i_axis, int narr, int64_t elem_bytes,
+                             int force_block, double headroom, const int64_t* iks, int64_t n_states, int64_t nk,
+                             int64_t n_batch_max, epb_tiled** out);
+/* tile_begin! for the 1-based k batch kstart:kend: the first call decides residency and allocates; in block
+   mode each call sets the tile range and zeroes its region. */
+EPB_API int epb_tiled_begin(epb_ctx* ctx, epb_tiled* t, int64_t kstart, int64_t kend);
+EPB_API int epb_tiled_get_info(const epb_tiled* t, epb_tiled_info* info);
+EPB_API int epb_tiled_device_array(const epb_tiled* t, int k, void** ptr);
+/* tile_download!: array k to host (block: the current tile, extent tile_length along the tiled axis,
+   contiguous; full: the whole array); synchronises the context stream. */
+EPB_API int epb_tiled_download(epb_ctx* ctx, const epb_tiled* t, int k, void* host);
+/* tile_free!: release the buffers and the residency decision (the object can be reused). */
+EPB_API int epb_tiled_free(epb_tiled* t);
+EPB_API int epb_tiled_destroy(epb_tiled* t);
+
 /* ---- SERTA Boltzmann consumer -------------------------------------------------------------- */
 typedef struct {
   int64_t ngrid;            /* k = q grid ngrid^3 (commensurate), k fastest (kpoints.jl:135-153)   */

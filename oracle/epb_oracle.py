@@ -512,6 +512,23 @@ def eph_window_scatter(g2_out, om_out, g2vals, imap_i_col, imap_f, ikqs, om, ni_
                         om_out[lin] = om[nu, j]
 
 
+def ind_range_for_k_range(iks, kstart, kend):
+    """1-based states with kstart <= iks[i] <= kend as a range; ValueError when they are not contiguous
+    (`src/band_states.jl:416-428`)."""
+    idx = [i + 1 for i, k in enumerate(iks) if kstart <= k <= kend]
+    if not idx:
+        return range(1, 1)
+    if idx[-1] - idx[0] + 1 != len(idx):
+        raise ValueError("non-contiguous state range")
+    return range(idx[0], idx[-1] + 1)
+
+
+def tile_capacity(iks, nk, n_batch_max):
+    """ni_cap of `tile_begin!` (`src/calculator/tiled_device_output.jl:107-108`)."""
+    return max((len(ind_range_for_k_range(iks, ks, min(ks + n_batch_max - 1, nk))) for ks in range(1, nk + 1, n_batch_max)),
+               default=0)
+
+
 def bte_window_accumulate(sout, sin, g2vals, om, imap_i_at_k, imap_f, ikqs, e_i, e_f, wf, mus, ts, etas, method,
                           omega_cutoff, i0):
     """`src/boltzmann/boltzmann_calculator.jl:336-362` (1-based maps, 0-based numpy arrays)."""

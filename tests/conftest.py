@@ -24,3 +24,11 @@ def gpu_lib():
     from epb200 import _lib
 
     return _lib.lib()
+
+
+@pytest.fixture(scope="session")
+def cpu_lib():
+    """The library loaded without a GPU, for its host-only entry points."""
+    from epb200 import _lib
+
+    return _lib.lib()
