@@ -86,6 +86,7 @@ SIGNATURES = {
     "epb_eph_Rq_to_kq": [P, P, I64, I64, P, P, I64, P, I64, P, I64, P, P, P, I32],
     "epb_eph_outer_q": [P, P, P, P, I64, P, I64, P, P, I32, P, P],
     "epb_ind_range_for_k_range": [P, I64, I64, I64, I64, P, P],
+    "epb_read_epmat": [P, C.c_char_p, I64, I64, I64, I64, P, P, P, I64, P, I64, I64, I32, I32, I32, P],
     "epb_tiled_plan": [P, I64, I64, I64, P],
     "epb_residency_use_block": [P, I64, D, P],
     "epb_tiled_create": [P, P, I32, I32, I32, I64, I32, D, P, I64, I64, I64, P],

@@ -417,6 +417,19 @@ EPB_API int epb_bte_window_accumulate(epb_ctx* ctx, double* sout, int64_t n_i, d
                                       int method, double omega_cutoff, int64_t nbandkq, int64_t nbandk,
                                       int64_t nmodes, int64_t nq_batch, int64_t i0);
 
+/* ---- EPW reader ------------------------------------------------------------------------------ */
+/* Reads `<prefix>.epmatwp` (raw complex128, EPW order (iw, jw, iRe, imode, iRp)) into `out` (device,
+   nw^2 nmodes nr_ep x nr_el for layout 0 = "el", nw^2 nmodes nr_el x nr_ep for layout 1 = "ph"), applying
+   the R sort (ind_el, ind_ep: Julia sortperm, 1-based, new <- old) and the Wigner-Seitz divisions with the
+   sorted degeneracy arrays: ndegen_ep (ndegen_ep_dim1 x ndegen_ep_dim2 x nr_ep, (1, 1) or (nw, nat))
+   unless skip_ndegen_ep or ndegen_pre_divided, then ndegen_el (d x d x nr_el, d = 1 or nw) unless
+   ndegen_pre_divided; zero where a degeneracy is 0. Replaces: read_epmat (src/model_new.jl:487-568). */
+EPB_API int epb_read_epmat(epb_ctx* ctx, const char* filename, int64_t nw, int64_t nmodes, int64_t nr_el,
+                           int64_t nr_ep, const int64_t* ind_el, const int64_t* ind_ep, const int32_t* ndegen_el,
+                           int64_t ndegen_el_dim, const int32_t* ndegen_ep, int64_t ndegen_ep_dim1,
+                           int64_t ndegen_ep_dim2, int skip_ndegen_ep, int ndegen_pre_divided, int layout,
+                           double* out);
+
 /* ---- tiled device output of the batched calculators ---------------------------------------- */
 /* TiledDeviceOutput (src/calculator/tiled_device_output.jl): narr arrays (elements of elem_bytes = 4, 8 or
    16) of the column-major shape dims, axis i_axis (0-based) running over the outer states; iks (n_states,
