@@ -651,7 +651,8 @@ def run_bte(args):
     ef = float(np.median(Es[NW // 2 - 1]))
     half = 0.3 * synth.UNIT_EV
     T, eta = 300 * O.UNIT_K, 0.01 * synth.UNIT_EV
-    kw = dict(method=5, k_batch=32, prec=pipeline.PREC_MIXED if args.prec != "fp64" else pipeline.PREC_FP64)
+    kw = dict(method=5, k_batch=args.k_batch if args.k_batch > 0 else 128,
+              prec=pipeline.PREC_MIXED if args.prec != "fp64" else pipeline.PREC_FP64)
     for _ in range(args.warmup):
         sig, st, _ = bte.serta(dm, ng, ef - half, ef + half, ef, T, eta, **kw)
     torch.cuda.synchronize()
@@ -690,11 +691,16 @@ def run_bte(args):
     nm, nr_el, nr_ep = 3 * NATOM, (2 * N_EL + 1) ** 3, (2 * N_PH + 1) ** 3
     W = max(int(st["width"]), 1)
     roof = None
-    if dom_name == "zgemm":   # kR->kq per kept k: (nw W nm) x nr_ep x pairs of that k, FP64
+    if dom_name == "umma_kq":   # grouped kR->kq of the kept k's pairs, split BF16x3
+        flops = 8.0 * NW * W * nm * nr_ep * st["pairs"]
+        peak, psrc = peaks["bf16_tflops_sustained"] / 6, f"{peak_src} bf16 sustained / 6 split products"
+    elif dom_name == "rotation":
+        flops = None
+    elif dom_name == "zgemm":   # kR->kq per kept k: (nw W nm) x nr_ep x pairs of that k, FP64
         flops = 8.0 * NW * W * nm * nr_ep * st["pairs"]
         peak, psrc = measure_fp64_peak(torch), "measured live: cuBLAS DGEMM 8192^3"
-    elif dom_name == "umma_rr":  # RR->kR over Re for the kept k, split BF16x3
-        flops = 8.0 * NW * W * nm * nr_ep * nr_el * st["kept_k"]
+    elif dom_name == "umma_rr":  # RR->kR over Re for the kept k (all nw^2 nm nr_ep rows), split BF16x3
+        flops = 8.0 * NW * NW * nm * nr_ep * nr_el * st["kept_k"]
         peak, psrc = peaks["bf16_tflops_sustained"] / 6, f"{peak_src} bf16 sustained / 6 split products"
     else:
         flops = None
@@ -721,7 +727,7 @@ def run_bte(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3/f64" if kw["prec"] == 1 else "f64",
             "data": "synthetic (seeded config-2 model; g(Re,Rp) generated on the device)",
             "config": {"workload": f"config5 SERTA: nw=16, nm=12, Re 9^3, Rp 5^3, {ng}^3 k = q grids, window E_F -/+ 0.3 eV, "
-                                   "T = 300 K, Gaussian 10 meV, method 5", "e_fermi_ry": ef, **st},
+                                   "T = 300 K, Gaussian 10 meV, method 5", "e_fermi_ry": ef, "k_batch": kw["k_batch"], **st},
             "sigma": sig.tolist(), "sigma_fp64": sig64.tolist(), "sigma_max_rel_dev_vs_fp64": rel,
             "fp64_ms_per_step": round(ms64, 3), "speedup_vs_fp64": round(ms64 / ms, 3), "roofline": roof, "cpu_baseline": cpu,
             "e2e": {"value": st["pairs"] / (ms * 1e-3), "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 72,

@@ -42,6 +42,14 @@ int eph_rotations_f64(epb_ctx* ctx, const double2* g, int64_t ldg, int nw, int n
 int mixed_rr_to_kR(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double2* uk, int nband,
                    double2* out);
 int split_gemm_check(epb_ctx* ctx);
+int eph_rotations_c64(epb_ctx* ctx, const float2* g, int64_t ldg, int nw, int nbk, int nm, int64_t nq,
+                      const double2* ukq, int nbkq, const double2* uph, const double* omega, double2* ep, double* g2);
+int64_t bte_a2_bytes(epb_model* m, int64_t nk, int64_t nband);
+int64_t bte_b_bytes(epb_model* m, int64_t ncols);
+int bte_pack_kR(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double2* uk, int nband, uint8_t* a2);
+int bte_kq_grouped(epb_ctx* ctx, epb_model* m, const uint8_t* a2, int64_t nk_a2, int nband, const double* x,
+                   int64_t ncols, const int64_t* grp, const int64_t* grp_a, int64_t ngrp, uint8_t* bmem, float2* C,
+                   int64_t ldc);
 
 static unsigned gsz(epb_ctx* ctx, int64_t total) {
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(total, 256), (int64_t)ctx->sm_count * 16));
@@ -276,6 +284,199 @@ __global__ void bte_accumulate_kernel(const double* __restrict__ g2, int64_t n, 
   }
 }
 
+// Columns of the grouped tensor-core kR->kq: group g (tiles [grp[g], grp[g+1]) of 128 columns) holds the
+// pairs plist[grp_p0[g] + j], j < grp_n[g], of the batch's kept k number grp_a[g]; the rest of its columns
+// are padding (zero u_{k+q}, so their g2 is zero, and ikq = -1). Per column: q, u_{k+q} slice, u_ph, omega.
+__global__ void bte_cols_kernel(const int64_t* __restrict__ grp, const int64_t* __restrict__ grp_a,
+                                const int64_t* __restrict__ grp_p0, const int64_t* __restrict__ grp_n, int64_t ngrp,
+                                int64_t ncols, const int64_t* __restrict__ plist, const int32_t* __restrict__ keep,
+                                int64_t b0, int64_t ng, const double* __restrict__ xgrid, const double2* __restrict__ U,
+                                const int32_t* __restrict__ bmin, int nw, int W, const double2* __restrict__ uph_g,
+                                const double* __restrict__ om_g, int nm, double* __restrict__ xq,
+                                double2* __restrict__ ukq, double2* __restrict__ uph, double* __restrict__ om,
+                                int32_t* __restrict__ ikq_out, int32_t* __restrict__ kk_out) {
+  const int64_t N = ng * ng * ng;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncols; c += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t tile = c / 128;
+    int64_t lo = 0, hi = ngrp;
+    while (hi - lo > 1) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (grp[mid] <= tile) lo = mid; else hi = mid;
+    }
+    const int64_t j = c - grp[lo] * 128;
+    if (j >= grp_n[lo]) {
+      for (int d = 0; d < 3; ++d) xq[3 * c + d] = 0.0;
+      for (int e = 0; e < W * nw; ++e) ukq[c * W * nw + e] = make_double2(0.0, 0.0);
+      for (int e = 0; e < nm * nm; ++e) uph[c * nm * nm + e] = make_double2(0.0, 0.0);
+      for (int e = 0; e < nm; ++e) om[c * nm + e] = 1.0;
+      ikq_out[c] = -1;
+      kk_out[c] = -1;
+      continue;
+    }
+    const int64_t kk = grp_a[lo];
+    const int64_t ik = keep[b0 + kk];
+    const int64_t iq = plist[grp_p0[lo] + j] % N;
+    const int64_t ikq = grid_index((ik / (ng * ng) + iq / (ng * ng)) % ng, ((ik / ng) % ng + (iq / ng) % ng) % ng,
+                                   (ik % ng + iq % ng) % ng, ng);
+    ikq_out[c] = (int32_t)ikq;
+    kk_out[c] = (int32_t)kk;
+    for (int d = 0; d < 3; ++d) xq[3 * c + d] = xgrid[3 * iq + d];
+    const int o = slice_offset(bmin[ikq], nw, W);
+    for (int b = 0; b < W; ++b)
+      for (int i = 0; i < nw; ++i) ukq[(c * W + b) * nw + i] = U[ikq * nw * nw + (int64_t)(o + b) * nw + i];
+    for (int e = 0; e < nm * nm; ++e) uph[c * nm * nm + e] = uph_g[iq * nm * nm + e];
+    for (int e = 0; e < nm; ++e) om[c * nm + e] = om_g[iq * nm + e];
+  }
+}
+
+// Light column map for narrow windows (W <= 4): the phase point x_q of every column (for the packed B
+// operand) and the column's kept k (local), q and k+q grid indices (-1 for padding).
+__global__ void bte_cols_meta_kernel(const int64_t* __restrict__ grp, const int64_t* __restrict__ grp_a,
+                                     const int64_t* __restrict__ grp_p0, const int64_t* __restrict__ grp_n,
+                                     int64_t ngrp, int64_t ncols, const int64_t* __restrict__ plist,
+                                     const int32_t* __restrict__ keep, int64_t b0, int64_t ng,
+                                     const double* __restrict__ xgrid, double* __restrict__ xq,
+                                     int32_t* __restrict__ kk_out, int32_t* __restrict__ iq_out,
+                                     int32_t* __restrict__ ikq_out) {
+  const int64_t N = ng * ng * ng;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncols; c += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t tile = c / 128;
+    int64_t lo = 0, hi = ngrp;
+    while (hi - lo > 1) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (grp[mid] <= tile) lo = mid; else hi = mid;
+    }
+    const int64_t j = c - grp[lo] * 128;
+    if (j >= grp_n[lo]) {
+      for (int d = 0; d < 3; ++d) xq[3 * c + d] = 0.0;
+      kk_out[c] = iq_out[c] = ikq_out[c] = -1;
+      continue;
+    }
+    const int64_t kk = grp_a[lo], ik = keep[b0 + kk];
+    const int64_t iq = plist[grp_p0[lo] + j] % N;
+    kk_out[c] = (int32_t)kk;
+    iq_out[c] = (int32_t)iq;
+    ikq_out[c] = (int32_t)grid_index((ik / (ng * ng) + iq / (ng * ng)) % ng, ((ik / ng) % ng + (iq / ng) % ng) % ng,
+                                     (ik % ng + iq % ng) % ng, ng);
+    for (int d = 0; d < 3; ++d) xq[3 * c + d] = xgrid[3 * iq + d];
+  }
+}
+
+// Rotation, |g|^2 fold and out-scattering accumulation, one column per 16-lane group (narrow windows,
+// W <= 4), two columns per warp:
+//   T[m, n, jm] = sum_iw conj(ukq[iw, m]) g[iw, n, jm],  ep[m, n, nu] = sum_jm T[m, n, jm] uph[jm, nu],
+//   g2 = |ep|^2 / (2 omega_nu), and S_out[n at k] += the method's increments over m, nu
+// (eph_rot_kernel + bte_accumulate_kernel in one pass). g(k, q) and u_ph are read straight from global
+// memory (each lane a contiguous run), u_{k+q} by grid index into a small shared slice; the per-column
+// sums over (m, nu) are reduced across the group, one atomic per state.
+constexpr int BTE_GROUPS = 16;  // 16-lane groups per block (256 threads)
+__global__ void __launch_bounds__(16 * BTE_GROUPS, 4) bte_rot_acc_kernel(
+    const float2* __restrict__ C, int64_t ldc, int64_t ncols, const int32_t* __restrict__ kk_col,
+    const int32_t* __restrict__ iq_col, const int32_t* __restrict__ ikq_col, const int32_t* __restrict__ keep,
+    int64_t b0, const double2* __restrict__ U, const int32_t* __restrict__ bmin, const int32_t* __restrict__ bmax,
+    const double* __restrict__ E, const double2* __restrict__ uph_g, const double* __restrict__ om_g, int nw, int W,
+    int nm, BteParams p, double* __restrict__ sout) {
+  extern __shared__ __align__(16) unsigned char bte_smem[];
+  const int grp = threadIdx.x >> 4, l = threadIdx.x & 15;
+  const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
+  const int nt = W * W * nm;
+  double2* su = reinterpret_cast<double2*>(bte_smem) + (size_t)grp * (nw * W + nt);  // ukq slice (nw x W)
+  double2* st = su + nw * W;                                                          // T (W, W, nm), m fastest
+  const int64_t gid = (int64_t)blockIdx.x * BTE_GROUPS + grp, ngroups = (int64_t)gridDim.x * BTE_GROUPS;
+  const int64_t iters = (ncols + ngroups - 1) / ngroups;  // same trip count in both halves of a warp
+  for (int64_t it = 0; it < iters; ++it) {
+    const int64_t c = gid + it * ngroups;
+    const int32_t f = c < ncols ? ikq_col[c] : -1;
+    const bool valid = f >= 0;
+    int64_t kk = 0, ik = 0, iq = 0;
+    int bmin_k = 0, bmax_k = -1, bmf = 0, bxf = -1, ok_ = 0, oq = 0;
+    if (valid) {
+      kk = kk_col[c];
+      iq = iq_col[c];
+      ik = keep[b0 + kk];
+      bmin_k = bmin[ik];
+      bmax_k = bmax[ik];
+      bmf = bmin[f];
+      bxf = bmax[f];
+      ok_ = slice_offset(bmin_k, nw, W);
+      oq = slice_offset(bmf, nw, W);
+      for (int e = l; e < nw * W; e += 16) su[e] = U[(int64_t)f * nw * nw + (int64_t)oq * nw + e];
+    }
+    __syncwarp(hmask);
+    if (valid) {
+      const float2* gc = C + c * ldc;
+      for (int e = l; e < nt; e += 16) {  // e = m + W (n + W jm)
+        const int m = e % W, r = e / W;   // r = n + W jm
+        const float2* gr = gc + (int64_t)r * nw;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int iw = 0; iw < nw; ++iw) {
+          const float2 gv = gr[iw];
+          cfma_conj(acc, su[m * nw + iw], make_double2(gv.x, gv.y));
+        }
+        st[e] = acc;
+      }
+    }
+    __syncwarp(hmask);
+    for (int n = 0; n < W; ++n) {
+      double part = 0.0;
+      const int bk = ok_ + n;
+      if (valid && bk >= bmin_k - 1 && bk <= bmax_k - 1) {
+        const double ek = E[ik * nw + bk];
+        for (int e = l; e < W * nm; e += 16) {
+          const int m = e % W, nu = e / W;
+          const int bq = oq + m;
+          if (bq < bmf - 1 || bq > bxf - 1) continue;
+          const double wq = om_g[iq * nm + nu];
+          if (wq < p.omega_cutoff) continue;
+          const double2* up = uph_g + iq * nm * nm + (int64_t)nu * nm;
+          double2 v = make_double2(0.0, 0.0);
+          for (int jm = 0; jm < nm; ++jm) cfma(v, st[m + W * (n + W * jm)], up[jm]);
+          const double g2 = (v.x * v.x + v.y * v.y) / (2.0 * wq);
+          part += bte_out_increment(p, ek, E[(int64_t)f * nw + bq], wq, g2);
+        }
+      }
+      for (int o = 8; o > 0; o >>= 1) part += __shfl_xor_sync(hmask, part, o);
+      if (l == 0 && part != 0.0) atomicAdd(sout + (b0 + kk) * W + n, part);
+    }
+    __syncwarp(hmask);
+  }
+}
+
+// bte_accumulate_kernel over columns of several kept k (column c belongs to kept k b0 + kk_c; padding skipped).
+__global__ void bte_accumulate_cols_kernel(const double* __restrict__ g2, int64_t n, int W, int nm,
+                                           const double* __restrict__ E, int nw, const int32_t* __restrict__ keep,
+                                           int64_t b0, const int32_t* __restrict__ kk_col,
+                                           const int32_t* __restrict__ ikq, const int32_t* __restrict__ bmin,
+                                           const int32_t* __restrict__ bmax, const double* __restrict__ om, BteParams p,
+                                           double* __restrict__ sout) {
+  const int64_t total = n * W;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int nb = (int)(e % W);
+    const int64_t j = e / W;
+    if (ikq[j] < 0) continue;
+    const int64_t kk = kk_col[j], ik = keep[b0 + kk];
+    const int bmin_k = bmin[ik], bmax_k = bmax[ik];
+    const int bk = slice_offset(bmin_k, nw, W) + nb;  // 0-based band at k
+    if (bk < bmin_k - 1 || bk > bmax_k - 1) continue;
+    const int64_t f = ikq[j];
+    const int bmf = bmin[f], bxf = bmax[f];
+    const int okq = slice_offset(bmf, nw, W);
+    const double ek = E[ik * nw + bk];
+    double acc = 0.0;
+    for (int m = 0; m < W; ++m) {
+      const int bq = okq + m;
+      if (bq < bmf - 1 || bq > bxf - 1) continue;
+      const double ekq = E[f * nw + bq];
+      for (int nu = 0; nu < nm; ++nu) {
+        const double wq = om[j * nm + nu];
+        if (wq < p.omega_cutoff) continue;
+        acc += bte_out_increment(p, ek, ekq, wq, g2[((j * nm + nu) * W + nb) * W + m]);
+      }
+    }
+    if (acc != 0.0) atomicAdd(sout + (b0 + kk) * W + nb, acc);
+  }
+}
+
 // sigma (9, column-major) += (1/N) (-f'(e - mu) / S_out) v v^T over the kept states; inv_tau listed.
 __global__ void bte_serta_kernel(const int32_t* __restrict__ keep, int64_t nkeep, const int32_t* __restrict__ bmin,
                                  const int32_t* __restrict__ bmax, const double* __restrict__ E, int nw, int W,
@@ -382,8 +583,10 @@ int epb_bte_serta(epb_ctx* ctx, epb_model* m, const epb_bte_params* prm, double*
   EPB_TRY(make_current(ctx));
   const int nw = (int)m->nw, nm = (int)m->nm;
   const int64_t N = ng * ng * ng, nw2 = (int64_t)nw * nw, nr_ep = m->nr_ep;
-  const int64_t KB = std::max<int64_t>(1, std::min<int64_t>(prm->k_batch > 0 ? prm->k_batch : 32, 256));
-  const int64_t QCH = 65536;  // pairs per rotation launch
+  // 128 kept k per batch by default: the RR->kR GEMM's column tile is 128 points wide
+  const int64_t KB = std::max<int64_t>(1, std::min<int64_t>(prm->k_batch > 0 ? prm->k_batch : 128, 256));
+  EPB_CHECK_ARG(prm->pair_chunk <= 0 || prm->pair_chunk % 128 == 0, "epb_bte_serta: pair_chunk must be a multiple of 128");
+  const int64_t QCH = prm->pair_chunk > 0 ? prm->pair_chunk : 65536;  // pairs per rotation launch
 
   // ---- persistent buffers (whole grid) ----
   size_t off = 0;
@@ -464,6 +667,11 @@ int epb_bte_serta(epb_ctx* ctx, epb_model* m, const epb_bte_params* prm, double*
                  o_uphq = take2(16 * (int64_t)nm * nm * QCH), o_omq = take2(8 * nm * QCH), o_ikq = take2(4 * QCH),
                  o_P = take2(16 * nr_ep * QCH), o_g = take2(16 * (int64_t)nw * W * nm * QCH),
                  o_g2 = take2(8 * (int64_t)W * W * nm * QCH), o_xkb = take2(24 * std::max(VB, KB));
+    const bool mixed = prm->prec == EPB_PREC_MIXED;
+    const int64_t MAXG = QCH / 128 + 1;  // groups of one column chunk
+    const size_t o_a2 = mixed ? take2(bte_a2_bytes(m, KB, W) + 1024) : 0, o_bq = mixed ? take2(bte_b_bytes(m, QCH) + 1024) : 0,
+                 o_grp = mixed ? take2(8 * 4 * (MAXG + 1)) : 0, o_kkc = mixed ? take2(4 * QCH) : 0,
+                 o_iqc = mixed ? take2(4 * QCH) : 0;
     void* ws2 = nullptr;
     EPB_TRY(ws_get(ctx, EPB_WS_PASS3, off2 + 256, &ws2));
     uint8_t* b2 = (uint8_t*)ws2;
@@ -489,6 +697,16 @@ int epb_bte_serta(epb_ctx* ctx, epb_model* m, const epb_bte_params* prm, double*
     double2* g = (double2*)(b2 + o_g);
     double* g2 = (double*)(b2 + o_g2);
     double* xkb = (double*)(b2 + o_xkb);
+    uint8_t* a2 = mixed ? (uint8_t*)(((uintptr_t)(b2 + o_a2) + 1023) & ~uintptr_t(1023)) : nullptr;
+    uint8_t* bq = mixed ? (uint8_t*)(((uintptr_t)(b2 + o_bq) + 1023) & ~uintptr_t(1023)) : nullptr;
+    int64_t* grp_d = (int64_t*)(b2 + o_grp);
+    int32_t* kkc = (int32_t*)(b2 + o_kkc);
+    int32_t* iqc = (int32_t*)(b2 + o_iqc);
+    const bool narrow = W <= 4;
+    const size_t rot_smem = (size_t)BTE_GROUPS * 16 * (nw * W + W * W * nm);
+    if (mixed && narrow && rot_smem > 48 * 1024)
+      EPB_CUDA(cudaFuncSetAttribute(bte_rot_acc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rot_smem));
+    std::vector<int64_t> grp_h(4 * (MAXG + 1));
     EPB_CUDA(cudaMemsetAsync(sout, 0, 8 * W * nkeep, ctx->stream));
 
     // 3. velocities of the kept points
@@ -520,8 +738,8 @@ int epb_bte_serta(epb_ctx* ctx, epb_model* m, const epb_bte_params* prm, double*
       EPB_LAUNCH_CHECK();
       bte_gather_uk_kernel<<<gsz(ctx, nkb * nw * W), 256, 0, ctx->stream>>>(U, keep, b0, nkb, bmin, nw, W, ukb);
       EPB_LAUNCH_CHECK();
-      if (prm->prec == EPB_PREC_MIXED)
-        EPB_TRY(mixed_rr_to_kR(ctx, m, xkb, nkb, ukb, W, kR));
+      if (mixed)
+        EPB_TRY(bte_pack_kR(ctx, m, xkb, nkb, ukb, W, a2));
       else
         EPB_TRY(epb_eph_RR_to_kR(ctx, (const double*)m->epmat, nw, nm, nr_ep, m->rs_el, xkb, nkb, (const double*)ukb, W,
                                  nullptr, (double*)kR, EPB_PREC_FP64));
@@ -545,6 +763,66 @@ int epb_bte_serta(epb_ctx* ctx, epb_model* m, const epb_bte_params* prm, double*
       EPB_CUDA(cudaMemcpyAsync(seg_h.data(), seg, 8 * (nkb + 1), cudaMemcpyDeviceToHost, ctx->stream));
       EPB_CUDA(cudaStreamSynchronize(ctx->stream));
       npairs_total += np;
+      if (mixed) {
+        // grouped tensor-core kR->kq: column chunks of at most QCH columns, each kept k's pairs padded to 128
+        int64_t kk = 0, off = 0;  // next pair of kept k kk not yet placed: seg_h[kk] + off
+        while (kk < nkb) {
+          int64_t ng_ = 0, tiles = 0;
+          int64_t* g_t = grp_h.data();          // tile prefix (ngrp + 1)
+          int64_t* g_a = g_t + (MAXG + 1);      // kept k of the group
+          int64_t* g_p = g_a + (MAXG + 1);      // first pair (index into plist)
+          int64_t* g_n = g_p + (MAXG + 1);      // pairs in the group
+          while (kk < nkb && ng_ < MAXG - 1) {
+            const int64_t left = seg_h[kk + 1] - seg_h[kk] - off;
+            if (left <= 0) {
+              ++kk;
+              off = 0;
+              continue;
+            }
+            const int64_t room = QCH / 128 - tiles;
+            if (room <= 0) break;
+            const int64_t take = std::min(left, room * 128);
+            g_t[ng_] = tiles;
+            g_a[ng_] = kk;
+            g_p[ng_] = seg_h[kk] + off;
+            g_n[ng_] = take;
+            tiles += cdiv(take, 128);
+            ++ng_;
+            off += take;
+          }
+          if (ng_ == 0) break;
+          g_t[ng_] = tiles;
+          const int64_t ncols = tiles * 128;
+          EPB_CUDA(cudaMemcpyAsync(grp_d, grp_h.data(), 8 * 4 * (MAXG + 1), cudaMemcpyHostToDevice, ctx->stream));
+          const int64_t* gt_d = grp_d;
+          const int64_t* ga_d = grp_d + (MAXG + 1);
+          if (narrow) {  // fused rotation + accumulation, grid arrays read by index
+            bte_cols_meta_kernel<<<gsz(ctx, ncols), 256, 0, ctx->stream>>>(
+                gt_d, ga_d, grp_d + 2 * (MAXG + 1), grp_d + 3 * (MAXG + 1), ng_, ncols, plist, keep, b0, ng, xg, xq, kkc,
+                iqc, ikq);
+            EPB_LAUNCH_CHECK();
+            EPB_TRY(bte_kq_grouped(ctx, m, a2, nkb, W, xq, ncols, gt_d, ga_d, ng_, bq, (float2*)g, Mrows));
+            const unsigned grid = (unsigned)std::max<int64_t>(
+                1, std::min<int64_t>(cdiv(ncols, BTE_GROUPS), (int64_t)ctx->sm_count * 8));
+            prof_begin(ctx, EPB_PROF_ROT);
+            bte_rot_acc_kernel<<<grid, 16 * BTE_GROUPS, rot_smem, ctx->stream>>>(
+                (const float2*)g, Mrows, ncols, kkc, iqc, ikq, keep, b0, U, bmin, bmax, E, uph, om, nw, W, nm, bp, sout);
+            prof_end(ctx);
+            EPB_LAUNCH_CHECK();
+            continue;
+          }
+          bte_cols_kernel<<<gsz(ctx, ncols), 256, 0, ctx->stream>>>(
+              gt_d, ga_d, grp_d + 2 * (MAXG + 1), grp_d + 3 * (MAXG + 1), ng_, ncols, plist, keep, b0, ng, xg, U, bmin, nw,
+              W, uph, om, nm, xq, ukq, uphq, omq, ikq, kkc);
+          EPB_LAUNCH_CHECK();
+          EPB_TRY(bte_kq_grouped(ctx, m, a2, nkb, W, xq, ncols, gt_d, ga_d, ng_, bq, (float2*)g, Mrows));
+          EPB_TRY(eph_rotations_c64(ctx, (const float2*)g, Mrows, nw, W, nm, ncols, ukq, W, uphq, omq, nullptr, g2));
+          bte_accumulate_cols_kernel<<<gsz(ctx, ncols * W), 256, 0, ctx->stream>>>(g2, ncols, W, nm, E, nw, keep, b0, kkc,
+                                                                                ikq, bmin, bmax, omq, bp, sout);
+          EPB_LAUNCH_CHECK();  // the next chunk's table upload is ordered after these kernels on the stream
+        }
+        continue;
+      }
       for (int64_t kk = 0; kk < nkb; ++kk) {
         const int64_t s0 = seg_h[kk], nk_pairs = seg_h[kk + 1] - s0, ik = keep_h[b0 + kk];
         for (int64_t c0 = 0; c0 < nk_pairs; c0 += QCH) {

@@ -121,7 +121,12 @@ __global__ void rr_rotate_kernel(const double2* __restrict__ g, const double2* _
 // ---------------------------------------------------------------------------------------------
 // Rotations: ep[m, n, nu, q] = sum_{iw, jm} conj(ukq[iw, m, q]) g[iw, n, jm, q] uph[jm, nu, q].
 // One CTA per q. Shared: g (nw*nbk*nm), T (nbkq*nbk*nm), ukq (nw*nbkq), uph (nm*nm).
-__global__ void eph_rot_kernel(const double2* __restrict__ g, int64_t ldg, const double2* __restrict__ ukq,
+__device__ __forceinline__ double2 rot_ld(double2 v) { return v; }
+__device__ __forceinline__ double2 rot_ld(float2 v) { return make_double2(v.x, v.y); }
+
+// G = double2, or float2 for a complex64 g (the tensor-core kR->kq output), widened on load.
+template <typename G>
+__global__ void eph_rot_kernel(const G* __restrict__ g, int64_t ldg, const double2* __restrict__ ukq,
                                const double2* __restrict__ uph, const double* __restrict__ omega,
                                double2* __restrict__ ep, double* __restrict__ g2, int nw, int nbk,
                                int nm, int nbkq, int64_t nq) {
@@ -132,8 +137,8 @@ __global__ void eph_rot_kernel(const double2* __restrict__ g, int64_t ldg, const
   double2* us = ts + nt;
   double2* ps = us + nw * nbkq;
   for (int64_t q = blockIdx.x; q < nq; q += gridDim.x) {
-    const double2* gq = g + q * ldg;
-    for (int e = threadIdx.x; e < ng; e += blockDim.x) gs[e] = gq[e];
+    const G* gq = g + q * ldg;
+    for (int e = threadIdx.x; e < ng; e += blockDim.x) gs[e] = rot_ld(gq[e]);
     for (int e = threadIdx.x; e < nw * nbkq; e += blockDim.x) us[e] = ukq[q * nw * nbkq + e];
     for (int e = threadIdx.x; e < nm * nm; e += blockDim.x) ps[e] = uph[q * nm * nm + e];
     __syncthreads();
@@ -161,25 +166,38 @@ __global__ void eph_rot_kernel(const double2* __restrict__ g, int64_t ldg, const
   }
 }
 
-int eph_rotations_f64(epb_ctx* ctx, const double2* g, int64_t ldg, int nw, int nbk, int nm,
-                      int64_t nq, const double2* ukq, int nbkq, const double2* uph,
-                      const double* omega, double2* ep, double* g2) {
+template <typename G>
+static int eph_rotations_t(epb_ctx* ctx, const G* g, int64_t ldg, int nw, int nbk, int nm, int64_t nq,
+                           const double2* ukq, int nbkq, const double2* uph, const double* omega, double2* ep,
+                           double* g2) {
   if (nq == 0) return EPB_OK;
   size_t smem = sizeof(double2) * ((size_t)nw * nbk * nm + (size_t)nbkq * nbk * nm + nw * nbkq + nm * nm);
   EPB_CHECK_ARG(smem <= 200 * 1024, "eph rotations: block (nw=%d, nbk=%d, nm=%d) exceeds shared memory",
                 nw, nbk, nm);
   static bool attr = false;
   if (!attr) {
-    EPB_CUDA(cudaFuncSetAttribute(eph_rot_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    EPB_CUDA(cudaFuncSetAttribute(eph_rot_kernel<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     attr = true;
   }
   int64_t blocks = nq < (int64_t)ctx->sm_count * 8 ? nq : (int64_t)ctx->sm_count * 8;
   prof_begin(ctx, EPB_PROF_ROT);
-  eph_rot_kernel<<<(unsigned)blocks, 256, smem, ctx->stream>>>(g, ldg, ukq, uph, omega, ep, g2, nw,
-                                                                nbk, nm, nbkq, nq);
+  eph_rot_kernel<G><<<(unsigned)blocks, 256, smem, ctx->stream>>>(g, ldg, ukq, uph, omega, ep, g2, nw, nbk, nm,
+                                                                   nbkq, nq);
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
+}
+
+int eph_rotations_f64(epb_ctx* ctx, const double2* g, int64_t ldg, int nw, int nbk, int nm,
+                      int64_t nq, const double2* ukq, int nbkq, const double2* uph,
+                      const double* omega, double2* ep, double* g2) {
+  return eph_rotations_t(ctx, g, ldg, nw, nbk, nm, nq, ukq, nbkq, uph, omega, ep, g2);
+}
+
+int eph_rotations_c64(epb_ctx* ctx, const float2* g, int64_t ldg, int nw, int nbk, int nm, int64_t nq,
+                      const double2* ukq, int nbkq, const double2* uph, const double* omega, double2* ep,
+                      double* g2) {
+  return eph_rotations_t(ctx, g, ldg, nw, nbk, nm, nq, ukq, nbkq, uph, omega, ep, g2);
 }
 
 }  // namespace epb

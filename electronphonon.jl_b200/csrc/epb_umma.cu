@@ -264,6 +264,11 @@ struct SplitGemmArgs {
   int64_t c_batch_stride, ldc_n;
   int* err;
   long long timeout;
+  // grouped mode (grp != nullptr): group g owns the B column tiles [grp[g], grp[g + 1]) and multiplies the
+  // A block grp_a[g] (m_tiles_per_batch tiles); m_tiles = m_tiles_per_batch, n_tiles = grp[ngrp]
+  const int64_t* grp;
+  const int64_t* grp_a;
+  int64_t ngrp;
 };
 
 template <bool BF16, int NPL>
@@ -348,6 +353,14 @@ __global__ void __launch_bounds__(192, 1) split_gemm_kernel(SplitGemmArgs a) {
     for (int64_t t = blockIdx.x; t < total && ok; t += gridDim.x) {
       int64_t mt = a.m_fastest ? t % a.m_tiles : t / a.n_tiles;
       int64_t nt = a.m_fastest ? t / a.m_tiles : t % a.n_tiles;
+      if (a.grp) {  // the group of column tile nt (binary search), then its A block
+        int64_t lo = 0, hi = a.ngrp;
+        while (hi - lo > 1) {
+          const int64_t mid = (lo + hi) >> 1;
+          if (a.grp[mid] <= nt) lo = mid; else hi = mid;
+        }
+        mt += a.grp_a[lo] * a.m_tiles_per_batch;
+      }
       for (int kc = 0; kc < a.KC; ++kc) {
         if (!mbar_wait(&empty[s], ph ^ 1u, err, a.timeout)) {
           ok = false;
@@ -833,23 +846,23 @@ int mixed_rr_to_kR(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, con
 // 2r / 2r+1 (r = iw + nw (n + nw nu)), K' = [cos p | sin p] with koff = round_up(nr_ep, 8).
 template <bool BF16, int NPL>
 __global__ void rr_rotate_pack_kernel(const float2* __restrict__ gk, const double2* __restrict__ uk, int nw,
-                                      int nm, int nr_ep, int64_t nk, int64_t rows_pad_k, int64_t KC,
+                                      int nband, int nm, int nr_ep, int64_t nk, int64_t rows_pad_k, int64_t KC,
                                       uint8_t* __restrict__ planes, int64_t plane_bytes) {
-  const int64_t nd = (int64_t)nw * nw * nm;  // complex rows r per k
+  const int64_t nd = (int64_t)nw * nband * nm;  // complex rows r per k
   const int64_t koff = sin_offset(nr_ep);
   const int64_t npc = koff / 8;               // 8-wide p chunks
   const int64_t total = nk * nd * npc;
-  const int64_t ndata = nd * nr_ep;           // complex length of g_k
+  const int64_t ndata = (int64_t)nw * nw * nm * nr_ep;  // complex length of g_k
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
     int64_t r = idx % nd;
     int64_t rest = idx / nd;
     int64_t pc = rest % npc, k = rest / npc;
     int iw = (int)(r % nw);
-    int n = (int)((r / nw) % nw);
-    int nu = (int)(r / ((int64_t)nw * nw));
+    int n = (int)((r / nw) % nband);
+    int nu = (int)(r / ((int64_t)nw * nband));
     const float2* g = gk + k * ndata;
-    const double2* u = uk + (k * nw + n) * nw;
+    const double2* u = uk + (k * nband + n) * nw;
     double re[8], im[8];
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
@@ -880,6 +893,91 @@ __global__ void rr_rotate_pack_kernel(const float2* __restrict__ gk, const doubl
 __global__ void c128_to_c64_kernel(const double2* __restrict__ in, float2* __restrict__ out, int64_t n) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     out[i] = make_float2((float)in[i].x, (float)in[i].y);
+}
+
+// ---- windowed kR->kq of the Boltzmann consumer on the tensor cores --------------------------------
+// A2 planes of G_k = g(k, Rp) u_k (nband columns of u_k) for nk points, one block of bte_rows_pad(nw, nband,
+// nm) rows per k, through the model's g(Re, Rp) planes (mixed flag of epb_model_create).
+int64_t bte_rows_pad(int64_t nw, int64_t nband, int64_t nm) { return round_up(2 * nw * nband * nm, 128); }
+int64_t bte_a2_bytes(epb_model* m, int64_t nk, int64_t nband) {
+  return MX_NPL * plane_bytes_for(bte_rows_pad(m->nw, nband, m->nm) * nk, kchunks(m->nr_ep));
+}
+int64_t bte_b_bytes(epb_model* m, int64_t ncols) { return MX_NPL * plane_bytes_for(round_up(ncols, MX_NT), kchunks(m->nr_ep)); }
+
+int bte_pack_kR(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double2* uk, int nband, uint8_t* a2) {
+  MixedModel* mm = (MixedModel*)m->mixed;
+  EPB_CHECK_ARG(mm, "windowed kR->kq: the model was created without the mixed operand planes");
+  if (nk == 0) return EPB_OK;
+  const int64_t nw = m->nw, nm = m->nm, nd_ep = nw * nw * nm * m->nr_ep;
+  const int64_t KC_el = kchunks(m->nr_el), KC_ep = kchunks(m->nr_ep);
+  const int64_t rpk = bte_rows_pad(nw, nband, nm);
+  const int64_t a2_plane = plane_bytes_for(rpk * nk, KC_ep);
+  if (rpk != 2 * nw * nband * nm) EPB_CUDA(cudaMemsetAsync(a2, 0, MX_NPL * a2_plane, ctx->stream));
+  int64_t kc = ((int64_t)768 << 20) / (8 * nd_ep);
+  kc = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(kc, 256), nk));
+  const int64_t bbytes = MX_NPL * plane_bytes_for(round_up(kc, MX_NT), KC_el);
+  void* ws = nullptr;
+  EPB_TRY(ws_get(ctx, EPB_WS_PASS4, bbytes + 8 * nd_ep * kc + 2048, &ws));
+  uint8_t* base = (uint8_t*)(((uintptr_t)ws + 1023) & ~uintptr_t(1023));
+  float* C0 = (float*)(base + ((bbytes + 1023) & ~int64_t(1023)));
+  for (int64_t k0 = 0; k0 < nk; k0 += kc) {
+    const int64_t kn = std::min(kc, nk - k0);
+    Planes Bk;
+    EPB_TRY(pack_b_phase(ctx, m->rs_el, xk + 3 * k0, nullptr, 1, kn, Bk, base));
+    EPB_TRY(split_gemm(ctx, EPB_PROF_UMMA_RR, mm->EP, Bk, mm->EP.rows_pad / 128, 1, 2 * nd_ep, kn, false, C0, 0,
+                       2 * nd_ep));
+    const int64_t total = kn * nw * nband * nm * (sin_offset(m->nr_ep) / 8);
+    prof_begin(ctx, EPB_PROF_RR_ROT);
+    rr_rotate_pack_kernel<MX_BF16, MX_NPL><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
+        (const float2*)C0, uk + k0 * nw * nband, (int)nw, nband, (int)nm, (int)m->nr_ep, kn, rpk, KC_ep,
+        a2 + k0 * rpk / 128 * KC_ep * TILE_BYTES, a2_plane);
+    prof_end(ctx);
+    EPB_LAUNCH_CHECK();
+  }
+  return EPB_OK;
+}
+
+// C (complex64 columns of nw nband nm rows, column stride ldc complex) for ncols phase columns x (3 x ncols;
+// ncols a multiple of 128): column tile t of group g multiplies the A2 block grp_a[g] (see bte_pack_kR),
+// tiles [grp[g], grp[g + 1]). Stream-ordered; the timeout flag is left for split_gemm_check.
+int bte_kq_grouped(epb_ctx* ctx, epb_model* m, const uint8_t* a2, int64_t nk_a2, int nband, const double* x,
+                   int64_t ncols, const int64_t* grp, const int64_t* grp_a, int64_t ngrp, uint8_t* bmem, float2* C,
+                   int64_t ldc) {
+  EPB_CHECK_ARG(ncols % MX_NT == 0, "windowed kR->kq: column count must be a multiple of 128");
+  if (ncols == 0 || ngrp == 0) return EPB_OK;
+  const int64_t KC_ep = kchunks(m->nr_ep), rpk = bte_rows_pad(m->nw, nband, m->nm);
+  Planes A, B;
+  A.rows_pad = rpk * nk_a2;
+  A.KC = KC_ep;
+  A.plane_bytes = plane_bytes_for(A.rows_pad, KC_ep);
+  A.npl = MX_NPL;
+  A.p = const_cast<uint8_t*>(a2);
+  EPB_TRY(pack_b_phase(ctx, m->rs_ep, x, nullptr, 1, ncols, B, bmem));
+  int* err = ctx->dstat + 2;
+  SplitGemmArgs a{};
+  a.A = A.p;
+  a.B = B.p;
+  a.a_plane_bytes = A.plane_bytes;
+  a.b_plane_bytes = B.plane_bytes;
+  a.KC = (int)KC_ep;
+  a.m_tiles = rpk / 128;
+  a.n_tiles = ncols / MX_NT;
+  a.m_fastest = 1;
+  a.m_tiles_per_batch = rpk / 128;
+  a.m_valid = 2 * m->nw * nband * m->nm;
+  a.n_valid = ncols;
+  a.C = (float*)C;
+  a.c_batch_stride = 0;
+  a.ldc_n = 2 * ldc;
+  a.err = err;
+  a.timeout = 4000000000LL;
+  a.grp = grp;
+  a.grp_a = grp_a;
+  a.ngrp = ngrp;
+  prof_begin(ctx, EPB_PROF_UMMA_KQ);
+  int st = launch_split_gemm<MX_BF16, MX_NPL, MX_NT>(ctx, a);
+  prof_end(ctx);
+  return st;
 }
 
 // Rotation + |g|^2 fold + in-place reduction, FP32, one (k, q) block at a time per CTA:
@@ -1121,7 +1219,7 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
       const int64_t total = nko * nd * (sin_offset(m->nr_ep) / 8);
       prof_begin(ctx, EPB_PROF_RR_ROT);
       rr_rotate_pack_kernel<MX_BF16, MX_NPL><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
-          (const float2*)C0, Hk, (int)nw, (int)nm, (int)m->nr_ep, nko, rows_pad_k, KC_ep, A2.p, A2.plane_bytes);
+          (const float2*)C0, Hk, (int)nw, (int)nw, (int)nm, (int)m->nr_ep, nko, rows_pad_k, KC_ep, A2.p, A2.plane_bytes);
       prof_end(ctx);
       EPB_LAUNCH_CHECK();
     }

@@ -18,7 +18,7 @@ OMEGA_ACOUSTIC = 0.01 * 0.03674932248 * 2 * 1e-3
 
 
 def serta(dm, ngrid, wmin, wmax, mu, temperature, smearing, method=5, omega_cutoff=OMEGA_ACOUSTIC, lattice=None,
-          volume=1.0, spin=2.0, prec=PREC_FP64, k_batch=32, want_inv_tau=False, inv_tau_cap=None):
+          volume=1.0, spin=2.0, prec=PREC_FP64, k_batch=0, want_inv_tau=False, inv_tau_cap=None, pair_chunk=0):
     """(sigma (3, 3), stats, inv_tau or None) for the model `dm` (pipeline.DeviceModel)."""
     import torch
 
@@ -30,6 +30,7 @@ def serta(dm, ngrid, wmin, wmax, mu, temperature, smearing, method=5, omega_cuto
     for i, v in enumerate(np.asarray(L, dtype=np.float64).reshape(-1, order="F")):
         p.lattice[i] = v
     p.method, p.prec, p.k_batch = int(method), int(prec), int(k_batch)
+    p.pair_chunk = int(pair_chunk)
     sig = np.zeros(9)
     stats = (C.c_int64 * 4)()
     cap = 0

@@ -480,7 +480,8 @@ typedef struct {
   int32_t method;           /* occupation method 1..6 (bte_scattering_core.jl:9-84)               */
   int32_t prec;             /* EPB_PREC_FP64, or EPB_PREC_MIXED: g(k, Rp) on the tensor cores (model
                                created with the mixed flag), everything else FP64                  */
-  int64_t k_batch;          /* kept k per batch (<= 256)                                         */
+  int64_t k_batch;          /* kept k per batch (<= 256); <= 0: 128                              */
+  int64_t pair_chunk;       /* (k, q) pairs per rotation launch, a multiple of 128; <= 0: 65536   */
 } epb_bte_params;
 
 /* SERTA conductivity over commensurate k = q grids: electron states, windows and phonons on the grid,

@@ -62,3 +62,27 @@ def test_gpu_serta_mixed_vs_fp64(gpu_lib):
     assert st64 == stmx
     assert np.max(np.abs(smx - s64)) <= 1e-4 * np.abs(s64).max()
     np.testing.assert_allclose(itmx, it64, rtol=1e-4, atol=1e-6 * np.abs(it64).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k_batch,pair_chunk", [(2, 256), (7, 128), (32, 0)])
+def test_gpu_serta_mixed_grouped(gpu_lib, k_batch, pair_chunk):
+    """The grouped tensor-core kR->kq (pairs of several kept k per launch, each padded to 128 columns,
+    a kept k split across column chunks when pair_chunk is small) gives the same rates as the FP64
+    path within the mixed tolerance, for any batching."""
+    from epb200 import bte, pipeline
+
+    m = synth.make_model(8, 2, 2, 1, seed=62)
+    ng = 8
+    x, _ = BO.grid_points(ng)
+    E = O.eigvals_batched(np.asfortranarray(
+        O.fourier_batched(m.el_ham.op_r, 64, m.el_ham.irvec, x).reshape(8, 8, -1, order="F")))
+    ef = float(np.median(E[4]))
+    dm = pipeline.DeviceModel(m, mixed=True)
+    args = (dm, ng, ef - 1.0, ef + 1.0, ef, 0.08, 0.06)
+    s64, st64, it64 = bte.serta(*args, prec=bte.PREC_FP64, want_inv_tau=True)
+    smx, stmx, itmx = bte.serta(*args, prec=1, want_inv_tau=True, k_batch=k_batch, pair_chunk=pair_chunk)
+    assert st64 == stmx and stmx["pairs"] > 128 * stmx["kept_k"] // 4
+    assert np.max(np.abs(smx - s64)) <= 1e-4 * np.abs(s64).max()
+    np.testing.assert_allclose(itmx, it64, rtol=1e-4, atol=1e-6 * np.abs(it64).max())
+
