@@ -622,7 +622,8 @@ int epb_bte_serta(epb_ctx* ctx, epb_model* m, const epb_bte_params* prm, double*
   for (int64_t k0 = 0; k0 < N; k0 += HC) {
     const int64_t kn = std::min(HC, N - k0);
     EPB_TRY(fourier_f64(ctx, m->ham, nw2, nw2, m->rs_el, xg + 3 * k0, kn, U + k0 * nw2, nw2));
-    EPB_TRY(eigh_async(ctx, U + k0 * nw2, nw, kn, E + k0 * nw, true, nullptr, EPB_PREC_FP64));
+    // the mixed mode solves in FP32 and refines in FP64 (eigenvalues to the FP64 level, vectors to ~1e-12)
+    EPB_TRY(eigh_async(ctx, U + k0 * nw2, nw, kn, E + k0 * nw, true, nullptr, prm->prec));
   }
   EPB_TRY(window_filter(ctx, E, nw, N, prm->wmin, prm->wmax, bmin, bmax, keep, nkeep_d, nullptr));
   // 2. phonons on the grid
@@ -630,7 +631,7 @@ int epb_bte_serta(epb_ctx* ctx, epb_model* m, const epb_bte_params* prm, double*
     const int64_t qn = std::min(HC, N - q0);
     EPB_TRY(fourier_f64(ctx, m->dyn, (int64_t)nm * nm, (int64_t)nm * nm, m->rs_ph, xg + 3 * q0, qn,
                         uph + q0 * nm * nm, (int64_t)nm * nm));
-    EPB_TRY(eigh_async(ctx, uph + q0 * nm * nm, nm, qn, om + q0 * nm, true, m->mass, EPB_PREC_FP64));
+    EPB_TRY(eigh_async(ctx, uph + q0 * nm * nm, nm, qn, om + q0 * nm, true, m->mass, prm->prec));
   }
   EPB_TRY(eigh_check(ctx));
   int64_t hk[2];

@@ -20,6 +20,7 @@ using ElectronPhonon: WannierObject, Vec3
 
 const LIB = Ref(joinpath(@__DIR__, "..", "lib", "libepb200.so"))
 const PREC = Ref{Cint}(1)  # 0: plain FP64, 1: split-BF16 tensor cores + FP32/FP64 eigensolve
+const NULLDEV = CuPtr{Cvoid}(0)  # an absent optional device buffer
 
 last_error() = unsafe_string(ccall((:epb_last_error, LIB[]), Cstring, ()))
 check(st::Integer) = st == 0 || error("libepb200: status $st: $(last_error())")
@@ -126,7 +127,7 @@ function ElectronPhonon.get_eph_RR_to_kR_batched!(ep_ekpR_all::CuArray{ComplexF6
     nw, nband, nk = size(uks)
     nmodes = div(epmat.ndata, nw^2 * nr_ep)
     xk = xk_device(ks)
-    ph = additional_phase === nothing ? CU_NULL : pointer(additional_phase)
+    ph = additional_phase === nothing ? NULLDEV : pointer(additional_phase)
     check(ccall((:epb_eph_RR_to_kR, LIB[]), Cint,
                 (Ptr{Cvoid}, CuPtr{ComplexF64}, Int64, Int64, Int64, Ptr{Cvoid}, CuPtr{Float64}, Int64,
                  CuPtr{ComplexF64}, Int64, CuPtr{ComplexF64}, CuPtr{ComplexF64}, Cint),
@@ -143,7 +144,7 @@ function ElectronPhonon.get_eph_kR_to_kq_batched!(ep_kq_all::CuArray{ComplexF64,
                 (Ptr{Cvoid}, CuPtr{ComplexF64}, Int64, Int64, Int64, Int64, Int64, CuPtr{ComplexF64}, Int64,
                  CuPtr{ComplexF64}, Int64, CuPtr{ComplexF64}, CuPtr{Float64}, CuPtr{ComplexF64}, CuPtr{Float64}, Cint),
                 ctx().h, ep_kR, size(ep_kR, 1), nw, nbandk, nmodes, size(ep_kR, 2), phase, nq, ukqs, nbandkq,
-                u_phs, ωq === nothing ? CU_NULL : ωq, ep_kq_all, g2_out === nothing ? CU_NULL : g2_out, PREC[]))
+                u_phs, ωq === nothing ? NULLDEV : ωq, ep_kq_all, g2_out === nothing ? NULLDEV : g2_out, PREC[]))
     ep_kq_all
 end
 
@@ -155,7 +156,7 @@ function ElectronPhonon.eph_apply_rotations!(ep_kq_all::CuArray{ComplexF64,4}, g
                 (Ptr{Cvoid}, CuPtr{ComplexF64}, Int64, Int64, Int64, Int64, Int64, CuPtr{ComplexF64}, Int64,
                  CuPtr{ComplexF64}, CuPtr{Float64}, CuPtr{ComplexF64}, CuPtr{Float64}),
                 ctx().h, g, nw * nbandk * nmodes, nw, nbandk, nmodes, nq, ukqs, nbandkq, u_phs,
-                ωq === nothing ? CU_NULL : ωq, ep_kq_all, g2_out === nothing ? CU_NULL : g2_out))
+                ωq === nothing ? NULLDEV : ωq, ep_kq_all, g2_out === nothing ? NULLDEV : g2_out))
     ep_kq_all
 end
 
@@ -171,6 +172,83 @@ function window_filter(E::CuMatrix{Float64}, wmin::Real, wmax::Real)
                 ctx().h, E, nw, nk, wmin, wmax, bmin, bmax, keep, nkeep, nbelow))
     n = Int(Array(nkeep)[1])
     bmin, bmax, keep[1:n] .+ Int32(1), nbelow   # 1-based k indices for the Julia side
+end
+
+# ---- outer-q chain (wannier_to_bloch.jl:277-300, wannier_to_bloch_batched.jl:317-377) -----------
+function ElectronPhonon.get_eph_Rq_to_kq_batched!(ep_kq_all::CuArray{ComplexF64,4},
+        itp_epobj_eRpq::ElectronPhonon.BatchedWannierInterpolator, ks, uks::CuArray{ComplexF64,3},
+        ukqs::CuArray{ComplexF64,3}; ws = nothing)
+    nbandkq, nbandk, nmodes, nk = size(ep_kq_all)
+    nw = size(uks, 1)
+    parent = itp_epobj_eRpq.parent
+    @assert parent.ndata == nw^2 * nmodes
+    check(ccall((:epb_eph_Rq_to_kq, LIB[]), Cint,
+                (Ptr{Cvoid}, CuPtr{ComplexF64}, Int64, Int64, Ptr{Cvoid}, CuPtr{Float64}, Int64, CuPtr{ComplexF64},
+                 Int64, CuPtr{ComplexF64}, Int64, CuPtr{Float64}, CuPtr{ComplexF64}, CuPtr{Float64}, Cint),
+                ctx().h, parent.op_r, nw, nmodes, rset(parent.irvec).h, xk_device(ks), nk, uks, nbandk, ukqs, nbandkq,
+                NULLDEV, ep_kq_all, NULLDEV, PREC[]))
+    ep_kq_all
+end
+
+# g(Re, q) for a list of q from the "ph"-layout epmat (rows (i, j, nu, Re)), in the eigenmode basis u_phs
+function eph_RR_to_Rq_batched!(ep_Rq_all::CuArray{ComplexF64,3}, epmat::ElectronPhonon.WannierObject, xqs,
+        u_phs::CuArray{ComplexF64,3})
+    nm = size(u_phs, 1)
+    nr_el = length(epmat.irvec_next)
+    nw = isqrt(div(epmat.ndata, nm * nr_el))
+    check(ccall((:epb_eph_RR_to_Rq, LIB[]), Cint,
+                (Ptr{Cvoid}, CuPtr{ComplexF64}, Int64, Int64, Int64, Ptr{Cvoid}, CuPtr{Float64}, Int64,
+                 CuPtr{ComplexF64}, CuPtr{ComplexF64}, Cint),
+                ctx().h, epmat.op_r, nw, nm, nr_el, rset(epmat.irvec).h, xk_device(xqs), size(u_phs, 3), u_phs,
+                ep_Rq_all, PREC[]))
+    ep_Rq_all
+end
+
+# ---- calculator hooks (calculator_utils.jl:36-50, boltzmann_calculator.jl:336-362) ----------------
+function ElectronPhonon.eph_window_scatter!(g2_out::CuArray{Float64}, ωq_out::CuArray{Float64},
+        g2vals::CuArray{Float64,4}, imap_i_col::CuVector{Int}, imap_f::CuMatrix{Int}, ikqs, ωq::CuMatrix{Float64},
+        nbandkq::Int, nbandk::Int, nm::Int, nq_batch::Int, ni_stride::Int, i0::Int)
+    ikq_d = CuArray{Int64}(collect(ikqs))
+    check(ccall((:epb_eph_window_scatter, LIB[]), Cint,
+                (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, CuPtr{Float64}, CuPtr{Int64}, CuPtr{Int64}, Int64,
+                 CuPtr{Int64}, CuPtr{Float64}, Int64, Int64, Int64, Int64, Int64, Int64),
+                ctx().h, g2_out, ωq_out, g2vals, imap_i_col, imap_f, size(imap_f, 1), ikq_d, ωq, nbandkq, nbandk,
+                nm, nq_batch, ni_stride, i0))
+    nothing
+end
+
+function ElectronPhonon.bte_window_accumulate!(Sₒ_out::CuMatrix{Float64}, Sᵢ_out, g2vals::CuArray{Float64,4},
+        ωqmat::CuMatrix{Float64}, imap_i_at_k::CuVector{Int}, imap_f::CuMatrix{Int}, ikqs, e_i, e_f, wf, μs, Ts,
+        ηs, method::Int, ω_cutoff, nbandkq::Int, nbandk::Int, nmodes::Int, nq_batch::Int, i0::Int)
+    ikq_d = CuArray{Int64}(collect(ikqs))
+    dev(x) = x isa CuArray ? x : CuArray{Float64}(collect(x))
+    sin_ptr = Sᵢ_out === nothing ? NULLDEV : Sᵢ_out
+    ni_tile, n_f = Sᵢ_out === nothing ? (0, 0) : (size(Sᵢ_out, 1), size(Sᵢ_out, 2))
+    check(ccall((:epb_bte_window_accumulate, LIB[]), Cint,
+                (Ptr{Cvoid}, CuPtr{Float64}, Int64, CuPtr{Float64}, Int64, Int64, CuPtr{Float64}, CuPtr{Float64},
+                 CuPtr{Int64}, CuPtr{Int64}, Int64, CuPtr{Int64}, CuPtr{Float64}, CuPtr{Float64}, CuPtr{Float64},
+                 CuPtr{Float64}, CuPtr{Float64}, CuPtr{Float64}, Int64, Cint, Float64, Int64, Int64, Int64, Int64,
+                 Int64),
+                ctx().h, Sₒ_out, size(Sₒ_out, 1), sin_ptr, ni_tile, n_f, g2vals, ωqmat, imap_i_at_k, imap_f,
+                size(imap_f, 1), ikq_d, dev(e_i), dev(e_f), dev(wf), dev(μs), dev(Ts), dev(ηs), length(μs), method,
+                ω_cutoff, nbandkq, nbandk, nmodes, nq_batch, i0))
+    nothing
+end
+
+# ---- EPW reader (model_new.jl:487-568): the epmatwp file straight into HBM -----------------------
+function read_epmat_device(filename, nw, nmodes, nr_el, nr_ep, irvec_el, irvec_ep, ind_el, ind_ep, ndegen_el,
+        ndegen_ep, epmat_outer_momentum; skip_ndegen_ep = false, ndegen_pre_divided = false)
+    layout = epmat_outer_momentum == "ph" ? Cint(1) : Cint(0)
+    nd = nw^2 * nmodes
+    out = layout == 0 ? CuMatrix{ComplexF64}(undef, nd * nr_ep, nr_el) : CuMatrix{ComplexF64}(undef, nd * nr_el, nr_ep)
+    nel = Int32.(ndegen_el); nep = Int32.(ndegen_ep)
+    check(ccall((:epb_read_epmat, LIB[]), Cint,
+                (Ptr{Cvoid}, Cstring, Int64, Int64, Int64, Int64, Ptr{Int64}, Ptr{Int64}, Ptr{Int32}, Int64,
+                 Ptr{Int32}, Int64, Int64, Cint, Cint, Cint, CuPtr{ComplexF64}),
+                ctx().h, filename, nw, nmodes, nr_el, nr_ep, Int64.(ind_el), Int64.(ind_ep), nel, size(nel, 1),
+                nep, size(nep, 1), size(nep, 2), skip_ndegen_ep, ndegen_pre_divided, layout, out))
+    layout == 0 ? ElectronPhonon.WannierObject(irvec_el, out; irvec_next = irvec_ep) :
+                  ElectronPhonon.WannierObject(irvec_ep, out; irvec_next = irvec_el)
 end
 
 end # module
