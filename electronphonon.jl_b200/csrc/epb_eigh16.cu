@@ -73,42 +73,49 @@ __device__ int onesided_sweeps(typename cplx<T>::type (&a)[E16], T tol, int max_
       for (int i = 0; i < E16; ++i) b[i] = shfl2(a[i], src);
       const T nb = shfl(nrm, src);
       const bool isP = l < pl;
+      // the p lane (l < partner) forms g = a_p^H a_q, decides and builds both columns' coefficients; the q
+      // lane takes its coefficients and new norm by shuffle (one decision per pair, no divergent update)
       C g0 = mk2(T(0), T(0)), g1 = mk2(T(0), T(0));  // two chains: shorter dependency
 #pragma unroll
       for (int i = 0; i < E16; i += 2) {
-        if (isP) {
-          cfma_conj(g0, a[i], b[i]);
-          cfma_conj(g1, a[i + 1], b[i + 1]);
-        } else {
-          cfma_conj(g0, b[i], a[i]);
-          cfma_conj(g1, b[i + 1], a[i + 1]);
-        }
+        cfma_conj(g0, a[i], b[i]);
+        cfma_conj(g1, a[i + 1], b[i + 1]);
       }
       const C g = mk2(g0.x + g1.x, g0.y + g1.y);
-      const T ap = isP ? nrm : nb, aq = isP ? nb : nrm;
       const T ag = sqrt(g.x * g.x + g.y * g.y);
-      if (ag > tol * sqrt(ap * aq) && ag > T(0)) {
-        rotated = 1;
-        const T tau = (aq - ap) / (T(2) * ag);
+      T c = T(1), fx = T(0), fy = T(0), qx = T(0), qy = T(0), np_ = nrm, nq_ = nb;
+      int rot = 0;
+      if (isP && ag > tol * sqrt(nrm * nb) && ag > T(0)) {
+        rot = 1;
+        const T tau = (nb - nrm) / (T(2) * ag);
         const T t = (tau >= T(0) ? T(1) : T(-1)) / (fabs(tau) + sqrt(T(1) + tau * tau));
-        const T c = T(1) / sqrt(T(1) + t * t), s = t * c;
-        const C e = mk2(g.x / ag, g.y / ag);
-        if (isP) {
-          const C ec = mk2(e.x, -e.y);
+        c = T(1) / sqrt(T(1) + t * t);
+        const T s = t * c, ex = g.x / ag, ey = g.y / ag;
+        fx = -s * ex;  // p: a_p <- c a_p - s conj(e) a_q
+        fy = s * ey;
+        qx = s * ex;   // q: a_q <- c a_q + s e a_p
+        qy = s * ey;
+        np_ = nrm - t * ag;
+        nq_ = nb + t * ag;
+      }
+      const T c_r = shfl(c, src), qx_r = shfl(qx, src), qy_r = shfl(qy, src), nq_r = shfl(nq_, src);
+      const int rot_r = __shfl_sync(0xffffffffu, rot, src);
+      if (!isP) {
+        rot = rot_r;
+        c = c_r;
+        fx = qx_r;
+        fy = qy_r;
+        np_ = nq_r;
+      }
+      if (rot) {
+        rotated = 1;
+        const C f = mk2(fx, fy);
 #pragma unroll
-          for (int i = 0; i < E16; ++i) {
-            C u = cmul(ec, b[i]);
-            a[i] = mk2(c * a[i].x - s * u.x, c * a[i].y - s * u.y);
-          }
-          nrm = ap - t * ag;
-        } else {
-#pragma unroll
-          for (int i = 0; i < E16; ++i) {
-            C u = cmul(e, b[i]);
-            a[i] = mk2(s * u.x + c * a[i].x, s * u.y + c * a[i].y);
-          }
-          nrm = aq + t * ag;
+        for (int i = 0; i < E16; ++i) {
+          const C u = cmul(f, b[i]);
+          a[i] = mk2(c * a[i].x + u.x, c * a[i].y + u.y);
         }
+        nrm = np_;
       }
     }
     if (!__any_sync(0xffffffffu, rotated)) break;
@@ -195,7 +202,7 @@ __device__ __forceinline__ void write_sorted(const Eigh16Args& a, int64_t b, boo
 // MODE 0: whole solve in FP64 (sorted output).  MODE 1: FP32 sweeps only; writes the normalised,
 // unsorted FP32 columns to a.V32 (16 x 16 per matrix) for MODE 2.
 template <int MODE>
-__global__ void __launch_bounds__(128) eigh16_jacobi_kernel(Eigh16Args a) {
+__global__ void __launch_bounds__(128, MODE == 0 ? 1 : 4) eigh16_jacobi_kernel(Eigh16Args a) {
   using T = typename std::conditional<MODE == 0, double, float>::type;
   using C = typename cplx<T>::type;
   const int lane = threadIdx.x & 31;
