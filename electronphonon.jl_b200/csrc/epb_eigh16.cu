@@ -449,14 +449,23 @@ __global__ void __launch_bounds__(128, 3) eigh16_refine2_kernel(Eigh16Args a) {
         } else {
           const double2 sp = make_double2(s.x - 0.5 * g.x * (dk + d), s.y - 0.5 * g.y * (dk + d));
           const double gap = dp - dpk;
-          const double asp = sqrt(sp.x * sp.x + sp.y * sp.y);
+          const double asp2 = sp.x * sp.x + sp.y * sp.y;
           t = make_double2(-0.5 * g.x, -0.5 * g.y);
           if (k < n && l < n) {
-            if (asp < 0.1 * fabs(gap)) {
-              t.x += sp.x / gap;
-              t.y += sp.y / gap;
-              lam_corr += asp * asp / gap;
-            } else if (asp > 1e-13 * sigma) {
+            if (asp2 < 0.01 * gap * gap) {
+              // 1 / gap: FP32 reciprocal + one FP64 Newton step (~1e-14 relative; t itself is O(1e-6))
+              const double ag = fabs(gap);
+              double rg;
+              if (ag > 1e-30 && ag < 1e30) {
+                rg = (double)__frcp_rn((float)gap);
+                rg = rg * (2.0 - gap * rg);
+              } else {
+                rg = 1.0 / gap;
+              }
+              t.x += sp.x * rg;
+              t.y += sp.y * rg;
+              lam_corr += asp2 * rg;
+            } else if (asp2 > 1e-26 * sigma * sigma) {
               cluster = true;
             }
           }
