@@ -398,7 +398,11 @@ __global__ void __launch_bounds__(128, 3) eigh16_refine2_kernel(Eigh16Args a) {
       }
     }
     double lam = 0.0;
-    bool cluster = false;
+    bool cluster = false;  // sticky over the iterations: once a pair is out of first-order range, the matrix is flagged
+    // first-order range |S'_kl| < theta |gap|: the update leaves O(theta^2) mixing per iteration. With an exact
+    // slow path for flagged matrices (public API) theta = 1e-3 (two iterations: O(1e-12)); without one (the
+    // pass's eigenvectors) theta = 0.1, correcting as much as first order can.
+    const double th2 = a.flag_list ? 1e-6 : 1e-2;
     for (int it = 0; it < a.refine; ++it) {
 #pragma unroll
       for (int r = 0; r < 8; ++r) V[(r0 + r) * RLD + l] = v[r];
@@ -424,7 +428,6 @@ __global__ void __launch_bounds__(128, 3) eigh16_refine2_kernel(Eigh16Args a) {
       fll -= 1.0;
       const double dp = d * (1.0 - fll);
       double lam_corr = 0.0;
-      cluster = false;
       double2 u[8];  // V t accumulated over k
 #pragma unroll
       for (int r = 0; r < 8; ++r) u[r] = make_double2(0.0, 0.0);
@@ -452,7 +455,7 @@ __global__ void __launch_bounds__(128, 3) eigh16_refine2_kernel(Eigh16Args a) {
           const double asp2 = sp.x * sp.x + sp.y * sp.y;
           t = make_double2(-0.5 * g.x, -0.5 * g.y);
           if (k < n && l < n) {
-            if (asp2 < 0.01 * gap * gap) {
+            if (asp2 < th2 * gap * gap) {
               // 1 / gap: FP32 reciprocal + one FP64 Newton step (~1e-14 relative; t itself is O(1e-6))
               const double ag = fabs(gap);
               double rg;

@@ -84,6 +84,24 @@ def test_eigh_batched(B, n, prec):
     assert np.max(np.abs(ev - eref)) <= tol * scale
 
 
+@pytest.mark.parametrize("n", [8, 16, 32, 96])
+def test_eigh_clusters_stress(B, n):
+    """Every instance with planted 2-4-fold clusters spaced 1e-10 (thousands for the register-resident
+    n <= 16 solver, where a first-order refinement range that was too wide once left 0.5 % of such
+    matrices with non-orthogonal cluster vectors): eigenvalues to 1e-11 and U diag(E) U^H to 1e-10 of the
+    largest |eigenvalue|, FP32 solve + FP64 refinement."""
+    count = 2400 if n <= 16 else 300
+    ns, mats = synth.config3_matrices(count, seed=101 + n, sizes=[n], degenerate_frac=1.0)
+    h = np.asfortranarray(np.stack(mats, axis=-1))
+    E, U = B.eigen_batched(B.jl(h), prec=1)
+    E, U = B.host(E), B.host(U)
+    eref = O.eigvals_batched(h.copy())
+    scale = np.abs(eref).max()
+    assert np.max(np.abs(E - eref)) <= 1e-11 * scale
+    rec = np.einsum("ijk,jk,ljk->ilk", U, E, U.conj())
+    assert np.max(np.abs(rec - h)) <= 1e-10 * scale
+
+
 def test_eigh_degenerate_clusters(B):
     """Planted 2-4-fold clusters spaced 1e-10: eigenvalues and the cluster projectors match."""
     ns, mats = synth.config3_matrices(200, seed=7, sizes=[8, 16, 24], degenerate_frac=1.0)
