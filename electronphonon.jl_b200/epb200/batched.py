@@ -172,10 +172,12 @@ def eigen_varlen(mats, prec=PREC_FP64, jobz="V"):
 
 
 def _fourier_hk_batched(itp, xks, prec=PREC_FP64):
+    """H(k) in FP64 in both modes: the mixed mode's FP64 refinement reads H, so an FP64 H(k) gives band
+    energies at the FP64 level (the split-BF16 H(k) of the e-ph pass is FP32-level). `prec` is unused."""
     nw = int(round(np.sqrt(itp.parent.ndata)))
     if nw * nw != itp.parent.ndata:
         raise ValueError(f"ndata={itp.parent.ndata} is not a perfect square; expected nw^2 for a Hamiltonian")
-    hk = get_fourier_batched(itp, xks, prec=prec)
+    hk = get_fourier_batched(itp, xks, prec=PREC_FP64)
     nk = hk.shape[0]
     return hk.view(nk, nw, nw)
 
