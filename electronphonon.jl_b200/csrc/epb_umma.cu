@@ -1144,6 +1144,51 @@ __global__ void __launch_bounds__(256, 2) eph_rot_reduce_f32_kernel(
   if (kcur >= 0) flush(kcur);
 }
 
+// The same rotation + |g|^2 fold + reduction for any (nw, nm) the tiled kernel above does not cover: one
+// CTA per (k, q) block, operands and T in shared memory, FP32 arithmetic, the per-mode sums of a block
+// added in shared memory (FP64) and then once into g2sum. Same inputs and outputs as the tiled kernel.
+__global__ void __launch_bounds__(256) eph_rot_reduce_gen_kernel(
+    const float2* __restrict__ g, int64_t g_stride, const float2* __restrict__ ukq, const float2* __restrict__ uph,
+    const double* __restrict__ omega, int nw, int nm, int64_t nkb, int64_t nq, double* __restrict__ g2sum,
+    double* __restrict__ sample, int64_t stride, int64_t nsamp) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nw2 = nw * nw, nd = nw2 * nm;
+  float2* gs = reinterpret_cast<float2*>(smem_raw);  // g[iw, n, jm]
+  float2* ts = gs + nd;                                // T[m, n, jm]
+  float2* us = ts + nd;                                // u_kq[iw, m]
+  float2* ps = us + nw2;                               // u_ph[jm, nu]
+  double* red = reinterpret_cast<double*>(ps + nm * nm);
+  const int64_t nblk = nkb * nq;
+  for (int64_t blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+    const int64_t kl = blk / nq, q = blk % nq;
+    for (int e = threadIdx.x; e < nd; e += blockDim.x) gs[e] = g[blk * g_stride + e];
+    for (int e = threadIdx.x; e < nw2; e += blockDim.x) us[e] = ukq[blk * nw2 + e];
+    for (int e = threadIdx.x; e < nm * nm; e += blockDim.x) ps[e] = uph[q * nm * nm + e];
+    for (int e = threadIdx.x; e < nm; e += blockDim.x) red[e] = 0.0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < nd; e += blockDim.x) {
+      const int m = e % nw, r = e / nw;  // r = n + nw jm
+      float2 acc = make_float2(0.f, 0.f);
+      for (int iw = 0; iw < nw; ++iw) cfma_conj(acc, us[iw + nw * m], gs[iw + nw * r]);
+      ts[e] = acc;
+    }
+    __syncthreads();
+    const bool samp = sample && (q % stride == 0);
+    double* sq = samp ? sample + ((kl * nsamp) + q / stride) * (int64_t)nd : nullptr;
+    for (int e = threadIdx.x; e < nd; e += blockDim.x) {
+      const int mn = e % nw2, nu = e / nw2;
+      float2 acc = make_float2(0.f, 0.f);
+      for (int jm = 0; jm < nm; ++jm) cfma(acc, ts[mn + nw2 * jm], ps[jm + nm * nu]);
+      const float v = (acc.x * acc.x + acc.y * acc.y) * (float)(0.5 / omega[q * nm + nu]);
+      if (samp) sq[e] = (double)v;
+      atomicAdd(&red[nu], (double)v);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nm; e += blockDim.x) atomicAdd(&g2sum[e + nm * kl], red[e]);
+    __syncthreads();  // red and the operand buffers are rewritten by the next block
+  }
+}
+
 int fourier_f64(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, const epb_rset* rs, const double* xk,
                 int64_t N, double2* out, int64_t ldo);
 int eigh_async(epb_ctx* ctx, double2* A, int64_t n, int64_t batch, double* E, bool want_v, const double* mass,
@@ -1157,7 +1202,11 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
   MixedModel* mm = (MixedModel*)m->mixed;
   const int64_t nw = m->nw, nm = m->nm, nw2 = nw * nw;
   const int64_t nd = nw2 * nm, nd_ep = nd * m->nr_ep;
-  EPB_CHECK_ARG(nw == 16 && nm == 12, "mixed pass: this build instantiates the rotation for nw=16, nm=12");
+  const bool tiled = nw == 16 && nm == 12;  // the register-tiled rotation; other shapes take the generic kernel
+  const size_t gen_smem = 8 * (size_t)(2 * nw2 * nm + nw2 + nm * nm) + 8 * (size_t)nm;
+  EPB_CHECK_ARG(tiled || gen_smem <= 200 * 1024,
+                "mixed pass: a (k, q) block of nw=%lld, nm=%lld needs %zu bytes of shared memory (over 200 KB); use "
+                "the FP64 pass", (long long)nw, (long long)nm, gen_smem);
   const int64_t KO = 256;                               // RR->kR batch (one read of the g(Re,Rp) planes)
   const int64_t kbi = kbi_max < KO ? kbi_max : KO;      // H(k+q) / kR->kq batch
   const int64_t KC_ep = kchunks(m->nr_ep), KC_el = kchunks(m->nr_el);
@@ -1237,7 +1286,20 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
       EPB_TRY(split_gemm(ctx, EPB_PROF_UMMA_KQ, A2i, Bp, rows_pad_k / 128, nki, 2 * nd, nq, false, C2,
                          2 * nd * nq, 2 * nd));
       // rotations, g2, in-place reduction
-      {
+      if (!tiled) {
+        static bool gattr = false;
+        if (!gattr) {
+          EPB_CUDA(cudaFuncSetAttribute(eph_rot_reduce_gen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+          gattr = true;
+        }
+        const unsigned grid = (unsigned)std::min<int64_t>(np, (int64_t)ctx->sm_count * 4);
+        prof_begin(ctx, EPB_PROF_ROT);
+        eph_rot_reduce_gen_kernel<<<grid, 256, gen_smem, ctx->stream>>>(
+            (const float2*)C2, nd, U32, uph32, omega, (int)nw, (int)nm, nki, nq, g2sum + nm * (ko + ki),
+            g2_sample ? g2_sample + (ko + ki) * nsamp * nd : nullptr, sample_stride, nsamp);
+        prof_end(ctx);
+        EPB_LAUNCH_CHECK();
+      } else {
         int64_t nblk = np;
         constexpr int RS = RotSmem<16, 12>::TOTAL;
         static bool rattr = false;

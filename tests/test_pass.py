@@ -79,6 +79,25 @@ def test_gpu_pass_mixed(gpu_lib, nk, nq, kb):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("nw,natom", [(8, 2), (12, 3), (20, 1)])
+def test_gpu_pass_mixed_other_shapes(gpu_lib, nw, natom):
+    """Shapes other than nw = 16, nm = 12 take the generic rotation kernel of the mixed pass (and, for
+    nw > 16, the shared-memory eigensolver): same bars as the config-2 shape against the FP64 CPU port."""
+    from epb200 import pipeline
+    from epb200.batched import host
+
+    m = synth.config2_model(seed=51 + nw, n_el=2, n_ph=1, nw=nw, natom=natom)
+    xks = synth.random_kpoints(6, 15)
+    xqs = synth.random_kpoints(40, 16)
+    dm = pipeline.DeviceModel(m, mixed=True)
+    r = pipeline.run_eph_over_k_and_q(dm, xks, xqs, prec=pipeline.PREC_MIXED, k_batch=4, sample_stride=3)
+    ref = cpu_pass.eph_pass_cpu(m, xks, xqs, sample_stride=3)
+    np.testing.assert_allclose(host(r.ek), ref["ek"], atol=1e-11 * np.abs(ref["ek"]).max())
+    np.testing.assert_allclose(host(r.g2sum), ref["g2sum"], rtol=1e-6)
+    assert _block_rel_err(host(r.g2_sample), ref["g2_sample"]) <= 1e-5
+
+
+@pytest.mark.gpu
 def test_gpu_pass_autotuned_k_batch(gpu_lib):
     """k_batch <= 0: the library times the candidates, keeps one, and the pass equals an explicit run."""
     from epb200 import pipeline
