@@ -24,6 +24,7 @@
 // Every wait is bounded (clock64 budget); on timeout the kernel raises an error flag, drains its
 // own copies and MMAs, frees TMEM and returns (EPB_ERR_TIMEOUT on the host).
 #include <algorithm>
+#include <cstring>
 
 #include "epb_common.cuh"
 
@@ -269,6 +270,8 @@ struct SplitGemmArgs {
   const int64_t* grp;
   const int64_t* grp_a;
   int64_t ngrp;
+  // power-of-two scale applied to C in the epilogue (undoing an operand's pre-scale); 0 = none
+  float cscale;
 };
 
 template <bool BF16, int NPL>
@@ -467,7 +470,10 @@ __global__ void __launch_bounds__(192, 1) split_gemm_kernel(SplitGemmArgs a) {
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
             int64_t col = nt * NT + c0 + j;
-            if (col < a.n_valid) cb[col * a.ldc_n] = (float)((double)v[j] + (double)w[j]);
+            if (col < a.n_valid) {
+              const float val = (float)((double)v[j] + (double)w[j]);
+              cb[col * a.ldc_n] = a.cscale != 0.f ? val * a.cscale : val;
+            }
           }
         }
       }
@@ -551,6 +557,37 @@ int split_gemm(epb_ctx* ctx, int prof_id, const Planes& A, const Planes& B, int6
   return st;
 }
 
+// The FP16x2 configuration (two FP16 planes per operand, three products: h*h, h*l, l*h, about 22 bits),
+// for operands pre-scaled by a power of two into FP16's range; cscale undoes the scale on C.
+int split_gemm_h(epb_ctx* ctx, int prof_id, const Planes& A, const Planes& B, int64_t m_tiles_per_batch,
+                 int64_t batches, int64_t m_valid, int64_t n_valid, bool m_fastest, float* C, int64_t c_batch_stride,
+                 int64_t ldc_n, float cscale) {
+  SplitGemmArgs a{};
+  a.A = A.p;
+  a.B = B.p;
+  a.a_plane_bytes = A.plane_bytes;
+  a.b_plane_bytes = B.plane_bytes;
+  a.KC = (int)A.KC;
+  a.m_tiles = m_tiles_per_batch * batches;
+  a.n_tiles = cdiv(n_valid, MX_NT);
+  a.m_fastest = m_fastest ? 1 : 0;
+  a.m_tiles_per_batch = m_tiles_per_batch;
+  a.m_valid = m_valid;
+  a.n_valid = n_valid;
+  a.C = C;
+  a.c_batch_stride = c_batch_stride;
+  a.ldc_n = ldc_n;
+  a.err = ctx->dstat + 2;
+  a.timeout = 4000000000LL;
+  a.cscale = cscale;
+  EPB_CHECK_ARG(A.KC == B.KC && A.npl == 2 && B.npl == 2, "FP16x2 GEMM: operand planes mismatch");
+  EPB_CHECK_ARG(B.rows_pad >= a.n_tiles * MX_NT, "FP16x2 GEMM: B planes too small");
+  prof_begin(ctx, prof_id);
+  int st = launch_split_gemm<false, 2, MX_NT>(ctx, a);
+  prof_end(ctx);
+  return st;
+}
+
 // Check the device error flag raised by bounded waits (one sync).
 int split_gemm_check(epb_ctx* ctx) {
   int* h = (int*)ctx->pinned;
@@ -605,6 +642,23 @@ int pack_b_phase(epb_ctx* ctx, const epb_rset* rs, const double* xa, const doubl
   prof_begin(ctx, EPB_PROF_SPLIT);
   pack_b_phase_kernel<MX_BF16, MX_NPL><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
       rs->dev, rs->nr, xa, xb, nb, pidx, pair0, N, out.rows_pad, out.KC, out.p, out.plane_bytes);
+  prof_end(ctx);
+  EPB_LAUNCH_CHECK();
+  return EPB_OK;
+}
+
+// Phase planes in the FP16x2 configuration (|phase| <= 1: no scaling needed).
+int pack_b_phase_h(epb_ctx* ctx, const epb_rset* rs, const double* xa, const double* xb, int64_t nb, int64_t N,
+                   Planes& out, uint8_t* mem) {
+  out.rows_pad = round_up(N, MX_NT);
+  out.KC = kchunks(rs->nr);
+  out.plane_bytes = plane_bytes_for(out.rows_pad, out.KC);
+  out.npl = 2;
+  out.p = mem;
+  int64_t total = out.rows_pad * (sin_offset(rs->nr) / 8);
+  prof_begin(ctx, EPB_PROF_SPLIT);
+  pack_b_phase_kernel<false, 2><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
+      rs->dev, rs->nr, xa, xb, nb, nullptr, 0, N, out.rows_pad, out.KC, out.p, out.plane_bytes);
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
@@ -745,7 +799,17 @@ struct MixedModel {
   uint8_t* mem = nullptr;
   Planes H;   // H(R), Hermitian-packed rows (nw^2), K = nr_el
   Planes EP;  // g(Re, Rp), complex rows (2 * nw^2 nm nr_ep), K = nr_el
+  double ep_absmax = 0.0;  // max |Re|, |Im| of g(Re, Rp): scales the FP16x2 kR->kq operand
 };
+
+// max(|Re|, |Im|) over n complex values into *out (non-negative doubles order like their bit patterns).
+__global__ void absmax_c128_kernel(const double2* __restrict__ v, int64_t n, unsigned long long* __restrict__ out) {
+  double mx = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    mx = fmax(mx, fmax(fabs(v[i].x), fabs(v[i].y)));
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(mx));
+}
 
 int mixed_model_prepare(epb_ctx* ctx, epb_model* m) {
   const int64_t nw = m->nw, nd_ep = m->nw * m->nw * m->nm * m->nr_ep;
@@ -767,7 +831,16 @@ int mixed_model_prepare(epb_ctx* ctx, epb_model* m) {
     delete mm;
     return st;
   }
-  m->mixed = mm;
+  m->mixed = mm;  // owned by the model from here on (freed with it on any later failure)
+  // max |g(Re, Rp)| (one sync at model creation)
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(ctx->dstat + 16);  // status words 16-17
+  EPB_CUDA(cudaMemsetAsync(d, 0, 8, ctx->stream));
+  absmax_c128_kernel<<<grid_for(ctx, nd_ep * m->nr_el), 256, 0, ctx->stream>>>(m->epmat, nd_ep * m->nr_el, d);
+  EPB_LAUNCH_CHECK();
+  unsigned long long h = 0;
+  EPB_CUDA(cudaMemcpyAsync(&h, d, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  EPB_CUDA(cudaStreamSynchronize(ctx->stream));
+  std::memcpy(&mm->ep_absmax, &h, 8);
   return EPB_OK;
 }
 
@@ -847,7 +920,7 @@ int mixed_rr_to_kR(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, con
 template <bool BF16, int NPL>
 __global__ void rr_rotate_pack_kernel(const float2* __restrict__ gk, const double2* __restrict__ uk, int nw,
                                       int nband, int nm, int nr_ep, int64_t nk, int64_t rows_pad_k, int64_t KC,
-                                      uint8_t* __restrict__ planes, int64_t plane_bytes) {
+                                      uint8_t* __restrict__ planes, int64_t plane_bytes, double scale = 1.0) {
   const int64_t nd = (int64_t)nw * nband * nm;  // complex rows r per k
   const int64_t koff = sin_offset(nr_ep);
   const int64_t npc = koff / 8;               // 8-wide p chunks
@@ -875,8 +948,8 @@ __global__ void rr_rotate_pack_kernel(const float2* __restrict__ gk, const doubl
           cfma(acc, make_double2(x.x, x.y), u[jw]);
         }
       }
-      re[e] = acc.x;
-      im[e] = acc.y;
+      re[e] = acc.x * scale;
+      im[e] = acc.y * scale;
     }
     const int64_t row0 = k * rows_pad_k + 2 * r;
     double t[8];
@@ -1240,17 +1313,23 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
   const int64_t nsamp = g2_sample ? (nq + sample_stride - 1) / sample_stride : 0;
 
   // ---- q side: phase planes of the q list, u_ph in complex64 ----
+  // kR->kq in the FP16x2 configuration (three products): G_k is pre-scaled by a power of two that keeps
+  // |G| <= sqrt(nw) nr_el max|g(Re,Rp)| below 2^14 (FP16 range), the epilogue multiplies it back out
   Planes Bp;
-  EPB_TRY(pack_b_phase(ctx, m->rs_ep, xq, nullptr, 1, nq, Bp, base + o_bp));
+  EPB_TRY(pack_b_phase_h(ctx, m->rs_ep, xq, nullptr, 1, nq, Bp, base + o_bp));
+  double gbound = std::sqrt((double)nw) * (double)m->nr_el * (mm->ep_absmax > 0.0 ? mm->ep_absmax : 1.0);
+  const int e2 = std::max(-120, std::min(120, 14 - (int)std::ceil(std::log2(gbound))));
+  const double a2_scale = std::ldexp(1.0, e2);
+  const float a2_unscale = (float)std::ldexp(1.0, -e2);
   c128_to_c64_kernel<<<grid_for(ctx, nm * nm * nq), 256, 0, ctx->stream>>>(uph, uph32, nm * nm * nq);
   EPB_LAUNCH_CHECK();
   Planes A2;
   A2.rows_pad = rows_pad_k * KO;
   A2.KC = KC_ep;
   A2.plane_bytes = plane_bytes_for(A2.rows_pad, KC_ep);
-  A2.npl = MX_NPL;
+  A2.npl = 2;
   A2.p = base + o_a2;
-  if (rows_pad_k != 2 * nd) EPB_CUDA(cudaMemsetAsync(A2.p, 0, MX_NPL * A2.plane_bytes, ctx->stream));
+  if (rows_pad_k != 2 * nd) EPB_CUDA(cudaMemsetAsync(A2.p, 0, 2 * A2.plane_bytes, ctx->stream));
 
   for (int64_t ko = 0; ko < nk; ko += KO) {
     const int64_t nko = nk - ko < KO ? nk - ko : KO;
@@ -1267,8 +1346,9 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
     {
       const int64_t total = nko * nd * (sin_offset(m->nr_ep) / 8);
       prof_begin(ctx, EPB_PROF_RR_ROT);
-      rr_rotate_pack_kernel<MX_BF16, MX_NPL><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
-          (const float2*)C0, Hk, (int)nw, (int)nw, (int)nm, (int)m->nr_ep, nko, rows_pad_k, KC_ep, A2.p, A2.plane_bytes);
+      rr_rotate_pack_kernel<false, 2><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
+          (const float2*)C0, Hk, (int)nw, (int)nw, (int)nm, (int)m->nr_ep, nko, rows_pad_k, KC_ep, A2.p, A2.plane_bytes,
+          a2_scale);
       prof_end(ctx);
       EPB_LAUNCH_CHECK();
     }
@@ -1283,8 +1363,8 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
       // kR->kq on the tensor cores, batched over the k of this inner batch
       Planes A2i = A2;
       A2i.p = A2.p + ki * rows_pad_k / 128 * KC_ep * TILE_BYTES;
-      EPB_TRY(split_gemm(ctx, EPB_PROF_UMMA_KQ, A2i, Bp, rows_pad_k / 128, nki, 2 * nd, nq, false, C2,
-                         2 * nd * nq, 2 * nd));
+      EPB_TRY(split_gemm_h(ctx, EPB_PROF_UMMA_KQ, A2i, Bp, rows_pad_k / 128, nki, 2 * nd, nq, false, C2,
+                           2 * nd * nq, 2 * nd, a2_unscale));
       // rotations, g2, in-place reduction
       if (!tiled) {
         static bool gattr = false;
