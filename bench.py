@@ -351,9 +351,10 @@ def run_epb(args):
     if flops is not None and dom_cnt > 0:
         avg_s = dom_ms / dom_cnt * 1e-3
         if dom_name.startswith("umma"):
-            nprod = 6  # split BF16x3: six bf16 products per real MAC
+            # split BF16x3: six products per real MAC; the pass's kR->kq runs FP16x2 (three products)
+            nprod = 3 if dom_name == "umma_kq" else 6
             peak = peaks["bf16_tflops_sustained"] / nprod
-            psrc = f"{peak_src} bf16 sustained / {nprod} split products"
+            psrc = f"{peak_src} bf16 (= fp16) sustained / {nprod} split products"
         else:
             peak = measure_fp64_peak(torch)
             psrc = "measured live: cuBLAS DGEMM 8192^3 (no FP64 figure in MEASURED_PEAKS.json)"
