@@ -123,6 +123,126 @@ __device__ int onesided_sweeps(typename cplx<T>::type (&a)[E16], T tol, int max_
   return sweep;
 }
 
+// ---- FP32 sweeps on packed pairs (sm_100 f32x2 arithmetic) ----------------------------------------
+// The column is held as 8 pairs of real parts and 8 pairs of imaginary parts (entries 2i, 2i+1), so the
+// Gram product and the rotation run as packed two-wide FMAs: half the FP32 instructions of the scalar
+// form. The rotation of each entry rounds as in the scalar form; the dot products accumulate even and
+// odd entries in two partial sums that are added at the end.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 pk(float x, float y) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
+  return r;
+}
+__device__ __forceinline__ float2 upk(f32x2 v) {
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+  return r;
+}
+__device__ __forceinline__ f32x2 pfma(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ f32x2 pmul(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ float hsum(f32x2 v) {
+  const float2 t = upk(v);
+  return t.x + t.y;
+}
+
+__device__ int onesided_sweeps_f32x2(float2 (&a)[E16], float tol, int max_sweeps) {
+  const int lane = threadIdx.x & 31;
+  const int l = lane & 15, base = lane & 16;
+  f32x2 X[E16 / 2], Y[E16 / 2];
+#pragma unroll
+  for (int i = 0; i < E16 / 2; ++i) {
+    X[i] = pk(a[2 * i].x, a[2 * i + 1].x);
+    Y[i] = pk(a[2 * i].y, a[2 * i + 1].y);
+  }
+  const f32x2 Z = pk(0.f, 0.f);
+  int sweep = 0;
+  for (; sweep < max_sweeps; ++sweep) {
+    f32x2 n2 = Z;
+#pragma unroll
+    for (int i = 0; i < E16 / 2; ++i) n2 = pfma(Y[i], Y[i], pfma(X[i], X[i], n2));
+    float nrm = hsum(n2);
+    int rotated = 0;
+#pragma unroll 1
+    for (int r = 0; r < 15; ++r) {
+      const int pl = circle_partner(l, r);
+      const int src = base + pl;
+      f32x2 BX[E16 / 2], BY[E16 / 2];
+#pragma unroll
+      for (int i = 0; i < E16 / 2; ++i) {
+        BX[i] = __shfl_sync(0xffffffffu, X[i], src);
+        BY[i] = __shfl_sync(0xffffffffu, Y[i], src);
+      }
+      const float nb = __shfl_sync(0xffffffffu, nrm, src);
+      const bool isP = l < pl;
+      // g = conj(own) . partner: Re = X.BX + Y.BY, Im = X.BY - Y.BX (a_p^H a_q on the p lane)
+      f32x2 gr = Z, gi = Z, gj = Z;
+#pragma unroll
+      for (int i = 0; i < E16 / 2; ++i) {
+        gr = pfma(Y[i], BY[i], pfma(X[i], BX[i], gr));
+        gi = pfma(X[i], BY[i], gi);
+        gj = pfma(Y[i], BX[i], gj);
+      }
+      const float gx = hsum(gr), gy = hsum(gi) - hsum(gj);
+      const float ag = sqrtf(gx * gx + gy * gy);
+      float c = 1.f, fx = 0.f, fy = 0.f, qx = 0.f, qy = 0.f, np_ = nrm, nq_ = nb;
+      int rot = 0;
+      if (isP && ag > tol * sqrtf(nrm * nb) && ag > 0.f) {
+        rot = 1;
+        const float tau = (nb - nrm) / (2.f * ag);
+        const float t = (tau >= 0.f ? 1.f : -1.f) / (fabsf(tau) + sqrtf(1.f + tau * tau));
+        c = 1.f / sqrtf(1.f + t * t);
+        const float sn = t * c, ex = gx / ag, ey = gy / ag;
+        fx = -sn * ex;  // p: a_p <- c a_p - s conj(e) a_q
+        fy = sn * ey;
+        qx = sn * ex;   // q: a_q <- c a_q + s e a_p
+        qy = sn * ey;
+        np_ = nrm - t * ag;
+        nq_ = nb + t * ag;
+      }
+      const float c_r = __shfl_sync(0xffffffffu, c, src), qx_r = __shfl_sync(0xffffffffu, qx, src),
+                  qy_r = __shfl_sync(0xffffffffu, qy, src), nq_r = __shfl_sync(0xffffffffu, nq_, src);
+      const int rot_r = __shfl_sync(0xffffffffu, rot, src);
+      if (!isP) {
+        rot = rot_r;
+        c = c_r;
+        fx = qx_r;
+        fy = qy_r;
+        np_ = nq_r;
+      }
+      if (rot) {
+        rotated = 1;
+        // a <- c a + f b:  Re = c X + fx BX - fy BY,  Im = c Y + fx BY + fy BX
+        const f32x2 C2 = pk(c, c), FX = pk(fx, fx), FY = pk(fy, fy), FYN = pk(-fy, -fy);
+#pragma unroll
+        for (int i = 0; i < E16 / 2; ++i) {
+          const f32x2 xr = pfma(C2, X[i], pfma(FX, BX[i], pmul(FYN, BY[i])));
+          const f32x2 yr = pfma(C2, Y[i], pfma(FX, BY[i], pmul(FY, BX[i])));
+          X[i] = xr;
+          Y[i] = yr;
+        }
+        nrm = np_;
+      }
+    }
+    if (!__any_sync(0xffffffffu, rotated)) break;
+  }
+#pragma unroll
+  for (int i = 0; i < E16 / 2; ++i) {
+    const float2 x = upk(X[i]), y = upk(Y[i]);
+    a[2 * i] = make_float2(x.x, y.x);
+    a[2 * i + 1] = make_float2(x.y, y.y);
+  }
+  return sweep;
+}
+
 struct Eigh16Args {
   const double2* A;   // c128 input (n x n per matrix, upper triangle), or null
   const float* Hp;    // packed FP32 Hermitian input (n*n per matrix), or null
@@ -227,7 +347,11 @@ __global__ void __launch_bounds__(128, MODE == 0 ? 1 : 4) eigh16_jacobi_kernel(E
     for (int i = 0; i < E16; ++i)
       if (i == l) col[i].x += (T)sigma;  // lanes >= n: sigma e_l
     const T tol = MODE == 0 ? T(1e-15) : T(1e-6);
-    int sw = onesided_sweeps<T>(col, tol, a.max_sweeps);
+    int sw;
+    if constexpr (MODE == 0)
+      sw = onesided_sweeps<T>(col, tol, a.max_sweeps);
+    else
+      sw = onesided_sweeps_f32x2(col, tol, a.max_sweeps);
     if (sw >= a.max_sweeps && lane == 0) atomicAdd(a.nonconv, 1);
     double nr2 = 0.0;
 #pragma unroll
