@@ -639,7 +639,12 @@ def run_bte(args):
     from oracle import bte_oracle as BO
     from oracle import epb_oracle as O
 
-    torch.cuda.set_device(0)
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:  # one process per GPU: each rank takes a contiguous share of the kept k (weak in the grid)
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
     ng = args.grid if args.grid != 96 else 64
     m = build_model_host_small()
     ep_dev = synth.epmat_el_device(SEED, NW, 3 * NATOM, m.el_ham.irvec, synth.irvec_box(N_PH))
@@ -653,10 +658,13 @@ def run_bte(args):
     half = 0.3 * synth.UNIT_EV
     T, eta = 300 * O.UNIT_K, 0.01 * synth.UNIT_EV
     kw = dict(method=5, k_batch=args.k_batch if args.k_batch > 0 else 128,
-              prec=pipeline.PREC_MIXED if args.prec != "fp64" else pipeline.PREC_FP64)
+              prec=pipeline.PREC_MIXED if args.prec != "fp64" else pipeline.PREC_FP64,
+              shard=(rank, ws) if ws > 1 else None)
     for _ in range(args.warmup):
         sig, st, _ = bte.serta(dm, ng, ef - half, ef + half, ef, T, eta, **kw)
     torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
     clk = clocks_start()
     l0 = dm.ctx.launch_count()
     s = torch.cuda.current_stream()
@@ -666,9 +674,17 @@ def run_bte(args):
         sig, st, _ = bte.serta(dm, ng, ef - half, ef + half, ef, T, eta, **kw)
     e1.record(s)
     torch.cuda.synchronize()
-    clocks = clocks_stop(clk, 0)
+    if ws > 1:
+        torch.distributed.barrier()
+    clocks = clocks_stop(clk, local)
     ms = e0.elapsed_time(e1) / args.steps
+    if ws > 1:
+        from epb200 import shard
+
+        ms = shard.max_over_ranks(ms, device="cuda")
     launches = dm.ctx.launch_count() - l0
+    st_rank = dict(st)  # this rank's shard: the per-launch roofline below is per GPU
+    sig, st = bte.reduce_shards(sig, st)
     dm.ctx.profile(True)
     bte.serta(dm, ng, ef - half, ef + half, ef, T, eta, **kw)
     torch.cuda.synchronize()
@@ -682,6 +698,9 @@ def run_bte(args):
     e1.record(s)
     torch.cuda.synchronize()
     ms64 = e0.elapsed_time(e1)
+    if ws > 1:
+        ms64 = shard.max_over_ranks(ms64, device="cuda")
+    sig64, st64 = bte.reduce_shards(sig64, st64)
     rel = float(np.max(np.abs(sig - sig64)) / np.abs(sig64).max())
     # roofline of the dominant family (total algorithmic flops of one step / its total device time)
     peaks, peak_src = measured_peaks()
@@ -693,11 +712,11 @@ def run_bte(args):
     W = max(int(st["width"]), 1)
     roof = None
     if dom_name == "umma_kq":   # grouped kR->kq of the kept k's pairs, split BF16x3
-        flops = 8.0 * NW * W * nm * nr_ep * st["pairs"]
+        flops = 8.0 * NW * W * nm * nr_ep * st_rank["pairs"]
         peak, psrc = peaks["bf16_tflops_sustained"] / 6, f"{peak_src} bf16 sustained / 6 split products"
     elif dom_name == "rotation":  # fused rotation + accumulation: HBM-bound on its per-pair operands
         flops = None
-        nb = st["pairs"] * (8 * NW * W * nm + 16 * nm * nm + 16 * NW * W + 8 * nm + 12)
+        nb = st_rank["pairs"] * (8 * NW * W * nm + 16 * nm * nm + 16 * NW * W + 8 * nm + 12)
         ach = nb / (dom_ms * 1e-3) / 1e9
         roof = {"bound": "hbm", "kernel": dom_name, "achieved": round(ach, 2), "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": round(ach / peaks["hbm_gbs"], 4), "traffic": None,
@@ -705,10 +724,13 @@ def run_bte(args):
                 "launches_per_step": dom_cnt, "algorithmic_bytes_per_step": nb,
                 "note": "per pair: g(k,q) complex64 block, u_ph, u_{k+q} slice, omega, column map"}
     elif dom_name == "zgemm":   # kR->kq per kept k: (nw W nm) x nr_ep x pairs of that k, FP64
-        flops = 8.0 * NW * W * nm * nr_ep * st["pairs"]
+        flops = 8.0 * NW * W * nm * nr_ep * st_rank["pairs"]
         peak, psrc = measure_fp64_peak(torch), "measured live: cuBLAS DGEMM 8192^3"
     elif dom_name == "umma_rr":  # RR->kR over Re for the kept k (all nw^2 nm nr_ep rows), split BF16x3
-        flops = 8.0 * NW * NW * nm * nr_ep * nr_el * st["kept_k"]
+        from epb200 import shard as _sh
+
+        a_k, b_k = _sh.shard_range(int(st_rank["kept_k"]), ws, rank)
+        flops = 8.0 * NW * NW * nm * nr_ep * nr_el * (b_k - a_k)
         peak, psrc = peaks["bf16_tflops_sustained"] / 6, f"{peak_src} bf16 sustained / 6 split products"
     else:
         flops = None
@@ -719,7 +741,7 @@ def run_bte(args):
                 "launch_ms": round(dom_ms / dom_cnt, 4), "launches_per_step": dom_cnt,
                 "algorithmic_flops_per_step": flops}
     cpu = None
-    if not args.no_cpu:
+    if not args.no_cpu and ws == 1:
         mh = m_host_for_cpu(m, ep_dev)
         cng = 16
         t0 = time.perf_counter()
@@ -730,7 +752,7 @@ def run_bte(args):
                "sample": f"the same model and window on a {cng}^3 k = q grid ({len(info['kept'])} kept k, "
                          f"{info['npairs']} pairs), {dt:.1f} s; numpy/scipy per-pair chain"}
         del mh
-    line = {"metric": BTE_METRIC, "value": st["pairs"] / (ms * 1e-3), "unit": "pairs/s", "n_gpus": 1,
+    line = {"metric": BTE_METRIC, "value": st["pairs"] / (ms * 1e-3), "unit": "pairs/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3/f64" if kw["prec"] == 1 else "f64",
             "data": "synthetic (seeded config-2 model; g(Re,Rp) generated on the device)",
@@ -742,7 +764,11 @@ def run_bte(args):
                     "note": "the public call takes the grid size and returns sigma (9 doubles) to the host"},
             "gpu_launches": launches,
             "clocks": clocks, "impl": "epb", "profile_one_step": profile}
-    print(json.dumps(line), flush=True)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
 
 
 OUTERQ_METRIC = "g(k,q,ν) elems/s of the batched outer-q loop, nw=16 config-2 model, all bands"

@@ -586,6 +586,9 @@ int epb_bte_serta(epb_ctx* ctx, epb_model* m, const epb_bte_params* prm, double*
   // 128 kept k per batch by default: the RR->kR GEMM's column tile is 128 points wide
   const int64_t KB = std::max<int64_t>(1, std::min<int64_t>(prm->k_batch > 0 ? prm->k_batch : 128, 256));
   EPB_CHECK_ARG(prm->pair_chunk <= 0 || prm->pair_chunk % 128 == 0, "epb_bte_serta: pair_chunk must be a multiple of 128");
+  EPB_CHECK_ARG(prm->shard_count <= 1 || (prm->shard_rank >= 0 && prm->shard_rank < prm->shard_count),
+                "epb_bte_serta: shard_rank %lld outside 0..%lld", (long long)prm->shard_rank,
+                (long long)prm->shard_count - 1);
   const int64_t QCH = prm->pair_chunk > 0 ? prm->pair_chunk : 65536;  // pairs per rotation launch
 
   // ---- persistent buffers (whole grid) ----
@@ -650,7 +653,23 @@ int epb_bte_serta(epb_ctx* ctx, epb_model* m, const epb_bte_params* prm, double*
     EPB_CUDA(cudaStreamSynchronize(ctx->stream));
   }
   int64_t npairs_total = 0;
-  if (nkeep > 0) {
+  // this shard's contiguous range [ks, ke) of the kept k (the reference's mpi_comm_k split)
+  int64_t ks = 0, ke = nkeep;
+  if (prm->shard_count > 1) {
+    const int64_t base_n = nkeep / prm->shard_count, extra = nkeep % prm->shard_count, r = prm->shard_rank;
+    ks = r * base_n + std::min(r, extra);
+    ke = ks + base_n + (r < extra ? 1 : 0);
+  }
+  if (nkeep > 0 && ke > ks && prm->shard_count > 1) {  // states of this shard
+    EPB_CUDA(cudaMemsetAsync(wmax_d, 0, 16, ctx->stream));
+    bte_width_kernel<<<gsz(ctx, ke - ks), 256, 0, ctx->stream>>>(keep + ks, ke - ks, bmin, bmax, wmax_d, nst_d);
+    EPB_LAUNCH_CHECK();
+    EPB_CUDA(cudaMemcpyAsync(&nstates, nst_d, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    EPB_CUDA(cudaStreamSynchronize(ctx->stream));
+  } else if (ke <= ks) {
+    nstates = 0;
+  }
+  if (nkeep > 0 && ke > ks) {
     // ---- kept-state buffers ----
     size_t off2 = 0;
     auto take2 = [&](size_t bytes) {
@@ -715,8 +734,8 @@ int epb_bte_serta(epb_ctx* ctx, epb_model* m, const epb_bte_params* prm, double*
     for (int i = 0; i < 9; ++i) L.a[i] = prm->lattice[i];
     bte_deriv_op_kernel<<<gsz(ctx, nw2 * m->nr_el), 256, 0, ctx->stream>>>(m->ham, nw2, m->rs_el->dev, m->nr_el, L, dop);
     EPB_LAUNCH_CHECK();
-    for (int64_t k0 = 0; k0 < nkeep; k0 += VB) {
-      const int64_t kn = std::min(VB, nkeep - k0);
+    for (int64_t k0 = ks; k0 < ke; k0 += VB) {
+      const int64_t kn = std::min(VB, ke - k0);
       bte_gather_x_kernel<<<gsz(ctx, kn), 256, 0, ctx->stream>>>(xg, keep, k0, kn, xkb);
       EPB_LAUNCH_CHECK();
       for (int a = 0; a < 3; ++a)
@@ -733,8 +752,8 @@ int epb_bte_serta(epb_ctx* ctx, epb_model* m, const epb_bte_params* prm, double*
     const int64_t Mrows = (int64_t)nw * W * nm;
     const int64_t outk = Mrows * nr_ep;
     std::vector<int64_t> seg_h(KB + 1);
-    for (int64_t b0 = 0; b0 < nkeep; b0 += KB) {
-      const int64_t nkb = std::min(KB, nkeep - b0);
+    for (int64_t b0 = ks; b0 < ke; b0 += KB) {
+      const int64_t nkb = std::min(KB, ke - b0);
       bte_gather_x_kernel<<<gsz(ctx, nkb), 256, 0, ctx->stream>>>(xg, keep, b0, nkb, xkb);
       EPB_LAUNCH_CHECK();
       bte_gather_uk_kernel<<<gsz(ctx, nkb * nw * W), 256, 0, ctx->stream>>>(U, keep, b0, nkb, bmin, nw, W, ukb);
@@ -841,14 +860,16 @@ int epb_bte_serta(epb_ctx* ctx, epb_model* m, const epb_bte_params* prm, double*
       }
     }
     // 5. SERTA conductivity and the per-state rates
-    bte_serta_kernel<<<gsz(ctx, nkeep * W), 256, 0, ctx->stream>>>(keep, nkeep, bmin, bmax, E, nw, W, sout, vel,
-                                                                    prm->mu, prm->temperature, 1.0 / (double)N, sig_d);
+    const int64_t nsh = ke - ks;
+    bte_serta_kernel<<<gsz(ctx, nsh * W), 256, 0, ctx->stream>>>(keep + ks, nsh, bmin, bmax, E, nw, W, sout + ks * W,
+                                                                  vel + ks * 3 * nw, prm->mu, prm->temperature,
+                                                                  1.0 / (double)N, sig_d);
     EPB_LAUNCH_CHECK();
     if (inv_tau_cap > 0) {
-      bte_state_offsets_kernel<<<1, 1024, 0, ctx->stream>>>(keep, nkeep, bmin, bmax, st_off);
+      bte_state_offsets_kernel<<<1, 1024, 0, ctx->stream>>>(keep + ks, nsh, bmin, bmax, st_off);
       EPB_LAUNCH_CHECK();
-      bte_list_states_kernel<<<gsz(ctx, nkeep), 256, 0, ctx->stream>>>(keep, nkeep, bmin, bmax, nw, W, sout, st_off,
-                                                                       inv_tau, inv_tau_cap);
+      bte_list_states_kernel<<<gsz(ctx, nsh), 256, 0, ctx->stream>>>(keep + ks, nsh, bmin, bmax, nw, W, sout + ks * W,
+                                                                     st_off, inv_tau, inv_tau_cap);
       EPB_LAUNCH_CHECK();
     }
   }

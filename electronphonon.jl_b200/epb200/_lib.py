@@ -116,7 +116,8 @@ class BteParams(C.Structure):
     """epb_bte_params."""
     _fields_ = [("ngrid", I64), ("wmin", D), ("wmax", D), ("mu", D), ("temperature", D), ("smearing", D),
                 ("omega_cutoff", D), ("spin_degeneracy", D), ("volume", D), ("lattice", D * 9), ("method", C.c_int32),
-                ("prec", C.c_int32), ("k_batch", I64), ("pair_chunk", I64)]
+                ("prec", C.c_int32), ("k_batch", I64), ("pair_chunk", I64), ("shard_rank", I64),
+                ("shard_count", I64)]
 
 
 class TiledInfo(C.Structure):

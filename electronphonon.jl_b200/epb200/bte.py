@@ -18,7 +18,8 @@ OMEGA_ACOUSTIC = 0.01 * 0.03674932248 * 2 * 1e-3
 
 
 def serta(dm, ngrid, wmin, wmax, mu, temperature, smearing, method=5, omega_cutoff=OMEGA_ACOUSTIC, lattice=None,
-          volume=1.0, spin=2.0, prec=PREC_FP64, k_batch=0, want_inv_tau=False, inv_tau_cap=None, pair_chunk=0):
+          volume=1.0, spin=2.0, prec=PREC_FP64, k_batch=0, want_inv_tau=False, inv_tau_cap=None, pair_chunk=0,
+          shard=None):
     """(sigma (3, 3), stats, inv_tau or None) for the model `dm` (pipeline.DeviceModel)."""
     import torch
 
@@ -31,6 +32,8 @@ def serta(dm, ngrid, wmin, wmax, mu, temperature, smearing, method=5, omega_cuto
         p.lattice[i] = v
     p.method, p.prec, p.k_batch = int(method), int(prec), int(k_batch)
     p.pair_chunk = int(pair_chunk)
+    if shard is not None:  # (rank, count): this rank's contiguous share of the kept k; sigma is partial
+        p.shard_rank, p.shard_count = int(shard[0]), int(shard[1])
     sig = np.zeros(9)
     stats = (C.c_int64 * 4)()
     cap = 0
@@ -41,3 +44,26 @@ def serta(dm, ngrid, wmin, wmax, mu, temperature, smearing, method=5, omega_cuto
     check(_lib.lib().epb_bte_serta(dm.ctx.h, dm.h, C.byref(p), sig.ctypes.data, ptr(it), cap, stats))
     st = dict(kept_k=stats[0], states=stats[1], pairs=stats[2], width=stats[3])
     return sig.reshape(3, 3, order="F"), st, (it[: st["states"]].cpu().numpy() if want_inv_tau else None)
+
+
+def reduce_shards(sigma, stats):
+    """Whole-run sigma and counts from this rank's shard result: sigma and the pair / state counts are
+    summed over the ranks of the initialised torch.distributed group (one small all-reduce; the kept-k
+    count and the window width are the same on every rank). Without a group, returns the inputs."""
+    from .shard import _dist
+
+    d = _dist()
+    if d is None:
+        return sigma, dict(stats)
+    import torch
+
+    t = torch.tensor(list(np.asarray(sigma, dtype=np.float64).reshape(-1, order="F")) +
+                     [float(stats["pairs"]), float(stats["states"])], dtype=torch.float64)
+    if d.get_backend() == "nccl":
+        t = t.cuda()
+    d.all_reduce(t, op=d.ReduceOp.SUM)
+    v = t.cpu().numpy()
+    out = dict(stats)
+    out["pairs"], out["states"] = int(round(v[9])), int(round(v[10]))
+    return v[:9].reshape(3, 3, order="F"), out
+

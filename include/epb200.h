@@ -482,6 +482,10 @@ typedef struct {
                                created with the mixed flag), everything else FP64                  */
   int64_t k_batch;          /* kept k per batch (<= 256); <= 0: 128                              */
   int64_t pair_chunk;       /* (k, q) pairs per rotation launch, a multiple of 128; <= 0: 65536   */
+  int64_t shard_rank;       /* this rank's share of the kept k (contiguous ranges, sizes within one)  */
+  int64_t shard_count;      /* number of shards (ranks); <= 1: all kept k. Each shard's sigma is a
+                               partial sum: the shards' sigmas add up to the whole (one 9-value
+                               all-reduce); inv_tau and the state / pair counts are the shard's */
 } epb_bte_params;
 
 /* SERTA conductivity over commensurate k = q grids: electron states, windows and phonons on the grid,

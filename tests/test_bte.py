@@ -86,3 +86,28 @@ def test_gpu_serta_mixed_grouped(gpu_lib, k_batch, pair_chunk):
     assert np.max(np.abs(smx - s64)) <= 1e-4 * np.abs(s64).max()
     np.testing.assert_allclose(itmx, it64, rtol=1e-4, atol=1e-6 * np.abs(it64).max())
 
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [0, 1])
+def test_gpu_serta_shards_add_up(gpu_lib, prec):
+    """k-sharded runs (one process here, three shards): the shards' sigmas sum to the whole-grid sigma, their
+    rates concatenate to the whole list, and the pair and state counts add up."""
+    from epb200 import bte, pipeline
+
+    m = synth.make_model(8, 2, 2, 1, seed=63)
+    ng = 6
+    x, _ = BO.grid_points(ng)
+    E = O.eigvals_batched(np.asfortranarray(
+        O.fourier_batched(m.el_ham.op_r, 64, m.el_ham.irvec, x).reshape(8, 8, -1, order="F")))
+    ef = float(np.median(E[4]))
+    dm = pipeline.DeviceModel(m, mixed=prec == 1)
+    args = (dm, ng, ef - 1.0, ef + 1.0, ef, 0.08, 0.06)
+    s_all, st_all, it_all = bte.serta(*args, prec=prec, want_inv_tau=True, k_batch=5)
+    parts = [bte.serta(*args, prec=prec, want_inv_tau=True, k_batch=5, shard=(r, 3)) for r in range(3)]
+    assert sum(p[1]["pairs"] for p in parts) == st_all["pairs"]
+    assert sum(p[1]["states"] for p in parts) == st_all["states"]
+    assert all(p[1]["kept_k"] == st_all["kept_k"] for p in parts)
+    np.testing.assert_allclose(sum(p[0] for p in parts), s_all, rtol=1e-10, atol=1e-12 * np.abs(s_all).max())
+    np.testing.assert_allclose(np.concatenate([p[2] for p in parts]), it_all, rtol=1e-10,
+                               atol=1e-14 * np.abs(it_all).max())
+

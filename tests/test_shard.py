@@ -84,3 +84,42 @@ def test_gloo_world2_window_offsets(tmp_path):
     assert r0[3] == r1[3] == len(ref)     # global sum
     g = np.where(r0[4:] >= 0, r0[4:], r1[4:]).astype(np.int64)
     np.testing.assert_array_equal(g, ref)
+
+
+def _sigma_worker(rank, world, port, out_dir):
+    import sys
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    for p in (os.path.dirname(here), os.path.join(os.path.dirname(here), "electronphonon.jl_b200")):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    import datetime
+
+    import torch.distributed as dist
+
+    from epb200 import bte
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        sig = np.arange(9, dtype=np.float64).reshape(3, 3, order="F") * (rank + 1)
+        st = dict(kept_k=10, states=3 + rank, pairs=100 * (rank + 1), width=2)
+        tot, st2 = bte.reduce_shards(sig, st)
+        np.save(os.path.join(out_dir, f"s{rank}.npy"),
+                np.array(list(tot.reshape(-1, order="F")) + [st2["pairs"], st2["states"], st2["kept_k"], st2["width"]]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_world2_bte_shard_reduction(tmp_path):
+    """The SERTA consumer's k shards: sigma (partial sums) and the pair / state counts add over the ranks;
+    the kept-k count and the window width are common."""
+    import torch.multiprocessing as mp
+
+    port = _free_port()
+    mp.start_processes(_sigma_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True, start_method="spawn")
+    r0, r1 = (np.load(tmp_path / f"s{r}.npy") for r in range(2))
+    np.testing.assert_array_equal(r0, r1)
+    np.testing.assert_array_equal(r0[:9], np.arange(9) * 3.0)
+    assert list(r0[9:]) == [300, 7, 10, 2]
