@@ -14,7 +14,8 @@
 // |g| <= tol sqrt(a b); a sweep with no rotation ends the solve. Lanes >= n carry sigma e_l,
 // orthogonal to every live column, so they never rotate.
 //
-// Mixed precision (EPB_PREC_MIXED): the sweeps run in FP32 to tol = 1e-6, then one FP64
+// Mixed precision (EPB_PREC_MIXED): the sweeps run in FP32 to tol = 1e-6 (or until a sweep whose
+// rotation angles were all below 1e-4, after which the columns are orthogonal to the FP32 floor), then one FP64
 // refinement on the same registers: Lowdin re-orthonormalisation V(I - F/2), F = V^H V - I
 // (this re-orthogonalises near-degenerate clusters, whose FP32 vectors are defined only up to a
 // rotation inside the cluster), and a first-order Rayleigh-Ritz update from S = V^H H V:
@@ -164,13 +165,14 @@ __device__ int onesided_sweeps_f32x2(float2 (&a)[E16], float tol, int max_sweeps
     Y[i] = pk(a[2 * i].y, a[2 * i + 1].y);
   }
   const f32x2 Z = pk(0.f, 0.f);
+  const float tol2 = tol * tol;
   int sweep = 0;
   for (; sweep < max_sweeps; ++sweep) {
     f32x2 n2 = Z;
 #pragma unroll
     for (int i = 0; i < E16 / 2; ++i) n2 = pfma(Y[i], Y[i], pfma(X[i], X[i], n2));
     float nrm = hsum(n2);
-    int rotated = 0;
+    int big = 0;  // a rotation by more than 1e-4 in this sweep
 #pragma unroll 1
     for (int r = 0; r < 15; ++r) {
       const int pl = circle_partner(l, r);
@@ -183,7 +185,10 @@ __device__ int onesided_sweeps_f32x2(float2 (&a)[E16], float tol, int max_sweeps
       }
       const float nb = __shfl_sync(0xffffffffu, nrm, src);
       const bool isP = l < pl;
-      // g = conj(own) . partner: Re = X.BX + Y.BY, Im = X.BY - Y.BX (a_p^H a_q on the p lane)
+      // Gram entry conj(own) . partner: Re = X.BX + Y.BY, Im = X.BY - Y.BX. The partner lane forms the
+      // same elementwise products in the same order, with the two imaginary sums trading places, so
+      // both lanes hold bitwise-identical g = a_p^H a_q and norms (a, b) in the p lane's orientation
+      // and derive the same rotation without exchanging it.
       f32x2 gr = Z, gi = Z, gj = Z;
 #pragma unroll
       for (int i = 0; i < E16 / 2; ++i) {
@@ -191,35 +196,21 @@ __device__ int onesided_sweeps_f32x2(float2 (&a)[E16], float tol, int max_sweeps
         gi = pfma(X[i], BY[i], gi);
         gj = pfma(Y[i], BX[i], gj);
       }
-      const float gx = hsum(gr), gy = hsum(gi) - hsum(gj);
-      const float ag = sqrtf(gx * gx + gy * gy);
-      float c = 1.f, fx = 0.f, fy = 0.f, qx = 0.f, qy = 0.f, np_ = nrm, nq_ = nb;
-      int rot = 0;
-      if (isP && ag > tol * sqrtf(nrm * nb) && ag > 0.f) {
-        rot = 1;
-        const float tau = (nb - nrm) / (2.f * ag);
-        const float t = (tau >= 0.f ? 1.f : -1.f) / (fabsf(tau) + sqrtf(1.f + tau * tau));
-        c = 1.f / sqrtf(1.f + t * t);
-        const float sn = t * c, ex = gx / ag, ey = gy / ag;
-        fx = -sn * ex;  // p: a_p <- c a_p - s conj(e) a_q
-        fy = sn * ey;
-        qx = sn * ex;   // q: a_q <- c a_q + s e a_p
-        qy = sn * ey;
-        np_ = nrm - t * ag;
-        nq_ = nb + t * ag;
-      }
-      const float c_r = __shfl_sync(0xffffffffu, c, src), qx_r = __shfl_sync(0xffffffffu, qx, src),
-                  qy_r = __shfl_sync(0xffffffffu, qy, src), nq_r = __shfl_sync(0xffffffffu, nq_, src);
-      const int rot_r = __shfl_sync(0xffffffffu, rot, src);
-      if (!isP) {
-        rot = rot_r;
-        c = c_r;
-        fx = qx_r;
-        fy = qy_r;
-        np_ = nq_r;
-      }
-      if (rot) {
-        rotated = 1;
+      const float hi = hsum(gi), hj = hsum(gj);
+      const float gx = hsum(gr), gy = isP ? hi - hj : hj - hi;
+      const float A = isP ? nrm : nb, B = isP ? nb : nrm;
+      const float ag2 = gx * gx + gy * gy;
+      if (ag2 > tol2 * (A * B) && ag2 > 0.f) {
+        const float rag = rsqrtf(ag2), ag = ag2 * rag;
+        const float tau = 0.5f * (B - A) * rag;
+        const float u = 1.f + tau * tau;
+        const float t = __fdividef(tau >= 0.f ? 1.f : -1.f, fabsf(tau) + u * rsqrtf(u));
+        const float c = rsqrtf(1.f + t * t);
+        const float sn = t * c, ex = gx * rag, ey = gy * rag;
+        big |= fabsf(t) > 1e-4f;
+        // p: a_p <- c a_p - s conj(e) a_q;  q: a_q <- c a_q + s e a_p
+        const float fx = isP ? -sn * ex : sn * ex, fy = sn * ey;
+        nrm = isP ? A - t * ag : B + t * ag;
         // a <- c a + f b:  Re = c X + fx BX - fy BY,  Im = c Y + fx BY + fy BX
         const f32x2 C2 = pk(c, c), FX = pk(fx, fx), FY = pk(fy, fy), FYN = pk(-fy, -fy);
 #pragma unroll
@@ -229,10 +220,11 @@ __device__ int onesided_sweeps_f32x2(float2 (&a)[E16], float tol, int max_sweeps
           X[i] = xr;
           Y[i] = yr;
         }
-        nrm = np_;
       }
     }
-    if (!__any_sync(0xffffffffu, rotated)) break;
+    // quadratic convergence: after a sweep whose rotations were all below 1e-4 the columns are
+    // orthogonal to O(1e-8), the FP32 floor; no confirmation sweep
+    if (!__any_sync(0xffffffffu, big)) break;
   }
 #pragma unroll
   for (int i = 0; i < E16 / 2; ++i) {
