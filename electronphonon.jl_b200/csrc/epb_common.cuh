@@ -236,6 +236,34 @@ __host__ __device__ __forceinline__ void cfma_conj(float2& acc, float2 a, float2
   acc.y = fmaf(-a.y, b.x, acc.y);
 }
 
+// Packed FP32 pairs (sm_100 f32x2 arithmetic): two floats in one 64-bit register pair, FMA and
+// multiply on both lanes with one instruction; every lane rounds as its scalar counterpart.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 pk(float x, float y) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
+  return r;
+}
+__device__ __forceinline__ float2 upk(f32x2 v) {
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+  return r;
+}
+__device__ __forceinline__ f32x2 pfma(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ f32x2 pmul(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ float hsum(f32x2 v) {
+  const float2 t = upk(v);
+  return t.x + t.y;
+}
+
 template <typename T> struct cplx;
 template <> struct cplx<double> { using type = double2; };
 template <> struct cplx<float> { using type = float2; };

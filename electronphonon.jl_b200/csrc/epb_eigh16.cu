@@ -129,31 +129,6 @@ __device__ int onesided_sweeps(typename cplx<T>::type (&a)[E16], T tol, int max_
 // Gram product and the rotation run as packed two-wide FMAs: half the FP32 instructions of the scalar
 // form. The rotation of each entry rounds as in the scalar form; the dot products accumulate even and
 // odd entries in two partial sums that are added at the end.
-typedef unsigned long long f32x2;
-__device__ __forceinline__ f32x2 pk(float x, float y) {
-  f32x2 r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
-  return r;
-}
-__device__ __forceinline__ float2 upk(f32x2 v) {
-  float2 r;
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
-  return r;
-}
-__device__ __forceinline__ f32x2 pfma(f32x2 a, f32x2 b, f32x2 c) {
-  f32x2 d;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-  return d;
-}
-__device__ __forceinline__ f32x2 pmul(f32x2 a, f32x2 b) {
-  f32x2 d;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ float hsum(f32x2 v) {
-  const float2 t = upk(v);
-  return t.x + t.y;
-}
 
 __device__ int onesided_sweeps_f32x2(float2 (&a)[E16], float tol, int max_sweeps) {
   const int lane = threadIdx.x & 31;
@@ -547,21 +522,35 @@ __global__ void __launch_bounds__(128, 3) eigh16_refine2_kernel(Eigh16Args a) {
       double2 u[8];  // V t accumulated over k
 #pragma unroll
       for (int r = 0; r < 8; ++r) u[r] = make_double2(0.0, 0.0);
-#pragma unroll 4
-      for (int k = 0; k < E16; ++k) {
+      // S and G columns for KB values of k at a time: 4 KB independent FP64 accumulation chains (KB = 2
+      // keeps the kernel inside 168 registers, three CTAs per SM)
+      constexpr int KB = 2;
+#pragma unroll 1
+      for (int k0 = 0; k0 < E16; k0 += KB) {
+        double2 sb[KB], gb[KB];
+#pragma unroll
+        for (int kk = 0; kk < KB; ++kk) sb[kk] = gb[kk] = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+#pragma unroll
+          for (int kk = 0; kk < KB; ++kk) {
+            const double2 vik = V[(r0 + r) * RLD + k0 + kk];
+            cfma_conj(sb[kk], vik, w[r]);
+            cfma_conj(gb[kk], vik, v[r]);
+          }
+#pragma unroll
+        for (int kk = 0; kk < KB; ++kk) {
+          sb[kk].x += __shfl_xor_sync(0xffffffffu, sb[kk].x, 16);
+          sb[kk].y += __shfl_xor_sync(0xffffffffu, sb[kk].y, 16);
+          gb[kk].x += __shfl_xor_sync(0xffffffffu, gb[kk].x, 16);
+          gb[kk].y += __shfl_xor_sync(0xffffffffu, gb[kk].y, 16);
+        }
+#pragma unroll
+        for (int kk = 0; kk < KB; ++kk) {
+        const int k = k0 + kk;
         const double dk = __shfl_sync(0xffffffffu, d, k);
         const double dpk = __shfl_sync(0xffffffffu, dp, k);
-        double2 s = make_double2(0.0, 0.0), g = s;
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          const double2 vik = V[(r0 + r) * RLD + k];
-          cfma_conj(s, vik, w[r]);
-          cfma_conj(g, vik, v[r]);
-        }
-        s.x += __shfl_xor_sync(0xffffffffu, s.x, 16);
-        s.y += __shfl_xor_sync(0xffffffffu, s.y, 16);
-        g.x += __shfl_xor_sync(0xffffffffu, g.x, 16);
-        g.y += __shfl_xor_sync(0xffffffffu, g.y, 16);
+        const double2 s = sb[kk], g = gb[kk];
         double2 t;
         if (k == l) {
           t = make_double2(-0.5 * fll, 0.0);
@@ -591,6 +580,7 @@ __global__ void __launch_bounds__(128, 3) eigh16_refine2_kernel(Eigh16Args a) {
         }
 #pragma unroll
         for (int r = 0; r < 8; ++r) cfma(u[r], V[(r0 + r) * RLD + k], t);
+        }
       }
 #pragma unroll
       for (int r = 0; r < 8; ++r) v[r] = make_double2(v[r].x + u[r].x, v[r].y + u[r].y);

@@ -104,6 +104,45 @@ __device__ __forceinline__ void store_split8(uint8_t* base, int64_t plane_bytes,
   }
 }
 
+// The same split of FP32 values, in FP32 arithmetic: each remainder is exact in FP32, so the planes sum
+// to the FP32 value exactly and its rounding (2^-24 relative) is the only difference from the FP64 split.
+template <bool BF16>
+__device__ __forceinline__ uint16_t f32_to_half_bits(float v) {
+  if (BF16) {
+    __nv_bfloat16 h = __float2bfloat16_rn(v);
+    return *reinterpret_cast<uint16_t*>(&h);
+  } else {
+    __half h = __float2half_rn(v);
+    return *reinterpret_cast<uint16_t*>(&h);
+  }
+}
+template <bool BF16>
+__device__ __forceinline__ float half_bits_to_f32(uint16_t b) {
+  if (BF16) return __bfloat162float(*reinterpret_cast<__nv_bfloat16*>(&b));
+  return __half2float(*reinterpret_cast<__half*>(&b));
+}
+template <bool BF16, int NPL>
+__device__ __forceinline__ void store_split8_f32(uint8_t* base, int64_t plane_bytes, int64_t off, const float* v) {
+  float r[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) r[e] = v[e];
+#pragma unroll
+  for (int p = 0; p < NPL; ++p) {
+    uint16_t b[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      b[e] = f32_to_half_bits<BF16>(r[e]);
+      r[e] -= half_bits_to_f32<BF16>(b[e]);
+    }
+    uint4 w;
+    w.x = (uint32_t)b[0] | ((uint32_t)b[1] << 16);
+    w.y = (uint32_t)b[2] | ((uint32_t)b[3] << 16);
+    w.z = (uint32_t)b[4] | ((uint32_t)b[5] << 16);
+    w.w = (uint32_t)b[6] | ((uint32_t)b[7] << 16);
+    *reinterpret_cast<uint4*>(base + p * plane_bytes + off) = w;
+  }
+}
+
 __host__ __device__ __forceinline__ int64_t sin_offset(int64_t K) { return (K + 7) / 8 * 8; }
 __host__ __device__ __forceinline__ int64_t kchunks(int64_t K) { return (sin_offset(K) + K + 63) / 64; }
 
@@ -245,6 +284,70 @@ __global__ void pack_b_phase_kernel(const int4* __restrict__ rv, int64_t K, cons
     for (int64_t z = 2 * ncos + ch; z < nch; z += ncos) {
       double zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       store_split8<BF16, NPL>(planes, plane_bytes, tiled_offset(j, z * 8, KC), zero);
+    }
+  }
+}
+
+// The same phase operand from per-axis tables: exp(2 pi i R.x) = prod_d exp(2 pi i R_d x_d). A block
+// takes SEP_PTS points at a time; their axis factors (R_d in [lo_d, lo_d + span_d), span_d <= SEP_SPAN)
+// are evaluated once into shared memory, and each entry is two FP64 complex products instead of one
+// FP64 sincospi. Every axis argument R_d x_d is reduced on its own, so the entries agree with the direct
+// evaluation to a few 1e-16; each entry is then rounded to FP32 and split in FP32 (the planes hold the
+// FP32 value exactly, 2^-24 relative, the same order as the truncation of the split itself).
+constexpr int SEP_PTS = 8, SEP_SPAN = 64;
+template <bool BF16, int NPL>
+__global__ void __launch_bounds__(256) pack_b_phase_sep_kernel(
+    const int4* __restrict__ rv, int64_t K, int lo0, int lo1, int lo2, int sp0, int sp1, int sp2,
+    const double* __restrict__ xa, const double* __restrict__ xb, int64_t nb, const int64_t* __restrict__ pidx,
+    int64_t pair0, int64_t N, int64_t rows_pad, int64_t KC, uint8_t* __restrict__ planes, int64_t plane_bytes) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* tab = reinterpret_cast<double2*>(smem_raw);  // [SEP_PTS][sp0 + sp1 + sp2]
+  const int spt = sp0 + sp1 + sp2;
+  const int koff = (int)sin_offset(K), ncos = koff / 8, nch = (int)KC * 8;
+  const int64_t ngroups = rows_pad / SEP_PTS;  // rows_pad is a multiple of 128
+  for (int64_t grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+    const int64_t j0 = grp * SEP_PTS;
+    __syncthreads();  // the previous group's table is no longer read
+    for (int e = threadIdx.x; e < SEP_PTS * spt; e += blockDim.x) {
+      const int p = e / spt, m = e - p * spt;
+      const int d = m < sp0 ? 0 : m < sp0 + sp1 ? 1 : 2;
+      const int r = d == 0 ? lo0 + m : d == 1 ? lo1 + m - sp0 : lo2 + m - sp0 - sp1;
+      const int64_t j = j0 + p;
+      double x = 0.0;
+      if (j < N) {
+        if (xb) {
+          const int64_t pj = pidx ? pidx[j] : pair0 + j;
+          x = xa[3 * (pj / nb) + d] + xb[3 * (pj % nb) + d];
+        } else {
+          x = xa[3 * j + d];
+        }
+      }
+      tab[e] = cis2pi(__dmul_rn((double)r, x));
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < SEP_PTS * ncos; it += blockDim.x) {
+      const int p = it / ncos, ch = it - p * ncos;
+      const int64_t j = j0 + p;
+      const double2* t = tab + p * spt;
+      float c[8], sn[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int q = ch * 8 + e;
+        c[e] = 0.f;
+        sn[e] = 0.f;
+        if (j < N && q < K) {
+          const int4 r = rv[q];
+          const double2 z = cmul(cmul(t[r.x - lo0], t[sp0 + r.y - lo1]), t[sp0 + sp1 + r.z - lo2]);
+          c[e] = (float)z.x;
+          sn[e] = (float)z.y;
+        }
+      }
+      store_split8_f32<BF16, NPL>(planes, plane_bytes, tiled_offset(j, ch * 8, KC), c);
+      store_split8_f32<BF16, NPL>(planes, plane_bytes, tiled_offset(j, koff + ch * 8, KC), sn);
+      for (int z = 2 * ncos + ch; z < nch; z += ncos) {
+        const float zero[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        store_split8_f32<BF16, NPL>(planes, plane_bytes, tiled_offset(j, (int64_t)z * 8, KC), zero);
+      }
     }
   }
 }
@@ -505,6 +608,16 @@ static unsigned grid_for(epb_ctx* ctx, int64_t total) {
   return (unsigned)(g < cap ? (g < 1 ? 1 : g) : cap);
 }
 
+// Per-axis phase tables apply when every axis of the R set spans at most SEP_SPAN values.
+static bool sep_spans_ok(const epb_rset* rs) {
+  for (int d = 0; d < 3; ++d)
+    if (rs->hi[d] - rs->lo[d] + 1 > SEP_SPAN) return false;
+  return true;
+}
+static unsigned sep_grid(epb_ctx* ctx, int64_t rows_pad) {
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(rows_pad / SEP_PTS, (int64_t)ctx->sm_count * 8));
+}
+
 template <bool BF16, int NPL, int NT>
 static int launch_split_gemm(epb_ctx* ctx, SplitGemmArgs& a) {
   using Cfg = GemmCfg<BF16, NPL, NT>;
@@ -640,8 +753,16 @@ int pack_b_phase(epb_ctx* ctx, const epb_rset* rs, const double* xa, const doubl
   out.p = mem;
   int64_t total = out.rows_pad * (sin_offset(rs->nr) / 8);
   prof_begin(ctx, EPB_PROF_SPLIT);
-  pack_b_phase_kernel<MX_BF16, MX_NPL><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
-      rs->dev, rs->nr, xa, xb, nb, pidx, pair0, N, out.rows_pad, out.KC, out.p, out.plane_bytes);
+  if (sep_spans_ok(rs)) {
+    const int sp0 = rs->hi[0] - rs->lo[0] + 1, sp1 = rs->hi[1] - rs->lo[1] + 1, sp2 = rs->hi[2] - rs->lo[2] + 1;
+    pack_b_phase_sep_kernel<MX_BF16, MX_NPL><<<sep_grid(ctx, out.rows_pad), 256, SEP_PTS * (sp0 + sp1 + sp2) * 16,
+                                               ctx->stream>>>(
+        rs->dev, rs->nr, rs->lo[0], rs->lo[1], rs->lo[2], sp0, sp1, sp2, xa, xb, nb, pidx, pair0, N, out.rows_pad,
+        out.KC, out.p, out.plane_bytes);
+  } else {
+    pack_b_phase_kernel<MX_BF16, MX_NPL><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
+        rs->dev, rs->nr, xa, xb, nb, pidx, pair0, N, out.rows_pad, out.KC, out.p, out.plane_bytes);
+  }
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
@@ -657,8 +778,16 @@ int pack_b_phase_h(epb_ctx* ctx, const epb_rset* rs, const double* xa, const dou
   out.p = mem;
   int64_t total = out.rows_pad * (sin_offset(rs->nr) / 8);
   prof_begin(ctx, EPB_PROF_SPLIT);
-  pack_b_phase_kernel<false, 2><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
-      rs->dev, rs->nr, xa, xb, nb, nullptr, 0, N, out.rows_pad, out.KC, out.p, out.plane_bytes);
+  if (sep_spans_ok(rs)) {
+    const int sp0 = rs->hi[0] - rs->lo[0] + 1, sp1 = rs->hi[1] - rs->lo[1] + 1, sp2 = rs->hi[2] - rs->lo[2] + 1;
+    pack_b_phase_sep_kernel<false, 2><<<sep_grid(ctx, out.rows_pad), 256, SEP_PTS * (sp0 + sp1 + sp2) * 16,
+                                        ctx->stream>>>(
+        rs->dev, rs->nr, rs->lo[0], rs->lo[1], rs->lo[2], sp0, sp1, sp2, xa, xb, nb, nullptr, 0, N, out.rows_pad,
+        out.KC, out.p, out.plane_bytes);
+  } else {
+    pack_b_phase_kernel<false, 2><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
+        rs->dev, rs->nr, xa, xb, nb, nullptr, 0, N, out.rows_pad, out.KC, out.p, out.plane_bytes);
+  }
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
@@ -921,45 +1050,57 @@ template <bool BF16, int NPL>
 __global__ void rr_rotate_pack_kernel(const float2* __restrict__ gk, const double2* __restrict__ uk, int nw,
                                       int nband, int nm, int nr_ep, int64_t nk, int64_t rows_pad_k, int64_t KC,
                                       uint8_t* __restrict__ planes, int64_t plane_bytes, double scale = 1.0) {
-  const int64_t nd = (int64_t)nw * nband * nm;  // complex rows r per k
-  const int64_t koff = sin_offset(nr_ep);
-  const int64_t npc = koff / 8;               // 8-wide p chunks
+  // FP32 products and sums (g is FP32; the planes hold at most 24 bits), u rounded to FP32 once per row
+  const int nd = nw * nband * nm;  // complex rows r per k
+  const int koff = (int)sin_offset(nr_ep);
+  const int npc = koff / 8;        // 8-wide p chunks
   const int64_t total = nk * nd * npc;
   const int64_t ndata = (int64_t)nw * nw * nm * nr_ep;  // complex length of g_k
+  const float sc = (float)scale;
+  const bool idx32 = total <= 0x7fffffff;
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
-    int64_t r = idx % nd;
-    int64_t rest = idx / nd;
-    int64_t pc = rest % npc, k = rest / npc;
-    int iw = (int)(r % nw);
-    int n = (int)((r / nw) % nband);
-    int nu = (int)(r / ((int64_t)nw * nband));
-    const float2* g = gk + k * ndata;
+    int r, pc;
+    int64_t k;
+    if (idx32) {
+      const uint32_t i = (uint32_t)idx, rest = i / (uint32_t)nd;
+      r = (int)(i - rest * (uint32_t)nd);
+      k = rest / (uint32_t)npc;
+      pc = (int)(rest - (uint32_t)k * (uint32_t)npc);
+    } else {
+      const int64_t rest = idx / nd;
+      r = (int)(idx - rest * nd);
+      k = rest / npc;
+      pc = (int)(rest - k * npc);
+    }
+    const int iw = r % nw, n = (r / nw) % nband, nu = r / (nw * nband);
+    const float2* g = gk + k * ndata + iw + (int64_t)nw * nw * nu;
     const double2* u = uk + (k * nband + n) * nw;
-    double re[8], im[8];
+    float2 acc[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) acc[e] = make_float2(0.f, 0.f);
+    for (int jw = 0; jw < nw; ++jw) {
+      const double2 ud = u[jw];
+      const float2 uf = make_float2((float)ud.x, (float)ud.y);
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int p = pc * 8 + e;
+        if (p < nr_ep) cfma(acc[e], g[(int64_t)nw * jw + (int64_t)nw * nw * nm * p], uf);
+      }
+    }
+    float re[8], im[8], t[8];
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
-      int p = (int)(pc * 8 + e);
-      double2 acc = make_double2(0.0, 0.0);
-      if (p < nr_ep) {
-        const float2* gp = g + iw + (int64_t)nw * nw * (nu + (int64_t)nm * p);
-        for (int jw = 0; jw < nw; ++jw) {
-          float2 x = gp[(int64_t)jw * nw];
-          cfma(acc, make_double2(x.x, x.y), u[jw]);
-        }
-      }
-      re[e] = acc.x * scale;
-      im[e] = acc.y * scale;
+      re[e] = acc[e].x * sc;
+      im[e] = acc[e].y * sc;
+      t[e] = -im[e];
     }
     const int64_t row0 = k * rows_pad_k + 2 * r;
-    double t[8];
     // real row: [Re G | -Im G];  imaginary row: [Im G | Re G]
-    store_split8<BF16, NPL>(planes, plane_bytes, tiled_offset(row0, pc * 8, KC), re);
-#pragma unroll
-    for (int e = 0; e < 8; ++e) t[e] = -im[e];
-    store_split8<BF16, NPL>(planes, plane_bytes, tiled_offset(row0, koff + pc * 8, KC), t);
-    store_split8<BF16, NPL>(planes, plane_bytes, tiled_offset(row0 + 1, pc * 8, KC), im);
-    store_split8<BF16, NPL>(planes, plane_bytes, tiled_offset(row0 + 1, koff + pc * 8, KC), re);
+    store_split8_f32<BF16, NPL>(planes, plane_bytes, tiled_offset(row0, pc * 8, KC), re);
+    store_split8_f32<BF16, NPL>(planes, plane_bytes, tiled_offset(row0, koff + pc * 8, KC), t);
+    store_split8_f32<BF16, NPL>(planes, plane_bytes, tiled_offset(row0 + 1, pc * 8, KC), im);
+    store_split8_f32<BF16, NPL>(planes, plane_bytes, tiled_offset(row0 + 1, koff + pc * 8, KC), re);
   }
 }
 
@@ -1098,9 +1239,8 @@ __global__ void __launch_bounds__(256, 2) eph_rot_reduce_f32_kernel(
   const int mg = tid >> 6, cg = tid & 63;          // stage 1
   const int mng = tid & 63, ng = tid >> 6;         // stage 2
   const int64_t nblk = nkb * nq;
-  auto prefetch = [&](int64_t blk, int buf) {
+  auto prefetch = [&](int64_t blk, int64_t q, int buf) {
     if (blk < nblk) {
-      const int64_t q = blk % nq;
       unsigned char* dst = smem_raw + buf * L::BUF;
       const char* gs = reinterpret_cast<const char*>(g + blk * g_stride);
       const char* us = reinterpret_cast<const char*>(ukq + blk * NW * NB);
@@ -1130,10 +1270,17 @@ __global__ void __launch_bounds__(256, 2) eph_rot_reduce_f32_kernel(
   };
   int64_t kcur = -1;
   int buf = 0;
-  prefetch(blockIdx.x, 0);
+  // (k, q) of the block, advanced by the grid stride without 64-bit divisions in the loop
+  const int64_t dk = gridDim.x / nq, dq = gridDim.x % nq;
+  int64_t kl = blockIdx.x / nq, q = blockIdx.x % nq;
+  prefetch(blockIdx.x, q, 0);
   for (int64_t blk = blockIdx.x; blk < nblk; blk += gridDim.x, buf ^= 1) {
-    prefetch(blk + gridDim.x, buf ^ 1);
-    const int64_t kl = blk / nq, q = blk % nq;
+    int64_t kn = kl + dk, qn = q + dq;
+    if (qn >= nq) {
+      qn -= nq;
+      ++kn;
+    }
+    prefetch(blk + gridDim.x, qn, buf ^ 1);
     if (kl != kcur) {  // uniform across the CTA
       if (kcur >= 0) flush(kcur);
       kcur = kl;
@@ -1195,8 +1342,8 @@ __global__ void __launch_bounds__(256, 2) eph_rot_reduce_f32_kernel(
 #pragma unroll
           for (int j = 0; j < 3; ++j) cfma(acc[i][j], tt[i], pp[j]);
       }
-      const bool samp = sample && (q % stride == 0);
-      double* sq = samp ? sample + ((kl * nsamp) + q / stride) * (int64_t)NT : nullptr;
+      const bool samp = sample && ((uint32_t)q % (uint32_t)stride == 0);
+      double* sq = samp ? sample + ((kl * nsamp) + (uint32_t)q / (uint32_t)stride) * (int64_t)NT : nullptr;
       const double* om = omega + q * NM;
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
@@ -1213,6 +1360,8 @@ __global__ void __launch_bounds__(256, 2) eph_rot_reduce_f32_kernel(
       }
     }
     __syncthreads();  // the next iteration's prefetch overwrites this buffer
+    kl = kn;
+    q = qn;
   }
   if (kcur >= 0) flush(kcur);
 }
@@ -1277,6 +1426,9 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
   const int64_t nd = nw2 * nm, nd_ep = nd * m->nr_ep;
   const bool tiled = nw == 16 && nm == 12;  // the register-tiled rotation; other shapes take the generic kernel
   const size_t gen_smem = 8 * (size_t)(2 * nw2 * nm + nw2 + nm * nm) + 8 * (size_t)nm;
+  EPB_CHECK_ARG(nq < (int64_t(1) << 31) && (!g2_sample || (sample_stride >= 1 && sample_stride < (int64_t(1) << 31))),
+                "mixed pass: nq = %lld and the sample stride %lld must lie in 1 .. 2^31 - 1", (long long)nq,
+                (long long)sample_stride);
   EPB_CHECK_ARG(tiled || gen_smem <= 200 * 1024,
                 "mixed pass: a (k, q) block of nw=%lld, nm=%lld needs %zu bytes of shared memory (over 200 KB); use "
                 "the FP64 pass", (long long)nw, (long long)nm, gen_smem);
