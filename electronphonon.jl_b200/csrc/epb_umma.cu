@@ -236,27 +236,82 @@ __global__ void pack_a_herm_kernel(const double2* __restrict__ op, int nw, int64
   }
 }
 
+// The Hermitian-packed rows of H(R) modulated by the phases of a batch of k points, for
+//   H(k + q) = sum_R [H_R exp(2 pi i R.k)] exp(2 pi i R.q):
+// batch b holds rows b * rows_pad .. b * rows_pad + nw^2 - 1 of A, and the B operand is the phase planes
+// of the q list, shared by every k of the pass. Same row and K' layout as pack_a_herm_kernel.
+template <bool BF16, int NPL>
+__global__ void pack_a_herm_mod_kernel(const double2* __restrict__ op, const int4* __restrict__ rv, int nw,
+                                       int64_t K, const double* __restrict__ xk, int64_t nk, int64_t rows_pad,
+                                       int64_t KC, uint8_t* __restrict__ planes, int64_t plane_bytes) {
+  const int64_t nch = KC * 8, koff = sin_offset(K);
+  const int64_t total = nk * rows_pad * nch;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t rowg = idx / nch, ch = idx - rowg * nch;
+    const int64_t b = rowg / rows_pad, row = rowg - b * rows_pad;
+    double v[8];
+    int i = 0, j = 0, part = 0;
+    const bool live = row < (int64_t)nw * nw;
+    if (live) herm_row_to_ij((int)row, nw, i, j, part);
+    const double x0 = xk[3 * b], x1 = xk[3 * b + 1], x2 = xk[3 * b + 2];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int64_t kk = ch * 8 + e;
+      double x = 0.0;
+      if (live) {
+        const bool cosc = kk < K, sinc = kk >= koff && kk < koff + K;
+        if (cosc || sinc) {
+          const int64_t p = cosc ? kk : kk - koff;
+          const int4 r = rv[p];
+          const double2 h = cmul(op[(i + (int64_t)j * nw) + p * (int64_t)nw * nw], cis2pi(rdotx(r.x, r.y, r.z, x0, x1, x2)));
+          // cos coefficient: Re h (real row) / Im h (imag row); sin coefficient: -Im h / Re h
+          x = cosc ? (part == 0 ? h.x : h.y) : (part == 0 ? -h.y : h.x);
+        }
+      }
+      v[e] = x;
+    }
+    store_split8<BF16, NPL>(planes, plane_bytes, tiled_offset(rowg, ch * 8, KC), v);
+  }
+}
+
 // Phase operand: row j of B2 = [cos 2 pi R.x_j | sin 2 pi R.x_j] (K-major), x_j = xa[:, p / nb] +
 // xb[:, p % nb] with p = pidx[j] (pidx != null) or pair0 + j when xb != null (x_{k+q} for pairs of
 // a k list and a q list), else x_j = xa[:, j].
+// A thread writes 8 consecutive R of one point. The first is evaluated directly; an R that follows its
+// predecessor by (0, 0, 1) (the usual order of an R list) takes the previous value times exp(2 pi i x_3)
+// (at most 7 products: a few 1e-16), any other R is evaluated directly. The values are rounded to FP32
+// and split in FP32 (exact: the planes hold the FP32 value), so the kernel stays on the HBM write bound.
 template <bool BF16, int NPL>
 __global__ void pack_b_phase_kernel(const int4* __restrict__ rv, int64_t K, const double* __restrict__ xa,
                                     const double* __restrict__ xb, int64_t nb, const int64_t* __restrict__ pidx,
                                     int64_t pair0, int64_t N, int64_t rows_pad, int64_t KC,
                                     uint8_t* __restrict__ planes, int64_t plane_bytes) {
-  const int64_t koff = sin_offset(K);
-  const int64_t ncos = koff / 8;           // chunks covering [0, koff)
-  const int64_t nch = KC * 8;
-  const int64_t total = rows_pad * ncos;    // one thread per (point, 8 R vectors): cos and sin chunks
+  const int koff = (int)sin_offset(K);
+  const int ncos = koff / 8;  // chunks covering [0, koff)
+  const int nch = (int)KC * 8;
+  const int64_t total = rows_pad * ncos;  // one thread per (point, 8 R vectors): cos and sin chunks
+  const bool idx32 = total <= 0x7fffffff;
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
-    int64_t ch = idx % ncos, j = idx / ncos;
-    double c[8], sn[8];
-    double x0 = 0, x1 = 0, x2 = 0;
+    int64_t j;
+    int ch;
+    if (idx32) {
+      const uint32_t i = (uint32_t)idx, jj = i / (uint32_t)ncos;
+      j = jj;
+      ch = (int)(i - jj * (uint32_t)ncos);
+    } else {
+      j = idx / ncos;
+      ch = (int)(idx - j * ncos);
+    }
+    float c[8], sn[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) c[e] = sn[e] = 0.f;
     if (j < N) {
+      double x0, x1, x2;
       if (xb) {
         const int64_t pj = pidx ? pidx[j] : pair0 + j;
-        int64_t ja = pj / nb, jb = pj % nb;
+        const int64_t ja = pj / nb, jb = pj - ja * nb;
         x0 = xa[3 * ja] + xb[3 * jb];
         x1 = xa[3 * ja + 1] + xb[3 * jb + 1];
         x2 = xa[3 * ja + 2] + xb[3 * jb + 2];
@@ -265,89 +320,30 @@ __global__ void pack_b_phase_kernel(const int4* __restrict__ rv, int64_t K, cons
         x1 = xa[3 * j + 1];
         x2 = xa[3 * j + 2];
       }
-    }
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      int64_t p = ch * 8 + e;
-      c[e] = 0.0;
-      sn[e] = 0.0;
-      if (j < N && p < K) {
-        int4 r = rv[p];
-        double2 z = cis2pi(rdotx(r.x, r.y, r.z, x0, x1, x2));
-        c[e] = z.x;
-        sn[e] = z.y;
-      }
-    }
-    store_split8<BF16, NPL>(planes, plane_bytes, tiled_offset(j, ch * 8, KC), c);
-    store_split8<BF16, NPL>(planes, plane_bytes, tiled_offset(j, koff + ch * 8, KC), sn);
-    // trailing zero chunks beyond koff + koff (when KC*64 > 2*koff)
-    for (int64_t z = 2 * ncos + ch; z < nch; z += ncos) {
-      double zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      store_split8<BF16, NPL>(planes, plane_bytes, tiled_offset(j, z * 8, KC), zero);
-    }
-  }
-}
-
-// The same phase operand from per-axis tables: exp(2 pi i R.x) = prod_d exp(2 pi i R_d x_d). A block
-// takes SEP_PTS points at a time; their axis factors (R_d in [lo_d, lo_d + span_d), span_d <= SEP_SPAN)
-// are evaluated once into shared memory, and each entry is two FP64 complex products instead of one
-// FP64 sincospi. Every axis argument R_d x_d is reduced on its own, so the entries agree with the direct
-// evaluation to a few 1e-16; each entry is then rounded to FP32 and split in FP32 (the planes hold the
-// FP32 value exactly, 2^-24 relative, the same order as the truncation of the split itself).
-constexpr int SEP_PTS = 8, SEP_SPAN = 64;
-template <bool BF16, int NPL>
-__global__ void __launch_bounds__(256) pack_b_phase_sep_kernel(
-    const int4* __restrict__ rv, int64_t K, int lo0, int lo1, int lo2, int sp0, int sp1, int sp2,
-    const double* __restrict__ xa, const double* __restrict__ xb, int64_t nb, const int64_t* __restrict__ pidx,
-    int64_t pair0, int64_t N, int64_t rows_pad, int64_t KC, uint8_t* __restrict__ planes, int64_t plane_bytes) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double2* tab = reinterpret_cast<double2*>(smem_raw);  // [SEP_PTS][sp0 + sp1 + sp2]
-  const int spt = sp0 + sp1 + sp2;
-  const int koff = (int)sin_offset(K), ncos = koff / 8, nch = (int)KC * 8;
-  const int64_t ngroups = rows_pad / SEP_PTS;  // rows_pad is a multiple of 128
-  for (int64_t grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
-    const int64_t j0 = grp * SEP_PTS;
-    __syncthreads();  // the previous group's table is no longer read
-    for (int e = threadIdx.x; e < SEP_PTS * spt; e += blockDim.x) {
-      const int p = e / spt, m = e - p * spt;
-      const int d = m < sp0 ? 0 : m < sp0 + sp1 ? 1 : 2;
-      const int r = d == 0 ? lo0 + m : d == 1 ? lo1 + m - sp0 : lo2 + m - sp0 - sp1;
-      const int64_t j = j0 + p;
-      double x = 0.0;
-      if (j < N) {
-        if (xb) {
-          const int64_t pj = pidx ? pidx[j] : pair0 + j;
-          x = xa[3 * (pj / nb) + d] + xb[3 * (pj % nb) + d];
-        } else {
-          x = xa[3 * j + d];
-        }
-      }
-      tab[e] = cis2pi(__dmul_rn((double)r, x));
-    }
-    __syncthreads();
-    for (int it = threadIdx.x; it < SEP_PTS * ncos; it += blockDim.x) {
-      const int p = it / ncos, ch = it - p * ncos;
-      const int64_t j = j0 + p;
-      const double2* t = tab + p * spt;
-      float c[8], sn[8];
+      const double2 step = cis2pi(x2);
+      double2 z = make_double2(1.0, 0.0);
+      int4 rp = make_int4(0, 0, 0, 0);
 #pragma unroll
       for (int e = 0; e < 8; ++e) {
         const int q = ch * 8 + e;
-        c[e] = 0.f;
-        sn[e] = 0.f;
-        if (j < N && q < K) {
+        if (q < K) {
           const int4 r = rv[q];
-          const double2 z = cmul(cmul(t[r.x - lo0], t[sp0 + r.y - lo1]), t[sp0 + sp1 + r.z - lo2]);
+          if (e > 0 && r.x == rp.x && r.y == rp.y && r.z == rp.z + 1)
+            z = cmul(z, step);
+          else
+            z = cis2pi(rdotx(r.x, r.y, r.z, x0, x1, x2));
+          rp = r;
           c[e] = (float)z.x;
           sn[e] = (float)z.y;
         }
       }
-      store_split8_f32<BF16, NPL>(planes, plane_bytes, tiled_offset(j, ch * 8, KC), c);
-      store_split8_f32<BF16, NPL>(planes, plane_bytes, tiled_offset(j, koff + ch * 8, KC), sn);
-      for (int z = 2 * ncos + ch; z < nch; z += ncos) {
-        const float zero[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        store_split8_f32<BF16, NPL>(planes, plane_bytes, tiled_offset(j, (int64_t)z * 8, KC), zero);
-      }
+    }
+    store_split8_f32<BF16, NPL>(planes, plane_bytes, tiled_offset(j, ch * 8, KC), c);
+    store_split8_f32<BF16, NPL>(planes, plane_bytes, tiled_offset(j, koff + ch * 8, KC), sn);
+    // trailing zero chunks beyond koff + koff (when KC*64 > 2*koff)
+    for (int z = 2 * ncos + ch; z < nch; z += ncos) {
+      const float zero[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      store_split8_f32<BF16, NPL>(planes, plane_bytes, tiled_offset(j, (int64_t)z * 8, KC), zero);
     }
   }
 }
@@ -608,16 +604,6 @@ static unsigned grid_for(epb_ctx* ctx, int64_t total) {
   return (unsigned)(g < cap ? (g < 1 ? 1 : g) : cap);
 }
 
-// Per-axis phase tables apply when every axis of the R set spans at most SEP_SPAN values.
-static bool sep_spans_ok(const epb_rset* rs) {
-  for (int d = 0; d < 3; ++d)
-    if (rs->hi[d] - rs->lo[d] + 1 > SEP_SPAN) return false;
-  return true;
-}
-static unsigned sep_grid(epb_ctx* ctx, int64_t rows_pad) {
-  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(rows_pad / SEP_PTS, (int64_t)ctx->sm_count * 8));
-}
-
 template <bool BF16, int NPL, int NT>
 static int launch_split_gemm(epb_ctx* ctx, SplitGemmArgs& a) {
   using Cfg = GemmCfg<BF16, NPL, NT>;
@@ -744,6 +730,23 @@ int pack_a_herm(epb_ctx* ctx, const double2* op, int nw, int64_t K, Planes& out,
   return EPB_OK;
 }
 
+// A operand of H(k + q) for nk k points (batches of rows_pad_k rows each).
+int pack_a_herm_mod(epb_ctx* ctx, const double2* op, const epb_rset* rs, int nw, const double* xk, int64_t nk,
+                    int64_t rows_pad_k, Planes& out, uint8_t* mem) {
+  out.rows_pad = nk * rows_pad_k;
+  out.KC = kchunks(rs->nr);
+  out.plane_bytes = plane_bytes_for(out.rows_pad, out.KC);
+  out.npl = MX_NPL;
+  out.p = mem;
+  const int64_t total = out.rows_pad * out.KC * 8;
+  prof_begin(ctx, EPB_PROF_SPLIT);
+  pack_a_herm_mod_kernel<MX_BF16, MX_NPL><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
+      op, rs->dev, nw, rs->nr, xk, nk, rows_pad_k, out.KC, out.p, out.plane_bytes);
+  prof_end(ctx);
+  EPB_LAUNCH_CHECK();
+  return EPB_OK;
+}
+
 int pack_b_phase(epb_ctx* ctx, const epb_rset* rs, const double* xa, const double* xb, int64_t nb, int64_t N,
                  Planes& out, uint8_t* mem, const int64_t* pidx = nullptr, int64_t pair0 = 0) {
   out.rows_pad = round_up(N, MX_NT);
@@ -753,16 +756,8 @@ int pack_b_phase(epb_ctx* ctx, const epb_rset* rs, const double* xa, const doubl
   out.p = mem;
   int64_t total = out.rows_pad * (sin_offset(rs->nr) / 8);
   prof_begin(ctx, EPB_PROF_SPLIT);
-  if (sep_spans_ok(rs)) {
-    const int sp0 = rs->hi[0] - rs->lo[0] + 1, sp1 = rs->hi[1] - rs->lo[1] + 1, sp2 = rs->hi[2] - rs->lo[2] + 1;
-    pack_b_phase_sep_kernel<MX_BF16, MX_NPL><<<sep_grid(ctx, out.rows_pad), 256, SEP_PTS * (sp0 + sp1 + sp2) * 16,
-                                               ctx->stream>>>(
-        rs->dev, rs->nr, rs->lo[0], rs->lo[1], rs->lo[2], sp0, sp1, sp2, xa, xb, nb, pidx, pair0, N, out.rows_pad,
-        out.KC, out.p, out.plane_bytes);
-  } else {
-    pack_b_phase_kernel<MX_BF16, MX_NPL><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
-        rs->dev, rs->nr, xa, xb, nb, pidx, pair0, N, out.rows_pad, out.KC, out.p, out.plane_bytes);
-  }
+  pack_b_phase_kernel<MX_BF16, MX_NPL><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
+      rs->dev, rs->nr, xa, xb, nb, pidx, pair0, N, out.rows_pad, out.KC, out.p, out.plane_bytes);
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
@@ -778,16 +773,8 @@ int pack_b_phase_h(epb_ctx* ctx, const epb_rset* rs, const double* xa, const dou
   out.p = mem;
   int64_t total = out.rows_pad * (sin_offset(rs->nr) / 8);
   prof_begin(ctx, EPB_PROF_SPLIT);
-  if (sep_spans_ok(rs)) {
-    const int sp0 = rs->hi[0] - rs->lo[0] + 1, sp1 = rs->hi[1] - rs->lo[1] + 1, sp2 = rs->hi[2] - rs->lo[2] + 1;
-    pack_b_phase_sep_kernel<false, 2><<<sep_grid(ctx, out.rows_pad), 256, SEP_PTS * (sp0 + sp1 + sp2) * 16,
-                                        ctx->stream>>>(
-        rs->dev, rs->nr, rs->lo[0], rs->lo[1], rs->lo[2], sp0, sp1, sp2, xa, xb, nb, nullptr, 0, N, out.rows_pad,
-        out.KC, out.p, out.plane_bytes);
-  } else {
-    pack_b_phase_kernel<false, 2><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
-        rs->dev, rs->nr, xa, xb, nb, nullptr, 0, N, out.rows_pad, out.KC, out.p, out.plane_bytes);
-  }
+  pack_b_phase_kernel<false, 2><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
+      rs->dev, rs->nr, xa, xb, nb, nullptr, 0, N, out.rows_pad, out.KC, out.p, out.plane_bytes);
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
@@ -1449,7 +1436,8 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
   const size_t o_bk = carve(MX_NPL * plane_bytes_for(round_up(KO, MX_NT), KC_el));
   const size_t o_c0 = carve(4 * 2 * nd_ep * KO);
   const size_t o_a2 = carve(MX_NPL * plane_bytes_for(rows_pad_k * KO, KC_ep));
-  const size_t o_bkq = carve(MX_NPL * plane_bytes_for(round_up(kbi * nq, MX_NT), KC_el));
+  const size_t o_bqel = carve(MX_NPL * plane_bytes_for(round_up(nq, MX_NT), KC_el));  // q phases over Re
+  const size_t o_ah = carve(MX_NPL * plane_bytes_for(kbi * mm->H.rows_pad, KC_el));     // modulated H(R) rows
   const size_t o_c1 = carve(4 * nw2 * kbi * nq);
   const size_t o_u32 = carve(8 * nw2 * kbi * nq);
   const size_t o_c2 = carve(4 * 2 * nd * kbi * nq);
@@ -1469,6 +1457,9 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
   // |G| <= sqrt(nw) nr_el max|g(Re,Rp)| below 2^14 (FP16 range), the epilogue multiplies it back out
   Planes Bp;
   EPB_TRY(pack_b_phase_h(ctx, m->rs_ep, xq, nullptr, 1, nq, Bp, base + o_bp));
+  // H(k+q) is (H(R) modulated by k) x (q phases over Re): the q side is packed once for the pass
+  Planes Bq_el;
+  EPB_TRY(pack_b_phase(ctx, m->rs_el, xq, nullptr, 1, nq, Bq_el, base + o_bqel));
   double gbound = std::sqrt((double)nw) * (double)m->nr_el * (mm->ep_absmax > 0.0 ? mm->ep_absmax : 1.0);
   const int e2 = std::max(-120, std::min(120, 14 - (int)std::ceil(std::log2(gbound))));
   const double a2_scale = std::ldexp(1.0, e2);
@@ -1507,10 +1498,12 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
     for (int64_t ki = 0; ki < nko; ki += kbi) {
       const int64_t nki = nko - ki < kbi ? nko - ki : kbi;
       const int64_t np = nki * nq;
-      // H(k+q) on the tensor cores (Hermitian-packed rows), then FP32 solve + FP64 refinement
-      Planes Bkq;
-      EPB_TRY(pack_b_phase(ctx, m->rs_el, xko + 3 * ki, xq, nq, np, Bkq, base + o_bkq));
-      EPB_TRY(split_gemm(ctx, EPB_PROF_UMMA_H, mm->H, Bkq, mm->H.rows_pad / 128, 1, nw2, np, true, C1, 0, nw2));
+      // H(k+q) on the tensor cores: Hermitian-packed rows of H(R) exp(2 pi i R.k) per k times the q phases,
+      // then FP32 solve + FP64 refinement
+      Planes Ah;
+      EPB_TRY(pack_a_herm_mod(ctx, m->ham, m->rs_el, (int)nw, xko + 3 * ki, nki, mm->H.rows_pad, Ah, base + o_ah));
+      EPB_TRY(split_gemm(ctx, EPB_PROF_UMMA_H, Ah, Bq_el, mm->H.rows_pad / 128, nki, nw2, nq, true, C1, nw2 * nq,
+                         nw2));
       EPB_TRY(eigh_mixed_packed(ctx, C1, nw, np, U32, nullptr));
       // kR->kq on the tensor cores, batched over the k of this inner batch
       Planes A2i = A2;
