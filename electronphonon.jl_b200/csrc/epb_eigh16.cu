@@ -164,15 +164,21 @@ __device__ int onesided_sweeps_f32x2(float2 (&a)[E16], float tol, int max_sweeps
       // same elementwise products in the same order, with the two imaginary sums trading places, so
       // both lanes hold bitwise-identical g = a_p^H a_q and norms (a, b) in the p lane's orientation
       // and derive the same rotation without exchanging it.
-      f32x2 gr = Z, gi = Z, gj = Z;
+      // (independent even / odd chains of four: the dot products are on the round's critical path)
+      f32x2 gx0 = Z, gx1 = Z, gy0 = Z, gy1 = Z, gi0 = Z, gi1 = Z, gj0 = Z, gj1 = Z;
 #pragma unroll
-      for (int i = 0; i < E16 / 2; ++i) {
-        gr = pfma(Y[i], BY[i], pfma(X[i], BX[i], gr));
-        gi = pfma(X[i], BY[i], gi);
-        gj = pfma(Y[i], BX[i], gj);
+      for (int i = 0; i < E16 / 2; i += 2) {
+        gx0 = pfma(X[i], BX[i], gx0);
+        gx1 = pfma(X[i + 1], BX[i + 1], gx1);
+        gy0 = pfma(Y[i], BY[i], gy0);
+        gy1 = pfma(Y[i + 1], BY[i + 1], gy1);
+        gi0 = pfma(X[i], BY[i], gi0);
+        gi1 = pfma(X[i + 1], BY[i + 1], gi1);
+        gj0 = pfma(Y[i], BX[i], gj0);
+        gj1 = pfma(Y[i + 1], BX[i + 1], gj1);
       }
-      const float hi = hsum(gi), hj = hsum(gj);
-      const float gx = hsum(gr), gy = isP ? hi - hj : hj - hi;
+      const float hi = hsum(gi0) + hsum(gi1), hj = hsum(gj0) + hsum(gj1);
+      const float gx = (hsum(gx0) + hsum(gx1)) + (hsum(gy0) + hsum(gy1)), gy = isP ? hi - hj : hj - hi;
       const float A = isP ? nrm : nb, B = isP ? nb : nrm;
       const float ag2 = gx * gx + gy * gy;
       if (ag2 > tol2 * (A * B) && ag2 > 0.f) {

@@ -570,7 +570,8 @@ __global__ void __launch_bounds__(192, 1) split_gemm_kernel(SplitGemmArgs a) {
           for (int j = 0; j < 16; ++j) {
             int64_t col = nt * NT + c0 + j;
             if (col < a.n_valid) {
-              const float val = (float)((double)v[j] + (double)w[j]);
+              // one FP32 rounding of the exact sum, as the FP64 route gives (no FP64 conversions)
+              const float val = v[j] + w[j];
               cb[col * a.ldc_n] = a.cscale != 0.f ? val * a.cscale : val;
             }
           }
