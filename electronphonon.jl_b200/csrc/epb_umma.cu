@@ -371,6 +371,8 @@ struct SplitGemmArgs {
   int64_t ngrp;
   // power-of-two scale applied to C in the epilogue (undoing an operand's pre-scale); 0 = none
   float cscale;
+  // A-resident kernel: column tiles per work unit (a unit = one A tile and a run of column tiles)
+  int64_t n_per_unit;
 };
 
 template <bool BF16, int NPL>
@@ -587,6 +589,233 @@ __global__ void __launch_bounds__(192, 1) split_gemm_kernel(SplitGemmArgs a) {
   if (warp == 0) tmem_dealloc(tmem, Cfg::TMEM_COLS);
 }
 
+// A-resident form of the same GEMM for short K (KC <= ARES_KC, i.e. K' <= 256): a work unit is one
+// 128-row A tile and a run of n_per_unit column tiles. The whole A tile (all K chunks, all planes) is
+// copied into shared memory once per unit and every column tile of the run streams only its B chunks,
+// so each 128 x 128 output tile costs one B tile of L2 traffic instead of an A and a B tile (the
+// kR->kq GEMM of the pass, K' = 256, is bound by that feed). A has its own full / empty barrier pair:
+// the MMA thread commits `a_empty` after the unit's last MMA, the producer waits on it before it
+// overwrites A. Same products, accumulators and epilogue as split_gemm_kernel; no grouped mode.
+constexpr int ARES_KC = 4, ARES_STAGES = 3;
+template <bool BF16, int NPL, int NT>
+struct AresCfg {
+  using G = GemmCfg<BF16, NPL, NT>;
+  static constexpr int A_BYTES = ARES_KC * NPL * TILE_BYTES;
+  static constexpr int STAGE = NPL * G::B_SUB * G::B_TILE;  // B chunks of one K step
+  static constexpr int SMEM = A_BYTES + ARES_STAGES * STAGE + 1024 /*align*/ + 256 /*barriers*/;
+  static constexpr int TMEM_COLS = G::TMEM_COLS;
+};
+
+template <bool BF16, int NPL, int NT>
+__global__ void __launch_bounds__(192, 1) split_gemm_ares_kernel(SplitGemmArgs a) {
+  using Cfg = AresCfg<BF16, NPL, NT>;
+  using G = GemmCfg<BF16, NPL, NT>;
+  using Pr = Products<BF16, NPL>;
+  constexpr int STAGES = ARES_STAGES;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  uint8_t* smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+  uint8_t* bst = smem + Cfg::A_BYTES;  // B stages
+  uint64_t* bars = reinterpret_cast<uint64_t*>(bst + STAGES * Cfg::STAGE);
+  uint64_t* full = bars;                 // [STAGES]
+  uint64_t* empty = bars + STAGES;       // [STAGES]
+  uint64_t* tfull = bars + 2 * STAGES;   // [2]
+  uint64_t* tempty = tfull + 2;          // [2]
+  uint64_t* afull = tempty + 2;          // [1]
+  uint64_t* aempty = afull + 1;          // [1]
+  uint64_t* done = aempty + 1;           // [1]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile int* err = a.err;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 128);
+    }
+    mbar_init(afull, 1);
+    mbar_init(aempty, 1);
+    mbar_init(done, 1);
+    fence_barrier_init();
+  }
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int64_t npu = a.n_per_unit;
+  const int64_t nsplit = (a.n_tiles + npu - 1) / npu;
+  const int64_t nunits = a.m_tiles * nsplit;
+  constexpr uint32_t IDESC = idesc_f16(128, NT, BF16);
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- producer ----------------
+    int s = 0;
+    uint32_t ph = 0;
+    bool ok = true;
+    uint32_t inflight = 0, inflight_ph = 0;  // B stages whose copies nobody has waited for yet
+    bool a_inflight = false;
+    uint32_t a_ph = 0;
+    int64_t uu = 0;
+    for (int64_t u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++uu) {
+      const int64_t mt = u / nsplit, n0 = (u % nsplit) * npu;
+      const int64_t n1 = n0 + npu < a.n_tiles ? n0 + npu : a.n_tiles;
+      if (!mbar_wait(aempty, (uint32_t)(uu & 1) ^ 1u, err, a.timeout)) break;
+      mbar_arrive_expect_tx(afull, (uint32_t)(a.KC * NPL * TILE_BYTES));
+      for (int kc = 0; kc < a.KC; ++kc)
+        for (int p = 0; p < NPL; ++p)
+          bulk_g2s(smem + (kc * NPL + p) * TILE_BYTES,
+                   a.A + p * a.a_plane_bytes + (mt * a.KC + kc) * (int64_t)TILE_BYTES, TILE_BYTES, afull);
+      a_inflight = true;
+      a_ph = (uint32_t)(uu & 1);
+      for (int64_t nt = n0; nt < n1 && ok; ++nt) {
+        for (int kc = 0; kc < a.KC; ++kc) {
+          if (!mbar_wait(&empty[s], ph ^ 1u, err, a.timeout)) {
+            ok = false;
+            break;
+          }
+          inflight &= ~(1u << s);
+          uint8_t* st = bst + s * Cfg::STAGE;
+          mbar_arrive_expect_tx(&full[s], Cfg::STAGE);
+          for (int p = 0; p < NPL; ++p)
+            for (int sb = 0; sb < G::B_SUB; ++sb) {
+              const int64_t bt = nt * G::B_SUB + sb;
+              const uint8_t* src = a.B + p * a.b_plane_bytes + (bt * a.KC + kc) * (int64_t)G::B_TILE;
+              bulk_g2s(st + (p * G::B_SUB + sb) * G::B_TILE, src, G::B_TILE, &full[s]);
+            }
+          inflight |= 1u << s;
+          inflight_ph = (inflight_ph & ~(1u << s)) | (ph << s);
+          if (++s == STAGES) {
+            s = 0;
+            ph ^= 1u;
+          }
+        }
+      }
+    }
+    // drain: wait (bounded) for every copy that may still be landing
+    for (int q = 0; q < STAGES; ++q)
+      if (inflight & (1u << q)) {
+        long long t0 = clock64();
+        while (!mbar_try_wait(&full[q], (inflight_ph >> q) & 1u) && clock64() - t0 < a.timeout) {
+        }
+      }
+    if (a_inflight) {
+      long long t0 = clock64();
+      while (!mbar_try_wait(afull, a_ph) && clock64() - t0 < a.timeout) {
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer ----------------
+    int s = 0;
+    uint32_t ph = 0;
+    bool ok = true;
+    int64_t tc = 0, uu = 0;  // output tiles and units of this CTA so far
+    const uint32_t abase = smem_u32(smem);
+    for (int64_t u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++uu) {
+      const int64_t n0 = (u % nsplit) * npu;
+      const int64_t n1 = n0 + npu < a.n_tiles ? n0 + npu : a.n_tiles;
+      if (!mbar_wait(afull, (uint32_t)(uu & 1), err, a.timeout)) break;
+      tc_fence_after();
+      for (int64_t nt = n0; nt < n1 && ok; ++nt, ++tc) {
+        const int b = (int)(tc & 1);
+        const uint32_t use = (uint32_t)(tc >> 1) & 1u;
+        if (!mbar_wait(&tempty[b], use ^ 1u, err, a.timeout)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        // accumulator 0 takes the leading h*h product, accumulator 1 the correction products
+        const uint32_t dcol = tmem + b * 2 * NT;
+        for (int kc = 0; kc < a.KC; ++kc) {
+          if (!mbar_wait(&full[s], ph, err, a.timeout)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t st = smem_u32(bst + s * Cfg::STAGE);
+#pragma unroll
+          for (int sub = 0; sub < 4; ++sub) {
+#pragma unroll
+            for (int pr = 0; pr < Pr::N; ++pr) {
+              const bool lead = Pr::a(pr) == 0 && Pr::b(pr) == 0;
+              uint64_t ad = smem_desc_sw128(abase + (kc * NPL + Pr::a(pr)) * TILE_BYTES + sub * 32);
+              uint64_t bd = smem_desc_sw128(st + Pr::b(pr) * G::B_SUB * G::B_TILE + sub * 32);
+              const bool first = kc == 0 && sub == 0 && (lead || pr == 0);
+              mma_f16(dcol + (lead ? 0u : (uint32_t)NT), ad, bd, IDESC, first ? 0u : 1u);
+            }
+          }
+          mma_commit(&empty[s]);
+          if (++s == STAGES) {
+            s = 0;
+            ph ^= 1u;
+          }
+        }
+        if (ok) mma_commit(&tfull[b]);
+      }
+      mma_commit(aempty);  // the A tile may be overwritten once this unit's MMAs have completed
+    }
+    // all issued MMAs must retire before TMEM is released
+    mma_commit(done);
+    long long t0 = clock64();
+    while (!mbar_try_wait(done, 0) && clock64() - t0 < a.timeout) {
+    }
+  } else if (warp >= 2) {
+    // ---------------- epilogue ----------------
+    const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31
+    const int row_in_tile = quarter * 32 + lane;
+    int64_t tc = 0;
+    bool go = true;
+    for (int64_t u = blockIdx.x; u < nunits && go; u += gridDim.x) {
+      const int64_t mt = u / nsplit, n0 = (u % nsplit) * npu;
+      const int64_t n1 = n0 + npu < a.n_tiles ? n0 + npu : a.n_tiles;
+      const int64_t batch = mt / a.m_tiles_per_batch;
+      const int64_t row = (mt % a.m_tiles_per_batch) * 128 + row_in_tile;
+      float* cb = a.C + batch * a.c_batch_stride + row;
+      const bool row_ok = row < a.m_valid;
+      for (int64_t nt = n0; nt < n1; ++nt, ++tc) {
+        const int b = (int)(tc & 1);
+        const uint32_t use = (uint32_t)(tc >> 1) & 1u;
+        bool okw = mbar_wait(&tfull[b], use, err, a.timeout);
+        if (!__all_sync(0xffffffffu, okw)) {  // warp-uniform: the TMEM loads below are .sync.aligned
+          go = false;
+          break;
+        }
+        tc_fence_after();
+#pragma unroll 1
+        for (int c0 = 0; c0 < NT; c0 += 16) {
+          float v[16], w[16];
+          const uint32_t ta = tmem + ((uint32_t)(quarter * 32) << 16) + b * 2 * NT + c0;
+          tmem_ld16(ta, v);
+          tmem_ld16(ta + NT, w);
+          if (row_ok) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const int64_t col = nt * NT + c0 + j;
+              if (col < a.n_valid) {
+                const float val = v[j] + w[j];
+                cb[col * a.ldc_n] = a.cscale != 0.f ? val * a.cscale : val;
+              }
+            }
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(&tempty[b]);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) tmem_dealloc(tmem, Cfg::TMEM_COLS);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Host-side helpers.
 struct Planes {
@@ -619,6 +848,26 @@ static int launch_split_gemm(epb_ctx* ctx, SplitGemmArgs& a) {
   if (total == 0) return EPB_OK;
   unsigned grid = (unsigned)(total < ctx->sm_count ? total : ctx->sm_count);
   split_gemm_kernel<BF16, NPL, NT><<<grid, 192, Cfg::SMEM, ctx->stream>>>(a);
+  EPB_LAUNCH_CHECK();
+  return EPB_OK;
+}
+
+template <bool BF16, int NPL, int NT>
+static int launch_split_gemm_ares(epb_ctx* ctx, SplitGemmArgs& a) {
+  using Cfg = AresCfg<BF16, NPL, NT>;
+  static_assert(Cfg::SMEM <= 227 * 1024, "A-resident GEMM: shared memory over the per-CTA limit");
+  static bool attr = false;
+  if (!attr) {
+    EPB_CUDA(cudaFuncSetAttribute(split_gemm_ares_kernel<BF16, NPL, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  Cfg::SMEM));
+    attr = true;
+  }
+  EPB_CHECK_ARG(a.KC <= ARES_KC && !a.grp && a.n_per_unit >= 1, "A-resident GEMM: K' over %d or grouped",
+                64 * ARES_KC);
+  const int64_t units = a.m_tiles * cdiv(a.n_tiles, a.n_per_unit);
+  if (units == 0) return EPB_OK;
+  const unsigned grid = (unsigned)(units < ctx->sm_count ? units : ctx->sm_count);
+  split_gemm_ares_kernel<BF16, NPL, NT><<<grid, 192, Cfg::SMEM, ctx->stream>>>(a);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
 }
@@ -683,7 +932,17 @@ int split_gemm_h(epb_ctx* ctx, int prof_id, const Planes& A, const Planes& B, in
   EPB_CHECK_ARG(A.KC == B.KC && A.npl == 2 && B.npl == 2, "FP16x2 GEMM: operand planes mismatch");
   EPB_CHECK_ARG(B.rows_pad >= a.n_tiles * MX_NT, "FP16x2 GEMM: B planes too small");
   prof_begin(ctx, prof_id);
-  int st = launch_split_gemm<false, 2, MX_NT>(ctx, a);
+  int st;
+  if (a.KC <= ARES_KC) {
+    // A-resident: a unit is one A tile and n_per_unit column tiles; enough units for ~16 per CTA, at
+    // least 8 column tiles per unit (the A copy is then under 1/8 of the unit's traffic)
+    const int64_t want = cdiv(16 * (int64_t)ctx->sm_count, std::max<int64_t>(a.m_tiles, 1));
+    const int64_t nsplit = std::max<int64_t>(1, std::min<int64_t>(want, a.n_tiles / 8));
+    a.n_per_unit = cdiv(a.n_tiles, nsplit);
+    st = launch_split_gemm_ares<false, 2, MX_NT>(ctx, a);
+  } else {
+    st = launch_split_gemm<false, 2, MX_NT>(ctx, a);
+  }
   prof_end(ctx);
   return st;
 }
