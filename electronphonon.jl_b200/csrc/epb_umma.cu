@@ -406,6 +406,34 @@ struct GemmCfg {
   static constexpr int TMEM_COLS = 4 * NT < 32 ? 32 : 4 * NT;
 };
 
+// Epilogue of one output tile (one thread per TMEM lane = tile row): C[row, col] = acc0 + acc1 (one FP32
+// rounding), times cscale when set. 64 columns of both accumulators are loaded per TMEM wait.
+template <int NT>
+__device__ __forceinline__ void epilogue_tile(const SplitGemmArgs& a, uint32_t tacc, float* cb, bool row_ok,
+                                              int64_t col0) {
+  constexpr int CB = NT < 64 ? NT : 64;
+#pragma unroll 1
+  for (int c0 = 0; c0 < NT; c0 += CB) {
+    uint32_t r[2 * CB];
+#pragma unroll
+    for (int j = 0; j < CB; j += 16) {
+      tmem_ld16_nowait(tacc + c0 + j, r + j);
+      tmem_ld16_nowait(tacc + NT + c0 + j, r + CB + j);
+    }
+    tmem_wait_ld(r);
+    if (row_ok) {
+      float* p = cb + (col0 + c0) * a.ldc_n;
+#pragma unroll
+      for (int j = 0; j < CB; ++j, p += a.ldc_n) {
+        if (col0 + c0 + j < a.n_valid) {
+          const float val = __uint_as_float(r[j]) + __uint_as_float(r[CB + j]);
+          *p = a.cscale != 0.f ? val * a.cscale : val;
+        }
+      }
+    }
+  }
+}
+
 template <bool BF16, int NPL, int NT>
 __global__ void __launch_bounds__(192, 1) split_gemm_kernel(SplitGemmArgs a) {
   using Cfg = GemmCfg<BF16, NPL, NT>;
@@ -561,24 +589,7 @@ __global__ void __launch_bounds__(192, 1) split_gemm_kernel(SplitGemmArgs a) {
       const int64_t row = (mt % a.m_tiles_per_batch) * 128 + row_in_tile;
       float* cb = a.C + batch * a.c_batch_stride + row;
       const bool row_ok = row < a.m_valid;
-#pragma unroll 1
-      for (int c0 = 0; c0 < NT; c0 += 16) {
-        float v[16], w[16];
-        const uint32_t ta = tmem + ((uint32_t)(quarter * 32) << 16) + b * 2 * NT + c0;
-        tmem_ld16(ta, v);
-        tmem_ld16(ta + NT, w);
-        if (row_ok) {
-#pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            int64_t col = nt * NT + c0 + j;
-            if (col < a.n_valid) {
-              // one FP32 rounding of the exact sum, as the FP64 route gives (no FP64 conversions)
-              const float val = v[j] + w[j];
-              cb[col * a.ldc_n] = a.cscale != 0.f ? val * a.cscale : val;
-            }
-          }
-        }
-      }
+      epilogue_tile<NT>(a, tmem + ((uint32_t)(quarter * 32) << 16) + b * 2 * NT, cb, row_ok, nt * NT);
       tc_fence_before();
       mbar_arrive(&tempty[b]);
     }
@@ -788,23 +799,7 @@ __global__ void __launch_bounds__(192, 1) split_gemm_ares_kernel(SplitGemmArgs a
           break;
         }
         tc_fence_after();
-#pragma unroll 1
-        for (int c0 = 0; c0 < NT; c0 += 16) {
-          float v[16], w[16];
-          const uint32_t ta = tmem + ((uint32_t)(quarter * 32) << 16) + b * 2 * NT + c0;
-          tmem_ld16(ta, v);
-          tmem_ld16(ta + NT, w);
-          if (row_ok) {
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-              const int64_t col = nt * NT + c0 + j;
-              if (col < a.n_valid) {
-                const float val = v[j] + w[j];
-                cb[col * a.ldc_n] = a.cscale != 0.f ? val * a.cscale : val;
-              }
-            }
-          }
-        }
+        epilogue_tile<NT>(a, tmem + ((uint32_t)(quarter * 32) << 16) + b * 2 * NT, cb, row_ok, nt * NT);
         tc_fence_before();
         mbar_arrive(&tempty[b]);
       }
