@@ -334,7 +334,9 @@ def run_epb(args):
             tp = os.path.join(ROOT, "profiles", "traffic.json")
             if os.path.exists(tp):
                 with open(tp) as fh:
-                    traffic = json.load(fh).get(dom_name)
+                    tr = json.load(fh).get(dom_name)
+                if isinstance(tr, dict):  # measured bytes per unit x the units of one launch
+                    traffic = int(tr["bytes_per_unit"] * kb_used * args.nq)
             roof = {"bound": "hbm", "kernel": dom_name, "achieved": round(ach, 2), "peak": peaks["hbm_gbs"],
                     "unit": "GB/s", "frac": round(ach / peaks["hbm_gbs"], 5), "traffic": traffic,
                     "peak_source": f"{peak_src} hbm copy", "launch_ms": round(dom_ms / dom_cnt, 4),
@@ -363,7 +365,9 @@ def run_epb(args):
         tp = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tp):
             with open(tp) as fh:
-                traffic = json.load(fh).get(dom_name)
+                tr = json.load(fh).get(dom_name)
+            if isinstance(tr, dict):  # measured bytes per unit x the units of one launch
+                traffic = int(tr["bytes_per_unit"] * kb_used * args.nq)
         roof = {"bound": "tensor", "kernel": dom_name, "achieved": round(ach, 3), "peak": round(peak, 2),
                 "unit": "TFLOP/s", "frac": round(ach / peak, 4), "traffic": traffic, "peak_source": psrc,
                 "launch_ms": round(dom_ms / dom_cnt, 4), "launches_per_pass": dom_cnt,
