@@ -133,6 +133,10 @@ struct epb_ctx {
   // autotuner results: shape key -> chosen parameter (epb_eph_pass inner k batch)
   std::vector<std::pair<std::string, int64_t>> tuned;
   int64_t prof_cnt[EPB_PROF_N] = {};
+  // side stream of the mixed pass (the kR->kq GEMM runs beside the eigensolvers) and its events,
+  // created on first use
+  cudaStream_t side = nullptr;
+  cudaEvent_t side_ev[5] = {};
 };
 
 struct epb_rset {
@@ -187,6 +191,7 @@ namespace epb {
 
 // Profiler brackets around a launch (no-ops unless epb_profile_enable was called).
 void prof_begin(epb_ctx* ctx, int id);
+int side_stream(epb_ctx* ctx);
 void prof_end(epb_ctx* ctx);
 
 // Grow-only workspace slot; returns EPB_ERR_OOM on failure.

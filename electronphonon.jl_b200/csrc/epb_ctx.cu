@@ -58,6 +58,27 @@ int ws_get(epb_ctx* ctx, int slot, size_t bytes, void** out) {
   return EPB_OK;
 }
 
+// The side stream and its events (non-blocking stream, timing-free events), created once.
+int side_stream(epb_ctx* ctx) {
+  if (ctx->side) return EPB_OK;
+  // highest priority: when CTA slots free up, the side stream's (few, persistent) CTAs are placed first
+  int lo = 0, hi = 0;
+  EPB_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+  cudaStream_t s = nullptr;
+  EPB_CUDA(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, hi));
+  for (auto& e : ctx->side_ev) {
+    cudaError_t r = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    if (r != cudaSuccess) {
+      cudaStreamDestroy(s);
+      for (auto& f : ctx->side_ev)
+        if (f) cudaEventDestroy(f), f = nullptr;
+      EPB_CUDA(r);
+    }
+  }
+  ctx->side = s;
+  return EPB_OK;
+}
+
 void prof_begin(epb_ctx* ctx, int id) {
   if (!ctx->prof_on) return;
   if (ctx->prof_used == ctx->prof.size()) {
@@ -142,6 +163,12 @@ int epb_destroy(epb_ctx* ctx) {
   if (!ctx) return EPB_OK;
   make_current(ctx);
   cudaStreamSynchronize(ctx->stream);
+  if (ctx->side) {
+    cudaStreamSynchronize(ctx->side);
+    cudaStreamDestroy(ctx->side);
+  }
+  for (auto& e : ctx->side_ev)
+    if (e) cudaEventDestroy(e);
   for (auto& r : ctx->prof) {
     cudaEventDestroy(r.a);
     cudaEventDestroy(r.b);

@@ -408,10 +408,10 @@ struct GemmCfg {
 
 // Epilogue of one output tile (one thread per TMEM lane = tile row): C[row, col] = acc0 + acc1 (one FP32
 // rounding), times cscale when set. 64 columns of both accumulators are loaded per TMEM wait.
-template <int NT>
+template <int NT, int CBMAX = 64>
 __device__ __forceinline__ void epilogue_tile(const SplitGemmArgs& a, uint32_t tacc, float* cb, bool row_ok,
                                               int64_t col0) {
-  constexpr int CB = NT < 64 ? NT : 64;
+  constexpr int CB = NT < CBMAX ? NT : CBMAX;
 #pragma unroll 1
   for (int c0 = 0; c0 < NT; c0 += CB) {
     uint32_t r[2 * CB];
@@ -607,7 +607,7 @@ __global__ void __launch_bounds__(192, 1) split_gemm_kernel(SplitGemmArgs a) {
 // kR->kq GEMM of the pass, K' = 256, is bound by that feed). A has its own full / empty barrier pair:
 // the MMA thread commits `a_empty` after the unit's last MMA, the producer waits on it before it
 // overwrites A. Same products, accumulators and epilogue as split_gemm_kernel; no grouped mode.
-constexpr int ARES_KC = 4, ARES_STAGES = 3;
+constexpr int ARES_KC = 4, ARES_STAGES = 2;
 template <bool BF16, int NPL, int NT>
 struct AresCfg {
   using G = GemmCfg<BF16, NPL, NT>;
@@ -618,7 +618,9 @@ struct AresCfg {
 };
 
 template <bool BF16, int NPL, int NT>
-__global__ void __launch_bounds__(192, 1) split_gemm_ares_kernel(SplitGemmArgs a) {
+// (at most 85 registers: one CTA of this kernel leaves room on its SM for three CTAs of the FP32 Jacobi,
+// which the pass runs beside it on another stream)
+__global__ void __launch_bounds__(192, 4) split_gemm_ares_kernel(SplitGemmArgs a) {
   using Cfg = AresCfg<BF16, NPL, NT>;
   using G = GemmCfg<BF16, NPL, NT>;
   using Pr = Products<BF16, NPL>;
@@ -799,7 +801,7 @@ __global__ void __launch_bounds__(192, 1) split_gemm_ares_kernel(SplitGemmArgs a
           break;
         }
         tc_fence_after();
-        epilogue_tile<NT>(a, tmem + ((uint32_t)(quarter * 32) << 16) + b * 2 * NT, cb, row_ok, nt * NT);
+        epilogue_tile<NT, 16>(a, tmem + ((uint32_t)(quarter * 32) << 16) + b * 2 * NT, cb, row_ok, nt * NT);
         tc_fence_before();
         mbar_arrive(&tempty[b]);
       }
@@ -1729,6 +1731,13 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
   A2.p = base + o_a2;
   if (rows_pad_k != 2 * nd) EPB_CUDA(cudaMemsetAsync(A2.p, 0, 2 * A2.plane_bytes, ctx->stream));
 
+  // side stream for the kR->kq GEMM (not while the per-family profile is recorded: it times each family
+  // on the main stream)
+  bool side = false;
+  if (!ctx->prof_on) {
+    EPB_TRY(side_stream(ctx));
+    side = true;
+  }
   for (int64_t ko = 0; ko < nk; ko += KO) {
     const int64_t nko = nk - ko < KO ? nk - ko : KO;
     const double* xko = xk + 3 * ko;
@@ -1759,12 +1768,31 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
       EPB_TRY(pack_a_herm_mod(ctx, m->ham, m->rs_el, (int)nw, xko + 3 * ki, nki, mm->H.rows_pad, Ah, base + o_ah));
       EPB_TRY(split_gemm(ctx, EPB_PROF_UMMA_H, Ah, Bq_el, mm->H.rows_pad / 128, nki, nw2, nq, true, C1, nw2 * nq,
                          nw2));
-      EPB_TRY(eigh_mixed_packed(ctx, C1, nw, np, U32, nullptr));
-      // kR->kq on the tensor cores, batched over the k of this inner batch
+      // kR->kq on the tensor cores, batched over the k of this inner batch. It needs neither the
+      // eigensolvers' results nor their resources (the FP32 Jacobi holds no shared memory), so outside the
+      // per-family profile it runs on the side stream beside them: it starts once the H(k+q) GEMM has
+      // finished (by then the previous batch's rotation, the last reader of C2, is done as well) and the
+      // rotation below waits for it.
       Planes A2i = A2;
       A2i.p = A2.p + ki * rows_pad_k / 128 * KC_ep * TILE_BYTES;
-      EPB_TRY(split_gemm_h(ctx, EPB_PROF_UMMA_KQ, A2i, Bp, rows_pad_k / 128, nki, 2 * nd, nq, false, C2,
-                           2 * nd * nq, 2 * nd, a2_unscale));
+      if (side) {
+        EPB_CUDA(cudaEventRecord(ctx->side_ev[0], ctx->stream));
+        EPB_CUDA(cudaStreamWaitEvent(ctx->side, ctx->side_ev[0], 0));
+        cudaStream_t main_stream = ctx->stream;
+        ctx->stream = ctx->side;
+        const int st = split_gemm_h(ctx, EPB_PROF_UMMA_KQ, A2i, Bp, rows_pad_k / 128, nki, 2 * nd, nq, false, C2,
+                                    2 * nd * nq, 2 * nd, a2_unscale);
+        ctx->stream = main_stream;
+        EPB_TRY(st);
+        EPB_CUDA(cudaEventRecord(ctx->side_ev[1], ctx->side));
+      }
+      EPB_TRY(eigh_mixed_packed(ctx, C1, nw, np, U32, nullptr));
+      if (side) {
+        EPB_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->side_ev[1], 0));
+      } else {
+        EPB_TRY(split_gemm_h(ctx, EPB_PROF_UMMA_KQ, A2i, Bp, rows_pad_k / 128, nki, 2 * nd, nq, false, C2,
+                             2 * nd * nq, 2 * nd, a2_unscale));
+      }
       // rotations, g2, in-place reduction
       if (!tiled) {
         static bool gattr = false;
