@@ -279,8 +279,8 @@ __global__ void pack_a_herm_mod_kernel(const double2* __restrict__ op, const int
 // xb[:, p % nb] with p = pidx[j] (pidx != null) or pair0 + j when xb != null (x_{k+q} for pairs of
 // a k list and a q list), else x_j = xa[:, j].
 // A thread writes 8 consecutive R of one point. The first is evaluated directly; an R that follows its
-// predecessor by (0, 0, 1) (the usual order of an R list) takes the previous value times exp(2 pi i x_3)
-// (at most 7 products: a few 1e-16), any other R is evaluated directly. The values are rounded to FP32
+// predecessor by (1, 0, 0) (R lists are sorted by reverse(R), so R1 varies fastest) takes the previous
+// value times exp(2 pi i x_1) (at most 7 products: a few 1e-16), any other R is evaluated directly. The values are rounded to FP32
 // and split in FP32 (exact: the planes hold the FP32 value), so the kernel stays on the HBM write bound.
 template <bool BF16, int NPL>
 __global__ void pack_b_phase_kernel(const int4* __restrict__ rv, int64_t K, const double* __restrict__ xa,
@@ -320,7 +320,7 @@ __global__ void pack_b_phase_kernel(const int4* __restrict__ rv, int64_t K, cons
         x1 = xa[3 * j + 1];
         x2 = xa[3 * j + 2];
       }
-      const double2 step = cis2pi(x2);
+      const double2 step = cis2pi(x0);
       double2 z = make_double2(1.0, 0.0);
       int4 rp = make_int4(0, 0, 0, 0);
 #pragma unroll
@@ -328,7 +328,7 @@ __global__ void pack_b_phase_kernel(const int4* __restrict__ rv, int64_t K, cons
         const int q = ch * 8 + e;
         if (q < K) {
           const int4 r = rv[q];
-          if (e > 0 && r.x == rp.x && r.y == rp.y && r.z == rp.z + 1)
+          if (e > 0 && r.x == rp.x + 1 && r.y == rp.y && r.z == rp.z)
             z = cmul(z, step);
           else
             z = cis2pi(rdotx(r.x, r.y, r.z, x0, x1, x2));
