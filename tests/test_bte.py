@@ -111,3 +111,33 @@ def test_gpu_serta_shards_add_up(gpu_lib, prec):
     np.testing.assert_allclose(np.concatenate([p[2] for p in parts]), it_all, rtol=1e-10,
                                atol=1e-14 * np.abs(it_all).max())
 
+
+@pytest.mark.gpu
+def test_gpu_serta_more_shards_than_kept_k(gpu_lib):
+    """More shards than kept k: the surplus shards have empty ranges (sigma 0, no pairs or states), the
+    shards still add up to the whole, and a rank outside 0 .. count - 1 is rejected."""
+    from epb200 import bte, pipeline
+
+    m = synth.make_model(8, 2, 2, 1, seed=64)
+    ng = 4
+    x, _ = BO.grid_points(ng)
+    E = O.eigvals_batched(np.asfortranarray(
+        O.fourier_batched(m.el_ham.op_r, 64, m.el_ham.irvec, x).reshape(8, 8, -1, order="F")))
+    ef = float(np.median(E[4]))
+    dm = pipeline.DeviceModel(m, mixed=False)
+    args = (dm, ng, ef - 0.05, ef + 0.05, ef, 0.08, 0.06)
+    s_all, st_all, it_all = bte.serta(*args, prec=0, want_inv_tau=True)
+    nk = st_all["kept_k"]
+    assert 0 < nk < 40
+    count = nk + 3
+    parts = [bte.serta(*args, prec=0, want_inv_tau=True, shard=(r, count)) for r in range(count)]
+    empty = [p for p in parts if p[1]["pairs"] == 0]
+    assert len(empty) >= 3
+    for p in empty:
+        assert p[1]["states"] == 0 and not np.any(p[0])
+    assert sum(p[1]["pairs"] for p in parts) == st_all["pairs"]
+    np.testing.assert_allclose(sum(p[0] for p in parts), s_all, rtol=1e-10, atol=1e-12 * np.abs(s_all).max())
+    np.testing.assert_allclose(np.concatenate([p[2] for p in parts]), it_all, rtol=1e-10,
+                               atol=1e-14 * np.abs(it_all).max())
+    with pytest.raises(Exception):
+        bte.serta(*args, prec=0, shard=(count, count))
