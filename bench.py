@@ -116,8 +116,8 @@ def config_dict(args, prec_name):
 # ---------------------------------------------------------------------------------------------
 def clocks_start():
     try:
-        f = open(os.path.join(ROOT, "gpurun_out", "bench_clocks.csv") if os.path.isdir(os.path.join(ROOT, "gpurun_out"))
-                 else os.devnull, "w")
+        # raw samples go to the file named by EPB_CLOCKS_CSV (if set); the JSON line carries the summary
+        f = open(os.environ.get("EPB_CLOCKS_CSV") or os.devnull, "w")
         p = subprocess.Popen(["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
                               "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
                               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"

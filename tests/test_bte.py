@@ -47,7 +47,7 @@ def test_gpu_serta_vs_oracle(gpu_lib, nw, natom, ng, method):
 @pytest.mark.gpu
 def test_gpu_serta_mixed_vs_fp64(gpu_lib):
     """Mixed mode (g(k, Rp) on the tensor cores): conductivity within 1e-4 of the FP64 path, the
-    tolerance the north star states for sigma."""
+    accuracy required of sigma."""
     from epb200 import bte, pipeline
 
     m = synth.make_model(8, 2, 2, 1, seed=61)
