@@ -390,7 +390,7 @@ int eigh_dispatch(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
     set_error("eigensolver: unknown precision mode %d", prec);
     return EPB_ERR_ARG;
   }
-  set_error("eigensolver: matrix order %d > 64 not supported by this build", nmax);
+  set_error("eigensolver: matrix order %d > 64 not supported here (orders up to 64 on this path)", nmax);
   return EPB_ERR_ARG;
 }
 
@@ -530,7 +530,7 @@ int eigh_run(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
       EPB_TRY(eigh_big_launch(ctx, a.A, nullptr, nullptr, n, a.batch, a.E, nullptr, a.want_v != 0, 0, prec, a.nonconv,
                               a.badsize));
     } else {
-      set_error("eigensolver: matrix order %d > 96 not supported by this build", n);
+      set_error("eigensolver: matrix order %d not supported (orders 1 to 96)", n);
       return EPB_ERR_ARG;
     }
     return eigh_check(ctx);
