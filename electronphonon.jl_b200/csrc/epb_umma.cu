@@ -105,7 +105,8 @@ __device__ __forceinline__ void store_split8(uint8_t* base, int64_t plane_bytes,
 }
 
 // The same split of FP32 values, in FP32 arithmetic: each remainder is exact in FP32, so the planes sum
-// to the FP32 value exactly and its rounding (2^-24 relative) is the only difference from the FP64 split.
+// to the FP32 value exactly (while the remainders stay normal, |v| >= 2^-100) and its rounding (2^-24
+// relative) is the only difference from the FP64 split.
 template <bool BF16>
 __device__ __forceinline__ uint16_t f32_to_half_bits(float v) {
   if (BF16) {
