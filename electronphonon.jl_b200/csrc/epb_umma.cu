@@ -814,6 +814,12 @@ __global__ void __launch_bounds__(192, 4) split_gemm_ares_kernel(SplitGemmArgs a
   if (warp == 0) tmem_dealloc(tmem, Cfg::TMEM_COLS);
 }
 
+// w = 1 / (2 omega) in FP32 (the |g|^2 weight of the rotation kernel), per q and mode, once per pass.
+__global__ void inv2w_kernel(const double* __restrict__ omega, float* __restrict__ w, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    w[i] = (float)(0.5 / omega[i]);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Host-side helpers.
 struct Planes {
@@ -1470,7 +1476,7 @@ struct RotSmem {
 template <int NW, int NM>
 __global__ void __launch_bounds__(256, 2) eph_rot_reduce_f32_kernel(
     const float* __restrict__ g, int64_t g_stride, const float2* __restrict__ ukq, const float2* __restrict__ uph,
-    const double* __restrict__ omega, int64_t nkb, int64_t nq, double* __restrict__ g2sum,
+    const float* __restrict__ inv2w, int64_t nkb, int64_t nq, double* __restrict__ g2sum,
     double* __restrict__ sample, int64_t stride, int64_t nsamp) {
   static_assert(NW == 16 && NM == 12, "thread tiling written for nw = 16, nm = 12");
   using L = RotSmem<NW, NM>;
@@ -1589,15 +1595,15 @@ __global__ void __launch_bounds__(256, 2) eph_rot_reduce_f32_kernel(
       }
       const bool samp = sample && ((uint32_t)q % (uint32_t)stride == 0);
       double* sq = samp ? sample + ((kl * nsamp) + (uint32_t)q / (uint32_t)stride) * (int64_t)NT : nullptr;
-      const double* om = omega + q * NM;
+      const float* w2 = inv2w + q * NM;  // 1 / (2 omega) of this q, FP32
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
         const int nu = 3 * ng + j;
-        const float inv2w = (float)(0.5 / om[nu]);
+        const float inv2w_nu = w2[nu];
         float s = 0.f;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-          const float v = (acc[i][j].x * acc[i][j].x + acc[i][j].y * acc[i][j].y) * inv2w;
+          const float v = (acc[i][j].x * acc[i][j].x + acc[i][j].y * acc[i][j].y) * inv2w_nu;
           s += v;
           if (samp) sq[mng + 64 * i + NB * NB * nu] = (double)v;
         }
@@ -1699,6 +1705,7 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
   const size_t o_c1 = carve(4 * nw2 * kbi * nq);
   const size_t o_u32 = carve(8 * nw2 * kbi * nq);
   const size_t o_c2 = carve(4 * 2 * nd * kbi * nq);
+  const size_t o_w2 = carve(4 * nm * nq);  // 1 / (2 omega), FP32
   void* ws = nullptr;
   EPB_TRY(ws_get(ctx, EPB_WS_PASS1, off + 1024, &ws));
   uint8_t* base = (uint8_t*)(((uintptr_t)ws + 1023) & ~uintptr_t(1023));
@@ -1723,6 +1730,9 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
   const double a2_scale = std::ldexp(1.0, e2);
   const float a2_unscale = (float)std::ldexp(1.0, -e2);
   c128_to_c64_kernel<<<grid_for(ctx, nm * nm * nq), 256, 0, ctx->stream>>>(uph, uph32, nm * nm * nq);
+  EPB_LAUNCH_CHECK();
+  float* inv2w = (float*)(base + o_w2);
+  inv2w_kernel<<<grid_for(ctx, nm * nq), 256, 0, ctx->stream>>>(omega, inv2w, nm * nq);
   EPB_LAUNCH_CHECK();
   Planes A2;
   A2.rows_pad = rows_pad_k * KO;
@@ -1819,7 +1829,7 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
         unsigned grid = (unsigned)(nblk < (int64_t)ctx->sm_count * 2 ? nblk : (int64_t)ctx->sm_count * 2);
         prof_begin(ctx, EPB_PROF_ROT);
         eph_rot_reduce_f32_kernel<16, 12><<<grid, 256, RS, ctx->stream>>>(
-            C2, 2 * nd, U32, uph32, omega, nki, nq, g2sum + nm * (ko + ki),
+            C2, 2 * nd, U32, uph32, inv2w, nki, nq, g2sum + nm * (ko + ki),
             g2_sample ? g2_sample + (ko + ki) * nsamp * nd : nullptr, sample_stride, nsamp);
         prof_end(ctx);
         EPB_LAUNCH_CHECK();
