@@ -251,4 +251,114 @@ function read_epmat_device(filename, nw, nmodes, nr_el, nr_ep, irvec_el, irvec_e
                   ElectronPhonon.WannierObject(irvec_ep, out; irvec_next = irvec_el)
 end
 
+
+# ---- whole e-ph pass (run_eph_over_k_and_q.jl:251-330, run the batched way) ---------------------
+"""
+    PassModel(model; mixed = true)
+
+Binds a model already moved to the device (`to_device`: `el_ham.op_r`, `ph_dyn.op_r` and `epmat.op_r`
+in the "el" layout as `CuMatrix{ComplexF64}`, `epmat.irvec_next` the Rp list) for `eph_pass` and
+`serta`. With `mixed`, also builds the split-BF16 operand planes of the tensor-core path (one-time
+cost, like `to_device`). The device operators stay owned by `model` and are kept alive here.
+"""
+mutable struct PassModel
+    h::Ptr{Cvoid}
+    nw::Int
+    nm::Int
+    ops::Tuple
+end
+function PassModel(model; mixed::Bool = true)
+    ham, dyn, ep = model.el_ham, model.ph_dyn, model.epmat
+    mass = model.mass isa CuArray ? model.mass : CuArray{Float64}(collect(model.mass))
+    nw = isqrt(size(ham.op_r, 1))
+    nm = isqrt(size(dyn.op_r, 1))
+    irel = collect(reinterpret(Int64, ham.irvec))
+    irph = collect(reinterpret(Int64, dyn.irvec))
+    irep = collect(reinterpret(Int64, ep.irvec_next))
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:epb_model_create, LIB[]), Cint,
+                (Ptr{Cvoid}, CuPtr{ComplexF64}, Int64, Ptr{Int64}, Int64, CuPtr{ComplexF64}, CuPtr{Float64}, Int64,
+                 Ptr{Int64}, Int64, CuPtr{ComplexF64}, Ptr{Int64}, Int64, Cint, Ptr{Ptr{Cvoid}}),
+                ctx().h, ham.op_r, nw, irel, length(ham.irvec), dyn.op_r, mass, nm, irph, length(dyn.irvec),
+                ep.op_r, irep, length(ep.irvec_next), Cint(mixed ? 1 : 0), r))
+    pm = PassModel(r[], nw, nm, (ham.op_r, dyn.op_r, mass, ep.op_r))
+    finalizer(x -> ccall((:epb_model_destroy, LIB[]), Cint, (Ptr{Cvoid},), x.h), pm)
+    pm
+end
+
+"""
+    eph_pass(pm, xks, xqs; prec = PREC[], k_batch = 0, sample_stride = 0)
+
+All-band e-ph pass over the k list x the q list: electrons at k and k+q, phonons at q,
+g2 = |u_kq' g u_ph|^2 / (2 omega). Returns device arrays `ek` (nw x nk), `omega` (nm x nq), `g2sum`
+(nm x nk, summed over bands and q) and, for `sample_stride > 0`, the full g2 blocks of every
+`sample_stride`-th q, (nw, nw, nm, nsamp, nk); `k_batch <= 0` lets the library time the batch sizes.
+"""
+function eph_pass(pm::PassModel, xks, xqs; prec::Integer = PREC[], k_batch::Integer = 0, sample_stride::Integer = 0)
+    xk = xk_device(xks)
+    xq = xk_device(xqs)
+    nk, nq = size(xk, 2), size(xq, 2)
+    ek = CuArray{Float64}(undef, pm.nw, nk)
+    om = CuArray{Float64}(undef, pm.nm, nq)
+    g2sum = CuArray{Float64}(undef, pm.nm, nk)  # zeroed by the library
+    samp = sample_stride > 0 ? CuArray{Float64}(undef, pm.nw, pm.nw, pm.nm, cld(nq, sample_stride), nk) : nothing
+    stats = zeros(Int64, 4)
+    check(ccall((:epb_eph_pass, LIB[]), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, CuPtr{Float64}, Int64, CuPtr{Float64}, Int64, Cint, Int64, Int64,
+                 CuPtr{Float64}, CuPtr{Float64}, CuPtr{Float64}, CuPtr{Float64}, Ptr{Int64}),
+                ctx().h, pm.h, xk, nk, xq, nq, Cint(prec), k_batch, max(sample_stride, 1), ek, om, g2sum,
+                samp === nothing ? CuPtr{Float64}(0) : samp, stats))
+    (ek = ek, omega = om, g2sum = g2sum, g2_sample = samp, n_elements = stats[1], k_batch = stats[2])
+end
+
+"Capture the pass as a CUDA graph on its second call with the same buffers and replay it afterwards."
+set_graph_mode(on::Bool) = check(ccall((:epb_set_graph_mode, LIB[]), Cint, (Ptr{Cvoid}, Cint), ctx().h, Cint(on)))
+
+# ---- SERTA consumer (run_eph_over_k_and_kq.jl:792-892, electron_lbte.jl:153-185) ----------------
+struct BteParams  # epb_bte_params, field for field (isbits: the C struct's layout)
+    ngrid::Int64
+    wmin::Float64
+    wmax::Float64
+    mu::Float64
+    temperature::Float64
+    smearing::Float64
+    omega_cutoff::Float64
+    spin_degeneracy::Float64
+    volume::Float64
+    lattice::NTuple{9,Float64}
+    method::Int32
+    prec::Int32
+    k_batch::Int64
+    pair_chunk::Int64
+    shard_rank::Int64
+    shard_count::Int64
+end
+
+"""
+    serta(pm, ngrid, wmin, wmax, mu, T, smearing; lattice, volume, spin = 2.0, method = 5,
+          omega_cutoff = ElectronPhonon.omega_acoustic, prec = PREC[], k_batch = 0, shard = (0, 1),
+          inv_tau = false)
+
+SERTA conductivity (3 x 3, host, in the reference's units) over commensurate ngrid^3 k = q grids.
+With `shard = (rank, count)` this call takes the rank's contiguous share of the kept k and returns
+that share's partial sigma: add the shards' sigmas over the ranks (`MPI.Allreduce!`, the reference's
+`mpi_comm_k` split). `inv_tau = true` also returns the out-scattering rates of the window states.
+"""
+function serta(pm::PassModel, ngrid::Integer, wmin, wmax, mu, T, smearing; lattice::AbstractMatrix, volume,
+               spin = 2.0, method::Integer = 5, omega_cutoff = ElectronPhonon.omega_acoustic,
+               prec::Integer = PREC[], k_batch::Integer = 0, shard = (0, 1), inv_tau::Bool = false)
+    p = Ref(BteParams(ngrid, wmin, wmax, mu, T, smearing, omega_cutoff, spin, volume,
+                      NTuple{9,Float64}(Float64.(vec(lattice))), Int32(method), Int32(prec), k_batch, 0,
+                      shard[1], shard[2]))
+    cap = inv_tau ? ngrid^3 * pm.nw : 0
+    it = inv_tau ? CuArray{Float64}(undef, cap) : nothing
+    sigma = zeros(Float64, 9)
+    stats = zeros(Int64, 4)
+    check(ccall((:epb_bte_serta, LIB[]), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, Ref{BteParams}, Ptr{Float64}, CuPtr{Float64}, Int64, Ptr{Int64}),
+                ctx().h, pm.h, p, sigma, it === nothing ? CuPtr{Float64}(0) : it, cap, stats))
+    sig = reshape(sigma, 3, 3)
+    inv_tau ? (sig, stats, it[1:stats[2]]) : (sig, stats)
+end
+
 end # module
