@@ -361,4 +361,122 @@ function serta(pm::PassModel, ngrid::Integer, wmin, wmax, mu, T, smearing; latti
     inv_tau ? (sig, stats, it[1:stats[2]]) : (sig, stats)
 end
 
+
+# ---- band energies and windows straight from H(R) (filter.jl:40-72, 109-133; electron_state.jl:118-150) --
+"Binds H(R) (`ham.op_r` a device matrix) for band-energy and window queries."
+mutable struct Bands
+    h::Ptr{Cvoid}
+    nw::Int
+    op::Any
+end
+function Bands(ham)
+    nw = isqrt(size(ham.op_r, 1))
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:epb_bands_create, LIB[]), Cint, (Ptr{Cvoid}, CuPtr{ComplexF64}, Int64, Ptr{Int64}, Int64,
+                Ptr{Ptr{Cvoid}}), ctx().h, ham.op_r, nw, collect(reinterpret(Int64, ham.irvec)), length(ham.irvec), r))
+    b = Bands(r[], nw, ham.op_r)
+    finalizer(x -> ccall((:epb_bands_destroy, LIB[]), Cint, (Ptr{Cvoid},), x.h), b)
+    b
+end
+
+"Ascending band energies (nw x nk) at the k list (get_el_eigen_valueonly_batched)."
+function band_eigvals(b::Bands, xks; prec::Integer = PREC[])
+    xk = xk_device(xks)
+    E = CuArray{Float64}(undef, b.nw, size(xk, 2))
+    check(ccall((:epb_bands_eigvals, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, CuPtr{Float64}, Int64, CuPtr{Float64},
+                Cint), ctx().h, b.h, xk, size(xk, 2), E, Cint(prec)))
+    E
+end
+
+"Energy of one band (1-based) at every point of the k list."
+function band_energy(b::Bands, xks, band::Integer; prec::Integer = PREC[])
+    xk = xk_device(xks)
+    E = CuArray{Float64}(undef, size(xk, 2))
+    check(ccall((:epb_bands_band_energy, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, CuPtr{Float64}, Int64, Int64,
+                CuPtr{Float64}, Cint), ctx().h, b.h, xk, size(xk, 2), band, E, Cint(prec)))
+    E
+end
+
+const WindowStats = NTuple{8,Int64}  # epb_window_stats: tested, culled, evaluated, rechecked, kept, audited,
+                                     # violations, fallback_chunks
+
+"""
+    bands_window(b, xks, wmin, wmax; prec, guard = 1e-3)
+
+`_filter_kpoints` from H(R) without downloading the energies: per point the 1-based band range
+(0 / 0 when empty) and the 0-based ascending list of kept points.
+"""
+function bands_window(b::Bands, xks, wmin, wmax; prec::Integer = PREC[], guard = 1e-3)
+    xk = xk_device(xks)
+    nk = size(xk, 2)
+    bmin = CuVector{Int32}(undef, nk)
+    bmax = CuVector{Int32}(undef, nk)
+    keep = CuVector{Int32}(undef, nk)
+    n = Ref{Int64}(0)
+    st = Ref{WindowStats}(ntuple(_ -> Int64(0), 8))
+    check(ccall((:epb_bands_window, LIB[]), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, CuPtr{Float64}, Int64, Float64, Float64, Cint, Float64, CuPtr{Int32},
+                 CuPtr{Int32}, CuPtr{Int32}, Ref{Int64}, Ref{WindowStats}),
+                ctx().h, b.h, xk, nk, wmin, wmax, Cint(prec), guard, bmin, bmax, keep, n, st))
+    (keep = keep[1:n[]], band_min = bmin, band_max = bmax, stats = st[])
+end
+
+"""
+    pair_window(b, xks, xqs, wmin, wmax; mlp = C_NULL, prec, guard = 1e-3, capacity)
+
+Kept (k, q) pairs (pair index ik * nq + iq, 0-based) with their band ranges at k + q; `mlp`, a
+calibrated surrogate handle, culls pairs before the plain evaluation.
+"""
+function pair_window(b::Bands, xks, xqs, wmin, wmax; mlp::Ptr{Cvoid} = C_NULL, prec::Integer = PREC[],
+                     guard = 1e-3, capacity::Integer)
+    xk = xk_device(xks)
+    xq = xk_device(xqs)
+    pairs = CuVector{Int64}(undef, capacity)
+    bmin = CuVector{Int32}(undef, capacity)
+    bmax = CuVector{Int32}(undef, capacity)
+    n = Ref{Int64}(0)
+    st = Ref{WindowStats}(ntuple(_ -> Int64(0), 8))
+    check(ccall((:epb_pair_window, LIB[]), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, CuPtr{Float64}, Int64, CuPtr{Float64}, Int64, Float64, Float64, Ptr{Cvoid},
+                 Cint, Float64, CuPtr{Int64}, CuPtr{Int32}, CuPtr{Int32}, Int64, Ref{Int64}, Ref{WindowStats}),
+                ctx().h, b.h, xk, size(xk, 2), xq, size(xq, 2), wmin, wmax, mlp, Cint(prec), guard, pairs, bmin, bmax,
+                capacity, n, st))
+    (pairs = pairs[1:n[]], band_min = bmin[1:n[]], band_max = bmax[1:n[]], stats = st[])
+end
+
+# ---- uneven eigensolve batches (eigen_batched over ragged inputs, ext:80-115) ---------------------
+"Eigen-decompose matrices of different orders packed in `A` (in place; orders 1..96)."
+function eigen_varlen!(A::CuVector{ComplexF64}, a_offset::CuVector{Int64}, n::CuVector{Int32}, E::CuVector{Float64},
+                       e_offset::CuVector{Int64}; jobz::Char = 'V', prec::Integer = PREC[])
+    check(ccall((:epb_eigh_varlen, LIB[]), Cint, (Ptr{Cvoid}, CuPtr{ComplexF64}, CuPtr{Int64}, CuPtr{Int32}, Int64,
+                CuPtr{Float64}, CuPtr{Int64}, Cchar, Cint), ctx().h, A, a_offset, n, length(n), E, e_offset,
+                Cchar(jobz), Cint(prec)))
+    A, E
+end
+
+# ---- q index of k+q on a commensurate grid (_fill_iqs!, run_eph_over_k_and_kq.jl:565-582) -----------
+function fill_iqs!(iqs::CuVector{Int64}, xkq_int::CuMatrix{Int64}, xk_int::AbstractVector{<:Integer}, ngrid,
+                   dense_hash_to_iq::CuVector{Int64})
+    check(ccall((:epb_fill_iqs, LIB[]), Cint, (Ptr{Cvoid}, CuPtr{Int64}, Int64, Ptr{Int64}, Int64, Int64, Int64,
+                CuPtr{Int64}, CuPtr{Int64}), ctx().h, xkq_int, size(xkq_int, 2), Int64.(collect(xk_int)),
+                ngrid[1], ngrid[2], ngrid[3], dense_hash_to_iq, iqs))
+    iqs
+end
+
+# ---- window filter without library allocations (for callers whose memory pool owns the device) ----
+"""
+    window_filter_noalloc(E, wmin, wmax, band_min, band_max, keep, nkeep)
+
+The window filter on caller-owned buffers (`nkeep` a one-element device vector), using the library's
+fixed static scratch (nk <= 16,777,216); calls that overlap on one device race.
+"""
+function window_filter_noalloc(E::CuMatrix{Float64}, wmin, wmax, band_min::CuVector{Int32}, band_max::CuVector{Int32},
+                               keep::CuVector{Int32}, nkeep::CuVector{Int64})
+    nw, nk = size(E)
+    check(ccall((:epb_window_filter_noalloc, LIB[]), Cint, (Ptr{Cvoid}, CuPtr{Float64}, Int64, Int64, Float64,
+                Float64, CuPtr{Int32}, CuPtr{Int32}, CuPtr{Int32}, CuPtr{Int64}, CuPtr{Float64}),
+                CUDA.stream().handle, E, nw, nk, wmin, wmax, band_min, band_max, keep, nkeep, CuPtr{Float64}(0)))
+    nkeep
+end
+
 end # module

@@ -112,7 +112,7 @@ EPB_API int epb_fourier(epb_ctx* ctx, const double* op_r, int64_t ld_op, int64_t
 EPB_API int epb_eigh_batched(epb_ctx* ctx, double* A, int64_t n, int64_t batch, double* E, char jobz,
                      int prec);
 
-/* Uneven batch: matrix b has order n[b] (1..128) and starts at complex element a_offset[b] of A;
+/* Uneven batch: matrix b has order n[b] (1..96) and starts at complex element a_offset[b] of A;
    its eigenvalues go to E + e_offset[b]. All index arrays are device arrays. Same semantics. */
 EPB_API int epb_eigh_varlen(epb_ctx* ctx, double* A, const int64_t* a_offset, const int32_t* n,
                     int64_t batch, double* E, const int64_t* e_offset, char jobz, int prec);
