@@ -479,4 +479,76 @@ function window_filter_noalloc(E::CuMatrix{Float64}, wmin, wmax, band_min::CuVec
     nkeep
 end
 
+
+# ---- TiledDeviceOutput (calculator/tiled_device_output.jl) ------------------------------------------
+struct TiledInfo  # epb_tiled_info, field for field
+    allocated::Int32
+    block::Int32
+    ni_cap::Int64
+    tile_offset::Int64
+    tile_length::Int64
+    tile_stride::Int64
+end
+
+"""
+    TiledOutput(dims, i_axis, narr, T, iks, nk, n_batch_max; force_block = -1, headroom = 1.2)
+
+`narr` arrays of element type `T` (4, 8 or 16 bytes) and shape `dims`, axis `i_axis` (1-based) running
+over the outer states whose 1-based k indices are `iks`; resident whole, or one outer-k tile at a time
+when the full output does not fit (`force_block`: -1 decide from free memory, 0 whole, 1 tiled).
+"""
+mutable struct TiledOutput
+    h::Ptr{Cvoid}
+    T::DataType
+end
+function TiledOutput(dims, i_axis::Integer, narr::Integer, T::DataType, iks::AbstractVector{<:Integer}, nk::Integer,
+                     n_batch_max::Integer; force_block::Integer = -1, headroom = 1.2)
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    d = Int64.(collect(dims))
+    check(ccall((:epb_tiled_create, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Int64}, Cint, Cint, Cint, Int64, Cint, Float64,
+                Ptr{Int64}, Int64, Int64, Int64, Ptr{Ptr{Cvoid}}), ctx().h, d, Cint(length(d)), Cint(i_axis - 1),
+                Cint(narr), Int64(sizeof(T)), Cint(force_block), headroom, Int64.(collect(iks)), length(iks), nk,
+                n_batch_max, r))
+    t = TiledOutput(r[], T)
+    finalizer(x -> ccall((:epb_tiled_destroy, LIB[]), Cint, (Ptr{Cvoid},), x.h), t)
+    t
+end
+"tile_begin! for the 1-based k batch kstart:kend (allocates on first use; zeroes the tile in block mode)."
+tile_begin!(t::TiledOutput, kstart::Integer, kend::Integer) =
+    check(ccall((:epb_tiled_begin, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Int64), ctx().h, t.h, kstart, kend))
+function tile_info(t::TiledOutput)
+    info = Ref{TiledInfo}(TiledInfo(0, 0, 0, 0, 0, 0))
+    check(ccall((:epb_tiled_get_info, LIB[]), Cint, (Ptr{Cvoid}, Ref{TiledInfo}), t.h, info))
+    info[]
+end
+"Device pointer of array k (1-based) for the scatter kernels (tile_offset / tile_stride apply)."
+function device_pointer(t::TiledOutput, k::Integer)
+    p = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:epb_tiled_device_array, LIB[]), Cint, (Ptr{Cvoid}, Cint, Ptr{Ptr{Cvoid}}), t.h, Cint(k - 1), p))
+    CuPtr{t.T}(UInt(p[]))
+end
+"tile_download!: array k (1-based) of the current tile (block mode) or the whole array into `host`."
+function tile_download!(host::Array, t::TiledOutput, k::Integer)
+    check(ccall((:epb_tiled_download, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Cint, Ptr{Cvoid}), ctx().h, t.h,
+                Cint(k - 1), host))
+    host
+end
+tile_free!(t::TiledOutput) = check(ccall((:epb_tiled_free, LIB[]), Cint, (Ptr{Cvoid},), t.h))
+
+"residency_use_block: would the full output (bytes, times headroom) not fit the free device memory?"
+function residency_use_block(full_bytes::Integer, headroom = 1.2)
+    b = Ref{Cint}(0)
+    check(ccall((:epb_residency_use_block, LIB[]), Cint, (Ptr{Cvoid}, Int64, Float64, Ref{Cint}), ctx().h,
+                full_bytes, headroom, b))
+    b[] != 0
+end
+"ind_range_for_k_range: the 1-based (first, last) states of k range kstart:kend ((1, 0) when empty)."
+function ind_range_for_k_range(iks::AbstractVector{<:Integer}, nk::Integer, kstart::Integer, kend::Integer)
+    f = Ref{Int64}(0)
+    l = Ref{Int64}(0)
+    check(ccall((:epb_ind_range_for_k_range, LIB[]), Cint, (Ptr{Int64}, Int64, Int64, Int64, Int64, Ref{Int64},
+                Ref{Int64}), Int64.(collect(iks)), length(iks), nk, kstart, kend, f, l))
+    f[]:l[]
+end
+
 end # module
