@@ -551,4 +551,104 @@ function ind_range_for_k_range(iks::AbstractVector{<:Integer}, nk::Integer, ksta
     f[]:l[]
 end
 
+
+# ---- outer-q loop with EPDataKBatched calculators (run_eph_over_q_and_k.jl:428-613) -------------------
+struct OuterQParams  # epb_outer_q_params
+    wmin_k::Float64
+    wmax_k::Float64
+    wmin_kq::Float64
+    wmax_kq::Float64
+    k_batch::Int64
+    q_chunk::Int64
+    prec::Cint
+    phonon_basis::Cint
+end
+struct KBatchPayload  # epb_kbatch_payload: device pointers valid during run_batch, ordered on `stream`
+    iq::Int64
+    k0::Int64
+    nk::Int64
+    nw::Int64
+    nm::Int64
+    eps::Ptr{ComplexF64}
+    ek::Ptr{Float64}
+    ekq::Ptr{Float64}
+    uk::Ptr{ComplexF64}
+    ukq::Ptr{ComplexF64}
+    wtk::Ptr{Float64}
+    xk::Ptr{Float64}
+    ik::Ptr{Int32}
+    omega::Ptr{Float64}
+    stream::Ptr{Cvoid}
+end
+struct OuterQCalc  # epb_outer_q_calc
+    begin_q::Ptr{Cvoid}
+    run_batch::Ptr{Cvoid}
+    end_q::Ptr{Cvoid}
+    user::Ptr{Cvoid}
+end
+
+# The hooks a calculator (a mutable object) implements: the OuterIteration brackets and
+# run_calculator!(::EPDataKBatched); the payload's device pointers become CuArrays with
+# unsafe_wrap(CuArray, CuPtr{T}(UInt(ptr)), dims) for the duration of the call.
+outer_q_begin!(calc, iq) = nothing
+outer_q_end!(calc, iq) = nothing
+function outer_q_run_batch! end
+
+function _oq_begin(user::Ptr{Cvoid}, iq::Int64, stream::Ptr{Cvoid})::Cint
+    try
+        outer_q_begin!(unsafe_pointer_to_objref(user), iq + 1)
+        return Cint(0)
+    catch
+        return Cint(1)
+    end
+end
+function _oq_run(user::Ptr{Cvoid}, p::Ptr{KBatchPayload})::Cint
+    try
+        outer_q_run_batch!(unsafe_pointer_to_objref(user), unsafe_load(p))
+        return Cint(0)
+    catch
+        return Cint(1)  # the library stops the loop and returns EPB_ERR_ARG
+    end
+end
+function _oq_end(user::Ptr{Cvoid}, iq::Int64, stream::Ptr{Cvoid})::Cint
+    try
+        outer_q_end!(unsafe_pointer_to_objref(user), iq + 1)
+        return Cint(0)
+    catch
+        return Cint(1)
+    end
+end
+
+"""
+    eph_outer_q(pm, xks, xqs, calcs; window_k, window_kq, wtk = nothing, prec = PREC[], k_batch = 0,
+                q_chunk = 0, phonon_basis = 0)
+
+The outer-q batched loop: per q, g(Re, q) and the phonon modes, then per batch of kept k the k+q states
+and ep = ukq' g(k, q) uk, handed to each calculator's `outer_q_run_batch!`. Returns the gauge-invariant
+record A[iq] = sum_k wtk sum |ep|^2 and the stats (kept k, k batch, q chunk, batches).
+"""
+function eph_outer_q(pm::PassModel, xks, xqs, calcs::AbstractVector; window_k, window_kq, wtk = nothing,
+                     prec::Integer = PREC[], k_batch::Integer = 0, q_chunk::Integer = 0, phonon_basis::Integer = 0)
+    xk = collect(reinterpret(reshape, Float64, collect(Vec3{Float64}, xks)))  # host 3 x nk
+    xq = collect(reinterpret(reshape, Float64, collect(Vec3{Float64}, xqs)))
+    nk, nq = size(xk, 2), size(xq, 2)
+    w = wtk === nothing ? nothing : Float64.(collect(wtk))
+    params = Ref(OuterQParams(window_k[1], window_k[2], window_kq[1], window_kq[2], k_batch, q_chunk, Cint(prec),
+                              Cint(phonon_basis)))
+    fb = @cfunction(_oq_begin, Cint, (Ptr{Cvoid}, Int64, Ptr{Cvoid}))
+    fr = @cfunction(_oq_run, Cint, (Ptr{Cvoid}, Ptr{KBatchPayload}))
+    fe = @cfunction(_oq_end, Cint, (Ptr{Cvoid}, Int64, Ptr{Cvoid}))
+    A = zeros(Float64, nq)
+    stats = zeros(Int64, 4)
+    GC.@preserve calcs begin
+        cs = [OuterQCalc(fb, fr, fe, pointer_from_objref(c)) for c in calcs]
+        check(ccall((:epb_eph_outer_q, LIB[]), Cint,
+                    (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int64, Ptr{Float64}, Int64, Ref{OuterQParams},
+                     Ptr{OuterQCalc}, Cint, Ptr{Float64}, Ptr{Int64}),
+                    ctx().h, pm.h, xk, w === nothing ? Ptr{Float64}(C_NULL) : w, nk, xq, nq, params, cs,
+                    Cint(length(cs)), A, stats))
+    end
+    A, stats
+end
+
 end # module
