@@ -83,3 +83,69 @@ def test_every_ccall_matches_its_prototype():
         assert len(types) == len(params), f"{name}: {len(types)} argument types, header has {len(params)}"
         for k, (t, p) in enumerate(zip(types, params)):
             assert jl_kind(t) == c_kind(p), f"{name} argument {k + 1}: Julia {t} vs C {p}"
+
+
+JL_SIZE = {"Int64": 8, "UInt64": 8, "Float64": 8, "Cint": 4, "Int32": 4, "Cdouble": 8}
+
+
+def jl_size_align(t):
+    t = t.strip()
+    if t in JL_SIZE:
+        return JL_SIZE[t], JL_SIZE[t]
+    if t.startswith("Ptr{") or t.startswith("CuPtr{"):
+        return 8, 8
+    m = re.fullmatch(r"NTuple\{(\d+),\s*(\w+)\}", t)
+    if m:
+        sz, al = jl_size_align(m.group(2))
+        return int(m.group(1)) * sz, al
+    raise AssertionError(f"no C layout known for Julia type {t}")
+
+
+def jl_structs():
+    """{C struct name: [(field, offset), ..., ('size', n)]} of the `struct X  # epb_name` mirrors."""
+    txt = open(JL).read()
+    out = {}
+    for m in re.finditer(r"^struct (\w+)\s*#\s*(epb_\w+)[^\n]*\n(.*?)^end", txt, flags=re.S | re.M):
+        off, align, fields = 0, 1, []
+        for line in m.group(3).splitlines():
+            f = re.match(r"\s*(\w+)::(.+?)\s*$", line)
+            if not f:
+                continue
+            sz, al = jl_size_align(f.group(2))
+            off = (off + al - 1) // al * al
+            fields.append((f.group(1), off))
+            off += sz
+            align = max(align, al)
+        fields.append(("size", (off + align - 1) // align * align))
+        out[m.group(2)] = fields
+    return out
+
+
+def test_julia_struct_mirrors_match_the_header(tmp_path):
+    import shutil
+    import subprocess
+
+    import pytest
+
+    if shutil.which("gcc") is None:
+        pytest.skip("needs gcc")
+    structs = jl_structs()
+    assert {"epb_bte_params", "epb_tiled_info", "epb_outer_q_params", "epb_kbatch_payload",
+            "epb_outer_q_calc"} <= set(structs)
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "epb200.h"', 'int main(void) {']
+    for cname, fields in structs.items():
+        for f, _ in fields:
+            expr = f"sizeof({cname})" if f == "size" else f"offsetof({cname}, {f})"
+            lines.append(f'  printf("{cname} {f} %zu\\n", {expr});')
+    lines += ['  return 0;', '}']
+    src = tmp_path / "probe.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        c, f, v = line.split()
+        got[(c, f)] = int(v)
+    for cname, fields in structs.items():
+        for f, off in fields:
+            assert got[(cname, f)] == off, (cname, f, off, got[(cname, f)])
