@@ -651,4 +651,67 @@ function eph_outer_q(pm::PassModel, xks, xqs, calcs::AbstractVector; window_k, w
     A, stats
 end
 
+
+# ---- learned band-energy surrogate for the pair window (no counterpart in the reference) ------------
+struct MlpTrainOpts  # epb_mlp_train_opts
+    epochs::Int64
+    batch::Int64
+    lr::Float64
+    lr_final::Float64
+    seed::UInt64
+    use_graph::Int32
+    reserved::Int32
+end
+
+"""
+    Surrogate(fvecs, nout; hidden = 256, nhidden = 3, seed = 1)
+
+MLP on the Fourier features [cos 2 pi f.k, sin 2 pi f.k] of the integer vectors `fvecs` (e.g. the H(R)
+lattice vectors), predicting `nout` band energies. Train it with `train!`, calibrate its culling margins
+on held-out points with `calibrate!`, then pass `s.h` as `mlp` to `pair_window`.
+"""
+mutable struct Surrogate
+    h::Ptr{Cvoid}
+    nout::Int
+end
+function Surrogate(fvecs::Vector{Vec3{Int}}, nout::Integer; hidden::Integer = 256, nhidden::Integer = 3,
+                   seed::Integer = 1)
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    f = Int32.(collect(reinterpret(Int64, fvecs)))
+    check(ccall((:epb_mlp_create, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Int32}, Int64, Int64, Int64, Int64, UInt64,
+                Ptr{Ptr{Cvoid}}), ctx().h, f, length(fvecs), hidden, nhidden, nout, UInt64(seed), r))
+    m = Surrogate(r[], nout)
+    finalizer(x -> ccall((:epb_mlp_destroy, LIB[]), Cint, (Ptr{Cvoid},), x.h), m)
+    m
+end
+
+"Adam training on points `xks` with band energies `E` (nout x n, device); returns the loss of each epoch."
+function train!(m::Surrogate, xks, E::CuMatrix{Float64}; epochs::Integer = 200, batch::Integer = 2048,
+                lr = 2e-3, lr_final = 2e-5, seed::Integer = 1, use_graph::Bool = true)
+    x = xk_device(xks)
+    opts = Ref(MlpTrainOpts(epochs, batch, lr, lr_final, UInt64(seed), Int32(use_graph), Int32(0)))
+    loss = zeros(Float64, epochs)
+    check(ccall((:epb_mlp_train, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, Int64,
+                Ref{MlpTrainOpts}, Ptr{Float64}), ctx().h, m.h, x, E, size(x, 2), opts, loss))
+    loss
+end
+
+"Culling margins from held-out points: safety x the largest prediction error of each band."
+function calibrate!(m::Surrogate, xks, E::CuMatrix{Float64}; safety = 1.5)
+    x = xk_device(xks)
+    margins = zeros(Float64, m.nout)
+    check(ccall((:epb_mlp_calibrate, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, Int64,
+                Float64, Ptr{Float64}), ctx().h, m.h, x, E, size(x, 2), safety, margins))
+    margins
+end
+
+"Predicted band energies (nout x n) at the points `xks`."
+function predict(m::Surrogate, xks)
+    x = xk_device(xks)
+    E = CuArray{Float64}(undef, m.nout, size(x, 2))
+    check(ccall((:epb_mlp_predict, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, CuPtr{Float64}, Int64, CuPtr{Float64}),
+                ctx().h, m.h, x, size(x, 2), E))
+    E
+end
+
 end # module
