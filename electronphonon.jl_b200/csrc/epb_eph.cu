@@ -8,6 +8,8 @@
 //    T = ukq^dagger g (contract iw) and ep = T uph (contract jm), folding g2 = |ep|^2/(2 omega)
 //    into the same pass. No size gate: the reference switches to two cuBLAS strided-batched
 //    GEMMs above nw*nm = 24 (wannier_to_bloch_batched.jl:406); this kernel covers all sizes.
+#include <algorithm>
+
 #include "epb_common.cuh"
 
 namespace epb {
@@ -88,6 +90,88 @@ int zgemm_nn(epb_ctx* ctx, const double2* A, int64_t lda, const double2* B, int6
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Strided-batched FP64 complex GEMM C_b = op(A_b) op(B_b) (alpha = 1, beta = 0) with op in {N, T, C}
+// (0, 1, 2), the operation of batched_gemm! (src/common/gpu_utils.jl:71-78): 32 x 32 output tiles,
+// 16-deep K steps staged in shared memory with each operand read along its contiguous axis, 2 x 2
+// outputs per thread, grid.z strides over the batch.
+constexpr int BG_BM = 32, BG_BN = 32, BG_BK = 16, BG_THREADS = 256;
+
+template <int OPA, int OPB>
+__global__ void __launch_bounds__(BG_THREADS) zgemm_batched_kernel(
+    const double2* __restrict__ A, int64_t lda, int64_t sa, const double2* __restrict__ B, int64_t ldb, int64_t sb,
+    double2* __restrict__ C, int64_t ldc, int64_t sc, int64_t M, int64_t N, int64_t K, int64_t batch) {
+  __shared__ double2 As[BG_BK][BG_BM + 1];
+  __shared__ double2 Bs[BG_BK][BG_BN + 1];
+  const int tid = threadIdx.x;
+  const int ty = tid >> 4, tx = tid & 15;  // rows 2 ty, 2 ty + 1; columns 2 tx, 2 tx + 1
+  const int64_t m0 = (int64_t)blockIdx.y * BG_BM, n0 = (int64_t)blockIdx.x * BG_BN;
+  for (int64_t b = blockIdx.z; b < batch; b += gridDim.z) {
+    const double2* Ab = A + b * sa;
+    const double2* Bb = B + b * sb;
+    double2 acc[2][2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) acc[i][j] = make_double2(0.0, 0.0);
+    for (int64_t k0 = 0; k0 < K; k0 += BG_BK) {
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int e = tid + t * BG_THREADS;
+        // A tile (m, k): read along m for 'N', along k for 'T' / 'C'
+        const int am = OPA == 0 ? e % BG_BM : e / BG_BK, ak = OPA == 0 ? e / BG_BM : e % BG_BK;
+        const int64_t row = m0 + am, kk = k0 + ak;
+        double2 av = make_double2(0.0, 0.0);
+        if (row < M && kk < K) {
+          av = OPA == 0 ? Ab[row + kk * lda] : Ab[kk + row * lda];
+          if (OPA == 2) av.y = -av.y;
+        }
+        As[ak][am] = av;
+        // B tile (k, n): read along k for 'N', along n for 'T' / 'C'
+        const int bk = OPB == 0 ? e % BG_BK : e / BG_BN, bn = OPB == 0 ? e / BG_BK : e % BG_BN;
+        const int64_t col = n0 + bn, kb = k0 + bk;
+        double2 bv = make_double2(0.0, 0.0);
+        if (col < N && kb < K) {
+          bv = OPB == 0 ? Bb[kb + col * ldb] : Bb[col + kb * ldb];
+          if (OPB == 2) bv.y = -bv.y;
+        }
+        Bs[bk][bn] = bv;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int kk = 0; kk < BG_BK; ++kk) {
+        const double2 a0 = As[kk][2 * ty], a1 = As[kk][2 * ty + 1];
+        const double2 b0 = Bs[kk][2 * tx], b1 = Bs[kk][2 * tx + 1];
+        cfma(acc[0][0], a0, b0);
+        cfma(acc[0][1], a0, b1);
+        cfma(acc[1][0], a1, b0);
+        cfma(acc[1][1], a1, b1);
+      }
+      __syncthreads();
+    }
+    double2* Cb = C + b * sc;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int64_t row = m0 + 2 * ty + i, col = n0 + 2 * tx + j;
+        if (row < M && col < N) Cb[row + col * ldc] = acc[i][j];
+      }
+  }
+}
+
+template <int OPA>
+static void launch_zgemm_batched(int opb, dim3 grid, cudaStream_t s, const double2* A, int64_t lda, int64_t sa,
+                                 const double2* B, int64_t ldb, int64_t sb, double2* C, int64_t ldc, int64_t sc,
+                                 int64_t M, int64_t N, int64_t K, int64_t batch) {
+  if (opb == 0)
+    zgemm_batched_kernel<OPA, 0><<<grid, BG_THREADS, 0, s>>>(A, lda, sa, B, ldb, sb, C, ldc, sc, M, N, K, batch);
+  else if (opb == 1)
+    zgemm_batched_kernel<OPA, 1><<<grid, BG_THREADS, 0, s>>>(A, lda, sa, B, ldb, sb, C, ldc, sc, M, N, K, batch);
+  else
+    zgemm_batched_kernel<OPA, 2><<<grid, BG_THREADS, 0, s>>>(A, lda, sa, B, ldb, sb, C, ldc, sc, M, N, K, batch);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -205,6 +289,40 @@ int eph_rotations_c64(epb_ctx* ctx, const float2* g, int64_t ldg, int nw, int nb
 using namespace epb;
 
 extern "C" {
+
+static int op_code(char t) { return t == 'N' || t == 'n' ? 0 : t == 'T' || t == 't' ? 1 : t == 'C' || t == 'c' ? 2 : -1; }
+
+int epb_batched_zgemm(epb_ctx* ctx, char transA, char transB, int64_t m, int64_t n, int64_t k, const double* A,
+                      int64_t lda, int64_t strideA, const double* B, int64_t ldb, int64_t strideB, double* C,
+                      int64_t ldc, int64_t strideC, int64_t batch) {
+  clear_error();
+  EPB_CHECK_ARG(ctx, "epb_batched_zgemm: NULL ctx");
+  const int oa = op_code(transA), ob = op_code(transB);
+  EPB_CHECK_ARG(oa >= 0 && ob >= 0, "epb_batched_zgemm: trans must be 'N', 'T' or 'C'");
+  EPB_CHECK_ARG(m >= 0 && n >= 0 && k >= 0 && batch >= 0, "epb_batched_zgemm: negative size");
+  if (m == 0 || n == 0 || batch == 0) return EPB_OK;
+  EPB_CHECK_ARG(C && (k == 0 || (A && B)), "epb_batched_zgemm: NULL buffer");
+  EPB_CHECK_ARG(lda >= std::max<int64_t>(1, oa == 0 ? m : k) && ldb >= std::max<int64_t>(1, ob == 0 ? k : n) &&
+                    ldc >= m,
+                "epb_batched_zgemm: leading dimension too small (lda=%lld ldb=%lld ldc=%lld)", (long long)lda,
+                (long long)ldb, (long long)ldc);
+  EPB_CHECK_ARG(cdiv(m, BG_BM) <= 65535, "epb_batched_zgemm: m=%lld too large", (long long)m);
+  EPB_TRY(make_current(ctx));
+  dim3 grid((unsigned)cdiv(n, BG_BN), (unsigned)cdiv(m, BG_BM),
+            (unsigned)std::min<int64_t>(batch, 65535));
+  const double2 *a = (const double2*)A, *b = (const double2*)B;
+  double2* c = (double2*)C;
+  prof_begin(ctx, EPB_PROF_ZGEMM);
+  if (oa == 0)
+    launch_zgemm_batched<0>(ob, grid, ctx->stream, a, lda, strideA, b, ldb, strideB, c, ldc, strideC, m, n, k, batch);
+  else if (oa == 1)
+    launch_zgemm_batched<1>(ob, grid, ctx->stream, a, lda, strideA, b, ldb, strideB, c, ldc, strideC, m, n, k, batch);
+  else
+    launch_zgemm_batched<2>(ob, grid, ctx->stream, a, lda, strideA, b, ldb, strideB, c, ldc, strideC, m, n, k, batch);
+  prof_end(ctx);
+  EPB_LAUNCH_CHECK();
+  return EPB_OK;
+}
 
 int epb_eph_RR_to_kR(epb_ctx* ctx, const double* epmat, int64_t nw, int64_t nm, int64_t nr_ep,
                      const epb_rset* rset_el, const double* xk, int64_t nk, const double* uk,

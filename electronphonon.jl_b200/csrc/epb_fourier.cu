@@ -7,6 +7,8 @@
 // tables exp(2 pi i m x_{d,j}) for m in [lo_d, hi_d] of each axis once, and forms every phase
 // element of a K-tile as the product of three table entries while staging it into shared memory.
 // The GEMM itself is a register-tiled FP64 complex GEMM (4 DFMA per complex MAC).
+#include <algorithm>
+
 #include "epb_common.cuh"
 
 namespace epb {
@@ -21,6 +23,20 @@ __global__ void phase_kernel(const int4* __restrict__ rv, int64_t nr, const doub
   int64_t ir = idx % nr, j = idx / nr;
   int4 r = rv[ir];
   phase[idx] = cis2pi(rdotx(r.x, r.y, r.z, xk[3 * j], xk[3 * j + 1], xk[3 * j + 2]));
+}
+
+// The same phase from the reference's own operands: R as an FP64 (nr x 3) column-major device matrix
+// (leading dimension ldr) and x as (3 x nk) with column stride ldx, the output with column stride ldp.
+__global__ void phase_mat_kernel(const double* __restrict__ rm, int64_t ldr, int64_t nr, const double* __restrict__ x,
+                                 int64_t ldx, int64_t nk, double2* __restrict__ phase, int64_t ldp) {
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < nr * nk;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t ir = idx % nr, j = idx / nr;
+    const double* xj = x + j * ldx;
+    const double t = __dadd_rn(__dadd_rn(__dmul_rn(rm[ir], xj[0]), __dmul_rn(rm[ir + ldr], xj[1])),
+                               __dmul_rn(rm[ir + 2 * ldr], xj[2]));
+    phase[ir + j * ldp] = cis2pi(t);
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -205,6 +221,22 @@ int fourier_mixed(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, const 
 using namespace epb;
 
 extern "C" {
+
+int epb_fourier_phase_mat(epb_ctx* ctx, const double* irvec_mat, int64_t ld_r, int64_t nr, const double* xkmat,
+                          int64_t ld_x, int64_t nk, double* phase, int64_t ld_p) {
+  clear_error();
+  EPB_CHECK_ARG(ctx, "epb_fourier_phase_mat: NULL ctx");
+  EPB_CHECK_ARG(nr >= 0 && nk >= 0, "epb_fourier_phase_mat: negative size");
+  EPB_CHECK_ARG(nr == 0 || nk == 0 || (irvec_mat && xkmat && phase), "epb_fourier_phase_mat: NULL buffer");
+  EPB_CHECK_ARG(ld_r >= nr && ld_x >= 3 && ld_p >= nr, "epb_fourier_phase_mat: leading dimension too small");
+  EPB_TRY(make_current(ctx));
+  if (nr == 0 || nk == 0) return EPB_OK;
+  const int64_t total = nr * nk;
+  const unsigned grid = (unsigned)std::min<int64_t>(cdiv(total, 256), (int64_t)ctx->sm_count * 16);
+  phase_mat_kernel<<<grid, 256, 0, ctx->stream>>>(irvec_mat, ld_r, nr, xkmat, ld_x, nk, (double2*)phase, ld_p);
+  EPB_LAUNCH_CHECK();
+  return EPB_OK;
+}
 
 int epb_fourier_phase(epb_ctx* ctx, const epb_rset* rset, const double* xk, int64_t nk,
                       double* phase) {

@@ -17,7 +17,10 @@
 //    one stream are ordered and safe. Each call rewrites every count it later reads, so nothing
 //    needs clearing between calls;
 //  * the first call on a device resolves the array's device address (cudaGetSymbolAddress) with
-//    that device current; make that first call before any stream capture on the device.
+//    that device current; make that first call before any stream capture on the device;
+//  * that address is kept for the life of the process: after a cudaDeviceReset of a device (CUDA.jl
+//    `device_reset!`), which unloads this module's device memory, do not call this entry point on that
+//    device again in the same process.
 #include <cuda_runtime.h>
 
 #include <mutex>

@@ -47,6 +47,8 @@ SIGNATURES = {
     "epb_rset_create": [P, P, I64, C.POINTER(P)],
     "epb_rset_destroy": [P],
     "epb_fourier_phase": [P, P, P, I64, P],
+    "epb_fourier_phase_mat": [P, P, I64, I64, P, I64, I64, P, I64],
+    "epb_batched_zgemm": [P, C.c_char, C.c_char, I64, I64, I64, P, I64, I64, P, I64, I64, P, I64, I64, I64],
     "epb_fourier": [P, P, I64, I64, P, P, I64, P, I32],
     "epb_eigh_batched": [P, P, I64, I64, P, C.c_char, I32],
     "epb_eigh_varlen": [P, P, P, P, I64, P, P, C.c_char, I32],

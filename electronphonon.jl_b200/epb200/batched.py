@@ -95,6 +95,43 @@ def fourier_phase(itp_or_irvec, xks):
     return out
 
 
+def _colstride(t):
+    """Column stride (in elements) of a Julia-layout device matrix view; its first axis is contiguous."""
+    assert t.stride(-1) == 1, "the first (Julia) axis must be contiguous"
+    return t.stride(-2) if t.dim() >= 2 else t.shape[-1]
+
+
+def fourier_phase_mat(phase, irvec_mat, xkmat):
+    """fourier_phase!(phase, irvec_mat, xkmat) with the reference's own operands
+    (batched_fourier_core.jl:24-30): irvec_mat the (nr, 3) f64 device matrix of
+    _irvec_to_device_matrix (WannierObject.jl:148-152), xkmat (3, nk) f64, phase (nr, nk) c128; column
+    views (e.g. P_mk[:, 1:nk]) keep their parent's column stride."""
+    nr, three = _jlshape(irvec_mat)
+    assert three == 3 and _jlshape(xkmat)[0] == 3
+    nk = _jlshape(xkmat)[1]
+    assert _jlshape(phase) == (nr, nk)
+    check(_lib.lib().epb_fourier_phase_mat(_ctx().h, ptr(irvec_mat), _colstride(irvec_mat), nr, ptr(xkmat),
+                                           _colstride(xkmat), nk, ptr(phase), _colstride(phase)))
+    return phase
+
+
+def batched_gemm(transA, transB, A, B, C):
+    """batched_gemm!(transA, transB, A, B, C) (src/common/gpu_utils.jl:71-78): C[:, :, b] =
+    op(A[:, :, b]) op(B[:, :, b]) for complex128 Julia-layout (rows, cols, batch) device arrays, op 'N',
+    'T' or 'C'; strided batch views keep their strides."""
+    ra, ca, nb = _jlshape(A)
+    rb, cb, nb2 = _jlshape(B)
+    m, n, nb3 = _jlshape(C)
+    assert nb == nb2 == nb3, "batch sizes differ"
+    am, k = (ra, ca) if transA == "N" else (ca, ra)     # op(A) is m x k
+    bk, bn = (rb, cb) if transB == "N" else (cb, rb)    # op(B) is k x n
+    assert am == m and bn == n and bk == k, "inner or outer dimensions do not match"
+    check(_lib.lib().epb_batched_zgemm(_ctx().h, transA.encode(), transB.encode(), m, n, k, ptr(A), _colstride(A),
+                                       A.stride(0), ptr(B), _colstride(B), B.stride(0), ptr(C), _colstride(C),
+                                       C.stride(0), nb))
+    return C
+
+
 def get_fourier_batched(itp: BatchedWannierInterpolator, xks, out=None, prec=PREC_FP64):
     """out (ndata, nk) = op_r[1:ndata, :] * exp(2 pi i R . x) (batched_interpolator.jl:200-214)."""
     torch = _torch()

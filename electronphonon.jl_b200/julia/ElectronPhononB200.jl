@@ -19,29 +19,72 @@ using ElectronPhonon
 using ElectronPhonon: WannierObject, Vec3
 
 const LIB = Ref(joinpath(@__DIR__, "..", "lib", "libepb200.so"))
-const PREC = Ref{Cint}(1)  # 0: plain FP64, 1: split-BF16 tensor cores + FP32/FP64 eigensolve
+# Precision of the methods that replace the reference's own (fourier, eigensolves, e-ph chain, rotations,
+# batched_gemm!): plain FP64 by default, the reference's semantics (cuBLAS ZGEMM + cuSOLVER heevj in
+# FP64, ext/ElectronPhononCUDAExt.jl:80-126). `set_precision!(:mixed)` opts into the split-precision
+# tensor-core path (FP32-level sums, FP32 eigensolve + FP64 refinement).
+const PREC = Ref{Cint}(0)
+# Precision of this library's own drivers (eph_pass, serta, eph_outer_q, the band / window calls, the
+# surrogate screen), which have no FP64 counterpart in the reference to match: mixed by default.
+const DRIVER_PREC = Ref{Cint}(1)
+function set_precision!(p::Symbol; drivers::Bool = false)
+    v = p === :fp64 ? Cint(0) : p === :mixed ? Cint(1) : throw(ArgumentError("precision :fp64 or :mixed"))
+    drivers ? (DRIVER_PREC[] = v) : (PREC[] = v)
+    v
+end
 const NULLDEV = CuPtr{Cvoid}(0)  # an absent optional device buffer
 
 last_error() = unsafe_string(ccall((:epb_last_error, LIB[]), Cstring, ()))
 check(st::Integer) = st == 0 || error("libepb200: status $st: $(last_error())")
 
-# ---- context: one per task (the reference's batched loop is single-threaded) -----------------
+# ---- context: one per (device, host thread); bound to the calling task's stream on every call ----
+# The library's workspace lives in the context, so one per device and thread is enough; CUDA.jl gives
+# each task its own stream, which `ctx()` installs (epb_set_stream) before the call, so a context never
+# holds a stream handle past the call that used it.
 mutable struct Ctx
     h::Ptr{Cvoid}
 end
-const CTX = Dict{Tuple{Int,UInt},Ctx}()
+const CTX = Dict{Tuple{Int,Int},Ctx}()
+const CTX_LOCK = ReentrantLock()
 function ctx()
     dev = CUDA.deviceid(CUDA.device())
     s = CUDA.stream()
-    key = (dev, UInt(pointer_from_objref(s)))
-    get!(CTX, key) do
-        r = Ref{Ptr{Cvoid}}(C_NULL)
-        check(ccall((:epb_create, LIB[]), Cint, (Ptr{Ptr{Cvoid}}, Cint, Ptr{Cvoid}), r, dev, s.handle))
-        c = Ctx(r[])
-        finalizer(x -> ccall((:epb_destroy, LIB[]), Cint, (Ptr{Cvoid},), x.h), c)
-        c
+    c = lock(CTX_LOCK) do
+        get!(CTX, (dev, Threads.threadid())) do
+            r = Ref{Ptr{Cvoid}}(C_NULL)
+            check(ccall((:epb_create, LIB[]), Cint, (Ptr{Ptr{Cvoid}}, Cint, Ptr{Cvoid}), r, dev, s.handle))
+            c = Ctx(r[])
+            finalizer(x -> ccall((:epb_destroy, LIB[]), Cint, (Ptr{Cvoid},), x.h), c)
+            c
+        end
     end
+    check(ccall((:epb_set_stream, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), c.h, s.handle))
+    c
 end
+
+# ---- device operands as the reference's loop passes them ---------------------------------------
+# The batched loop hands over contiguous device VIEWS (view(epkq_dev, :,:,:, rng_q), view(P_kq, :, rng_q),
+# view(ep_ekpR_all, :, :, ik_ind); run_eph_over_k_and_kq.jl:821-869) and reshapes of them
+# (reshape(view(ws.g, :, 1:nq), ...), wannier_to_bloch_batched.jl:270), so the overrides are typed
+# DenseCuArray / StridedCuArray / AnyCuArray like the extension's own methods (ext:172-179), never a bare
+# CuArray. `devptr` is the device address of such an operand; `colstride` its column stride.
+function assert_dense(a)
+    c = a isa Base.ReshapedArray ? Base.iscontiguous(parent(a)) : Base.iscontiguous(a)
+    c || throw(ArgumentError("libepb200: this operand must be contiguous (got $(typeof(a)))"))
+    a
+end
+function devptr(a)
+    a === nothing && return NULLDEV
+    assert_dense(a)
+    p = a isa Base.ReshapedArray && !(a isa DenseCuArray) ? parent(a) : a  # reshape(view(...)): the view's address
+    p isa StridedCuArray || throw(ArgumentError("libepb200: expected a device array, got $(typeof(a))"))
+    Base.unsafe_convert(CuPtr{eltype(p)}, p)  # the conversion ccall applies to a device array argument
+end
+function colstride(a::AbstractArray)
+    stride(a, 1) == 1 || throw(ArgumentError("libepb200: the first axis of a device operand must be contiguous"))
+    ndims(a) >= 2 ? stride(a, 2) : length(a)
+end
+colstride(a::Base.ReshapedArray) = size(a, 1)  # a reshape of a contiguous array is contiguous
 
 # ---- lattice-vector sets (BatchedFourierCore's irvec_mat, WannierObject.jl:148-152) ---------
 mutable struct RSet
@@ -59,7 +102,9 @@ function rset(irvec::Vector{Vec3{Int}})
     end
 end
 
+# k lists: a host Vector{Vec3} (or a view of one) is uploaded; a (3 x nk) device matrix is used in place
 xk_device(xks) = CuArray(reinterpret(reshape, Float64, collect(Vec3{Float64}, xks)))  # 3 x nk
+xk_device(xks::DenseCuMatrix{Float64}) = xks
 
 # ---- backend (ext:34-37) -----------------------------------------------------------------------
 function ElectronPhonon.free_bytes(::ElectronPhonon.GPUBackend)
@@ -71,14 +116,20 @@ ElectronPhonon.synchronize(::ElectronPhonon.GPUBackend) =
     check(ccall((:epb_synchronize, LIB[]), Cint, (Ptr{Cvoid},), ctx().h))
 
 # ---- Fourier (batched_fourier_core.jl:24-30, 117-139) ----------------------------------------
-function ElectronPhonon.fourier_phase!(phase::CuMatrix{ComplexF64}, irvec::Vector{Vec3{Int}}, xks)
-    xk = xk_device(xks)
-    check(ccall((:epb_fourier_phase, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, CuPtr{Float64}, Int64, CuPtr{ComplexF64}),
-                ctx().h, rset(irvec).h, xk, size(xk, 2), phase))
+# fourier_phase!(phase, irvec_mat, xkmat): the reference's own operands, the (nr x 3) FP64 R matrix of
+# _irvec_to_device_matrix and a (3 x nk) coordinate matrix, views included (P_mk[:, 1:nk_batch] and
+# mxk_dev[:, iks_batch] at run_eph_over_k_and_kq.jl:821; batched_fourier_core.jl:104).
+function ElectronPhonon.fourier_phase!(phase::StridedCuMatrix{ComplexF64}, irvec_mat::StridedCuMatrix{Float64},
+        xkmat::StridedCuMatrix{Float64})
+    nr, nk = size(phase)
+    @assert size(irvec_mat) == (nr, 3) && size(xkmat) == (3, nk)
+    check(ccall((:epb_fourier_phase_mat, LIB[]), Cint,
+                (Ptr{Cvoid}, CuPtr{Float64}, Int64, Int64, CuPtr{Float64}, Int64, Int64, CuPtr{ComplexF64}, Int64),
+                ctx().h, irvec_mat, colstride(irvec_mat), nr, xkmat, colstride(xkmat), nk, phase, colstride(phase)))
     phase
 end
 
-function ElectronPhonon.get_fourier_batched!(out::CuMatrix{ComplexF64},
+function ElectronPhonon.get_fourier_batched!(out::DenseCuMatrix{ComplexF64},
         itp::ElectronPhonon.BatchedWannierInterpolator, xks)
     p = itp.parent
     xk = xk_device(xks)
@@ -89,8 +140,26 @@ function ElectronPhonon.get_fourier_batched!(out::CuMatrix{ComplexF64},
     out
 end
 
+# batched_gemm! (src/common/gpu_utils.jl:71-78; CUDA method ext:122-126): strided-batched, alpha = 1, beta = 0
+function ElectronPhonon.batched_gemm!(transA::Char, transB::Char, A::StridedCuArray{ComplexF64,3},
+        B::StridedCuArray{ComplexF64,3}, C::StridedCuArray{ComplexF64,3})
+    m, n, nb = size(C)
+    k = transA == 'N' ? size(A, 2) : size(A, 1)
+    @assert size(A, 3) == size(B, 3) == nb
+    @assert (transA == 'N' ? size(A, 1) : size(A, 2)) == m && (transB == 'N' ? size(B, 1) : size(B, 2)) == k &&
+            (transB == 'N' ? size(B, 2) : size(B, 1)) == n
+    check(ccall((:epb_batched_zgemm, LIB[]), Cint,
+                (Ptr{Cvoid}, Cchar, Cchar, Int64, Int64, Int64, CuPtr{ComplexF64}, Int64, Int64, CuPtr{ComplexF64},
+                 Int64, Int64, CuPtr{ComplexF64}, Int64, Int64, Int64),
+                ctx().h, transA, transB, m, n, k, A, colstride(A), stride(A, 3), B, colstride(B), stride(B, 3),
+                C, colstride(C), stride(C, 3), nb))
+    C
+end
+
 # ---- eigensolves (ext:80-115) -----------------------------------------------------------------
-function ElectronPhonon.eigvals_batched(Hk::CuArray{ComplexF64,3})
+# Hk as the callers pass it: a CuArray or a reshape / contiguous view of one
+# (eigen_batched(reshape(Hkq_flat, nw, nw, nk_batch_max)), run_eph_over_q_and_k.jl:578).
+function ElectronPhonon.eigvals_batched(Hk::DenseCuArray{ComplexF64,3})
     nw, _, nk = size(Hk)
     E = CuArray{Float64}(undef, nw, nk)
     check(ccall((:epb_eigh_batched, LIB[]), Cint,
@@ -99,7 +168,7 @@ function ElectronPhonon.eigvals_batched(Hk::CuArray{ComplexF64,3})
     E
 end
 
-function ElectronPhonon.eigen_batched(Hk::CuArray{ComplexF64,3})
+function ElectronPhonon.eigen_batched(Hk::DenseCuArray{ComplexF64,3})
     nw, _, nk = size(Hk)
     E = CuArray{Float64}(undef, nw, nk)
     check(ccall((:epb_eigh_batched, LIB[]), Cint,
@@ -109,7 +178,7 @@ function ElectronPhonon.eigen_batched(Hk::CuArray{ComplexF64,3})
 end
 
 # phonons: D(q) / sqrt(m_i m_j) -> eigen -> omega = sign sqrt, u ./= sqrt(m) (compute_states.jl:293-300)
-function phonon_eigen_batched!(Dq::CuArray{ComplexF64,3}, mass::CuVector{Float64})
+function phonon_eigen_batched!(Dq::DenseCuArray{ComplexF64,3}, mass::DenseCuVector{Float64})
     nm, _, nq = size(Dq)
     ω = CuArray{Float64}(undef, nm, nq)
     check(ccall((:epb_ph_eigen_batched, LIB[]), Cint,
@@ -119,49 +188,65 @@ function phonon_eigen_batched!(Dq::CuArray{ComplexF64,3}, mass::CuVector{Float64
 end
 
 # ---- e-ph chain (wannier_to_bloch_batched.jl:178-273, 442-455) -------------------------------
-function ElectronPhonon.get_eph_RR_to_kR_batched!(ep_ekpR_all::CuArray{ComplexF64,3},
-        itp_epmat::ElectronPhonon.BatchedWannierInterpolator, ks, uks::CuArray{ComplexF64,3};
-        additional_phase = nothing)
+# call site: get_eph_RR_to_kR_batched!(ep_ekpR_all, itp_epmat, ks_batch, uks_dev; additional_phase = P_mk)
+# (run_eph_over_k_and_kq.jl:822): device buffers, a host k list
+function ElectronPhonon.get_eph_RR_to_kR_batched!(ep_ekpR_all::DenseCuArray{ComplexF64,3},
+        itp_epmat::ElectronPhonon.BatchedWannierInterpolator, ks, uks::DenseCuArray{ComplexF64,3};
+        additional_phase::Union{Nothing,DenseCuMatrix{ComplexF64}} = nothing)
     epmat = itp_epmat.parent
     nr_ep = length(epmat.irvec_next)
     nw, nband, nk = size(uks)
     nmodes = div(epmat.ndata, nw^2 * nr_ep)
+    @assert size(ep_ekpR_all) == (nw * nband * nmodes, nr_ep, nk)
+    additional_phase === nothing || @assert size(additional_phase) == (nr_ep, nk)
     xk = xk_device(ks)
-    ph = additional_phase === nothing ? NULLDEV : pointer(additional_phase)
     check(ccall((:epb_eph_RR_to_kR, LIB[]), Cint,
                 (Ptr{Cvoid}, CuPtr{ComplexF64}, Int64, Int64, Int64, Ptr{Cvoid}, CuPtr{Float64}, Int64,
                  CuPtr{ComplexF64}, Int64, CuPtr{ComplexF64}, CuPtr{ComplexF64}, Cint),
-                ctx().h, epmat.op_r, nw, nmodes, nr_ep, rset(epmat.irvec).h, xk, nk, uks, nband, ph,
-                ep_ekpR_all, PREC[]))
+                ctx().h, epmat.op_r, nw, nmodes, nr_ep, rset(epmat.irvec).h, xk, nk, uks, nband,
+                devptr(additional_phase), ep_ekpR_all, PREC[]))
     ep_ekpR_all
 end
 
-function ElectronPhonon.get_eph_kR_to_kq_batched!(ep_kq_all::CuArray{ComplexF64,4}, ep_kR::CuMatrix{ComplexF64},
-        phase::CuMatrix{ComplexF64}, u_phs, ukqs; ws = nothing, g2_out = nothing, ωq = nothing)
+# call site (run_eph_over_k_and_kq.jl:866-869): every array argument a contiguous device view,
+#   get_eph_kR_to_kq_batched!(view(epkq_dev, :,:,:, rng_q), view(ep_ekpR_all, :, :, ik_ind), view(P_kq, :, rng_q),
+#       view(uphs_dev, :, :, rng_q), view(ukqs_all_dev, :, :, qstart:qend); ws, g2_out = view(g2_dev, ...), ωq = view(ωq_dev, :, rng_q))
+function ElectronPhonon.get_eph_kR_to_kq_batched!(ep_kq_all::DenseCuArray{ComplexF64,4},
+        ep_kR::StridedCuMatrix{ComplexF64}, phase::StridedCuMatrix{ComplexF64}, u_phs::DenseCuArray{ComplexF64,3},
+        ukqs::DenseCuArray{ComplexF64,3}; ws = nothing, g2_out::Union{Nothing,DenseCuArray{Float64,4}} = nothing,
+        ωq::Union{Nothing,DenseCuMatrix{Float64}} = nothing)
     nbandkq, nbandk, nmodes, nq = size(ep_kq_all)
     nw = size(ukqs, 1)
+    nr_ep = size(ep_kR, 2)
+    @assert size(ep_kR, 1) == nw * nbandk * nmodes && size(phase) == (nr_ep, nq)
+    @assert size(ukqs) == (nw, nbandkq, nq) && size(u_phs) == (nmodes, nmodes, nq)
+    colstride(phase) == nr_ep || throw(ArgumentError("libepb200: the phase columns must be contiguous (stride nr)"))
     check(ccall((:epb_eph_kR_to_kq, LIB[]), Cint,
                 (Ptr{Cvoid}, CuPtr{ComplexF64}, Int64, Int64, Int64, Int64, Int64, CuPtr{ComplexF64}, Int64,
                  CuPtr{ComplexF64}, Int64, CuPtr{ComplexF64}, CuPtr{Float64}, CuPtr{ComplexF64}, CuPtr{Float64}, Cint),
-                ctx().h, ep_kR, size(ep_kR, 1), nw, nbandk, nmodes, size(ep_kR, 2), phase, nq, ukqs, nbandkq,
-                u_phs, ωq === nothing ? NULLDEV : ωq, ep_kq_all, g2_out === nothing ? NULLDEV : g2_out, PREC[]))
+                ctx().h, ep_kR, colstride(ep_kR), nw, nbandk, nmodes, nr_ep, phase, nq, ukqs, nbandkq,
+                u_phs, devptr(ωq), ep_kq_all, devptr(g2_out), PREC[]))
     ep_kq_all
 end
 
-function ElectronPhonon.eph_apply_rotations!(ep_kq_all::CuArray{ComplexF64,4}, g::CuArray{ComplexF64,4},
-        ukqs::CuArray, u_phs::CuArray, tmp; g2_out = nothing, ωq = nothing)
+# g arrives as reshape(view(ws.g, :, 1:nq), nw, nbandk, nmodes, nq) (wannier_to_bloch_batched.jl:270), a
+# reshape of a view, hence AnyCuArray (as ext:176); its per-q stride is nw * nbandk * nmodes.
+function ElectronPhonon.eph_apply_rotations!(ep_kq_all::DenseCuArray{ComplexF64,4}, g::AnyCuArray{ComplexF64,4},
+        ukqs::DenseCuArray{ComplexF64,3}, u_phs::DenseCuArray{ComplexF64,3}, tmp; g2_out = nothing, ωq = nothing)
     nbandkq, nbandk, nmodes, nq = size(ep_kq_all)
     nw = size(ukqs, 1)
+    @assert size(g) == (nw, nbandk, nmodes, nq)
+    assert_dense(g)
     check(ccall((:epb_eph_apply_rotations, LIB[]), Cint,
                 (Ptr{Cvoid}, CuPtr{ComplexF64}, Int64, Int64, Int64, Int64, Int64, CuPtr{ComplexF64}, Int64,
                  CuPtr{ComplexF64}, CuPtr{Float64}, CuPtr{ComplexF64}, CuPtr{Float64}),
-                ctx().h, g, nw * nbandk * nmodes, nw, nbandk, nmodes, nq, ukqs, nbandkq, u_phs,
-                ωq === nothing ? NULLDEV : ωq, ep_kq_all, g2_out === nothing ? NULLDEV : g2_out))
+                ctx().h, devptr(g), nw * nbandk * nmodes, nw, nbandk, nmodes, nq, ukqs, nbandkq, u_phs,
+                devptr(ωq), ep_kq_all, devptr(g2_out)))
     ep_kq_all
 end
 
 # ---- energy window (filter.jl:19,40-72): band ranges and kept k without copying E to the host --
-function window_filter(E::CuMatrix{Float64}, wmin::Real, wmax::Real)
+function window_filter(E::DenseCuMatrix{Float64}, wmin::Real, wmax::Real)
     nw, nk = size(E)
     bmin = CuVector{Int32}(undef, nk); bmax = CuVector{Int32}(undef, nk)
     keep = CuVector{Int32}(undef, max(nk, 1)); nkeep = CUDA.zeros(Int64, 1)
@@ -175,9 +260,11 @@ function window_filter(E::CuMatrix{Float64}, wmin::Real, wmax::Real)
 end
 
 # ---- outer-q chain (wannier_to_bloch.jl:277-300, wannier_to_bloch_batched.jl:317-377) -----------
-function ElectronPhonon.get_eph_Rq_to_kq_batched!(ep_kq_all::CuArray{ComplexF64,4},
-        itp_epobj_eRpq::ElectronPhonon.BatchedWannierInterpolator, ks, uks::CuArray{ComplexF64,3},
-        ukqs::CuArray{ComplexF64,3}; ws = nothing)
+# call site: get_eph_Rq_to_kq_batched!(ep_batch, itp_ep_eRpq, ks_batch, Uk_batch, Ukq_batch; ws = ep_ws)
+# (run_eph_over_q_and_k.jl:588)
+function ElectronPhonon.get_eph_Rq_to_kq_batched!(ep_kq_all::DenseCuArray{ComplexF64,4},
+        itp_epobj_eRpq::ElectronPhonon.BatchedWannierInterpolator, ks, uks::DenseCuArray{ComplexF64,3},
+        ukqs::DenseCuArray{ComplexF64,3}; ws = nothing)
     nbandkq, nbandk, nmodes, nk = size(ep_kq_all)
     nw = size(uks, 1)
     parent = itp_epobj_eRpq.parent
@@ -191,8 +278,8 @@ function ElectronPhonon.get_eph_Rq_to_kq_batched!(ep_kq_all::CuArray{ComplexF64,
 end
 
 # g(Re, q) for a list of q from the "ph"-layout epmat (rows (i, j, nu, Re)), in the eigenmode basis u_phs
-function eph_RR_to_Rq_batched!(ep_Rq_all::CuArray{ComplexF64,3}, epmat::ElectronPhonon.WannierObject, xqs,
-        u_phs::CuArray{ComplexF64,3})
+function eph_RR_to_Rq_batched!(ep_Rq_all::DenseCuArray{ComplexF64,3}, epmat::ElectronPhonon.WannierObject, xqs,
+        u_phs::DenseCuArray{ComplexF64,3})
     nm = size(u_phs, 1)
     nr_el = length(epmat.irvec_next)
     nw = isqrt(div(epmat.ndata, nm * nr_el))
@@ -205,33 +292,39 @@ function eph_RR_to_Rq_batched!(ep_Rq_all::CuArray{ComplexF64,3}, epmat::Electron
 end
 
 # ---- calculator hooks (calculator_utils.jl:36-50, boltzmann_calculator.jl:336-362) ----------------
-function ElectronPhonon.eph_window_scatter!(g2_out::CuArray{Float64}, ωq_out::CuArray{Float64},
-        g2vals::CuArray{Float64,4}, imap_i_col::CuVector{Int}, imap_f::CuMatrix{Int}, ikqs, ωq::CuMatrix{Float64},
-        nbandkq::Int, nbandk::Int, nm::Int, nq_batch::Int, ni_stride::Int, i0::Int)
+# The extension leaves the loop-side operands untyped (ext:303, 361): they arrive as views of the loop's
+# buffers (view(g2_dev, :,:,:, rng_q), view(dev.imap_i, rng, ik)). Here they are any device array
+# (AnyCuArray), so these methods are the ones dispatched for every device form the extension takes; the
+# library reads them through plain pointers, so a non-contiguous one is refused with an ArgumentError.
+function ElectronPhonon.eph_window_scatter!(g2_out::DenseCuArray{Float64}, ωq_out::DenseCuArray{Float64},
+        g2vals::AnyCuArray{Float64,4}, imap_i_col::AnyCuArray{Int,1}, imap_f::AnyCuArray{Int,2}, ikqs,
+        ωq::AnyCuArray{Float64,2}, nbandkq::Int, nbandk::Int, nm::Int, nq_batch::Int, ni_stride::Int, i0::Int)
+    foreach(assert_dense, (g2vals, imap_i_col, imap_f, ωq))
     ikq_d = CuArray{Int64}(collect(ikqs))
     check(ccall((:epb_eph_window_scatter, LIB[]), Cint,
                 (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, CuPtr{Float64}, CuPtr{Int64}, CuPtr{Int64}, Int64,
                  CuPtr{Int64}, CuPtr{Float64}, Int64, Int64, Int64, Int64, Int64, Int64),
-                ctx().h, g2_out, ωq_out, g2vals, imap_i_col, imap_f, size(imap_f, 1), ikq_d, ωq, nbandkq, nbandk,
-                nm, nq_batch, ni_stride, i0))
+                ctx().h, g2_out, ωq_out, devptr(g2vals), devptr(imap_i_col), devptr(imap_f), colstride(imap_f), ikq_d,
+                devptr(ωq), nbandkq, nbandk, nm, nq_batch, ni_stride, i0))
     nothing
 end
 
-function ElectronPhonon.bte_window_accumulate!(Sₒ_out::CuMatrix{Float64}, Sᵢ_out, g2vals::CuArray{Float64,4},
-        ωqmat::CuMatrix{Float64}, imap_i_at_k::CuVector{Int}, imap_f::CuMatrix{Int}, ikqs, e_i, e_f, wf, μs, Ts,
-        ηs, method::Int, ω_cutoff, nbandkq::Int, nbandk::Int, nmodes::Int, nq_batch::Int, i0::Int)
+function ElectronPhonon.bte_window_accumulate!(Sₒ_out::DenseCuArray{Float64}, Sᵢ_out, g2vals::AnyCuArray{Float64,4},
+        ωqmat::AnyCuArray{Float64,2}, imap_i_at_k::AnyCuArray{Int,1}, imap_f::AnyCuArray{Int,2}, ikqs, e_i, e_f, wf,
+        μs, Ts, ηs, method::Int, ω_cutoff, nbandkq::Int, nbandk::Int, nmodes::Int, nq_batch::Int, i0::Int)
+    foreach(assert_dense, (g2vals, ωqmat, imap_i_at_k, imap_f))
     ikq_d = CuArray{Int64}(collect(ikqs))
-    dev(x) = x isa CuArray ? x : CuArray{Float64}(collect(x))
-    sin_ptr = Sᵢ_out === nothing ? NULLDEV : Sᵢ_out
+    dev(x) = x isa DenseCuArray{Float64} ? x : CuArray{Float64}(collect(x))
+    sin_ptr = Sᵢ_out === nothing ? NULLDEV : devptr(assert_dense(Sᵢ_out))
     ni_tile, n_f = Sᵢ_out === nothing ? (0, 0) : (size(Sᵢ_out, 1), size(Sᵢ_out, 2))
     check(ccall((:epb_bte_window_accumulate, LIB[]), Cint,
                 (Ptr{Cvoid}, CuPtr{Float64}, Int64, CuPtr{Float64}, Int64, Int64, CuPtr{Float64}, CuPtr{Float64},
                  CuPtr{Int64}, CuPtr{Int64}, Int64, CuPtr{Int64}, CuPtr{Float64}, CuPtr{Float64}, CuPtr{Float64},
                  CuPtr{Float64}, CuPtr{Float64}, CuPtr{Float64}, Int64, Cint, Float64, Int64, Int64, Int64, Int64,
                  Int64),
-                ctx().h, Sₒ_out, size(Sₒ_out, 1), sin_ptr, ni_tile, n_f, g2vals, ωqmat, imap_i_at_k, imap_f,
-                size(imap_f, 1), ikq_d, dev(e_i), dev(e_f), dev(wf), dev(μs), dev(Ts), dev(ηs), length(μs), method,
-                ω_cutoff, nbandkq, nbandk, nmodes, nq_batch, i0))
+                ctx().h, Sₒ_out, size(Sₒ_out, 1), sin_ptr, ni_tile, n_f, devptr(g2vals), devptr(ωqmat),
+                devptr(imap_i_at_k), devptr(imap_f), colstride(imap_f), ikq_d, dev(e_i), dev(e_f), dev(wf), dev(μs),
+                dev(Ts), dev(ηs), length(μs), method, ω_cutoff, nbandkq, nbandk, nmodes, nq_batch, i0))
     nothing
 end
 
@@ -287,14 +380,14 @@ function PassModel(model; mixed::Bool = true)
 end
 
 """
-    eph_pass(pm, xks, xqs; prec = PREC[], k_batch = 0, sample_stride = 0)
+    eph_pass(pm, xks, xqs; prec = DRIVER_PREC[], k_batch = 0, sample_stride = 0)
 
 All-band e-ph pass over the k list x the q list: electrons at k and k+q, phonons at q,
 g2 = |u_kq' g u_ph|^2 / (2 omega). Returns device arrays `ek` (nw x nk), `omega` (nm x nq), `g2sum`
 (nm x nk, summed over bands and q) and, for `sample_stride > 0`, the full g2 blocks of every
 `sample_stride`-th q, (nw, nw, nm, nsamp, nk); `k_batch <= 0` lets the library time the batch sizes.
 """
-function eph_pass(pm::PassModel, xks, xqs; prec::Integer = PREC[], k_batch::Integer = 0, sample_stride::Integer = 0)
+function eph_pass(pm::PassModel, xks, xqs; prec::Integer = DRIVER_PREC[], k_batch::Integer = 0, sample_stride::Integer = 0)
     xk = xk_device(xks)
     xq = xk_device(xqs)
     nk, nq = size(xk, 2), size(xq, 2)
@@ -336,7 +429,7 @@ end
 
 """
     serta(pm, ngrid, wmin, wmax, mu, T, smearing; lattice, volume, spin = 2.0, method = 5,
-          omega_cutoff = ElectronPhonon.omega_acoustic, prec = PREC[], k_batch = 0, shard = (0, 1),
+          omega_cutoff = ElectronPhonon.omega_acoustic, prec = DRIVER_PREC[], k_batch = 0, shard = (0, 1),
           inv_tau = false)
 
 SERTA conductivity (3 x 3, host, in the reference's units) over commensurate ngrid^3 k = q grids.
@@ -346,7 +439,7 @@ that share's partial sigma: add the shards' sigmas over the ranks (`MPI.Allreduc
 """
 function serta(pm::PassModel, ngrid::Integer, wmin, wmax, mu, T, smearing; lattice::AbstractMatrix, volume,
                spin = 2.0, method::Integer = 5, omega_cutoff = ElectronPhonon.omega_acoustic,
-               prec::Integer = PREC[], k_batch::Integer = 0, shard = (0, 1), inv_tau::Bool = false)
+               prec::Integer = DRIVER_PREC[], k_batch::Integer = 0, shard = (0, 1), inv_tau::Bool = false)
     p = Ref(BteParams(ngrid, wmin, wmax, mu, T, smearing, omega_cutoff, spin, volume,
                       NTuple{9,Float64}(Float64.(vec(lattice))), Int32(method), Int32(prec), k_batch, 0,
                       shard[1], shard[2]))
@@ -380,7 +473,7 @@ function Bands(ham)
 end
 
 "Ascending band energies (nw x nk) at the k list (get_el_eigen_valueonly_batched)."
-function band_eigvals(b::Bands, xks; prec::Integer = PREC[])
+function band_eigvals(b::Bands, xks; prec::Integer = DRIVER_PREC[])
     xk = xk_device(xks)
     E = CuArray{Float64}(undef, b.nw, size(xk, 2))
     check(ccall((:epb_bands_eigvals, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, CuPtr{Float64}, Int64, CuPtr{Float64},
@@ -389,7 +482,7 @@ function band_eigvals(b::Bands, xks; prec::Integer = PREC[])
 end
 
 "Energy of one band (1-based) at every point of the k list."
-function band_energy(b::Bands, xks, band::Integer; prec::Integer = PREC[])
+function band_energy(b::Bands, xks, band::Integer; prec::Integer = DRIVER_PREC[])
     xk = xk_device(xks)
     E = CuArray{Float64}(undef, size(xk, 2))
     check(ccall((:epb_bands_band_energy, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, CuPtr{Float64}, Int64, Int64,
@@ -406,7 +499,7 @@ const WindowStats = NTuple{8,Int64}  # epb_window_stats: tested, culled, evaluat
 `_filter_kpoints` from H(R) without downloading the energies: per point the 1-based band range
 (0 / 0 when empty) and the 0-based ascending list of kept points.
 """
-function bands_window(b::Bands, xks, wmin, wmax; prec::Integer = PREC[], guard = 1e-3)
+function bands_window(b::Bands, xks, wmin, wmax; prec::Integer = DRIVER_PREC[], guard = 1e-3)
     xk = xk_device(xks)
     nk = size(xk, 2)
     bmin = CuVector{Int32}(undef, nk)
@@ -427,7 +520,7 @@ end
 Kept (k, q) pairs (pair index ik * nq + iq, 0-based) with their band ranges at k + q; `mlp`, a
 calibrated surrogate handle, culls pairs before the plain evaluation.
 """
-function pair_window(b::Bands, xks, xqs, wmin, wmax; mlp::Ptr{Cvoid} = C_NULL, prec::Integer = PREC[],
+function pair_window(b::Bands, xks, xqs, wmin, wmax; mlp::Ptr{Cvoid} = C_NULL, prec::Integer = DRIVER_PREC[],
                      guard = 1e-3, capacity::Integer)
     xk = xk_device(xks)
     xq = xk_device(xqs)
@@ -446,8 +539,8 @@ end
 
 # ---- uneven eigensolve batches (eigen_batched over ragged inputs, ext:80-115) ---------------------
 "Eigen-decompose matrices of different orders packed in `A` (in place; orders 1..96)."
-function eigen_varlen!(A::CuVector{ComplexF64}, a_offset::CuVector{Int64}, n::CuVector{Int32}, E::CuVector{Float64},
-                       e_offset::CuVector{Int64}; jobz::Char = 'V', prec::Integer = PREC[])
+function eigen_varlen!(A::DenseCuVector{ComplexF64}, a_offset::DenseCuVector{Int64}, n::DenseCuVector{Int32}, E::DenseCuVector{Float64},
+                       e_offset::DenseCuVector{Int64}; jobz::Char = 'V', prec::Integer = PREC[])
     check(ccall((:epb_eigh_varlen, LIB[]), Cint, (Ptr{Cvoid}, CuPtr{ComplexF64}, CuPtr{Int64}, CuPtr{Int32}, Int64,
                 CuPtr{Float64}, CuPtr{Int64}, Cchar, Cint), ctx().h, A, a_offset, n, length(n), E, e_offset,
                 Cchar(jobz), Cint(prec)))
@@ -455,8 +548,8 @@ function eigen_varlen!(A::CuVector{ComplexF64}, a_offset::CuVector{Int64}, n::Cu
 end
 
 # ---- q index of k+q on a commensurate grid (_fill_iqs!, run_eph_over_k_and_kq.jl:565-582) -----------
-function fill_iqs!(iqs::CuVector{Int64}, xkq_int::CuMatrix{Int64}, xk_int::AbstractVector{<:Integer}, ngrid,
-                   dense_hash_to_iq::CuVector{Int64})
+function fill_iqs!(iqs::DenseCuVector{Int64}, xkq_int::DenseCuMatrix{Int64}, xk_int::AbstractVector{<:Integer}, ngrid,
+                   dense_hash_to_iq::DenseCuVector{Int64})
     check(ccall((:epb_fill_iqs, LIB[]), Cint, (Ptr{Cvoid}, CuPtr{Int64}, Int64, Ptr{Int64}, Int64, Int64, Int64,
                 CuPtr{Int64}, CuPtr{Int64}), ctx().h, xkq_int, size(xkq_int, 2), Int64.(collect(xk_int)),
                 ngrid[1], ngrid[2], ngrid[3], dense_hash_to_iq, iqs))
@@ -470,8 +563,8 @@ end
 The window filter on caller-owned buffers (`nkeep` a one-element device vector), using the library's
 fixed static scratch (nk <= 16,777,216); calls that overlap on one device race.
 """
-function window_filter_noalloc(E::CuMatrix{Float64}, wmin, wmax, band_min::CuVector{Int32}, band_max::CuVector{Int32},
-                               keep::CuVector{Int32}, nkeep::CuVector{Int64})
+function window_filter_noalloc(E::DenseCuMatrix{Float64}, wmin, wmax, band_min::DenseCuVector{Int32}, band_max::DenseCuVector{Int32},
+                               keep::DenseCuVector{Int32}, nkeep::DenseCuVector{Int64})
     nw, nk = size(E)
     check(ccall((:epb_window_filter_noalloc, LIB[]), Cint, (Ptr{Cvoid}, CuPtr{Float64}, Int64, Int64, Float64,
                 Float64, CuPtr{Int32}, CuPtr{Int32}, CuPtr{Int32}, CuPtr{Int64}, CuPtr{Float64}),
@@ -620,7 +713,7 @@ function _oq_end(user::Ptr{Cvoid}, iq::Int64, stream::Ptr{Cvoid})::Cint
 end
 
 """
-    eph_outer_q(pm, xks, xqs, calcs; window_k, window_kq, wtk = nothing, prec = PREC[], k_batch = 0,
+    eph_outer_q(pm, xks, xqs, calcs; window_k, window_kq, wtk = nothing, prec = DRIVER_PREC[], k_batch = 0,
                 q_chunk = 0, phonon_basis = 0)
 
 The outer-q batched loop: per q, g(Re, q) and the phonon modes, then per batch of kept k the k+q states
@@ -628,7 +721,7 @@ and ep = ukq' g(k, q) uk, handed to each calculator's `outer_q_run_batch!`. Retu
 record A[iq] = sum_k wtk sum |ep|^2 and the stats (kept k, k batch, q chunk, batches).
 """
 function eph_outer_q(pm::PassModel, xks, xqs, calcs::AbstractVector; window_k, window_kq, wtk = nothing,
-                     prec::Integer = PREC[], k_batch::Integer = 0, q_chunk::Integer = 0, phonon_basis::Integer = 0)
+                     prec::Integer = DRIVER_PREC[], k_batch::Integer = 0, q_chunk::Integer = 0, phonon_basis::Integer = 0)
     xk = collect(reinterpret(reshape, Float64, collect(Vec3{Float64}, xks)))  # host 3 x nk
     xq = collect(reinterpret(reshape, Float64, collect(Vec3{Float64}, xqs)))
     nk, nq = size(xk, 2), size(xq, 2)
@@ -686,7 +779,7 @@ function Surrogate(fvecs::Vector{Vec3{Int}}, nout::Integer; hidden::Integer = 25
 end
 
 "Adam training on points `xks` with band energies `E` (nout x n, device); returns the loss of each epoch."
-function train!(m::Surrogate, xks, E::CuMatrix{Float64}; epochs::Integer = 200, batch::Integer = 2048,
+function train!(m::Surrogate, xks, E::DenseCuMatrix{Float64}; epochs::Integer = 200, batch::Integer = 2048,
                 lr = 2e-3, lr_final = 2e-5, seed::Integer = 1, use_graph::Bool = true)
     x = xk_device(xks)
     opts = Ref(MlpTrainOpts(epochs, batch, lr, lr_final, UInt64(seed), Int32(use_graph), Int32(0)))
@@ -697,7 +790,7 @@ function train!(m::Surrogate, xks, E::CuMatrix{Float64}; epochs::Integer = 200, 
 end
 
 "Culling margins from held-out points: safety x the largest prediction error of each band."
-function calibrate!(m::Surrogate, xks, E::CuMatrix{Float64}; safety = 1.5)
+function calibrate!(m::Surrogate, xks, E::DenseCuMatrix{Float64}; safety = 1.5)
     x = xk_device(xks)
     margins = zeros(Float64, m.nout)
     check(ccall((:epb_mlp_calibrate, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, Int64,

@@ -95,6 +95,15 @@ EPB_API int epb_rset_destroy(epb_rset* rset);
 EPB_API int epb_fourier_phase(epb_ctx* ctx, const epb_rset* rset, const double* xk, int64_t nk,
                       double* phase);
 
+/* The same phase from the reference method's own arguments, fourier_phase!(phase, irvec_mat, xkmat)
+   (src/wannier/batched_fourier_core.jl:24-30): irvec_mat f64 (nr x 3, column-major, leading dimension
+   ld_r >= nr, the device matrix of _irvec_to_device_matrix, src/wannier/WannierObject.jl:148-152),
+   xkmat f64 (3 x nk, column stride ld_x >= 3), phase c128 (nr x nk, column stride ld_p >= nr); strided
+   column views such as P_mk[:, 1:nk_batch] (src/calculator/run_eph_over_k_and_kq.jl:821) pass their
+   parent's leading dimension. R . x is rounded as the reference's broadcast, (R1 x1 + R2 x2) + R3 x3. */
+EPB_API int epb_fourier_phase_mat(epb_ctx* ctx, const double* irvec_mat, int64_t ld_r, int64_t nr,
+                                  const double* xkmat, int64_t ld_x, int64_t nk, double* phase, int64_t ld_p);
+
 /* out[i, j] = sum_r op_r[i, r] exp(2 pi i R_r . x_j) for i < ndata; op_r c128 with leading
    dimension ld_op >= ndata; out c128 (ndata x nk). The phase is generated on the fly.
    Replaces: fourier_batched! / get_fourier_batched! (src/wannier/batched_fourier_core.jl:117-139,
@@ -145,6 +154,15 @@ EPB_API int epb_eph_apply_rotations(epb_ctx* ctx, const double* g, int64_t ldg, 
                             const double* uph, const double* omega, double* ep_out,
                             double* g2_out);
 
+/* Strided-batched complex FP64 GEMM: C_b = op(transA, A_b) * op(transB, B_b) for b < batch (alpha = 1,
+   beta = 0), op 'N' (X), 'T' (transpose) or 'C' (adjoint); A_b = A + b * strideA (c128 elements),
+   column-major with leading dimension lda (likewise B, C); C_b is m x n, the inner dimension k.
+   Replaces: batched_gemm! (src/common/gpu_utils.jl:71-78; CUDA method ext/ElectronPhononCUDAExt.jl:122-126,
+   CUBLAS.gemm_strided_batched!). */
+EPB_API int epb_batched_zgemm(epb_ctx* ctx, char transA, char transB, int64_t m, int64_t n, int64_t k,
+                              const double* A, int64_t lda, int64_t strideA, const double* B, int64_t ldb,
+                              int64_t strideB, double* C, int64_t ldc, int64_t strideC, int64_t batch);
+
 /* g(k, q) = ep_kR . phase (Fourier over Rp) followed by the rotations above. ep_kR c128
    ((nw nbk nm) x nr_ep) with leading dimension ld; phase c128 (nr_ep x nq).
    Replaces: get_eph_kR_to_kq_batched! (src/wannier_to_bloch_batched.jl:245-273). */
@@ -170,7 +188,9 @@ EPB_API int epb_window_filter(epb_ctx* ctx, const double* E, int64_t nw, int64_t
    device array held by every GPU that loads the library until exit: nk <= 16,777,216, larger nk
    returns EPB_ERR_ARG. Calls share that array, so calls that overlap on the GPU race; calls on one
    stream are safe. The first call on a device resolves the array's address with that device
-   current and should come before any stream capture. Results equal epb_window_filter's. */
+   current and should come before any stream capture; that address is kept for the life of the process,
+   so after a cudaDeviceReset of a device do not call it on that device again. Results equal
+   epb_window_filter's. */
 EPB_API int epb_window_filter_noalloc(void* stream, const double* E, int64_t nw, int64_t nk, double wmin,
                                       double wmax, int32_t* band_min, int32_t* band_max, int32_t* keep_idx,
                                       int64_t* nkeep_dev, double* nbelow);

@@ -149,3 +149,160 @@ def test_julia_struct_mirrors_match_the_header(tmp_path):
     for cname, fields in structs.items():
         for f, off in fields:
             assert got[(cname, f)] == off, (cname, f, off, got[(cname, f)])
+
+
+# ---------------------------------------------------------------------------------------------
+# Dispatch: the glue's methods must be the ones Julia selects at the reference's own call sites.
+# tests/golden/julia_call_sites.json (made by tests/golden/make_julia_call_sites.py from the reference)
+# lists every device-path call of an overridden method with each argument's kind; the CUDA extension's
+# method signatures are listed there too. CUDA.jl's array aliases order as
+#   CuArray < DenseCuArray (adds contiguous views, reshapes) < StridedCuArray (adds strided views)
+#   < AnyCuArray (adds any wrapper, e.g. a reshape of a view) < untyped.
+import json  # noqa: E402
+
+GOLD = os.path.join(ROOT, "tests", "golden", "julia_call_sites.json")
+ALIAS = {"CuArray": ("CuArray", None), "CuMatrix": ("CuArray", 2), "CuVector": ("CuArray", 1),
+         "DenseCuArray": ("DenseCuArray", None), "DenseCuMatrix": ("DenseCuArray", 2),
+         "DenseCuVector": ("DenseCuArray", 1), "StridedCuArray": ("StridedCuArray", None),
+         "StridedCuMatrix": ("StridedCuArray", 2), "StridedCuVector": ("StridedCuArray", 1),
+         "AnyCuArray": ("AnyCuArray", None), "AnyCuMatrix": ("AnyCuArray", 2), "AnyCuVector": ("AnyCuArray", 1)}
+FAMILY_OK = {"dev": {"CuArray", "DenseCuArray", "StridedCuArray", "AnyCuArray"},
+             "dense": {"DenseCuArray", "StridedCuArray", "AnyCuArray"},
+             "strided": {"StridedCuArray", "AnyCuArray"}, "rview": {"AnyCuArray"}}
+ELT = {"Int": "Int64", "Complex{Float64}": "ComplexF64", "Complex{T}": "ComplexF64", "T": None}
+
+
+def _norm_elt(e):
+    e = e.strip()
+    return ELT.get(e, e)
+
+
+def _family(kind):
+    if kind.startswith("dev:"):
+        return "dev"
+    if kind.startswith("view:"):
+        return kind.split(":")[3]
+    if kind.startswith("rview:"):
+        return "rview"
+    return kind
+
+
+def accepts(decl, kind):
+    """Does a Julia parameter declared `decl` (None = untyped) accept an argument of `kind`?"""
+    if decl is None or decl == "Any":
+        return True
+    decl = decl.strip()
+    m = re.fullmatch(r"Union\{(.*)\}", decl)
+    if m:
+        return any(accepts(d, kind) for d in split_top(m.group(1)))
+    if kind == "nothing":
+        return decl == "Nothing"
+    if kind in ("char", "int", "any", "range", "host-kvec", "itp"):
+        return {"char": {"Char"}, "int": {"Int", "Integer", "Int64"}, "itp": {
+            "ElectronPhonon.BatchedWannierInterpolator", "BatchedWannierInterpolator"}}.get(kind, set()) >= {decl} \
+            if kind in ("char", "int", "itp") else False
+    m = re.fullmatch(r"(\w+)(?:\{(.*)\})?", decl)
+    if not m or m.group(1) not in ALIAS:
+        return False
+    base, nd_alias = ALIAS[m.group(1)]
+    params = split_top(m.group(2)) if m.group(2) else []
+    elt = _norm_elt(params[0]) if params else None
+    nd = int(params[1]) if len(params) > 1 else nd_alias
+    fam = _family(kind)
+    if fam not in FAMILY_OK or base not in FAMILY_OK[fam]:
+        return False
+    _, k_elt, k_nd = kind.split(":")[:3]
+    return (elt is None or elt == _norm_elt(k_elt)) and (nd is None or nd == int(k_nd))
+
+
+def glue_methods():
+    """{name: [(positional [(name, decl)], keywords {name: decl})]} of `function ElectronPhonon.name(...)`."""
+    txt = open(JL).read()
+    out = {}
+    for m in re.finditer(r"^function ElectronPhonon\.([\w!]+)\(", txt, flags=re.M):
+        i, depth = m.end() - 1, 0
+        for j in range(i, len(txt)):
+            depth += txt[j] == "("
+            depth -= txt[j] == ")"
+            if depth == 0:
+                break
+        body = " ".join(txt[i + 1:j].split())
+        pos_txt, _, kw_txt = body.partition(";")
+        pos = []
+        for p in split_top(pos_txt):
+            nm, _, ty = p.partition("::")
+            pos.append((nm.strip(), ty.strip() or None))
+        kw = {}
+        for p in split_top(kw_txt):
+            lhs = p.split("=", 1)[0].strip()
+            nm, _, ty = lhs.partition("::")
+            kw[nm.strip()] = ty.strip() or None
+        out.setdefault(m.group(1), []).append((pos, kw))
+    return out
+
+
+def _sig_accepts(sig, pos_kinds, kw_kinds):
+    pos, kw = sig
+    if len(pos) != len(pos_kinds):
+        return False
+    if not all(accepts(d, k) for (_, d), k in zip(pos, pos_kinds)):
+        return False
+    return all(name in kw and accepts(kw[name], k) for name, k in kw_kinds.items())
+
+
+def test_call_site_fixture_matches_the_reference():
+    import pytest
+
+    if not os.path.isdir("/root/reference"):
+        pytest.skip("reference sources not present")
+    import sys
+
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_julia_call_sites as M
+
+    gold = json.load(open(GOLD))
+    assert M.build("/root/reference") == gold["sites"]
+    assert M.ext_methods("/root/reference") == gold["ext_methods"]
+
+
+def test_glue_methods_dispatch_at_every_reference_call_site():
+    """Each device-path call of an overridden method in the reference (views included) matches a glue method
+    by its declared types, so the reference loop reaches the library instead of the generic CPU method."""
+    gold = json.load(open(GOLD))
+    glue = glue_methods()
+    assert len(gold["sites"]) >= 12
+    for s in gold["sites"]:
+        sigs = glue.get(s["method"])
+        assert sigs, f"no glue method {s['method']} ({s['file']}:{s['line']})"
+        assert any(_sig_accepts(sig, s["positional_kinds"], s["keyword_kinds"]) for sig in sigs), \
+            f"{s['file']}:{s['line']} {s['method']}{tuple(s['positional_kinds'])} matches no glue method {sigs}"
+
+
+def test_glue_methods_accept_every_device_form_the_extension_accepts():
+    """For T = Float64, every device argument form (CuArray, contiguous view, strided view, reshape of a view)
+    that a CUDA-extension method accepts in a position, the glue method of the same name accepts too."""
+    gold = json.load(open(GOLD))
+    glue = glue_methods()
+    assert len(gold["ext_methods"]) >= 6
+    for e in gold["ext_methods"]:
+        sigs = [g for g in glue.get(e["method"], []) if len(g[0]) == len(e["positional"])]
+        assert sigs, f"no glue method {e['method']} with {len(e['positional'])} positional parameters"
+        pos, _ = sigs[0]
+        for (nm, edecl), (gnm, gdecl) in zip(e["positional"], pos):
+            # representative element type / rank: the extension's when it states one, else the glue's
+            ref = gdecl or edecl or "AnyCuArray{ComplexF64,3}"
+            mm = re.fullmatch(r"(?:Union\{Nothing,\s*)?(\w+)(?:\{(.*?)\})?\}?", edecl or ref)
+            params = split_top(mm.group(2)) if mm and mm.group(2) else []
+            gm = re.fullmatch(r"(?:Union\{Nothing,\s*)?(\w+)(?:\{(.*?)\})?\}?", ref)
+            gparams = split_top(gm.group(2)) if gm and gm.group(2) else []
+            elt = _norm_elt(params[0]) if params and _norm_elt(params[0]) else (
+                _norm_elt(gparams[0]) if gparams else "ComplexF64")
+            nd = params[1] if len(params) > 1 else (gparams[1] if len(gparams) > 1 else str(
+                ALIAS.get(gm.group(1) if gm else "", (None, None))[1] or 3))
+            if edecl in ("Int", "Char"):
+                kinds = ["int" if edecl == "Int" else "char"]
+            else:
+                kinds = [f"dev:{elt}:{nd}", f"view:{elt}:{nd}:dense", f"view:{elt}:{nd}:strided", f"rview:{elt}:{nd}"]
+            for k in kinds:
+                if accepts(edecl, k):
+                    assert accepts(gdecl, k), f"{e['method']} parameter {nm}: extension {edecl} takes {k}, glue {gdecl} does not"

@@ -170,3 +170,44 @@ def test_gpu_pass_graph_mode(gpu_lib):
         np.testing.assert_array_equal(host(out.g2sum), host(ref2.g2sum))
     finally:
         dm.ctx.set_graph_mode(False)
+
+
+@pytest.fixture(scope="module")
+def config2_full():
+    """The config-2 model at its own sizes (nw = 16, 12 modes, Re 9^3 = 729, Rp 5^3 = 125; the 4.48 GB
+    g(Re, Rp) generated on the host), uploaded once with the mixed operand planes, plus the CPU port's
+    result on 3 k x 256 q of it."""
+    from epb200 import pipeline
+
+    m = synth.config2_model(seed=2)
+    assert m.el_ham.irvec.shape[0] == 729 and m.epmat.irvec_next.shape[0] == 125 and m.nmodes == 12
+    xks = synth.random_kpoints(3, 61)
+    xqs = synth.random_kpoints(256, 62)
+    ref = cpu_pass.eph_pass_cpu(m, xks, xqs, sample_stride=3)
+    dm = pipeline.DeviceModel(m, mixed=True)
+    yield dm, xks, xqs, ref
+    dm.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_gpu_pass_config2_grids(gpu_lib, config2_full, prec):
+    """The pass at the headline configuration's own R grids (the FP16x2 kR->kq pre-scale grows with the Re
+    grid, so the small-grid tests above do not cover it): FP64 at the FP64 bars, mixed at |g|^2 <= 1e-5
+    per (k, q) block and band/q sums <= 1e-6, against the CPU port of the reference's batched path."""
+    from epb200 import pipeline
+    from epb200.batched import host
+
+    dm, xks, xqs, ref = config2_full
+    p = pipeline.PREC_FP64 if prec == "fp64" else pipeline.PREC_MIXED
+    r = pipeline.run_eph_over_k_and_q(dm, xks, xqs, prec=p, k_batch=2, sample_stride=3)
+    np.testing.assert_allclose(host(r.ek), ref["ek"], atol=1e-11 * np.abs(ref["ek"]).max())
+    np.testing.assert_allclose(host(r.omega), ref["omega"], rtol=1e-10)
+    err = _block_rel_err(host(r.g2_sample), ref["g2_sample"])
+    print(prec, "config-2 grids: max per-block |g|^2 normwise rel err", err)
+    if prec == "fp64":
+        np.testing.assert_allclose(host(r.g2sum), ref["g2sum"], rtol=1e-9)
+        assert err <= 1e-9
+    else:
+        np.testing.assert_allclose(host(r.g2sum), ref["g2sum"], rtol=1e-6)
+        assert err <= 1e-5
