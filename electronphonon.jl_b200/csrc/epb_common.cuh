@@ -137,6 +137,9 @@ struct epb_ctx {
   // created on first use
   cudaStream_t side = nullptr;
   cudaEvent_t side_ev[5] = {};
+  // rotation kernel of the mixed pass for nw = 16, nm = 12: 0 = warp tensor cores (mma.sync),
+  // 1 = FP32 CUDA cores; -1 = chosen by the autotuner
+  int rot_variant = 0;
 };
 
 struct epb_rset {

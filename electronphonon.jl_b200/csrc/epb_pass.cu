@@ -283,6 +283,14 @@ int epb_eph_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const
   return EPB_OK;
 }
 
+int epb_set_rotation_variant(epb_ctx* ctx, int variant) {
+  clear_error();
+  EPB_CHECK_ARG(ctx, "epb_set_rotation_variant: NULL ctx");
+  EPB_CHECK_ARG(variant >= -1 && variant <= 1, "epb_set_rotation_variant: variant must be -1, 0 or 1");
+  ctx->rot_variant = variant;
+  return EPB_OK;
+}
+
 int epb_set_graph_mode(epb_ctx* ctx, int on) {
   clear_error();
   EPB_CHECK_ARG(ctx, "epb_set_graph_mode: NULL ctx");

@@ -18,9 +18,10 @@
 // Kernel: persistent, one CTA per SM, 6 warps:
 //   warp 0      bulk-copy producer (one thread), STAGES-deep ring of operand stages
 //   warp 1      MMA issuer (one thread): 4 K-substeps x 6 products per stage into a TMEM
-//               accumulator of 128 lanes x NT columns; two accumulators alternate so the epilogue
-//               of one tile overlaps the MMAs of the next
-//   warps 2-5   epilogue: tcgen05.ld of the accumulator, FP32 stores to C
+//               accumulator of 128 lanes x NT columns, restarted for every 64-wide K chunk; two
+//               accumulators alternate by chunk so the epilogue of one chunk overlaps the next chunk's MMAs
+//   warps 2-5   epilogue: tcgen05.ld of each chunk's accumulators, added into FP32 registers with
+//               round-to-nearest (the tensor core's own accumulation truncates), FP32 stores to C
 // Every wait is bounded (clock64 budget); on timeout the kernel raises an error flag, drains its
 // own copies and MMAs, frees TMEM and returns (EPB_ERR_TIMEOUT on the host).
 #include <algorithm>
@@ -407,32 +408,44 @@ struct GemmCfg {
   static constexpr int TMEM_COLS = 4 * NT < 32 ? 32 : 4 * NT;
 };
 
-// Epilogue of one output tile (one thread per TMEM lane = tile row): C[row, col] = acc0 + acc1 (one FP32
-// rounding), times cscale when set. 64 columns of both accumulators are loaded per TMEM wait.
-template <int NT, int CBMAX = 64>
-__device__ __forceinline__ void epilogue_tile(const SplitGemmArgs& a, uint32_t tacc, float* cb, bool row_ok,
-                                              int64_t col0) {
-  constexpr int CB = NT < CBMAX ? NT : CBMAX;
-#pragma unroll 1
+// Accumulator promotion. The tensor core adds each K-step's products into its FP32 accumulator with
+// truncation (round toward zero), so a long K loop loses about half an ulp of the running sum per step
+// and every |C| comes out biased low: with the 92 K-steps of the 729-vector Re sum this measured a
+// -3.4e-6 relative bias of |g|^2 in the full pass. The kernels therefore restart the accumulator after
+// every 64-wide K chunk (four K-steps) and the epilogue adds each chunk's lead + correction
+// accumulators into FP32 registers with round-to-nearest, which leaves ~2e-7 (numpy emulation of the
+// truncating accumulator). `run` holds the tile row's NT running sums; the two TMEM buffers alternate by
+// chunk, so the MMAs of the next chunk overlap the epilogue of this one.
+template <int NT, int CB = 16>
+__device__ __forceinline__ void promote_chunk(uint32_t tacc, float (&run)[NT], bool first) {
+#pragma unroll
   for (int c0 = 0; c0 < NT; c0 += CB) {
     uint32_t r[2 * CB];
-#pragma unroll
-    for (int j = 0; j < CB; j += 16) {
-      tmem_ld16_nowait(tacc + c0 + j, r + j);
-      tmem_ld16_nowait(tacc + NT + c0 + j, r + CB + j);
+    if (CB == 16) {
+      tmem_ld16_nowait(tacc + c0, r);
+      tmem_ld16_nowait(tacc + NT + c0, r + 16);
+    } else {
+      tmem_ld8_nowait(tacc + c0, r);
+      tmem_ld8_nowait(tacc + NT + c0, r + 8);
     }
     tmem_wait_ld(r);
-    if (row_ok) {
-      float* p = cb + (col0 + c0) * a.ldc_n;
 #pragma unroll
-      for (int j = 0; j < CB; ++j, p += a.ldc_n) {
-        if (col0 + c0 + j < a.n_valid) {
-          const float val = __uint_as_float(r[j]) + __uint_as_float(r[CB + j]);
-          *p = a.cscale != 0.f ? val * a.cscale : val;
-        }
-      }
+    for (int j = 0; j < CB; ++j) {
+      const float v = __uint_as_float(r[j]) + __uint_as_float(r[CB + j]);
+      run[c0 + j] = first ? v : run[c0 + j] + v;
     }
   }
+}
+
+// C[row, col0 + j] = run[j] (times cscale when set) for the valid columns of one tile row.
+template <int NT>
+__device__ __forceinline__ void store_row(const SplitGemmArgs& a, const float (&run)[NT], float* cb, bool row_ok,
+                                          int64_t col0) {
+  if (!row_ok) return;
+  float* p = cb + col0 * a.ldc_n;
+#pragma unroll
+  for (int j = 0; j < NT; ++j, p += a.ldc_n)
+    if (col0 + j < a.n_valid) *p = a.cscale != 0.f ? run[j] * a.cscale : run[j];
 }
 
 template <bool BF16, int NPL, int NT>
@@ -531,17 +544,20 @@ __global__ void __launch_bounds__(192, 1) split_gemm_kernel(SplitGemmArgs a) {
     int s = 0;
     uint32_t ph = 0;
     bool ok = true;
-    int64_t u = 0;
-    for (int64_t t = blockIdx.x; t < total && ok; t += gridDim.x, ++u) {
-      const int b = (int)(u & 1);
-      const uint32_t use = (uint32_t)(u >> 1) & 1u;
-      if (!mbar_wait(&tempty[b], use ^ 1u, err, a.timeout)) break;
-      tc_fence_after();
-      // accumulator 0 (columns [0, NT)) takes the leading h*h product, accumulator 1 (columns
-      // [NT, 2NT)) all correction products: the tensor core aligns addends to the accumulator, so
-      // O(2^-16) corrections added onto the O(1) sum would lose their low bits.
-      const uint32_t dcol = tmem + b * 2 * NT;
-      for (int kc = 0; kc < a.KC; ++kc) {
+    int64_t sg = 0;  // K chunks issued so far: chunk sg goes to TMEM buffer sg & 1
+    for (int64_t t = blockIdx.x; t < total && ok; t += gridDim.x) {
+      for (int kc = 0; kc < a.KC; ++kc, ++sg) {
+        const int b = (int)(sg & 1);
+        const uint32_t use = (uint32_t)(sg >> 1) & 1u;
+        if (!mbar_wait(&tempty[b], use ^ 1u, err, a.timeout)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        // accumulator 0 (columns [0, NT)) takes the leading h*h product, accumulator 1 (columns
+        // [NT, 2NT)) all correction products: the tensor core aligns addends to the accumulator, so
+        // O(2^-16) corrections added onto the O(1) sum would lose their low bits.
+        const uint32_t dcol = tmem + b * 2 * NT;
         if (!mbar_wait(&full[s], ph, err, a.timeout)) {
           ok = false;
           break;
@@ -555,18 +571,18 @@ __global__ void __launch_bounds__(192, 1) split_gemm_kernel(SplitGemmArgs a) {
             const bool lead = Pr::a(pr) == 0 && Pr::b(pr) == 0;
             uint64_t ad = smem_desc_sw128(st + Pr::a(pr) * TILE_BYTES + sub * 32);
             uint64_t bd = smem_desc_sw128(st + NPL * TILE_BYTES + Pr::b(pr) * Cfg::B_SUB * Cfg::B_TILE + sub * 32);
-            // first MMA into each accumulator of the tile overwrites it
-            const bool first = kc == 0 && sub == 0 && (lead || pr == 0);
+            // the first MMA into each accumulator of the chunk overwrites it
+            const bool first = sub == 0 && (lead || pr == 0);
             mma_f16(dcol + (lead ? 0u : (uint32_t)NT), ad, bd, IDESC, first ? 0u : 1u);
           }
         }
         mma_commit(&empty[s]);
+        mma_commit(&tfull[b]);  // the chunk's accumulators are ready for promotion
         if (++s == STAGES) {
           s = 0;
           ph ^= 1u;
         }
       }
-      if (ok) mma_commit(&tfull[b]);
     }
     // all issued MMAs must retire before TMEM is released
     mma_commit(done);
@@ -577,22 +593,29 @@ __global__ void __launch_bounds__(192, 1) split_gemm_kernel(SplitGemmArgs a) {
     // ---------------- epilogue ----------------
     const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31
     const int row_in_tile = quarter * 32 + lane;
-    int64_t u = 0;
-    for (int64_t t = blockIdx.x; t < total; t += gridDim.x, ++u) {
-      const int b = (int)(u & 1);
-      const uint32_t use = (uint32_t)(u >> 1) & 1u;
-      bool okw = mbar_wait(&tfull[b], use, err, a.timeout);
-      if (!__all_sync(0xffffffffu, okw)) break;  // warp-uniform: the TMEM loads below are .sync.aligned
-      tc_fence_after();
+    int64_t sg = 0;
+    bool go = true;
+    for (int64_t t = blockIdx.x; t < total && go; t += gridDim.x) {
+      float run[NT];
+      for (int kc = 0; kc < a.KC; ++kc, ++sg) {
+        const int b = (int)(sg & 1);
+        const uint32_t use = (uint32_t)(sg >> 1) & 1u;
+        bool okw = mbar_wait(&tfull[b], use, err, a.timeout);
+        if (!__all_sync(0xffffffffu, okw)) {  // warp-uniform: the TMEM loads below are .sync.aligned
+          go = false;
+          break;
+        }
+        tc_fence_after();
+        promote_chunk<NT>(tmem + ((uint32_t)(quarter * 32) << 16) + b * 2 * NT, run, kc == 0);
+        tc_fence_before();
+        mbar_arrive(&tempty[b]);
+      }
+      if (!go) break;
       int64_t mt = a.m_fastest ? t % a.m_tiles : t / a.n_tiles;
       int64_t nt = a.m_fastest ? t / a.m_tiles : t % a.n_tiles;
       const int64_t batch = mt / a.m_tiles_per_batch;
       const int64_t row = (mt % a.m_tiles_per_batch) * 128 + row_in_tile;
-      float* cb = a.C + batch * a.c_batch_stride + row;
-      const bool row_ok = row < a.m_valid;
-      epilogue_tile<NT>(a, tmem + ((uint32_t)(quarter * 32) << 16) + b * 2 * NT, cb, row_ok, nt * NT);
-      tc_fence_before();
-      mbar_arrive(&tempty[b]);
+      store_row<NT>(a, run, a.C + batch * a.c_batch_stride + row, row < a.m_valid, nt * NT);
     }
   }
   tc_fence_before();
@@ -619,9 +642,9 @@ struct AresCfg {
 };
 
 template <bool BF16, int NPL, int NT>
-// (at most 85 registers: one CTA of this kernel leaves room on its SM for three CTAs of the FP32 Jacobi,
-// which the pass runs beside it on another stream)
-__global__ void __launch_bounds__(192, 4) split_gemm_ares_kernel(SplitGemmArgs a) {
+// (at most 168 registers, the promotion's running sums included: one CTA of this kernel leaves room
+// on its SM for two CTAs of the FP32 Jacobi, which the pass runs beside it on another stream)
+__global__ void __launch_bounds__(192, 2) split_gemm_ares_kernel(SplitGemmArgs a) {
   using Cfg = AresCfg<BF16, NPL, NT>;
   using G = GemmCfg<BF16, NPL, NT>;
   using Pr = Products<BF16, NPL>;
@@ -737,17 +760,17 @@ __global__ void __launch_bounds__(192, 4) split_gemm_ares_kernel(SplitGemmArgs a
       const int64_t n1 = n0 + npu < a.n_tiles ? n0 + npu : a.n_tiles;
       if (!mbar_wait(afull, (uint32_t)(uu & 1), err, a.timeout)) break;
       tc_fence_after();
-      for (int64_t nt = n0; nt < n1 && ok; ++nt, ++tc) {
-        const int b = (int)(tc & 1);
-        const uint32_t use = (uint32_t)(tc >> 1) & 1u;
-        if (!mbar_wait(&tempty[b], use ^ 1u, err, a.timeout)) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-        // accumulator 0 takes the leading h*h product, accumulator 1 the correction products
-        const uint32_t dcol = tmem + b * 2 * NT;
-        for (int kc = 0; kc < a.KC; ++kc) {
+      for (int64_t nt = n0; nt < n1 && ok; ++nt) {
+        for (int kc = 0; kc < a.KC; ++kc, ++tc) {  // chunk tc goes to TMEM buffer tc & 1 (promotion)
+          const int b = (int)(tc & 1);
+          const uint32_t use = (uint32_t)(tc >> 1) & 1u;
+          if (!mbar_wait(&tempty[b], use ^ 1u, err, a.timeout)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          // accumulator 0 takes the leading h*h product, accumulator 1 the correction products
+          const uint32_t dcol = tmem + b * 2 * NT;
           if (!mbar_wait(&full[s], ph, err, a.timeout)) {
             ok = false;
             break;
@@ -761,17 +784,17 @@ __global__ void __launch_bounds__(192, 4) split_gemm_ares_kernel(SplitGemmArgs a
               const bool lead = Pr::a(pr) == 0 && Pr::b(pr) == 0;
               uint64_t ad = smem_desc_sw128(abase + (kc * NPL + Pr::a(pr)) * TILE_BYTES + sub * 32);
               uint64_t bd = smem_desc_sw128(st + Pr::b(pr) * G::B_SUB * G::B_TILE + sub * 32);
-              const bool first = kc == 0 && sub == 0 && (lead || pr == 0);
+              const bool first = sub == 0 && (lead || pr == 0);
               mma_f16(dcol + (lead ? 0u : (uint32_t)NT), ad, bd, IDESC, first ? 0u : 1u);
             }
           }
           mma_commit(&empty[s]);
+          mma_commit(&tfull[b]);
           if (++s == STAGES) {
             s = 0;
             ph ^= 1u;
           }
         }
-        if (ok) mma_commit(&tfull[b]);
       }
       mma_commit(aempty);  // the A tile may be overwritten once this unit's MMAs have completed
     }
@@ -793,18 +816,22 @@ __global__ void __launch_bounds__(192, 4) split_gemm_ares_kernel(SplitGemmArgs a
       const int64_t row = (mt % a.m_tiles_per_batch) * 128 + row_in_tile;
       float* cb = a.C + batch * a.c_batch_stride + row;
       const bool row_ok = row < a.m_valid;
-      for (int64_t nt = n0; nt < n1; ++nt, ++tc) {
-        const int b = (int)(tc & 1);
-        const uint32_t use = (uint32_t)(tc >> 1) & 1u;
-        bool okw = mbar_wait(&tfull[b], use, err, a.timeout);
-        if (!__all_sync(0xffffffffu, okw)) {  // warp-uniform: the TMEM loads below are .sync.aligned
-          go = false;
-          break;
+      for (int64_t nt = n0; nt < n1 && go; ++nt) {
+        float run[NT];
+        for (int kc = 0; kc < a.KC; ++kc, ++tc) {
+          const int b = (int)(tc & 1);
+          const uint32_t use = (uint32_t)(tc >> 1) & 1u;
+          bool okw = mbar_wait(&tfull[b], use, err, a.timeout);
+          if (!__all_sync(0xffffffffu, okw)) {  // warp-uniform: the TMEM loads below are .sync.aligned
+            go = false;
+            break;
+          }
+          tc_fence_after();
+          promote_chunk<NT, 8>(tmem + ((uint32_t)(quarter * 32) << 16) + b * 2 * NT, run, kc == 0);
+          tc_fence_before();
+          mbar_arrive(&tempty[b]);
         }
-        tc_fence_after();
-        epilogue_tile<NT, 16>(a, tmem + ((uint32_t)(quarter * 32) << 16) + b * 2 * NT, cb, row_ok, nt * NT);
-        tc_fence_before();
-        mbar_arrive(&tempty[b]);
+        if (go) store_row<NT>(a, run, cb, row_ok, nt * NT);
       }
     }
   }
@@ -1300,7 +1327,8 @@ int mixed_rr_to_kR(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, con
 template <bool BF16, int NPL>
 __global__ void rr_rotate_pack_kernel(const float2* __restrict__ gk, const double2* __restrict__ uk, int nw,
                                       int nband, int nm, int nr_ep, int64_t nk, int64_t rows_pad_k, int64_t KC,
-                                      uint8_t* __restrict__ planes, int64_t plane_bytes, double scale = 1.0) {
+                                      uint8_t* __restrict__ planes, int64_t plane_bytes, double scale = 1.0,
+                                      unsigned* __restrict__ absmax = nullptr) {
   // FP32 products and sums (g is FP32; the planes hold at most 24 bits), u rounded to FP32 once per row
   const int nd = nw * nband * nm;  // complex rows r per k
   const int koff = (int)sin_offset(nr_ep);
@@ -1346,6 +1374,17 @@ __global__ void rr_rotate_pack_kernel(const float2* __restrict__ gk, const doubl
       im[e] = acc[e].y * sc;
       t[e] = -im[e];
     }
+    if (absmax) {  // max |Re G|, |Im G| of the written (scaled) values: bounds the kR->kq output
+      float mx = 0.f;
+#pragma unroll
+      for (int e = 0; e < 8; ++e) mx = fmaxf(mx, fmaxf(fabsf(re[e]), fabsf(im[e])));
+      if (__activemask() == 0xffffffffu) {  // whole warp: one atomic; a partial last warp: one per thread
+        for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if ((threadIdx.x & 31) == 0) atomicMax(absmax, __float_as_uint(mx));
+      } else {
+        atomicMax(absmax, __float_as_uint(mx));
+      }
+    }
     const int64_t row0 = k * rows_pad_k + 2 * r;
     // real row: [Re G | -Im G];  imaginary row: [Im G | Re G]
     store_split8_f32<BF16, NPL>(planes, plane_bytes, tiled_offset(row0, pc * 8, KC), re);
@@ -1359,6 +1398,23 @@ __global__ void c128_to_c64_kernel(const double2* __restrict__ in, float2* __res
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     out[i] = make_float2((float)in[i].x, (float)in[i].y);
 }
+
+// The same conversion, also raising *absmax (float bits) to the largest |Re|, |Im| converted.
+__global__ void c128_to_c64_absmax_kernel(const double2* __restrict__ in, float2* __restrict__ out, int64_t n,
+                                          unsigned* __restrict__ absmax) {
+  float mx = 0.f;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float2 v = make_float2((float)in[i].x, (float)in[i].y);
+    out[i] = v;
+    mx = fmaxf(mx, fmaxf(fabsf(v.x), fabsf(v.y)));
+  }
+  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(absmax, __float_as_uint(mx));
+}
+
+int rot_mma_launch(epb_ctx* ctx, const float* g, int64_t g_stride, const float2* ukq, const float2* uph,
+                   const float* inv2w, const unsigned* gmax, const unsigned* phmax, float gscale_inv, int nr_ep,
+                   int64_t nkb, int64_t nq, double* g2sum, double* sample, int64_t stride, int64_t nsamp);
 
 // ---- windowed kR->kq of the Boltzmann consumer on the tensor cores --------------------------------
 // A2 planes of G_k = g(k, Rp) u_k (nband columns of u_k) for nk points, one block of bte_rows_pad(nw, nband,
@@ -1706,6 +1762,7 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
   const size_t o_u32 = carve(8 * nw2 * kbi * nq);
   const size_t o_c2 = carve(4 * 2 * nd * kbi * nq);
   const size_t o_w2 = carve(4 * nm * nq);  // 1 / (2 omega), FP32
+  const size_t o_mx = carve(16);           // float bits: max |G| of the outer batch, max |u_ph|
   void* ws = nullptr;
   EPB_TRY(ws_get(ctx, EPB_WS_PASS1, off + 1024, &ws));
   uint8_t* base = (uint8_t*)(((uintptr_t)ws + 1023) & ~uintptr_t(1023));
@@ -1729,7 +1786,10 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
   const int e2 = std::max(-120, std::min(120, 14 - (int)std::ceil(std::log2(gbound))));
   const double a2_scale = std::ldexp(1.0, e2);
   const float a2_unscale = (float)std::ldexp(1.0, -e2);
-  c128_to_c64_kernel<<<grid_for(ctx, nm * nm * nq), 256, 0, ctx->stream>>>(uph, uph32, nm * nm * nq);
+  unsigned* gmax = (unsigned*)(base + o_mx);
+  unsigned* phmax = gmax + 1;
+  EPB_CUDA(cudaMemsetAsync(gmax, 0, 2 * sizeof(unsigned), ctx->stream));
+  c128_to_c64_absmax_kernel<<<grid_for(ctx, nm * nm * nq), 256, 0, ctx->stream>>>(uph, uph32, nm * nm * nq, phmax);
   EPB_LAUNCH_CHECK();
   float* inv2w = (float*)(base + o_w2);
   inv2w_kernel<<<grid_for(ctx, nm * nq), 256, 0, ctx->stream>>>(omega, inv2w, nm * nq);
@@ -1763,10 +1823,12 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
     // k-leg rotation by u_k fused into the A2 packing of the kR->kq GEMM
     {
       const int64_t total = nko * nd * (sin_offset(m->nr_ep) / 8);
+      // the previous outer batch's rotations (readers of gmax) precede this on the stream
+      EPB_CUDA(cudaMemsetAsync(gmax, 0, sizeof(unsigned), ctx->stream));
       prof_begin(ctx, EPB_PROF_RR_ROT);
       rr_rotate_pack_kernel<false, 2><<<grid_for(ctx, total), 256, 0, ctx->stream>>>(
           (const float2*)C0, Hk, (int)nw, (int)nw, (int)nm, (int)m->nr_ep, nko, rows_pad_k, KC_ep, A2.p, A2.plane_bytes,
-          a2_scale);
+          a2_scale, gmax);
       prof_end(ctx);
       EPB_LAUNCH_CHECK();
     }
@@ -1818,6 +1880,13 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
             g2_sample ? g2_sample + (ko + ki) * nsamp * nd : nullptr, sample_stride, nsamp);
         prof_end(ctx);
         EPB_LAUNCH_CHECK();
+      } else if (ctx->rot_variant == 0) {
+        prof_begin(ctx, EPB_PROF_ROT);
+        const int st = rot_mma_launch(ctx, C2, 2 * nd, U32, uph32, inv2w, gmax, phmax, a2_unscale, (int)m->nr_ep, nki,
+                                      nq, g2sum + nm * (ko + ki), g2_sample ? g2_sample + (ko + ki) * nsamp * nd : nullptr,
+                                      sample_stride, nsamp);
+        prof_end(ctx);
+        EPB_TRY(st);
       } else {
         int64_t nblk = np;
         constexpr int RS = RotSmem<16, 12>::TOTAL;

@@ -62,6 +62,7 @@ SIGNATURES = {
     "epb_model_create": [P, P, I64, P, I64, P, P, I64, P, I64, P, P, I64, I32, C.POINTER(P)],
     "epb_model_destroy": [P],
     "epb_eph_pass": [P, P, P, I64, P, I64, I32, I64, I64, P, P, P, P, P],
+    "epb_set_rotation_variant": [P, I32],
     "epb_bands_create": [P, P, I64, P, I64, C.POINTER(P)],
     "epb_bands_destroy": [P],
     "epb_bands_eigvals": [P, P, P, I64, P, I32],
@@ -221,6 +222,10 @@ class Context:
 
     def synchronize(self):
         check(lib().epb_synchronize(self.h))
+
+    def set_rotation_variant(self, variant):
+        """Rotation kernel of the mixed pass (nw = 16, nm = 12): 0 warp tensor cores, 1 FP32, -1 autotuned."""
+        check(lib().epb_set_rotation_variant(self.h, int(variant)))
 
     def set_graph_mode(self, on=True):
         """Capture epb_eph_pass as a CUDA graph and replay it for repeated calls on the same buffers."""

@@ -339,6 +339,11 @@ EPB_API int epb_model_destroy(epb_model* model);
    (the production loop refills the same device buffers). Ignored on the legacy default stream and
    while profiling. */
 EPB_API int epb_set_graph_mode(epb_ctx* ctx, int on);
+/* Rotation kernel of the mixed pass for nw = 16, nm = 12 (the fused rotation of
+   ext/ElectronPhononCUDAExt.jl:146-201 and its two-GEMM fallback): 0 = warp-level tensor cores
+   (default), 1 = FP32 CUDA cores, -1 = timed by the pass's autotuner on its first call per shape.
+   Both give |g|^2 within the mixed path's 1e-5 per-block bar of the FP64 pass. */
+EPB_API int epb_set_rotation_variant(epb_ctx* ctx, int variant);
 EPB_API int epb_eph_pass(epb_ctx* ctx, epb_model* model, const double* xk, int64_t nk, const double* xq,
                          int64_t nq, int prec, int64_t k_batch, int64_t sample_stride, double* ek_out,
                          double* omega_out, double* g2sum_out, double* g2_sample, int64_t* stats_host);

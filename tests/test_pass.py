@@ -57,10 +57,12 @@ def _block_rel_err(s, sr):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("rot", [0, 1])
 @pytest.mark.parametrize("nk,nq,kb", [(5, 64, 2), (3, 200, 3)])
-def test_gpu_pass_mixed(gpu_lib, nk, nq, kb):
+def test_gpu_pass_mixed(gpu_lib, nk, nq, kb, rot):
     """Mixed-precision pass vs the FP64 CPU port: |g|^2 normwise error per (k, q) block <= 1e-5,
-    band/q sums <= 1e-6, electron energies (FP64 k side) and phonons at the FP64 level."""
+    band/q sums <= 1e-6, electron energies (FP64 k side) and phonons at the FP64 level; both rotation
+    kernels (0: warp tensor cores, 1: FP32 CUDA cores)."""
     from epb200 import pipeline
     from epb200.batched import host
 
@@ -68,7 +70,11 @@ def test_gpu_pass_mixed(gpu_lib, nk, nq, kb):
     xks = synth.random_kpoints(nk, 5)
     xqs = synth.random_kpoints(nq, 6)
     dm = pipeline.DeviceModel(m, mixed=True)
-    r = pipeline.run_eph_over_k_and_q(dm, xks, xqs, prec=pipeline.PREC_MIXED, k_batch=kb, sample_stride=5)
+    dm.ctx.set_rotation_variant(rot)
+    try:
+        r = pipeline.run_eph_over_k_and_q(dm, xks, xqs, prec=pipeline.PREC_MIXED, k_batch=kb, sample_stride=5)
+    finally:
+        dm.ctx.set_rotation_variant(0)
     ref = cpu_pass.eph_pass_cpu(m, xks, xqs, sample_stride=5)
     np.testing.assert_allclose(host(r.ek), ref["ek"], atol=1e-11 * np.abs(ref["ek"]).max())
     np.testing.assert_allclose(host(r.omega), ref["omega"], rtol=1e-10)
@@ -190,7 +196,7 @@ def config2_full():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("prec", ["fp64", "mixed", "mixed-fp32rot"])
 def test_gpu_pass_config2_grids(gpu_lib, config2_full, prec):
     """The pass at the headline configuration's own R grids (the FP16x2 kR->kq pre-scale grows with the Re
     grid, so the small-grid tests above do not cover it): FP64 at the FP64 bars, mixed at |g|^2 <= 1e-5
@@ -200,7 +206,11 @@ def test_gpu_pass_config2_grids(gpu_lib, config2_full, prec):
 
     dm, xks, xqs, ref = config2_full
     p = pipeline.PREC_FP64 if prec == "fp64" else pipeline.PREC_MIXED
-    r = pipeline.run_eph_over_k_and_q(dm, xks, xqs, prec=p, k_batch=2, sample_stride=3)
+    dm.ctx.set_rotation_variant(1 if prec == "mixed-fp32rot" else 0)
+    try:
+        r = pipeline.run_eph_over_k_and_q(dm, xks, xqs, prec=p, k_batch=2, sample_stride=3)
+    finally:
+        dm.ctx.set_rotation_variant(0)
     np.testing.assert_allclose(host(r.ek), ref["ek"], atol=1e-11 * np.abs(ref["ek"]).max())
     np.testing.assert_allclose(host(r.omega), ref["omega"], rtol=1e-10)
     err = _block_rel_err(host(r.g2_sample), ref["g2_sample"])
