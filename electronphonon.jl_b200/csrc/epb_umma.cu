@@ -416,17 +416,19 @@ struct GemmCfg {
 // accumulators into FP32 registers with round-to-nearest, which leaves ~2e-7 (numpy emulation of the
 // truncating accumulator). `run` holds the tile row's NT running sums; the two TMEM buffers alternate by
 // chunk, so the MMAs of the next chunk overlap the epilogue of this one.
-template <int NT, int CB = 16>
+// NT running sums of one tile row: columns [0, NT) of the lead accumulator at tacc and of the correction
+// accumulator ACC_STRIDE columns further.
+template <int NT, int CB = 16, int ACC_STRIDE = NT>
 __device__ __forceinline__ void promote_chunk(uint32_t tacc, float (&run)[NT], bool first) {
 #pragma unroll
   for (int c0 = 0; c0 < NT; c0 += CB) {
     uint32_t r[2 * CB];
     if (CB == 16) {
       tmem_ld16_nowait(tacc + c0, r);
-      tmem_ld16_nowait(tacc + NT + c0, r + 16);
+      tmem_ld16_nowait(tacc + ACC_STRIDE + c0, r + 16);
     } else {
       tmem_ld8_nowait(tacc + c0, r);
-      tmem_ld8_nowait(tacc + NT + c0, r + 8);
+      tmem_ld8_nowait(tacc + ACC_STRIDE + c0, r + 8);
     }
     tmem_wait_ld(r);
 #pragma unroll
@@ -630,8 +632,10 @@ __global__ void __launch_bounds__(192, 1) split_gemm_kernel(SplitGemmArgs a) {
 // so each 128 x 128 output tile costs one B tile of L2 traffic instead of an A and a B tile (the
 // kR->kq GEMM of the pass, K' = 256, is bound by that feed). A has its own full / empty barrier pair:
 // the MMA thread commits `a_empty` after the unit's last MMA, the producer waits on it before it
-// overwrites A. Same products, accumulators and epilogue as split_gemm_kernel; no grouped mode.
+// overwrites A. Same products, accumulators and promotion as split_gemm_kernel, with eight epilogue warps
+// (two per TMEM lane quarter, each holding half of a row's running sums); no grouped mode.
 constexpr int ARES_KC = 4, ARES_STAGES = 2;
+constexpr int ARES_THREADS = 320;  // producer, MMA issuer, 8 epilogue warps (two per TMEM lane quarter)
 template <bool BF16, int NPL, int NT>
 struct AresCfg {
   using G = GemmCfg<BF16, NPL, NT>;
@@ -642,9 +646,10 @@ struct AresCfg {
 };
 
 template <bool BF16, int NPL, int NT>
-// (at most 168 registers, the promotion's running sums included: one CTA of this kernel leaves room
-// on its SM for two CTAs of the FP32 Jacobi, which the pass runs beside it on another stream)
-__global__ void __launch_bounds__(192, 2) split_gemm_ares_kernel(SplitGemmArgs a) {
+// (8 epilogue warps, each promoting half of a tile row's columns: 128 registers, no spills; one CTA of this
+// kernel leaves room on its SM for one CTA of the FP32 Jacobi, which the pass runs beside it on another
+// stream)
+__global__ void __launch_bounds__(ARES_THREADS, 1) split_gemm_ares_kernel(SplitGemmArgs a) {
   using Cfg = AresCfg<BF16, NPL, NT>;
   using G = GemmCfg<BF16, NPL, NT>;
   using Pr = Products<BF16, NPL>;
@@ -672,7 +677,7 @@ __global__ void __launch_bounds__(192, 2) split_gemm_ares_kernel(SplitGemmArgs a
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&tfull[b], 1);
-      mbar_init(&tempty[b], 128);
+      mbar_init(&tempty[b], ARES_THREADS - 64);
     }
     mbar_init(afull, 1);
     mbar_init(aempty, 1);
@@ -807,6 +812,8 @@ __global__ void __launch_bounds__(192, 2) split_gemm_ares_kernel(SplitGemmArgs a
     // ---------------- epilogue ----------------
     const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31
     const int row_in_tile = quarter * 32 + lane;
+    const int half = (warp - 2) >> 2;  // two warps per lane quarter: columns [half NT/2, half NT/2 + NT/2)
+    constexpr int NH = NT / 2;
     int64_t tc = 0;
     bool go = true;
     for (int64_t u = blockIdx.x; u < nunits && go; u += gridDim.x) {
@@ -817,7 +824,7 @@ __global__ void __launch_bounds__(192, 2) split_gemm_ares_kernel(SplitGemmArgs a
       float* cb = a.C + batch * a.c_batch_stride + row;
       const bool row_ok = row < a.m_valid;
       for (int64_t nt = n0; nt < n1 && go; ++nt) {
-        float run[NT];
+        float run[NH];
         for (int kc = 0; kc < a.KC; ++kc, ++tc) {
           const int b = (int)(tc & 1);
           const uint32_t use = (uint32_t)(tc >> 1) & 1u;
@@ -827,11 +834,11 @@ __global__ void __launch_bounds__(192, 2) split_gemm_ares_kernel(SplitGemmArgs a
             break;
           }
           tc_fence_after();
-          promote_chunk<NT, 8>(tmem + ((uint32_t)(quarter * 32) << 16) + b * 2 * NT, run, kc == 0);
+          promote_chunk<NH, 16, NT>(tmem + ((uint32_t)(quarter * 32) << 16) + b * 2 * NT + half * NH, run, kc == 0);
           tc_fence_before();
           mbar_arrive(&tempty[b]);
         }
-        if (go) store_row<NT>(a, run, cb, row_ok, nt * NT);
+        if (go) store_row<NH>(a, run, cb, row_ok, nt * NT + half * NH);
       }
     }
   }
@@ -898,7 +905,7 @@ static int launch_split_gemm_ares(epb_ctx* ctx, SplitGemmArgs& a) {
   const int64_t units = a.m_tiles * cdiv(a.n_tiles, a.n_per_unit);
   if (units == 0) return EPB_OK;
   const unsigned grid = (unsigned)(units < ctx->sm_count ? units : ctx->sm_count);
-  split_gemm_ares_kernel<BF16, NPL, NT><<<grid, 192, Cfg::SMEM, ctx->stream>>>(a);
+  split_gemm_ares_kernel<BF16, NPL, NT><<<grid, ARES_THREADS, Cfg::SMEM, ctx->stream>>>(a);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
 }
