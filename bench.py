@@ -429,7 +429,12 @@ def run_epb(args):
             "dtype": ("fp16x2 (kR->kq, 3 products) + bf16x3 (RR->kR, H(k+q), 6 products) on tcgen05, f32 "
                       "accumulate / rotations / Jacobi, f64 refinement and k, q sides") if mixed else "f64",
             "data": "synthetic (seeded generator; random-init Wannier model of the config-2 shape)",
-            "config": dict(config_dict(args, prec_name), k_batch_used=kb_used), "roofline": roof,
+            "config": dict(config_dict(args, prec_name), k_batch_used=kb_used,
+                           autotuned={"k_batch": kb_used, "rotation": {0: "warp tensor cores (mma.sync)",
+                                                                      1: "FP32 CUDA cores"}.get(out_holder[0].rot_variant, "fp64"),
+                                      "kq_gemm": {1: "A-resident tcgen05", 0: "streamed tcgen05"}.get(
+                                          out_holder[0].kq_form, "fp64"),
+                                      "table": dm.ctx.tune_text()}), "roofline": roof,
             "roofline_compute": roof_compute,
             "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": clocks, "impl": "epb", "profile_one_pass": profile}

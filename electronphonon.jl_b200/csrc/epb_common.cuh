@@ -130,7 +130,7 @@ struct epb_ctx {
   size_t prof_used = 0;
   double prof_ms[EPB_PROF_N] = {};
   bool graph_mode = false;  // epb_eph_pass: capture and replay as a CUDA graph (epb_set_graph_mode)
-  // autotuner results: shape key -> chosen parameter (epb_eph_pass inner k batch)
+  // autotuner results: shape key -> chosen parameter (epb_tune.cu lists the keys)
   std::vector<std::pair<std::string, int64_t>> tuned;
   int64_t prof_cnt[EPB_PROF_N] = {};
   // side stream of the mixed pass (the kR->kq GEMM runs beside the eigensolvers) and its events,
@@ -138,8 +138,11 @@ struct epb_ctx {
   cudaStream_t side = nullptr;
   cudaEvent_t side_ev[5] = {};
   // rotation kernel of the mixed pass for nw = 16, nm = 12: 0 = warp tensor cores (mma.sync),
-  // 1 = FP32 CUDA cores; -1 = chosen by the autotuner
-  int rot_variant = 0;
+  // 1 = FP32 CUDA cores; -1 = the tuning table's choice (timed when epb_eph_pass autotunes), else 0
+  int rot_variant = -1;
+  // the choices of the pass in progress (set by epb_eph_pass): rotation kernel, A-resident kR->kq GEMM
+  int cur_rot = 0, cur_kq_ares = 1;
+  // measured tuning choices (shape key -> value), see epb_tune.cu
 };
 
 struct epb_rset {
@@ -161,9 +164,10 @@ struct PassKey {
   int prec = -1;
   int64_t k_batch = 0, stride = 0;
   const void *ek = nullptr, *om = nullptr, *g2 = nullptr, *samp = nullptr;
+  int rot = 0, kq = 1;  // rotation kernel and kR->kq form the graph was captured with
   bool operator==(const PassKey& o) const {
     return xk == o.xk && nk == o.nk && xq == o.xq && nq == o.nq && prec == o.prec && k_batch == o.k_batch &&
-           stride == o.stride && ek == o.ek && om == o.om && g2 == o.g2 && samp == o.samp;
+           stride == o.stride && ek == o.ek && om == o.om && g2 == o.g2 && samp == o.samp && rot == o.rot && kq == o.kq;
   }
 };
 struct PassGraph {

@@ -181,3 +181,138 @@ int epb_fill_iqs(epb_ctx* ctx, const int64_t* xkq_int, int64_t nkq, const int64_
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// FilteredStates on the device (src/band_states.jl:85-121, 283-287): from the per-k in-window band ranges
+// of the window filter, the states ordered by k then band (state i = 1, 2, ...), their k and band indices,
+// and the index map in the physical-band form the device calculators read, indmap[b - 1, k] = i for the
+// states, 0 elsewhere (the reference builds it on the host and uploads it, _indmap_to_device). One pass
+// counts the states per k with a block-local scan, one block scans the block totals, one pass writes.
+namespace epb {
+
+__device__ __forceinline__ int fs_count(const int32_t* bmin, const int32_t* bmax, int64_t k, int64_t nk, int nw) {
+  if (k >= nk) return 0;
+  const int lo = bmin[k], hi = bmax[k];
+  return (lo >= 1 && hi >= lo && hi <= nw) ? hi - lo + 1 : 0;
+}
+
+// exclusive prefix of v over the block (W_THREADS threads); returns it, and the block total in *tot
+__device__ __forceinline__ int64_t block_excl_scan(int v, int64_t* tot) {
+  __shared__ int64_t wsum[W_THREADS / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int incl = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int64_t s = 0;
+    for (int w = 0; w < W_THREADS / 32; ++w) {
+      const int64_t t = wsum[w];
+      wsum[w] = s;
+      s += t;
+    }
+    *tot = s;  // wsum[w] now holds the exclusive warp offsets
+  }
+  __syncthreads();
+  return wsum[warp] + (incl - v);
+}
+
+__global__ void fs_count_kernel(const int32_t* __restrict__ bmin, const int32_t* __restrict__ bmax, int64_t nk,
+                                int nw, int64_t* __restrict__ block_tot, int* __restrict__ minmax) {
+  const int64_t k = (int64_t)blockIdx.x * W_THREADS + threadIdx.x;
+  const int c = fs_count(bmin, bmax, k, nk, nw);
+  __shared__ int64_t tot;
+  block_excl_scan(c, &tot);
+  if (c > 0) {
+    atomicMin(&minmax[0], bmin[k]);
+    atomicMax(&minmax[1], bmax[k]);
+  }
+  if (threadIdx.x == 0) block_tot[blockIdx.x] = tot;
+}
+
+// single block: exclusive scan of the block totals (in place); counts[0] = number of states,
+// counts[1] = nband_ignore, counts[2] = nband of the compact map (0, 0 when no state is kept)
+__global__ void fs_scan_kernel(int64_t* __restrict__ block_tot, int64_t nblocks, const int* __restrict__ minmax,
+                               int64_t* __restrict__ counts) {
+  __shared__ int64_t carry;
+  __shared__ int64_t buf[W_THREADS];
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int64_t base = 0; base < nblocks; base += W_THREADS) {
+    const int64_t i = base + threadIdx.x;
+    const int64_t v = i < nblocks ? block_tot[i] : 0;
+    buf[threadIdx.x] = v;
+    __syncthreads();
+    for (int off = 1; off < W_THREADS; off <<= 1) {
+      const int64_t t = threadIdx.x >= off ? buf[threadIdx.x - off] : 0;
+      __syncthreads();
+      buf[threadIdx.x] += t;
+      __syncthreads();
+    }
+    if (i < nblocks) block_tot[i] = carry + buf[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == W_THREADS - 1) carry += buf[W_THREADS - 1];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    counts[0] = carry;
+    const bool any = carry > 0;
+    counts[1] = any ? (int64_t)minmax[0] - 1 : 0;
+    counts[2] = any ? (int64_t)minmax[1] - (int64_t)minmax[0] + 1 : 0;
+  }
+}
+
+__global__ void fs_write_kernel(const int32_t* __restrict__ bmin, const int32_t* __restrict__ bmax, int64_t nk,
+                                int nw, const int64_t* __restrict__ block_off, int64_t* __restrict__ indmap,
+                                int64_t* __restrict__ iks, int64_t* __restrict__ ibands, int64_t cap) {
+  const int64_t k = (int64_t)blockIdx.x * W_THREADS + threadIdx.x;
+  const int c = fs_count(bmin, bmax, k, nk, nw);
+  __shared__ int64_t tot;
+  const int64_t base = block_off[blockIdx.x] + block_excl_scan(c, &tot);  // 0-based index of k's first state
+  if (k >= nk) return;
+  const int lo = c > 0 ? bmin[k] : 1;
+  int64_t* col = indmap + k * (int64_t)nw;
+  for (int b = 1; b <= nw; ++b) col[b - 1] = (c > 0 && b >= lo && b < lo + c) ? base + (b - lo) + 1 : 0;
+  for (int j = 0; j < c; ++j) {
+    const int64_t i = base + j;
+    if (i < cap) {
+      if (iks) iks[i] = k + 1;
+      if (ibands) ibands[i] = lo + j;
+    }
+  }
+}
+
+}  // namespace epb
+
+extern "C" int epb_filtered_states(epb_ctx* ctx, const int32_t* band_min, const int32_t* band_max, int64_t nw,
+                                   int64_t nk, int64_t* indmap, int64_t* iks, int64_t* ibands, int64_t capacity,
+                                   int64_t* counts_dev) {
+  using namespace epb;
+  clear_error();
+  EPB_CHECK_ARG(ctx && counts_dev, "epb_filtered_states: NULL argument");
+  EPB_CHECK_ARG(nw >= 1 && nw <= 4096 && nk >= 0 && capacity >= 0, "epb_filtered_states: bad sizes");
+  EPB_CHECK_ARG(nk == 0 || (band_min && band_max && indmap), "epb_filtered_states: NULL buffer");
+  EPB_TRY(make_current(ctx));
+  if (nk == 0) {
+    EPB_CUDA(cudaMemsetAsync(counts_dev, 0, 3 * sizeof(int64_t), ctx->stream));
+    return EPB_OK;
+  }
+  const int64_t nblocks = cdiv(nk, W_THREADS);
+  void* ws = nullptr;
+  EPB_TRY(ws_get(ctx, EPB_WS_FLAGS, 64 + sizeof(int64_t) * nblocks, &ws));
+  int* minmax = (int*)ws;
+  int64_t* bt = (int64_t*)((char*)ws + 64);
+  EPB_CUDA(cudaMemsetAsync(minmax, 0x7f, sizeof(int), ctx->stream));  // min band: 0x7f7f7f7f
+  EPB_CUDA(cudaMemsetAsync(minmax + 1, 0, sizeof(int), ctx->stream));   // max band
+  fs_count_kernel<<<(unsigned)nblocks, W_THREADS, 0, ctx->stream>>>(band_min, band_max, nk, (int)nw, bt, minmax);
+  EPB_LAUNCH_CHECK();
+  fs_scan_kernel<<<1, W_THREADS, 0, ctx->stream>>>(bt, nblocks, minmax, counts_dev);
+  EPB_LAUNCH_CHECK();
+  fs_write_kernel<<<(unsigned)nblocks, W_THREADS, 0, ctx->stream>>>(band_min, band_max, nk, (int)nw, bt, indmap, iks,
+                                                                    ibands, capacity);
+  EPB_LAUNCH_CHECK();
+  return EPB_OK;
+}

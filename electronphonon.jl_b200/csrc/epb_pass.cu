@@ -30,6 +30,8 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
                const double2* uph, const double* omega, double* ek_out, double* g2sum, double* g2_sample,
                int64_t sample_stride, int64_t kbi_max, bool defer_checks);
 int split_gemm_check(epb_ctx* ctx);
+bool tune_lookup(const std::vector<std::pair<std::string, int64_t>>& kv, const std::string& key, int64_t* value);
+void tune_store(std::vector<std::pair<std::string, int64_t>>& kv, const std::string& key, int64_t value);
 int mixed_model_prepare(epb_ctx* ctx, epb_model* m);
 void mixed_model_free(epb_model* m);
 
@@ -167,55 +169,127 @@ static int eph_pass_run(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk
                         int prec, int64_t k_batch, int64_t sample_stride, double* ek_out, double* omega_out,
                         double* g2sum_out, double* g2_sample, int64_t* stats_host, bool defer_checks = false);
 
-// Autotuner of the pass's inner k batch (the k+q eigensolve / kR->kq / rotation batch): times each
-// candidate on the first min(nk, 64) k against the caller's q list (CUDA events on the context stream,
-// one untimed run first), keeps the fastest per (nw, nm, nq, prec) in the context. The trial passes
-// write the caller's outputs for those k, which the real pass then rewrites.
-static int tune_k_batch(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double* xq, int64_t nq, int prec,
-                        double* ek_out, double* omega_out, double* g2sum_out, int64_t* chosen) {
+// Choices of one pass: inner k batch, rotation kernel of the mixed pass (0 warp tensor cores, 1 FP32 CUDA
+// cores) and kR->kq GEMM form (1 A-resident, 0 streamed operands). The mixed pass reads the last two from
+// ctx->cur_rot / ctx->cur_kq_ares.
+struct PassChoice {
+  int64_t kb = 16;
+  int rot = 0;
+  int kq = 1;
+};
+
+static std::string pass_key(const char* what, const epb_model* m, int64_t nq, int prec) {
   char key[128];
-  snprintf(key, sizeof(key), "pass_kb/%lld/%lld/%lld/%d", (long long)m->nw, (long long)m->nm, (long long)nq, prec);
-  for (auto& kv : ctx->tuned)
-    if (kv.first == key) {
-      *chosen = kv.second;
+  snprintf(key, sizeof(key), "pass_%s/%lld/%lld/%lld/%d", what, (long long)m->nw, (long long)m->nm, (long long)nq,
+           prec);
+  return key;
+}
+// the mixed pass has a second rotation kernel only for the register-tiled shape, and an A-resident kR->kq
+// only for K' = 2 round_up(nr_ep, 8) <= 256
+static bool rot_alternatives(const epb_model* m, int prec) { return prec == EPB_PREC_MIXED && m->nw == 16 && m->nm == 12; }
+static bool kq_alternatives(const epb_model* m, int prec) { return prec == EPB_PREC_MIXED && m->nr_ep <= 128; }
+
+// The choices from the context's table, else the defaults (a forced rotation kernel wins).
+static PassChoice pass_choice(const epb_ctx* ctx, const epb_model* m, int64_t nq, int prec, int64_t k_batch) {
+  PassChoice c;
+  int64_t v;
+  c.kb = k_batch > 0 ? k_batch : (tune_lookup(ctx->tuned, pass_key("kb", m, nq, prec), &v) ? v : 16);
+  c.rot = ctx->rot_variant >= 0 ? ctx->rot_variant : (tune_lookup(ctx->tuned, pass_key("rot", m, nq, prec), &v) ? (int)v : 0);
+  c.kq = tune_lookup(ctx->tuned, pass_key("kq", m, nq, prec), &v) ? (int)v : 1;
+  return c;
+}
+
+// Autotuner of the pass (k_batch <= 0): times the candidates on the first min(nk, 64) k against the
+// caller's q list (CUDA events on the context stream, one untimed run before each timed one) and keeps the
+// fastest per (nw, nm, nq, prec) in the context's table: first the inner k batch (4, 8, 16, 32) -- the
+// k+q eigensolve / kR->kq / rotation batch --, then with it the rotation kernel (unless one is forced) and
+// the kR->kq GEMM form. Choices already in the table (measured earlier or loaded with epb_tune_import) are
+// not timed again. The trial passes write the caller's outputs for those k; the real pass rewrites them.
+static int tune_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double* xq, int64_t nq, int prec,
+                     double* ek_out, double* omega_out, double* g2sum_out, PassChoice* out) {
+  PassChoice c = pass_choice(ctx, m, nq, prec, 0);
+  int64_t v;
+  const std::string kkb = pass_key("kb", m, nq, prec), krot = pass_key("rot", m, nq, prec),
+                    kkq = pass_key("kq", m, nq, prec);
+  const bool need_kb = !tune_lookup(ctx->tuned, kkb, &v);
+  const bool need_rot = ctx->rot_variant < 0 && rot_alternatives(m, prec) && !tune_lookup(ctx->tuned, krot, &v);
+  const bool need_kq = kq_alternatives(m, prec) && !tune_lookup(ctx->tuned, kkq, &v);
+  if (need_kb || need_rot || need_kq) {
+    const int64_t ns = std::min<int64_t>(nk, 64);
+    cudaEvent_t e0, e1;
+    EPB_CUDA(cudaEventCreate(&e0));
+    EPB_CUDA(cudaEventCreate(&e1));
+    // time one candidate; <0 when it does not fit (out of memory), the error status otherwise
+    auto trial = [&](const PassChoice& t, float* ms) -> int {
+      ctx->cur_rot = t.rot;
+      ctx->cur_kq_ares = t.kq;
+      int st = eph_pass_run(ctx, m, xk, ns, xq, nq, prec, t.kb, 1, ek_out, omega_out, g2sum_out, nullptr, nullptr);
+      if (st == EPB_OK) {
+        cudaEventRecord(e0, ctx->stream);
+        st = eph_pass_run(ctx, m, xk, ns, xq, nq, prec, t.kb, 1, ek_out, omega_out, g2sum_out, nullptr, nullptr);
+        cudaEventRecord(e1, ctx->stream);
+      }
+      if (st != EPB_OK) return st;
+      cudaEventSynchronize(e1);
+      cudaEventElapsedTime(ms, e0, e1);
       return EPB_OK;
+    };
+    int st = EPB_OK;
+    if (need_kb) {
+      const int64_t cands[4] = {4, 8, 16, 32};
+      float best = 1e30f;
+      for (int64_t kb : cands) {
+        if (kb > ns && kb != cands[0]) continue;
+        PassChoice t = c;
+        t.kb = kb;
+        float ms = 0.f;
+        st = trial(t, &ms);
+        if (st == EPB_ERR_OOM) {  // a larger batch does not fit: the smaller ones stand
+          clear_error();
+          st = EPB_OK;
+          break;
+        }
+        if (st != EPB_OK) break;
+        if (ms < best) {
+          best = ms;
+          c.kb = kb;
+        }
+      }
+      if (st == EPB_OK) tune_store(ctx->tuned, kkb, c.kb);
     }
-  const int64_t ns = std::min<int64_t>(nk, 64);
-  const int64_t cands[4] = {4, 8, 16, 32};
-  cudaEvent_t e0, e1;
-  EPB_CUDA(cudaEventCreate(&e0));
-  EPB_CUDA(cudaEventCreate(&e1));
-  float best = 1e30f;
-  int64_t pick = 16;
-  for (int64_t c : cands) {
-    if (c > ns && c != cands[0]) continue;
-    int st = eph_pass_run(ctx, m, xk, ns, xq, nq, prec, c, 1, ek_out, omega_out, g2sum_out, nullptr, nullptr);
-    if (st == EPB_OK) {
-      cudaEventRecord(e0, ctx->stream);
-      st = eph_pass_run(ctx, m, xk, ns, xq, nq, prec, c, 1, ek_out, omega_out, g2sum_out, nullptr, nullptr);
-      cudaEventRecord(e1, ctx->stream);
+    if (st == EPB_OK && need_rot) {
+      float best = 1e30f;
+      for (int r : {0, 1}) {
+        PassChoice t = c;
+        t.rot = r;
+        float ms = 0.f;
+        if ((st = trial(t, &ms)) != EPB_OK) break;
+        if (ms < best) {
+          best = ms;
+          c.rot = r;
+        }
+      }
+      if (st == EPB_OK) tune_store(ctx->tuned, krot, c.rot);
     }
-    if (st == EPB_ERR_OOM) {  // a larger batch does not fit: the smaller ones stand
-      clear_error();
-      break;
+    if (st == EPB_OK && need_kq) {
+      float best = 1e30f;
+      for (int f : {1, 0}) {
+        PassChoice t = c;
+        t.kq = f;
+        float ms = 0.f;
+        if ((st = trial(t, &ms)) != EPB_OK) break;
+        if (ms < best) {
+          best = ms;
+          c.kq = f;
+        }
+      }
+      if (st == EPB_OK) tune_store(ctx->tuned, kkq, c.kq);
     }
-    if (st != EPB_OK) {
-      cudaEventDestroy(e0);
-      cudaEventDestroy(e1);
-      return st;
-    }
-    cudaEventSynchronize(e1);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    if (ms < best) {
-      best = ms;
-      pick = c;
-    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != EPB_OK) return st;
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  ctx->tuned.emplace_back(key, pick);
-  *chosen = pick;
+  *out = c;
   return EPB_OK;
 }
 
@@ -228,18 +302,29 @@ int epb_eph_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const
   EPB_CHECK_ARG(prec == EPB_PREC_FP64 || prec == EPB_PREC_MIXED, "epb_eph_pass: bad prec");
   EPB_CHECK_ARG(prec != EPB_PREC_MIXED || m->mixed, "epb_eph_pass: model was created without mixed planes");
   EPB_TRY(make_current(ctx));
-  if (k_batch <= 0) EPB_TRY(tune_k_batch(ctx, m, xk, nk, xq, nq, prec, ek_out, omega_out, g2sum_out, &k_batch));
+  PassChoice ch = pass_choice(ctx, m, nq, prec, k_batch);
+  if (k_batch <= 0) EPB_TRY(tune_pass(ctx, m, xk, nk, xq, nq, prec, ek_out, omega_out, g2sum_out, &ch));
+  k_batch = ch.kb;
+  ctx->cur_rot = ch.rot;
+  ctx->cur_kq_ares = ch.kq;
   const bool capturable = ctx->graph_mode && !ctx->prof_on && ctx->stream != nullptr && ctx->stream != cudaStreamLegacy;
+  auto report = [&](int64_t* sh) {  // stats: elements, inner k batch, rotation kernel, kR->kq form
+    if (!sh) return;
+    sh[0] = nk * nq * m->nw * m->nw * m->nm;
+    sh[1] = k_batch;
+    sh[2] = prec == EPB_PREC_MIXED ? ch.rot : -1;
+    sh[3] = prec == EPB_PREC_MIXED ? ch.kq : -1;
+  };
   if (!capturable) {
     int st = eph_pass_run(ctx, m, xk, nk, xq, nq, prec, k_batch, sample_stride, ek_out, omega_out, g2sum_out, g2_sample,
                           stats_host);
-    if (st == EPB_OK && stats_host) stats_host[1] = k_batch;
+    if (st == EPB_OK) report(stats_host);
     return st;
   }
   // Graph mode: the first call with these arguments runs eagerly (sizing every workspace), the
   // second captures the pass (status checks left out of the graph), later ones replay it.
   PassGraph& pg = m->graph;
-  const PassKey key{xk, nk, xq, nq, prec, k_batch, sample_stride, ek_out, omega_out, g2sum_out, g2_sample};
+  const PassKey key{xk, nk, xq, nq, prec, k_batch, sample_stride, ek_out, omega_out, g2sum_out, g2_sample, ch.rot, ch.kq};
   if (pg.exec && pg.key == key) {
     EPB_CUDA(cudaGraphLaunch(pg.exec, ctx->stream));
     ctx->launches += pg.launches;
@@ -275,11 +360,7 @@ int epb_eph_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const
   }
   EPB_TRY(eigh_check(ctx));
   if (prec == EPB_PREC_MIXED) EPB_TRY(split_gemm_check(ctx));
-  if (stats_host) {
-    stats_host[0] = nk * nq * m->nw * m->nw * m->nm;
-    stats_host[1] = k_batch;
-    stats_host[2] = stats_host[3] = 0;
-  }
+  report(stats_host);
   return EPB_OK;
 }
 

@@ -146,7 +146,7 @@ struct RotArgs {
   float gscale_inv;      // the kR->kq operand's power-of-two pre-scale undone (g = GEMM(G) with G scaled back)
   int nr_ep;
   int64_t nkb, nq;
-  double* g2sum;         // (nm, nkb) of this batch
+  double* partial;       // (nm, warps, nkb): each warp's sum over its blocks of k, in a fixed slot
   double* sample;        // (nw, nw, nm, nsamp, nkb) or null
   int64_t stride, nsamp;
 };
@@ -175,9 +175,12 @@ __global__ void __launch_bounds__(32 * ROT_MMA_WARPS, 1) eph_rot_mma_kernel(RotA
   const float unscale2 = unscale * unscale;
 
   const int64_t nblk = a.nkb * a.nq;
-  const int64_t wstride = (int64_t)gridDim.x * ROT_MMA_WARPS;
+  const int64_t nwarps = (int64_t)gridDim.x * ROT_MMA_WARPS;
+  const int64_t gw = (int64_t)blockIdx.x * ROT_MMA_WARPS + warp;
   int64_t kcur = -1;
   double part[3] = {0.0, 0.0, 0.0};  // modes t, t + 4, t + 8 of block rows g, g + 8 over this warp's blocks of k
+  // A warp meets each k in one run of consecutive blocks (k = blk / nq grows with blk), so its sum for k
+  // goes to the slot (k, gw) with a plain store; rot_reduce_kernel adds the slots in a fixed order.
   auto flush = [&](int64_t k) {
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
@@ -185,12 +188,12 @@ __global__ void __launch_bounds__(32 * ROT_MMA_WARPS, 1) eph_rot_mma_kernel(RotA
       v += __shfl_xor_sync(0xffffffffu, v, 4);
       v += __shfl_xor_sync(0xffffffffu, v, 8);
       v += __shfl_xor_sync(0xffffffffu, v, 16);
-      if (gq == 0 && v != 0.0) atomicAdd(&a.g2sum[(t + 4 * j) + NM * k], v);
+      if (gq == 0) a.partial[(t + 4 * j) + NM * (gw + nwarps * k)] = v;
       part[j] = 0.0;
     }
   };
 
-  for (int64_t blk = (int64_t)blockIdx.x * ROT_MMA_WARPS + warp; blk < nblk; blk += wstride) {
+  for (int64_t blk = gw; blk < nblk; blk += nwarps) {
     const int64_t kl = blk / a.nq, q = blk - kl * a.nq;
     if (kl != kcur) {
       if (kcur >= 0) flush(kcur);
@@ -320,9 +323,31 @@ __global__ void __launch_bounds__(32 * ROT_MMA_WARPS, 1) eph_rot_mma_kernel(RotA
   if (kcur >= 0) flush(kcur);
 }
 
+// g2sum[nu, k] += sum over the warps' slots in slot order (one block per k, deterministic).
+__global__ void rot_reduce_kernel(const double* __restrict__ partial, int64_t nwarps, double* __restrict__ g2sum) {
+  constexpr int NM = 12, PARTS = 8;
+  __shared__ double red[PARTS][NM];
+  const int64_t k = blockIdx.x;
+  const int nu = threadIdx.x % NM, part = threadIdx.x / NM;
+  if (part < PARTS) {
+    double s = 0.0;
+    for (int64_t w = part; w < nwarps; w += PARTS) s += partial[nu + NM * (w + nwarps * k)];
+    red[part][nu] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < NM) {
+    double s = 0.0;
+    for (int p = 0; p < PARTS; ++p) s += red[p][threadIdx.x];
+    g2sum[threadIdx.x + NM * k] += s;
+  }
+}
+
+int64_t rot_mma_partial_doubles(epb_ctx* ctx, int64_t nkb) { return nkb * (int64_t)ctx->sm_count * ROT_MMA_WARPS * 12; }
+
 int rot_mma_launch(epb_ctx* ctx, const float* g, int64_t g_stride, const float2* ukq, const float2* uph,
                    const float* inv2w, const unsigned* gmax, const unsigned* phmax, float gscale_inv, int nr_ep,
-                   int64_t nkb, int64_t nq, double* g2sum, double* sample, int64_t stride, int64_t nsamp) {
+                   int64_t nkb, int64_t nq, double* g2sum, double* partial, double* sample, int64_t stride,
+                   int64_t nsamp) {
   RotArgs a;
   a.g = g;
   a.g_stride = g_stride;
@@ -335,7 +360,7 @@ int rot_mma_launch(epb_ctx* ctx, const float* g, int64_t g_stride, const float2*
   a.nr_ep = nr_ep;
   a.nkb = nkb;
   a.nq = nq;
-  a.g2sum = g2sum;
+  a.partial = partial;
   a.sample = sample;
   a.stride = stride < 1 ? 1 : stride;
   a.nsamp = nsamp;
@@ -343,7 +368,11 @@ int rot_mma_launch(epb_ctx* ctx, const float* g, int64_t g_stride, const float2*
   if (nblk == 0) return EPB_OK;
   const int64_t want = cdiv(nblk, ROT_MMA_WARPS);
   const unsigned grid = (unsigned)std::min<int64_t>(want, (int64_t)ctx->sm_count);
+  const int64_t nwarps = (int64_t)grid * ROT_MMA_WARPS;
+  EPB_CUDA(cudaMemsetAsync(partial, 0, sizeof(double) * 12 * nwarps * nkb, ctx->stream));
   eph_rot_mma_kernel<<<grid, 32 * ROT_MMA_WARPS, 0, ctx->stream>>>(a);
+  EPB_LAUNCH_CHECK();
+  rot_reduce_kernel<<<(unsigned)nkb, 128, 0, ctx->stream>>>(partial, nwarps, g2sum);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
 }

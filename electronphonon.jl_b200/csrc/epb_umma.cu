@@ -948,7 +948,7 @@ int split_gemm(epb_ctx* ctx, int prof_id, const Planes& A, const Planes& B, int6
 // for operands pre-scaled by a power of two into FP16's range; cscale undoes the scale on C.
 int split_gemm_h(epb_ctx* ctx, int prof_id, const Planes& A, const Planes& B, int64_t m_tiles_per_batch,
                  int64_t batches, int64_t m_valid, int64_t n_valid, bool m_fastest, float* C, int64_t c_batch_stride,
-                 int64_t ldc_n, float cscale) {
+                 int64_t ldc_n, float cscale, bool allow_ares) {
   SplitGemmArgs a{};
   a.A = A.p;
   a.B = B.p;
@@ -971,7 +971,7 @@ int split_gemm_h(epb_ctx* ctx, int prof_id, const Planes& A, const Planes& B, in
   EPB_CHECK_ARG(B.rows_pad >= a.n_tiles * MX_NT, "FP16x2 GEMM: B planes too small");
   prof_begin(ctx, prof_id);
   int st;
-  if (a.KC <= ARES_KC) {
+  if (a.KC <= ARES_KC && allow_ares) {
     // A-resident: a unit is one A tile and n_per_unit column tiles; enough units for ~16 per CTA, at
     // least 8 column tiles per unit (the A copy is then under 1/8 of the unit's traffic)
     const int64_t want = cdiv(16 * (int64_t)ctx->sm_count, std::max<int64_t>(a.m_tiles, 1));
@@ -1421,7 +1421,9 @@ __global__ void c128_to_c64_absmax_kernel(const double2* __restrict__ in, float2
 
 int rot_mma_launch(epb_ctx* ctx, const float* g, int64_t g_stride, const float2* ukq, const float2* uph,
                    const float* inv2w, const unsigned* gmax, const unsigned* phmax, float gscale_inv, int nr_ep,
-                   int64_t nkb, int64_t nq, double* g2sum, double* sample, int64_t stride, int64_t nsamp);
+                   int64_t nkb, int64_t nq, double* g2sum, double* partial, double* sample, int64_t stride,
+                   int64_t nsamp);
+int64_t rot_mma_partial_doubles(epb_ctx* ctx, int64_t nkb);
 
 // ---- windowed kR->kq of the Boltzmann consumer on the tensor cores --------------------------------
 // A2 planes of G_k = g(k, Rp) u_k (nband columns of u_k) for nk points, one block of bte_rows_pad(nw, nband,
@@ -1770,6 +1772,7 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
   const size_t o_c2 = carve(4 * 2 * nd * kbi * nq);
   const size_t o_w2 = carve(4 * nm * nq);  // 1 / (2 omega), FP32
   const size_t o_mx = carve(16);           // float bits: max |G| of the outer batch, max |u_ph|
+  const size_t o_rp = carve(8 * rot_mma_partial_doubles(ctx, kbi));  // per-warp mode sums of the rotation
   void* ws = nullptr;
   EPB_TRY(ws_get(ctx, EPB_WS_PASS1, off + 1024, &ws));
   uint8_t* base = (uint8_t*)(((uintptr_t)ws + 1023) & ~uintptr_t(1023));
@@ -1861,7 +1864,7 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
         cudaStream_t main_stream = ctx->stream;
         ctx->stream = ctx->side;
         const int st = split_gemm_h(ctx, EPB_PROF_UMMA_KQ, A2i, Bp, rows_pad_k / 128, nki, 2 * nd, nq, false, C2,
-                                    2 * nd * nq, 2 * nd, a2_unscale);
+                                    2 * nd * nq, 2 * nd, a2_unscale, ctx->cur_kq_ares != 0);
         ctx->stream = main_stream;
         EPB_TRY(st);
         EPB_CUDA(cudaEventRecord(ctx->side_ev[1], ctx->side));
@@ -1871,7 +1874,7 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
         EPB_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->side_ev[1], 0));
       } else {
         EPB_TRY(split_gemm_h(ctx, EPB_PROF_UMMA_KQ, A2i, Bp, rows_pad_k / 128, nki, 2 * nd, nq, false, C2,
-                             2 * nd * nq, 2 * nd, a2_unscale));
+                             2 * nd * nq, 2 * nd, a2_unscale, ctx->cur_kq_ares != 0));
       }
       // rotations, g2, in-place reduction
       if (!tiled) {
@@ -1887,11 +1890,11 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
             g2_sample ? g2_sample + (ko + ki) * nsamp * nd : nullptr, sample_stride, nsamp);
         prof_end(ctx);
         EPB_LAUNCH_CHECK();
-      } else if (ctx->rot_variant == 0) {
+      } else if (ctx->cur_rot == 0) {
         prof_begin(ctx, EPB_PROF_ROT);
         const int st = rot_mma_launch(ctx, C2, 2 * nd, U32, uph32, inv2w, gmax, phmax, a2_unscale, (int)m->nr_ep, nki,
-                                      nq, g2sum + nm * (ko + ki), g2_sample ? g2_sample + (ko + ki) * nsamp * nd : nullptr,
-                                      sample_stride, nsamp);
+                                      nq, g2sum + nm * (ko + ki), (double*)(base + o_rp),
+                                      g2_sample ? g2_sample + (ko + ki) * nsamp * nd : nullptr, sample_stride, nsamp);
         prof_end(ctx);
         EPB_TRY(st);
       } else {

@@ -58,11 +58,21 @@ SIGNATURES = {
     "epb_eph_kR_to_kq": [P, P, I64, I64, I64, I64, I64, P, I64, P, I64, P, P, P, P, I32],
     "epb_window_filter": [P, P, I64, I64, D, D, P, P, P, P, P],
     "epb_window_filter_noalloc": [P, P, I64, I64, D, D, P, P, P, P, P],
+    "epb_filtered_states": [P, P, P, I64, I64, P, P, P, I64, P],
     "epb_fill_iqs": [P, P, I64, P, I64, I64, I64, P, P],
     "epb_model_create": [P, P, I64, P, I64, P, P, I64, P, I64, P, P, I64, I32, C.POINTER(P)],
     "epb_model_destroy": [P],
     "epb_eph_pass": [P, P, P, I64, P, I64, I32, I64, I64, P, P, P, P, P],
     "epb_set_rotation_variant": [P, I32],
+    "epb_tune_table_create": [C.POINTER(P)],
+    "epb_tune_table_destroy": [P],
+    "epb_tune_table_set": [P, C.c_char_p, I64],
+    "epb_tune_table_get": [P, C.c_char_p, C.POINTER(I64), C.POINTER(I32)],
+    "epb_tune_table_size": [P, C.POINTER(I64)],
+    "epb_tune_table_serialize": [P, C.c_char_p, I64, C.POINTER(I64)],
+    "epb_tune_table_parse": [P, C.c_char_p],
+    "epb_tune_export": [P, P],
+    "epb_tune_import": [P, P],
     "epb_bands_create": [P, P, I64, P, I64, C.POINTER(P)],
     "epb_bands_destroy": [P],
     "epb_bands_eigvals": [P, P, P, I64, P, I32],
@@ -227,6 +237,12 @@ class Context:
         """Rotation kernel of the mixed pass (nw = 16, nm = 12): 0 warp tensor cores, 1 FP32, -1 autotuned."""
         check(lib().epb_set_rotation_variant(self.h, int(variant)))
 
+    def tune_text(self):
+        """The context's tuning table as text (one "key value" per line)."""
+        t = TuneTable()
+        t.export_from(self)
+        return t.text()
+
     def set_graph_mode(self, on=True):
         """Capture epb_eph_pass as a CUDA graph and replay it for repeated calls on the same buffers."""
         check(lib().epb_set_graph_mode(self.h, 1 if on else 0))
@@ -299,6 +315,54 @@ class RSet:
 
 
 _default_ctx = {}
+
+
+class TuneTable:
+    """The autotuner's choices as a host table (epb_tune_table_*): set / get / text round trip; export
+    from and import into a context."""
+
+    def __init__(self, text=None):
+        h = C.c_void_p()
+        check(lib().epb_tune_table_create(C.byref(h)))
+        self.h = h
+        if text is not None:
+            self.parse(text)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().epb_tune_table_destroy(self.h)
+            self.h = None
+
+    def set(self, key, value):
+        check(lib().epb_tune_table_set(self.h, key.encode(), int(value)))
+
+    def get(self, key):
+        v, f = I64(0), I32(0)
+        check(lib().epb_tune_table_get(self.h, key.encode(), C.byref(v), C.byref(f)))
+        return int(v.value) if f.value else None
+
+    def __len__(self):
+        n = I64(0)
+        check(lib().epb_tune_table_size(self.h, C.byref(n)))
+        return int(n.value)
+
+    def text(self):
+        n = I64(0)
+        st = lib().epb_tune_table_serialize(self.h, None, 0, C.byref(n))
+        if st not in (EPB_OK, EPB_ERR_ARG):
+            check(st)
+        buf = C.create_string_buffer(int(n.value) + 1)
+        check(lib().epb_tune_table_serialize(self.h, buf, int(n.value) + 1, C.byref(n)))
+        return buf.value.decode()
+
+    def parse(self, text):
+        check(lib().epb_tune_table_parse(self.h, text.encode()))
+
+    def export_from(self, ctx):
+        check(lib().epb_tune_export(ctx.h, self.h))
+
+    def import_into(self, ctx):
+        check(lib().epb_tune_import(ctx.h, self.h))
 
 
 def default_context(device=None):

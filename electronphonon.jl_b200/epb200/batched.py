@@ -363,6 +363,24 @@ def window_filter(E, wmin, wmax):
     return bmin, bmax, keep[:n], nbelow
 
 
+def filtered_states(band_min, band_max, nw, capacity=None):
+    """FilteredStates of per-k band ranges on the device (band_states.jl:85-121, 283-287).
+
+    Returns (indmap (nw, nk) int64 physical-band map, 0 outside; iks, ibands (n,) int64 1-based;
+    n, nband_ignore, nband)."""
+    torch = _torch()
+    nk = band_min.numel()
+    cap = nk * nw if capacity is None else int(capacity)
+    indmap = jl_empty((nw, nk), torch.int64)
+    iks = torch.empty(max(cap, 1), dtype=torch.int64, device=band_min.device)
+    ibands = torch.empty(max(cap, 1), dtype=torch.int64, device=band_min.device)
+    counts = torch.zeros(3, dtype=torch.int64, device=band_min.device)
+    check(_lib.lib().epb_filtered_states(_ctx().h, ptr(band_min), ptr(band_max), nw, nk, ptr(indmap), ptr(iks),
+                                         ptr(ibands), cap, ptr(counts)))
+    n, ign, nband = (int(v) for v in counts.cpu())
+    return indmap, iks[:min(n, cap)], ibands[:min(n, cap)], n, ign, nband
+
+
 def fill_iqs(xkq_int, xk_int, ngrid, dense_hash_to_iq):
     """iq (1-based) of x_{k+q} - x_k per column of xkq_int (3, nkq); raises on a miss."""
     torch = _torch()

@@ -27,6 +27,8 @@ class PassResult:
     n_elements: int
     sample_stride: int
     k_batch: int = 0  # inner k batch the library used (autotuned when not given)
+    rot_variant: int = -1  # rotation kernel of the mixed pass (0 warp tensor cores, 1 FP32; -1 FP64 pass)
+    kq_form: int = -1      # kR->kq GEMM form of the mixed pass (1 A-resident, 0 streamed; -1 FP64 pass)
 
 
 class DeviceModel:
@@ -37,7 +39,7 @@ class DeviceModel:
     timed region; `mixed=True` also prepares the split-BF16 operand planes.
     """
 
-    def __init__(self, model, mixed=False, device="cuda"):
+    def __init__(self, model, mixed=False, device="cuda", ctx=None):
         import torch
 
         self.nw, self.nm = model.nw, model.nmodes
@@ -50,7 +52,7 @@ class DeviceModel:
         self.irvec_ph = np.ascontiguousarray(model.ph_dyn.irvec, dtype=np.int64)
         self.irvec_ep = np.ascontiguousarray(model.epmat.irvec_next, dtype=np.int64)
         assert np.array_equal(model.epmat.irvec, model.el_ham.irvec), "epmat Re grid must equal the H grid"
-        self.ctx = _lib.default_context()
+        self.ctx = ctx if ctx is not None else _lib.default_context()
         h = C.c_void_p()
         check(_lib.lib().epb_model_create(
             self.ctx.h, ptr(self.ham), self.nw, self.irvec_el.ctypes.data, self.irvec_el.shape[0],
@@ -95,4 +97,6 @@ def run_eph_over_k_and_q(dm: DeviceModel, xks, xqs, *, prec=PREC_FP64, k_batch=1
                                   ptr(out.g2_sample), stats.ctypes.data))
     out.n_elements = int(stats[0])
     out.k_batch = int(stats[1])
+    out.rot_variant = int(stats[2])
+    out.kq_form = int(stats[3])
     return out

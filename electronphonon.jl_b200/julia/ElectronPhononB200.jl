@@ -401,7 +401,8 @@ function eph_pass(pm::PassModel, xks, xqs; prec::Integer = DRIVER_PREC[], k_batc
                  CuPtr{Float64}, CuPtr{Float64}, CuPtr{Float64}, CuPtr{Float64}, Ptr{Int64}),
                 ctx().h, pm.h, xk, nk, xq, nq, Cint(prec), k_batch, max(sample_stride, 1), ek, om, g2sum,
                 samp === nothing ? CuPtr{Float64}(0) : samp, stats))
-    (ek = ek, omega = om, g2sum = g2sum, g2_sample = samp, n_elements = stats[1], k_batch = stats[2])
+    (ek = ek, omega = om, g2sum = g2sum, g2_sample = samp, n_elements = stats[1], k_batch = stats[2],
+     rotation = stats[3], kq_form = stats[4])
 end
 
 "Capture the pass as a CUDA graph on its second call with the same buffers and replay it afterwards."

@@ -181,6 +181,17 @@ EPB_API int epb_window_filter(epb_ctx* ctx, const double* E, int64_t nw, int64_t
                       double wmax, int32_t* band_min, int32_t* band_max, int32_t* keep_idx,
                       int64_t* nkeep_dev, double* nbelow);
 
+/* FilteredStates of the window filter's band ranges on the device (src/band_states.jl:85-121): states
+   ordered by k, then band; iks[i], ibands[i] (int64, 1-based; i < capacity written, either may be NULL) and
+   the index map in the physical-band form the device calculators read, indmap[b - 1, k] = i + 1 for the
+   states and 0 elsewhere (int64, nw x nk; _indmap_to_device, band_states.jl:283-287, builds it on the host
+   and uploads it). band_min / band_max as written by epb_window_filter (0 = k not kept). counts_dev
+   (device int64[3]): number of states, nband_ignore and nband of the compact FilteredStates map (the
+   band_extent of k is band_min[k]:band_max[k]). Stream-ordered, no host synchronisation. */
+EPB_API int epb_filtered_states(epb_ctx* ctx, const int32_t* band_min, const int32_t* band_max, int64_t nw,
+                                int64_t nk, int64_t* indmap, int64_t* iks, int64_t* ibands, int64_t capacity,
+                                int64_t* counts_dev);
+
 /* The same window filter, allocating nothing: no counterpart in the reference. For callers that
    cannot let a library allocate device memory (their memory is owned by a caching allocator such as
    a Julia CUDA.jl or PyTorch pool, or a hot loop must not pay an allocation's latency or risk its
@@ -330,8 +341,9 @@ EPB_API int epb_model_destroy(epb_model* model);
    g2 block (nw x nw x nm) of every q with q % sample_stride == 0, laid out
    (nw, nw, nm, nsamp, nk) with nsamp = ceil(nq / sample_stride). k_batch: k per inner batch, or
    <= 0 to let the autotuner pick it (candidates 4, 8, 16, 32 timed on the first 64 k with this q list,
-   cached in the context per (nw, nm, nq, prec)). stats_host (4 int64, may be NULL): [0] = g elements
-   produced, [1] = k batch used. Replaces: the per-(k, q) loop of run_eph_over_k_and_q
+   then the rotation kernel and the kR->kq GEMM form; kept in the context's tuning table per (nw, nm, nq,
+   prec)). stats_host (4 int64, may be NULL): [0] = g elements produced, [1] = k batch used, [2] = rotation
+   kernel (0 tensor cores, 1 FP32; -1 for FP64), [3] = kR->kq form (1 A-resident, 0 streamed; -1). Replaces: the per-(k, q) loop of run_eph_over_k_and_q
    (src/calculator/run_eph_over_k_and_q.jl:251-330) run the batched way of
    _loop_eph_over_k_and_kq_batched (src/calculator/run_eph_over_k_and_kq.jl:792-892). */
 /* Graph mode (off by default): epb_eph_pass runs the first call with a given argument set eagerly,
@@ -340,10 +352,32 @@ EPB_API int epb_model_destroy(epb_model* model);
    while profiling. */
 EPB_API int epb_set_graph_mode(epb_ctx* ctx, int on);
 /* Rotation kernel of the mixed pass for nw = 16, nm = 12 (the fused rotation of
-   ext/ElectronPhononCUDAExt.jl:146-201 and its two-GEMM fallback): 0 = warp-level tensor cores
-   (default), 1 = FP32 CUDA cores, -1 = timed by the pass's autotuner on its first call per shape.
-   Both give |g|^2 within the mixed path's 1e-5 per-block bar of the FP64 pass. */
+   ext/ElectronPhononCUDAExt.jl:146-201 and its two-GEMM fallback): 0 = warp-level tensor cores,
+   1 = FP32 CUDA cores, -1 (default) = the tuning table's choice, timed when epb_eph_pass autotunes
+   (k_batch <= 0), else 0. Both give |g|^2 within the mixed path's 1e-5 per-block bar of the FP64 pass. */
 EPB_API int epb_set_rotation_variant(epb_ctx* ctx, int variant);
+
+/* ---- tuning table -------------------------------------------------------------------------- */
+/* The autotuner's measured choices, keyed by shape, replacing the reference's fixed crossovers
+   _FUSED_ROT_MAX_NWNM (src/wannier_to_bloch_batched.jl:406) and _FUSED_RQKQ_MAX_NW2NM
+   (ext/ElectronPhononCUDAExt.jl:214) with timings on the caller's shapes. Keys (all per nw, nm, nq,
+   prec): pass_kb/... inner k batch of epb_eph_pass, pass_rot/... rotation kernel (0 tensor cores,
+   1 FP32), pass_kq/... kR->kq GEMM form (1 A-resident, 0 streamed). A table is host memory only; its
+   text form is one "key value" pair per line ('#' comment lines allowed). epb_tune_export copies a
+   context's choices into a table, epb_tune_import loads a table's choices into a context (later calls
+   of those shapes then use them without timing). get: *found = 0 when the key is absent. serialize:
+   *len = text length; EPB_ERR_ARG (nothing written) when cap <= *len. parse: a malformed line rejects
+   the whole text, the table unchanged. */
+typedef struct epb_tune_table epb_tune_table;
+EPB_API int epb_tune_table_create(epb_tune_table** table);
+EPB_API int epb_tune_table_destroy(epb_tune_table* table);
+EPB_API int epb_tune_table_set(epb_tune_table* table, const char* key, int64_t value);
+EPB_API int epb_tune_table_get(const epb_tune_table* table, const char* key, int64_t* value, int* found);
+EPB_API int epb_tune_table_size(const epb_tune_table* table, int64_t* n);
+EPB_API int epb_tune_table_serialize(const epb_tune_table* table, char* buf, int64_t cap, int64_t* len);
+EPB_API int epb_tune_table_parse(epb_tune_table* table, const char* text);
+EPB_API int epb_tune_export(epb_ctx* ctx, epb_tune_table* table);
+EPB_API int epb_tune_import(epb_ctx* ctx, const epb_tune_table* table);
 EPB_API int epb_eph_pass(epb_ctx* ctx, epb_model* model, const double* xk, int64_t nk, const double* xq,
                          int64_t nq, int prec, int64_t k_batch, int64_t sample_stride, double* ek_out,
                          double* omega_out, double* g2sum_out, double* g2_sample, int64_t* stats_host);

@@ -220,6 +220,34 @@ def test_window_filter_exact(B):
     assert keep0.numel() == 0
 
 
+def test_filtered_states_device_indmap(B):
+    """Device FilteredStates from the window filter's band ranges, bit-exact against the oracle's
+    filtered_states_indmap (band_states.jl:99-121) embedded in physical band rows as the device calculators
+    read it (_indmap_to_device, band_states.jl:283-287): several blocks of k, an all-out window, and a
+    state-list capacity below the state count (the map stays complete)."""
+    rng = np.random.default_rng(19)
+    nw, nk = 16, 5000
+    E = np.sort(rng.standard_normal((nw, nk)) * 3, axis=0)
+    wmin, wmax = -0.5, 0.9
+    bmin, bmax, keep, _ = B.window_filter(B.jl(np.asfortranarray(E)), wmin, wmax)
+    indmap, iks, ibands, n, ign, nband = B.filtered_states(bmin, bmax, nw)
+    ref = O.filter_kpoints(E, np.ones(nk), wmin, wmax)
+    riks, ribs, rmap, rign = O.filtered_states_indmap(ref["ik_keep"], ref["band_min_per_k"], ref["band_max_per_k"])
+    assert n == len(riks) > 0 and ign == rign and nband == rmap.shape[0]
+    assert np.array_equal(iks.cpu().numpy(), riks) and np.array_equal(ibands.cpu().numpy(), ribs)
+    phys = np.zeros((nw, nk), dtype=np.int64)
+    phys[rign:rign + rmap.shape[0], :] = rmap
+    assert np.array_equal(B.host(indmap), phys)
+    # capacity below n: identical map, the first `cap` states only
+    indmap2, iks2, ibands2, n2, _, _ = B.filtered_states(bmin, bmax, nw, capacity=n // 3)
+    assert n2 == n and np.array_equal(B.host(indmap2), phys)
+    assert np.array_equal(iks2.cpu().numpy(), riks[: n // 3]) and np.array_equal(ibands2.cpu().numpy(), ribs[: n // 3])
+    # nothing in the window
+    b0, b1, _, _ = B.window_filter(B.jl(np.asfortranarray(E)), 100.0, 101.0)
+    indmap0, iks0, _, n0, ign0, nband0 = B.filtered_states(b0, b1, nw)
+    assert (n0, ign0, nband0) == (0, 0, 0) and iks0.numel() == 0 and not B.host(indmap0).any()
+
+
 def test_fill_iqs_vs_oracle(B):
     import torch
 

@@ -74,7 +74,7 @@ def test_gpu_pass_mixed(gpu_lib, nk, nq, kb, rot):
     try:
         r = pipeline.run_eph_over_k_and_q(dm, xks, xqs, prec=pipeline.PREC_MIXED, k_batch=kb, sample_stride=5)
     finally:
-        dm.ctx.set_rotation_variant(0)
+        dm.ctx.set_rotation_variant(-1)
     ref = cpu_pass.eph_pass_cpu(m, xks, xqs, sample_stride=5)
     np.testing.assert_allclose(host(r.ek), ref["ek"], atol=1e-11 * np.abs(ref["ek"]).max())
     np.testing.assert_allclose(host(r.omega), ref["omega"], rtol=1e-10)
@@ -210,7 +210,7 @@ def test_gpu_pass_config2_grids(gpu_lib, config2_full, prec):
     try:
         r = pipeline.run_eph_over_k_and_q(dm, xks, xqs, prec=p, k_batch=2, sample_stride=3)
     finally:
-        dm.ctx.set_rotation_variant(0)
+        dm.ctx.set_rotation_variant(-1)
     np.testing.assert_allclose(host(r.ek), ref["ek"], atol=1e-11 * np.abs(ref["ek"]).max())
     np.testing.assert_allclose(host(r.omega), ref["omega"], rtol=1e-10)
     err = _block_rel_err(host(r.g2_sample), ref["g2_sample"])
