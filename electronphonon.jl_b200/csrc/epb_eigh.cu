@@ -493,23 +493,40 @@ static int eigh_small(epb_ctx* ctx, const EighArgs& a, int prec) {
 int eigh_big_launch(epb_ctx* ctx, double2* A, const int64_t* a_off, const int32_t* nvec, int n_uniform, int64_t batch,
                     double* E, const int64_t* e_off, bool want_v, int n_lo, int prec, int* nonconv, int* badsize);
 
-// Orders per size class of a varlen batch: [0] 1..16, [1] 17..32, [2] 33..64, [3] 65..96, [4] outside
-// 0..96 (unsupported; order 0 is an empty matrix).
-__global__ void eigh_class_count_kernel(const int32_t* __restrict__ nvec, int64_t batch, int* __restrict__ cnt) {
-  int c[5] = {0, 0, 0, 0, 0};
+// Orders of a varlen batch outside 0..96 (no kernel handles them; order 0 is an empty matrix).
+__global__ void eigh_badorder_kernel(const int32_t* __restrict__ nvec, int64_t batch, int* __restrict__ badsize) {
+  int c = 0;
   for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < batch; b += (int64_t)gridDim.x * blockDim.x) {
     const int n = nvec[b];
-    c[0] += n >= 1 && n <= 16;
-    c[1] += n > 16 && n <= 32;
-    c[2] += n > 32 && n <= 64;
-    c[3] += n > 64 && n <= 96;
-    c[4] += n < 0 || n > 96;
+    c += n < 0 || n > 96;
   }
-  for (int i = 0; i < 5; ++i) {
-    int v = c[i];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0 && v) atomicAdd(cnt + i, v);
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(badsize, c);
+}
+
+// The varlen batch without any host read-back (capturable in a CUDA graph): every size class kernel runs
+// -- orders 1..16, 17..32, 33..64 on the shared-memory Jacobi, 65..96 on the persistent big kernel -- each
+// taking the matrices of its class from the whole batch and skipping the others; orders outside 0..96 are
+// counted into the status words that eigh_check reads.
+int eigh_varlen_async(epb_ctx* ctx, EighArgs& a, int prec) {
+  if (a.batch == 0) return EPB_OK;
+  EPB_CHECK_ARG(prec == EPB_PREC_FP64 || prec == EPB_PREC_MIXED, "eigensolver: unknown precision mode %d", prec);
+  EPB_CHECK_ARG(!a.mass, "eigensolver: varlen batches take no masses");
+  a.nonconv = ctx->dstat + 0;
+  a.badsize = ctx->dstat + 1;
+  a.max_sweeps = prec == EPB_PREC_FP64 ? 30 : 20;
+  eigh_badorder_kernel<<<(unsigned)std::min<int64_t>(cdiv(a.batch, 256), (int64_t)ctx->sm_count * 8), 256, 0,
+                         ctx->stream>>>(a.nvec, a.batch, a.badsize);
+  EPB_LAUNCH_CHECK();
+  const int lo[3] = {0, 16, 32}, hi[3] = {16, 32, 64};
+  for (int c = 0; c < 3; ++c) {
+    EighArgs s = a;
+    s.n_lo = lo[c];
+    s.skip_hi = 1;
+    EPB_TRY(eigh_dispatch(ctx, s, hi[c], prec));
   }
+  return eigh_big_launch(ctx, a.A, a.a_off, a.nvec, 0, a.batch, a.E, a.e_off, a.want_v != 0, 64, prec, a.nonconv,
+                         a.badsize);
 }
 
 int eigh_run(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
@@ -535,36 +552,11 @@ int eigh_run(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
     }
     return eigh_check(ctx);
   }
-  // varlen: one kernel per size class present in the batch (one small read-back of the class counts)
+  // varlen: every size class, no read-back, then the status words
   (void)nmax;
-  int* cnt = ctx->dstat + 8;
-  EPB_CUDA(cudaMemsetAsync(cnt, 0, 5 * sizeof(int), ctx->stream));
-  eigh_class_count_kernel<<<(unsigned)std::min<int64_t>(cdiv(a.batch, 256), (int64_t)ctx->sm_count * 8), 256, 0,
-                            ctx->stream>>>(a.nvec, a.batch, cnt);
-  EPB_LAUNCH_CHECK();
-  int hc[5];
-  EPB_CUDA(cudaMemcpyAsync(ctx->pinned, cnt, 5 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  EPB_CUDA(cudaStreamSynchronize(ctx->stream));
-  memcpy(hc, ctx->pinned, sizeof(hc));
-  const int lo[3] = {0, 16, 32}, hi[3] = {16, 32, 64};
-  for (int c = 0; c < 3; ++c) {
-    if (hc[c] == 0) continue;
-    EighArgs s = a;
-    s.n_lo = lo[c];
-    s.skip_hi = 1;
-    EPB_TRY(eigh_dispatch(ctx, s, hi[c], prec));
-  }
-  if (hc[3] > 0) {
-    EPB_CHECK_ARG(!a.mass, "eigensolver: phonon (mass-scaled) batches are limited to order 64");
-    EPB_TRY(eigh_big_launch(ctx, a.A, a.a_off, a.nvec, 0, a.batch, a.E, a.e_off, a.want_v != 0, 64, prec, a.nonconv,
-                            a.badsize));
-  }
-  EPB_TRY(eigh_check(ctx));
-  if (hc[4] > 0) {
-    set_error("eigensolver: %d matrices have an order outside 0..96 (skipped)", hc[4]);
-    return EPB_ERR_ARG;
-  }
-  return EPB_OK;
+  EPB_CUDA(cudaMemsetAsync(ctx->dstat, 0, 2 * sizeof(int), ctx->stream));
+  EPB_TRY(eigh_varlen_async(ctx, a, prec));
+  return eigh_check(ctx);
 }
 
 // Stream-ordered variant for the pass pipeline: counters accumulate in a context slot until
@@ -661,9 +653,33 @@ int epb_eigh_varlen(epb_ctx* ctx, double* A, const int64_t* a_offset, const int3
   a.E = E;
   a.e_off = e_offset;
   a.want_v = jobz == 'V';
-  // The kernel variant is chosen by the largest order; it is read back once (small D2H).
-  // Callers that know the maximum should use uniform batches per size class.
   return eigh_run(ctx, a, 64, prec);
+}
+
+int epb_eigh_varlen_async(epb_ctx* ctx, double* A, const int64_t* a_offset, const int32_t* n, int64_t batch, double* E,
+                          const int64_t* e_offset, char jobz, int prec) {
+  clear_error();
+  EPB_CHECK_ARG(ctx, "epb_eigh_varlen_async: NULL ctx");
+  EPB_CHECK_ARG(batch >= 0, "epb_eigh_varlen_async: batch < 0");
+  EPB_CHECK_ARG(batch == 0 || (A && a_offset && n && E && e_offset), "epb_eigh_varlen_async: NULL buffer");
+  EPB_CHECK_ARG(jobz == 'N' || jobz == 'V', "epb_eigh_varlen_async: jobz must be 'N' or 'V'");
+  EPB_TRY(make_current(ctx));
+  EighArgs a{};
+  a.A = (double2*)A;
+  a.a_off = a_offset;
+  a.nvec = n;
+  a.batch = batch;
+  a.E = E;
+  a.e_off = e_offset;
+  a.want_v = jobz == 'V';
+  return eigh_varlen_async(ctx, a, prec);
+}
+
+int epb_eigh_status(epb_ctx* ctx) {
+  clear_error();
+  EPB_CHECK_ARG(ctx, "epb_eigh_status: NULL ctx");
+  EPB_TRY(make_current(ctx));
+  return eigh_check(ctx);
 }
 
 int epb_ph_eigen_batched(epb_ctx* ctx, double* D, const double* mass, int64_t nm, int64_t nq,

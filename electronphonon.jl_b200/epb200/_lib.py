@@ -52,6 +52,8 @@ SIGNATURES = {
     "epb_fourier": [P, P, I64, I64, P, P, I64, P, I32],
     "epb_eigh_batched": [P, P, I64, I64, P, C.c_char, I32],
     "epb_eigh_varlen": [P, P, P, P, I64, P, P, C.c_char, I32],
+    "epb_eigh_varlen_async": [P, P, P, P, I64, P, P, C.c_char, I32],
+    "epb_eigh_status": [P],
     "epb_ph_eigen_batched": [P, P, P, I64, I64, P, I32],
     "epb_eph_RR_to_kR": [P, P, I64, I64, I64, P, P, I64, P, I64, P, P, I32],
     "epb_eph_apply_rotations": [P, P, I64, I64, I64, I64, I64, P, I64, P, P, P, P],

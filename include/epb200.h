@@ -126,6 +126,17 @@ EPB_API int epb_eigh_batched(epb_ctx* ctx, double* A, int64_t n, int64_t batch, 
 EPB_API int epb_eigh_varlen(epb_ctx* ctx, double* A, const int64_t* a_offset, const int32_t* n,
                     int64_t batch, double* E, const int64_t* e_offset, char jobz, int prec);
 
+/* The same uneven batch with no host synchronisation and no read-back (every size-class kernel is
+   launched; each takes its class from the whole batch): the call is stream-ordered and can be captured
+   in a CUDA graph once an eager call of the same size has sized the context's workspace. Status
+   (matrices at the sweep limit, orders outside 0..96) accumulates in the context until epb_eigh_status,
+   which synchronises the context stream and returns EPB_ERR_NOCONVERGE / EPB_ERR_ARG / EPB_OK (and
+   clears it). Replaces: the chunked heevjBatched loop of eigen_batched (ext/ElectronPhononCUDAExt.jl:78-115)
+   for ragged batches. */
+EPB_API int epb_eigh_varlen_async(epb_ctx* ctx, double* A, const int64_t* a_offset, const int32_t* n,
+                                  int64_t batch, double* E, const int64_t* e_offset, char jobz, int prec);
+EPB_API int epb_eigh_status(epb_ctx* ctx);
+
 /* Phonon eigenmodes from D(q): D c128 (nm x nm x nq) is scaled by 1/sqrt(m_i m_j), diagonalised,
    and overwritten by u with u[i, :] /= sqrt(m_i); omega f64 (nm x nq) = sign(l) sqrt|l|.
    mass: f64 (nm). Replaces: the device phonon branch of compute_phonon_states

@@ -87,3 +87,48 @@ def test_eigh_varlen_bad_order_reported(B):
     es, _ = vb.unpack()
     for k in (0, 2):
         np.testing.assert_allclose(es[k], O._zheev(mats[k].copy(), "N")[0], atol=1e-11 * np.abs(es[k]).max())
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_eigh_varlen_async_graph_capture(B, prec):
+    """The read-back-free varlen solve (epb_eigh_varlen_async) captured in a CUDA graph after one eager call
+    sized the workspace: a replay on the refilled batch equals the eager solve bit for bit and matches
+    LAPACK; epb_eigh_status reports an order outside 1..96 that a replayed batch contains."""
+    import torch
+
+    from epb200 import _lib
+
+    L = _lib.lib()
+    s = torch.cuda.Stream()
+    ctx = _lib.Context(0, s)
+    for bad in (False, True):
+        ns, mats = synth.config3_matrices(48, seed=31 + prec, degenerate_frac=0.25)
+        if bad:
+            rng = np.random.default_rng(3)
+            a = rng.standard_normal((100, 100)) + 1j * rng.standard_normal((100, 100))
+            mats = mats[:20] + [np.asfortranarray((a + a.conj().T) / 2)] + mats[20:]
+        vb = B.VarlenBatch(mats)
+        A0 = vb.A.clone()
+        args = (ctx.h, B.ptr(vb.A), B.ptr(vb.a_off), B.ptr(vb.n), len(mats), B.ptr(vb.E), B.ptr(vb.e_off), b"V", prec)
+        vb.E.zero_()  # the slots of a skipped (unsupported) matrix are left as they were
+        torch.cuda.synchronize()
+        with torch.cuda.stream(s):
+            _lib.check(L.epb_eigh_varlen_async(*args))
+        st = L.epb_eigh_status(ctx.h)
+        assert st == (_lib.EPB_ERR_ARG if bad else _lib.EPB_OK)
+        E_eager, A_eager = vb.E.clone(), vb.A.clone()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            _lib.check(L.epb_eigh_varlen_async(*args))
+        vb.A.copy_(A0)
+        vb.E.zero_()
+        torch.cuda.synchronize()
+        g.replay()
+        torch.cuda.synchronize()
+        st = L.epb_eigh_status(ctx.h)
+        assert st == (_lib.EPB_ERR_ARG if bad else _lib.EPB_OK)
+        assert torch.equal(vb.E, E_eager) and torch.equal(vb.A, A_eager)
+        es, us = vb.unpack()
+        keep = [i for i, m in enumerate(mats) if m.shape[0] <= 96]
+        _check([es[i] for i in keep], [us[i] for i in keep], [mats[i] for i in keep], 1e-11 if prec == 0 else 1e-10)
+        del g
