@@ -127,12 +127,12 @@ __device__ __forceinline__ THalf thalf(const S1Acc& a) {
 }
 
 // Stage-2 B fragments of u_ph for one n8 tile of the 24 output columns: K step 0 (Re T rows) and K step 1
-// (Im T rows); b01 rows kk = 2t, 2t+1 (jm 0..7), b23 rows kk = 2t+8, 2t+9 in two variants: v0 (jm = kk,
-// zero for kk >= 12) for the first band of a pair, v1 (zero for kk < 12, jm = kk - 4) for the second.
+// (Im T rows); b01 rows kk = 2t, 2t+1 (jm 0..7), b23 rows kk = 2t+8, 2t+9 in two variants: for the first
+// band of a pair jm = kk (zero for kk >= 12, i.e. lanes t >= 2), for the second zero for kk < 12 (lanes
+// t < 2) and jm = kk - 4. Each lane keeps only its nonzero variant, v.
 struct PhFrag {
   uint32_t b01h[2], b01l[2];   // [ks]
-  uint32_t v0h[2], v0l[2];     // [ks]
-  uint32_t v1h[2], v1l[2];     // [ks]
+  uint32_t vh[2], vl[2];       // [ks]
 };
 
 struct RotArgs {
@@ -161,7 +161,7 @@ __device__ __forceinline__ float pow2_scale(float max_abs, int target) {
 
 }  // namespace
 
-constexpr int ROT_MMA_WARPS = 8;
+constexpr int ROT_MMA_WARPS = 12;
 
 __global__ void __launch_bounds__(32 * ROT_MMA_WARPS, 1) eph_rot_mma_kernel(RotArgs a) {
   constexpr int NW = 16, NM = 12, ND = NW * NW * NM;
@@ -235,12 +235,12 @@ __global__ void __launch_bounds__(32 * ROT_MMA_WARPS, 1) eph_rot_mma_kernel(RotA
           const float x = ks == 0 ? (reim ? v.y : v.x) : (reim ? v.x : -v.y);
           return x * sph;
         };
+        // rows kk = 2t+8, 2t+9: jm = kk for t < 2 (first band), jm = kk - 4 for t >= 2 (second band)
+        const int jv = t < 2 ? 2 * t + 8 : 2 * t + 4;
 #pragma unroll
         for (int ks = 0; ks < 2; ++ks) {
           split2(val(2 * t, ks), val(2 * t + 1, ks), P[nt].b01h[ks], P[nt].b01l[ks]);
-          split2(val(2 * t + 8, ks), val(2 * t + 9, ks), P[nt].v0h[ks], P[nt].v0l[ks]);
-          const int j1 = 2 * t + 8 >= 12 ? 2 * t + 4 : -1;  // variant 1: kk 12..15 -> jm 8..11
-          split2(val(j1, ks), val(j1 < 0 ? -1 : j1 + 1, ks), P[nt].v1h[ks], P[nt].v1l[ks]);
+          split2(val(jv, ks), val(jv + 1, ks), P[nt].vh[ks], P[nt].vl[ks]);
         }
       }
     }
@@ -264,20 +264,19 @@ __global__ void __launch_bounds__(32 * ROT_MMA_WARPS, 1) eph_rot_mma_kernel(RotA
     for (int tl = 0; tl < 3; ++tl) gc[tl] = load_gcol(gb, combo(0, tl), t);
 #pragma unroll 1
     for (int p = 0; p < NW / 2; ++p) {
-      // ---- stage 1 for the pair's three tiles (the next pair's g is requested first) ----
-      S1Acc s1[3];
-      {
-        BFrag gre[3], gim[3];
+      // ---- stage 1 for the pair's three tiles, one at a time (each tile's g column is replaced by the next
+      // pair's request as soon as it is split) ----
+      THalf th[3];
 #pragma unroll
-        for (int tl = 0; tl < 3; ++tl) gfrags(gc[tl], sg, gre[tl], gim[tl]);
-        if (p + 1 < NW / 2) {
-#pragma unroll
-          for (int tl = 0; tl < 3; ++tl) gc[tl] = load_gcol(gb, combo(p + 1, tl), t);
-        }
-#pragma unroll
-        for (int tl = 0; tl < 3; ++tl) stage1_tile(s1[tl], X, Y, Yn, gre[tl], gim[tl]);
+      for (int tl = 0; tl < 3; ++tl) {
+        BFrag gre, gim;
+        gfrags(gc[tl], sg, gre, gim);
+        if (p + 1 < NW / 2) gc[tl] = load_gcol(gb, combo(p + 1, tl), t);
+        S1Acc s1;
+        stage1_tile(s1, X, Y, Yn, gre, gim);
+        th[tl] = thalf(s1);
       }
-      const THalf tA = thalf(s1[0]), tB = thalf(s1[1]), tC = thalf(s1[2]);
+      const THalf &tA = th[0], &tB = th[1], &tC = th[2];
       // ---- stage 2 for n0 = 2p (tiles A, C; variant 0) and n1 = 2p + 1 (tiles B, C; variant 1) ----
 #pragma unroll
       for (int nb = 0; nb < 2; ++nb) {
@@ -294,10 +293,11 @@ __global__ void __launch_bounds__(32 * ROT_MMA_WARPS, 1) eph_rot_mma_kernel(RotA
           BFrag br, bi;
           br.h[0] = P[nt].b01h[0]; br.l[0] = P[nt].b01l[0];
           bi.h[0] = P[nt].b01h[1]; bi.l[0] = P[nt].b01l[1];
-          br.h[1] = nb == 0 ? P[nt].v0h[0] : P[nt].v1h[0];
-          br.l[1] = nb == 0 ? P[nt].v0l[0] : P[nt].v1l[0];
-          bi.h[1] = nb == 0 ? P[nt].v0h[1] : P[nt].v1h[1];
-          bi.l[1] = nb == 0 ? P[nt].v0l[1] : P[nt].v1l[1];
+          const bool mine = (nb == 0) == (t < 2);  // this lane's rows kk 2t+8, 2t+9 belong to band nb
+          br.h[1] = mine ? P[nt].vh[0] : 0u;
+          br.l[1] = mine ? P[nt].vl[0] : 0u;
+          bi.h[1] = mine ? P[nt].vh[1] : 0u;
+          bi.l[1] = mine ? P[nt].vl[1] : 0u;
           float lead[4], corr[4];
           zero4(lead);
           zero4(corr);

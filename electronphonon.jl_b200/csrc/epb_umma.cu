@@ -632,10 +632,11 @@ __global__ void __launch_bounds__(192, 1) split_gemm_kernel(SplitGemmArgs a) {
 // so each 128 x 128 output tile costs one B tile of L2 traffic instead of an A and a B tile (the
 // kR->kq GEMM of the pass, K' = 256, is bound by that feed). A has its own full / empty barrier pair:
 // the MMA thread commits `a_empty` after the unit's last MMA, the producer waits on it before it
-// overwrites A. Same products, accumulators and promotion as split_gemm_kernel, with eight epilogue warps
-// (two per TMEM lane quarter, each holding half of a row's running sums); no grouped mode.
+// overwrites A. Same products, accumulators and promotion as split_gemm_kernel, with sixteen epilogue warps
+// (four per TMEM lane quarter, each holding a quarter of a row's running sums); no grouped mode.
 constexpr int ARES_KC = 4, ARES_STAGES = 2;
-constexpr int ARES_THREADS = 320;  // producer, MMA issuer, 8 epilogue warps (two per TMEM lane quarter)
+constexpr int ARES_EPI = 4;  // epilogue warps per TMEM lane quarter (each promotes NT / ARES_EPI columns of a row)
+constexpr int ARES_THREADS = 64 + 32 * 4 * ARES_EPI;  // producer, MMA issuer, epilogue warps
 template <bool BF16, int NPL, int NT>
 struct AresCfg {
   using G = GemmCfg<BF16, NPL, NT>;
@@ -646,9 +647,8 @@ struct AresCfg {
 };
 
 template <bool BF16, int NPL, int NT>
-// (8 epilogue warps, each promoting half of a tile row's columns: 128 registers, no spills; one CTA of this
-// kernel leaves room on its SM for one CTA of the FP32 Jacobi, which the pass runs beside it on another
-// stream)
+// (16 epilogue warps, each promoting a quarter of a tile row's columns; one CTA of this kernel leaves room
+// on its SM for one CTA of the FP32 Jacobi, which the pass runs beside it on another stream)
 __global__ void __launch_bounds__(ARES_THREADS, 1) split_gemm_ares_kernel(SplitGemmArgs a) {
   using Cfg = AresCfg<BF16, NPL, NT>;
   using G = GemmCfg<BF16, NPL, NT>;
@@ -812,8 +812,8 @@ __global__ void __launch_bounds__(ARES_THREADS, 1) split_gemm_ares_kernel(SplitG
     // ---------------- epilogue ----------------
     const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31
     const int row_in_tile = quarter * 32 + lane;
-    const int half = (warp - 2) >> 2;  // two warps per lane quarter: columns [half NT/2, half NT/2 + NT/2)
-    constexpr int NH = NT / 2;
+    const int half = (warp - 2) >> 2;  // ARES_EPI warps per lane quarter: columns [half NH, half NH + NH)
+    constexpr int NH = NT / ARES_EPI;
     int64_t tc = 0;
     bool go = true;
     for (int64_t u = blockIdx.x; u < nunits && go; u += gridDim.x) {
