@@ -137,6 +137,11 @@ struct epb_ctx {
   // created on first use
   cudaStream_t side = nullptr;
   cudaEvent_t side_ev[5] = {};
+  // the mixed pass's inner-batch pipeline (nw = 16, nm = 12): a second stream for the FP64 refinement and
+  // the rotation of batch i while the caller's stream runs the H(k+q) GEMM and FP32 Jacobi of batch i + 1,
+  // and its events (per buffer parity: H GEMM, Jacobi, kR->kq, refinement, rotation done), made on first use
+  cudaStream_t tail = nullptr;
+  cudaEvent_t pipe_ev[10] = {};
   // rotation kernel of the mixed pass for nw = 16, nm = 12: 0 = warp tensor cores (mma.sync),
   // 1 = FP32 CUDA cores; -1 = the tuning table's choice (timed when epb_eph_pass autotunes), else 0
   int rot_variant = -1;
@@ -199,6 +204,7 @@ namespace epb {
 // Profiler brackets around a launch (no-ops unless epb_profile_enable was called).
 void prof_begin(epb_ctx* ctx, int id);
 int side_stream(epb_ctx* ctx);
+int pipe_streams(epb_ctx* ctx);
 void prof_end(epb_ctx* ctx);
 
 // Grow-only workspace slot; returns EPB_ERR_OOM on failure.

@@ -79,6 +79,27 @@ int side_stream(epb_ctx* ctx) {
   return EPB_OK;
 }
 
+// The pipeline stream of the mixed pass (high priority, like the side stream) and its events.
+int pipe_streams(epb_ctx* ctx) {
+  EPB_TRY(side_stream(ctx));
+  if (ctx->tail) return EPB_OK;
+  int lo = 0, hi = 0;
+  EPB_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+  cudaStream_t s = nullptr;
+  EPB_CUDA(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, hi));
+  for (auto& e : ctx->pipe_ev) {
+    cudaError_t r = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    if (r != cudaSuccess) {
+      cudaStreamDestroy(s);
+      for (auto& f : ctx->pipe_ev)
+        if (f) cudaEventDestroy(f), f = nullptr;
+      EPB_CUDA(r);
+    }
+  }
+  ctx->tail = s;
+  return EPB_OK;
+}
+
 void prof_begin(epb_ctx* ctx, int id) {
   if (!ctx->prof_on) return;
   if (ctx->prof_used == ctx->prof.size()) {
@@ -168,6 +189,12 @@ int epb_destroy(epb_ctx* ctx) {
     cudaStreamDestroy(ctx->side);
   }
   for (auto& e : ctx->side_ev)
+    if (e) cudaEventDestroy(e);
+  if (ctx->tail) {
+    cudaStreamSynchronize(ctx->tail);
+    cudaStreamDestroy(ctx->tail);
+  }
+  for (auto& e : ctx->pipe_ev)
     if (e) cudaEventDestroy(e);
   for (auto& r : ctx->prof) {
     cudaEventDestroy(r.a);

@@ -666,4 +666,43 @@ int eigh16_launch(epb_ctx* ctx, Eigh16Args& a, bool mixed) {
   return EPB_OK;
 }
 
+// The two halves of the pass's mixed eigensolve of packed FP32 H(k+q) (n = 16), launched separately so that
+// the pass can run the refinement of one batch beside the Jacobi of the next: FP32 Jacobi into V32 (unsorted
+// FP32 vectors), then the FP64 refinement of V32 against H into U (sorted, complex64). Stream-ordered on
+// ctx->stream; the sweep-limit counter accumulates in the context status words.
+static Eigh16Args pass_args(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V32, float2* U) {
+  Eigh16Args b{};
+  b.Hp = Hp;
+  b.U32 = U;
+  b.n = E16;
+  b.batch = batch;
+  b.max_sweeps = 20;
+  b.nonconv = ctx->dstat + 0;
+  b.refine = 1;
+  b.V32 = V32;
+  return b;
+}
+
+int eigh16_mixed_jacobi(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V32) {
+  if (batch == 0) return EPB_OK;
+  Eigh16Args b = pass_args(ctx, Hp, batch, V32, nullptr);
+  const int64_t blocks = std::min<int64_t>(cdiv(batch, 8), (int64_t)ctx->sm_count * 16);
+  prof_begin(ctx, EPB_PROF_EIGH);
+  eigh16_jacobi_kernel<1><<<(unsigned)blocks, 128, 0, ctx->stream>>>(b);
+  prof_end(ctx);
+  EPB_LAUNCH_CHECK();
+  return EPB_OK;
+}
+
+int eigh16_mixed_refine(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V32, float2* U) {
+  if (batch == 0) return EPB_OK;
+  Eigh16Args b = pass_args(ctx, Hp, batch, V32, U);
+  const int64_t blocks = std::min<int64_t>(cdiv(batch, 4), (int64_t)ctx->sm_count * 8);
+  prof_begin(ctx, EPB_PROF_REFINE);
+  eigh16_refine2_kernel<<<(unsigned)blocks, 128, 0, ctx->stream>>>(b);
+  prof_end(ctx);
+  EPB_LAUNCH_CHECK();
+  return EPB_OK;
+}
+
 }  // namespace epb

@@ -632,10 +632,10 @@ __global__ void __launch_bounds__(192, 1) split_gemm_kernel(SplitGemmArgs a) {
 // so each 128 x 128 output tile costs one B tile of L2 traffic instead of an A and a B tile (the
 // kR->kq GEMM of the pass, K' = 256, is bound by that feed). A has its own full / empty barrier pair:
 // the MMA thread commits `a_empty` after the unit's last MMA, the producer waits on it before it
-// overwrites A. Same products, accumulators and promotion as split_gemm_kernel, with sixteen epilogue warps
-// (four per TMEM lane quarter, each holding a quarter of a row's running sums); no grouped mode.
+// overwrites A. Same products, accumulators and promotion as split_gemm_kernel, with eight epilogue warps
+// (two per TMEM lane quarter, each holding half of a row's running sums); no grouped mode.
 constexpr int ARES_KC = 4, ARES_STAGES = 2;
-constexpr int ARES_EPI = 4;  // epilogue warps per TMEM lane quarter (each promotes NT / ARES_EPI columns of a row)
+constexpr int ARES_EPI = 2;  // epilogue warps per TMEM lane quarter (each promotes NT / ARES_EPI columns of a row)
 constexpr int ARES_THREADS = 64 + 32 * 4 * ARES_EPI;  // producer, MMA issuer, epilogue warps
 template <bool BF16, int NPL, int NT>
 struct AresCfg {
@@ -647,8 +647,9 @@ struct AresCfg {
 };
 
 template <bool BF16, int NPL, int NT>
-// (16 epilogue warps, each promoting a quarter of a tile row's columns; one CTA of this kernel leaves room
-// on its SM for one CTA of the FP32 Jacobi, which the pass runs beside it on another stream)
+// (8 epilogue warps, each promoting half of a tile row's columns: 128 registers; one CTA of this kernel
+// leaves room on its SM for one CTA of the FP32 Jacobi, which the pass runs beside it on another stream.
+// Sixteen epilogue warps, tried, left no room for it and made the pass slower)
 __global__ void __launch_bounds__(ARES_THREADS, 1) split_gemm_ares_kernel(SplitGemmArgs a) {
   using Cfg = AresCfg<BF16, NPL, NT>;
   using G = GemmCfg<BF16, NPL, NT>;
@@ -1732,6 +1733,8 @@ int fourier_f64(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, const ep
 int eigh_async(epb_ctx* ctx, double2* A, int64_t n, int64_t batch, double* E, bool want_v, const double* mass,
                int prec);
 int eigh_mixed_packed(epb_ctx* ctx, const float* Hp, int64_t n, int64_t batch, float2* U, double* E);
+int eigh16_mixed_jacobi(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V32);
+int eigh16_mixed_refine(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V32, float2* U);
 
 // The whole mixed pass after the q side (omega, u_ph in FP64) has been computed.
 int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double* xq, int64_t nq,
@@ -1773,6 +1776,12 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
   const size_t o_w2 = carve(4 * nm * nq);  // 1 / (2 omega), FP32
   const size_t o_mx = carve(16);           // float bits: max |G| of the outer batch, max |u_ph|
   const size_t o_rp = carve(8 * rot_mma_partial_doubles(ctx, kbi));  // per-warp mode sums of the rotation
+  // the inner-batch pipeline (register-tiled shape, streams allowed): second buffers of packed H(k+q) and
+  // g(k, q), and the FP32 Jacobi vectors of both parities
+  const bool pipe = tiled && !ctx->prof_on;
+  const size_t o_c1b = carve(pipe ? 4 * nw2 * kbi * nq : 0);
+  const size_t o_c2b = carve(pipe ? 4 * 2 * nd * kbi * nq : 0);
+  const size_t o_v32 = carve(pipe ? 2 * 8 * nw2 * kbi * nq : 0);
   void* ws = nullptr;
   EPB_TRY(ws_get(ctx, EPB_WS_PASS1, off + 1024, &ws));
   uint8_t* base = (uint8_t*)(((uintptr_t)ws + 1023) & ~uintptr_t(1023));
@@ -1819,7 +1828,31 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
     EPB_TRY(side_stream(ctx));
     side = true;
   }
+  if (pipe) EPB_TRY(pipe_streams(ctx));
+  // Inner-batch pipeline: batch i (buffer parity p = i & 1) runs the H(k+q) GEMM and the FP32 Jacobi on the
+  // caller's stream, the kR->kq GEMM on the side stream, and the FP64 refinement + rotation on the tail
+  // stream, so the tail work of batch i overlaps the H GEMM and Jacobi of batch i + 1 (different pipes:
+  // FP64 and warp tensor cores beside FP32 and tcgen05). Events per parity: H GEMM, Jacobi, kR->kq,
+  // refinement, rotation done. A buffer of parity p is rewritten only after its last reader (of batch
+  // i - 2) has finished: the caller's stream waits for refinement[p] before the H GEMM (packed H and the
+  // Jacobi vectors), the side stream waits for rotation[p] before kR->kq (g). The refined vectors and the
+  // rotation's partial sums stay single: their writer and reader are both on the tail stream.
+  cudaEvent_t* evH = ctx->pipe_ev + 0;
+  cudaEvent_t* evJ = ctx->pipe_ev + 2;
+  cudaEvent_t* evK = ctx->pipe_ev + 4;
+  cudaEvent_t* evR = ctx->pipe_ev + 6;
+  cudaEvent_t* evT = ctx->pipe_ev + 8;
+  bool recK[2] = {false, false}, recR[2] = {false, false}, recT[2] = {false, false};
+  int64_t bi = 0;  // inner batches so far (buffer parity across outer batches)
+  const cudaStream_t main_stream = ctx->stream;
   for (int64_t ko = 0; ko < nk; ko += KO) {
+    if (pipe) {
+      // the previous outer batch's kR->kq GEMMs read A2 and its rotations read gmax: both are rewritten below
+      for (int p = 0; p < 2; ++p) {
+        if (recK[p]) EPB_CUDA(cudaStreamWaitEvent(main_stream, evK[p], 0));
+        if (recT[p]) EPB_CUDA(cudaStreamWaitEvent(main_stream, evT[p], 0));
+      }
+    }
     const int64_t nko = nk - ko < KO ? nk - ko : KO;
     const double* xko = xk + 3 * ko;
     // electrons at k (FP64: the k side is 0.01% of the pass and fixes the k-leg gauge)
@@ -1845,6 +1878,64 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
     for (int64_t ki = 0; ki < nko; ki += kbi) {
       const int64_t nki = nko - ki < kbi ? nko - ki : kbi;
       const int64_t np = nki * nq;
+      if (pipe) {
+        const int p = (int)(bi++ & 1);
+        float* C1p = p ? (float*)(base + o_c1b) : C1;
+        float* C2p = p ? (float*)(base + o_c2b) : C2;
+        float2* V32p = (float2*)(base + o_v32) + (size_t)p * nw2 * kbi * nq;
+        if (recR[p]) EPB_CUDA(cudaStreamWaitEvent(main_stream, evR[p], 0));  // C1p, V32p free again
+        Planes Ah;
+        EPB_TRY(pack_a_herm_mod(ctx, m->ham, m->rs_el, (int)nw, xko + 3 * ki, nki, mm->H.rows_pad, Ah, base + o_ah));
+        EPB_TRY(split_gemm(ctx, EPB_PROF_UMMA_H, Ah, Bq_el, mm->H.rows_pad / 128, nki, nw2, nq, true, C1p, nw2 * nq,
+                           nw2));
+        EPB_CUDA(cudaEventRecord(evH[p], main_stream));
+        // side: kR->kq into C2p once the rotation of batch i - 2 has read it
+        Planes A2i = A2;
+        A2i.p = A2.p + ki * rows_pad_k / 128 * KC_ep * TILE_BYTES;
+        EPB_CUDA(cudaStreamWaitEvent(ctx->side, evH[p], 0));
+        if (recT[p]) EPB_CUDA(cudaStreamWaitEvent(ctx->side, evT[p], 0));
+        ctx->stream = ctx->side;
+        int st = split_gemm_h(ctx, EPB_PROF_UMMA_KQ, A2i, Bp, rows_pad_k / 128, nki, 2 * nd, nq, false, C2p,
+                              2 * nd * nq, 2 * nd, a2_unscale, ctx->cur_kq_ares != 0);
+        if (st == EPB_OK) st = cudaEventRecord(evK[p], ctx->side) == cudaSuccess ? EPB_OK : EPB_ERR_CUDA;
+        ctx->stream = main_stream;
+        EPB_TRY(st);
+        recK[p] = true;
+        // caller's stream: FP32 Jacobi of the packed H(k+q)
+        EPB_TRY(eigh16_mixed_jacobi(ctx, C1p, np, V32p));
+        EPB_CUDA(cudaEventRecord(evJ[p], main_stream));
+        // tail: FP64 refinement, then the rotation + |g|^2 fold + reduction
+        EPB_CUDA(cudaStreamWaitEvent(ctx->tail, evJ[p], 0));
+        EPB_CUDA(cudaStreamWaitEvent(ctx->tail, evK[p], 0));
+        ctx->stream = ctx->tail;
+        st = eigh16_mixed_refine(ctx, C1p, np, V32p, U32);
+        if (st == EPB_OK) st = cudaEventRecord(evR[p], ctx->tail) == cudaSuccess ? EPB_OK : EPB_ERR_CUDA;
+        if (st == EPB_OK) {
+          if (ctx->cur_rot == 0) {
+            st = rot_mma_launch(ctx, C2p, 2 * nd, U32, uph32, inv2w, gmax, phmax, a2_unscale, (int)m->nr_ep, nki, nq,
+                                g2sum + nm * (ko + ki), (double*)(base + o_rp),
+                                g2_sample ? g2_sample + (ko + ki) * nsamp * nd : nullptr, sample_stride, nsamp);
+          } else {
+            constexpr int RS = RotSmem<16, 12>::TOTAL;
+            static bool pattr = false;
+            if (!pattr && cudaFuncSetAttribute(eph_rot_reduce_f32_kernel<16, 12>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, RS) == cudaSuccess)
+              pattr = true;
+            const unsigned grid = (unsigned)std::min<int64_t>(np, (int64_t)ctx->sm_count * 2);
+            eph_rot_reduce_f32_kernel<16, 12><<<grid, 256, RS, ctx->stream>>>(
+                C2p, 2 * nd, U32, uph32, inv2w, nki, nq, g2sum + nm * (ko + ki),
+                g2_sample ? g2_sample + (ko + ki) * nsamp * nd : nullptr, sample_stride, nsamp);
+            ++ctx->launches;
+            if (cudaGetLastError() != cudaSuccess) st = EPB_ERR_CUDA;
+          }
+        }
+        if (st == EPB_OK) st = cudaEventRecord(evT[p], ctx->tail) == cudaSuccess ? EPB_OK : EPB_ERR_CUDA;
+        ctx->stream = main_stream;
+        if (st == EPB_ERR_CUDA) set_error("mixed pass pipeline: a launch or event on the tail stream failed");
+        EPB_TRY(st);
+        recR[p] = recT[p] = true;
+        continue;
+      }
       // H(k+q) on the tensor cores: Hermitian-packed rows of H(R) exp(2 pi i R.k) per k times the q phases,
       // then FP32 solve + FP64 refinement
       Planes Ah;
@@ -1913,6 +2004,12 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
         prof_end(ctx);
         EPB_LAUNCH_CHECK();
       }
+    }
+  }
+  if (pipe) {  // join the side and tail streams back into the caller's stream
+    for (int p = 0; p < 2; ++p) {
+      if (recK[p]) EPB_CUDA(cudaStreamWaitEvent(main_stream, evK[p], 0));
+      if (recT[p]) EPB_CUDA(cudaStreamWaitEvent(main_stream, evT[p], 0));
     }
   }
   return defer_checks ? EPB_OK : split_gemm_check(ctx);
