@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--nk", type=int, default=NK)
     ap.add_argument("--nq", type=int, default=NQ)
     ap.add_argument("--k-batch", type=int, default=0, help="inner k batch of the pass; 0 = autotuned")
+    ap.add_argument("--tune-table", default=None,
+                    help="pass workload: load the autotuner's choices from this text table (skips the timing trials)")
+    ap.add_argument("--save-tune", default=None, help="pass workload: write the autotuner's choices to this file")
     ap.add_argument("--sample-stride", type=int, default=4096)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -274,14 +277,17 @@ def run_epb(args):
         want_mixed = False
     if prec is None:
         prec = pipeline.PREC_MIXED if want_mixed else pipeline.PREC_FP64
-    prec_name = ("mixed (tcgen05: FP16x2 kR->kq, split-BF16x3 RR->kR and H(k+q); FP32 rotations; FP32 Jacobi + "
-                 "FP64 refinement)") if prec == pipeline.PREC_MIXED else "fp64"
+    prec_name = ("mixed (tcgen05: FP16x2 kR->kq, split-BF16x3 RR->kR and H(k+q); rotation on the warp tensor cores "
+                 "(FP16x2, FP32 accumulate) or in FP32, autotuned; FP32 Jacobi + FP64 refinement)") if prec == pipeline.PREC_MIXED else "fp64"
     xks = synth.random_kpoints(args.nk, 1000 + rank)
     xqs = synth.random_kpoints(args.nq, 2000)
     from epb200.batched import jl
 
     xk_d, xq_d = jl(xks), jl(xqs)
     ctx = dm.ctx
+    if args.tune_table:
+        with open(args.tune_table) as f:
+            _lib.TuneTable(f.read()).import_into(ctx)
     ctx.set_graph_mode(True)  # repeated passes on the same buffers replay one captured CUDA graph
     run = lambda: pipeline.run_eph_over_k_and_q(dm, xk_d, xq_d, prec=prec, k_batch=args.k_batch,
                                                 sample_stride=args.sample_stride, out=out_holder[0])
@@ -443,19 +449,25 @@ def run_epb(args):
             if fp64 else None,
             "fp64_plain": fp64,
             "dtype": ("fp16x2 (kR->kq, 3 products) + bf16x3 (RR->kR, H(k+q), 6 products) on tcgen05, f32 "
-                      "accumulate / rotations / Jacobi, f64 refinement and k, q sides") if mixed else "f64",
+                      "accumulate; fp16x2 rotation on mma.sync (f32 accumulate); f32 Jacobi, f64 refinement and "
+                      "k, q sides") if mixed else "f64",
             "data": "synthetic (seeded generator; random-init Wannier model of the config-2 shape)",
             "config": dict(config_dict(args, prec_name), k_batch_used=kb_used,
                            autotuned={"k_batch": kb_used, "rotation": {0: "warp tensor cores (mma.sync)",
                                                                       1: "FP32 CUDA cores"}.get(out_holder[0].rot_variant, "fp64"),
                                       "kq_gemm": {1: "A-resident tcgen05", 0: "streamed tcgen05"}.get(
                                           out_holder[0].kq_form, "fp64"),
-                                      "table": dm.ctx.tune_text()}), "roofline": roof,
+                                      "table": dm.ctx.tune_text(),
+                                      "source": "loaded table" if args.tune_table else "timed in the first warm-up pass"}),
+            "roofline": roof,
             "roofline_compute": roof_compute, "roofline_pass": roof_pass,
             "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": clocks, "impl": "epb", "profile_one_pass": profile}
     if rank == 0:
         print(json.dumps(line), flush=True)
+        if args.save_tune:
+            with open(args.save_tune, "w") as f:
+                f.write(dm.ctx.tune_text())
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -488,11 +500,14 @@ def fp64_denominator(args, torch, pipeline, dm, xk_d, xq_d, r_mixed, ws, n_el, v
     v64 = ws * n_el / (ms64 * 1e-3)
     err = {}
     if r_mixed.g2_sample is not None:
-        a, b = r_mixed.g2_sample, r64.g2_sample          # (nw, nw, nm, nsamp, nk), same (k, q) blocks
-        d = (a - b).reshape(-1, a.shape[3] * a.shape[4])
-        bb = b.reshape(-1, a.shape[3] * a.shape[4])
-        blk = torch.linalg.vector_norm(d, dim=0) / torch.linalg.vector_norm(bb, dim=0)
-        floor = 1e-6 * bb.abs().amax(dim=0, keepdim=True)
+        # Julia (nw, nw, nm, nsamp, nk) arrays are torch tensors of shape (nk, nsamp, nm, nw, nw): one (k, q)
+        # block per row after flattening the first two axes
+        a, b = r_mixed.g2_sample, r64.g2_sample
+        nblk = a.shape[0] * a.shape[1]
+        d = (a - b).reshape(nblk, -1)
+        bb = b.reshape(nblk, -1)
+        blk = torch.linalg.vector_norm(d, dim=1) / torch.linalg.vector_norm(bb, dim=1)
+        floor = 1e-6 * bb.abs().amax(dim=1, keepdim=True)
         big = bb.abs() > floor
         elem = torch.where(big, d.abs() / torch.where(big, bb.abs(), torch.ones_like(bb)), torch.zeros_like(bb))
         err = {"g2_block_normwise_max": float(blk.max()), "g2_block_normwise_median": float(blk.median()),
@@ -501,9 +516,19 @@ def fp64_denominator(args, torch, pipeline, dm, xk_d, xq_d, r_mixed, ws, n_el, v
     err["ek_abs_max_ry"] = float((r_mixed.ek - r64.ek).abs().max())
     err["omega_abs_max_ry"] = float((r_mixed.omega - r64.omega).abs().max())
     ctx.set_graph_mode(True)
+    # the denominator's own roofline: the pass's algorithmic flops (same count as the mixed pass) against a
+    # live cuBLAS DGEMM; its GEMMs are the CUDA-core FP64 kernels of csrc/epb_eph.cu and csrc/epb_fourier.cu
+    nw2, nm_, nr_el, nr_ep = NW * NW, 3 * NATOM, (2 * N_EL + 1) ** 3, (2 * N_PH + 1) ** 3
+    per_pair = 8.0 * (nw2 * nm_ * nr_ep + nw2 * nr_el + NW ** 3 * nm_ + nw2 * nm_ * nm_ +
+                      nw2 * nm_ * nr_ep * nr_el / args.nq) + 40.0 * NW ** 3
+    tf64 = per_pair * args.nk * args.nq / (ms64 * 1e-3) / 1e12
+    p64 = measure_fp64_peak(torch)
     return {"value": v64, "unit": UNIT, "ms_per_step": round(ms64, 1), "steps": args.fp64_steps,
             "ratio": value / v64, "target_ratio": 3.0, "error_vs_fp64": err, "error_bar": 1e-5,
-            "kept_set": "identical by construction (all bands, every (k, q) pair in both paths)"}
+            "kept_set": "identical by construction (all bands, every (k, q) pair in both paths)",
+            "roofline": {"bound": "fp64", "achieved": round(tf64, 2), "peak": round(p64, 2), "unit": "TFLOP/s",
+                         "frac": round(tf64 / p64, 4), "peak_source": "measured live: cuBLAS DGEMM 8192^3",
+                         "note": "whole FP64 pass: FP64 Fourier sums and ZGEMM on CUDA cores, FP64 Jacobi"}}
 
 
 def m_host_for_cpu(m, ep_dev):
