@@ -507,11 +507,16 @@ def fp64_denominator(args, torch, pipeline, dm, xk_d, xq_d, r_mixed, ws, n_el, v
         d = (a - b).reshape(nblk, -1)
         bb = b.reshape(nblk, -1)
         blk = torch.linalg.vector_norm(d, dim=1) / torch.linalg.vector_norm(bb, dim=1)
-        floor = 1e-6 * bb.abs().amax(dim=1, keepdim=True)
-        big = bb.abs() > floor
-        elem = torch.where(big, d.abs() / torch.where(big, bb.abs(), torch.ones_like(bb)), torch.zeros_like(bb))
+        bmax = bb.abs().amax(dim=1, keepdim=True)
         err = {"g2_block_normwise_max": float(blk.max()), "g2_block_normwise_median": float(blk.median()),
-               "g2_elementwise_max_above_1e-6_floor": float(elem.max()), "blocks_compared": int(blk.numel())}
+               "blocks_compared": int(blk.numel())}
+        # elementwise relative error of the entries above a floor (fraction of their block's largest entry);
+        # an entry at the floor f carries the block's absolute error / f, so the figure grows as f falls
+        for f in (1e-6, 1e-4, 1e-2):
+            big = bb.abs() > f * bmax
+            elem = torch.where(big, d.abs() / torch.where(big, bb.abs(), torch.ones_like(bb)), torch.zeros_like(bb))
+            err[f"g2_elementwise_max_above_{f:g}_floor"] = float(elem.max())
+        err["g2_abs_err_max_over_block_max"] = float((d.abs().amax(dim=1, keepdim=True) / bmax).max())
     err["g2sum_rel_max"] = float(((r_mixed.g2sum - r64.g2sum).abs() / r64.g2sum.abs()).max())
     err["ek_abs_max_ry"] = float((r_mixed.ek - r64.ek).abs().max())
     err["omega_abs_max_ry"] = float((r_mixed.omega - r64.omega).abs().max())
@@ -1344,6 +1349,15 @@ def run_eigh(args):
     roof = {"bound": "hbm", "kernel": "eigh (all size classes)", "achieved": round(ach, 2), "peak": peaks["hbm_gbs"],
             "unit": "GB/s", "frac": round(ach / peaks["hbm_gbs"], 5), "traffic": None,
             "peak_source": f"{psrc} hbm copy; the solve is FP32/FP64 CUDA-core compute bound (about 90 flop/B)"}
+    # compute roofline: 40 n^3 real flops per matrix (the dense Hermitian eigensolve with vectors counted as
+    # tridiagonalisation + implicit QR + back-transformation in complex arithmetic), against a live FFMA peak
+    flops = float((40.0 * sizes.astype(np.float64) ** 3).sum())
+    fp32 = measure_fp32_simt_peak(torch)
+    ach_f = flops / (ms * 1e-3) / 1e12
+    roof_c = {"bound": "fp32 simt", "kernel": "eigh (all size classes)", "achieved": round(ach_f, 3), "peak": round(fp32, 2),
+              "unit": "TFLOP/s", "frac": round(ach_f / fp32, 4),
+              "peak_source": "measured live: cuBLAS SGEMM 8192^3, TF32 off",
+              "note": "algorithmic flops 40 n^3 per matrix; the Jacobi solves do several times more"}
     cpu = None
     if not args.no_cpu:
         t0 = time.perf_counter()
@@ -1365,7 +1379,8 @@ def run_eigh(args):
                                    "2-4-fold clusters spaced 1e-10", "precision": args.prec,
                        "input_bytes": int(16 * (sizes * sizes).sum()), "generation_s": round(t_gen, 1),
                        "l2": "inputs larger than L2"},
-            "max_abs_eig_err_vs_lapack_sample64": worst, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "max_abs_eig_err_vs_lapack_sample64": worst, "roofline": roof, "roofline_compute": roof_c,
+            "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": clocks, "impl": "epb", "profile_one_step": profile}
     print(json.dumps(line), flush=True)
 

@@ -109,7 +109,7 @@ __global__ void eigh_kernel(EighArgs a) {
     team_sync<TEAM>();
     const T eps = sizeof(T) == 8 ? T(2.220446049250313e-16) : T(1.1920929e-07);
     const T thr = eps * sqrt(tot) / T(n > 0 ? n : 1);
-    int sweeps = jacobi_team<T, TEAM>(As, lda, Vs, n, n, a.want_v != 0, prm, flag, thr, a.max_sweeps);
+    int sweeps = jacobi_team<T, TEAM>(As, lda, Vs, n, n, a.want_v != 0, flag, thr, a.max_sweeps);
     if (sweeps >= a.max_sweeps && tid == 0) atomicAdd(a.nonconv, 1);
     // sort eigenvalues ascending (rank by value, ties by index) and write out
     for (int i = tid; i < n; i += TEAM) {
@@ -168,7 +168,6 @@ __global__ void eigh_mixed_kernel(EighArgs a) {
   float2* V32 = A32 + NMAX * LDA;
   double2* S = reinterpret_cast<double2*>(R);
   RotParam<double>* prm64 = reinterpret_cast<RotParam<double>*>(base + 2 * h64 + regR);
-  RotParam<float>* prm32 = reinterpret_cast<RotParam<float>*>(prm64);
   int* flag = reinterpret_cast<int*>(prm64 + NMAX / 2 + 1);
   __shared__ double red[TEAMS * (TEAM / 32)];
 
@@ -218,7 +217,7 @@ __global__ void eigh_mixed_kernel(EighArgs a) {
     const double fro = sqrt(tot);
     // FP32 stop at 8 eps32 x the RMS eigenvalue (rounding of degenerate pairs stays below it); the FP64
     // stage below supplies the accuracy
-    int sw = jacobi_team<float, TEAM>(A32, lda, V32, n, n, true, prm32, flag,
+    int sw = jacobi_team<float, TEAM>(A32, lda, V32, n, n, true, flag,
                                       8.f * 1.1920929e-07f * (float)(fro / sqrt((double)n)), a.max_sweeps);
     if (sw >= a.max_sweeps && tid == 0) atomicAdd(a.nonconv, 1);
     // V64 <- V32, then modified Gram-Schmidt (column by column)
@@ -285,7 +284,7 @@ __global__ void eigh_mixed_kernel(EighArgs a) {
       S[i + c * n] = make_double2(i == c ? 1.0 : 0.0, 0.0);
     }
     team_sync<TEAM>();
-    jacobi_team<double, TEAM>(H, lda, S, n, n, true, prm64, flag, 2.220446049250313e-16 * fro / n, 8);
+    jacobi_team<double, TEAM>(H, lda, S, n, n, true, flag, 2.220446049250313e-16 * fro / n, 8);
     // V <- V Q, written in place row by row (each thread owns whole rows)
     for (int i = tid; i < n; i += TEAM) {
       double2 row[NMAX];

@@ -630,6 +630,153 @@ __global__ void __launch_bounds__(128, 3) eigh16_refine2_kernel(Eigh16Args a) {
   }
 }
 
+// MODE 2 for complex64 output (the e-ph pass): the same first-order update as eigh16_refine2_kernel with
+// the residual in FP64 and the correction in FP32. With R = H V - V diag(d), d_l = Re v_l^H H v_l (FP64,
+// the products of FP32 data are exact), the coupling of the update is
+//     S'_kl = S_kl - G_kl (d_k + d_l) / 2 = v_k^H r_l + G_kl (d_l - d_k) / 2        (k != l),
+// where every term is small: r_l = O(off-diagonal coupling) is rounded to FP32 (relative 6e-8 of a small
+// number) and v_k^H r_l, G_kl = v_k^H v_l and the update V t run in FP32. The FP32 rounding of G_kl
+// (a few 1e-8, from a sum of O(1) products) enters t at the size of the FP32 rounding of the output
+// columns, so the stored complex64 vectors are as accurate as with the all-FP64 update; |v_l|^2 - 1 and
+// the Rayleigh quotients (the eigenvalues, used for the order) stay FP64. FP64 work: W = H V (128 complex
+// FMAs per lane); FP32: S, G and V t (384 complex FMAs per lane), against 512 FP64 complex FMAs per lane
+// for the all-FP64 update. Pass only: no mass scaling, no flag list, one iteration.
+__global__ void __launch_bounds__(128, 4) eigh16_refine_c64_kernel(Eigh16Args a) {
+  __shared__ double2 Hs[4][E16 * RLD];  // H[i][k] at i * RLD + k
+  __shared__ float2 Vs[4][E16 * RLD];   // V[i][k] (FP32 Jacobi vectors)
+  __shared__ float2 Rs[4][E16 * RLD];   // R[i][l] = (H V - V d)[i][l], rounded to FP32
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int l = lane & 15, h = lane >> 4, r0 = 8 * h;
+  const int n = a.n;
+  double2* H = Hs[warp];
+  float2* V = Vs[warp];
+  float2* R = Rs[warp];
+  constexpr double th2 = 1e-2;  // first-order range |S'_kl| < 0.1 |gap| (no slow path in the pass)
+  for (int64_t b = (int64_t)blockIdx.x * 4 + warp; b - warp < a.batch; b += (int64_t)gridDim.x * 4) {
+    const bool live = b < a.batch;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) H[(r0 + r) * RLD + l] = live ? load_h(a, b, r0 + r, l, n) : make_double2(0.0, 0.0);
+    float2 v[8];
+    {
+      const float2* vi = a.V32 + (live ? b : 0) * (int64_t)E16 * E16 + (int64_t)E16 * l + r0;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        v[r] = live ? vi[r] : make_float2(r0 + r == l ? 1.f : 0.f, 0.f);
+        V[(r0 + r) * RLD + l] = v[r];
+      }
+    }
+    __syncwarp();
+    // w = H v on this lane's rows (FP64)
+    double2 w[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) w[r] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int k = 0; k < E16; ++k) {
+      const float2 vk32 = V[k * RLD + l];
+      const double2 vk = make_double2(vk32.x, vk32.y);
+#pragma unroll
+      for (int r = 0; r < 8; ++r) cfma(w[r], H[(r0 + r) * RLD + k], vk);
+    }
+    // d = Re v^H w, fll = |v|^2 - 1 (whole column, FP64)
+    double d = 0.0, fll = 0.0;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const double vx = v[r].x, vy = v[r].y;
+      d = fma(vx, w[r].x, fma(vy, w[r].y, d));
+      fll = fma(vx, vx, fma(vy, vy, fll));
+    }
+    d += __shfl_xor_sync(0xffffffffu, d, 16);
+    fll += __shfl_xor_sync(0xffffffffu, fll, 16);
+    fll -= 1.0;
+    const double dp = d * (1.0 - fll);
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+      R[(r0 + r) * RLD + l] = make_float2((float)(w[r].x - (double)v[r].x * d), (float)(w[r].y - (double)v[r].y * d));
+    __syncwarp();
+    float2 u[8];  // V t accumulated over k (FP32)
+#pragma unroll
+    for (int r = 0; r < 8; ++r) u[r] = make_float2(0.f, 0.f);
+    float2 rl[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) rl[r] = R[(r0 + r) * RLD + l];
+    float lam_corr = 0.f;
+    constexpr int KB = 4;
+#pragma unroll 1
+    for (int k0 = 0; k0 < E16; k0 += KB) {
+      float2 sb[KB], gb[KB];
+#pragma unroll
+      for (int kk = 0; kk < KB; ++kk) sb[kk] = gb[kk] = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int kk = 0; kk < KB; ++kk) {
+          const float2 vik = V[(r0 + r) * RLD + k0 + kk];
+          cfma_conj(sb[kk], vik, rl[r]);
+          cfma_conj(gb[kk], vik, v[r]);
+        }
+#pragma unroll
+      for (int kk = 0; kk < KB; ++kk) {
+        sb[kk].x += __shfl_xor_sync(0xffffffffu, sb[kk].x, 16);
+        sb[kk].y += __shfl_xor_sync(0xffffffffu, sb[kk].y, 16);
+        gb[kk].x += __shfl_xor_sync(0xffffffffu, gb[kk].x, 16);
+        gb[kk].y += __shfl_xor_sync(0xffffffffu, gb[kk].y, 16);
+      }
+#pragma unroll
+      for (int kk = 0; kk < KB; ++kk) {
+        const int k = k0 + kk;
+        const double dk = __shfl_sync(0xffffffffu, d, k);
+        const double dpk = __shfl_sync(0xffffffffu, dp, k);
+        const float2 g = gb[kk];
+        float2 t;
+        if (k == l) {
+          t = make_float2((float)(-0.5 * fll), 0.f);
+        } else {
+          const float hd = (float)(0.5 * (d - dk));
+          const float2 sp = make_float2(fmaf(g.x, hd, sb[kk].x), fmaf(g.y, hd, sb[kk].y));
+          const double gap = dp - dpk;
+          const float asp2 = fmaf(sp.x, sp.x, sp.y * sp.y);
+          t = make_float2(-0.5f * g.x, -0.5f * g.y);
+          if (k < n && l < n && (double)asp2 < th2 * gap * gap) {
+            const double ag = fabs(gap);
+            const float rg = (ag > 1e-30 && ag < 1e30) ? __frcp_rn((float)gap) : (float)(1.0 / gap);
+            t.x = fmaf(sp.x, rg, t.x);
+            t.y = fmaf(sp.y, rg, t.y);
+            lam_corr = fmaf(asp2, rg, lam_corr);
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < 8; ++r) cfma(u[r], V[(r0 + r) * RLD + k], t);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r] = make_float2(v[r].x + u[r].x, v[r].y + u[r].y);
+    const double lam = dp + (double)lam_corr;
+    int rank = 0;
+#pragma unroll
+    for (int k = 0; k < E16; ++k) {
+      const double lk = __shfl_sync(0xffffffffu, lam, k);
+      rank += (k < n) && (lk < lam || (lk == lam && k < l));
+    }
+    if (live && l < n) {
+      if (a.E && h == 0) a.E[b * n + rank] = lam;
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+        if (r0 + r < n) a.U32[b * (int64_t)n * n + r0 + r + (int64_t)rank * n] = v[r];
+    }
+    __syncwarp();
+  }
+}
+
+// The refinement kernel of a mixed solve: the FP32-correction form for the pass's complex64 output,
+// the all-FP64 form otherwise.
+static void refine_launch(epb_ctx* ctx, const Eigh16Args& a) {
+  const int64_t blocks = std::min<int64_t>(cdiv(a.batch, 4), (int64_t)ctx->sm_count * 8);
+  if (a.U32 && !a.U64 && !a.mass && !a.flag_list && a.refine == 1)
+    eigh16_refine_c64_kernel<<<(unsigned)blocks, 128, 0, ctx->stream>>>(a);
+  else
+    eigh16_refine2_kernel<<<(unsigned)blocks, 128, 0, ctx->stream>>>(a);
+}
+
 int eigh16_launch(epb_ctx* ctx, Eigh16Args& a, bool mixed) {
   if (a.batch == 0) return EPB_OK;
   const int threads = 128;  // 8 matrices per block
@@ -657,10 +804,7 @@ int eigh16_launch(epb_ctx* ctx, Eigh16Args& a, bool mixed) {
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   prof_begin(ctx, EPB_PROF_REFINE);
-  {
-    const int64_t blocks = std::min<int64_t>(cdiv(a.batch, 4), (int64_t)ctx->sm_count * 8);
-    eigh16_refine2_kernel<<<(unsigned)blocks, 128, 0, ctx->stream>>>(a);
-  }
+  refine_launch(ctx, a);
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
@@ -668,7 +812,8 @@ int eigh16_launch(epb_ctx* ctx, Eigh16Args& a, bool mixed) {
 
 // The two halves of the pass's mixed eigensolve of packed FP32 H(k+q) (n = 16), launched separately so that
 // the pass can run the refinement of one batch beside the Jacobi of the next: FP32 Jacobi into V32 (unsorted
-// FP32 vectors), then the FP64 refinement of V32 against H into U (sorted, complex64). Stream-ordered on
+// FP32 vectors), then the refinement of V32 against H into U (sorted, complex64; FP64 residual, FP32
+// correction). Stream-ordered on
 // ctx->stream; the sweep-limit counter accumulates in the context status words.
 static Eigh16Args pass_args(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V32, float2* U) {
   Eigh16Args b{};
@@ -697,9 +842,8 @@ int eigh16_mixed_jacobi(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V3
 int eigh16_mixed_refine(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V32, float2* U) {
   if (batch == 0) return EPB_OK;
   Eigh16Args b = pass_args(ctx, Hp, batch, V32, U);
-  const int64_t blocks = std::min<int64_t>(cdiv(batch, 4), (int64_t)ctx->sm_count * 8);
   prof_begin(ctx, EPB_PROF_REFINE);
-  eigh16_refine2_kernel<<<(unsigned)blocks, 128, 0, ctx->stream>>>(b);
+  refine_launch(ctx, b);
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;

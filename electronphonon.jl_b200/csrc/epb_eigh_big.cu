@@ -166,7 +166,6 @@ __global__ void __launch_bounds__(BIG_T, 1) eigh_big_kernel(BigArgs a) {
     // ---- 1. FP32 Jacobi ----
     float2* A32 = reinterpret_cast<float2*>(sm);
     float2* V32 = reinterpret_cast<float2*>(sm + BigSmem::A32);
-    void* prm = sm + BigSmem::A32 + BigSmem::V32;
     int* flag = reinterpret_cast<int*>(sm + BigSmem::A32 + BigSmem::V32 + BigSmem::PRM);
     const int lda = n + 1;
     double fro2 = 0.0;
@@ -194,7 +193,7 @@ __global__ void __launch_bounds__(BIG_T, 1) eigh_big_kernel(BigArgs a) {
     __syncthreads();
     // stop at 8 eps32 x the RMS eigenvalue: below that, FP32 rounding of (near-)degenerate pairs would
     // re-trigger 45-degree rotations forever; the FP64 refinement supplies the remaining accuracy
-    const int sw = jacobi_team<float, BIG_T>(A32, lda, V32, n, n, true, reinterpret_cast<RotParam<float>*>(prm), flag,
+    const int sw = jacobi_team<float, BIG_T>(A32, lda, V32, n, n, true, flag,
                                              8.f * 1.1920929e-07f * (float)(fro / sqrt((double)n)), a.max_sweeps);
     if (sw >= a.max_sweeps && tid == 0) atomicAdd(a.nonconv, 1);
     for (int e = tid; e < n * n; e += BIG_T) {
@@ -296,7 +295,7 @@ __global__ void __launch_bounds__(BIG_T, 1) eigh_big_kernel(BigArgs a) {
               Qc[p + q * k] = make_double2(p == q ? 1.0 : 0.0, 0.0);
             }
             __syncwarp();
-            jacobi_team<double, 32>(Ac, 33, Qc, k, k, true, reinterpret_cast<RotParam<double>*>(prmc), flc,
+            jacobi_team<double, 32>(Ac, 33, Qc, k, k, true, flc,
                                     2.220446049250313e-16 * fmax(dmax, 1e-300), 30);
             // M[:, c] <- M[:, c] Q_c: the cluster columns of (I + X) rotated into the cluster's eigenbasis
             for (int i = tid; i < n; i += 32) {

@@ -37,26 +37,34 @@ struct RotParam {
 
 // One full Jacobi solve of the n x n Hermitian matrix in A (column-major, leading dim lda) with
 // eigenvectors accumulated into V (leading dim ldv; must hold identity on entry if want_v).
-// Returns the number of sweeps used (max_sweeps + 1 if not converged).
+// Returns the number of sweeps used (max_sweeps + 1 if not converged, or if n > 64 TEAM / 32).
 template <typename T, int TEAM>
 __device__ int jacobi_team(typename cplx<T>::type* A, int lda, typename cplx<T>::type* V, int ldv,
-                           int n, bool want_v, RotParam<T>* prm, int* flag, T thr,
-                           int max_sweeps) {
+                           int n, bool want_v, int* flag, T thr, int max_sweeps) {
   using C = typename cplx<T>::type;
+  static_assert(TEAM % 32 == 0, "jacobi_team: the team is whole warps");
+  constexpr int NWT = TEAM / 32;  // warps of the team
   const int tid = threadIdx.x % TEAM;
   const int m = (n + 1) & ~1;
   const int npair = m / 2;
+  const int lane = tid & 31, wt = tid >> 5;
+  const int mine = npair > wt ? (npair - wt + NWT - 1) / NWT : 0;  // pairs of this warp: wt, wt + NWT, ...
+  if (npair > 32 * NWT) return max_sweeps + 1;  // a lane per pair of the warp: n <= 64 TEAM / 32
   int sweep = 0;
   for (; sweep < max_sweeps; ++sweep) {
     if (tid == 0) *flag = 0;
     team_sync<TEAM>();
     for (int r = 0; r < m - 1; ++r) {
-      for (int i = tid; i < npair; i += TEAM) {
+      // A warp owns the pairs wt + j NWT (j < mine <= 32): lane j forms pair j's rotation (in parallel),
+      // then the warp applies each pair with the lanes over the rows, taking the parameters by shuffle.
+      // Columns p, q of a pair are touched by its warp only, so no barrier separates the parameters
+      // from the column update; every element gets the same operations as in a flat task loop.
+      T Pc = T(1), Ps = T(0), Pex = T(1), Pey = T(0);
+      int Pp = -1, Pq = 0;
+      if (lane < mine) {
         int p, q;
-        rr_pair(m, r, i, p, q);
-        RotParam<T> P;
-        P.p = -1;
-        P.q = q;
+        rr_pair(m, r, wt + lane * NWT, p, q);
+        Pq = q;
         if (q < n) {
           C b = A[p + q * lda];
           T ab = sqrt(b.x * b.x + b.y * b.y);
@@ -69,45 +77,59 @@ __device__ int jacobi_team(typename cplx<T>::type* A, int lda, typename cplx<T>:
             else
               t = (tau >= T(0) ? T(1) : T(-1)) / (fabs(tau) + sqrt(T(1) + tau * tau));
             T c = T(1) / sqrt(T(1) + t * t);
-            P.c = c;
-            P.s = t * c;
-            P.e = mk2(b.x / ab, b.y / ab);
-            P.p = p;
+            Pc = c;
+            Ps = t * c;
+            Pex = b.x / ab;
+            Pey = b.y / ab;
+            Pp = p;
             *flag = 1;
           }
         }
-        prm[i] = P;
       }
-      team_sync<TEAM>();
+      __syncwarp();
       // columns: A <- A J, V <- V J
-      for (int task = tid; task < npair * n; task += TEAM) {
-        int i = task / n, row = task % n;
-        RotParam<T> P = prm[i];
-        if (P.p < 0) continue;
-        C ap = A[row + P.p * lda], aq = A[row + P.q * lda];
-        C ec = mk2(P.e.x, -P.e.y);
-        C sp = cmul(ec, aq);
-        C sq = cmul(P.e, ap);
-        A[row + P.p * lda] = mk2(P.c * ap.x - P.s * sp.x, P.c * ap.y - P.s * sp.y);
-        A[row + P.q * lda] = mk2(P.s * sq.x + P.c * aq.x, P.s * sq.y + P.c * aq.y);
+      for (int j = 0; j < mine; ++j) {
+        const int pp = __shfl_sync(0xffffffffu, Pp, j);
+        if (pp < 0) continue;
+        const int pq = __shfl_sync(0xffffffffu, Pq, j);
+        const T c = __shfl_sync(0xffffffffu, Pc, j), sn = __shfl_sync(0xffffffffu, Ps, j);
+        const C e = mk2(__shfl_sync(0xffffffffu, Pex, j), __shfl_sync(0xffffffffu, Pey, j));
+        const C ec = mk2(e.x, -e.y);
+        C* Ap = A + pp * lda;
+        C* Aq = A + pq * lda;
+        for (int row = lane; row < n; row += 32) {
+          const C ap = Ap[row], aq = Aq[row];
+          const C sp = cmul(ec, aq), sq = cmul(e, ap);
+          Ap[row] = mk2(c * ap.x - sn * sp.x, c * ap.y - sn * sp.y);
+          Aq[row] = mk2(sn * sq.x + c * aq.x, sn * sq.y + c * aq.y);
+        }
         if (want_v) {
-          C vp = V[row + P.p * ldv], vq = V[row + P.q * ldv];
-          C tp = cmul(ec, vq), tq = cmul(P.e, vp);
-          V[row + P.p * ldv] = mk2(P.c * vp.x - P.s * tp.x, P.c * vp.y - P.s * tp.y);
-          V[row + P.q * ldv] = mk2(P.s * tq.x + P.c * vq.x, P.s * tq.y + P.c * vq.y);
+          C* Vp = V + pp * ldv;
+          C* Vq = V + pq * ldv;
+          for (int row = lane; row < n; row += 32) {
+            const C vp = Vp[row], vq = Vq[row];
+            const C tp = cmul(ec, vq), tq = cmul(e, vp);
+            Vp[row] = mk2(c * vp.x - sn * tp.x, c * vp.y - sn * tp.y);
+            Vq[row] = mk2(sn * tq.x + c * vq.x, sn * tq.y + c * vq.y);
+          }
         }
       }
       team_sync<TEAM>();
-      // rows: A <- J^H A
-      for (int task = tid; task < npair * n; task += TEAM) {
-        int i = task / n, col = task % n;
-        RotParam<T> P = prm[i];
-        if (P.p < 0) continue;
-        C ap = A[P.p + col * lda], aq = A[P.q + col * lda];
-        C ec = mk2(P.e.x, -P.e.y);
-        C sp = cmul(P.e, aq), sq = cmul(ec, ap);
-        A[P.p + col * lda] = mk2(P.c * ap.x - P.s * sp.x, P.c * ap.y - P.s * sp.y);
-        A[P.q + col * lda] = mk2(P.s * sq.x + P.c * aq.x, P.s * sq.y + P.c * aq.y);
+      // rows: A <- J^H A (the same pairs and parameters, lanes over the columns)
+      for (int j = 0; j < mine; ++j) {
+        const int pp = __shfl_sync(0xffffffffu, Pp, j);
+        if (pp < 0) continue;
+        const int pq = __shfl_sync(0xffffffffu, Pq, j);
+        const T c = __shfl_sync(0xffffffffu, Pc, j), sn = __shfl_sync(0xffffffffu, Ps, j);
+        const C e = mk2(__shfl_sync(0xffffffffu, Pex, j), __shfl_sync(0xffffffffu, Pey, j));
+        const C ec = mk2(e.x, -e.y);
+        for (int col = lane; col < n; col += 32) {
+          C* Ac = A + col * lda;
+          const C ap = Ac[pp], aq = Ac[pq];
+          const C sp = cmul(e, aq), sq = cmul(ec, ap);
+          Ac[pp] = mk2(c * ap.x - sn * sp.x, c * ap.y - sn * sp.y);
+          Ac[pq] = mk2(sn * sq.x + c * aq.x, sn * sq.y + c * aq.y);
+        }
       }
       team_sync<TEAM>();
     }
