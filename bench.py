@@ -482,8 +482,11 @@ def fp64_denominator(args, torch, pipeline, dm, xk_d, xq_d, r_mixed, ws, n_el, v
     s = torch.cuda.current_stream()
     run64 = lambda o: pipeline.run_eph_over_k_and_q(dm, xk_d, xq_d, prec=pipeline.PREC_FP64, k_batch=16,
                                                     sample_stride=args.sample_stride, out=o)
-    r64 = run64(None)  # untimed: sizes the FP64 workspace
+    ctx.profile(True)
+    r64 = run64(None)  # untimed: sizes the FP64 workspace; its per-family profile goes into the line
     torch.cuda.synchronize()
+    prof64 = {k: round(v[0], 1) for k, v in ctx.profile_read(reset=True).items() if v[1]}
+    ctx.profile(False)
     if ws > 1:
         torch.distributed.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -533,7 +536,8 @@ def fp64_denominator(args, torch, pipeline, dm, xk_d, xq_d, r_mixed, ws, n_el, v
             "kept_set": "identical by construction (all bands, every (k, q) pair in both paths)",
             "roofline": {"bound": "fp64", "achieved": round(tf64, 2), "peak": round(p64, 2), "unit": "TFLOP/s",
                          "frac": round(tf64 / p64, 4), "peak_source": "measured live: cuBLAS DGEMM 8192^3",
-                         "note": "whole FP64 pass: FP64 Fourier sums and ZGEMM on CUDA cores, FP64 Jacobi"}}
+                         "note": "whole FP64 pass: FP64 Fourier sums and ZGEMM on CUDA cores, FP64 Jacobi"},
+            "profile_ms": prof64}
 
 
 def m_host_for_cpu(m, ep_dev):

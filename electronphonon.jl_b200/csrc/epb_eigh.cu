@@ -109,7 +109,7 @@ __global__ void eigh_kernel(EighArgs a) {
     team_sync<TEAM>();
     const T eps = sizeof(T) == 8 ? T(2.220446049250313e-16) : T(1.1920929e-07);
     const T thr = eps * sqrt(tot) / T(n > 0 ? n : 1);
-    int sweeps = jacobi_team<T, TEAM>(As, lda, Vs, n, n, a.want_v != 0, flag, thr, a.max_sweeps);
+    int sweeps = jacobi_team<T, TEAM>(As, lda, Vs, n, n, a.want_v != 0, prm, flag, thr, a.max_sweeps);
     if (sweeps >= a.max_sweeps && tid == 0) atomicAdd(a.nonconv, 1);
     // sort eigenvalues ascending (rank by value, ties by index) and write out
     for (int i = tid; i < n; i += TEAM) {
@@ -168,6 +168,7 @@ __global__ void eigh_mixed_kernel(EighArgs a) {
   float2* V32 = A32 + NMAX * LDA;
   double2* S = reinterpret_cast<double2*>(R);
   RotParam<double>* prm64 = reinterpret_cast<RotParam<double>*>(base + 2 * h64 + regR);
+  RotParam<float>* prm32 = reinterpret_cast<RotParam<float>*>(prm64);
   int* flag = reinterpret_cast<int*>(prm64 + NMAX / 2 + 1);
   __shared__ double red[TEAMS * (TEAM / 32)];
 
@@ -217,7 +218,7 @@ __global__ void eigh_mixed_kernel(EighArgs a) {
     const double fro = sqrt(tot);
     // FP32 stop at 8 eps32 x the RMS eigenvalue (rounding of degenerate pairs stays below it); the FP64
     // stage below supplies the accuracy
-    int sw = jacobi_team<float, TEAM>(A32, lda, V32, n, n, true, flag,
+    int sw = jacobi_team<float, TEAM>(A32, lda, V32, n, n, true, prm32, flag,
                                       8.f * 1.1920929e-07f * (float)(fro / sqrt((double)n)), a.max_sweeps);
     if (sw >= a.max_sweeps && tid == 0) atomicAdd(a.nonconv, 1);
     // V64 <- V32, then modified Gram-Schmidt (column by column)
@@ -227,29 +228,40 @@ __global__ void eigh_mixed_kernel(EighArgs a) {
       V[i + j * lda] = make_double2(v.x, v.y);
     }
     team_sync<TEAM>();
-    for (int j = 0; j < n; ++j) {
-      // norm of column j (one thread; n <= 64 so this is cheap relative to the n^3 work below)
-      if (tid == 0) {
-        double s = 0;
-        for (int i = 0; i < n; ++i) s += V[i + j * lda].x * V[i + j * lda].x + V[i + j * lda].y * V[i + j * lda].y;
-        red[team * (TEAM / 32)] = 1.0 / sqrt(s);
-      }
-      team_sync<TEAM>();
-      double inv = red[team * (TEAM / 32)];
-      for (int i = tid; i < n; i += TEAM) {
-        V[i + j * lda].x *= inv;
-        V[i + j * lda].y *= inv;
-      }
-      team_sync<TEAM>();
-      // project column j out of columns > j
-      for (int c = j + 1 + tid; c < n; c += TEAM) {
-        double2 d = make_double2(0, 0);
-        for (int i = 0; i < n; ++i) cfma_conj(d, V[i + j * lda], V[i + c * lda]);
-        for (int i = 0; i < n; ++i) {
-          double2 vj = V[i + j * lda];
-          V[i + c * lda].x -= d.x * vj.x - d.y * vj.y;
-          V[i + c * lda].y -= d.x * vj.y + d.y * vj.x;
+    // Modified Gram-Schmidt, one barrier per column: every warp forms the norm of column j itself (lanes
+    // over the rows, butterfly sum, the same order in every warp), the projections use the unnormalised
+    // column j with 1 / |v_j|^2, and column j is scaled in the next column's phase, where nobody reads it.
+    {
+      const int lane = tid & 31;
+      double inv_prev = 1.0;
+      for (int j = 0; j < n; ++j) {
+        double s2 = 0.0;
+        for (int i = lane; i < n; i += 32) s2 += V[i + j * lda].x * V[i + j * lda].x + V[i + j * lda].y * V[i + j * lda].y;
+        for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+        const double inv2 = 1.0 / s2;
+        if (j > 0)
+          for (int i = tid; i < n; i += TEAM) {
+            V[i + (j - 1) * lda].x *= inv_prev;
+            V[i + (j - 1) * lda].y *= inv_prev;
+          }
+        // project column j out of columns > j
+        for (int c = j + 1 + tid; c < n; c += TEAM) {
+          double2 d = make_double2(0, 0);
+          for (int i = 0; i < n; ++i) cfma_conj(d, V[i + j * lda], V[i + c * lda]);
+          d.x *= inv2;
+          d.y *= inv2;
+          for (int i = 0; i < n; ++i) {
+            double2 vj = V[i + j * lda];
+            V[i + c * lda].x -= d.x * vj.x - d.y * vj.y;
+            V[i + c * lda].y -= d.x * vj.y + d.y * vj.x;
+          }
         }
+        inv_prev = sqrt(inv2);
+        team_sync<TEAM>();
+      }
+      for (int i = tid; i < n; i += TEAM) {
+        V[i + (n - 1) * lda].x *= inv_prev;
+        V[i + (n - 1) * lda].y *= inv_prev;
       }
       team_sync<TEAM>();
     }
@@ -284,18 +296,9 @@ __global__ void eigh_mixed_kernel(EighArgs a) {
       S[i + c * n] = make_double2(i == c ? 1.0 : 0.0, 0.0);
     }
     team_sync<TEAM>();
-    jacobi_team<double, TEAM>(H, lda, S, n, n, true, flag, 2.220446049250313e-16 * fro / n, 8);
-    // V <- V Q, written in place row by row (each thread owns whole rows)
-    for (int i = tid; i < n; i += TEAM) {
-      double2 row[NMAX];
-      for (int c = 0; c < n; ++c) {
-        double2 acc = make_double2(0, 0);
-        for (int k = 0; k < n; ++k) cfma(acc, V[i + k * lda], S[k + c * n]);
-        row[c] = acc;
-      }
-      for (int c = 0; c < n; ++c) V[i + c * lda] = row[c];
-    }
-    team_sync<TEAM>();
+    jacobi_team<double, TEAM>(H, lda, S, n, n, true, prm64, flag, 2.220446049250313e-16 * fro / n, 8);
+    // eigenvalue ranks, then the eigenvectors V Q straight into their sorted output columns (one thread per
+    // output entry; Q is the rotation accumulated in S)
     for (int i = tid; i < n; i += TEAM) {
       double ei = H[i + i * lda].x;
       int rank = 0;
@@ -311,13 +314,14 @@ __global__ void eigh_mixed_kernel(EighArgs a) {
     team_sync<TEAM>();
     if (a.want_v) {
       for (int e = tid; e < n * n; e += TEAM) {
-        int row = e % n, col = e / n;
-        int rank = (int)H[col + col * lda].y;
-        double2 o = V[row + col * lda];
+        const int row = e % n, col = e / n;
+        const int rank = (int)H[col + col * lda].y;
+        double2 o = make_double2(0, 0);
+        for (int k = 0; k < n; ++k) cfma(o, V[row + k * lda], S[k + col * n]);
         if (a.mass) {
-          double s = 1.0 / sqrt(a.mass[row]);
-          o.x *= s;
-          o.y *= s;
+          double sc = 1.0 / sqrt(a.mass[row]);
+          o.x *= sc;
+          o.y *= sc;
         }
         if (a.U32)
           a.U32[b * (int64_t)n * n + row + (int64_t)rank * n] = make_float2((float)o.x, (float)o.y);
@@ -369,7 +373,8 @@ static int launch_eigh(epb_ctx* ctx, Kern kern, size_t smem, int threads, EighAr
   return EPB_OK;
 }
 
-// Dispatch on max order and precision.
+// Dispatch on max order and precision. The mixed solver of orders 33..48 has its own instance: its shared
+// memory (111 KB per team) lets two teams share an SM, against one at orders up to 64.
 int eigh_dispatch(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
   if (prec == EPB_PREC_FP64) {
     if (nmax <= 16)
@@ -383,6 +388,8 @@ int eigh_dispatch(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
       return launch_eigh(ctx, eigh_mixed_kernel<32, 16>, eigh_mixed_smem<32, 16>(), 128, a);
     if (nmax <= 32)
       return launch_eigh(ctx, eigh_mixed_kernel<32, 32>, eigh_mixed_smem<32, 32>(), 128, a);
+    if (nmax <= 48)
+      return launch_eigh(ctx, eigh_mixed_kernel<128, 48>, eigh_mixed_smem<128, 48>(), 128, a);
     if (nmax <= 64)
       return launch_eigh(ctx, eigh_mixed_kernel<128, 64>, eigh_mixed_smem<128, 64>(), 128, a);
   } else {
@@ -491,6 +498,8 @@ static int eigh_small(epb_ctx* ctx, const EighArgs& a, int prec) {
 
 int eigh_big_launch(epb_ctx* ctx, double2* A, const int64_t* a_off, const int32_t* nvec, int n_uniform, int64_t batch,
                     double* E, const int64_t* e_off, bool want_v, int n_lo, int prec, int* nonconv, int* badsize);
+int eigh_mid_launch(epb_ctx* ctx, double2* A, const int64_t* a_off, const int32_t* nvec, int n_uniform, int64_t batch,
+                    double* E, const int64_t* e_off, bool want_v, int n_lo, int* nonconv, int* badsize);
 
 // Orders of a varlen batch outside 0..96 (no kernel handles them; order 0 is an empty matrix).
 __global__ void eigh_badorder_kernel(const int32_t* __restrict__ nvec, int64_t batch, int* __restrict__ badsize) {
@@ -504,7 +513,8 @@ __global__ void eigh_badorder_kernel(const int32_t* __restrict__ nvec, int64_t b
 }
 
 // The varlen batch without any host read-back (capturable in a CUDA graph): every size class kernel runs
-// -- orders 1..16, 17..32, 33..64 on the shared-memory Jacobi, 65..96 on the persistent big kernel -- each
+// -- orders 1..16, 17..32, 33..48 (FP64: 33..64) on the shared-memory Jacobi, 49..64 (mixed) and 65..96 on
+// the persistent L2-scratch solver -- each
 // taking the matrices of its class from the whole batch and skipping the others; orders outside 0..96 are
 // counted into the status words that eigh_check reads.
 int eigh_varlen_async(epb_ctx* ctx, EighArgs& a, int prec) {
@@ -522,8 +532,12 @@ int eigh_varlen_async(epb_ctx* ctx, EighArgs& a, int prec) {
     EighArgs s = a;
     s.n_lo = lo[c];
     s.skip_hi = 1;
-    EPB_TRY(eigh_dispatch(ctx, s, hi[c], prec));
+    // mixed: 33..48 here (two teams per SM), 49..64 on the L2-scratch solver below
+    EPB_TRY(eigh_dispatch(ctx, s, prec == EPB_PREC_MIXED && c == 2 ? 48 : hi[c], prec));
   }
+  if (prec == EPB_PREC_MIXED)
+    EPB_TRY(eigh_mid_launch(ctx, a.A, a.a_off, a.nvec, 0, a.batch, a.E, a.e_off, a.want_v != 0, 48, a.nonconv,
+                            a.badsize));
   return eigh_big_launch(ctx, a.A, a.a_off, a.nvec, 0, a.batch, a.E, a.e_off, a.want_v != 0, 64, prec, a.nonconv,
                          a.badsize);
 }
@@ -539,6 +553,9 @@ int eigh_run(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
     const int n = a.n_uniform;
     if (n <= 16)
       EPB_TRY(eigh_small(ctx, a, prec));
+    else if (n > 48 && n <= 64 && prec == EPB_PREC_MIXED && !a.mass && !a.Hp && !a.U32)
+      EPB_TRY(eigh_mid_launch(ctx, a.A, nullptr, nullptr, n, a.batch, a.E, nullptr, a.want_v != 0, 0, a.nonconv,
+                              a.badsize));
     else if (n <= 64)
       EPB_TRY(eigh_dispatch(ctx, a, n, prec));
     else if (n <= 96) {

@@ -5,7 +5,7 @@
 // src/wannier_to_bloch_batched.jl:30-65, LAPACK ZHEEV) for the orders whose FP64 Jacobi state
 // (A and V, 2 n^2 complex doubles) does not fit in shared memory.
 //
-// One CTA (256 threads) per matrix, persistent, matrices taken from a device work counter so that
+// One CTA (512 threads) per matrix, persistent, matrices taken from a device work counter so that
 // uneven orders balance. Per matrix:
 //  1. A (Hermitian completion of the upper triangle) in FP32 in shared memory, cyclic two-sided
 //     Jacobi with round-robin pairs (jacobi_team) accumulating V in FP32.
@@ -27,7 +27,6 @@
 
 namespace epb {
 
-constexpr int BIG_T = 256;
 constexpr int BIG_NMAX = 96;
 
 struct BigArgs {
@@ -51,19 +50,20 @@ struct BigArgs {
 // Complex FP64 n x n GEMM, C = op(A) B, operands in global memory (L2-resident scratch or the input),
 // 32 x 32 output tiles staged through shared memory. OPA: 0 = A, 1 = A^H, 2 = Hermitian completion of
 // the upper triangle of A (diagonal imaginary part dropped).
-template <int OPA>
+template <int OPA, int NT>
 __device__ void big_gemm(int n, const double2* __restrict__ A, int lda, const double2* __restrict__ B, int ldb,
                          double2* __restrict__ C, int ldc, double2* As, double2* Bs) {
+  constexpr int NWB = NT / 32, RPT = 32 / NWB;  // warps; output rows per thread (ty + NWB r)
   const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
   const int nt = (n + 31) / 32;
   for (int t = 0; t < nt * nt; ++t) {
     const int i0 = (t % nt) * 32, j0 = (t / nt) * 32;
-    double2 acc[4];
+    double2 acc[RPT];
 #pragma unroll
-    for (int r = 0; r < 4; ++r) acc[r] = make_double2(0.0, 0.0);
+    for (int r = 0; r < RPT; ++r) acc[r] = make_double2(0.0, 0.0);
     for (int k0 = 0; k0 < n; k0 += 32) {
       __syncthreads();
-      for (int e = tid; e < 1024; e += BIG_T) {
+      for (int e = tid; e < 1024; e += NT) {
         const int r = e & 31, c = e >> 5;  // As[r][c] = op(A)(i0 + r, k0 + c); Bs[c][r] = B(k0 + c, j0 + r)
         const int i = i0 + r, k = k0 + c;
         double2 v = make_double2(0.0, 0.0);
@@ -92,59 +92,63 @@ __device__ void big_gemm(int n, const double2* __restrict__ A, int lda, const do
       for (int kk = 0; kk < 32; ++kk) {
         const double2 b = Bs[kk * 33 + tx];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) cfma(acc[r], As[(ty + 8 * r) * 33 + kk], b);
+        for (int r = 0; r < RPT; ++r) cfma(acc[r], As[(ty + NWB * r) * 33 + kk], b);
       }
     }
-    // C(i0 + ty + 8r, j0 + tx)
+    // C(i0 + ty + NWB r, j0 + tx)
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int i = i0 + ty + 8 * r, j = j0 + tx;
+    for (int r = 0; r < RPT; ++r) {
+      const int i = i0 + ty + NWB * r, j = j0 + tx;
       if (i < n && j < n) C[i + (int64_t)j * ldc] = acc[r];
     }
   }
   __syncthreads();
 }
 
+template <int NT>
 __device__ __forceinline__ double block_max(double v, double* red) {
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   __syncthreads();
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
   __syncthreads();
   double m = 0.0;
-  for (int w = 0; w < BIG_T / 32; ++w) m = fmax(m, red[w]);
+  for (int w = 0; w < NT / 32; ++w) m = fmax(m, red[w]);
   __syncthreads();
   return m;
 }
 
 // Shared memory: FP32 Jacobi state (A32 NMAX x (NMAX+1), V32 NMAX x NMAX, rotation parameters),
 // reused by the refinement for GEMM tiles and the cluster solve.
+template <int NMAX>
 struct BigSmem {
-  static constexpr int A32 = BIG_NMAX * (BIG_NMAX + 1) * 8;
-  static constexpr int V32 = BIG_NMAX * BIG_NMAX * 8;
-  static constexpr int PRM = (BIG_NMAX / 2 + 1) * 64;
+  static constexpr int A32 = NMAX * (NMAX + 1) * 8;
+  static constexpr int V32 = NMAX * NMAX * 8;
+  static constexpr int PRM = (NMAX / 2 + 1) * 64;
   static constexpr int JAC = A32 + V32 + PRM + 64;
   static constexpr int TILES = 2 * 32 * 33 * 16;
   static constexpr int CLU = 32 * 33 * 16 + 32 * 32 * 16 + 17 * 64 + 64;
   static constexpr int REF = TILES > CLU ? TILES : CLU;
-  static constexpr int TOTAL = (JAC > REF ? JAC : REF) + 4 * BIG_NMAX * 8 + 64 * 8;
+  static constexpr int TOTAL = (JAC > REF ? JAC : REF) + 4 * NMAX * 8 + 64 * 8;
 };
 
-__global__ void __launch_bounds__(BIG_T, 1) eigh_big_kernel(BigArgs a) {
+template <int NMAX, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) eigh_big_kernel(BigArgs a) {
+  using SM = BigSmem<NMAX>;
   extern __shared__ __align__(16) unsigned char sm[];
   // per-matrix vectors after the union region
-  constexpr int U = BigSmem::TOTAL - 4 * BIG_NMAX * 8 - 64 * 8;
+  constexpr int U = SM::TOTAL - 4 * NMAX * 8 - 64 * 8;
   double* lam = reinterpret_cast<double*>(sm + U);           // NMAX
-  int* rank = reinterpret_cast<int*>(lam + BIG_NMAX);         // NMAX
-  int* perm = rank + BIG_NMAX;                                // NMAX
-  int* cid = perm + BIG_NMAX;                                 // NMAX
-  int* csize = cid + BIG_NMAX;                                // NMAX (cluster sizes by first sorted index)
-  double* red = reinterpret_cast<double*>(sm + BigSmem::TOTAL - 64 * 8);  // reductions, flags
+  int* rank = reinterpret_cast<int*>(lam + NMAX);         // NMAX
+  int* perm = rank + NMAX;                                // NMAX
+  int* cid = perm + NMAX;                                 // NMAX
+  int* csize = cid + NMAX;                                // NMAX (cluster sizes by first sorted index)
+  double* red = reinterpret_cast<double*>(sm + SM::TOTAL - 64 * 8);  // reductions, flags
   __shared__ long long s_b;
   __shared__ int s_flag;
-  double2* slab = a.scratch + (int64_t)blockIdx.x * 3 * BIG_NMAX * BIG_NMAX;
+  double2* slab = a.scratch + (int64_t)blockIdx.x * 3 * NMAX * NMAX;
   double2* V = slab;
-  double2* W = slab + BIG_NMAX * BIG_NMAX;
-  double2* G = slab + 2 * BIG_NMAX * BIG_NMAX;
+  double2* W = slab + NMAX * NMAX;
+  double2* G = slab + 2 * NMAX * NMAX;
   const int tid = threadIdx.x;
 
   for (;;) {
@@ -155,7 +159,7 @@ __global__ void __launch_bounds__(BIG_T, 1) eigh_big_kernel(BigArgs a) {
     if (b >= a.batch) break;
     const int n = a.nvec ? a.nvec[b] : a.n_uniform;
     if (n <= a.n_lo) continue;
-    if (n > BIG_NMAX) {
+    if (n > NMAX) {
       if (tid == 0 && a.n_lo == 0) atomicAdd(a.badsize, 1);  // varlen batches count bad orders on the host
       continue;
     }
@@ -165,11 +169,12 @@ __global__ void __launch_bounds__(BIG_T, 1) eigh_big_kernel(BigArgs a) {
 
     // ---- 1. FP32 Jacobi ----
     float2* A32 = reinterpret_cast<float2*>(sm);
-    float2* V32 = reinterpret_cast<float2*>(sm + BigSmem::A32);
-    int* flag = reinterpret_cast<int*>(sm + BigSmem::A32 + BigSmem::V32 + BigSmem::PRM);
+    float2* V32 = reinterpret_cast<float2*>(sm + SM::A32);
+    void* prm = sm + SM::A32 + SM::V32;
+    int* flag = reinterpret_cast<int*>(sm + SM::A32 + SM::V32 + SM::PRM);
     const int lda = n + 1;
     double fro2 = 0.0;
-    for (int e = tid; e < n * n; e += BIG_T) {
+    for (int e = tid; e < n * n; e += NT) {
       const int i = e % n, j = e / n;
       double2 v;
       if (i <= j) {
@@ -188,15 +193,15 @@ __global__ void __launch_bounds__(BIG_T, 1) eigh_big_kernel(BigArgs a) {
     if ((tid & 31) == 0) red[tid >> 5] = fro2;
     __syncthreads();
     double fro = 0.0;
-    for (int w = 0; w < BIG_T / 32; ++w) fro += red[w];
+    for (int w = 0; w < NT / 32; ++w) fro += red[w];
     fro = sqrt(fro);
     __syncthreads();
     // stop at 8 eps32 x the RMS eigenvalue: below that, FP32 rounding of (near-)degenerate pairs would
     // re-trigger 45-degree rotations forever; the FP64 refinement supplies the remaining accuracy
-    const int sw = jacobi_team<float, BIG_T>(A32, lda, V32, n, n, true, flag,
+    const int sw = jacobi_team<float, NT>(A32, lda, V32, n, n, true, reinterpret_cast<RotParam<float>*>(prm), flag,
                                              8.f * 1.1920929e-07f * (float)(fro / sqrt((double)n)), a.max_sweeps);
     if (sw >= a.max_sweeps && tid == 0) atomicAdd(a.nonconv, 1);
-    for (int e = tid; e < n * n; e += BIG_T) {
+    for (int e = tid; e < n * n; e += NT) {
       const float2 v = V32[e];
       V[e] = make_double2(v.x, v.y);
     }
@@ -207,24 +212,24 @@ __global__ void __launch_bounds__(BIG_T, 1) eigh_big_kernel(BigArgs a) {
     double2* Bs = As + 32 * 33;
     for (int it = 0; it <= a.refine; ++it) {
       // Loewdin: G = V^H V; W = V (3/2 I - 1/2 G); swap
-      big_gemm<1>(n, V, n, V, n, G, n, As, Bs);
-      for (int e = tid; e < n * n; e += BIG_T) {
+      big_gemm<1, NT>(n, V, n, V, n, G, n, As, Bs);
+      for (int e = tid; e < n * n; e += NT) {
         const int i = e % n, j = e / n;
         double2 g = G[e];
         G[e] = make_double2((i == j ? 1.5 : 0.0) - 0.5 * g.x, -0.5 * g.y);
       }
       __syncthreads();
-      big_gemm<0>(n, V, n, G, n, W, n, As, Bs);
+      big_gemm<0, NT>(n, V, n, G, n, W, n, As, Bs);
       {
         double2* t = V;
         V = W;
         W = t;
       }
       // S = V^H (H V)
-      big_gemm<2>(n, H, n, V, n, W, n, As, Bs);
-      big_gemm<1>(n, V, n, W, n, G, n, As, Bs);
+      big_gemm<2, NT>(n, H, n, V, n, W, n, As, Bs);
+      big_gemm<1, NT>(n, V, n, W, n, G, n, As, Bs);
       double off = 0.0, dmax = 0.0;
-      for (int e = tid; e < n * n; e += BIG_T) {
+      for (int e = tid; e < n * n; e += NT) {
         const int i = e % n, j = e / n;
         const double2 s = G[e];
         if (i == j) {
@@ -235,10 +240,10 @@ __global__ void __launch_bounds__(BIG_T, 1) eigh_big_kernel(BigArgs a) {
         }
       }
       __syncthreads();
-      off = block_max(off, red);
-      dmax = block_max(dmax, red);
+      off = block_max<NT>(off, red);
+      dmax = block_max<NT>(dmax, red);
       // ascending order (ties by index)
-      for (int i = tid; i < n; i += BIG_T) {
+      for (int i = tid; i < n; i += NT) {
         int r = 0;
         for (int j = 0; j < n; ++j) r += (lam[j] < lam[i]) || (lam[j] == lam[i] && j < i);
         rank[i] = r;
@@ -269,7 +274,7 @@ __global__ void __launch_bounds__(BIG_T, 1) eigh_big_kernel(BigArgs a) {
       __syncthreads();
       if (s_flag && tid == 0) atomicAdd(a.nonconv, 1);  // oversize cluster: first-order only within it
       // M (in W): first-order Rayleigh-Ritz between clusters, identity inside clusters for now
-      for (int e = tid; e < n * n; e += BIG_T) {
+      for (int e = tid; e < n * n; e += NT) {
         const int i = e % n, j = e / n;
         double2 m = make_double2(i == j ? 1.0 : 0.0, 0.0);
         if (i != j && cid[i] != cid[j]) {
@@ -295,7 +300,7 @@ __global__ void __launch_bounds__(BIG_T, 1) eigh_big_kernel(BigArgs a) {
               Qc[p + q * k] = make_double2(p == q ? 1.0 : 0.0, 0.0);
             }
             __syncwarp();
-            jacobi_team<double, 32>(Ac, 33, Qc, k, k, true, flc,
+            jacobi_team<double, 32>(Ac, 33, Qc, k, k, true, reinterpret_cast<RotParam<double>*>(prmc), flc,
                                     2.220446049250313e-16 * fmax(dmax, 1e-300), 30);
             // M[:, c] <- M[:, c] Q_c: the cluster columns of (I + X) rotated into the cluster's eigenbasis
             for (int i = tid; i < n; i += 32) {
@@ -314,7 +319,7 @@ __global__ void __launch_bounds__(BIG_T, 1) eigh_big_kernel(BigArgs a) {
       }
       __syncthreads();
       // V <- V M
-      big_gemm<0>(n, V, n, W, n, G, n, As, Bs);
+      big_gemm<0, NT>(n, V, n, W, n, G, n, As, Bs);
       {
         double2* t = V;
         V = G;
@@ -323,17 +328,17 @@ __global__ void __launch_bounds__(BIG_T, 1) eigh_big_kernel(BigArgs a) {
     }
     // outputs: eigenvalues ascending, eigenvectors over the input (column rank[i] = V[:, i])
     if (a.E)
-      for (int i = tid; i < n; i += BIG_T) a.E[eoff + rank[i]] = lam[i];
+      for (int i = tid; i < n; i += NT) a.E[eoff + rank[i]] = lam[i];
     if (a.want_v)
-      for (int e = tid; e < n * n; e += BIG_T) {
+      for (int e = tid; e < n * n; e += NT) {
         const int row = e % n, col = e / n;
         H[row + (int64_t)rank[col] * n] = V[e];
       }
     __syncthreads();
     // restore the slab order for the next matrix
     V = slab;
-    W = slab + BIG_NMAX * BIG_NMAX;
-    G = slab + 2 * BIG_NMAX * BIG_NMAX;
+    W = slab + NMAX * NMAX;
+    G = slab + 2 * NMAX * NMAX;
   }
 }
 
@@ -341,20 +346,39 @@ __global__ void __launch_bounds__(BIG_T, 1) eigh_big_kernel(BigArgs a) {
 
 namespace epb {
 
+// One instance of the persistent solver over a (uniform or varlen) batch: orders in (n_lo, NMAX] are solved,
+// the others left to the other kernels. The L2 scratch slab (3 NMAX^2 complex doubles per CTA) shares the
+// workspace slot of every instance; its size is that of the largest instance, so that the slot is not
+// reallocated between the launches of one varlen batch (which may be captured in a graph).
+template <int NMAX, int NT, int MINB>
+static int launch_big(epb_ctx* ctx, BigArgs a, int64_t batch) {
+  using SM = BigSmem<NMAX>;
+  static bool attr = false;
+  if (!attr) {
+    EPB_CUDA(cudaFuncSetAttribute(eigh_big_kernel<NMAX, NT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  SM::TOTAL));
+    attr = true;
+  }
+  const int64_t grid = std::min<int64_t>((int64_t)ctx->sm_count * MINB, batch);
+  const size_t slab_max = (size_t)3 * BIG_NMAX * BIG_NMAX * sizeof(double2) * (size_t)ctx->sm_count;
+  const size_t slab = (size_t)3 * NMAX * NMAX * sizeof(double2) * (size_t)grid;
+  void* ws = nullptr;
+  EPB_TRY(ws_get(ctx, EPB_WS_EIGH_BIG, (slab > slab_max ? slab : slab_max) + 256, &ws));
+  a.scratch = (double2*)((uint8_t*)ws + 256);
+  a.counter = (unsigned long long*)ws;
+  EPB_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), ctx->stream));
+  prof_begin(ctx, EPB_PROF_EIGH);
+  eigh_big_kernel<NMAX, NT, MINB><<<(unsigned)grid, NT, SM::TOTAL, ctx->stream>>>(a);
+  prof_end(ctx);
+  EPB_LAUNCH_CHECK();
+  return EPB_OK;
+}
+
 // Launch the order-65..96 solver over a (uniform or varlen) batch; matrices of order <= n_lo are
 // left to the other kernels. Status words as in the other eigensolvers.
 int eigh_big_launch(epb_ctx* ctx, double2* A, const int64_t* a_off, const int32_t* nvec, int n_uniform, int64_t batch,
                     double* E, const int64_t* e_off, bool want_v, int n_lo, int prec, int* nonconv, int* badsize) {
   if (batch == 0) return EPB_OK;
-  static bool attr = false;
-  if (!attr) {
-    EPB_CUDA(cudaFuncSetAttribute(eigh_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, BigSmem::TOTAL));
-    attr = true;
-  }
-  const int64_t grid = std::min<int64_t>((int64_t)ctx->sm_count, batch);
-  const size_t slab = (size_t)3 * BIG_NMAX * BIG_NMAX * sizeof(double2);
-  void* ws = nullptr;
-  EPB_TRY(ws_get(ctx, EPB_WS_EIGH_BIG, slab * grid + 256, &ws));
   BigArgs a{};
   a.A = A;
   a.a_off = a_off;
@@ -369,14 +393,30 @@ int eigh_big_launch(epb_ctx* ctx, double2* A, const int64_t* a_off, const int32_
   a.n_lo = n_lo;
   a.nonconv = nonconv;
   a.badsize = badsize;
-  a.scratch = (double2*)((uint8_t*)ws + 256);
-  a.counter = (unsigned long long*)ws;
-  EPB_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), ctx->stream));
-  prof_begin(ctx, EPB_PROF_EIGH);
-  eigh_big_kernel<<<(unsigned)grid, BIG_T, BigSmem::TOTAL, ctx->stream>>>(a);
-  prof_end(ctx);
-  EPB_LAUNCH_CHECK();
-  return EPB_OK;
+  return launch_big<BIG_NMAX, 512, 1>(ctx, a, batch);
+}
+
+// The same solver for orders 49..64 (mixed precision, c128 in and out): 69 KB of shared memory and 256
+// threads per CTA, two CTAs per SM (the shared-memory FP64 Rayleigh-Ritz solver of epb_eigh.cu keeps H, V
+// and S in FP64 in shared memory, 200 KB at order 64, one team per SM).
+int eigh_mid_launch(epb_ctx* ctx, double2* A, const int64_t* a_off, const int32_t* nvec, int n_uniform, int64_t batch,
+                    double* E, const int64_t* e_off, bool want_v, int n_lo, int* nonconv, int* badsize) {
+  if (batch == 0) return EPB_OK;
+  BigArgs a{};
+  a.A = A;
+  a.a_off = a_off;
+  a.nvec = nvec;
+  a.n_uniform = n_uniform;
+  a.batch = batch;
+  a.E = E;
+  a.e_off = e_off;
+  a.want_v = want_v ? 1 : 0;
+  a.max_sweeps = 20;
+  a.refine = 2;
+  a.n_lo = n_lo;
+  a.nonconv = nonconv;
+  a.badsize = badsize;
+  return launch_big<64, 256, 2>(ctx, a, batch);
 }
 
 }  // namespace epb

@@ -40,7 +40,7 @@ struct RotParam {
 // Returns the number of sweeps used (max_sweeps + 1 if not converged, or if n > 64 TEAM / 32).
 template <typename T, int TEAM>
 __device__ int jacobi_team(typename cplx<T>::type* A, int lda, typename cplx<T>::type* V, int ldv,
-                           int n, bool want_v, int* flag, T thr, int max_sweeps) {
+                           int n, bool want_v, RotParam<T>* prm, int* flag, T thr, int max_sweeps) {
   using C = typename cplx<T>::type;
   static_assert(TEAM % 32 == 0, "jacobi_team: the team is whole warps");
   constexpr int NWT = TEAM / 32;  // warps of the team
@@ -55,16 +55,18 @@ __device__ int jacobi_team(typename cplx<T>::type* A, int lda, typename cplx<T>:
     if (tid == 0) *flag = 0;
     team_sync<TEAM>();
     for (int r = 0; r < m - 1; ++r) {
-      // A warp owns the pairs wt + j NWT (j < mine <= 32): lane j forms pair j's rotation (in parallel),
-      // then the warp applies each pair with the lanes over the rows, taking the parameters by shuffle.
-      // Columns p, q of a pair are touched by its warp only, so no barrier separates the parameters
-      // from the column update; every element gets the same operations as in a flat task loop.
-      T Pc = T(1), Ps = T(0), Pex = T(1), Pey = T(0);
-      int Pp = -1, Pq = 0;
+      // A warp owns the pairs wt + j NWT (j < mine <= 32): lane j forms pair j's rotation (in parallel)
+      // into the team's parameter slots, then the warp applies each pair with the lanes over the rows
+      // (a broadcast read of the slot). Columns p, q of a pair are touched by its warp only, so the
+      // parameters need no barrier before the column update; every element gets the same operations as
+      // in a flat (pair, row) task loop.
       if (lane < mine) {
+        const int i = wt + lane * NWT;
         int p, q;
-        rr_pair(m, r, wt + lane * NWT, p, q);
-        Pq = q;
+        rr_pair(m, r, i, p, q);
+        RotParam<T> P;
+        P.p = -1;
+        P.q = q;
         if (q < n) {
           C b = A[p + q * lda];
           T ab = sqrt(b.x * b.x + b.y * b.y);
@@ -77,58 +79,52 @@ __device__ int jacobi_team(typename cplx<T>::type* A, int lda, typename cplx<T>:
             else
               t = (tau >= T(0) ? T(1) : T(-1)) / (fabs(tau) + sqrt(T(1) + tau * tau));
             T c = T(1) / sqrt(T(1) + t * t);
-            Pc = c;
-            Ps = t * c;
-            Pex = b.x / ab;
-            Pey = b.y / ab;
-            Pp = p;
+            P.c = c;
+            P.s = t * c;
+            P.e = mk2(b.x / ab, b.y / ab);
+            P.p = p;
             *flag = 1;
           }
         }
+        prm[i] = P;
       }
       __syncwarp();
       // columns: A <- A J, V <- V J
-      for (int j = 0; j < mine; ++j) {
-        const int pp = __shfl_sync(0xffffffffu, Pp, j);
-        if (pp < 0) continue;
-        const int pq = __shfl_sync(0xffffffffu, Pq, j);
-        const T c = __shfl_sync(0xffffffffu, Pc, j), sn = __shfl_sync(0xffffffffu, Ps, j);
-        const C e = mk2(__shfl_sync(0xffffffffu, Pex, j), __shfl_sync(0xffffffffu, Pey, j));
-        const C ec = mk2(e.x, -e.y);
-        C* Ap = A + pp * lda;
-        C* Aq = A + pq * lda;
+      for (int i = wt; i < npair; i += NWT) {
+        const RotParam<T> P = prm[i];
+        if (P.p < 0) continue;
+        const C ec = mk2(P.e.x, -P.e.y);
+        C* Ap = A + P.p * lda;
+        C* Aq = A + P.q * lda;
         for (int row = lane; row < n; row += 32) {
           const C ap = Ap[row], aq = Aq[row];
-          const C sp = cmul(ec, aq), sq = cmul(e, ap);
-          Ap[row] = mk2(c * ap.x - sn * sp.x, c * ap.y - sn * sp.y);
-          Aq[row] = mk2(sn * sq.x + c * aq.x, sn * sq.y + c * aq.y);
+          const C sp = cmul(ec, aq), sq = cmul(P.e, ap);
+          Ap[row] = mk2(P.c * ap.x - P.s * sp.x, P.c * ap.y - P.s * sp.y);
+          Aq[row] = mk2(P.s * sq.x + P.c * aq.x, P.s * sq.y + P.c * aq.y);
         }
         if (want_v) {
-          C* Vp = V + pp * ldv;
-          C* Vq = V + pq * ldv;
+          C* Vp = V + P.p * ldv;
+          C* Vq = V + P.q * ldv;
           for (int row = lane; row < n; row += 32) {
             const C vp = Vp[row], vq = Vq[row];
-            const C tp = cmul(ec, vq), tq = cmul(e, vp);
-            Vp[row] = mk2(c * vp.x - sn * tp.x, c * vp.y - sn * tp.y);
-            Vq[row] = mk2(sn * tq.x + c * vq.x, sn * tq.y + c * vq.y);
+            const C tp = cmul(ec, vq), tq = cmul(P.e, vp);
+            Vp[row] = mk2(P.c * vp.x - P.s * tp.x, P.c * vp.y - P.s * tp.y);
+            Vq[row] = mk2(P.s * tq.x + P.c * vq.x, P.s * tq.y + P.c * vq.y);
           }
         }
       }
       team_sync<TEAM>();
       // rows: A <- J^H A (the same pairs and parameters, lanes over the columns)
-      for (int j = 0; j < mine; ++j) {
-        const int pp = __shfl_sync(0xffffffffu, Pp, j);
-        if (pp < 0) continue;
-        const int pq = __shfl_sync(0xffffffffu, Pq, j);
-        const T c = __shfl_sync(0xffffffffu, Pc, j), sn = __shfl_sync(0xffffffffu, Ps, j);
-        const C e = mk2(__shfl_sync(0xffffffffu, Pex, j), __shfl_sync(0xffffffffu, Pey, j));
-        const C ec = mk2(e.x, -e.y);
+      for (int i = wt; i < npair; i += NWT) {
+        const RotParam<T> P = prm[i];
+        if (P.p < 0) continue;
+        const C ec = mk2(P.e.x, -P.e.y);
         for (int col = lane; col < n; col += 32) {
           C* Ac = A + col * lda;
-          const C ap = Ac[pp], aq = Ac[pq];
-          const C sp = cmul(e, aq), sq = cmul(ec, ap);
-          Ac[pp] = mk2(c * ap.x - sn * sp.x, c * ap.y - sn * sp.y);
-          Ac[pq] = mk2(sn * sq.x + c * aq.x, sn * sq.y + c * aq.y);
+          const C ap = Ac[P.p], aq = Ac[P.q];
+          const C sp = cmul(P.e, aq), sq = cmul(ec, ap);
+          Ac[P.p] = mk2(P.c * ap.x - P.s * sp.x, P.c * ap.y - P.s * sp.y);
+          Ac[P.q] = mk2(P.s * sq.x + P.c * aq.x, P.s * sq.y + P.c * aq.y);
         }
       }
       team_sync<TEAM>();
