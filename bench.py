@@ -525,7 +525,7 @@ def fp64_denominator(args, torch, pipeline, dm, xk_d, xq_d, r_mixed, ws, n_el, v
     err["omega_abs_max_ry"] = float((r_mixed.omega - r64.omega).abs().max())
     ctx.set_graph_mode(True)
     # the denominator's own roofline: the pass's algorithmic flops (same count as the mixed pass) against a
-    # live cuBLAS DGEMM; its GEMMs are the CUDA-core FP64 kernels of csrc/epb_eph.cu and csrc/epb_fourier.cu
+    # live cuBLAS DGEMM; its GEMMs are cuBLAS ZGEMMs (csrc/epb_f64blas.cu), as in the reference's GPU path
     nw2, nm_, nr_el, nr_ep = NW * NW, 3 * NATOM, (2 * N_EL + 1) ** 3, (2 * N_PH + 1) ** 3
     per_pair = 8.0 * (nw2 * nm_ * nr_ep + nw2 * nr_el + NW ** 3 * nm_ + nw2 * nm_ * nm_ +
                       nw2 * nm_ * nr_ep * nr_el / args.nq) + 40.0 * NW ** 3
@@ -536,7 +536,8 @@ def fp64_denominator(args, torch, pipeline, dm, xk_d, xq_d, r_mixed, ws, n_el, v
             "kept_set": "identical by construction (all bands, every (k, q) pair in both paths)",
             "roofline": {"bound": "fp64", "achieved": round(tf64, 2), "peak": round(p64, 2), "unit": "TFLOP/s",
                          "frac": round(tf64 / p64, 4), "peak_source": "measured live: cuBLAS DGEMM 8192^3",
-                         "note": "whole FP64 pass: FP64 Fourier sums and ZGEMM on CUDA cores, FP64 Jacobi"},
+                         "note": "whole FP64 pass: H(k+q) Fourier, kR->kq and both rotations as cuBLAS ZGEMMs (the "
+                                 "reference's GPU path), FP64 Jacobi eigensolves of this project"},
             "profile_ms": prof64}
 
 

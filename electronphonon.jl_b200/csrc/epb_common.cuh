@@ -147,7 +147,9 @@ struct epb_ctx {
   int rot_variant = -1;
   // the choices of the pass in progress (set by epb_eph_pass): rotation kernel, A-resident kR->kq GEMM
   int cur_rot = 0, cur_kq_ares = 1;
-  // measured tuning choices (shape key -> value), see epb_tune.cu
+  // cuBLAS handle of the plain FP64 pass (its GEMMs are library ZGEMMs, as in the reference's GPU path),
+  // created on first use
+  void* cublas = nullptr;
 };
 
 struct epb_rset {
@@ -205,6 +207,7 @@ namespace epb {
 void prof_begin(epb_ctx* ctx, int id);
 int side_stream(epb_ctx* ctx);
 int pipe_streams(epb_ctx* ctx);
+void cublas_release(epb_ctx* ctx);
 void prof_end(epb_ctx* ctx);
 
 // Grow-only workspace slot; returns EPB_ERR_OOM on failure.

@@ -200,6 +200,7 @@ int epb_destroy(epb_ctx* ctx) {
     cudaEventDestroy(r.a);
     cudaEventDestroy(r.b);
   }
+  cublas_release(ctx);
   for (int i = 0; i < EPB_WS_NSLOTS; ++i)
     if (ctx->ws[i]) cudaFree(ctx->ws[i]);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);

@@ -10,6 +10,8 @@
 // The 5e10 g2 values of a full pass are never materialised: the rotation kernel consumes each
 // (k, q) block in place, accumulating g2sum[nu, k] = sum_{m, n, q} g2 and writing the full block
 // only for the sampled q (q % sample_stride == 0), which is what the parity checks read.
+// The plain FP64 pass (the mixed pass's denominator) runs its dense algebra the way the reference's GPU
+// path does, as library ZGEMMs (epb_f64blas.cu); the mixed pass is this project's kernels throughout.
 #include <algorithm>
 #include <vector>
 
@@ -21,8 +23,6 @@ namespace epb {
 
 int fourier_f64(epb_ctx* ctx, const double2* op, int64_t ld, int64_t M, const epb_rset* rs,
                 const double* xk, int64_t N, double2* out, int64_t ldo);
-int zgemm_nn(epb_ctx* ctx, const double2* A, int64_t lda, const double2* B, int64_t ldb, double2* C,
-             int64_t ldc, int64_t M, int64_t N, int64_t K);
 int eigh_async(epb_ctx* ctx, double2* A, int64_t n, int64_t batch, double* E, bool want_v,
                const double* mass, int prec);
 int eigh_check(epb_ctx* ctx);
@@ -47,69 +47,15 @@ __global__ void xkq_kernel(const double* __restrict__ xk, int64_t nkb, const dou
 }
 
 int launch_phase(epb_ctx* ctx, const epb_rset* rs, const double* xk, int64_t nk, double2* phase);
-
-// Rotation + |g|^2 fold + in-place reduction for one k over all q (FP64).
-// g: (nw, nw, nm, nq) for this k (ld = nw*nw*nm per q); ukq: (nw, nw, nq) for this k.
-__global__ void eph_rot_reduce_kernel(const double2* __restrict__ g, const double2* __restrict__ ukq,
-                                      const double2* __restrict__ uph, const double* __restrict__ omega,
-                                      int nw, int nm, int64_t nq, double* __restrict__ g2sum,
-                                      double* __restrict__ sample, int64_t stride) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int nb = nw;  // full band window
-  const int ng = nw * nb * nm, nt = nb * nb * nm;
-  double2* gs = reinterpret_cast<double2*>(smem_raw);
-  double2* ts = gs + ng;
-  double2* us = ts + nt;
-  double2* ps = us + nw * nb;
-  double* red = reinterpret_cast<double*>(ps + nm * nm);  // [nm]
-  for (int e = threadIdx.x; e < nm; e += blockDim.x) red[e] = 0.0;
-  // Per-thread partial sums: element e belongs to mode e / (nb*nb); with blockDim a multiple of
-  // nb*nb each thread always sees the same modes, so 32 register accumulators cover nm <= 32.
-  double part[32];
-#pragma unroll
-  for (int i = 0; i < 32; ++i) part[i] = 0.0;
-  for (int64_t q = blockIdx.x; q < nq; q += gridDim.x) {
-    __syncthreads();
-    const double2* gq = g + q * (int64_t)ng;
-    for (int e = threadIdx.x; e < ng; e += blockDim.x) gs[e] = gq[e];
-    for (int e = threadIdx.x; e < nw * nb; e += blockDim.x) us[e] = ukq[q * nw * nb + e];
-    for (int e = threadIdx.x; e < nm * nm; e += blockDim.x) ps[e] = uph[q * nm * nm + e];
-    __syncthreads();
-    for (int e = threadIdx.x; e < nt; e += blockDim.x) {
-      int m = e % nb, r = e / nb;
-      double2 acc = make_double2(0, 0);
-      const double2* gc = gs + r * nw;
-      const double2* uc = us + m * nw;
-      for (int iw = 0; iw < nw; ++iw) cfma_conj(acc, uc[iw], gc[iw]);
-      ts[e] = acc;
-    }
-    __syncthreads();
-    const int mn = nb * nb;
-    const bool samp = sample && (q % stride == 0);
-    double* sq = samp ? sample + (q / stride) * (int64_t)nt : nullptr;
-    for (int e = threadIdx.x; e < nt; e += blockDim.x) {
-      int mnidx = e % mn, nu = e / mn;
-      double2 acc = make_double2(0, 0);
-      for (int jm = 0; jm < nm; ++jm) cfma(acc, ts[mnidx + jm * mn], ps[jm + nu * nm]);
-      double v = (acc.x * acc.x + acc.y * acc.y) / (2.0 * omega[nu + q * nm]);
-      if (samp) sq[e] = v;
-#pragma unroll
-      for (int i = 0; i < 32; ++i)
-        if (i == nu) part[i] += v;
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int i = 0; i < 32; ++i) {
-    if (i < nm) {
-      double v = part[i];
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&red[i], v);
-    }
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < nm; e += blockDim.x) atomicAdd(&g2sum[e], red[e]);
-}
+int zgemm_blas(epb_ctx* ctx, char ta, char tb, int64_t m, int64_t n, int64_t k, const double2* A, int64_t lda,
+               const double2* B, int64_t ldb, double2* C, int64_t ldc);
+int zgemm_blas_strided(epb_ctx* ctx, char ta, char tb, int64_t m, int64_t n, int64_t k, const double2* A,
+                       int64_t lda, int64_t sa, const double2* B, int64_t ldb, int64_t sb, double2* C, int64_t ldc,
+                       int64_t sc, int64_t batch);
+int fourier_zgemm(epb_ctx* ctx, const double2* op_r, int64_t ndata, int64_t ld_op, const epb_rset* rs,
+                  const double* x, int64_t npts, double2* phase_scratch, double2* out, int64_t ldo);
+int g2_fold_f64(epb_ctx* ctx, const double2* ep, const double* omega, int nw, int nm, int64_t nq, double* g2sum,
+                double* sample, int64_t stride);
 
 }  // namespace epb
 
@@ -405,6 +351,8 @@ static int eph_pass_run(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk
   const size_t o_xkq = carve(f64 ? 24ull * k_batch * nq : 0);
   const size_t o_hkq = carve(f64 ? 16ull * nw2 * k_batch * nq : 0);
   const size_t o_g = carve(f64 ? 16ull * nw2 * nm * nq : 0);
+  const size_t o_t = carve(f64 ? 16ull * nw2 * nm * nq : 0);                   // u_kq^H g per q
+  const size_t o_pkq = carve(f64 ? 16ull * m->nr_el * k_batch * nq : 0);      // phases of the k+q points
   void* base = nullptr;
   EPB_TRY(ws_get(ctx, EPB_WS_PASS0, off, &base));
   char* b = (char*)base;
@@ -415,6 +363,8 @@ static int eph_pass_run(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk
   double* Xkq = (double*)(b + o_xkq);
   double2* Hkq = (double2*)(b + o_hkq);
   double2* gb = (double2*)(b + o_g);
+  double2* Tb = (double2*)(b + o_t);
+  double2* Pkq = (double2*)(b + o_pkq);
   EPB_CUDA(cudaMemsetAsync(g2sum_out, 0, sizeof(double) * nm * nk, ctx->stream));
   const int64_t nsamp = g2_sample ? (nq + sample_stride - 1) / sample_stride : 0;
   int64_t stats[4] = {0, 0, 0, 0};
@@ -425,13 +375,6 @@ static int eph_pass_run(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk
   EPB_TRY(launch_phase(ctx, m->rs_ep, xq, nq, P));
 
   // ---- k batches -----------------------------------------------------------------------------
-  static bool attr = false;
-  size_t rsmem = sizeof(double2) * (nw2 * nm * 2 + nw2 + nm * nm) + sizeof(double) * nm;
-  EPB_CHECK_ARG(rsmem <= 200 * 1024, "epb_eph_pass: rotation block too large");
-  if (!attr) {
-    EPB_CUDA(cudaFuncSetAttribute(eph_rot_reduce_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    attr = true;
-  }
   if (prec == EPB_PREC_MIXED) {
     EPB_TRY(mixed_pass(ctx, m, xk, nk, xq, nq, Dq, omega_out, ek_out, g2sum_out, g2_sample, sample_stride, k_batch,
                        defer_checks));
@@ -447,18 +390,25 @@ static int eph_pass_run(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk
     EPB_LAUNCH_CHECK();
     EPB_TRY(epb_eph_RR_to_kR(ctx, (const double*)m->epmat, nw, nm, nr_ep, m->rs_el, xkb, nkb,
                              (const double*)Hk, nw, nullptr, (double*)G, EPB_PREC_FP64));
-    EPB_TRY(fourier_f64(ctx, m->ham, nw2, nw2, m->rs_el, Xkq, nkb * nq, Hkq, nw2));
+    // H(k+q) of every pair of the batch: phase matrix and one ZGEMM (the reference's fourier_batched!)
+    prof_begin(ctx, EPB_PROF_FOURIER_F64);
+    EPB_TRY(fourier_zgemm(ctx, m->ham, nw2, nw2, m->rs_el, Xkq, nkb * nq, Pkq, Hkq, nw2));
+    prof_end(ctx);
     EPB_TRY(eigh_async(ctx, Hkq, nw, nkb * nq, nullptr, true, nullptr, EPB_PREC_FP64));
     const int64_t ndata = nw2 * nm;
     for (int64_t kl = 0; kl < nkb; ++kl) {
-      EPB_TRY(zgemm_nn(ctx, G + kl * ndata * nr_ep, ndata, P, nr_ep, gb, ndata, ndata, nq, nr_ep));
-      int64_t blocks = nq < (int64_t)ctx->sm_count * 8 ? nq : (int64_t)ctx->sm_count * 8;
-      prof_begin(ctx, EPB_PROF_ROT);
-      eph_rot_reduce_kernel<<<(unsigned)blocks, 256, rsmem, ctx->stream>>>(
-          gb, Hkq + kl * nq * nw2, Dq, omega_out, (int)nw, (int)nm, nq, g2sum_out + nm * (k0 + kl),
-          g2_sample ? g2_sample + (k0 + kl) * nsamp * nw2 * nm : nullptr, sample_stride);
+      // g(k, q) = g(k, Rp) P (ZGEMM), then per q: T = u_kq^H g (nw x nw nm), ep = T u_ph (nw^2 x nm), two
+      // strided-batched ZGEMMs as in the reference's eph_apply_rotations!; ep overwrites g
+      prof_begin(ctx, EPB_PROF_ZGEMM);
+      EPB_TRY(zgemm_blas(ctx, 'N', 'N', ndata, nq, nr_ep, G + kl * ndata * nr_ep, ndata, P, nr_ep, gb, ndata));
       prof_end(ctx);
-      EPB_LAUNCH_CHECK();
+      prof_begin(ctx, EPB_PROF_ROT);
+      EPB_TRY(zgemm_blas_strided(ctx, 'C', 'N', nw, nw * nm, nw, Hkq + kl * nq * nw2, nw, nw2, gb, nw, ndata, Tb, nw,
+                                 ndata, nq));
+      EPB_TRY(zgemm_blas_strided(ctx, 'N', 'N', nw2, nm, nm, Tb, nw2, ndata, Dq, nm, nm * nm, gb, nw2, ndata, nq));
+      EPB_TRY(g2_fold_f64(ctx, gb, omega_out, (int)nw, (int)nm, nq, g2sum_out + nm * (k0 + kl),
+                          g2_sample ? g2_sample + (k0 + kl) * nsamp * nw2 * nm : nullptr, sample_stride));
+      prof_end(ctx);
     }
   }
   if (!defer_checks) EPB_TRY(eigh_check(ctx));
