@@ -360,7 +360,9 @@ static int launch_big(epb_ctx* ctx, BigArgs a, int64_t batch) {
     attr = true;
   }
   const int64_t grid = std::min<int64_t>((int64_t)ctx->sm_count * MINB, batch);
-  const size_t slab_max = (size_t)3 * BIG_NMAX * BIG_NMAX * sizeof(double2) * (size_t)ctx->sm_count;
+  // largest slab of the instances below: <96, 512, 1>, <80, 256, 2>, <64, 256, 2>
+  const size_t per_sm = std::max<size_t>({(size_t)3 * 96 * 96, (size_t)3 * 80 * 80 * 2, (size_t)3 * 64 * 64 * 2});
+  const size_t slab_max = per_sm * sizeof(double2) * (size_t)ctx->sm_count;
   const size_t slab = (size_t)3 * NMAX * NMAX * sizeof(double2) * (size_t)grid;
   void* ws = nullptr;
   EPB_TRY(ws_get(ctx, EPB_WS_EIGH_BIG, (slab > slab_max ? slab : slab_max) + 256, &ws));
@@ -393,6 +395,15 @@ int eigh_big_launch(epb_ctx* ctx, double2* A, const int64_t* a_off, const int32_
   a.n_lo = n_lo;
   a.nonconv = nonconv;
   a.badsize = badsize;
+  // orders up to 80 on a two-CTA-per-SM instance (106 KB of shared memory each), 81..96 on one 512-thread
+  // CTA per SM; a uniform batch takes the one instance that covers its order
+  if (nvec == nullptr) {
+    if (n_uniform <= 80) return launch_big<80, 256, 2>(ctx, a, batch);
+    return launch_big<BIG_NMAX, 512, 1>(ctx, a, batch);
+  }
+  const int st = launch_big<80, 256, 2>(ctx, a, batch);
+  if (st != EPB_OK) return st;
+  a.n_lo = std::max(n_lo, 80);
   return launch_big<BIG_NMAX, 512, 1>(ctx, a, batch);
 }
 
