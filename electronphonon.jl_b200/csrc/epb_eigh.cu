@@ -499,7 +499,7 @@ static int eigh_small(epb_ctx* ctx, const EighArgs& a, int prec) {
 int eigh_big_launch(epb_ctx* ctx, double2* A, const int64_t* a_off, const int32_t* nvec, int n_uniform, int64_t batch,
                     double* E, const int64_t* e_off, bool want_v, int n_lo, int prec, int* nonconv, int* badsize);
 int eigh_mid_launch(epb_ctx* ctx, double2* A, const int64_t* a_off, const int32_t* nvec, int n_uniform, int64_t batch,
-                    double* E, const int64_t* e_off, bool want_v, int n_lo, int* nonconv, int* badsize);
+                    double* E, const int64_t* e_off, bool want_v, int n_lo, int n_hi, int* nonconv, int* badsize);
 
 // Orders of a varlen batch outside 0..96 (no kernel handles them; order 0 is an empty matrix).
 __global__ void eigh_badorder_kernel(const int32_t* __restrict__ nvec, int64_t batch, int* __restrict__ badsize) {
@@ -513,8 +513,8 @@ __global__ void eigh_badorder_kernel(const int32_t* __restrict__ nvec, int64_t b
 }
 
 // The varlen batch without any host read-back (capturable in a CUDA graph): every size class kernel runs
-// -- orders 1..16, 17..32, 33..48 (FP64: 33..64) on the shared-memory Jacobi, 49..64 (mixed) and 65..96 on
-// the persistent L2-scratch solver -- each
+// -- orders 1..16 (and, FP64, 17..32, 33..64) on the shared-memory Jacobi, the others on the persistent
+// L2-scratch solver (mixed: 17..32, 33..48, 49..64; both: 65..80, 81..96) -- each
 // taking the matrices of its class from the whole batch and skipping the others; orders outside 0..96 are
 // counted into the status words that eigh_check reads.
 int eigh_varlen_async(epb_ctx* ctx, EighArgs& a, int prec) {
@@ -529,15 +529,18 @@ int eigh_varlen_async(epb_ctx* ctx, EighArgs& a, int prec) {
   EPB_LAUNCH_CHECK();
   const int lo[3] = {0, 16, 32}, hi[3] = {16, 32, 64};
   for (int c = 0; c < 3; ++c) {
+    // mixed: 17..32, 33..48 and 49..64 on the L2-scratch solver (more matrices per SM than the FP64
+    // shared-memory Rayleigh-Ritz solver)
+    if (prec == EPB_PREC_MIXED && c > 0) break;
     EighArgs s = a;
     s.n_lo = lo[c];
     s.skip_hi = 1;
-    // mixed: 33..48 here (two teams per SM), 49..64 on the L2-scratch solver below
-    EPB_TRY(eigh_dispatch(ctx, s, prec == EPB_PREC_MIXED && c == 2 ? 48 : hi[c], prec));
+    EPB_TRY(eigh_dispatch(ctx, s, hi[c], prec));
   }
   if (prec == EPB_PREC_MIXED)
-    EPB_TRY(eigh_mid_launch(ctx, a.A, a.a_off, a.nvec, 0, a.batch, a.E, a.e_off, a.want_v != 0, 48, a.nonconv,
-                            a.badsize));
+    for (int c = 0; c < 3; ++c)
+      EPB_TRY(eigh_mid_launch(ctx, a.A, a.a_off, a.nvec, 0, a.batch, a.E, a.e_off, a.want_v != 0, 16 + 16 * c,
+                              32 + 16 * c, a.nonconv, a.badsize));
   return eigh_big_launch(ctx, a.A, a.a_off, a.nvec, 0, a.batch, a.E, a.e_off, a.want_v != 0, 64, prec, a.nonconv,
                          a.badsize);
 }
@@ -553,9 +556,9 @@ int eigh_run(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
     const int n = a.n_uniform;
     if (n <= 16)
       EPB_TRY(eigh_small(ctx, a, prec));
-    else if (n > 48 && n <= 64 && prec == EPB_PREC_MIXED && !a.mass && !a.Hp && !a.U32)
-      EPB_TRY(eigh_mid_launch(ctx, a.A, nullptr, nullptr, n, a.batch, a.E, nullptr, a.want_v != 0, 0, a.nonconv,
-                              a.badsize));
+    else if (n <= 64 && prec == EPB_PREC_MIXED && !a.mass && !a.Hp && !a.U32)
+      EPB_TRY(eigh_mid_launch(ctx, a.A, nullptr, nullptr, n, a.batch, a.E, nullptr, a.want_v != 0, 0,
+                              n <= 32 ? 32 : n <= 48 ? 48 : 64, a.nonconv, a.badsize));
     else if (n <= 64)
       EPB_TRY(eigh_dispatch(ctx, a, n, prec));
     else if (n <= 96) {

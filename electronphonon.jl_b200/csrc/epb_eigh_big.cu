@@ -360,8 +360,9 @@ static int launch_big(epb_ctx* ctx, BigArgs a, int64_t batch) {
     attr = true;
   }
   const int64_t grid = std::min<int64_t>((int64_t)ctx->sm_count * MINB, batch);
-  // largest slab of the instances below: <96, 512, 1>, <80, 256, 2>, <64, 256, 2>
-  const size_t per_sm = std::max<size_t>({(size_t)3 * 96 * 96, (size_t)3 * 80 * 80 * 2, (size_t)3 * 64 * 64 * 2});
+  // largest slab of the instances below: <96, 512, 1>, <80, 256, 2>, <64, 256, 2>, <48, 256, 2>, <32, 128, 4>
+  const size_t per_sm = std::max<size_t>({(size_t)3 * 96 * 96, (size_t)3 * 80 * 80 * 2, (size_t)3 * 64 * 64 * 2,
+                                          (size_t)3 * 48 * 48 * 2, (size_t)3 * 32 * 32 * 4});
   const size_t slab_max = per_sm * sizeof(double2) * (size_t)ctx->sm_count;
   const size_t slab = (size_t)3 * NMAX * NMAX * sizeof(double2) * (size_t)grid;
   void* ws = nullptr;
@@ -407,11 +408,13 @@ int eigh_big_launch(epb_ctx* ctx, double2* A, const int64_t* a_off, const int32_
   return launch_big<BIG_NMAX, 512, 1>(ctx, a, batch);
 }
 
-// The same solver for orders 49..64 (mixed precision, c128 in and out): 69 KB of shared memory and 256
-// threads per CTA, two CTAs per SM (the shared-memory FP64 Rayleigh-Ritz solver of epb_eigh.cu keeps H, V
-// and S in FP64 in shared memory, 200 KB at order 64, one team per SM).
+// The same solver for the mixed-precision classes below 65 (c128 in and out): orders (n_lo, n_hi] with
+// n_hi = 32, 48 or 64 on instances sized for them -- 18, 40 and 69 KB of shared memory, four 128-thread,
+// two 256-thread and two 256-thread CTAs per SM. (The shared-memory FP64 Rayleigh-Ritz solver of
+// epb_eigh.cu keeps H, V and S in FP64 in shared memory: 51 KB per matrix at order 32, 111 KB at 48,
+// 200 KB at 64, i.e. 4, 2 and 1 matrices per SM.)
 int eigh_mid_launch(epb_ctx* ctx, double2* A, const int64_t* a_off, const int32_t* nvec, int n_uniform, int64_t batch,
-                    double* E, const int64_t* e_off, bool want_v, int n_lo, int* nonconv, int* badsize) {
+                    double* E, const int64_t* e_off, bool want_v, int n_lo, int n_hi, int* nonconv, int* badsize) {
   if (batch == 0) return EPB_OK;
   BigArgs a{};
   a.A = A;
@@ -427,6 +430,8 @@ int eigh_mid_launch(epb_ctx* ctx, double2* A, const int64_t* a_off, const int32_
   a.n_lo = n_lo;
   a.nonconv = nonconv;
   a.badsize = badsize;
+  if (n_hi <= 32) return launch_big<32, 128, 4>(ctx, a, batch);
+  if (n_hi <= 48) return launch_big<48, 256, 2>(ctx, a, batch);
   return launch_big<64, 256, 2>(ctx, a, batch);
 }
 
