@@ -576,12 +576,17 @@ int epb_pair_window(epb_ctx* ctx, const epb_bands* bd, const double* xk, int64_t
   cc.boff = (int64_t*)(base + o_bo);
   EPB_CUDA(cudaMemsetAsync(running, 0, sizeof(int64_t), ctx->stream));
 
+  // The screen pays only where it culls: inference costs about a quarter of the plain evaluation of a pair
+  // (H(x) GEMM + Householder/Sturm), so once 2^20 screened pairs have culled under a fifth of them the
+  // remaining chunks skip it. Skipping never changes the kept set (culling only removes pairs the plain
+  // evaluation would reject).
+  bool screen = mlp != nullptr;
   for (int64_t k0 = 0; k0 < nk; k0 += krows) {
     const int64_t nkr = std::min(krows, nk - k0);
     const int64_t np = nkr * nq, pair0 = k0 * nq;
     int64_t ncand = np;
     const int64_t* cl = nullptr;  // candidate list (null: all pairs of the chunk)
-    if (mlp) {
+    if (screen) {
       prof_begin(ctx, EPB_PROF_MLP_INFER);
       EPB_TRY(mlp_predict_norm(ctx, mlp, xk, xq, nq, nullptr, pair0, np, pred));
       mlp_screen_kernel<<<grid_pts(ctx, np), 256, 0, ctx->stream>>>(pred, nout, np, mu, sc, margin, wmin, wmax, flag);
@@ -628,6 +633,8 @@ int epb_pair_window(epb_ctx* ctx, const epb_bands* bd, const double* xk, int64_t
       }
       cl = cand;
       st.culled += np - ncand;
+      st.screened += np;
+      if (st.screened >= (int64_t(1) << 20) && st.culled * 5 < st.screened) screen = false;
     }
     st.evaluated += ncand;
     EPB_TRY(eval_candidates(ctx, bd, w, xk, xq, nq, cl, pair0, ncand, wmin, wmax, prec, guard, cmin, cmax, rc_list,

@@ -121,7 +121,7 @@ SIGNATURES = {
 class WindowStats(C.Structure):
     """epb_window_stats."""
     _fields_ = [("tested", I64), ("culled", I64), ("evaluated", I64), ("rechecked", I64), ("kept", I64),
-                ("audited", I64), ("violations", I64), ("fallback_chunks", I64)]
+                ("audited", I64), ("violations", I64), ("fallback_chunks", I64), ("screened", I64)]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}

@@ -491,8 +491,8 @@ function band_energy(b::Bands, xks, band::Integer; prec::Integer = DRIVER_PREC[]
     E
 end
 
-const WindowStats = NTuple{8,Int64}  # epb_window_stats: tested, culled, evaluated, rechecked, kept, audited,
-                                     # violations, fallback_chunks
+const WindowStats = NTuple{9,Int64}  # epb_window_stats: tested, culled, evaluated, rechecked, kept, audited,
+                                     # violations, fallback_chunks, screened
 
 """
     bands_window(b, xks, wmin, wmax; prec, guard = 1e-3)

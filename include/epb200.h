@@ -235,9 +235,11 @@ typedef struct epb_mlp epb_mlp;
    points re-evaluated in FP64 by the mixed path's guard; kept: points / pairs with a non-empty
    window; audited: culled pairs re-evaluated by the plain path as a check of the surrogate (one in
    64 per chunk); violations: audited pairs whose window was not empty; fallback_chunks: chunks
-   that, after a violation, were evaluated entirely by the plain path. */
+   that, after a violation, were evaluated entirely by the plain path; screened: pairs given to the
+   surrogate (the screen stops once 2^20 screened pairs have culled under a fifth of them, where
+   inference costs more than it saves; the rest go to the plain evaluation directly). */
 typedef struct {
-  int64_t tested, culled, evaluated, rechecked, kept, audited, violations, fallback_chunks;
+  int64_t tested, culled, evaluated, rechecked, kept, audited, violations, fallback_chunks, screened;
 } epb_window_stats;
 
 /* Bind an electron Hamiltonian H(R) (c128, (nw^2, nr), caller-owned; irvec int64 3 x nr, host)
