@@ -1384,6 +1384,9 @@ def run_eigh(args):
                                    "2-4-fold clusters spaced 1e-10", "precision": args.prec,
                        "input_bytes": int(16 * (sizes * sizes).sum()), "generation_s": round(t_gen, 1),
                        "l2": "inputs larger than L2"},
+            "autotuned_classes": {l.split()[0]: ("L2-scratch solver instance" if l.split()[1] == "1" else
+                                                 "shared-memory / 512-thread solver")
+                                  for l in ctx.tune_text().splitlines() if l.startswith("eigh_varlen/")},
             "max_abs_eig_err_vs_lapack_sample64": worst, "roofline": roof, "roofline_compute": roof_c,
             "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": clocks, "impl": "epb", "profile_one_step": profile}

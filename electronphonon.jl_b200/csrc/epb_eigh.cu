@@ -500,6 +500,11 @@ int eigh_big_launch(epb_ctx* ctx, double2* A, const int64_t* a_off, const int32_
                     double* E, const int64_t* e_off, bool want_v, int n_lo, int prec, int* nonconv, int* badsize);
 int eigh_mid_launch(epb_ctx* ctx, double2* A, const int64_t* a_off, const int32_t* nvec, int n_uniform, int64_t batch,
                     double* E, const int64_t* e_off, bool want_v, int n_lo, int n_hi, int* nonconv, int* badsize);
+int eigh_l2_launch(epb_ctx* ctx, double2* A, const int64_t* a_off, const int32_t* nvec, int n_uniform, int64_t batch,
+                   double* E, const int64_t* e_off, bool want_v, int n_lo, int n_hi, int inst, int refine,
+                   int* nonconv, int* badsize);
+bool tune_lookup(const std::vector<std::pair<std::string, int64_t>>& kv, const std::string& key, int64_t* value);
+void tune_store(std::vector<std::pair<std::string, int64_t>>& kv, const std::string& key, int64_t value);
 
 // Orders of a varlen batch outside 0..96 (no kernel handles them; order 0 is an empty matrix).
 __global__ void eigh_badorder_kernel(const int32_t* __restrict__ nvec, int64_t batch, int* __restrict__ badsize) {
@@ -512,11 +517,37 @@ __global__ void eigh_badorder_kernel(const int32_t* __restrict__ nvec, int64_t b
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(badsize, c);
 }
 
+// Size classes of a mixed-precision varlen batch with two candidate kernels each, (lo, hi]: candidate 0 is
+// the shared-memory FP64 Rayleigh-Ritz solver (orders <= 64) or, for 65..80, the 512-thread instance of the
+// L2-scratch solver; candidate 1 the L2-scratch instance sized for the class.
+constexpr int VL_NCLS = 4;
+constexpr int VL_LO[VL_NCLS] = {16, 32, 48, 64}, VL_HI[VL_NCLS] = {32, 48, 64, 80};
+
+static std::string varlen_key(int c) {
+  char key[64];
+  snprintf(key, sizeof(key), "eigh_varlen/%d/%d/%d", VL_LO[c], VL_HI[c], (int)EPB_PREC_MIXED);
+  return key;
+}
+
+// Candidate `v` of mixed class c over the whole batch (the kernel takes the matrices of its class only).
+static int varlen_class(epb_ctx* ctx, const EighArgs& a, int c, int v) {
+  if (v == 0 && VL_HI[c] <= 64) {
+    EighArgs s = a;
+    s.n_lo = VL_LO[c];
+    s.skip_hi = 1;
+    return eigh_dispatch(ctx, s, VL_HI[c], EPB_PREC_MIXED);
+  }
+  const int inst = v == 0 ? 96 : VL_HI[c];
+  return eigh_l2_launch(ctx, a.A, a.a_off, a.nvec, 0, a.batch, a.E, a.e_off, a.want_v != 0, VL_LO[c], VL_HI[c], inst, 2,
+                        a.nonconv, a.badsize);
+}
+
 // The varlen batch without any host read-back (capturable in a CUDA graph): every size class kernel runs
-// -- orders 1..16 (and, FP64, 17..32, 33..64) on the shared-memory Jacobi, the others on the persistent
-// L2-scratch solver (mixed: 17..32, 33..48, 49..64; both: 65..80, 81..96) -- each
-// taking the matrices of its class from the whole batch and skipping the others; orders outside 0..96 are
-// counted into the status words that eigh_check reads.
+// over the whole batch, taking the matrices of its class and skipping the others -- FP64: orders 1..16,
+// 17..32, 33..64 on the shared-memory Jacobi, 65..96 on the persistent L2-scratch solver; mixed: 1..16 on
+// the register Jacobi, then for 17..32, 33..48, 49..64, 65..80 the candidate in the context's tuning table
+// (epb_eigh_varlen times them on the first batch; default the L2-scratch instance), 81..96 on the
+// L2-scratch solver. Orders outside 0..96 are counted into the status words that eigh_check reads.
 int eigh_varlen_async(epb_ctx* ctx, EighArgs& a, int prec) {
   if (a.batch == 0) return EPB_OK;
   EPB_CHECK_ARG(prec == EPB_PREC_FP64 || prec == EPB_PREC_MIXED, "eigensolver: unknown precision mode %d", prec);
@@ -527,22 +558,106 @@ int eigh_varlen_async(epb_ctx* ctx, EighArgs& a, int prec) {
   eigh_badorder_kernel<<<(unsigned)std::min<int64_t>(cdiv(a.batch, 256), (int64_t)ctx->sm_count * 8), 256, 0,
                          ctx->stream>>>(a.nvec, a.batch, a.badsize);
   EPB_LAUNCH_CHECK();
-  const int lo[3] = {0, 16, 32}, hi[3] = {16, 32, 64};
-  for (int c = 0; c < 3; ++c) {
-    // mixed: 17..32, 33..48 and 49..64 on the L2-scratch solver (more matrices per SM than the FP64
-    // shared-memory Rayleigh-Ritz solver)
-    if (prec == EPB_PREC_MIXED && c > 0) break;
-    EighArgs s = a;
-    s.n_lo = lo[c];
-    s.skip_hi = 1;
-    EPB_TRY(eigh_dispatch(ctx, s, hi[c], prec));
+  if (prec == EPB_PREC_FP64) {
+    const int lo[3] = {0, 16, 32}, hi[3] = {16, 32, 64};
+    for (int c = 0; c < 3; ++c) {
+      EighArgs s = a;
+      s.n_lo = lo[c];
+      s.skip_hi = 1;
+      EPB_TRY(eigh_dispatch(ctx, s, hi[c], prec));
+    }
+    return eigh_big_launch(ctx, a.A, a.a_off, a.nvec, 0, a.batch, a.E, a.e_off, a.want_v != 0, 64, prec, a.nonconv,
+                           a.badsize);
   }
-  if (prec == EPB_PREC_MIXED)
-    for (int c = 0; c < 3; ++c)
-      EPB_TRY(eigh_mid_launch(ctx, a.A, a.a_off, a.nvec, 0, a.batch, a.E, a.e_off, a.want_v != 0, 16 + 16 * c,
-                              32 + 16 * c, a.nonconv, a.badsize));
-  return eigh_big_launch(ctx, a.A, a.a_off, a.nvec, 0, a.batch, a.E, a.e_off, a.want_v != 0, 64, prec, a.nonconv,
-                         a.badsize);
+  {
+    EighArgs s = a;
+    s.n_lo = 0;
+    s.skip_hi = 1;
+    EPB_TRY(eigh_dispatch(ctx, s, 16, prec));
+  }
+  for (int c = 0; c < VL_NCLS; ++c) {
+    int64_t v = 1;
+    tune_lookup(ctx->tuned, varlen_key(c), &v);
+    EPB_TRY(varlen_class(ctx, a, c, (int)v));
+  }
+  return eigh_l2_launch(ctx, a.A, a.a_off, a.nvec, 0, a.batch, a.E, a.e_off, a.want_v != 0, 80, 96, 96, 2, a.nonconv,
+                        a.badsize);
+}
+
+// max over the batch of a_off[b] + n_b^2 and e_off[b] + n_b: the extents of A (complex entries) and E
+__global__ void varlen_extent_kernel(const int64_t* __restrict__ a_off, const int64_t* __restrict__ e_off,
+                                     const int32_t* __restrict__ nvec, int64_t batch, unsigned long long* ext) {
+  unsigned long long ea = 0, ee = 0;
+  for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < batch; b += (int64_t)gridDim.x * blockDim.x) {
+    const int n = nvec[b];
+    if (n < 1 || n > 96) continue;
+    ea = max(ea, (unsigned long long)(a_off[b] + (int64_t)n * n));
+    ee = max(ee, (unsigned long long)(e_off[b] + n));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    ea = max(ea, __shfl_xor_sync(0xffffffffu, ea, o));
+    ee = max(ee, __shfl_xor_sync(0xffffffffu, ee, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(ext, ea);
+    atomicMax(ext + 1, ee);
+  }
+}
+
+// Autotuner of the mixed varlen classes (synchronous calls only): for every class whose choice is not in
+// the context's table, both candidates solve a copy of the first (at most 32768) matrices of the caller's
+// batch (the copy restored before each), timed with CUDA events; the faster goes into the table under
+// eigh_varlen/<lo>/<hi>/<prec>. Costs two copies of that sample in a workspace and twice its solve time,
+// once per context (or never, with an imported table).
+static int varlen_tune(epb_ctx* ctx, const EighArgs& a_in) {
+  bool need = false;
+  int64_t v;
+  for (int c = 0; c < VL_NCLS; ++c) need = need || !tune_lookup(ctx->tuned, varlen_key(c), &v);
+  if (!need || a_in.batch == 0) return EPB_OK;
+  EighArgs a = a_in;
+  a.batch = std::min<int64_t>(a.batch, 32768);
+  unsigned long long* ext = (unsigned long long*)(ctx->dstat + 20);  // status words 20..23
+  EPB_CUDA(cudaMemsetAsync(ext, 0, 2 * sizeof(unsigned long long), ctx->stream));
+  varlen_extent_kernel<<<(unsigned)std::min<int64_t>(cdiv(a.batch, 256), (int64_t)ctx->sm_count * 8), 256, 0,
+                         ctx->stream>>>(a.a_off, a.e_off, a.nvec, a.batch, ext);
+  EPB_LAUNCH_CHECK();
+  unsigned long long h[2] = {0, 0};
+  EPB_CUDA(cudaMemcpyAsync(h, ext, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  EPB_CUDA(cudaStreamSynchronize(ctx->stream));
+  const size_t abytes = (size_t)h[0] * sizeof(double2), ebytes = (size_t)h[1] * sizeof(double);
+  void* ws = nullptr;
+  EPB_TRY(ws_get(ctx, EPB_WS_PASS5, 2 * abytes + ebytes + 512, &ws));
+  double2* orig = (double2*)ws;
+  double2* work = (double2*)((char*)ws + ((abytes + 255) & ~size_t(255)));
+  double* ework = (double*)((char*)work + ((abytes + 255) & ~size_t(255)));
+  EPB_CUDA(cudaMemcpyAsync(orig, a.A, abytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  EighArgs t = a;
+  t.A = work;
+  t.E = ework;
+  t.nonconv = ctx->dstat + 24;  // trial counters, not reported
+  t.badsize = ctx->dstat + 25;
+  t.max_sweeps = 20;
+  cudaEvent_t e0, e1;
+  EPB_CUDA(cudaEventCreate(&e0));
+  EPB_CUDA(cudaEventCreate(&e1));
+  int st = EPB_OK;
+  for (int c = 0; c < VL_NCLS && st == EPB_OK; ++c) {
+    if (tune_lookup(ctx->tuned, varlen_key(c), &v)) continue;
+    float ms[2] = {0.f, 0.f};
+    for (int cand = 0; cand < 2 && st == EPB_OK; ++cand) {
+      if (cudaMemcpyAsync(work, orig, abytes, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess) st = EPB_ERR_CUDA;
+      if (st == EPB_OK) st = cudaEventRecord(e0, ctx->stream) == cudaSuccess ? EPB_OK : EPB_ERR_CUDA;
+      if (st == EPB_OK) st = varlen_class(ctx, t, c, cand);
+      if (st == EPB_OK) st = cudaEventRecord(e1, ctx->stream) == cudaSuccess ? EPB_OK : EPB_ERR_CUDA;
+      if (st == EPB_OK) st = cudaEventSynchronize(e1) == cudaSuccess ? EPB_OK : EPB_ERR_CUDA;
+      if (st == EPB_OK) cudaEventElapsedTime(&ms[cand], e0, e1);
+    }
+    if (st == EPB_OK) tune_store(ctx->tuned, varlen_key(c), ms[1] <= ms[0] ? 1 : 0);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st == EPB_ERR_CUDA) set_error("eigensolver autotuner: a copy, launch or event failed");
+  return st;
 }
 
 int eigh_run(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
@@ -571,8 +686,10 @@ int eigh_run(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
     }
     return eigh_check(ctx);
   }
-  // varlen: every size class, no read-back, then the status words
+  // varlen: the class autotuner (first mixed batch of the context), every size class without read-back,
+  // then the status words
   (void)nmax;
+  if (prec == EPB_PREC_MIXED && !a.mass) EPB_TRY(varlen_tune(ctx, a));
   EPB_CUDA(cudaMemsetAsync(ctx->dstat, 0, 2 * sizeof(int), ctx->stream));
   EPB_TRY(eigh_varlen_async(ctx, a, prec));
   return eigh_check(ctx);

@@ -41,6 +41,7 @@ struct BigArgs {
   int max_sweeps;
   int refine;
   int n_lo;                        // orders <= n_lo belong to other kernels (skipped silently)
+  int n_hi;                        // > 0: orders above n_hi belong to other kernels (skipped silently)
   int* nonconv;
   int* badsize;
   unsigned long long* counter;     // work counter (zeroed before launch)
@@ -158,7 +159,7 @@ __global__ void __launch_bounds__(NT, MINB) eigh_big_kernel(BigArgs a) {
     __syncthreads();
     if (b >= a.batch) break;
     const int n = a.nvec ? a.nvec[b] : a.n_uniform;
-    if (n <= a.n_lo) continue;
+    if (n <= a.n_lo || (a.n_hi > 0 && n > a.n_hi)) continue;
     if (n > NMAX) {
       if (tid == 0 && a.n_lo == 0) atomicAdd(a.badsize, 1);  // varlen batches count bad orders on the host
       continue;
@@ -433,6 +434,37 @@ int eigh_mid_launch(epb_ctx* ctx, double2* A, const int64_t* a_off, const int32_
   if (n_hi <= 32) return launch_big<32, 128, 4>(ctx, a, batch);
   if (n_hi <= 48) return launch_big<48, 256, 2>(ctx, a, batch);
   return launch_big<64, 256, 2>(ctx, a, batch);
+}
+
+// Any instance of the solver for the orders (n_lo, n_hi] of a (uniform or varlen) batch: inst = 32, 48, 64,
+// 80 or 96 picks the instance (the largest order it holds), refine the FP64 refinement iterations (2 mixed, 3
+// FP64). Used by the varlen size classes and their autotuner.
+int eigh_l2_launch(epb_ctx* ctx, double2* A, const int64_t* a_off, const int32_t* nvec, int n_uniform, int64_t batch,
+                   double* E, const int64_t* e_off, bool want_v, int n_lo, int n_hi, int inst, int refine,
+                   int* nonconv, int* badsize) {
+  if (batch == 0) return EPB_OK;
+  BigArgs a{};
+  a.A = A;
+  a.a_off = a_off;
+  a.nvec = nvec;
+  a.n_uniform = n_uniform;
+  a.batch = batch;
+  a.E = E;
+  a.e_off = e_off;
+  a.want_v = want_v ? 1 : 0;
+  a.max_sweeps = 20;
+  a.refine = refine;
+  a.n_lo = n_lo;
+  a.n_hi = n_hi;
+  a.nonconv = nonconv;
+  a.badsize = badsize;
+  switch (inst) {
+    case 32: return launch_big<32, 128, 4>(ctx, a, batch);
+    case 48: return launch_big<48, 256, 2>(ctx, a, batch);
+    case 64: return launch_big<64, 256, 2>(ctx, a, batch);
+    case 80: return launch_big<80, 256, 2>(ctx, a, batch);
+    default: return launch_big<BIG_NMAX, 512, 1>(ctx, a, batch);
+  }
 }
 
 }  // namespace epb

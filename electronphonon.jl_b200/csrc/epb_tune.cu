@@ -9,6 +9,8 @@
 //   pass_kb/<nw>/<nm>/<nq>/<prec>    inner k batch of epb_eph_pass (4, 8, 16, 32)
 //   pass_rot/<nw>/<nm>/<nq>/<prec>   rotation kernel of the mixed pass (0 warp tensor cores, 1 FP32)
 //   pass_kq/<nw>/<nm>/<nq>/<prec>    kR->kq GEMM form (1 A-resident, 0 streamed operands)
+//   eigh_varlen/<lo>/<hi>/<prec>     kernel of the uneven-eigensolve class (lo, hi] (1 the L2-scratch
+//                                    instance for the class, 0 the shared-memory / 512-thread solver)
 // Text form: one "key value" pair per line; '#' starts a comment line; keys are printable ASCII without
 // spaces, at most 120 characters.
 #include <cctype>

@@ -122,7 +122,10 @@ EPB_API int epb_eigh_batched(epb_ctx* ctx, double* A, int64_t n, int64_t batch, 
                      int prec);
 
 /* Uneven batch: matrix b has order n[b] (1..96) and starts at complex element a_offset[b] of A;
-   its eigenvalues go to E + e_offset[b]. All index arrays are device arrays. Same semantics. */
+   its eigenvalues go to E + e_offset[b]. All index arrays are device arrays. Same semantics. In mixed
+   precision the first call of a context times the candidate kernels of each size class on a copy of the
+   batch's first 32768 matrices (two workspace copies of that sample) and records the faster in the
+   tuning table (eigh_varlen/...), unless the table already holds it. */
 EPB_API int epb_eigh_varlen(epb_ctx* ctx, double* A, const int64_t* a_offset, const int32_t* n,
                     int64_t batch, double* E, const int64_t* e_offset, char jobz, int prec);
 
@@ -375,7 +378,10 @@ EPB_API int epb_set_rotation_variant(epb_ctx* ctx, int variant);
    _FUSED_ROT_MAX_NWNM (src/wannier_to_bloch_batched.jl:406) and _FUSED_RQKQ_MAX_NW2NM
    (ext/ElectronPhononCUDAExt.jl:214) with timings on the caller's shapes. Keys (all per nw, nm, nq,
    prec): pass_kb/... inner k batch of epb_eph_pass, pass_rot/... rotation kernel (0 tensor cores,
-   1 FP32), pass_kq/... kR->kq GEMM form (1 A-resident, 0 streamed). A table is host memory only; its
+   1 FP32), pass_kq/... kR->kq GEMM form (1 A-resident, 0 streamed); eigh_varlen/<lo>/<hi>/<prec>: the
+   kernel of a mixed uneven-eigensolve size class (lo, hi] (1 the L2-scratch instance for the class, 0 the
+   shared-memory or 512-thread solver), timed by the first epb_eigh_varlen call of a context on a copy of
+   the first 32768 matrices of its batch (epb_eigh_varlen_async only reads the table). A table is host memory only; its
    text form is one "key value" pair per line ('#' comment lines allowed). epb_tune_export copies a
    context's choices into a table, epb_tune_import loads a table's choices into a context (later calls
    of those shapes then use them without timing). get: *found = 0 when the key is absent. serialize:

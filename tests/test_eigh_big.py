@@ -132,3 +132,44 @@ def test_eigh_varlen_async_graph_capture(B, prec):
         keep = [i for i, m in enumerate(mats) if m.shape[0] <= 96]
         _check([es[i] for i in keep], [us[i] for i in keep], [mats[i] for i in keep], 1e-11 if prec == 0 else 1e-10)
         del g
+
+
+def test_eigh_varlen_autotuned_classes(B):
+    """The mixed varlen call times both candidate kernels of the classes 17..32, 33..48, 49..64 and 65..80
+    on its first batch (on a copy of the batch) and keeps the faster in the context's tuning table; each
+    candidate is accurate, and a second context given the table's text solves bit for bit alike without
+    timing."""
+    import torch
+
+    from epb200 import _lib
+
+    L = _lib.lib()
+    ns, mats = synth.config3_matrices(160, seed=41, degenerate_frac=0.25)
+    keys = ["eigh_varlen/16/32/1", "eigh_varlen/32/48/1", "eigh_varlen/48/64/1", "eigh_varlen/64/80/1"]
+    outs = []
+    for forced in (None, 0, 1):
+        s = torch.cuda.Stream()
+        ctx = _lib.Context(0, s)
+        if forced is not None:  # every class on the given candidate
+            t = _lib.TuneTable("".join(f"{k} {forced}\n" for k in keys))
+            t.import_into(ctx)
+        vb = B.VarlenBatch(mats)
+        with torch.cuda.stream(s):
+            _lib.check(L.epb_eigh_varlen(ctx.h, B.ptr(vb.A), B.ptr(vb.a_off), B.ptr(vb.n), len(mats), B.ptr(vb.E),
+                                         B.ptr(vb.e_off), b"V", 1))
+        torch.cuda.synchronize()
+        table = _lib.TuneTable(ctx.tune_text())
+        assert all(table.get(k) in (0, 1) for k in keys), ctx.tune_text()
+        es, us = vb.unpack()
+        _check(es, us, mats, 1e-10)
+        outs.append((table, vb.E.clone(), vb.A.clone()))
+    # replay of the autotuned choices from the table text
+    s = torch.cuda.Stream()
+    ctx = _lib.Context(0, s)
+    outs[0][0].import_into(ctx)
+    vb = B.VarlenBatch(mats)
+    with torch.cuda.stream(s):
+        _lib.check(L.epb_eigh_varlen(ctx.h, B.ptr(vb.A), B.ptr(vb.a_off), B.ptr(vb.n), len(mats), B.ptr(vb.E),
+                                     B.ptr(vb.e_off), b"V", 1))
+    torch.cuda.synchronize()
+    assert torch.equal(vb.E, outs[0][1]) and torch.equal(vb.A, outs[0][2])
