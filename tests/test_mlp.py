@@ -320,7 +320,7 @@ def test_learned_filter_identical_set_and_gain(L):
     for a in (fp64, learned):
         assert torch.equal(a[0], plain[0]) and torch.equal(a[1], plain[1]) and torch.equal(a[2], plain[2])
     st = learned[3]
-    assert st["culled"] + st["evaluated"] == st["tested"] == 64 * 2048
+    assert st["culled"] + st["evaluated"] == st["tested"] == 64 * 2048 == st["screened"]
     assert st["audited"] > 0 and st["violations"] == 0 and st["fallback_chunks"] == 0, st
     # the gain: with margins of 1.5 x the maximum held-out error the plain evaluation still runs on
     # well under two thirds of the pairs
@@ -351,5 +351,33 @@ def test_learned_filter_audit_repairs_bad_margins(L):
     learned = L.pair_window(bm, xk, xq, ef - 0.1, ef + 0.1, mlp=s, prec=L.PREC_MIXED)
     st = learned[3]
     assert st["violations"] > 0 and st["fallback_chunks"] > 0, st
+    for a, b in zip(learned[:3], plain[:3]):
+        assert torch.equal(a, b)
+
+
+@pytest.mark.gpu
+def test_learned_filter_screen_stops_when_it_culls_nothing(L):
+    """A surrogate of a rough band structure (held-out errors far wider than the window) culls nothing;
+    after 2^20 screened pairs the screen stops and the remaining chunks go straight to the plain
+    evaluation (stats: screened < tested), with the kept set still the plain filter's."""
+    import torch
+
+    nw = 16
+    ham = _ham(nw, 3, 80, decay=1.5)
+    bm = L.BandModel(ham)
+    rng = np.random.default_rng(81)
+    xt, xh = rng.random((3, 4096)), rng.random((3, 2048))
+    s = L.Surrogate(nf=32, hidden=64, nhidden=2, nout=nw, seed=82)
+    s.train(xt, bm.eigvals(xt), epochs=10, batch=512)
+    Eh = bm.eigvals(xh)
+    s.calibrate(xh, Eh)
+    ef = float(torch.median(Eh[:, nw // 2 - 1]).item())
+    xk, xq = rng.random((3, 96)), rng.random((3, 16384))
+    plain = L.pair_window(bm, xk, xq, ef - 0.02, ef + 0.02, prec=L.PREC_MIXED)
+    learned = L.pair_window(bm, xk, xq, ef - 0.02, ef + 0.02, mlp=s, prec=L.PREC_MIXED)
+    st = learned[3]
+    assert st["tested"] == 96 * 16384 and st["screened"] >= (1 << 20) and st["screened"] < st["tested"], st
+    assert st["culled"] * 5 < st["screened"], st
+    assert st["culled"] + st["evaluated"] == st["tested"], st
     for a, b in zip(learned[:3], plain[:3]):
         assert torch.equal(a, b)
