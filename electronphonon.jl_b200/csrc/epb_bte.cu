@@ -35,6 +35,8 @@ int eigh_check(epb_ctx* ctx);
 int window_filter(epb_ctx* ctx, const double* E, int64_t nw, int64_t nk, double wmin, double wmax, int32_t* bmin,
                   int32_t* bmax, int32_t* keep_idx, int64_t* nkeep, double* nbelow);
 int launch_phase(epb_ctx* ctx, const epb_rset* rs, const double* xk, int64_t nk, double2* phase);
+int fourier_zgemm(epb_ctx* ctx, const double2* op_r, int64_t ndata, int64_t ld_op, const epb_rset* rs,
+                  const double* x, int64_t npts, double2* phase_scratch, double2* out, int64_t ldo);
 int zgemm_nn(epb_ctx* ctx, const double2* A, int64_t lda, const double2* B, int64_t ldb, double2* C, int64_t ldc,
              int64_t M, int64_t N, int64_t K);
 int eph_rotations_f64(epb_ctx* ctx, const double2* g, int64_t ldg, int nw, int nbk, int nm, int64_t nq,
@@ -622,9 +624,15 @@ int epb_bte_serta(epb_ctx* ctx, epb_model* m, const epb_bte_params* prm, double*
   bte_grid_points_kernel<<<gsz(ctx, N), 256, 0, ctx->stream>>>(ng, xg);
   EPB_LAUNCH_CHECK();
   const int64_t HC = 65536;
+  // H(k) of the grid as a phase matrix times H(R) (one cuBLAS ZGEMM per chunk of 65536 points, the phase
+  // chunk in a workspace): the FP64 Fourier sum at library-GEMM rate
+  void* phs = nullptr;
+  EPB_TRY(ws_get(ctx, EPB_WS_PASS6, (size_t)m->rs_el->nr * std::min(HC, N) * sizeof(double2) + 256, &phs));
   for (int64_t k0 = 0; k0 < N; k0 += HC) {
     const int64_t kn = std::min(HC, N - k0);
-    EPB_TRY(fourier_f64(ctx, m->ham, nw2, nw2, m->rs_el, xg + 3 * k0, kn, U + k0 * nw2, nw2));
+    prof_begin(ctx, EPB_PROF_FOURIER_F64);
+    EPB_TRY(fourier_zgemm(ctx, m->ham, nw2, nw2, m->rs_el, xg + 3 * k0, kn, (double2*)phs, U + k0 * nw2, nw2));
+    prof_end(ctx);
     // the mixed mode solves in FP32 and refines in FP64 (eigenvalues to the FP64 level, vectors to ~1e-12)
     EPB_TRY(eigh_async(ctx, U + k0 * nw2, nw, kn, E + k0 * nw, true, nullptr, prm->prec));
   }
