@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cstring>
 
+#include "epb_eigh16.cuh"
 #include "epb_jacobi.cuh"
 
 namespace epb {
@@ -402,24 +403,6 @@ int eigh_dispatch(epb_ctx* ctx, EighArgs& a, int nmax, int prec) {
 
 int eigh_check(epb_ctx* ctx);
 
-struct Eigh16Args {
-  const double2* A;
-  const float* Hp;
-  double2* U64;
-  float2* U32;
-  double* E;
-  const double* mass;
-  int n;
-  int64_t batch;
-  int max_sweeps;
-  int* nonconv;
-  int refine;
-  int64_t* flag_list;
-  int* flag_count;
-  float2* V32;
-};
-int eigh16_launch(epb_ctx* ctx, Eigh16Args& a, bool mixed);
-
 // Offsets of the listed matrices for the FP64 slow path.
 __global__ void flag_offsets_kernel(const int64_t* __restrict__ list, const int* __restrict__ count, int64_t n,
                                     int64_t* __restrict__ a_off, int64_t* __restrict__ e_off, int32_t* __restrict__ nvec,
@@ -453,6 +436,7 @@ static int eigh_small(epb_ctx* ctx, const EighArgs& a, int prec) {
   b.max_sweeps = prec == EPB_PREC_FP64 ? 30 : 20;
   b.nonconv = ctx->dstat + 0;
   b.refine = a.U32 ? 1 : 2;
+  b.angle_stop = a.U32 ? 1e-2f : 1e-4f;  // the pass's packed path (complex64 output) as in eigh16_mixed_jacobi
   const bool slow_path = prec == EPB_PREC_MIXED && !a.Hp && a.A;
   int64_t* list = nullptr;
   if (prec == EPB_PREC_MIXED) {

@@ -15,7 +15,8 @@
 // orthogonal to every live column, so they never rotate.
 //
 // Mixed precision (EPB_PREC_MIXED): the sweeps run in FP32 to tol = 1e-6 (or until a sweep whose
-// rotation angles were all below 1e-4, after which the columns are orthogonal to the FP32 floor), then one FP64
+// rotation angles were all below 1e-4 -- 1e-2 for the pass, see PASS_ANGLE_STOP -- after which the columns
+// are orthogonal to the FP32 floor, resp. to 1e-4), then one FP64
 // refinement on the same registers: Lowdin re-orthonormalisation V(I - F/2), F = V^H V - I
 // (this re-orthogonalises near-degenerate clusters, whose FP32 vectors are defined only up to a
 // rotation inside the cluster), and a first-order Rayleigh-Ritz update from S = V^H H V:
@@ -28,6 +29,7 @@
 #include <type_traits>
 
 #include "epb_common.cuh"
+#include "epb_eigh16.cuh"
 
 namespace epb {
 
@@ -130,7 +132,7 @@ __device__ int onesided_sweeps(typename cplx<T>::type (&a)[E16], T tol, int max_
 // form. The rotation of each entry rounds as in the scalar form; the dot products accumulate even and
 // odd entries in two partial sums that are added at the end.
 
-__device__ int onesided_sweeps_f32x2(float2 (&a)[E16], float tol, int max_sweeps) {
+__device__ int onesided_sweeps_f32x2(float2 (&a)[E16], float tol, int max_sweeps, float angle_stop) {
   const int lane = threadIdx.x & 31;
   const int l = lane & 15, base = lane & 16;
   f32x2 X[E16 / 2], Y[E16 / 2];
@@ -188,7 +190,7 @@ __device__ int onesided_sweeps_f32x2(float2 (&a)[E16], float tol, int max_sweeps
         const float t = __fdividef(tau >= 0.f ? 1.f : -1.f, fabsf(tau) + u * rsqrtf(u));
         const float c = rsqrtf(1.f + t * t);
         const float sn = t * c, ex = gx * rag, ey = gy * rag;
-        big |= fabsf(t) > 1e-4f;
+        big |= fabsf(t) > angle_stop;
         // p: a_p <- c a_p - s conj(e) a_q;  q: a_q <- c a_q + s e a_p
         const float fx = isP ? -sn * ex : sn * ex, fy = sn * ey;
         nrm = isP ? A - t * ag : B + t * ag;
@@ -203,8 +205,9 @@ __device__ int onesided_sweeps_f32x2(float2 (&a)[E16], float tol, int max_sweeps
         }
       }
     }
-    // quadratic convergence: after a sweep whose rotations were all below 1e-4 the columns are
-    // orthogonal to O(1e-8), the FP32 floor; no confirmation sweep
+    // quadratic convergence: after a sweep whose rotations were all below angle_stop the mixing left is
+    // O(angle_stop^2) (1e-4 -> the FP32 floor; the pass's 1e-2 -> 1e-4, which its refinement removes); no
+    // confirmation sweep
     if (!__any_sync(0xffffffffu, big)) break;
   }
 #pragma unroll
@@ -215,23 +218,6 @@ __device__ int onesided_sweeps_f32x2(float2 (&a)[E16], float tol, int max_sweeps
   }
   return sweep;
 }
-
-struct Eigh16Args {
-  const double2* A;   // c128 input (n x n per matrix, upper triangle), or null
-  const float* Hp;    // packed FP32 Hermitian input (n*n per matrix), or null
-  double2* U64;       // c128 eigenvector output (may alias A), or null
-  float2* U32;        // c64 eigenvector output, or null
-  double* E;          // eigenvalues (n per matrix), or null
-  const double* mass; // phonon mode: scale by 1/sqrt(m_i m_j), omega = sign sqrt, u /= sqrt(m)
-  int n;
-  int64_t batch;
-  int max_sweeps;
-  int* nonconv;
-  int refine;         // FP64 refinement iterations (mixed only)
-  int64_t* flag_list; // if non-null: matrices with a near-degenerate pair are listed, not written
-  int* flag_count;
-  float2* V32;        // FP32 eigenvector workspace between the Jacobi and refinement kernels
-};
 
 // Load column l of matrix b (FP64), optionally mass-scaled; zero outside the live n x n block.
 __device__ __forceinline__ double2 load_h(const Eigh16Args& a, int64_t b, int i, int l, int n) {
@@ -324,7 +310,7 @@ __global__ void __launch_bounds__(128, MODE == 0 ? 1 : 4) eigh16_jacobi_kernel(E
     if constexpr (MODE == 0)
       sw = onesided_sweeps<T>(col, tol, a.max_sweeps);
     else
-      sw = onesided_sweeps_f32x2(col, tol, a.max_sweeps);
+      sw = onesided_sweeps_f32x2(col, tol, a.max_sweeps, a.angle_stop > 0.f ? a.angle_stop : 1e-4f);
     if (sw >= a.max_sweeps && lane == 0) atomicAdd(a.nonconv, 1);
     double nr2 = 0.0;
 #pragma unroll
@@ -815,6 +801,12 @@ int eigh16_launch(epb_ctx* ctx, Eigh16Args& a, bool mixed) {
 // FP32 vectors), then the refinement of V32 against H into U (sorted, complex64; FP64 residual, FP32
 // correction). Stream-ordered on
 // ctx->stream; the sweep-limit counter accumulates in the context status words.
+// The pass's FP32 sweeps stop after a sweep whose rotations all stayed below 1e-2 rad: quadratic convergence
+// leaves eigenvector mixing of O(1e-4), well inside the refinement's first-order range (|S'_kl| < 0.1 |gap|
+// means mixing < 0.1), whose update then leaves O(1e-8), under the complex64 output's rounding. An FP32
+// emulation of the sweeps gives 5.1 instead of 6.0 sweeps per matrix pair of a warp.
+constexpr float PASS_ANGLE_STOP = 1e-2f;
+
 static Eigh16Args pass_args(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V32, float2* U) {
   Eigh16Args b{};
   b.Hp = Hp;
@@ -825,6 +817,7 @@ static Eigh16Args pass_args(epb_ctx* ctx, const float* Hp, int64_t batch, float2
   b.nonconv = ctx->dstat + 0;
   b.refine = 1;
   b.V32 = V32;
+  b.angle_stop = PASS_ANGLE_STOP;
   return b;
 }
 
