@@ -3,8 +3,8 @@
 // Replaces eigvals_batched / eigen_batched (ext/ElectronPhononCUDAExt.jl:80-115, cuSOLVER
 // heevjBatched) for the small matrices of the e-ph pass (nw = 16 electrons, nm = 12 modes).
 //
-// A 16-lane half-warp owns one matrix; lane l holds column l of A = H + sigma I in registers
-// (sigma = 1.1 ||H||_F makes A positive definite, so its right singular vectors are the
+// FP64 sweeps: a 16-lane half-warp owns one matrix; lane l holds column l of A = H + sigma I in
+// registers (sigma = 1.1 ||H||_F makes A positive definite, so its right singular vectors are the
 // eigenvectors of H and the column norms after orthogonalisation are lambda + sigma). Each round
 // pairs the lanes by the circle method (lane 15 fixed); partners swap columns with shuffles,
 // form the 2x2 Gram matrix [[a, g], [g*, b]] and both apply the same plane rotation
@@ -12,7 +12,8 @@
 //     a_p <- c a_p - s conj(e) a_q,   a_q <- s e a_p + c a_q,
 // (the same J as the two-sided solver, applied to columns only). A pair is skipped when
 // |g| <= tol sqrt(a b); a sweep with no rotation ends the solve. Lanes >= n carry sigma e_l,
-// orthogonal to every live column, so they never rotate.
+// orthogonal to every live column, so they never rotate. FP32 sweeps (mixed precision) hold two
+// columns per lane, 8 lanes per matrix (eigh16_jacobi2c_kernel; the pair order is described there).
 //
 // Mixed precision (EPB_PREC_MIXED): the sweeps run in FP32 to tol = 1e-6 (or until a sweep whose
 // rotation angles were all below 1e-4 -- 1e-2 for the pass, see PASS_ANGLE_STOP -- after which the columns
@@ -26,7 +27,6 @@
 // orthonormalisation (their vectors are accurate as a subspace, which is what gauge-invariant
 // quantities use). EPB_PREC_FP64 runs the sweeps in FP64 to tol = 1e-15 and skips the refinement.
 #include <algorithm>
-#include <type_traits>
 
 #include "epb_common.cuh"
 #include "epb_eigh16.cuh"
@@ -126,99 +126,6 @@ __device__ int onesided_sweeps(typename cplx<T>::type (&a)[E16], T tol, int max_
   return sweep;
 }
 
-// ---- FP32 sweeps on packed pairs (sm_100 f32x2 arithmetic) ----------------------------------------
-// The column is held as 8 pairs of real parts and 8 pairs of imaginary parts (entries 2i, 2i+1), so the
-// Gram product and the rotation run as packed two-wide FMAs: half the FP32 instructions of the scalar
-// form. The rotation of each entry rounds as in the scalar form; the dot products accumulate even and
-// odd entries in two partial sums that are added at the end.
-
-__device__ int onesided_sweeps_f32x2(float2 (&a)[E16], float tol, int max_sweeps, float angle_stop) {
-  const int lane = threadIdx.x & 31;
-  const int l = lane & 15, base = lane & 16;
-  f32x2 X[E16 / 2], Y[E16 / 2];
-#pragma unroll
-  for (int i = 0; i < E16 / 2; ++i) {
-    X[i] = pk(a[2 * i].x, a[2 * i + 1].x);
-    Y[i] = pk(a[2 * i].y, a[2 * i + 1].y);
-  }
-  const f32x2 Z = pk(0.f, 0.f);
-  const float tol2 = tol * tol;
-  int sweep = 0;
-  for (; sweep < max_sweeps; ++sweep) {
-    f32x2 n2 = Z;
-#pragma unroll
-    for (int i = 0; i < E16 / 2; ++i) n2 = pfma(Y[i], Y[i], pfma(X[i], X[i], n2));
-    float nrm = hsum(n2);
-    int big = 0;  // a rotation by more than 1e-4 in this sweep
-#pragma unroll 1
-    for (int r = 0; r < 15; ++r) {
-      const int pl = circle_partner(l, r);
-      const int src = base + pl;
-      f32x2 BX[E16 / 2], BY[E16 / 2];
-#pragma unroll
-      for (int i = 0; i < E16 / 2; ++i) {
-        BX[i] = __shfl_sync(0xffffffffu, X[i], src);
-        BY[i] = __shfl_sync(0xffffffffu, Y[i], src);
-      }
-      const float nb = __shfl_sync(0xffffffffu, nrm, src);
-      const bool isP = l < pl;
-      // Gram entry conj(own) . partner: Re = X.BX + Y.BY, Im = X.BY - Y.BX. The partner lane forms the
-      // same elementwise products in the same order, with the two imaginary sums trading places, so
-      // both lanes hold bitwise-identical g = a_p^H a_q and norms (a, b) in the p lane's orientation
-      // and derive the same rotation without exchanging it.
-      // (independent even / odd chains of four: the dot products are on the round's critical path)
-      f32x2 gx0 = Z, gx1 = Z, gy0 = Z, gy1 = Z, gi0 = Z, gi1 = Z, gj0 = Z, gj1 = Z;
-#pragma unroll
-      for (int i = 0; i < E16 / 2; i += 2) {
-        gx0 = pfma(X[i], BX[i], gx0);
-        gx1 = pfma(X[i + 1], BX[i + 1], gx1);
-        gy0 = pfma(Y[i], BY[i], gy0);
-        gy1 = pfma(Y[i + 1], BY[i + 1], gy1);
-        gi0 = pfma(X[i], BY[i], gi0);
-        gi1 = pfma(X[i + 1], BY[i + 1], gi1);
-        gj0 = pfma(Y[i], BX[i], gj0);
-        gj1 = pfma(Y[i + 1], BX[i + 1], gj1);
-      }
-      const float hi = hsum(gi0) + hsum(gi1), hj = hsum(gj0) + hsum(gj1);
-      const float gx = (hsum(gx0) + hsum(gx1)) + (hsum(gy0) + hsum(gy1)), gy = isP ? hi - hj : hj - hi;
-      const float A = isP ? nrm : nb, B = isP ? nb : nrm;
-      const float ag2 = gx * gx + gy * gy;
-      if (ag2 > tol2 * (A * B) && ag2 > 0.f) {
-        const float rag = rsqrtf(ag2), ag = ag2 * rag;
-        const float tau = 0.5f * (B - A) * rag;
-        const float u = 1.f + tau * tau;
-        const float t = __fdividef(tau >= 0.f ? 1.f : -1.f, fabsf(tau) + u * rsqrtf(u));
-        const float c = rsqrtf(1.f + t * t);
-        const float sn = t * c, ex = gx * rag, ey = gy * rag;
-        big |= fabsf(t) > angle_stop;
-        // p: a_p <- c a_p - s conj(e) a_q;  q: a_q <- c a_q + s e a_p
-        const float fx = isP ? -sn * ex : sn * ex, fy = sn * ey;
-        nrm = isP ? A - t * ag : B + t * ag;
-        // a <- c a + f b:  Re = c X + fx BX - fy BY,  Im = c Y + fx BY + fy BX
-        const f32x2 C2 = pk(c, c), FX = pk(fx, fx), FY = pk(fy, fy), FYN = pk(-fy, -fy);
-#pragma unroll
-        for (int i = 0; i < E16 / 2; ++i) {
-          const f32x2 xr = pfma(C2, X[i], pfma(FX, BX[i], pmul(FYN, BY[i])));
-          const f32x2 yr = pfma(C2, Y[i], pfma(FX, BY[i], pmul(FY, BX[i])));
-          X[i] = xr;
-          Y[i] = yr;
-        }
-      }
-    }
-    // quadratic convergence: after a sweep whose rotations were all below angle_stop the mixing left is
-    // O(angle_stop^2) (1e-4 -> the FP32 floor; the pass's 1e-2 -> 1e-4, which its refinement removes); no
-    // confirmation sweep
-    if (!__any_sync(0xffffffffu, big)) break;
-  }
-#pragma unroll
-  for (int i = 0; i < E16 / 2; ++i) {
-    const float2 x = upk(X[i]), y = upk(Y[i]);
-    a[2 * i] = make_float2(x.x, y.x);
-    a[2 * i + 1] = make_float2(x.y, y.y);
-  }
-  return sweep;
-}
-
 // Load column l of matrix b (FP64), optionally mass-scaled; zero outside the live n x n block.
 __device__ __forceinline__ double2 load_h(const Eigh16Args& a, int64_t b, int i, int l, int n) {
   double2 v = make_double2(0.0, 0.0);
@@ -278,12 +185,233 @@ __device__ __forceinline__ void write_sorted(const Eigh16Args& a, int64_t b, boo
   }
 }
 
-// MODE 0: whole solve in FP64 (sorted output).  MODE 1: FP32 sweeps only; writes the normalised,
-// unsorted FP32 columns to a.V32 (16 x 16 per matrix) for MODE 2.
-template <int MODE>
-__global__ void __launch_bounds__(128, MODE == 0 ? 1 : 4) eigh16_jacobi_kernel(Eigh16Args a) {
-  using T = typename std::conditional<MODE == 0, double, float>::type;
-  using C = typename cplx<T>::type;
+// ---- FP32 sweeps, two columns per lane (8 lanes per matrix, 4 matrices per warp) ------------------------
+// Lane l of a matrix's 8-lane group keeps columns l ("a") and l + 8 ("b") of H + sigma I for the whole solve,
+// as packed f32x2 pairs (real / imaginary parts of entries 2i, 2i+1). A sweep is 15 steps of 8 disjoint
+// pairs, in the same order every sweep:
+//   steps 0..7: lane l rotates its own pair (a_l, b_{(l+s) mod 8}); between steps the b columns move one lane
+//     down the ring (after the eighth move they are home again). These are the 64 pairs between the two
+//     halves, each formed by one lane alone: no duplicated Gram product, one column shuffle per pair.
+//   steps 8..14: the round-robin over the 8 lanes, lane l rotating a_l with the partner's a and b_l with the
+//     partner's b; both lanes of such a pair form the same Gram entry bit for bit (the 16-lane rule below).
+// Against one column per lane this drops a quarter of the Gram products and of the column shuffles per sweep
+// and holds two matrices per 16 lanes. An FP32 emulation of the sweeps (GUE matrices, stop at 1e-2) gives
+// 5.07 sweeps per warp of four matrices, 5.2-5.3 for the 16-lane round-robin per warp of two, and 5.6-6.0 for
+// two-column orders whose pair sequence changes from sweep to sweep.
+
+__device__ __forceinline__ int circle8_partner(int l, int r) {
+  // 8 players, player 7 fixed, 7 rounds
+  if (l == 7) return r;
+  if (l == r) return 7;
+  const int p = (2 * r - l) % 7;
+  return p < 0 ? p + 7 : p;
+}
+
+// Rotation of the pair (p, q) with g = a_p^H a_q and squared norms A, B: c, and w with s e = w g and
+// t |g| = tg (signed); see the 16-lane form. Returns false below the tolerance.
+__device__ __forceinline__ bool pair_rotation(float gx, float gy, float A, float B, float tol2, float as2, float& c,
+                                              float& w, float& tg, int& big) {
+  const float ag2 = gx * gx + gy * gy;
+  if (!(ag2 > tol2 * (A * B) && ag2 > 0.f)) return false;
+  const float d = B - A;
+  const float rr = rsqrtf(fmaf(d, d, 4.f * ag2));
+  const float c2 = fmaf(0.5f * fabsf(d), rr, 0.5f);
+  const float ic = rsqrtf(c2);
+  c = c2 * ic;
+  w = copysignf(rr * ic, d);
+  const float tq = rr * ic * ic;
+  big |= ag2 * (tq * tq) > as2;
+  tg = w * ic * ag2;
+  return true;
+}
+
+// Squared norm of a packed column.
+__device__ __forceinline__ float col_norm2(const f32x2 (&X)[8], const f32x2 (&Y)[8]) {
+  f32x2 n0 = pk(0.f, 0.f), n1 = pk(0.f, 0.f);
+#pragma unroll
+  for (int i = 0; i < 8; i += 2) {
+    n0 = pfma(Y[i], Y[i], pfma(X[i], X[i], n0));
+    n1 = pfma(Y[i + 1], Y[i + 1], pfma(X[i + 1], X[i + 1], n1));
+  }
+  return hsum(padd(n0, n1));
+}
+
+// One round-robin pair between lanes: rotate this lane's column (X, Y; squared norm nrm) against the partner
+// lane's column of the same half. Both lanes derive the same rotation (bitwise-identical Gram sums).
+__device__ __forceinline__ void robin_pair(f32x2 (&X)[8], f32x2 (&Y)[8], float& nrm, int src, bool isP, float tol2,
+                                           float as2, int& big) {
+  const f32x2 Z = pk(0.f, 0.f);
+  f32x2 PX[8], PY[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    PX[i] = __shfl_sync(0xffffffffu, X[i], src);
+    PY[i] = __shfl_sync(0xffffffffu, Y[i], src);
+  }
+  const float nb = __shfl_sync(0xffffffffu, nrm, src);
+  f32x2 gx0 = Z, gx1 = Z, gy0 = Z, gy1 = Z, gi0 = Z, gi1 = Z, gj0 = Z, gj1 = Z;
+#pragma unroll
+  for (int i = 0; i < 8; i += 2) {
+    gx0 = pfma(X[i], PX[i], gx0);
+    gx1 = pfma(X[i + 1], PX[i + 1], gx1);
+    gy0 = pfma(Y[i], PY[i], gy0);
+    gy1 = pfma(Y[i + 1], PY[i + 1], gy1);
+    gi0 = pfma(X[i], PY[i], gi0);
+    gi1 = pfma(X[i + 1], PY[i + 1], gi1);
+    gj0 = pfma(Y[i], PX[i], gj0);
+    gj1 = pfma(Y[i + 1], PX[i + 1], gj1);
+  }
+  const float hi = hsum(padd(gi0, gi1)), hj = hsum(padd(gj0, gj1));
+  const float gx = hsum(padd(padd(gx0, gx1), padd(gy0, gy1))), gy = isP ? hi - hj : hj - hi;
+  const float A = isP ? nrm : nb, B = isP ? nb : nrm;
+  float c, w, tg;
+  if (pair_rotation(gx, gy, A, B, tol2, as2, c, w, tg, big)) {
+    // p: a_p <- c a_p - w conj(g) a_q;  q: a_q <- c a_q + w g a_p
+    const float fx = isP ? -w * gx : w * gx, fy = w * gy;
+    nrm = isP ? A - tg : B + tg;
+    const f32x2 C2 = pk(c, c), FX = pk(fx, fx), FY = pk(fy, fy), FYN = pk(-fy, -fy);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const f32x2 xr = pfma(C2, X[i], pfma(FX, PX[i], pmul(FYN, PY[i])));
+      const f32x2 yr = pfma(C2, Y[i], pfma(FX, PY[i], pmul(FY, PX[i])));
+      X[i] = xr;
+      Y[i] = yr;
+    }
+  }
+}
+
+__device__ int onesided_sweeps_2col(f32x2 (&XA)[8], f32x2 (&YA)[8], f32x2 (&XB)[8], f32x2 (&YB)[8], float tol,
+                                    int max_sweeps, float angle_stop) {
+  const int lane = threadIdx.x & 31;
+  const int l = lane & 7, base = lane & 24;
+  const f32x2 Z = pk(0.f, 0.f);
+  const float tol2 = tol * tol, as2 = angle_stop * angle_stop;
+  const int down = base + ((l + 1) & 7);
+  int sweep = 0;
+  for (; sweep < max_sweeps; ++sweep) {
+    float nA = col_norm2(XA, YA), nB = col_norm2(XB, YB);
+    int big = 0;
+    // steps 0..7: the lane's own pair (a, b), then b moves one lane down the ring
+#pragma unroll 1
+    for (int s = 0; s < 8; ++s) {
+      f32x2 gx0 = Z, gx1 = Z, gi0 = Z, gi1 = Z, gj0 = Z, gj1 = Z;
+#pragma unroll
+      for (int i = 0; i < 8; i += 2) {
+        gx0 = pfma(YA[i], YB[i], pfma(XA[i], XB[i], gx0));
+        gx1 = pfma(YA[i + 1], YB[i + 1], pfma(XA[i + 1], XB[i + 1], gx1));
+        gi0 = pfma(XA[i], YB[i], gi0);
+        gi1 = pfma(XA[i + 1], YB[i + 1], gi1);
+        gj0 = pfma(YA[i], XB[i], gj0);
+        gj1 = pfma(YA[i + 1], XB[i + 1], gj1);
+      }
+      // g = a^H b
+      const float gx = hsum(padd(gx0, gx1)), gy = hsum(padd(gi0, gi1)) - hsum(padd(gj0, gj1));
+      float c, w, tg;
+      if (pair_rotation(gx, gy, nA, nB, tol2, as2, c, w, tg, big)) {
+        // a <- c a - w conj(g) b;  b <- c b + w g a
+        const float fx = w * gx, fy = w * gy;
+        nA -= tg;
+        nB += tg;
+        const f32x2 C2 = pk(c, c), FX = pk(fx, fx), FY = pk(fy, fy), FXN = pk(-fx, -fx), FYN = pk(-fy, -fy);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const f32x2 xa = pfma(C2, XA[i], pfma(FXN, XB[i], pmul(FYN, YB[i])));
+          const f32x2 ya = pfma(C2, YA[i], pfma(FXN, YB[i], pmul(FY, XB[i])));
+          const f32x2 xb = pfma(C2, XB[i], pfma(FX, XA[i], pmul(FYN, YA[i])));
+          const f32x2 yb = pfma(C2, YB[i], pfma(FX, YA[i], pmul(FY, XA[i])));
+          XA[i] = xa;
+          YA[i] = ya;
+          XB[i] = xb;
+          YB[i] = yb;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        XB[i] = __shfl_sync(0xffffffffu, XB[i], down);
+        YB[i] = __shfl_sync(0xffffffffu, YB[i], down);
+      }
+      nB = __shfl_sync(0xffffffffu, nB, down);
+    }
+    // steps 8..14: round-robin over the 8 lanes within each half
+#pragma unroll 1
+    for (int r = 0; r < 7; ++r) {
+      const int p = circle8_partner(l, r);
+      const int src = base + p;
+      robin_pair(XA, YA, nA, src, l < p, tol2, as2, big);
+      robin_pair(XB, YB, nB, src, l < p, tol2, as2, big);
+    }
+    if (!__any_sync(0xffffffffu, big)) break;
+  }
+  return sweep;
+}
+
+// Mixed precision, first half: FP32 sweeps with two columns per lane; writes the normalised, unsorted FP32
+// columns to a.V32 (16 x 16 per matrix, column j = the rotated column j of H + sigma I) for the refinement.
+__global__ void __launch_bounds__(128, 4) eigh16_jacobi2c_kernel(Eigh16Args a) {
+  const int lane = threadIdx.x & 31;
+  const int l = lane & 7;
+  const int slot = threadIdx.x >> 3;
+  const int n = a.n;
+  const int64_t per_block = blockDim.x / 8;
+  for (int64_t b0 = (int64_t)blockIdx.x * per_block; b0 < a.batch; b0 += (int64_t)gridDim.x * per_block) {
+    const int64_t b = b0 + slot;
+    const bool live = b < a.batch;
+    float ar[E16], ai[E16], br[E16], bi[E16];
+    double f2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < E16; ++i) {
+      const double2 u = live ? load_h(a, b, i, l, n) : make_double2(0.0, 0.0);
+      const double2 v = live ? load_h(a, b, i, l + 8, n) : make_double2(0.0, 0.0);
+      f2 += (u.x * u.x + u.y * u.y) + (v.x * v.x + v.y * v.y);
+      ar[i] = (float)u.x;
+      ai[i] = (float)u.y;
+      br[i] = (float)v.x;
+      bi[i] = (float)v.y;
+    }
+    for (int o = 4; o > 0; o >>= 1) f2 += __shfl_xor_sync(0xffffffffu, f2, o);  // within the 8-lane group
+    const double sigma = f2 > 0.0 ? 1.1 * sqrt(f2) : 1.0;                       // zero (or padding): shift 1
+#pragma unroll
+    for (int i = 0; i < E16; ++i) {
+      if (i == l) ar[i] += (float)sigma;  // columns >= n: sigma e_j
+      if (i == l + 8) br[i] += (float)sigma;
+    }
+    f32x2 XA[8], YA[8], XB[8], YB[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      XA[i] = pk(ar[2 * i], ar[2 * i + 1]);
+      YA[i] = pk(ai[2 * i], ai[2 * i + 1]);
+      XB[i] = pk(br[2 * i], br[2 * i + 1]);
+      YB[i] = pk(bi[2 * i], bi[2 * i + 1]);
+    }
+    const int sw = onesided_sweeps_2col(XA, YA, XB, YB, 1e-6f, a.max_sweeps, a.angle_stop > 0.f ? a.angle_stop : 1e-4f);
+    if (sw >= a.max_sweeps && lane == 0) atomicAdd(a.nonconv, 1);
+    if (live) {
+      float2* vo = a.V32 + b * (int64_t)E16 * E16;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const f32x2(&X)[8] = h ? XB : XA;
+        const f32x2(&Y)[8] = h ? YB : YA;
+        double nr2 = 0.0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const float2 x = upk(X[i]), y = upk(Y[i]);
+          nr2 += (double)x.x * x.x + (double)y.x * y.x;
+          nr2 += (double)x.y * x.y + (double)y.y * y.y;
+        }
+        const double inv = 1.0 / sqrt(nr2);
+        float2* vc = vo + (int64_t)E16 * (l + 8 * h);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const float2 x = upk(X[i]), y = upk(Y[i]);
+          vc[2 * i] = make_float2((float)(x.x * inv), (float)(y.x * inv));
+          vc[2 * i + 1] = make_float2((float)(x.y * inv), (float)(y.y * inv));
+        }
+      }
+    }
+  }
+}
+
+// Whole solve in FP64 (sorted output): a 16-lane half-warp per matrix, lane l holding column l.
+__global__ void __launch_bounds__(128, 1) eigh16_jacobi_kernel(Eigh16Args a) {
   const int lane = threadIdx.x & 31;
   const int l = lane & 15;
   const int slot = threadIdx.x >> 4;
@@ -292,42 +420,28 @@ __global__ void __launch_bounds__(128, MODE == 0 ? 1 : 4) eigh16_jacobi_kernel(E
   for (int64_t b0 = (int64_t)blockIdx.x * per_block; b0 < a.batch; b0 += (int64_t)gridDim.x * per_block) {
     const int64_t b = b0 + slot;
     const bool live = b < a.batch;
-    C col[E16];
+    double2 col[E16];
     double f2 = 0.0;
 #pragma unroll
     for (int i = 0; i < E16; ++i) {
-      double2 v = live ? load_h(a, b, i, l, n) : make_double2(0.0, 0.0);
-      f2 += v.x * v.x + v.y * v.y;
-      col[i] = mk2((T)v.x, (T)v.y);
+      col[i] = live ? load_h(a, b, i, l, n) : make_double2(0.0, 0.0);
+      f2 += col[i].x * col[i].x + col[i].y * col[i].y;
     }
     for (int o = 8; o > 0; o >>= 1) f2 += __shfl_xor_sync(0xffffffffu, f2, o);  // within the half-warp
     const double sigma = f2 > 0.0 ? 1.1 * sqrt(f2) : 1.0;  // zero (or padding) matrices: shift 1
 #pragma unroll
     for (int i = 0; i < E16; ++i)
-      if (i == l) col[i].x += (T)sigma;  // lanes >= n: sigma e_l
-    const T tol = MODE == 0 ? T(1e-15) : T(1e-6);
-    int sw;
-    if constexpr (MODE == 0)
-      sw = onesided_sweeps<T>(col, tol, a.max_sweeps);
-    else
-      sw = onesided_sweeps_f32x2(col, tol, a.max_sweeps, a.angle_stop > 0.f ? a.angle_stop : 1e-4f);
+      if (i == l) col[i].x += sigma;  // lanes >= n: sigma e_l
+    const int sw = onesided_sweeps<double>(col, 1e-15, a.max_sweeps);
     if (sw >= a.max_sweeps && lane == 0) atomicAdd(a.nonconv, 1);
     double nr2 = 0.0;
 #pragma unroll
-    for (int i = 0; i < E16; ++i) nr2 += (double)col[i].x * col[i].x + (double)col[i].y * col[i].y;
+    for (int i = 0; i < E16; ++i) nr2 += col[i].x * col[i].x + col[i].y * col[i].y;
     const double inv = 1.0 / sqrt(nr2);
-    if (MODE == 1) {
-      if (live) {
-        float2* vo = a.V32 + b * (int64_t)E16 * E16 + (int64_t)E16 * l;
+    double2 v[E16];
 #pragma unroll
-        for (int i = 0; i < E16; ++i) vo[i] = make_float2((float)(col[i].x * inv), (float)(col[i].y * inv));
-      }
-    } else {
-      double2 v[E16];
-#pragma unroll
-      for (int i = 0; i < E16; ++i) v[i] = make_double2(col[i].x * inv, col[i].y * inv);
-      write_sorted(a, b, live, lane, l, n, sqrt(nr2) - sigma, v);
-    }
+    for (int i = 0; i < E16; ++i) v[i] = make_double2(col[i].x * inv, col[i].y * inv);
+    write_sorted(a, b, live, lane, l, n, sqrt(nr2) - sigma, v);
   }
 }
 
@@ -773,7 +887,7 @@ int eigh16_launch(epb_ctx* ctx, Eigh16Args& a, bool mixed) {
   };
   if (!mixed) {
     prof_begin(ctx, EPB_PROF_EIGH);
-    eigh16_jacobi_kernel<0><<<grid_cap(8), threads, 0, ctx->stream>>>(a);
+    eigh16_jacobi_kernel<<<grid_cap(8), threads, 0, ctx->stream>>>(a);
     prof_end(ctx);
     EPB_LAUNCH_CHECK();
     return EPB_OK;
@@ -786,7 +900,8 @@ int eigh16_launch(epb_ctx* ctx, Eigh16Args& a, bool mixed) {
     attr = true;
   }
   prof_begin(ctx, EPB_PROF_EIGH);
-  eigh16_jacobi_kernel<1><<<grid_cap(16), threads, 0, ctx->stream>>>(a);
+  eigh16_jacobi2c_kernel<<<(unsigned)std::min<int64_t>(cdiv(a.batch, 16), (int64_t)ctx->sm_count * 16), 128, 0,
+                           ctx->stream>>>(a);
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   prof_begin(ctx, EPB_PROF_REFINE);
@@ -804,7 +919,7 @@ int eigh16_launch(epb_ctx* ctx, Eigh16Args& a, bool mixed) {
 // The pass's FP32 sweeps stop after a sweep whose rotations all stayed below 1e-2 rad: quadratic convergence
 // leaves eigenvector mixing of O(1e-4), well inside the refinement's first-order range (|S'_kl| < 0.1 |gap|
 // means mixing < 0.1), whose update then leaves O(1e-8), under the complex64 output's rounding. An FP32
-// emulation of the sweeps gives 5.1 instead of 6.0 sweeps per matrix pair of a warp.
+// emulation of the sweeps gives 5.07 instead of 5.99 sweeps per warp of four matrices.
 constexpr float PASS_ANGLE_STOP = 1e-2f;
 
 static Eigh16Args pass_args(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V32, float2* U) {
@@ -824,9 +939,9 @@ static Eigh16Args pass_args(epb_ctx* ctx, const float* Hp, int64_t batch, float2
 int eigh16_mixed_jacobi(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V32) {
   if (batch == 0) return EPB_OK;
   Eigh16Args b = pass_args(ctx, Hp, batch, V32, nullptr);
-  const int64_t blocks = std::min<int64_t>(cdiv(batch, 8), (int64_t)ctx->sm_count * 16);
+  const int64_t blocks = std::min<int64_t>(cdiv(batch, 16), (int64_t)ctx->sm_count * 16);
   prof_begin(ctx, EPB_PROF_EIGH);
-  eigh16_jacobi_kernel<1><<<(unsigned)blocks, 128, 0, ctx->stream>>>(b);
+  eigh16_jacobi2c_kernel<<<(unsigned)blocks, 128, 0, ctx->stream>>>(b);
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
