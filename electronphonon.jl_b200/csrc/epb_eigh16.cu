@@ -741,10 +741,22 @@ __global__ void __launch_bounds__(128, 3) eigh16_refine2_kernel(Eigh16Args a) {
 // the Rayleigh quotients (the eigenvalues, used for the order) stay FP64. FP64 work: W = H V (128 complex
 // FMAs per lane); FP32: S, G and V t (384 complex FMAs per lane), against 512 FP64 complex FMAs per lane
 // for the all-FP64 update. Pass only: no mass scaling, no flag list, one iteration.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 __global__ void __launch_bounds__(128, 4) eigh16_refine_c64_kernel(Eigh16Args a) {
   __shared__ double2 Hs[4][E16 * RLD];  // H[i][k] at i * RLD + k
   __shared__ float2 Vs[4][E16 * RLD];   // V[i][k] (FP32 Jacobi vectors)
   __shared__ float2 Rs[4][E16 * RLD];   // R[i][l] = (H V - V d)[i][l], rounded to FP32
+  // packed FP32 H (n = 16) and FP32 vectors of the warp's next matrix, fetched with cp.async while the
+  // current one is refined (the solve is latency-bound at 16 warps per SM)
+  __shared__ __align__(16) float HpS[4][E16 * E16];
+  __shared__ __align__(16) float2 VpS[4][E16 * E16];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int l = lane & 15, h = lane >> 4, r0 = 8 * h;
   const int n = a.n;
@@ -752,12 +764,41 @@ __global__ void __launch_bounds__(128, 4) eigh16_refine_c64_kernel(Eigh16Args a)
   float2* V = Vs[warp];
   float2* R = Rs[warp];
   constexpr double th2 = 1e-2;  // first-order range |S'_kl| < 0.1 |gap| (no slow path in the pass)
-  for (int64_t b = (int64_t)blockIdx.x * 4 + warp; b - warp < a.batch; b += (int64_t)gridDim.x * 4) {
+  const int64_t step = (int64_t)gridDim.x * 4;
+  const bool staged = a.Hp != nullptr && n == E16 &&
+                      ((reinterpret_cast<uintptr_t>(a.Hp) | reinterpret_cast<uintptr_t>(a.V32)) & 15) == 0;
+  auto prefetch = [&](int64_t bn) {
+    if (bn < a.batch) {
+      const float4* hs = reinterpret_cast<const float4*>(a.Hp + bn * (E16 * E16));     // 64 x 16 bytes
+      const float4* vs = reinterpret_cast<const float4*>(a.V32 + bn * (E16 * E16));    // 128 x 16 bytes
+      for (int c = lane; c < 64; c += 32) cp_async16(&HpS[warp][4 * c], hs + c);
+      for (int c = lane; c < 128; c += 32) cp_async16(&VpS[warp][2 * c], vs + c);
+    }
+    cp_async_commit();
+  };
+  if (staged) prefetch((int64_t)blockIdx.x * 4 + warp);
+  for (int64_t b = (int64_t)blockIdx.x * 4 + warp; b - warp < a.batch; b += step) {
     const bool live = b < a.batch;
-#pragma unroll
-    for (int r = 0; r < 8; ++r) H[(r0 + r) * RLD + l] = live ? load_h(a, b, r0 + r, l, n) : make_double2(0.0, 0.0);
     float2 v[8];
-    {
+    if (staged) {
+      cp_async_wait0();
+      __syncwarp();
+      const float* hp = HpS[warp];
+      constexpr int NRE = E16 * (E16 + 1) / 2;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int i = r0 + r, ii = i <= l ? i : l, jj = i <= l ? l : i;
+        const float re = hp[jj * (jj + 1) / 2 + ii];
+        const float im = ii < jj ? hp[NRE + jj * (jj - 1) / 2 + ii] : 0.f;
+        H[i * RLD + l] = live ? make_double2(re, i <= l ? im : -im) : make_double2(0.0, 0.0);
+        v[r] = live ? VpS[warp][E16 * l + i] : make_float2(i == l ? 1.f : 0.f, 0.f);
+        V[i * RLD + l] = v[r];
+      }
+      __syncwarp();  // every lane has read the staging buffers
+      prefetch(b + step);
+    } else {
+#pragma unroll
+      for (int r = 0; r < 8; ++r) H[(r0 + r) * RLD + l] = live ? load_h(a, b, r0 + r, l, n) : make_double2(0.0, 0.0);
       const float2* vi = a.V32 + (live ? b : 0) * (int64_t)E16 * E16 + (int64_t)E16 * l + r0;
 #pragma unroll
       for (int r = 0; r < 8; ++r) {
