@@ -323,22 +323,26 @@ __global__ void __launch_bounds__(32 * ROT_MMA_WARPS, 1) eph_rot_mma_kernel(RotA
   if (kcur >= 0) flush(kcur);
 }
 
-// g2sum[nu, k] += sum over the warps' slots in slot order (one block per k, deterministic).
-__global__ void rot_reduce_kernel(const double* __restrict__ partial, int64_t nwarps, double* __restrict__ g2sum) {
-  constexpr int NM = 12, PARTS = 8;
-  __shared__ double red[PARTS][NM];
-  const int64_t k = blockIdx.x;
-  const int nu = threadIdx.x % NM, part = threadIdx.x / NM;
-  if (part < PARTS) {
-    double s = 0.0;
-    for (int64_t w = part; w < nwarps; w += PARTS) s += partial[nu + NM * (w + nwarps * k)];
-    red[part][nu] = s;
-  }
+// g2sum[nu, k] += sum over the warps' slots in a fixed order: one 64-thread block per (mode, k), so that the
+// blocks fit beside the pipeline's other kernels; each thread adds every 64th slot, then a fixed tree.
+constexpr int ROT_RED_THREADS = 64;
+__global__ void __launch_bounds__(ROT_RED_THREADS) rot_reduce_kernel(const double* __restrict__ partial,
+                                                                     int64_t nwarps, double* __restrict__ g2sum) {
+  constexpr int NM = 12;
+  __shared__ double red[ROT_RED_THREADS / 32];
+  const int nu = blockIdx.x % NM;
+  const int64_t k = blockIdx.x / NM;
+  double s = 0.0;
+  for (int64_t w = threadIdx.x; w < nwarps; w += ROT_RED_THREADS) s += partial[nu + NM * (w + nwarps * k)];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
   __syncthreads();
-  if (threadIdx.x < NM) {
-    double s = 0.0;
-    for (int p = 0; p < PARTS; ++p) s += red[p][threadIdx.x];
-    g2sum[threadIdx.x + NM * k] += s;
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+#pragma unroll
+    for (int p = 0; p < ROT_RED_THREADS / 32; ++p) t += red[p];
+    g2sum[nu + NM * k] += t;
   }
 }
 
@@ -372,7 +376,7 @@ int rot_mma_launch(epb_ctx* ctx, const float* g, int64_t g_stride, const float2*
   EPB_CUDA(cudaMemsetAsync(partial, 0, sizeof(double) * 12 * nwarps * nkb, ctx->stream));
   eph_rot_mma_kernel<<<grid, 32 * ROT_MMA_WARPS, 0, ctx->stream>>>(a);
   EPB_LAUNCH_CHECK();
-  rot_reduce_kernel<<<(unsigned)nkb, 128, 0, ctx->stream>>>(partial, nwarps, g2sum);
+  rot_reduce_kernel<<<(unsigned)(12 * nkb), ROT_RED_THREADS, 0, ctx->stream>>>(partial, nwarps, g2sum);
   EPB_LAUNCH_CHECK();
   return EPB_OK;
 }
