@@ -412,9 +412,10 @@ struct GemmCfg {
 // truncation (round toward zero), so a long K loop loses about half an ulp of the running sum per step
 // and every |C| comes out biased low: with the 92 K-steps of the 729-vector Re sum this measured a
 // -3.4e-6 relative bias of |g|^2 in the full pass. The kernels therefore restart the accumulator after
-// every 64-wide K chunk (four K-steps) and the epilogue adds each chunk's lead + correction
-// accumulators into FP32 registers with round-to-nearest, which leaves ~2e-7 (numpy emulation of the
-// truncating accumulator). `run` holds the tile row's NT running sums; the two TMEM buffers alternate by
+// every 64-wide K chunk (four K-steps; the A-resident kernel after every two) and the epilogue adds each
+// chunk's lead + correction accumulators into FP32 registers with round-to-nearest, which leaves ~2e-7
+// (numpy emulation of the truncating accumulator; the pass's measured |g|^2 error barely moves at two
+// chunks and grows by a third at four). `run` holds the tile row's NT running sums; the two TMEM buffers alternate by
 // chunk, so the MMAs of the next chunk overlap the epilogue of this one.
 // NT running sums of one tile row: columns [0, NT) of the lead accumulator at tacc and of the correction
 // accumulator ACC_STRIDE columns further.
@@ -632,9 +633,13 @@ __global__ void __launch_bounds__(192, 1) split_gemm_kernel(SplitGemmArgs a) {
 // so each 128 x 128 output tile costs one B tile of L2 traffic instead of an A and a B tile (the
 // kR->kq GEMM of the pass, K' = 256, is bound by that feed). A has its own full / empty barrier pair:
 // the MMA thread commits `a_empty` after the unit's last MMA, the producer waits on it before it
-// overwrites A. Same products, accumulators and promotion as split_gemm_kernel, with eight epilogue warps
-// (two per TMEM lane quarter, each holding half of a row's running sums); no grouped mode.
+// overwrites A. Same products and accumulators as split_gemm_kernel, the promotion after every second K
+// chunk (ARES_PROMO), eight epilogue warps (two per TMEM lane quarter, each holding half of a row's running
+// sums); no grouped mode.
 constexpr int ARES_KC = 4, ARES_STAGES = 2;
+// K chunks per accumulator promotion in the A-resident kernel: the accumulators restart every
+// 64 * ARES_PROMO K values (the truncation bias grows with that length: about 3e-7 of |g|^2 at 128)
+constexpr int ARES_PROMO = 2;
 constexpr int ARES_EPI = 2;  // epilogue warps per TMEM lane quarter (each promotes NT / ARES_EPI columns of a row)
 constexpr int ARES_THREADS = 64 + 32 * 4 * ARES_EPI;  // producer, MMA issuer, epilogue warps
 template <bool BF16, int NPL, int NT>
@@ -767,10 +772,11 @@ __global__ void __launch_bounds__(ARES_THREADS, 1) split_gemm_ares_kernel(SplitG
       if (!mbar_wait(afull, (uint32_t)(uu & 1), err, a.timeout)) break;
       tc_fence_after();
       for (int64_t nt = n0; nt < n1 && ok; ++nt) {
-        for (int kc = 0; kc < a.KC; ++kc, ++tc) {  // chunk tc goes to TMEM buffer tc & 1 (promotion)
+        for (int kc = 0; kc < a.KC; ++kc) {  // promotion period tc (ARES_PROMO chunks) -> TMEM buffer tc & 1
           const int b = (int)(tc & 1);
           const uint32_t use = (uint32_t)(tc >> 1) & 1u;
-          if (!mbar_wait(&tempty[b], use ^ 1u, err, a.timeout)) {
+          const bool pstart = kc % ARES_PROMO == 0, pend = kc % ARES_PROMO == ARES_PROMO - 1 || kc == a.KC - 1;
+          if (pstart && !mbar_wait(&tempty[b], use ^ 1u, err, a.timeout)) {
             ok = false;
             break;
           }
@@ -790,12 +796,15 @@ __global__ void __launch_bounds__(ARES_THREADS, 1) split_gemm_ares_kernel(SplitG
               const bool lead = Pr::a(pr) == 0 && Pr::b(pr) == 0;
               uint64_t ad = smem_desc_sw128(abase + (kc * NPL + Pr::a(pr)) * TILE_BYTES + sub * 32);
               uint64_t bd = smem_desc_sw128(st + Pr::b(pr) * G::B_SUB * G::B_TILE + sub * 32);
-              const bool first = sub == 0 && (lead || pr == 0);
+              const bool first = pstart && sub == 0 && (lead || pr == 0);
               mma_f16(dcol + (lead ? 0u : (uint32_t)NT), ad, bd, IDESC, first ? 0u : 1u);
             }
           }
           mma_commit(&empty[s]);
-          mma_commit(&tfull[b]);
+          if (pend) {
+            mma_commit(&tfull[b]);
+            ++tc;
+          }
           if (++s == STAGES) {
             s = 0;
             ph ^= 1u;
@@ -826,7 +835,7 @@ __global__ void __launch_bounds__(ARES_THREADS, 1) split_gemm_ares_kernel(SplitG
       const bool row_ok = row < a.m_valid;
       for (int64_t nt = n0; nt < n1 && go; ++nt) {
         float run[NH];
-        for (int kc = 0; kc < a.KC; ++kc, ++tc) {
+        for (int kc = 0; kc < a.KC; kc += ARES_PROMO, ++tc) {
           const int b = (int)(tc & 1);
           const uint32_t use = (uint32_t)(tc >> 1) & 1u;
           bool okw = mbar_wait(&tfull[b], use, err, a.timeout);
@@ -949,7 +958,7 @@ int split_gemm(epb_ctx* ctx, int prof_id, const Planes& A, const Planes& B, int6
 // for operands pre-scaled by a power of two into FP16's range; cscale undoes the scale on C.
 int split_gemm_h(epb_ctx* ctx, int prof_id, const Planes& A, const Planes& B, int64_t m_tiles_per_batch,
                  int64_t batches, int64_t m_valid, int64_t n_valid, bool m_fastest, float* C, int64_t c_batch_stride,
-                 int64_t ldc_n, float cscale, bool allow_ares) {
+                 int64_t ldc_n, float cscale, int form /* 1 A-resident when K' <= 256, 0 streamed operands */) {
   SplitGemmArgs a{};
   a.A = A.p;
   a.B = B.p;
@@ -972,7 +981,7 @@ int split_gemm_h(epb_ctx* ctx, int prof_id, const Planes& A, const Planes& B, in
   EPB_CHECK_ARG(B.rows_pad >= a.n_tiles * MX_NT, "FP16x2 GEMM: B planes too small");
   prof_begin(ctx, prof_id);
   int st;
-  if (a.KC <= ARES_KC && allow_ares) {
+  if (a.KC <= ARES_KC && form == 1) {
     // A-resident: a unit is one A tile and n_per_unit column tiles; enough units for ~16 per CTA, at
     // least 8 column tiles per unit (the A copy is then under 1/8 of the unit's traffic)
     const int64_t want = cdiv(16 * (int64_t)ctx->sm_count, std::max<int64_t>(a.m_tiles, 1));
@@ -1896,7 +1905,7 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
         if (recT[p]) EPB_CUDA(cudaStreamWaitEvent(ctx->side, evT[p], 0));
         ctx->stream = ctx->side;
         int st = split_gemm_h(ctx, EPB_PROF_UMMA_KQ, A2i, Bp, rows_pad_k / 128, nki, 2 * nd, nq, false, C2p,
-                              2 * nd * nq, 2 * nd, a2_unscale, ctx->cur_kq_ares != 0);
+                              2 * nd * nq, 2 * nd, a2_unscale, ctx->cur_kq_ares);
         if (st == EPB_OK) st = cudaEventRecord(evK[p], ctx->side) == cudaSuccess ? EPB_OK : EPB_ERR_CUDA;
         ctx->stream = main_stream;
         EPB_TRY(st);
@@ -1955,7 +1964,7 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
         cudaStream_t main_stream = ctx->stream;
         ctx->stream = ctx->side;
         const int st = split_gemm_h(ctx, EPB_PROF_UMMA_KQ, A2i, Bp, rows_pad_k / 128, nki, 2 * nd, nq, false, C2,
-                                    2 * nd * nq, 2 * nd, a2_unscale, ctx->cur_kq_ares != 0);
+                                    2 * nd * nq, 2 * nd, a2_unscale, ctx->cur_kq_ares);
         ctx->stream = main_stream;
         EPB_TRY(st);
         EPB_CUDA(cudaEventRecord(ctx->side_ev[1], ctx->side));
@@ -1965,7 +1974,7 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
         EPB_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->side_ev[1], 0));
       } else {
         EPB_TRY(split_gemm_h(ctx, EPB_PROF_UMMA_KQ, A2i, Bp, rows_pad_k / 128, nki, 2 * nd, nq, false, C2,
-                             2 * nd * nq, 2 * nd, a2_unscale, ctx->cur_kq_ares != 0));
+                             2 * nd * nq, 2 * nd, a2_unscale, ctx->cur_kq_ares));
       }
       // rotations, g2, in-place reduction
       if (!tiled) {

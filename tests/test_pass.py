@@ -56,13 +56,22 @@ def _block_rel_err(s, sr):
     return (num / den).max()
 
 
+def _force_kq_form(ctx, nq, form):
+    """Load a kR->kq GEMM form (0 streamed operands, 1 A tile resident in shared memory) for the
+    mixed pass of nw = 16, nm = 12 and this q count into the context's tuning table."""
+    from epb200 import _lib, pipeline
+
+    _lib.TuneTable(f"pass_kq/16/12/{nq}/{pipeline.PREC_MIXED} {form}\n").import_into(ctx)
+
+
 @pytest.mark.gpu
+@pytest.mark.parametrize("kq", [1, 0])
 @pytest.mark.parametrize("rot", [0, 1])
 @pytest.mark.parametrize("nk,nq,kb", [(5, 64, 2), (3, 200, 3)])
-def test_gpu_pass_mixed(gpu_lib, nk, nq, kb, rot):
+def test_gpu_pass_mixed(gpu_lib, nk, nq, kb, rot, kq):
     """Mixed-precision pass vs the FP64 CPU port: |g|^2 normwise error per (k, q) block <= 1e-5,
     band/q sums <= 1e-6, electron energies (FP64 k side) and phonons at the FP64 level; both rotation
-    kernels (0: warp tensor cores, 1: FP32 CUDA cores)."""
+    kernels (0: warp tensor cores, 1: FP32 CUDA cores) and both kR->kq GEMM forms."""
     from epb200 import pipeline
     from epb200.batched import host
 
@@ -71,10 +80,13 @@ def test_gpu_pass_mixed(gpu_lib, nk, nq, kb, rot):
     xqs = synth.random_kpoints(nq, 6)
     dm = pipeline.DeviceModel(m, mixed=True)
     dm.ctx.set_rotation_variant(rot)
+    _force_kq_form(dm.ctx, nq, kq)
     try:
         r = pipeline.run_eph_over_k_and_q(dm, xks, xqs, prec=pipeline.PREC_MIXED, k_batch=kb, sample_stride=5)
     finally:
         dm.ctx.set_rotation_variant(-1)
+        _force_kq_form(dm.ctx, nq, 1)
+    assert r.kq_form == kq
     ref = cpu_pass.eph_pass_cpu(m, xks, xqs, sample_stride=5)
     np.testing.assert_allclose(host(r.ek), ref["ek"], atol=1e-11 * np.abs(ref["ek"]).max())
     np.testing.assert_allclose(host(r.omega), ref["omega"], rtol=1e-10)
@@ -196,7 +208,7 @@ def config2_full():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("prec", ["fp64", "mixed", "mixed-fp32rot"])
+@pytest.mark.parametrize("prec", ["fp64", "mixed", "mixed-fp32rot", "mixed-kq-streamed"])
 def test_gpu_pass_config2_grids(gpu_lib, config2_full, prec):
     """The pass at the headline configuration's own R grids (the FP16x2 kR->kq pre-scale grows with the Re
     grid, so the small-grid tests above do not cover it): FP64 at the FP64 bars, mixed at |g|^2 <= 1e-5
@@ -207,10 +219,15 @@ def test_gpu_pass_config2_grids(gpu_lib, config2_full, prec):
     dm, xks, xqs, ref = config2_full
     p = pipeline.PREC_FP64 if prec == "fp64" else pipeline.PREC_MIXED
     dm.ctx.set_rotation_variant(1 if prec == "mixed-fp32rot" else 0)
+    kq = 0 if prec == "mixed-kq-streamed" else 1
+    _force_kq_form(dm.ctx, xqs.shape[1], kq)
     try:
         r = pipeline.run_eph_over_k_and_q(dm, xks, xqs, prec=p, k_batch=2, sample_stride=3)
     finally:
         dm.ctx.set_rotation_variant(-1)
+        _force_kq_form(dm.ctx, xqs.shape[1], 1)
+    if p == pipeline.PREC_MIXED:
+        assert r.kq_form == kq
     np.testing.assert_allclose(host(r.ek), ref["ek"], atol=1e-11 * np.abs(ref["ek"]).max())
     np.testing.assert_allclose(host(r.omega), ref["omega"], rtol=1e-10)
     err = _block_rel_err(host(r.g2_sample), ref["g2_sample"])
