@@ -73,6 +73,8 @@ def parse():
                     help="pass workload: load the autotuner's choices from this text table (skips the timing trials)")
     ap.add_argument("--save-tune", default=None, help="pass workload: write the autotuner's choices to this file")
     ap.add_argument("--sample-stride", type=int, default=4096)
+    ap.add_argument("--err-stride", type=int, default=512,
+                    help="pass workload: q stride of the blocks compared against the FP64 pass (untimed runs)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="pass workload: skip the FP64 plain-pass denominator")
@@ -475,18 +477,25 @@ def run_epb(args):
 
 def fp64_denominator(args, torch, pipeline, dm, xk_d, xq_d, r_mixed, ws, n_el, value):
     """Time the plain FP64 GPU pass (FP64 Fourier sums, FP64 Jacobi, FP64 rotations) on the same k and q
-    lists and compare its results with the mixed pass: the sampled |g|^2 blocks (normwise per (k, q)
-    block, and elementwise above 1e-6 of the block maximum), the mode sums g2sum[nu, k] and the energies."""
+    lists and compare the results of both passes on a denser sample (every err_stride-th q, untimed runs):
+    the sampled |g|^2 blocks (normwise per (k, q) block with its tail, and elementwise above floors of the
+    block maximum), the mode sums g2sum[nu, k] and the energies."""
     ctx = dm.ctx
     ctx.set_graph_mode(False)
     s = torch.cuda.current_stream()
     run64 = lambda o: pipeline.run_eph_over_k_and_q(dm, xk_d, xq_d, prec=pipeline.PREC_FP64, k_batch=16,
                                                     sample_stride=args.sample_stride, out=o)
     ctx.profile(True)
-    r64 = run64(None)  # untimed: sizes the FP64 workspace; its per-family profile goes into the line
+    # untimed: sizes the FP64 workspace, gives the per-family profile of the line and the FP64 side of the
+    # accuracy comparison, sampled every err_stride-th q (denser than the timed runs' samples)
+    r64e = pipeline.run_eph_over_k_and_q(dm, xk_d, xq_d, prec=pipeline.PREC_FP64, k_batch=16,
+                                         sample_stride=args.err_stride)
     torch.cuda.synchronize()
     prof64 = {k: round(v[0], 1) for k, v in ctx.profile_read(reset=True).items() if v[1]}
     ctx.profile(False)
+    rme = pipeline.run_eph_over_k_and_q(dm, xk_d, xq_d, prec=pipeline.PREC_MIXED, k_batch=r_mixed.k_batch,
+                                        sample_stride=args.err_stride)
+    r64 = run64(None)
     if ws > 1:
         torch.distributed.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -502,17 +511,23 @@ def fp64_denominator(args, torch, pipeline, dm, xk_d, xq_d, r_mixed, ws, n_el, v
         ms64 = float(t.item())
     v64 = ws * n_el / (ms64 * 1e-3)
     err = {}
-    if r_mixed.g2_sample is not None:
+    if rme.g2_sample is not None:
         # Julia (nw, nw, nm, nsamp, nk) arrays are torch tensors of shape (nk, nsamp, nm, nw, nw): one (k, q)
         # block per row after flattening the first two axes
-        a, b = r_mixed.g2_sample, r64.g2_sample
+        a, b = rme.g2_sample, r64e.g2_sample
         nblk = a.shape[0] * a.shape[1]
         d = (a - b).reshape(nblk, -1)
         bb = b.reshape(nblk, -1)
         blk = torch.linalg.vector_norm(d, dim=1) / torch.linalg.vector_norm(bb, dim=1)
         bmax = bb.abs().amax(dim=1, keepdim=True)
+        srt = torch.sort(blk).values
+        worst = int(blk.argmax())
         err = {"g2_block_normwise_max": float(blk.max()), "g2_block_normwise_median": float(blk.median()),
-               "blocks_compared": int(blk.numel())}
+               "g2_block_normwise_p99": float(srt[int(0.99 * (srt.numel() - 1))]),
+               "g2_block_normwise_p999": float(srt[int(0.999 * (srt.numel() - 1))]),
+               "blocks_above_1e-5": int((blk > 1e-5).sum()), "blocks_compared": int(blk.numel()),
+               "sample_q_stride": args.err_stride,
+               "worst_block_k_q": [worst // a.shape[1], (worst % a.shape[1]) * args.err_stride]}
         # elementwise relative error of the entries above a floor (fraction of their block's largest entry);
         # an entry at the floor f carries the block's absolute error / f, so the figure grows as f falls
         for f in (1e-6, 1e-4, 1e-2):
@@ -520,9 +535,10 @@ def fp64_denominator(args, torch, pipeline, dm, xk_d, xq_d, r_mixed, ws, n_el, v
             elem = torch.where(big, d.abs() / torch.where(big, bb.abs(), torch.ones_like(bb)), torch.zeros_like(bb))
             err[f"g2_elementwise_max_above_{f:g}_floor"] = float(elem.max())
         err["g2_abs_err_max_over_block_max"] = float((d.abs().amax(dim=1, keepdim=True) / bmax).max())
-    err["g2sum_rel_max"] = float(((r_mixed.g2sum - r64.g2sum).abs() / r64.g2sum.abs()).max())
-    err["ek_abs_max_ry"] = float((r_mixed.ek - r64.ek).abs().max())
-    err["omega_abs_max_ry"] = float((r_mixed.omega - r64.omega).abs().max())
+    err["g2sum_rel_max"] = float(((rme.g2sum - r64e.g2sum).abs() / r64e.g2sum.abs()).max())
+    err["ek_abs_max_ry"] = float((rme.ek - r64e.ek).abs().max())
+    err["omega_abs_max_ry"] = float((rme.omega - r64e.omega).abs().max())
+    del rme, r64e
     ctx.set_graph_mode(True)
     # the denominator's own roofline: the pass's algorithmic flops (same count as the mixed pass) against a
     # live cuBLAS DGEMM; its GEMMs are cuBLAS ZGEMMs (csrc/epb_f64blas.cu), as in the reference's GPU path

@@ -893,10 +893,24 @@ __global__ void __launch_bounds__(128, 4) eigh16_refine_c64_kernel(Eigh16Args a)
     for (int r = 0; r < 8; ++r) v[r] = make_float2(v[r].x + u[r].x, v[r].y + u[r].y);
     const double lam = dp + (double)lam_corr;
     int rank = 0;
+    double gmin = 1e300, amax = 0.0;  // smallest gap to another eigenvalue, largest |eigenvalue|
 #pragma unroll
     for (int k = 0; k < E16; ++k) {
       const double lk = __shfl_sync(0xffffffffu, lam, k);
       rank += (k < n) && (lk < lam || (lk == lam && k < l));
+      if (k < n) {
+        amax = fmax(amax, fabs(lk));
+        if (k != l) gmin = fmin(gmin, fabs(lk - lam));
+      }
+    }
+    if (a.gap_count) {
+      // a near-degenerate pair: its eigenvectors turn by the FP32-level error of H over the gap, so the
+      // matrix is listed for the FP64 re-solve
+      for (int o = 8; o > 0; o >>= 1) gmin = fmin(gmin, __shfl_xor_sync(0xffffffffu, gmin, o));
+      if (live && lane == 0 && gmin < (double)a.gap_rel * amax) {
+        const int pos = atomicAdd(a.gap_count, 1);
+        if (pos < a.gap_cap) a.gap_list[pos] = b;
+      }
     }
     if (live && l < n) {
       if (a.E && h == 0) a.E[b * n + rank] = lam;
@@ -988,11 +1002,135 @@ int eigh16_mixed_jacobi(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V3
   return EPB_OK;
 }
 
-int eigh16_mixed_refine(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V32, float2* U) {
+int eigh16_mixed_refine(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V32, float2* U, int64_t* gap_list,
+                        int* gap_count, int gap_cap, float gap_rel) {
   if (batch == 0) return EPB_OK;
   Eigh16Args b = pass_args(ctx, Hp, batch, V32, U);
+  b.gap_list = gap_list;
+  b.gap_count = gap_count;
+  b.gap_cap = gap_cap;
+  b.gap_rel = gap_rel;
   prof_begin(ctx, EPB_PROF_REFINE);
   refine_launch(ctx, b);
+  prof_end(ctx);
+  EPB_LAUNCH_CHECK();
+  return EPB_OK;
+}
+
+// FP64 re-solve of the listed near-degenerate matrices (see eigh16_fixup_launch), a 256-thread block per
+// matrix, thread e owning entry (e % 16, e / 16):
+//  * H(x) in FP64 over the R vectors, eight independent partial sums per thread added in a fixed order (the
+//    loop is bound by L2 latency: one pass over the 3 MB of H(R));
+//  * the refinement's complex64 eigenvectors V as the start: Lowdin orthonormalisation in FP64,
+//    V' = V (I - F / 2), F = V^H V - I (leaves O(F^2) = 1e-14), then W = (H + sigma I) V';
+//  * warp 0 runs the FP64 one-sided Jacobi on the columns of W, which are orthogonal except within the
+//    near-degenerate pairs, so two or three sweeps finish it; the normalised columns are the eigenvectors
+//    (both half-warps on the same matrix, the first writes them sorted).
+constexpr int FIX_RB = 1024, FIX_T = 256;
+__global__ void __launch_bounds__(FIX_T) eigh16_fixup_kernel(const int64_t* __restrict__ list, const int* __restrict__ count,
+                                                             int cap, const double2* __restrict__ ham,
+                                                             const int4* __restrict__ rv, int64_t nr,
+                                                             const double* __restrict__ xk, const double* __restrict__ xq,
+                                                             int64_t nq, float2* __restrict__ U32) {
+  __shared__ double2 ph[FIX_RB];
+  __shared__ double2 Hs[E16 * E16];  // H[i][j] at i + 16 j
+  __shared__ double2 Vs[E16 * E16];  // V[i][l] at i + 16 l
+  __shared__ double2 Fs[E16 * E16];  // F[k][l] at k + 16 l, then W
+  __shared__ double red[FIX_T / 32];
+  const int nfix = min(*count, cap);
+  const int e = threadIdx.x, lane = threadIdx.x & 31, ei = e & 15, el = e >> 4;
+  for (int t = blockIdx.x; t < nfix; t += gridDim.x) {
+    const int64_t b = list[t];
+    const int64_t kb = b / nq, q = b - kb * nq;
+    const double x0 = xk[3 * kb] + xq[3 * q], x1 = xk[3 * kb + 1] + xq[3 * q + 1], x2 = xk[3 * kb + 2] + xq[3 * q + 2];
+    const float2 v32 = U32[b * (E16 * E16) + e];
+    Vs[e] = make_double2(v32.x, v32.y);
+    double2 acc[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) acc[u] = make_double2(0.0, 0.0);
+    for (int64_t r0 = 0; r0 < nr; r0 += FIX_RB) {
+      const int64_t r1 = nr - r0 < FIX_RB ? nr : r0 + FIX_RB;
+      __syncthreads();
+      for (int64_t r = r0 + e; r < r1; r += FIX_T) {
+        const int4 R = rv[r];
+        ph[r - r0] = cis2pi(rdotx(R.x, R.y, R.z, x0, x1, x2));
+      }
+      __syncthreads();
+      int64_t r = r0;
+      for (; r + 7 < r1; r += 8) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) cfma(acc[u], ham[e + (r + u) * (E16 * E16)], ph[r + u - r0]);
+      }
+      for (; r < r1; ++r) cfma(acc[0], ham[e + r * (E16 * E16)], ph[r - r0]);
+    }
+    double2 h = acc[0];
+#pragma unroll
+    for (int u = 1; u < 8; ++u) h = make_double2(h.x + acc[u].x, h.y + acc[u].y);
+    Hs[e] = h;
+    // sigma = 1.1 ||H||_F
+    double f2 = h.x * h.x + h.y * h.y;
+    for (int o = 16; o > 0; o >>= 1) f2 += __shfl_xor_sync(0xffffffffu, f2, o);
+    if (lane == 0) red[e >> 5] = f2;
+    __syncthreads();
+    double hf = 0.0;
+#pragma unroll
+    for (int w = 0; w < FIX_T / 32; ++w) hf += red[w];
+    const double sigma = hf > 0.0 ? 1.1 * sqrt(hf) : 1.0;
+    // F = V^H V - I
+    {
+      double2 g = make_double2(ei == el ? -1.0 : 0.0, 0.0);
+#pragma unroll
+      for (int i = 0; i < E16; ++i) cfma_conj(g, Vs[i + E16 * ei], Vs[i + E16 * el]);
+      Fs[e] = g;
+    }
+    __syncthreads();
+    // V' = V - V F / 2
+    double2 vp = Vs[e];
+    {
+      double2 c = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < E16; ++k) cfma(c, Vs[ei + E16 * k], Fs[k + E16 * el]);
+      vp = make_double2(vp.x - 0.5 * c.x, vp.y - 0.5 * c.y);
+    }
+    __syncthreads();
+    Vs[e] = vp;
+    __syncthreads();
+    // W = (H + sigma I) V'
+    {
+      double2 w = make_double2(sigma * vp.x, sigma * vp.y);
+#pragma unroll
+      for (int j = 0; j < E16; ++j) cfma(w, Hs[ei + E16 * j], Vs[j + E16 * el]);
+      Fs[e] = w;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const int l = lane & 15;
+      double2 col[E16];
+#pragma unroll
+      for (int i = 0; i < E16; ++i) col[i] = Fs[i + E16 * l];
+      onesided_sweeps<double>(col, 1e-15, 30);
+      double nr2 = 0.0;
+#pragma unroll
+      for (int i = 0; i < E16; ++i) nr2 += col[i].x * col[i].x + col[i].y * col[i].y;
+      const double inv = 1.0 / sqrt(nr2);
+      double2 v[E16];
+#pragma unroll
+      for (int i = 0; i < E16; ++i) v[i] = make_double2(col[i].x * inv, col[i].y * inv);
+      Eigh16Args a{};
+      a.U32 = U32;
+      a.n = E16;
+      write_sorted(a, b, lane < 16, lane, l, E16, sqrt(nr2) - sigma, v);
+    }
+    __syncthreads();  // the shared matrices are rewritten for the next matrix
+  }
+}
+
+int eigh16_fixup_launch(epb_ctx* ctx, const int64_t* list, const int* count, int cap, const double2* ham,
+                        const int4* rv, int64_t nr, const double* xk, const double* xq, int64_t nq, float2* U32) {
+  if (cap <= 0) return EPB_OK;
+  const unsigned grid = (unsigned)std::min<int64_t>(cap, (int64_t)ctx->sm_count);
+  prof_begin(ctx, EPB_PROF_REFINE);
+  eigh16_fixup_kernel<<<grid, FIX_T, 0, ctx->stream>>>(list, count, cap, ham, rv, nr, xk, xq, nq, U32);
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;

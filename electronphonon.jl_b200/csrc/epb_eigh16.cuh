@@ -22,8 +22,20 @@ struct Eigh16Args {
   int* flag_count;
   float2* V32;        // FP32 eigenvector workspace between the Jacobi and refinement kernels
   float angle_stop;   // mixed: the FP32 sweeps end after a sweep whose rotation angles all stay below it
+  // complex64 refinement: matrices whose smallest eigenvalue gap is below gap_rel * max |lambda| are listed
+  // (gap_list[0 .. gap_cap), count in *gap_count) for the FP64 re-solve of eigh16_fixup_launch
+  int64_t* gap_list;
+  int* gap_count;
+  int gap_cap;
+  float gap_rel;
 };
 
 int eigh16_launch(epb_ctx* ctx, Eigh16Args& a, bool mixed);
+
+// FP64 re-solve of the matrices listed by the complex64 refinement: H(x) = sum_R H(R) exp(2 pi i R.x) formed
+// in FP64 at x = xk[b / nq] + xq[b % nq] for each listed matrix b, FP64 one-sided Jacobi, the sorted
+// eigenvectors written over U32 (16 x 16 per matrix). The list count is read on the device.
+int eigh16_fixup_launch(epb_ctx* ctx, const int64_t* list, const int* count, int cap, const double2* ham,
+                        const int4* rv, int64_t nr, const double* xk, const double* xq, int64_t nq, float2* U32);
 
 }  // namespace epb

@@ -1743,7 +1743,16 @@ int eigh_async(epb_ctx* ctx, double2* A, int64_t n, int64_t batch, double* E, bo
                int prec);
 int eigh_mixed_packed(epb_ctx* ctx, const float* Hp, int64_t n, int64_t batch, float2* U, double* E);
 int eigh16_mixed_jacobi(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V32);
-int eigh16_mixed_refine(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V32, float2* U);
+int eigh16_mixed_refine(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V32, float2* U, int64_t* gap_list,
+                        int* gap_count, int gap_cap, float gap_rel);
+int eigh16_fixup_launch(epb_ctx* ctx, const int64_t* list, const int* count, int cap, const double2* ham,
+                        const int4* rv, int64_t nr, const double* xk, const double* xq, int64_t nq, float2* U32);
+// Near-degenerate k+q matrices: H(k+q) is formed at the FP32 level (error ~1e-7 of max |lambda|), which turns
+// the eigenvectors of a pair with gap g by about that error over g and so reaches |g|^2 (a pair with a
+// relative gap of 6.5e-4 measured 1.0e-5 per-block |g|^2 error). Matrices whose smallest gap is below
+// PASS_GAP_REL * max |lambda| are listed by the refinement and re-solved from an FP64 H(k+q); the rest then
+// stay under about 3e-6. About 1e-4 of random k+q points fall below the threshold.
+constexpr float PASS_GAP_REL = 2e-3f;
 
 // The whole mixed pass after the q side (omega, u_ph in FP64) has been computed.
 int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const double* xq, int64_t nq,
@@ -1790,7 +1799,10 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
   const bool pipe = tiled && !ctx->prof_on;
   const size_t o_c1b = carve(pipe ? 4 * nw2 * kbi * nq : 0);
   const size_t o_c2b = carve(pipe ? 4 * 2 * nd * kbi * nq : 0);
-  const size_t o_v32 = carve(pipe ? 2 * 8 * nw2 * kbi * nq : 0);
+  const size_t o_v32 = carve(tiled ? (pipe ? 2 : 1) * 8 * nw2 * kbi * nq : 0);
+  // list of the near-degenerate matrices of an inner batch (refinement -> FP64 re-solve) and its count
+  const int gap_cap = (int)std::min<int64_t>(kbi * nq, std::max<int64_t>(4096, kbi * nq / 64));
+  const size_t o_gap = carve(tiled ? 8 * (int64_t)gap_cap + 256 : 0);
   void* ws = nullptr;
   EPB_TRY(ws_get(ctx, EPB_WS_PASS1, off + 1024, &ws));
   uint8_t* base = (uint8_t*)(((uintptr_t)ws + 1023) & ~uintptr_t(1023));
@@ -1917,7 +1929,14 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
         EPB_CUDA(cudaStreamWaitEvent(ctx->tail, evJ[p], 0));
         EPB_CUDA(cudaStreamWaitEvent(ctx->tail, evK[p], 0));
         ctx->stream = ctx->tail;
-        st = eigh16_mixed_refine(ctx, C1p, np, V32p, U32);
+        {
+          int64_t* gl = (int64_t*)(base + o_gap);
+          int* gc = (int*)(base + o_gap + 8 * (size_t)gap_cap);
+          if (cudaMemsetAsync(gc, 0, sizeof(int), ctx->stream) != cudaSuccess) st = EPB_ERR_CUDA;
+          if (st == EPB_OK) st = eigh16_mixed_refine(ctx, C1p, np, V32p, U32, gl, gc, gap_cap, PASS_GAP_REL);
+          if (st == EPB_OK)
+            st = eigh16_fixup_launch(ctx, gl, gc, gap_cap, m->ham, m->rs_el->dev, m->nr_el, xko + 3 * ki, xq, nq, U32);
+        }
         if (st == EPB_OK) st = cudaEventRecord(evR[p], ctx->tail) == cudaSuccess ? EPB_OK : EPB_ERR_CUDA;
         if (st == EPB_OK) {
           if (ctx->cur_rot == 0) {
@@ -1969,7 +1988,17 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
         EPB_TRY(st);
         EPB_CUDA(cudaEventRecord(ctx->side_ev[1], ctx->side));
       }
-      EPB_TRY(eigh_mixed_packed(ctx, C1, nw, np, U32, nullptr));
+      if (tiled) {  // the same solve as the pipeline's: FP32 Jacobi, refinement, FP64 re-solve of near-degenerate
+        float2* V32 = (float2*)(base + o_v32);
+        int64_t* gl = (int64_t*)(base + o_gap);
+        int* gc = (int*)(base + o_gap + 8 * (size_t)gap_cap);
+        EPB_TRY(eigh16_mixed_jacobi(ctx, C1, np, V32));
+        EPB_CUDA(cudaMemsetAsync(gc, 0, sizeof(int), ctx->stream));
+        EPB_TRY(eigh16_mixed_refine(ctx, C1, np, V32, U32, gl, gc, gap_cap, PASS_GAP_REL));
+        EPB_TRY(eigh16_fixup_launch(ctx, gl, gc, gap_cap, m->ham, m->rs_el->dev, m->nr_el, xko + 3 * ki, xq, nq, U32));
+      } else {
+        EPB_TRY(eigh_mixed_packed(ctx, C1, nw, np, U32, nullptr));
+      }
       if (side) {
         EPB_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->side_ev[1], 0));
       } else {
