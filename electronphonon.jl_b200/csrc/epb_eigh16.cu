@@ -1017,22 +1017,67 @@ int eigh16_mixed_refine(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V3
   return EPB_OK;
 }
 
-// FP64 re-solve of the listed near-degenerate matrices (see eigh16_fixup_launch), a 256-thread block per
-// matrix, thread e owning entry (e % 16, e / 16):
-//  * H(x) in FP64 over the R vectors, eight independent partial sums per thread added in a fixed order (the
-//    loop is bound by L2 latency: one pass over the 3 MB of H(R));
+// FP64 H(x) of the listed near-degenerate matrices (see eigh16_fixup_launch): a 1024-thread block per
+// matrix; thread (e, s) adds entry (e % 16, e / 16) over the R vectors r = s mod 4, eight independent
+// partial sums each (the loop is bound by the latency of one pass over the 3 MB of H(R)); the four
+// quarters are added in a fixed order into hbuf[t] (256 complex per listed matrix).
+constexpr int FIX_RB = 1024, FIX_HT = 1024, FIX_T = 256;
+__global__ void __launch_bounds__(FIX_HT) eigh16_fixup_h_kernel(const int64_t* __restrict__ list,
+                                                                const int* __restrict__ count, int cap,
+                                                                const double2* __restrict__ ham,
+                                                                const int4* __restrict__ rv, int64_t nr,
+                                                                const double* __restrict__ xk,
+                                                                const double* __restrict__ xq, int64_t nq,
+                                                                double2* __restrict__ hbuf) {
+  __shared__ double2 ph[FIX_RB];
+  __shared__ double2 Hq[4][E16 * E16];
+  const int nfix = min(*count, cap);
+  const int e = threadIdx.x & 255, sq = threadIdx.x >> 8;
+  for (int t = blockIdx.x; t < nfix; t += gridDim.x) {
+    const int64_t b = list[t];
+    const int64_t kb = b / nq, q = b - kb * nq;
+    const double x0 = xk[3 * kb] + xq[3 * q], x1 = xk[3 * kb + 1] + xq[3 * q + 1], x2 = xk[3 * kb + 2] + xq[3 * q + 2];
+    double2 acc[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) acc[u] = make_double2(0.0, 0.0);
+    for (int64_t r0 = 0; r0 < nr; r0 += FIX_RB) {
+      const int64_t r1 = nr - r0 < FIX_RB ? nr : r0 + FIX_RB;
+      __syncthreads();
+      for (int64_t r = r0 + threadIdx.x; r < r1; r += FIX_HT) {
+        const int4 R = rv[r];
+        ph[r - r0] = cis2pi(rdotx(R.x, R.y, R.z, x0, x1, x2));
+      }
+      __syncthreads();
+      int64_t r = r0 + sq;
+      for (; r + 28 < r1; r += 32) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) cfma(acc[u], ham[e + (r + 4 * u) * (E16 * E16)], ph[r + 4 * u - r0]);
+      }
+      for (; r < r1; r += 4) cfma(acc[0], ham[e + r * (E16 * E16)], ph[r - r0]);
+    }
+    double2 h = acc[0];
+#pragma unroll
+    for (int u = 1; u < 8; ++u) h = make_double2(h.x + acc[u].x, h.y + acc[u].y);
+    Hq[sq][e] = h;
+    __syncthreads();
+    if (sq == 0)
+      hbuf[(int64_t)t * (E16 * E16) + e] =
+          make_double2((Hq[0][e].x + Hq[1][e].x) + (Hq[2][e].x + Hq[3][e].x),
+                       (Hq[0][e].y + Hq[1][e].y) + (Hq[2][e].y + Hq[3][e].y));
+    __syncthreads();  // ph and Hq are rewritten for the next matrix
+  }
+}
+
+// FP64 re-solve of the listed matrices from their FP64 H(x) in hbuf, a 256-thread block per matrix, thread e
+// owning entry (e % 16, e / 16):
 //  * the refinement's complex64 eigenvectors V as the start: Lowdin orthonormalisation in FP64,
 //    V' = V (I - F / 2), F = V^H V - I (leaves O(F^2) = 1e-14), then W = (H + sigma I) V';
 //  * warp 0 runs the FP64 one-sided Jacobi on the columns of W, which are orthogonal except within the
 //    near-degenerate pairs, so two or three sweeps finish it; the normalised columns are the eigenvectors
 //    (both half-warps on the same matrix, the first writes them sorted).
-constexpr int FIX_RB = 1024, FIX_T = 256;
 __global__ void __launch_bounds__(FIX_T) eigh16_fixup_kernel(const int64_t* __restrict__ list, const int* __restrict__ count,
-                                                             int cap, const double2* __restrict__ ham,
-                                                             const int4* __restrict__ rv, int64_t nr,
-                                                             const double* __restrict__ xk, const double* __restrict__ xq,
-                                                             int64_t nq, float2* __restrict__ U32) {
-  __shared__ double2 ph[FIX_RB];
+                                                             int cap, const double2* __restrict__ hbuf,
+                                                             float2* __restrict__ U32) {
   __shared__ double2 Hs[E16 * E16];  // H[i][j] at i + 16 j
   __shared__ double2 Vs[E16 * E16];  // V[i][l] at i + 16 l
   __shared__ double2 Fs[E16 * E16];  // F[k][l] at k + 16 l, then W
@@ -1041,31 +1086,9 @@ __global__ void __launch_bounds__(FIX_T) eigh16_fixup_kernel(const int64_t* __re
   const int e = threadIdx.x, lane = threadIdx.x & 31, ei = e & 15, el = e >> 4;
   for (int t = blockIdx.x; t < nfix; t += gridDim.x) {
     const int64_t b = list[t];
-    const int64_t kb = b / nq, q = b - kb * nq;
-    const double x0 = xk[3 * kb] + xq[3 * q], x1 = xk[3 * kb + 1] + xq[3 * q + 1], x2 = xk[3 * kb + 2] + xq[3 * q + 2];
     const float2 v32 = U32[b * (E16 * E16) + e];
     Vs[e] = make_double2(v32.x, v32.y);
-    double2 acc[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) acc[u] = make_double2(0.0, 0.0);
-    for (int64_t r0 = 0; r0 < nr; r0 += FIX_RB) {
-      const int64_t r1 = nr - r0 < FIX_RB ? nr : r0 + FIX_RB;
-      __syncthreads();
-      for (int64_t r = r0 + e; r < r1; r += FIX_T) {
-        const int4 R = rv[r];
-        ph[r - r0] = cis2pi(rdotx(R.x, R.y, R.z, x0, x1, x2));
-      }
-      __syncthreads();
-      int64_t r = r0;
-      for (; r + 7 < r1; r += 8) {
-#pragma unroll
-        for (int u = 0; u < 8; ++u) cfma(acc[u], ham[e + (r + u) * (E16 * E16)], ph[r + u - r0]);
-      }
-      for (; r < r1; ++r) cfma(acc[0], ham[e + r * (E16 * E16)], ph[r - r0]);
-    }
-    double2 h = acc[0];
-#pragma unroll
-    for (int u = 1; u < 8; ++u) h = make_double2(h.x + acc[u].x, h.y + acc[u].y);
+    const double2 h = hbuf[(int64_t)t * (E16 * E16) + e];
     Hs[e] = h;
     // sigma = 1.1 ||H||_F
     double f2 = h.x * h.x + h.y * h.y;
@@ -1126,11 +1149,14 @@ __global__ void __launch_bounds__(FIX_T) eigh16_fixup_kernel(const int64_t* __re
 }
 
 int eigh16_fixup_launch(epb_ctx* ctx, const int64_t* list, const int* count, int cap, const double2* ham,
-                        const int4* rv, int64_t nr, const double* xk, const double* xq, int64_t nq, float2* U32) {
+                        const int4* rv, int64_t nr, const double* xk, const double* xq, int64_t nq, float2* U32,
+                        double2* hbuf) {
   if (cap <= 0) return EPB_OK;
   const unsigned grid = (unsigned)std::min<int64_t>(cap, (int64_t)ctx->sm_count);
   prof_begin(ctx, EPB_PROF_REFINE);
-  eigh16_fixup_kernel<<<grid, FIX_T, 0, ctx->stream>>>(list, count, cap, ham, rv, nr, xk, xq, nq, U32);
+  eigh16_fixup_h_kernel<<<grid, FIX_HT, 0, ctx->stream>>>(list, count, cap, ham, rv, nr, xk, xq, nq, hbuf);
+  ++ctx->launches;
+  eigh16_fixup_kernel<<<grid, FIX_T, 0, ctx->stream>>>(list, count, cap, hbuf, U32);
   prof_end(ctx);
   EPB_LAUNCH_CHECK();
   return EPB_OK;

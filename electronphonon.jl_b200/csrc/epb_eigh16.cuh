@@ -36,6 +36,7 @@ int eigh16_launch(epb_ctx* ctx, Eigh16Args& a, bool mixed);
 // in FP64 at x = xk[b / nq] + xq[b % nq] for each listed matrix b, FP64 one-sided Jacobi, the sorted
 // eigenvectors written over U32 (16 x 16 per matrix). The list count is read on the device.
 int eigh16_fixup_launch(epb_ctx* ctx, const int64_t* list, const int* count, int cap, const double2* ham,
-                        const int4* rv, int64_t nr, const double* xk, const double* xq, int64_t nq, float2* U32);
+                        const int4* rv, int64_t nr, const double* xk, const double* xq, int64_t nq, float2* U32,
+                        double2* hbuf);
 
 }  // namespace epb

@@ -1746,7 +1746,8 @@ int eigh16_mixed_jacobi(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V3
 int eigh16_mixed_refine(epb_ctx* ctx, const float* Hp, int64_t batch, float2* V32, float2* U, int64_t* gap_list,
                         int* gap_count, int gap_cap, float gap_rel);
 int eigh16_fixup_launch(epb_ctx* ctx, const int64_t* list, const int* count, int cap, const double2* ham,
-                        const int4* rv, int64_t nr, const double* xk, const double* xq, int64_t nq, float2* U32);
+                        const int4* rv, int64_t nr, const double* xk, const double* xq, int64_t nq, float2* U32,
+                        double2* hbuf);
 // Near-degenerate k+q matrices: H(k+q) is formed at the FP32 level (error ~1e-7 of max |lambda|), which turns
 // the eigenvectors of a pair with gap g by about that error over g and so reaches |g|^2 (a pair with a
 // relative gap of 6.5e-4 measured 1.0e-5 per-block |g|^2 error). Matrices whose smallest gap is below
@@ -1803,6 +1804,7 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
   // list of the near-degenerate matrices of an inner batch (refinement -> FP64 re-solve) and its count
   const int gap_cap = (int)std::min<int64_t>(kbi * nq, std::max<int64_t>(4096, kbi * nq / 64));
   const size_t o_gap = carve(tiled ? 8 * (int64_t)gap_cap + 256 : 0);
+  const size_t o_gaph = carve(tiled ? 16 * 256 * (int64_t)gap_cap : 0);  // their FP64 H(k+q), nw = 16
   void* ws = nullptr;
   EPB_TRY(ws_get(ctx, EPB_WS_PASS1, off + 1024, &ws));
   uint8_t* base = (uint8_t*)(((uintptr_t)ws + 1023) & ~uintptr_t(1023));
@@ -1935,7 +1937,8 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
           if (cudaMemsetAsync(gc, 0, sizeof(int), ctx->stream) != cudaSuccess) st = EPB_ERR_CUDA;
           if (st == EPB_OK) st = eigh16_mixed_refine(ctx, C1p, np, V32p, U32, gl, gc, gap_cap, PASS_GAP_REL);
           if (st == EPB_OK)
-            st = eigh16_fixup_launch(ctx, gl, gc, gap_cap, m->ham, m->rs_el->dev, m->nr_el, xko + 3 * ki, xq, nq, U32);
+            st = eigh16_fixup_launch(ctx, gl, gc, gap_cap, m->ham, m->rs_el->dev, m->nr_el, xko + 3 * ki, xq, nq, U32,
+                                     (double2*)(base + o_gaph));
         }
         if (st == EPB_OK) st = cudaEventRecord(evR[p], ctx->tail) == cudaSuccess ? EPB_OK : EPB_ERR_CUDA;
         if (st == EPB_OK) {
@@ -1995,7 +1998,8 @@ int mixed_pass(epb_ctx* ctx, epb_model* m, const double* xk, int64_t nk, const d
         EPB_TRY(eigh16_mixed_jacobi(ctx, C1, np, V32));
         EPB_CUDA(cudaMemsetAsync(gc, 0, sizeof(int), ctx->stream));
         EPB_TRY(eigh16_mixed_refine(ctx, C1, np, V32, U32, gl, gc, gap_cap, PASS_GAP_REL));
-        EPB_TRY(eigh16_fixup_launch(ctx, gl, gc, gap_cap, m->ham, m->rs_el->dev, m->nr_el, xko + 3 * ki, xq, nq, U32));
+        EPB_TRY(eigh16_fixup_launch(ctx, gl, gc, gap_cap, m->ham, m->rs_el->dev, m->nr_el, xko + 3 * ki, xq, nq, U32,
+                                    (double2*)(base + o_gaph)));
       } else {
         EPB_TRY(eigh_mixed_packed(ctx, C1, nw, np, U32, nullptr));
       }
