@@ -905,9 +905,11 @@ __global__ void __launch_bounds__(128, 4) eigh16_refine_c64_kernel(Eigh16Args a)
     }
     if (a.gap_count) {
       // a near-degenerate pair: its eigenvectors turn by the FP32-level error of H over the gap, so the
-      // matrix is listed for the FP64 re-solve
+      // matrix is listed for the FP64 re-solve. Gaps under 1e-6 of max |lambda| are degenerate at the
+      // precision of the data (symmetry-enforced pairs, e.g. Kramers): there the split of |g|^2 between the
+      // pair's bands is a gauge choice in any precision, and such matrices are not listed
       for (int o = 8; o > 0; o >>= 1) gmin = fmin(gmin, __shfl_xor_sync(0xffffffffu, gmin, o));
-      if (live && lane == 0 && gmin < (double)a.gap_rel * amax) {
+      if (live && lane == 0 && gmin < (double)a.gap_rel * amax && gmin >= 1e-6 * amax) {
         const int pos = atomicAdd(a.gap_count, 1);
         if (pos < a.gap_cap) a.gap_list[pos] = b;
       }

@@ -22,8 +22,9 @@ struct Eigh16Args {
   int* flag_count;
   float2* V32;        // FP32 eigenvector workspace between the Jacobi and refinement kernels
   float angle_stop;   // mixed: the FP32 sweeps end after a sweep whose rotation angles all stay below it
-  // complex64 refinement: matrices whose smallest eigenvalue gap is below gap_rel * max |lambda| are listed
-  // (gap_list[0 .. gap_cap), count in *gap_count) for the FP64 re-solve of eigh16_fixup_launch
+  // complex64 refinement: matrices whose smallest eigenvalue gap lies in [1e-6, gap_rel) * max |lambda| are
+  // listed (gap_list[0 .. gap_cap), count in *gap_count) for the FP64 re-solve of eigh16_fixup_launch; a
+  // count above gap_cap leaves the excess with their mixed-precision vectors
   int64_t* gap_list;
   int* gap_count;
   int gap_cap;
